@@ -1,0 +1,89 @@
+/*
+ * Oracle (test infrastructure only; never linked into the product path).
+ * FP64 CPU restatement of the reference's demag + field + LLG + RK4/RKDP54 path.
+ * Every function names the reference file:line it follows. Arrays are AoS
+ * (x, y, z per cell), cells x fastest, then y, then z.
+ */
+#ifndef BORIS_ORACLE_H
+#define BORIS_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_MU0 1.256637061435916e-6   /* BorisLib/Funcs_Math_base.h:9 */
+#define ORC_GAMMA 2.212761569e5        /* BorisLib/Funcs_Math_base.h:16 */
+
+/* module bits (same values as the product's BM_* flags) */
+#define ORC_DEMAG   1
+#define ORC_EXCH    2
+#define ORC_IDMI    4
+#define ORC_ANIUNI  8
+#define ORC_ZEEMAN 16
+
+/* ---- Newell tensor ---- */
+double orc_newell_f(double x, double y, double z);
+double orc_newell_g(double x, double y, double z);
+void orc_selfdemag(double hx, double hy, double hz, double *out3);
+/* far-field expansion of D = -N at normalised offset (x,y,z) for cell (hx,hy,hz): out6 = xx,yy,zz,xy,xz,yz */
+void orc_asymptotic(double hx, double hy, double hz, double x, double y, double z, double *out6);
+/* D = -N on the N grid, same layout as the reference (ref_tensor). */
+int orc_tensor(int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz,
+               double *diag, double *odiag);
+/* octant kernel spectra (Nx/2+1)(Ny/2+1)(Nz/2+1) x 3 each; kodiag = (xy, xz, yz) */
+int orc_kernels(int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz,
+                double *kdiag, double *kodiag);
+
+/* ---- demag convolution ---- */
+typedef struct orc_demag orc_demag;
+orc_demag *orc_demag_create(int nx, int ny, int nz, double hx, double hy, double hz, int Nx, int Ny, int Nz);
+/* H = D * M; if add, H += instead of H =. Returns sum_i M_i . Hdemag_i */
+double orc_demag_apply(orc_demag *d, const double *M, double *H, int add);
+void orc_demag_destroy(orc_demag *d);
+
+/* ---- field terms (add into H) ---- */
+void orc_field_exchange(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
+                        double A, const double *Ms_cell, double *H);
+void orc_field_idmi(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
+                    double A, double D, const double *Ms_cell, double *H);
+void orc_field_aniuni(int n, const double *M, const double *Ms_cell, const double *K1_cell, double K2,
+                      const double *ea, double *H);
+
+/* ---- solver over one or more meshes with a common time step ---- */
+typedef struct {
+    int nx, ny, nz;
+    double hx, hy, hz;
+    double Ms, A, D, alpha, grel, K1, K2;
+    double ea[3];
+    const double *Ms_map;  /* per-cell Ms (absolute), or NULL */
+    const double *K1_map;  /* per-cell K1 (absolute), or NULL */
+    int modules;
+    const double *Ha;      /* 3 * nHa piecewise-constant applied-field samples over [0, Ha_tspan) */
+    int nHa;
+    double Ha_tspan;
+} orc_mesh_desc;
+
+typedef struct {
+    long accepted, rejected, evals;
+    double time, dT, last_lte;
+} orc_stats;
+
+typedef struct orc_solver orc_solver;
+#define ORC_RK4 0
+#define ORC_RKDP54 1
+orc_solver *orc_solver_create(int nmesh, const orc_mesh_desc *desc, int eval, double dt, double tol,
+                              double dT_incr, double dT_min, double dT_max);
+int orc_set_m(orc_solver *s, int mesh, const double *M);
+int orc_get_m(orc_solver *s, int mesh, double *M);
+/* effective field at the current M and time; H has 3n doubles */
+int orc_compute_heff(orc_solver *s, int mesh, double *H);
+/* advance until `steps` more steps are accepted */
+int orc_run(orc_solver *s, int steps, orc_stats *st);
+void orc_solver_destroy(orc_solver *s);
+
+/* FP64 in-place complex DFT (fftw_shim.c) */
+void bm_oracle_fft(int n, double *data, int sign);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
