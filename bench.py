@@ -1,0 +1,310 @@
+"""Benchmark of the B200 micromagnetic step (one JSON line on rank 0).
+
+Workload (default): the large 3D precision configuration — a film of 512 x 512 x 16 cells
+of 2 x 2 x 2 nm (padded FFT 1024 x 1024 x 32), Ms = 1.1e6 A/m, A = 1.5e-11 J/m, uniaxial
+K1 = 5e5 J/m^3 along z, interfacial DMI D = 1.5e-3 J/m^2, alpha = 0.1, initial m = +z with
+seeded 0..15 degree tilts, RKDP54 with relative error tolerance 1e-5, mixed precision
+(FP32 FFTs and stages, FP64 tensor build and error norm). A step is one accepted RKDP54
+step (six field evaluations). Data is synthetic (seeded), built here.
+
+  value      Mcell-steps/s over the timed steps, state resident in HBM (device-event time,
+             max over ranks, aggregate over ranks)
+  e2e        the same metric through the C ABI with host buffers: set M from pinned host
+             memory, run, read M back, all inside the timed region
+  roofline   the dominant kernel's algorithmic bytes per launch / its average launch time
+  cpu_baseline  the reference's own CPU demag convolution (compiled from its sources,
+             oracle/_ref) on a bounded sample: 256 x 256 x 16 cells of the same film,
+             6 H_demag evaluations per step
+
+--impl reference runs that CPU reference arm alone with the same metric and config.
+Multi-GPU: independent replicas, one per rank (the path has no data exchange).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "film3d_512x512x16": dict(n=(512, 512, 16), h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, K1=5e5, D=1.5e-3,
+                              alpha=0.1, modules=1 | 4 | 8 | 16, eval="RKDP54", dt=1e-14, tol=1e-5, init="tilt"),
+    "film2d_128x64": dict(n=(128, 64, 1), h=(5e-9, 5e-9, 3e-9), Ms=8e5, A=1.3e-11, K1=0.0, D=0.0, alpha=0.5,
+                          grel=2.211e5 / 2.212761569e5, modules=1 | 2 | 16, Ha=(1e3, 0, 0), eval="RK4", dt=1e-13,
+                          init="sphere"),
+    "film2d_256x256": dict(n=(256, 256, 1), h=(4e-9, 4e-9, 3e-9), Ms=8e5, A=1.3e-11, K1=1e5, D=0.0, alpha=0.02,
+                           modules=1 | 2 | 8 | 16, Ha=(0, 0, 0), eval="RK4", dt=1e-13, init="sphere"),
+}
+MU0 = 1.256637061435916e-6
+
+
+def init_m(cfg, seed):
+    n = cfg["n"][0] * cfg["n"][1] * cfg["n"][2]
+    rng = np.random.default_rng(seed)
+    if cfg["init"] == "tilt":
+        th = np.deg2rad(rng.uniform(0.0, 15.0, n))
+        ph = rng.uniform(0.0, 2 * np.pi, n)
+        v = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=1)
+    else:
+        v = rng.normal(size=(n, 3))
+        v /= np.linalg.norm(v, axis=1)[:, None]
+    return np.ascontiguousarray(v * cfg["Ms"])
+
+
+def make_ctx(bm, cfg, device, precision):
+    c = bm.Context(device=device, precision=precision)
+    c.add_mesh(cfg["n"], cfg["h"])
+    c.set_material(0, Ms=cfg["Ms"], A=cfg["A"], alpha=cfg["alpha"], grel=cfg.get("grel", 1.0), K1=cfg["K1"],
+                   ea=(0, 0, 1), D=cfg["D"])
+    c.set_modules(0, cfg["modules"])
+    c.set_field(0, cfg.get("Ha", (0, 0, 0)))
+    c.setode(cfg["eval"], cfg["dt"])
+    if cfg["eval"] == "RKDP54":
+        c.astepctrl(cfg["tol"], 2.0, 1e-15, 3e-12)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_reference_rate(cfg, sample_n=(256, 256, 16), evals=2, threads=None):
+    """Mcell-steps/s of the reference's compiled CPU demag (6 evaluations per RKDP54 step)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_libs import reference, dp, P
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    R = reference()
+    if R is None:
+        return None
+    nz = min(sample_n[2], cfg["n"][2])
+    sn = (min(sample_n[0], cfg["n"][0]), min(sample_n[1], cfg["n"][1]), nz)
+    ncell = sn[0] * sn[1] * sn[2]
+    sub = dict(cfg, n=sn)
+    M = np.ascontiguousarray(init_m(sub, 7).reshape(-1))
+    H = np.zeros_like(M)
+    h = R.ref_demag_create(sn[0], sn[1], sn[2], cfg["h"][0], cfg["h"][1], cfg["h"][2])
+    R.ref_demag_eval(P(h), dp(M), dp(H))          # warm-up
+    t0 = time.perf_counter()
+    for _ in range(evals):
+        R.ref_demag_eval(P(h), dp(M), dp(H))
+    dt = (time.perf_counter() - t0) / evals
+    R.ref_demag_destroy(P(h))
+    per_step = 6 if cfg["eval"] == "RKDP54" else 4
+    return {"value": ncell / (per_step * dt) / 1e6, "unit": "Mcell-steps/s", "cores": os.cpu_count(),
+            "kind": "reference",
+            "sample": "reference CPU Convolution<DemagKernel> (project FFTW-API shim) on %dx%dx%d cells of the same film, "
+                      "%d H_demag evaluations, %d per step; other field terms not timed" % (sn + (evals, per_step)),
+            "sec_per_eval": dt}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    import datetime
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, ws, local, dist
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="film3d_512x512x16", choices=sorted(CONFIGS))
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    ncell = cfg["n"][0] * cfg["n"][1] * cfg["n"][2]
+    rank, ws, local, dist = dist_setup()
+    base = {"metric": "Mcell-steps/s", "unit": "Mcell-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "data": "synthetic (seeded initial magnetization, random-init state of the named film)",
+            "config": {"workload": args.config, "cells": list(cfg["n"]), "cellsize_m": list(cfg["h"]),
+                       "evaluation": cfg["eval"], "modules": cfg["modules"], "parallelism": "replicas x%d" % ws,
+                       "l2": "working set above L2 (126 MB) every step"}}
+
+    if args.impl == "reference":
+        if rank != 0:
+            if dist:
+                dist.barrier()
+                dist.destroy_process_group()
+            return
+        vals = []
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_libs import reference, dp, P
+        R = reference()
+        if R is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not present"}))
+            return
+        sn = (256, 256, min(16, cfg["n"][2])) if ncell > 256 * 256 * 16 else cfg["n"]
+        sub = dict(cfg, n=sn)
+        M = np.ascontiguousarray(init_m(sub, 7).reshape(-1))
+        H = np.zeros_like(M)
+        h = R.ref_demag_create(sn[0], sn[1], sn[2], cfg["h"][0], cfg["h"][1], cfg["h"][2])
+        per_step = 6 if cfg["eval"] == "RKDP54" else 4
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            R.ref_demag_eval(P(h), dp(M), dp(H))
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                vals.append(dt * per_step)
+        R.ref_demag_destroy(P(h))
+        nsc = sn[0] * sn[1] * sn[2]
+        tstep = float(np.mean(vals))
+        v = nsc / tstep / 1e6
+        out = dict(base, impl="reference", value=v, ms_per_step=tstep * 1e3, dtype="f64",
+                   cpu_baseline={"value": v, "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                                 "sample": "each step = %d H_demag evaluations of the reference CPU build on %dx%dx%d "
+                                           "cells of the same film (project FFTW-API shim)" % ((per_step,) + tuple(sn))},
+                   e2e={"value": v, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(out))
+        return
+
+    import boris2_b200 as bm
+    prec = bm.MIXED if args.precision == "mixed" else bm.FP64
+    c = make_ctx(bm, cfg, local, prec)
+    M0 = init_m(cfg, 1234 + rank)
+    c.set_m(M0)
+    # warm-up (also builds kernels and the CUDA graph)
+    c.run(args.warmup)
+    c.sync()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    st0 = c.stats()
+    st, ms = c.run_timed(args.steps)
+    clocks = sampler.stop()
+    if dist:
+        import torch
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    steps_done = st["accepted"] - st0["accepted"]
+    value = ncell * steps_done * ws / (ms * 1e-3) / 1e6
+    attempts = st["attempts"] - st0["attempts"]
+    # e2e through the C ABI with host buffers (pinned), copies inside the timed region
+    try:
+        import torch
+        Mpin = torch.from_numpy(M0.reshape(-1).copy()).pin_memory()
+        Mout = torch.empty_like(Mpin).pin_memory()
+        Min_np = Mpin.numpy()
+        Mout_np = Mout.numpy()
+    except Exception:
+        Min_np = M0.reshape(-1).copy()
+        Mout_np = np.empty_like(Min_np)
+    c.sync()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    c.set_m(Min_np)
+    st1 = c.stats()
+    st2 = c.run(args.steps)
+    c.get_m(out=Mout_np)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        import torch
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_steps = st2["accepted"] - st1["accepted"]
+    e2e = ncell * e2e_steps * ws / e2e_s / 1e6
+    # kernel timing for the roofline
+    kms, kbytes = c.time_kernels(0, reps=20)
+    names = ["ymid2d" if cfg["n"][2] == 1 else "yfwd", "zmid", "yinv", "stage"]
+    # dominant kernel: largest share of one field evaluation
+    share = kms.copy()
+    dom = int(np.argmax(share))
+    peak, peak_kind = peaks()
+    achieved = kbytes[dom] / (kms[dom] * 1e-3) / 1e9
+    kpe = c.kernels_per_step()
+    out = dict(base, value=value, ms_per_step=ms / max(steps_done, 1), dtype="f32" if prec == bm.MIXED else "f64",
+               e2e={"value": e2e, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 3 * ncell * 8 / max(e2e_steps, 1),
+                    "d2h_bytes_per_step": 3 * ncell * 8 / max(e2e_steps, 1)},
+               gpu_launches=int(kpe * attempts if cfg["eval"] == "RKDP54" else kpe * steps_done),
+               clocks=clocks,
+               roofline={"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "algorithmic_bytes_per_launch": kbytes[dom],
+                         "launch_ms": kms[dom]},
+               kernels={names[i]: {"ms": kms[i], "GB/s": (kbytes[i] / (kms[i] * 1e-3) / 1e9 if kms[i] > 0 else None)}
+                        for i in range(4) if kms[i] > 0},
+               rkdp={"attempts": attempts, "accepted": steps_done, "dT": st["dT"]})
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_reference_rate(cfg)
+        except Exception as e:  # reported, not fatal
+            out["cpu_baseline"] = {"error": str(e)}
+    c.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

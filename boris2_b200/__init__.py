@@ -1,0 +1,286 @@
+"""boris2_b200 — B200-native micromagnetic field-and-integrate path behind a C ABI.
+
+Python access to ``libboris_b200.so`` (see include/boris_b200.h) through ctypes. The
+names follow the reference's command and module vocabulary:
+
+=====================  ============================================================
+this module            reference (Boris2)
+=====================  ============================================================
+``Context``            SuperMesh + ODECommon (one simulation, one GPU)
+``add_mesh``           a ferromagnetic Mesh with n, h, meshRect
+``set_material``       MeshParams (Ms, A, D, alpha, grel, K1, K2, mcanis_ea1)
+``set_modules``        addmodule / delmodule (demag, exchange, iDMexchange, aniuni, Zeeman)
+``set_field``          Zeeman applied field (setfield / equation)
+``setode``             setode LLG RK4|RKDP54 (Boris/DiffEq_Common.cpp:79)
+``setdt``              setdt (Boris/Commands.cpp:1914)
+``astepctrl``          astepctrl (Boris/Commands.cpp:1931)
+``update_field``       Module::UpdateField / MeshBase::UpdateModules (Heff)
+``demag_field``        Demag::UpdateField (Boris/Demag.cpp:170)
+``run``                AdvanceTime over ODECommon_Base::Iterate
+=====================  ============================================================
+
+Errors from the library raise :class:`BorisError` with the library's message, the
+equivalent of the reference's BError return values. There is no CPU fallback: if the
+CUDA library is missing or no GPU is present, loading or creating a context fails.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libboris_b200.so")
+
+DEMAG, EXCH, IDMI, ANIUNI, ZEEMAN = 1, 2, 4, 8, 16
+RK4, RKDP54 = 0, 1
+FP64, MIXED = 0, 1
+
+_lib = None
+
+
+class BorisError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("accepted", ctypes.c_longlong), ("rejected", ctypes.c_longlong),
+                ("attempts", ctypes.c_longlong), ("time", ctypes.c_double),
+                ("dT", ctypes.c_double), ("last_lte", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+_SIGS = {
+    "bm_create": (_I, [_I, ctypes.POINTER(_P)]),
+    "bm_destroy": (_I, [_P]),
+    "bm_last_error": (ctypes.c_char_p, []),
+    "bm_version": (_I, []),
+    "bm_add_mesh": (_I, [_P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _IP]),
+    "bm_set_material": (_I, [_P, _I, _D, _D, _D, _D, _D, _D, _DP, _D]),
+    "bm_set_material_maps": (_I, [_P, _I, _DP, _DP]),
+    "bm_set_modules": (_I, [_P, _I, _I]),
+    "bm_set_field": (_I, [_P, _I, _DP, _I, _D]),
+    "bm_set_ode": (_I, [_P, _I, _D]),
+    "bm_set_astepctrl": (_I, [_P, _D, _D, _D, _D]),
+    "bm_set_precision": (_I, [_P, _I]),
+    "bm_set_m": (_I, [_P, _I, _DP]),
+    "bm_get_m": (_I, [_P, _I, _DP]),
+    "bm_compute_hdemag": (_I, [_P, _I, _DP, _DP]),
+    "bm_compute_heff": (_I, [_P, _I, _DP]),
+    "bm_run": (_I, [_P, _I, ctypes.POINTER(Stats)]),
+    "bm_get_stats": (_I, [_P, ctypes.POINTER(Stats)]),
+    "bm_mesh_info": (_I, [_P, _I, _IP, _IP]),
+    "bm_device_m": (_I, [_P, _I, ctypes.POINTER(_P), _IP]),
+    "bm_sync": (_I, [_P]),
+    "bm_kernels_per_step": (_I, [_P, _IP]),
+    "bm_run_timed": (_I, [_P, _I, ctypes.POINTER(Stats), _DP]),
+    "bm_time_kernels": (_I, [_P, _I, _I, _DP, _DP]),
+    "bm_debug_kernels": (_I, [_P, _I, _DP]),
+    "bm_debug_tensor": (_I, [_I, _I, _I, _I, _D, _D, _D, _DP]),
+    "bm_debug_fft": (_I, [_I, _I, _I, _I, _I, _DP]),
+}
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise BorisError("libboris_b200.so not built (run boris2_b200/build.py): %s" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise BorisError("boris_b200 error %d: %s" % (rc, lib().bm_last_error().decode()))
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _vec(a, n):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+    if a.size != 3 * n:
+        raise ValueError("expected %d values (3 per cell), got %d" % (3 * n, a.size))
+    return a
+
+
+class Context:
+    """One simulation on one GPU (SuperMesh + ODE solver of the reference)."""
+
+    def __init__(self, device=0, precision=MIXED):
+        self._h = _P()
+        _check(lib().bm_create(int(device), ctypes.byref(self._h)))
+        self.meshes = []
+        _check(lib().bm_set_precision(self._h, int(precision)))
+
+    def close(self):
+        if self._h:
+            lib().bm_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------------ meshes
+    def add_mesh(self, n, h, origin=(0.0, 0.0, 0.0)):
+        mid = _I()
+        _check(lib().bm_add_mesh(self._h, int(n[0]), int(n[1]), int(n[2]), float(h[0]), float(h[1]),
+                                 float(h[2]), float(origin[0]), float(origin[1]), float(origin[2]),
+                                 ctypes.byref(mid)))
+        self.meshes.append((tuple(int(v) for v in n), tuple(float(v) for v in h)))
+        return mid.value
+
+    def ncells(self, mesh=0):
+        n = self.meshes[mesh][0]
+        return n[0] * n[1] * n[2]
+
+    def set_material(self, mesh=0, Ms=8e5, A=1.3e-11, alpha=0.5, grel=1.0, K1=0.0, K2=0.0,
+                     ea=(0.0, 0.0, 1.0), D=0.0):
+        e = np.asarray(ea, dtype=np.float64)
+        _check(lib().bm_set_material(self._h, mesh, Ms, A, alpha, grel, K1, K2, _dp(e), D))
+
+    def set_material_maps(self, mesh=0, Ms_map=None, K1_map=None):
+        n = self.ncells(mesh)
+        a = None if Ms_map is None else np.ascontiguousarray(np.asarray(Ms_map, dtype=np.float64).reshape(n))
+        b = None if K1_map is None else np.ascontiguousarray(np.asarray(K1_map, dtype=np.float64).reshape(n))
+        _check(lib().bm_set_material_maps(self._h, mesh, None if a is None else _dp(a), None if b is None else _dp(b)))
+
+    def set_modules(self, mesh=0, modules=DEMAG | EXCH | ZEEMAN):
+        _check(lib().bm_set_modules(self._h, mesh, int(modules)))
+
+    def set_field(self, mesh=0, Ha=(0.0, 0.0, 0.0), t_span=0.0):
+        a = np.ascontiguousarray(np.asarray(Ha, dtype=np.float64).reshape(-1, 3))
+        _check(lib().bm_set_field(self._h, mesh, _dp(a), a.shape[0], float(t_span)))
+
+    def set_precision(self, precision):
+        _check(lib().bm_set_precision(self._h, int(precision)))
+
+    # ------------------------------------------------------------------ ODE
+    def setode(self, evaluation="RK4", dt=None):
+        ev = {"RK4": RK4, "RKDP54": RKDP54}[evaluation] if isinstance(evaluation, str) else int(evaluation)
+        if dt is None:
+            dt = 1e-13 if ev == RK4 else 0.5e-12   # Boris/DiffEq_Defs.h defaults
+        self._eval = ev
+        _check(lib().bm_set_ode(self._h, ev, float(dt)))
+
+    def setdt(self, dt):
+        _check(lib().bm_set_ode(self._h, getattr(self, "_eval", RK4), float(dt)))
+
+    def astepctrl(self, err_fail, dT_incr, dT_min, dT_max):
+        _check(lib().bm_set_astepctrl(self._h, float(err_fail), float(dT_incr), float(dT_min), float(dT_max)))
+
+    # ------------------------------------------------------------------ state
+    def set_m(self, M, mesh=0):
+        a = _vec(M, self.ncells(mesh))
+        _check(lib().bm_set_m(self._h, mesh, _dp(a)))
+
+    def get_m(self, mesh=0, out=None):
+        n = self.ncells(mesh)
+        out = np.empty(3 * n) if out is None else out
+        _check(lib().bm_get_m(self._h, mesh, _dp(out)))
+        return out.reshape(n, 3)
+
+    def demag_field(self, mesh=0, with_energy=False):
+        n = self.ncells(mesh)
+        H = np.empty(3 * n)
+        e = ctypes.c_double(0.0)
+        _check(lib().bm_compute_hdemag(self._h, mesh, _dp(H), ctypes.byref(e)))
+        return (H.reshape(n, 3), e.value) if with_energy else H.reshape(n, 3)
+
+    def update_field(self, mesh=0):
+        n = self.ncells(mesh)
+        H = np.empty(3 * n)
+        _check(lib().bm_compute_heff(self._h, mesh, _dp(H)))
+        return H.reshape(n, 3)
+
+    def run(self, steps):
+        st = Stats()
+        _check(lib().bm_run(self._h, int(steps), ctypes.byref(st)))
+        return st.as_dict()
+
+    def run_timed(self, steps):
+        """Run and return (stats, device milliseconds measured on the library's stream)."""
+        st = Stats()
+        ms = ctypes.c_double(0.0)
+        _check(lib().bm_run_timed(self._h, int(steps), ctypes.byref(st), ctypes.byref(ms)))
+        return st.as_dict(), ms.value
+
+    def time_kernels(self, mesh=0, reps=20):
+        """Average ms per launch and algorithmic bytes of each kernel of one field evaluation:
+        [y pass / ymid2d, zmid, yinv, stage]."""
+        ms = np.zeros(4)
+        by = np.zeros(4)
+        _check(lib().bm_time_kernels(self._h, mesh, int(reps), _dp(ms), _dp(by)))
+        return ms, by
+
+    def stats(self):
+        st = Stats()
+        _check(lib().bm_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def fft_sizes(self, mesh=0):
+        n3 = (ctypes.c_int * 3)()
+        N3 = (ctypes.c_int * 3)()
+        _check(lib().bm_mesh_info(self._h, mesh, n3, N3))
+        return tuple(N3)
+
+    def device_m(self, mesh=0):
+        p = _P()
+        eb = _I()
+        _check(lib().bm_device_m(self._h, mesh, ctypes.byref(p), ctypes.byref(eb)))
+        return p.value, eb.value
+
+    def sync(self):
+        _check(lib().bm_sync(self._h))
+
+    def kernels_per_step(self):
+        c = _I()
+        _check(lib().bm_kernels_per_step(self._h, ctypes.byref(c)))
+        return c.value
+
+    def debug_kernels(self, mesh=0):
+        N = self.fft_sizes(mesh)
+        nk = (N[0] // 2 + 1) * (N[1] // 2 + 1) * (N[2] // 2 + 1)
+        K = np.empty(6 * nk)
+        _check(lib().bm_debug_kernels(self._h, mesh, _dp(K)))
+        return K.reshape(6, N[2] // 2 + 1, N[1] // 2 + 1, N[0] // 2 + 1)
+
+
+def debug_tensor(n, h, device=0):
+    oct6 = np.empty(6 * n[0] * n[1] * n[2])
+    _check(lib().bm_debug_tensor(device, int(n[0]), int(n[1]), int(n[2]), float(h[0]), float(h[1]), float(h[2]), _dp(oct6)))
+    return oct6.reshape(n[2], n[1], n[0], 6)
+
+
+def debug_fft(x, precision=FP64, inverse=False, device=0):
+    """Batched 1D complex FFT along the last axis on the GPU (unnormalised)."""
+    x = np.asarray(x, dtype=np.complex128)
+    L = x.shape[-1]
+    flat = np.ascontiguousarray(x.reshape(-1, L))
+    buf = np.ascontiguousarray(flat.view(np.float64).reshape(-1))
+    _check(lib().bm_debug_fft(device, L, flat.shape[0], int(precision), int(bool(inverse)), _dp(buf)))
+    return buf.view(np.complex128).reshape(x.shape)

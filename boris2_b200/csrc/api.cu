@@ -1,0 +1,1111 @@
+// Host runtime behind the C ABI (include/boris_b200.h): contexts, meshes, device buffers,
+// kernel-spectrum build, step sequencing and CUDA-graph replay.
+//
+// Step structure (per mesh, per effective-field evaluation):
+//   [stage kernel of the previous evaluation wrote S1 = x-FFT(M_stage)]
+//   2D: ymid2d            3D: yfwd -> zmid -> yinv
+//   stage kernel: inverse x FFT -> Heff -> LLG -> stage update -> x-FFT of the new M
+// RK4 (Boris/DiffEqFM_Evals_RK4.cpp): 4 evaluations per step, the last one finishes the step.
+// RKDP54 (Boris/DiffEqFM_Evals_RKDP54.cpp, DiffEq_CommonBase_Iterate.cpp:1214): one attempt =
+//   [restore if the previous attempt was rejected] -> evaluation 0 (FSAL rhs, FP64 error norm,
+//   step controller in the last block) -> advance -> evaluations 1..5 (skipped on reject).
+// The step controller runs on the device, so a bm_run of many steps needs no host round trip
+// except one read of the accepted-step counter per batch of graph launches.
+#include "../../include/boris_b200.h"
+#include "kernels.h"
+#include "util.h"
+#include <vector>
+#include <string>
+#include <cmath>
+#include <cstring>
+#include <cstdio>
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(BM_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKL(rc, what)                                                                             \
+    do {                                                                                          \
+        int r_ = (rc);                                                                            \
+        if (r_) return fail(BM_ECUDA, std::string(what) + " launch failed (" + std::to_string(r_) + "): " + \
+                                          cudaGetErrorString(cudaGetLastError()));                \
+    } while (0)
+
+// smallest 2^p or 3*2^p >= n
+int nice_size(int n)
+{
+    int best = 1;
+    while (best < n) best *= 2;
+    for (int t = 3; t < best; t *= 2)
+        if (t >= n) { best = t; break; }
+    return best;
+}
+
+struct Mesh {
+    int nx = 0, ny = 0, nz = 0;
+    double h[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+    double Ms = 8e5, A = 1.3e-11, D = 0.0, alpha = 0.5, grel = 1.0, K1 = 0.0, K2 = 0.0;
+    double ea[3] = {0, 0, 1};
+    std::vector<double> Ms_map, K1_map;
+    int modules = BM_DEMAG | BM_EXCH | BM_ZEEMAN;
+    std::vector<double> Ha{0.0, 0.0, 0.0};
+    double Ha_tspan = 0.0;
+    std::vector<double> M0;     // host copy of M until the device is ready
+    // derived
+    long long n = 0;
+    int Nx = 1, Ny = 1, Nz = 1, LX = 1;
+    FFTPlan px, py, pz;
+    int W2 = 1, Wy = 1, Wz = 1, rpb = 1;
+    // device (element type depends on the context precision)
+    void *buf[4] = {nullptr, nullptr, nullptr, nullptr};   // A (M), P (sM1), B, C
+    void *ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    void *S1 = nullptr, *S2 = nullptr, *K = nullptr;
+    void *twx = nullptr, *twx2 = nullptr, *twy = nullptr, *twz = nullptr;
+    void *Msd = nullptr, *K1d = nullptr, *Hout = nullptr;
+    double *Had = nullptr, *stage64 = nullptr;
+    int nHa = 1;
+};
+
+}  // namespace
+
+struct bm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int precision = BM_MIXED;
+    int eval = BM_RK4;
+    double dt = 1e-13;
+    double tol = 1e-4, dT_incr = 2.0, dT_min = 1e-15, dT_max = 3e-12;
+    std::vector<Mesh> meshes;
+    StepState *st = nullptr;
+    bool ready = false;
+    bool s1_dirty = true;
+    bool state_dirty = true;   // host-side step parameters need upload
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    int graph_eval = -1;
+    bool eval_chosen = false;
+    int kernels_per_step = 0;
+    double *farq = nullptr;
+    StepState host_st;
+};
+
+namespace {
+
+template <typename T> size_t esz() { return sizeof(T); }
+
+void free_mesh(Mesh &m)
+{
+    for (auto &p : m.buf) { if (p) cudaFree(p); p = nullptr; }
+    for (auto &p : m.ev) { if (p) cudaFree(p); p = nullptr; }
+    void **ps[] = {&m.S1, &m.S2, &m.K, &m.twx, &m.twx2, &m.twy, &m.twz, &m.Msd, &m.K1d, &m.Hout};
+    for (auto pp : ps) { if (*pp) cudaFree(*pp); *pp = nullptr; }
+    if (m.Had) cudaFree(m.Had);
+    m.Had = nullptr;
+    if (m.stage64) cudaFree(m.stage64);
+    m.stage64 = nullptr;
+}
+
+void drop_graph(bm_ctx *c)
+{
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
+    c->graph_eval = -1;
+}
+
+void unprepare(bm_ctx *c)
+{
+    if (!c->ready) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    drop_graph(c);
+    // keep the current M on the host
+    for (auto &m : c->meshes) {
+        if (m.buf[0]) {
+            std::vector<double> tmp(3 * (size_t)m.n);
+            double *d = nullptr;
+            if (cudaMalloc(&d, sizeof(double) * 3 * m.n) == cudaSuccess) {
+                if (c->precision == BM_FP64) launch_planes_to_aos<double>(d, (double *)m.buf[0], m.n, c->stream);
+                else launch_planes_to_aos<float>(d, (float *)m.buf[0], m.n, c->stream);
+                cudaMemcpyAsync(tmp.data(), d, sizeof(double) * 3 * m.n, cudaMemcpyDeviceToHost, c->stream);
+                cudaStreamSynchronize(c->stream);
+                cudaFree(d);
+                m.M0 = tmp;
+            }
+        }
+        free_mesh(m);
+    }
+    c->ready = false;
+    c->s1_dirty = true;
+}
+
+template <typename T>
+int upload_table(void **dst, int L, bool fp64_only, cudaStream_t s)
+{
+    std::vector<double> tw(2 * (size_t)L);
+    for (int m = 0; m < L; m++) {
+        long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)L;
+        tw[2 * m] = (double)cosl(a);
+        tw[2 * m + 1] = (double)-sinl(a);
+    }
+    size_t bytes = (fp64_only ? sizeof(double) : sizeof(T)) * 2 * (size_t)L;
+    if (cudaMalloc(dst, bytes) != cudaSuccess) return fail(BM_ENOMEM, "twiddle table allocation failed");
+    if (fp64_only || sizeof(T) == sizeof(double)) {
+        if (cudaMemcpyAsync(*dst, tw.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return fail(BM_ECUDA, "twiddle upload");
+    } else {
+        std::vector<float> f(2 * (size_t)L);
+        for (size_t i = 0; i < f.size(); i++) f[i] = (float)tw[i];
+        if (cudaMemcpyAsync(*dst, f.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return fail(BM_ECUDA, "twiddle upload");
+        cudaStreamSynchronize(s);
+    }
+    cudaStreamSynchronize(s);
+    return 0;
+}
+
+int pow2_floor(int v)
+{
+    int p = 1;
+    while (p * 2 <= v) p *= 2;
+    return p;
+}
+
+template <typename T>
+void choose_tiles(Mesh &m)
+{
+    const size_t cs = sizeof(cpx<T>);
+    const int lim = bm_lb<T>::v;
+    // 2D y pass: 3 components per block, transformed one after another
+    {
+        int W = 16;
+        while (W > 1 && ((size_t)3 * m.Ny * W * cs > 100 * 1024 || W * m.py.tpl > lim)) W /= 2;
+        if (W > m.LX) W = pow2_floor(m.LX);
+        m.W2 = W;
+    }
+    // 3D y passes
+    {
+        int W = 16;
+        while (W > 1 && ((size_t)m.Ny * W * cs > 100 * 1024 || W * m.py.tpl > lim)) W /= 2;
+        if (W > m.LX) W = pow2_floor(m.LX);
+        m.Wy = W;
+    }
+    // 3D z pass: two mirror pencils in parallel, components one after another
+    {
+        int W = 64;
+        while (W > 1 && ((size_t)6 * m.Nz * W * cs > 100 * 1024 || 2 * W * m.pz.tpl > lim)) W /= 2;
+        if (W > m.LX) W = pow2_floor(m.LX);
+        m.Wz = W;
+    }
+    // stage kernel rows per block
+    {
+        int tpl = m.px.tpl;
+        int rpb = lim / (3 * tpl);
+        if (rpb < 1) rpb = 1;
+        while (rpb > 1 && (size_t)3 * rpb * padded_len(m.LX) * cs > 64 * 1024) rpb--;
+        int rows = m.ny * m.nz;
+        if (rpb > rows) rpb = rows;
+        m.rpb = rpb;
+    }
+}
+
+template <typename T>
+int prepare_mesh(bm_ctx *c, Mesh &m)
+{
+    cudaStream_t s = c->stream;
+    m.n = (long long)m.nx * m.ny * m.nz;
+    m.Nx = 2 * nice_size(m.nx);
+    m.Ny = 2 * nice_size(m.ny);
+    m.Nz = m.nz > 1 ? 2 * nice_size(m.nz) : 1;
+    m.LX = m.Nx / 2;
+    if (!bm_make_plan(m.LX, m.px) || !bm_make_plan(m.Ny, m.py) || !bm_make_plan(m.Nz, m.pz))
+        return fail(BM_EUNSUPPORTED, "unsupported FFT size");
+    choose_tiles<T>(m);
+    size_t v3 = sizeof(T) * 3 * (size_t)m.n;
+    int nbuf = (c->eval == BM_RKDP54) ? 4 : 4;
+    int nev = (c->eval == BM_RKDP54) ? 6 : 3;
+    for (int i = 0; i < nbuf; i++) {
+        if (cudaMalloc(&m.buf[i], v3) != cudaSuccess) return fail(BM_ENOMEM, "M buffers");
+        cudaMemsetAsync(m.buf[i], 0, v3, s);
+    }
+    for (int i = 0; i < nev; i++) {
+        if (cudaMalloc(&m.ev[i], v3) != cudaSuccess) return fail(BM_ENOMEM, "stage buffers");
+        cudaMemsetAsync(m.ev[i], 0, v3, s);
+    }
+    if (cudaMalloc(&m.Hout, v3) != cudaSuccess) return fail(BM_ENOMEM, "H buffer");
+    if (cudaMalloc(&m.stage64, sizeof(double) * 3 * m.n) != cudaSuccess) return fail(BM_ENOMEM, "staging buffer");
+    if (m.modules & BM_DEMAG) {
+        size_t s1 = sizeof(cpx<T>) * 3 * (size_t)m.nz * m.ny * m.LX;
+        if (cudaMalloc(&m.S1, s1) != cudaSuccess) return fail(BM_ENOMEM, "S1");
+        cudaMemsetAsync(m.S1, 0, s1, s);
+        if (m.nz > 1) {
+            size_t s2 = sizeof(cpx<T>) * 3 * (size_t)m.nz * m.Ny * m.LX;
+            if (cudaMalloc(&m.S2, s2) != cudaSuccess) return fail(BM_ENOMEM, "S2");
+        }
+        size_t nk = (size_t)(m.Nx / 2 + 1) * (m.Ny / 2 + 1) * (m.Nz / 2 + 1);
+        if (cudaMalloc(&m.K, sizeof(T) * 6 * nk) != cudaSuccess) return fail(BM_ENOMEM, "kernel spectra");
+        int rc;
+        if ((rc = upload_table<T>(&m.twx, m.LX, false, s))) return rc;
+        if ((rc = upload_table<T>(&m.twx2, m.Nx, false, s))) return rc;
+        if ((rc = upload_table<T>(&m.twy, m.Ny, false, s))) return rc;
+        if ((rc = upload_table<T>(&m.twz, m.Nz, false, s))) return rc;
+        void *tx = nullptr, *ty = nullptr, *tz = nullptr;
+        if ((rc = upload_table<double>(&tx, m.Nx, true, s))) return rc;
+        if ((rc = upload_table<double>(&ty, m.Ny, true, s))) return rc;
+        if ((rc = upload_table<double>(&tz, m.Nz, true, s))) return rc;
+        double hm = std::fmax(m.h[0], std::fmax(m.h[1], m.h[2]));
+        std::vector<double> fq(6 * BM_FARQ_PER_COMP);
+        bm_far_coeffs(m.h[0] / hm, m.h[1] / hm, m.h[2] / hm, fq.data());
+        CK(cudaMemcpyAsync(c->farq, fq.data(), sizeof(double) * fq.size(), cudaMemcpyHostToDevice, s));
+        rc = build_kernels_device<T>((T *)m.K, m.nx, m.ny, m.nz, m.Nx, m.Ny, m.Nz, m.h[0], m.h[1], m.h[2], c->farq,
+                                     (const cpx<double> *)tx, (const cpx<double> *)ty, (const cpx<double> *)tz, s);
+        cudaFree(tx); cudaFree(ty); cudaFree(tz);
+        if (rc) return fail(BM_ECUDA, "kernel build failed (" + std::to_string(rc) + ")");
+    }
+    // material maps
+    if (!m.Ms_map.empty()) {
+        if (cudaMalloc(&m.Msd, sizeof(T) * m.n) != cudaSuccess) return fail(BM_ENOMEM, "Ms map");
+        CK(cudaMemcpyAsync(m.stage64, m.Ms_map.data(), sizeof(double) * m.n, cudaMemcpyHostToDevice, s));
+        CKL(launch_convert<T>((T *)m.Msd, m.stage64, m.n, s), "convert");
+    }
+    if (!m.K1_map.empty()) {
+        if (cudaMalloc(&m.K1d, sizeof(T) * m.n) != cudaSuccess) return fail(BM_ENOMEM, "K1 map");
+        CK(cudaStreamSynchronize(s));
+        CK(cudaMemcpyAsync(m.stage64, m.K1_map.data(), sizeof(double) * m.n, cudaMemcpyHostToDevice, s));
+        CKL(launch_convert<T>((T *)m.K1d, m.stage64, m.n, s), "convert");
+    }
+    m.nHa = (int)(m.Ha.size() / 3);
+    if (cudaMalloc(&m.Had, sizeof(double) * m.Ha.size()) != cudaSuccess) return fail(BM_ENOMEM, "Ha");
+    CK(cudaMemcpyAsync(m.Had, m.Ha.data(), sizeof(double) * m.Ha.size(), cudaMemcpyHostToDevice, s));
+    // initial M
+    CK(cudaStreamSynchronize(s));
+    if (m.M0.size() == 3 * (size_t)m.n) {
+        CK(cudaMemcpyAsync(m.stage64, m.M0.data(), sizeof(double) * 3 * m.n, cudaMemcpyHostToDevice, s));
+        CKL(launch_aos_to_planes<T>((T *)m.buf[0], m.stage64, m.n, s), "aos_to_planes");
+    }
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int upload_state(bm_ctx *c)
+{
+    StepState &h = c->host_st;
+    h.dT = c->dt;
+    h.tol = c->tol;
+    h.dT_incr = c->dT_incr;
+    h.dT_min = c->dT_min;
+    h.dT_max = c->dT_max;
+    h.eval_order = (c->eval == BM_RKDP54) ? 5 : 4;
+    h.reject_flag = 0;
+    h.need_restore = 0;
+    h.lte_bits = 0;
+    h.blocks_done = 0;
+    CK(cudaMemcpyAsync(c->st, &h, sizeof(StepState), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->state_dirty = false;
+    return 0;
+}
+
+int read_state(bm_ctx *c)
+{
+    CK(cudaMemcpyAsync(&c->host_st, c->st, sizeof(StepState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+template <typename T>
+int prepare_T(bm_ctx *c)
+{
+    for (auto &m : c->meshes) {
+        int rc = prepare_mesh<T>(c, m);
+        if (rc) { for (auto &mm : c->meshes) free_mesh(mm); return rc; }
+    }
+    return 0;
+}
+
+int prepare(bm_ctx *c)
+{
+    if (c->ready) return 0;
+    if (c->meshes.empty()) return fail(BM_ESTATE, "no mesh");
+    CK(cudaSetDevice(c->device));
+    int rc = (c->precision == BM_FP64) ? prepare_T<double>(c) : prepare_T<float>(c);
+    if (rc) return rc;
+    c->ready = true;
+    c->s1_dirty = true;
+    return upload_state(c);
+}
+
+// ------------------------------------------------------------------ kernel argument builders
+template <typename T>
+YZArgs<T> yz_args(bm_ctx *c, Mesh &m, int gate)
+{
+    YZArgs<T> a;
+    a.S1 = (cpx<T> *)m.S1; a.S2 = (cpx<T> *)m.S2; a.K = (const T *)m.K;
+    a.twy = (const cpx<T> *)m.twy; a.twz = (const cpx<T> *)m.twz;
+    a.py = m.py; a.pz = m.pz;
+    a.nx = m.nx; a.ny = m.ny; a.nz = m.nz; a.LX = m.LX; a.Ny = m.Ny; a.Nz = m.Nz;
+    a.W = m.nz > 1 ? m.Wy : m.W2;
+    a.st = c->st; a.gate = gate;
+    return a;
+}
+
+template <typename T>
+int enqueue_yz(bm_ctx *c, Mesh &m, int gate, int *count)
+{
+    if (!(m.modules & BM_DEMAG)) return 0;
+    YZArgs<T> a = yz_args<T>(c, m, gate);
+    if (m.nz == 1) {
+        CKL(launch_ymid2d<T>(a, c->stream), "ymid2d");
+        (*count)++;
+    } else {
+        CKL(launch_yfwd<T>(a, c->stream), "yfwd");
+        a.W = m.Wz;
+        CKL(launch_zmid<T>(a, c->stream), "zmid");
+        a.W = m.Wy;
+        CKL(launch_yinv<T>(a, c->stream), "yinv");
+        (*count) += 3;
+    }
+    return 0;
+}
+
+template <typename T>
+StageArgs<T> stage_args(bm_ctx *c, Mesh &m)
+{
+    StageArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.nx = m.nx; a.ny = m.ny; a.nz = m.nz; a.LX = m.LX; a.Nx = m.Nx;
+    a.hx = m.h[0]; a.hy = m.h[1]; a.hz = m.h[2];
+    a.S1 = (cpx<T> *)m.S1;
+    a.twx = (const cpx<T> *)m.twx; a.twx2 = (const cpx<T> *)m.twx2;
+    a.px = m.px;
+    a.rpb = m.rpb;
+    a.scale = (T)(2.0 / ((double)m.Nx * m.Ny * m.Nz));
+    a.modules = m.modules;
+    a.Ms = (T)m.Ms; a.A = (T)m.A; a.D = (T)m.D; a.alpha = (T)m.alpha; a.grel = (T)m.grel;
+    a.K1 = (T)m.K1; a.K2 = (T)m.K2;
+    double en = std::sqrt(m.ea[0] * m.ea[0] + m.ea[1] * m.ea[1] + m.ea[2] * m.ea[2]);
+    for (int i = 0; i < 3; i++) a.ea[i] = (T)(en > 0 ? m.ea[i] / en : 0.0);
+    a.Ms_map = (const T *)m.Msd; a.K1_map = (const T *)m.K1d;
+    a.Ha = m.Had; a.nHa = m.nHa; a.Ha_tspan = m.Ha_tspan;
+    a.st = c->st;
+    a.n = m.n;
+    a.do_xfwd = (m.modules & BM_DEMAG) ? 1 : 0;
+    return a;
+}
+
+template <typename T> T *B(Mesh &m, int i) { return (T *)m.buf[i]; }
+template <typename T> T *E(Mesh &m, int i) { return (T *)m.ev[i]; }
+
+// S1 = x-FFT(M) for every mesh (after set_m, compute_* or a fresh start)
+template <typename T>
+int enqueue_prime(bm_ctx *c, int *count)
+{
+    for (auto &m : c->meshes) {
+        if (!(m.modules & BM_DEMAG)) continue;
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.mode = BM_MODE_UPDATE;
+        a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0);
+        a.nev = 0;
+        CKL(launch_stage<T>(a, c->stream), "prime");
+        (*count)++;
+    }
+    return 0;
+}
+
+template <typename T>
+int enqueue_rk4_step(bm_ctx *c, int *count)
+{
+    // buffers: 0 = M (step start, sM1), 2 = B, 3 = C ; evals 0..2
+    const int nm = (int)c->meshes.size();
+    for (int s = 0; s < 4; s++) {
+        for (int i = 0; i < nm; i++) {
+            int rc = enqueue_yz<T>(c, c->meshes[i], BM_GATE_ALWAYS, count);
+            if (rc) return rc;
+        }
+        for (int i = 0; i < nm; i++) {
+            Mesh &m = c->meshes[i];
+            StageArgs<T> a = stage_args<T>(c, m);
+            a.mode = BM_MODE_STAGE;
+            a.Mbase = B<T>(m, 0);
+            if (s == 0) { a.Min = B<T>(m, 0); a.ev_out = E<T>(m, 0); a.crhs = 0.5; a.Mout = B<T>(m, 2); }
+            else if (s == 1) { a.Min = B<T>(m, 2); a.ev_out = E<T>(m, 1); a.crhs = 0.5; a.Mout = B<T>(m, 3); }
+            else if (s == 2) { a.Min = B<T>(m, 3); a.ev_out = E<T>(m, 2); a.crhs = 1.0; a.Mout = B<T>(m, 2); }
+            else {
+                a.Min = B<T>(m, 2);
+                a.nev = 3;
+                a.ev[0] = E<T>(m, 0); a.ev[1] = E<T>(m, 1); a.ev[2] = E<T>(m, 2);
+                a.cev[0] = 1.0 / 6; a.cev[1] = 2.0 / 6; a.cev[2] = 2.0 / 6;
+                a.crhs = 1.0 / 6;
+                a.Mout = B<T>(m, 0);
+                a.renorm = 1;
+                if (i == nm - 1) a.last_kind = BM_LAST_FINISH;
+            }
+            CKL(launch_stage<T>(a, c->stream), "stage");
+            (*count)++;
+        }
+    }
+    return 0;
+}
+
+template <typename T>
+int enqueue_rkdp_attempt(bm_ctx *c, int *count)
+{
+    // buffers: 0 = M, 1 = P (sM1), 2 = B, 3 = C ; evals 0..5
+    const int nm = (int)c->meshes.size();
+    // restore after a rejection: M = sM1 and its x transform
+    for (int i = 0; i < nm; i++) {
+        Mesh &m = c->meshes[i];
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.mode = BM_MODE_UPDATE;
+        a.gate = BM_GATE_RESTORE;
+        a.Min = B<T>(m, 1); a.Mbase = B<T>(m, 1); a.Mout = B<T>(m, 0);
+        if (i == nm - 1) a.last_kind = BM_LAST_RESTORED;
+        CKL(launch_stage<T>(a, c->stream), "restore");
+        (*count)++;
+    }
+    // evaluation 0: FSAL rhs + error of the previous step + controller
+    for (int i = 0; i < nm; i++) {
+        int rc = enqueue_yz<T>(c, c->meshes[i], BM_GATE_ALWAYS, count);
+        if (rc) return rc;
+    }
+    static const double bs[5] = {5179.0 / 57600, 7571.0 / 16695, 393.0 / 640, -92097.0 / 339200, 187.0 / 2100};
+    for (int i = 0; i < nm; i++) {
+        Mesh &m = c->meshes[i];
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.mode = BM_MODE_LTE;
+        a.do_xfwd = 0;
+        a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 1);
+        a.nev = 5;
+        a.ev[0] = E<T>(m, 0); a.ev[1] = E<T>(m, 2); a.ev[2] = E<T>(m, 3); a.ev[3] = E<T>(m, 4); a.ev[4] = E<T>(m, 5);
+        for (int k = 0; k < 5; k++) a.cev[k] = bs[k];
+        a.crhs = 1.0 / 40;
+        a.ev_out = E<T>(m, 0);
+        if (i == nm - 1) a.last_kind = BM_LAST_CONTROL;
+        CKL(launch_stage<T>(a, c->stream), "rkdp eval0");
+        (*count)++;
+    }
+    // advance: sM1 = M, M1 = M + dT/5 k0
+    for (int i = 0; i < nm; i++) {
+        Mesh &m = c->meshes[i];
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.mode = BM_MODE_UPDATE;
+        a.gate = BM_GATE_ACCEPTED;
+        a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0); a.copy_to = B<T>(m, 1);
+        a.nev = 1; a.ev[0] = E<T>(m, 0); a.cev[0] = 0.2;
+        a.Mout = B<T>(m, 2);
+        CKL(launch_stage<T>(a, c->stream), "rkdp advance");
+        (*count)++;
+    }
+    static const double av[6][6] = {
+        {0},
+        {3.0 / 40, 9.0 / 40},
+        {44.0 / 45, -56.0 / 15, 32.0 / 9},
+        {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729},
+        {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656},
+        {35.0 / 384, 0.0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
+    for (int s = 1; s <= 5; s++) {
+        for (int i = 0; i < nm; i++) {
+            int rc = enqueue_yz<T>(c, c->meshes[i], BM_GATE_ACCEPTED, count);
+            if (rc) return rc;
+        }
+        for (int i = 0; i < nm; i++) {
+            Mesh &m = c->meshes[i];
+            StageArgs<T> a = stage_args<T>(c, m);
+            a.mode = BM_MODE_STAGE;
+            a.gate = BM_GATE_ACCEPTED;
+            a.Min = (s % 2 == 1) ? B<T>(m, 2) : B<T>(m, 3);
+            a.Mbase = B<T>(m, 1);
+            a.ev_out = E<T>(m, s);
+            a.nev = 0;
+            for (int e = 0; e < s; e++) {
+                if (av[s][e] == 0.0) continue;
+                a.ev[a.nev] = E<T>(m, e);
+                a.cev[a.nev] = av[s][e];
+                a.nev++;
+            }
+            a.crhs = av[s][s];
+            if (s < 5) a.Mout = (s % 2 == 1) ? B<T>(m, 3) : B<T>(m, 2);
+            else {
+                a.Mout = B<T>(m, 0);
+                a.renorm = 1;
+                if (i == nm - 1) a.last_kind = BM_LAST_FINISH;
+            }
+            CKL(launch_stage<T>(a, c->stream), "rkdp stage");
+            (*count)++;
+        }
+    }
+    return 0;
+}
+
+template <typename T>
+int build_graph(bm_ctx *c)
+{
+    drop_graph(c);
+    int count = 0;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = (c->eval == BM_RKDP54) ? enqueue_rkdp_attempt<T>(c, &count) : enqueue_rk4_step<T>(c, &count);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(BM_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    c->graph = g;
+    CK(cudaGraphInstantiate(&c->gexec, g, 0));
+    c->graph_eval = c->eval;
+    c->kernels_per_step = count;
+    return 0;
+}
+
+template <typename T>
+int run_T(bm_ctx *c, int steps)
+{
+    if (c->s1_dirty) {
+        int cnt = 0;
+        int rc = enqueue_prime<T>(c, &cnt);
+        if (rc) return rc;
+        c->s1_dirty = false;
+    }
+    if (!c->gexec || c->graph_eval != c->eval) {
+        int rc = build_graph<T>(c);
+        if (rc) return rc;
+    }
+    int rc = read_state(c);
+    if (rc) return rc;
+    long long target = c->host_st.accepted + steps;
+    long long guard = 0;
+    while (c->host_st.accepted < target) {
+        long long k = target - c->host_st.accepted;
+        for (long long i = 0; i < k; i++) CK(cudaGraphLaunch(c->gexec, c->stream));
+        guard += k;
+        if ((rc = read_state(c))) return rc;
+        if (c->eval == BM_RK4) break;
+        if (guard > 100LL * steps + 1000) return fail(BM_ESTATE, "step control did not converge");
+    }
+    return 0;
+}
+
+template <typename T>
+int compute_field_T(bm_ctx *c, Mesh &m, int modules_mask, double *H)
+{
+    int cnt = 0;
+    if (m.modules & BM_DEMAG) {
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.mode = BM_MODE_UPDATE;
+        a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0);
+        CKL(launch_stage<T>(a, c->stream), "xfwd");
+        int rc = enqueue_yz<T>(c, m, BM_GATE_ALWAYS, &cnt);
+        if (rc) return rc;
+    }
+    StageArgs<T> a = stage_args<T>(c, m);
+    a.mode = BM_MODE_HEFF;
+    a.modules = m.modules & modules_mask;
+    a.do_xfwd = 0;
+    a.Min = B<T>(m, 0);
+    a.Hout = (T *)m.Hout;
+    CKL(launch_stage<T>(a, c->stream), "heff");
+    CKL(launch_planes_to_aos<T>(m.stage64, (const T *)m.Hout, m.n, c->stream), "planes_to_aos");
+    CK(cudaMemcpyAsync(H, m.stage64, sizeof(double) * 3 * m.n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->s1_dirty = true;
+    return 0;
+}
+
+int check_ctx(bm_ctx *c) { return c ? 0 : fail(BM_EINVAL, "null context"); }
+int check_mesh(bm_ctx *c, int mesh)
+{
+    if (!c) return fail(BM_EINVAL, "null context");
+    if (mesh < 0 || mesh >= (int)c->meshes.size()) return fail(BM_EINVAL, "bad mesh index");
+    return 0;
+}
+
+}  // namespace
+
+// =============================================================================== C ABI
+extern "C" {
+
+const char *bm_last_error(void) { return g_err.c_str(); }
+int bm_version(void) { return 1; }
+
+int bm_create(int device, bm_ctx **out)
+{
+    if (!out) return fail(BM_EINVAL, "null out");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return fail(BM_ECUDA, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(BM_EINVAL, "bad device index");
+    bm_ctx *c = new bm_ctx();
+    c->device = device;
+    cudaSetDevice(device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return fail(BM_ECUDA, "stream"); }
+    if (cudaMalloc(&c->st, sizeof(StepState)) != cudaSuccess) { delete c; return fail(BM_ENOMEM, "state"); }
+    if (cudaMalloc(&c->farq, sizeof(double) * 6 * BM_FARQ_PER_COMP) != cudaSuccess) { delete c; return fail(BM_ENOMEM, "farq"); }
+    memset(&c->host_st, 0, sizeof(StepState));
+    *out = c;
+    return 0;
+}
+
+int bm_destroy(bm_ctx *c)
+{
+    if (!c) return 0;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
+    for (auto &m : c->meshes) free_mesh(m);
+    if (c->st) cudaFree(c->st);
+    if (c->farq) cudaFree(c->farq);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return 0;
+}
+
+int bm_add_mesh(bm_ctx *c, int nx, int ny, int nz, double hx, double hy, double hz, double ox, double oy, double oz, int *mesh_id)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (nx < 1 || ny < 1 || nz < 1) return fail(BM_EINVAL, "mesh dimensions must be >= 1");
+    if (!(hx > 0 && hy > 0 && hz > 0)) return fail(BM_EINVAL, "cellsize must be > 0");
+    if ((long long)nx * ny * nz > (1LL << 31)) return fail(BM_EINVAL, "mesh too large");
+    if (nice_size(nx) > 4096 || nice_size(ny) > 4096 || nice_size(nz) > 2048) return fail(BM_EUNSUPPORTED, "mesh dimension above the supported FFT size");
+    unprepare(c);
+    Mesh m;
+    m.nx = nx; m.ny = ny; m.nz = nz;
+    m.h[0] = hx; m.h[1] = hy; m.h[2] = hz;
+    m.o[0] = ox; m.o[1] = oy; m.o[2] = oz;
+    m.n = (long long)nx * ny * nz;
+    m.M0.assign(3 * (size_t)m.n, 0.0);
+    for (long long i = 0; i < m.n; i++) m.M0[3 * i] = m.Ms;
+    c->meshes.push_back(m);
+    if (mesh_id) *mesh_id = (int)c->meshes.size() - 1;
+    return 0;
+}
+
+int bm_set_material(bm_ctx *c, int mesh, double Ms, double A, double alpha, double grel, double K1, double K2, const double *ea3, double D)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!(Ms > 0)) return fail(BM_EINVAL, "Ms must be > 0");
+    unprepare(c);
+    Mesh &m = c->meshes[mesh];
+    m.Ms = Ms; m.A = A; m.alpha = alpha; m.grel = grel; m.K1 = K1; m.K2 = K2; m.D = D;
+    if (ea3) { m.ea[0] = ea3[0]; m.ea[1] = ea3[1]; m.ea[2] = ea3[2]; }
+    return 0;
+}
+
+int bm_set_material_maps(bm_ctx *c, int mesh, const double *Ms_map, const double *K1_map)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    unprepare(c);
+    Mesh &m = c->meshes[mesh];
+    if (Ms_map) {
+        for (long long i = 0; i < m.n; i++) if (!(Ms_map[i] > 0)) return fail(BM_EINVAL, "Ms map values must be > 0");
+        m.Ms_map.assign(Ms_map, Ms_map + m.n);
+    } else m.Ms_map.clear();
+    if (K1_map) m.K1_map.assign(K1_map, K1_map + m.n);
+    else m.K1_map.clear();
+    return 0;
+}
+
+int bm_set_modules(bm_ctx *c, int mesh, int modules)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (modules & ~(BM_DEMAG | BM_EXCH | BM_IDMI | BM_ANIUNI | BM_ZEEMAN)) return fail(BM_EINVAL, "unknown module bit");
+    if ((modules & BM_EXCH) && (modules & BM_IDMI)) return fail(BM_EINVAL, "BM_EXCH and BM_IDMI are exclusive");
+    unprepare(c);
+    c->meshes[mesh].modules = modules;
+    return 0;
+}
+
+int bm_set_field(bm_ctx *c, int mesh, const double *Ha, int nsamples, double t_span)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!Ha || nsamples < 1) return fail(BM_EINVAL, "field samples");
+    Mesh &m = c->meshes[mesh];
+    m.Ha.assign(Ha, Ha + 3 * (size_t)nsamples);
+    m.Ha_tspan = t_span;
+    m.nHa = nsamples;
+    if (c->ready) {
+        cudaSetDevice(c->device);
+        CK(cudaStreamSynchronize(c->stream));
+        if (m.Had) cudaFree(m.Had);
+        m.Had = nullptr;
+        CK(cudaMalloc(&m.Had, sizeof(double) * m.Ha.size()));
+        CK(cudaMemcpy(m.Had, m.Ha.data(), sizeof(double) * m.Ha.size(), cudaMemcpyHostToDevice));
+        drop_graph(c);
+    }
+    return 0;
+}
+
+int bm_set_ode(bm_ctx *c, int eval, double dt)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (eval != BM_RK4 && eval != BM_RKDP54) return fail(BM_EUNSUPPORTED, "evaluation method");
+    if (!(dt > 0)) return fail(BM_EINVAL, "dt must be > 0");
+    bool changed = (eval != c->eval) || !c->eval_chosen;
+    if (eval != c->eval) unprepare(c);
+    c->eval = eval;
+    c->eval_chosen = true;
+    c->dt = dt;
+    if (eval == BM_RKDP54 && changed) {
+        // Boris/DiffEq_Defs.h:58-63 defaults, Boris/DiffEq_CommonBase_Control.cpp:111
+        c->tol = 1e-4; c->dT_incr = 2.0; c->dT_min = 1e-15; c->dT_max = 3e-12;
+    }
+    if (c->ready) {
+        if (int rc = read_state(c)) return rc;
+        c->host_st.primed = 0;
+        return upload_state(c);
+    }
+    return 0;
+}
+
+int bm_set_astepctrl(bm_ctx *c, double err_fail, double dT_incr, double dT_min, double dT_max)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (!(err_fail > 0) || !(dT_incr >= 1) || !(dT_min > 0) || !(dT_max >= dT_min)) return fail(BM_EINVAL, "astepctrl values");
+    c->tol = err_fail; c->dT_incr = dT_incr; c->dT_min = dT_min; c->dT_max = dT_max;
+    if (c->ready) {
+        if (int rc = read_state(c)) return rc;
+        c->host_st.tol = err_fail; c->host_st.dT_incr = dT_incr; c->host_st.dT_min = dT_min; c->host_st.dT_max = dT_max;
+        c->dt = c->host_st.dT;
+        return upload_state(c);
+    }
+    return 0;
+}
+
+int bm_set_precision(bm_ctx *c, int precision)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (precision != BM_FP64 && precision != BM_MIXED) return fail(BM_EINVAL, "precision");
+    if (precision != c->precision) unprepare(c);
+    c->precision = precision;
+    return 0;
+}
+
+int bm_set_m(bm_ctx *c, int mesh, const double *M)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!M) return fail(BM_EINVAL, "null M");
+    Mesh &m = c->meshes[mesh];
+    if (!c->ready) {
+        m.M0.assign(M, M + 3 * (size_t)m.n);
+        return 0;
+    }
+    cudaSetDevice(c->device);
+    CK(cudaMemcpyAsync(m.stage64, M, sizeof(double) * 3 * m.n, cudaMemcpyHostToDevice, c->stream));
+    if (c->precision == BM_FP64) CKL(launch_aos_to_planes<double>((double *)m.buf[0], m.stage64, m.n, c->stream), "aos_to_planes");
+    else CKL(launch_aos_to_planes<float>((float *)m.buf[0], m.stage64, m.n, c->stream), "aos_to_planes");
+    c->s1_dirty = true;
+    // a new M un-primes the RKDP54 error estimate, as a restart of the reference solver does
+    if (int rc = read_state(c)) return rc;
+    c->host_st.primed = 0;
+    c->dt = c->host_st.dT;
+    return upload_state(c);
+}
+
+int bm_get_m(bm_ctx *c, int mesh, double *M)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!M) return fail(BM_EINVAL, "null M");
+    Mesh &m = c->meshes[mesh];
+    if (!c->ready) {
+        memcpy(M, m.M0.data(), sizeof(double) * 3 * m.n);
+        return 0;
+    }
+    cudaSetDevice(c->device);
+    if (c->precision == BM_FP64) CKL(launch_planes_to_aos<double>(m.stage64, (const double *)m.buf[0], m.n, c->stream), "planes_to_aos");
+    else CKL(launch_planes_to_aos<float>(m.stage64, (const float *)m.buf[0], m.n, c->stream), "planes_to_aos");
+    CK(cudaMemcpyAsync(M, m.stage64, sizeof(double) * 3 * m.n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bm_compute_hdemag(bm_ctx *c, int mesh, double *H, double *energy)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!H) return fail(BM_EINVAL, "null H");
+    if (!(c->meshes[mesh].modules & BM_DEMAG)) return fail(BM_ESTATE, "mesh has no demag module");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    Mesh &m = c->meshes[mesh];
+    int rc = (c->precision == BM_FP64) ? compute_field_T<double>(c, m, BM_DEMAG, H) : compute_field_T<float>(c, m, BM_DEMAG, H);
+    if (rc) return rc;
+    if (energy) {
+        std::vector<double> Mh(3 * (size_t)m.n);
+        if ((rc = bm_get_m(c, mesh, Mh.data()))) return rc;
+        double dot = 0.0;
+        for (size_t i = 0; i < Mh.size(); i++) dot += Mh[i] * H[i];
+        *energy = -BM_MU0 * dot / (2.0 * (double)m.n);
+    }
+    return 0;
+}
+
+int bm_compute_heff(bm_ctx *c, int mesh, double *H)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!H) return fail(BM_EINVAL, "null H");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    Mesh &m = c->meshes[mesh];
+    return (c->precision == BM_FP64) ? compute_field_T<double>(c, m, ~0, H) : compute_field_T<float>(c, m, ~0, H);
+}
+
+int bm_run(bm_ctx *c, int steps, bm_stats *out)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (steps < 0) return fail(BM_EINVAL, "steps < 0");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    if (steps > 0) {
+        int rc = (c->precision == BM_FP64) ? run_T<double>(c, steps) : run_T<float>(c, steps);
+        if (rc) return rc;
+    }
+    return bm_get_stats(c, out);
+}
+
+int bm_get_stats(bm_ctx *c, bm_stats *out)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (c->ready)
+        if (int rc = read_state(c)) return rc;
+    if (out) {
+        out->accepted = c->host_st.accepted;
+        out->rejected = c->host_st.rejected;
+        out->attempts = c->host_st.attempts;
+        out->time = c->host_st.time;
+        out->dT = c->ready ? c->host_st.dT : c->dt;
+        out->last_lte = c->host_st.last_lte;
+    }
+    return 0;
+}
+
+int bm_mesh_info(bm_ctx *c, int mesh, int *n3, int *N3)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    Mesh &m = c->meshes[mesh];
+    if (n3) { n3[0] = m.nx; n3[1] = m.ny; n3[2] = m.nz; }
+    if (N3) {
+        N3[0] = 2 * nice_size(m.nx);
+        N3[1] = 2 * nice_size(m.ny);
+        N3[2] = m.nz > 1 ? 2 * nice_size(m.nz) : 1;
+    }
+    return 0;
+}
+
+int bm_device_m(bm_ctx *c, int mesh, void **dptr, int *elem_bytes)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (int rc = prepare(c)) return rc;
+    if (dptr) *dptr = c->meshes[mesh].buf[0];
+    if (elem_bytes) *elem_bytes = (c->precision == BM_FP64) ? 8 : 4;
+    return 0;
+}
+
+int bm_sync(bm_ctx *c)
+{
+    if (int rc = check_ctx(c)) return rc;
+    cudaSetDevice(c->device);
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bm_kernels_per_step(bm_ctx *c, int *count)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (count) *count = c->kernels_per_step;
+    return 0;
+}
+
+int bm_run_timed(bm_ctx *c, int steps, bm_stats *out, double *device_ms)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    if (c->s1_dirty) {
+        int cnt = 0;
+        int rc = (c->precision == BM_FP64) ? enqueue_prime<double>(c, &cnt) : enqueue_prime<float>(c, &cnt);
+        if (rc) return rc;
+        c->s1_dirty = false;
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, c->stream));
+    int rc = bm_run(c, steps, out);
+    if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (device_ms) *device_ms = ms;
+    return 0;
+}
+
+}  // extern "C"
+
+namespace {
+template <typename T>
+int time_kernels_T(bm_ctx *c, Mesh &m, int reps, double *ms4, double *bytes4)
+{
+    for (int i = 0; i < 4; i++) { ms4[i] = 0.0; bytes4[i] = 0.0; }
+    cudaStream_t s = c->stream;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const double cs = sizeof(cpx<T>), rs = sizeof(T);
+    const double s1 = 3.0 * m.nz * m.ny * m.LX * cs, s2 = 3.0 * m.nz * m.Ny * m.LX * cs;
+    const double kb = 6.0 * (m.LX + 1) * (m.Ny / 2 + 1) * (m.Nz / 2 + 1) * rs;
+    auto timeit = [&](auto launch, int slot, double bytes) -> int {
+        for (int w = 0; w < 2; w++) { int rc = launch(); if (rc) return rc; }
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps; r++) { int rc = launch(); if (rc) return rc; }
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms4[slot] = ms / reps;
+        bytes4[slot] = bytes;
+        return 0;
+    };
+    int rc = 0;
+    if (m.modules & BM_DEMAG) {
+        YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
+        if (m.nz == 1) {
+            rc = timeit([&]() { return launch_ymid2d<T>(a, s); }, 0, 2.0 * s1 + 4.0 / 6.0 * kb);
+        } else {
+            a.W = m.Wy;
+            rc = timeit([&]() { return launch_yfwd<T>(a, s); }, 0, s1 + s2);
+            YZArgs<T> b = a;
+            b.W = m.Wz;
+            if (!rc) rc = timeit([&]() { return launch_zmid<T>(b, s); }, 1, 2.0 * s2 + kb);
+            if (!rc) rc = timeit([&]() { return launch_yinv<T>(a, s); }, 2, s1 + s2);
+        }
+    }
+    // the stage kernel as RKDP54 stage 3 uses it: 3 earlier evaluations, writes rhs and next M
+    T *tmp = nullptr;
+    if (!rc && cudaMalloc(&tmp, sizeof(T) * 6 * m.n) != cudaSuccess) rc = BM_ENOMEM;
+    if (!rc) {
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.mode = BM_MODE_STAGE;
+        a.Min = (const T *)m.buf[0];
+        a.Mbase = (const T *)m.buf[0];
+        a.nev = 3;
+        a.ev[0] = (const T *)m.buf[0]; a.ev[1] = (const T *)m.buf[0]; a.ev[2] = (const T *)m.buf[0];
+        a.cev[0] = a.cev[1] = a.cev[2] = 0.0;
+        a.crhs = 0.0;
+        a.ev_out = tmp;
+        a.Mout = tmp + 3 * m.n;
+        double bytes = 3.0 * m.n * rs * (1 + 1 + 3 + 1 + 1);
+        if (m.modules & BM_DEMAG) bytes += 2.0 * s1;
+        if (a.Ms_map) bytes += m.n * rs;
+        if (a.K1_map) bytes += m.n * rs;
+        rc = timeit([&]() { return launch_stage<T>(a, s); }, 3, bytes);
+    }
+    cudaStreamSynchronize(s);
+    if (tmp) cudaFree(tmp);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->s1_dirty = true;
+    return rc ? fail(BM_ECUDA, "kernel timing launch failed (" + std::to_string(rc) + ")") : 0;
+}
+}  // namespace
+
+extern "C" {
+
+int bm_time_kernels(bm_ctx *c, int mesh, int reps, double *ms4, double *bytes4)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!ms4 || !bytes4 || reps < 1) return fail(BM_EINVAL, "args");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    Mesh &m = c->meshes[mesh];
+    return (c->precision == BM_FP64) ? time_kernels_T<double>(c, m, reps, ms4, bytes4)
+                                     : time_kernels_T<float>(c, m, reps, ms4, bytes4);
+}
+
+int bm_debug_kernels(bm_ctx *c, int mesh, double *K6)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    Mesh &m = c->meshes[mesh];
+    cudaSetDevice(c->device);
+    int Nx = 2 * nice_size(m.nx), Ny = 2 * nice_size(m.ny), Nz = m.nz > 1 ? 2 * nice_size(m.nz) : 1;
+    size_t nk = (size_t)(Nx / 2 + 1) * (Ny / 2 + 1) * (Nz / 2 + 1);
+    double *K = nullptr;
+    void *tx = nullptr, *ty = nullptr, *tz = nullptr;
+    CK(cudaMalloc(&K, sizeof(double) * 6 * nk));
+    int rc = 0;
+    if ((rc = upload_table<double>(&tx, Nx, true, c->stream)) || (rc = upload_table<double>(&ty, Ny, true, c->stream)) ||
+        (rc = upload_table<double>(&tz, Nz, true, c->stream))) { cudaFree(K); return rc; }
+    double hm = std::fmax(m.h[0], std::fmax(m.h[1], m.h[2]));
+    std::vector<double> fq(6 * BM_FARQ_PER_COMP);
+    bm_far_coeffs(m.h[0] / hm, m.h[1] / hm, m.h[2] / hm, fq.data());
+    CK(cudaMemcpy(c->farq, fq.data(), sizeof(double) * fq.size(), cudaMemcpyHostToDevice));
+    rc = build_kernels_device<double>(K, m.nx, m.ny, m.nz, Nx, Ny, Nz, m.h[0], m.h[1], m.h[2], c->farq,
+                                      (const cpx<double> *)tx, (const cpx<double> *)ty, (const cpx<double> *)tz, c->stream);
+    cudaFree(tx); cudaFree(ty); cudaFree(tz);
+    if (rc) { cudaFree(K); return fail(BM_ECUDA, "kernel build failed"); }
+    CK(cudaMemcpy(K6, K, sizeof(double) * 6 * nk, cudaMemcpyDeviceToHost));
+    cudaFree(K);
+    return 0;
+}
+
+int bm_debug_tensor(int device, int nx, int ny, int nz, double hx, double hy, double hz, double *oct6)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || !oct6) return fail(BM_EINVAL, "args");
+    CK(cudaSetDevice(device));
+    size_t np = (size_t)nx * ny * nz;
+    double *d = nullptr, *fq_d = nullptr;
+    CK(cudaMalloc(&d, sizeof(double) * 6 * np));
+    CK(cudaMalloc(&fq_d, sizeof(double) * 6 * BM_FARQ_PER_COMP));
+    double hm = std::fmax(hx, std::fmax(hy, hz));
+    std::vector<double> fq(6 * BM_FARQ_PER_COMP);
+    bm_far_coeffs(hx / hm, hy / hm, hz / hm, fq.data());
+    CK(cudaMemcpy(fq_d, fq.data(), sizeof(double) * fq.size(), cudaMemcpyHostToDevice));
+    int rc = tensor_octant_device(d, nx, ny, nz, hx, hy, hz, fq_d, 0);
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(oct6, d, sizeof(double) * 6 * np, cudaMemcpyDeviceToHost));
+    cudaFree(d);
+    cudaFree(fq_d);
+    return rc ? fail(BM_ECUDA, "tensor launch") : 0;
+}
+
+int bm_debug_fft(int device, int L, int howmany, int precision, int inverse, double *data)
+{
+    if (L < 1 || howmany < 1 || !data) return fail(BM_EINVAL, "args");
+    FFTPlan P;
+    if (!bm_make_plan(L, P)) return fail(BM_EUNSUPPORTED, "length");
+    CK(cudaSetDevice(device));
+    size_t nv = 2 * (size_t)L * howmany;
+    double *d64 = nullptr;
+    CK(cudaMalloc(&d64, sizeof(double) * nv));
+    CK(cudaMemcpy(d64, data, sizeof(double) * nv, cudaMemcpyHostToDevice));
+    int rc = 0;
+    void *tw = nullptr;
+    if (precision == BM_FP64) {
+        if ((rc = upload_table<double>(&tw, L, false, 0))) { cudaFree(d64); return rc; }
+        rc = launch_fft_strided<double>((cpx<double> *)d64, P, (const cpx<double> *)tw, 1, L, howmany, 0, 1, inverse != 0, 0);
+    } else {
+        float *d32 = nullptr;
+        CK(cudaMalloc(&d32, sizeof(float) * nv));
+        launch_convert<float>(d32, d64, (long long)nv, 0);
+        if ((rc = upload_table<float>(&tw, L, false, 0))) { cudaFree(d64); cudaFree(d32); return rc; }
+        rc = launch_fft_strided<float>((cpx<float> *)d32, P, (const cpx<float> *)tw, 1, L, howmany, 0, 1, inverse != 0, 0);
+        launch_convert_back<float>(d64, d32, (long long)nv, 0);
+        cudaDeviceSynchronize();
+        cudaFree(d32);
+    }
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(data, d64, sizeof(double) * nv, cudaMemcpyDeviceToHost));
+    cudaFree(d64);
+    cudaFree(tw);
+    return rc ? fail(BM_ECUDA, "fft launch failed " + std::to_string(rc)) : 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+// Common device/host helpers for the B200 micromagnetic path.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define BM_HD __host__ __device__ __forceinline__
+
+template <typename T> struct cpx_t;
+template <> struct alignas(8) cpx_t<float> { float x, y; };
+template <> struct alignas(16) cpx_t<double> { double x, y; };
+template <typename T> using cpx = cpx_t<T>;
+
+template <typename T> BM_HD cpx<T> mk(T a, T b) { cpx<T> r; r.x = a; r.y = b; return r; }
+template <typename T> BM_HD cpx<T> operator+(cpx<T> a, cpx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> BM_HD cpx<T> operator-(cpx<T> a, cpx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> BM_HD cpx<T> cmul(cpx<T> a, cpx<T> b) { return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename T> BM_HD cpx<T> cscale(cpx<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
+template <typename T> BM_HD cpx<T> conj(cpx<T> a) { return mk<T>(a.x, -a.y); }
+// multiply by -i (forward) or +i (inverse): s = -1 gives -i*a, s = +1 gives +i*a
+template <typename T> BM_HD cpx<T> mul_i(cpx<T> a) { return mk<T>(-a.y, a.x); }
+template <typename T> BM_HD cpx<T> mul_mi(cpx<T> a) { return mk<T>(a.y, -a.x); }
+
+// Physical constants (the reference's BorisLib/Funcs_Math_base.h:9,16)
+#define BM_MU0 1.256637061435916e-6
+#define BM_GAMMA 2.212761569e5
+
+// module bits
+#define BM_MOD_DEMAG 1
+#define BM_MOD_EXCH 2
+#define BM_MOD_IDMI 4
+#define BM_MOD_ANIUNI 8
+#define BM_MOD_ZEEMAN 16
+
+// device-resident step state shared by all kernels of a solver
+struct StepState {
+    double time, stagetime, dT, dT_last;
+    double lte, last_lte;
+    double tol, dT_incr, dT_min, dT_max;
+    long long accepted, rejected, attempts;
+    int primed, reject_flag, need_restore, error;
+    unsigned long long lte_bits;   // running max of lte (non-negative doubles order like their bits)
+    unsigned int blocks_done;      // last-block-done counter for grid reductions
+    unsigned int restore_done;
+    int eval_order;
+    int pad_;
+};

@@ -1,0 +1,85 @@
+// Internal declarations shared by the kernel translation units and the host runtime.
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+
+#define BM_FARQ_PER_COMP 94   // 6 + 15 + 28 + 45 monomials for orders 2, 4, 6, 8
+
+// ---------------------------------------------------------------- tensor / kernels
+template <typename T>
+int build_kernels_device(T *K, int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz,
+                         const double *farq_dev, const cpx<double> *twx, const cpx<double> *twy,
+                         const cpx<double> *twz, cudaStream_t s);
+int tensor_octant_device(double *oct_dev, int nx, int ny, int nz, double hx, double hy, double hz, const double *farq_dev,
+                         cudaStream_t s);
+template <typename T>
+int launch_fft_strided(cpx<T> *data, const FFTPlan &P, const cpx<T> *tw, long long es, long long ls, int ninner,
+                       long long os, int nouter, bool inv, cudaStream_t s);
+// host: far-field polynomial coefficients (6 * BM_FARQ_PER_COMP doubles) for normalised cellsize
+void bm_far_coeffs(double hx, double hy, double hz, double *out);
+
+// ---------------------------------------------------------------- gating of kernels by step state
+#define BM_GATE_ALWAYS 0
+#define BM_GATE_ACCEPTED 1      // skip when the current attempt was rejected
+#define BM_GATE_RESTORE 2       // run only when a restore is pending
+
+// ---------------------------------------------------------------- y / z passes
+template <typename T>
+struct YZArgs {
+    cpx<T> *S1;          // [3][nz][ny][LX]
+    cpx<T> *S2;          // [3][nz][Ny][LX] (3D only)
+    const T *K;          // 6 planes [(kz*Ky1 + ky)*Kx1 + kx]
+    const cpx<T> *twy, *twz;
+    FFTPlan py, pz;
+    int nx, ny, nz, LX, Ny, Nz;
+    int W;               // column tile width
+    StepState *st;
+    int gate;
+};
+
+template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s);
+template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s);
+template <typename T> int launch_zmid(const YZArgs<T> &a, cudaStream_t s);
+template <typename T> int launch_yinv(const YZArgs<T> &a, cudaStream_t s);
+
+// ---------------------------------------------------------------- fused x / field / LLG stage kernel
+#define BM_MODE_STAGE 0     // fields, LLG, stage update, forward x-FFT of the new M
+#define BM_MODE_HEFF 1      // fields only, write Heff to Hout
+#define BM_MODE_LTE 2       // fields, LLG, RKDP54 4th-order prediction error (FP64 max), FSAL rhs
+#define BM_MODE_UPDATE 3    // no fields: M_out = M_base + dT * sum c_i ev_i, forward x-FFT
+
+#define BM_LAST_NONE 0
+#define BM_LAST_FINISH 1    // time += dT, accepted++
+#define BM_LAST_CONTROL 2   // RKDP54 step control on the reduced lte
+#define BM_LAST_RESTORED 3  // clear need_restore
+
+template <typename T>
+struct StageArgs {
+    int nx, ny, nz, LX, Nx;
+    double hx, hy, hz;
+    cpx<T> *S1;
+    const cpx<T> *twx;   // length LX
+    const cpx<T> *twx2;  // length Nx (R2C split twiddles)
+    FFTPlan px;
+    int rpb;             // rows per block
+    T scale;             // 2 / (Nx Ny Nz)
+    int modules;
+    T Ms, A, D, alpha, grel, K1, K2;
+    T ea[3];
+    const T *Ms_map, *K1_map;
+    const double *Ha;
+    int nHa;
+    double Ha_tspan;
+    StepState *st;
+    const T *Min, *Mbase;
+    T *Mout, *copy_to, *ev_out, *Hout;
+    int nev;
+    const T *ev[6];
+    double cev[6];
+    double crhs;
+    int renorm, mode, do_xfwd, last_kind, gate;
+    long long n;         // cells
+};
+
+template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s);
+int launch_scalar_reset(StepState *st, cudaStream_t s);

@@ -1,0 +1,379 @@
+// Fused per-row stage kernel: the x passes of the demag convolution around every
+// effective-field evaluation, with the field terms, the LLG right-hand side and the
+// Runge-Kutta stage update in between.
+//
+// Per block: rpb rows (y, z) x 3 components.
+//   A. (fields needed, demag on) load the spectrum rows S1 produced by the y/z passes,
+//      undo the packed R2C split, inverse FFT along x  ->  H_demag for the rows (in smem).
+//   B. per cell: Heff = Zeeman + H_demag + exchange/iDMI + uniaxial anisotropy,
+//      rhs = LLG(M, Heff), then one of: stage update / RKDP54 error estimate / Heff out.
+//   C. (forward transform requested) forward FFT along x of the new M rows, R2C split,
+//      store to S1 for the next stage's y/z passes.
+// Reference physics: Zeeman Boris/Zeeman.cpp:164 (sets Heff, evaluated at the stage time),
+// demag Boris/Demag.cpp:170 + Convolution.h:262/659, exchange Boris/Exchange.cpp:108 with
+// BorisLib/VEC_VC_Del.h:10, iDMI Boris/iDMExchange.cpp:97 with VEC_VC_Del.h:141 and
+// VEC_VC_Grad.h:10,139, anisotropy Boris/Anisotropy.cpp:82, LLG Boris/DiffEqFM_Equations.cpp:12,
+// RK4 Boris/DiffEqFM_Evals_RK4.cpp, RKDP54 Boris/DiffEqFM_Evals_RKDP54.cpp, step control
+// Boris/DiffEq_CommonBase_Iterate.cpp:15 (SetAdaptiveTimeStep) and :1214 (prime / restore).
+#include "kernels.h"
+
+template <typename T>
+__device__ __forceinline__ bool stage_gated_out(const StepState *st, int gate)
+{
+    if (gate == BM_GATE_ALWAYS || st == nullptr) return false;
+    if (gate == BM_GATE_ACCEPTED) return *((volatile const int *)&st->reject_flag) != 0;
+    return *((volatile const int *)&st->need_restore) == 0;
+}
+
+// real value at x of a packed line (complex element x/2, .x for even x, .y for odd x)
+template <typename T> __device__ __forceinline__ T *rptr(cpx<T> *line, int x)
+{
+    return reinterpret_cast<T *>(&line[eaddr<true>(x >> 1, 1)]) + (x & 1);
+}
+
+// after a forward complex FFT of z[m] = x[2m] + i x[2m+1]: split into the packed half spectrum
+template <typename T>
+__device__ __forceinline__ void xfwd_post(cpx<T> *line, int LX, const cpx<T> *__restrict__ tw2, int t, int tpl, bool act)
+{
+    if (act) {
+        for (int k = t; k <= LX / 2; k += tpl) {
+            if (k == 0) {
+                cpx<T> z0 = line[eaddr<true>(0, 1)];
+                line[eaddr<true>(0, 1)] = mk<T>(z0.x + z0.y, z0.x - z0.y);
+                continue;
+            }
+            int k2 = LX - k;
+            cpx<T> A = line[eaddr<true>(k, 1)], Bc = conj(line[eaddr<true>(k2, 1)]);
+            cpx<T> E = cscale(A + Bc, (T)0.5);
+            cpx<T> O = cscale(mul_mi(A - Bc), (T)0.5);
+            cpx<T> wO = cmul(tw2[k], O);
+            line[eaddr<true>(k, 1)] = E + wO;
+            if (k2 != k) line[eaddr<true>(k2, 1)] = conj(E - wO);
+        }
+    }
+    __syncthreads();
+}
+
+// inverse of xfwd_post: packed half spectrum -> Z (complex FFT input of the even/odd split)
+template <typename T>
+__device__ __forceinline__ void xinv_pre(cpx<T> *line, int LX, const cpx<T> *__restrict__ tw2, int t, int tpl, bool act)
+{
+    if (act) {
+        for (int k = t; k <= LX / 2; k += tpl) {
+            if (k == 0) {
+                cpx<T> p0 = line[eaddr<true>(0, 1)];
+                line[eaddr<true>(0, 1)] = mk<T>((p0.x + p0.y) * (T)0.5, (p0.x - p0.y) * (T)0.5);
+                continue;
+            }
+            int k2 = LX - k;
+            cpx<T> Xk = line[eaddr<true>(k, 1)], Xk2c = conj(line[eaddr<true>(k2, 1)]);
+            cpx<T> E = cscale(Xk + Xk2c, (T)0.5);
+            cpx<T> O = cscale(cmul(Xk - Xk2c, conj(tw2[k])), (T)0.5);
+            line[eaddr<true>(k, 1)] = E + mul_i(O);
+            if (k2 != k) line[eaddr<true>(k2, 1)] = conj(E) + mul_i(conj(O));
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ void ld3(const T *P, long long n, long long i, T v[3])
+{
+    v[0] = P[i]; v[1] = P[n + i]; v[2] = P[2 * n + i];
+}
+
+// one axis of the Neumann / non-homogeneous Neumann stencils for a full rectangular mesh
+template <typename T>
+__device__ __forceinline__ void axis_stencil(const T m[3], const T *mp, const T *mm, bool hp, bool hm, T h, const T bd[3],
+                                             T d2[3], T g[3])
+{
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if (hp && hm) {
+            d2[c] = (mp[c] + mm[c] - 2 * m[c]) / (h * h);
+            g[c] = (mp[c] - mm[c]) / (2 * h);
+        } else if (hp) {
+            d2[c] = ((mp[c] - m[c]) - bd[c] * h) / (h * h);
+            g[c] = (T)0.5 * ((mp[c] - m[c]) / h + bd[c]);
+        } else if (hm) {
+            d2[c] = ((mm[c] - m[c]) + bd[c] * h) / (h * h);
+            g[c] = (T)0.5 * ((m[c] - mm[c]) / h + bd[c]);
+        } else {
+            d2[c] = 0;
+            g[c] = 0;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
+{
+    if (stage_gated_out<T>(a.st, a.gate)) return;
+    extern __shared__ unsigned char smraw[];
+    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
+    __shared__ double red[32];
+    __shared__ int is_last;
+
+    const int LX = a.LX, nx = a.nx, ny = a.ny, nz = a.nz, rpb = a.rpb, tpl = a.px.tpl;
+    const int LSP = padded_len(LX);
+    const int nrows = ny * nz;
+    const int r0 = blockIdx.x * rpb;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const long long n = a.n;
+    const int q = tid / tpl, t = tid % tpl;
+    const int qc = q / rpb, qr = q % rpb;
+    const bool qact = (q < 3 * rpb) && (r0 + qr < nrows);
+    cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
+
+    const bool fields = (a.mode != BM_MODE_UPDATE);
+    const bool demag = fields && (a.modules & BM_MOD_DEMAG);
+
+    if (demag) {
+        if (qact) {
+            const cpx<T> *src = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
+            for (int m = t; m < LX; m += tpl) line[eaddr<true>(m, 1)] = src[m];
+        }
+        __syncthreads();
+        xinv_pre<T>(line, LX, a.twx2, t, tpl, qact);
+        fft_line<T, true, true>(line, 1, t, qact, a.px, a.twx);
+    }
+
+    const double dT = a.st ? *((volatile double *)&a.st->dT) : 0.0;
+    T Ha[3] = {0, 0, 0};
+    if (fields && (a.modules & BM_MOD_ZEEMAN) && a.Ha && a.nHa > 0) {
+        double tm = a.st ? *((volatile double *)&a.st->stagetime) : 0.0;
+        int hi = 0;
+        if (a.nHa > 1 && a.Ha_tspan > 0.0) {
+            hi = (int)floor(tm / a.Ha_tspan * a.nHa);
+            hi = hi < 0 ? 0 : (hi >= a.nHa ? a.nHa - 1 : hi);
+        }
+        Ha[0] = (T)a.Ha[3 * hi]; Ha[1] = (T)a.Ha[3 * hi + 1]; Ha[2] = (T)a.Ha[3 * hi + 2];
+    }
+    const bool exch = fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
+    const T Dv = (a.modules & BM_MOD_IDMI) ? a.D : (T)0;
+    const T hx = (T)a.hx, hy = (T)a.hy, hz = (T)a.hz;
+    T cev[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) cev[i] = (T)(a.cev[i] * dT);
+    const T crhs = (T)(a.crhs * dT);
+    double lmax = 0.0;
+
+    for (int ci = tid; ci < rpb * nx; ci += nt) {
+        int r = ci / nx, x = ci - r * nx;
+        int row = r0 + r;
+        if (row >= nrows) continue;
+        long long cell = (long long)row * nx + x;
+        T m[3];
+        ld3(a.Min, n, cell, m);
+        T Ms = a.Ms_map ? a.Ms_map[cell] : a.Ms;
+        T rhs[3] = {0, 0, 0};
+        if (fields) {
+            T H[3] = {Ha[0], Ha[1], Ha[2]};
+            if (demag) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) H[c] += a.scale * *rptr<T>(sm + (c * rpb + r) * LSP, x);
+            }
+            if (exch) {
+                int y = row % ny, z = row / ny;
+                T mxp[3], mxm[3], myp[3], mym[3], mzp[3], mzm[3];
+                bool hxp = x + 1 < nx, hxm = x > 0, hyp = y + 1 < ny, hym = y > 0, hzp = z + 1 < nz, hzm = z > 0;
+                if (hxp) ld3(a.Min, n, cell + 1, mxp);
+                if (hxm) ld3(a.Min, n, cell - 1, mxm);
+                if (hyp) ld3(a.Min, n, cell + nx, myp);
+                if (hym) ld3(a.Min, n, cell - nx, mym);
+                if (hzp) ld3(a.Min, n, cell + (long long)nx * ny, mzp);
+                if (hzm) ld3(a.Min, n, cell - (long long)nx * ny, mzm);
+                T rr = (a.A != (T)0) ? Dv / (2 * a.A) : (T)0;
+                T bx[3] = {rr * m[2], 0, -rr * m[0]};
+                T by[3] = {0, rr * m[2], -rr * m[1]};
+                T bz[3] = {0, 0, 0};
+                T dx[3], dy[3], dz[3], gx[3], gy[3], gz[3];
+                axis_stencil<T>(m, mxp, mxm, hxp, hxm, hx, bx, dx, gx);
+                axis_stencil<T>(m, myp, mym, hyp, hym, hy, by, dy, gy);
+                axis_stencil<T>(m, mzp, mzm, hzp, hzm, hz, bz, dz, gz);
+                T Ac = 2 * a.A / ((T)BM_MU0 * Ms * Ms);
+                T Dc = -2 * Dv / ((T)BM_MU0 * Ms * Ms);
+                T hd[3] = {gx[2], gy[2], -gx[0] - gy[1]};
+#pragma unroll
+                for (int c = 0; c < 3; c++) H[c] += Ac * (dx[c] + dy[c] + dz[c]) + Dc * hd[c];
+            }
+            if (a.modules & BM_MOD_ANIUNI) {
+                T K1 = a.K1_map ? a.K1_map[cell] : a.K1;
+                T dp = (m[0] * a.ea[0] + m[1] * a.ea[1] + m[2] * a.ea[2]) / Ms;
+                T s = (2 / ((T)BM_MU0 * Ms)) * dp * (K1 + 2 * a.K2 * (1 - dp * dp));
+#pragma unroll
+                for (int c = 0; c < 3; c++) H[c] += s * a.ea[c];
+            }
+            if (a.mode == BM_MODE_HEFF) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.Hout[c * n + cell] = H[c];
+                continue;
+            }
+            T mxh[3] = {m[1] * H[2] - m[2] * H[1], m[2] * H[0] - m[0] * H[2], m[0] * H[1] - m[1] * H[0]};
+            T mu[3] = {m[0] / Ms, m[1] / Ms, m[2] / Ms};
+            T mmxh[3] = {mu[1] * mxh[2] - mu[2] * mxh[1], mu[2] * mxh[0] - mu[0] * mxh[2], mu[0] * mxh[1] - mu[1] * mxh[0]};
+            T pre = -(T)BM_GAMMA * a.grel / (1 + a.alpha * a.alpha);
+#pragma unroll
+            for (int c = 0; c < 3; c++) rhs[c] = pre * (mxh[c] + a.alpha * mmxh[c]);
+        }
+        if (a.mode == BM_MODE_LTE) {
+            // 4th-order prediction from the previous step's stages (FSAL), error in FP64
+            double d2 = 0.0, m2 = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                double acc = 0.0;
+                for (int i = 0; i < a.nev; i++) acc += a.cev[i] * (double)a.ev[i][c * n + cell];
+                double pred = (double)a.Mbase[c * n + cell] + dT * (acc + a.crhs * (double)rhs[c]);
+                double d = (double)m[c] - pred;
+                d2 += d * d;
+                m2 += (double)m[c] * (double)m[c];
+            }
+            double l = sqrt(d2) / sqrt(m2);
+            if (l != l) l = 1e300;   // NaN counts as a huge error so the step is rejected
+            if (l > lmax) lmax = l;
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.ev_out[c * n + cell] = rhs[c];
+            continue;
+        }
+        T mn[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            T acc = crhs * rhs[c];
+            for (int i = 0; i < a.nev; i++) acc += cev[i] * a.ev[i][c * n + cell];
+            mn[c] = a.Mbase[c * n + cell] + acc;
+        }
+        if (a.renorm) {
+            T f = Ms / sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
+            mn[0] *= f; mn[1] *= f; mn[2] *= f;
+        }
+        if (a.ev_out) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.ev_out[c * n + cell] = rhs[c];
+        }
+        if (a.copy_to) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.copy_to[c * n + cell] = m[c];
+        }
+        if (a.Mout) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.Mout[c * n + cell] = mn[c];
+        }
+        if (a.do_xfwd) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                cpx<T> *ln = sm + (c * rpb + r) * LSP;
+                *rptr<T>(ln, x) = mn[c];
+                if ((x & 1) == 0 && x == nx - 1) *rptr<T>(ln, x + 1) = 0;   // odd nx: zero the partner slot
+            }
+        }
+    }
+
+    if (a.do_xfwd) {
+        // zero padding beyond the mesh, then forward x transform and store
+        const int first_pad = (nx + 1) >> 1;
+        for (int idx = tid; idx < 3 * rpb * LX; idx += nt) {
+            int qq = idx / LX, mm = idx - qq * LX;
+            if (mm >= first_pad) sm[qq * LSP + eaddr<true>(mm, 1)] = mk<T>(0, 0);
+        }
+        __syncthreads();
+        fft_line<T, true, false>(line, 1, t, qact, a.px, a.twx);
+        xfwd_post<T>(line, LX, a.twx2, t, tpl, qact);
+        if (qact) {
+            cpx<T> *dst = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
+            for (int mm = t; mm < LX; mm += tpl) dst[mm] = line[eaddr<true>(mm, 1)];
+        }
+    }
+
+    if (a.mode == BM_MODE_LTE) {
+        // block max -> device max (bit order of non-negative doubles)
+        for (int o = 16; o > 0; o >>= 1) {
+            double v = __shfl_xor_sync(0xffffffffu, lmax, o);
+            if (v > lmax) lmax = v;
+        }
+        if ((tid & 31) == 0) red[tid >> 5] = lmax;
+        __syncthreads();
+        if (tid == 0) {
+            double b = 0.0;
+            for (int w = 0; w < (nt + 31) / 32; w++) if (red[w] > b) b = red[w];
+            atomicMax(&a.st->lte_bits, (unsigned long long)__double_as_longlong(b));
+        }
+    }
+    if (a.last_kind == BM_LAST_NONE || a.st == nullptr) return;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        unsigned int tk = atomicAdd(&a.st->blocks_done, 1u);
+        is_last = (tk == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last || tid != 0) return;
+    __threadfence();
+    volatile StepState *st = a.st;
+    if (a.last_kind == BM_LAST_FINISH) {
+        st->time = st->time + st->dT;
+        st->stagetime = st->stagetime + st->dT;
+        st->accepted = st->accepted + 1;
+    } else if (a.last_kind == BM_LAST_RESTORED) {
+        st->need_restore = 0;
+    } else if (a.last_kind == BM_LAST_CONTROL) {
+        double lte = __longlong_as_double((long long)atomicAdd(&a.st->lte_bits, 0ull));
+        st->attempts = st->attempts + 1;
+        st->reject_flag = 0;
+        if (!st->primed) {
+            st->primed = 1;
+        } else {
+            st->dT_last = st->dT;
+            st->last_lte = lte;
+            st->lte = lte;
+            double tol = st->tol, dT = st->dT, dmin = st->dT_min, dmax = st->dT_max;
+            double ord = (double)(st->eval_order + 1);
+            if (dmin != dmax) {
+                if (lte > tol && dT > dmin) {
+                    st->time = st->time - dT;
+                    st->stagetime = st->stagetime - dT;
+                    st->accepted = st->accepted - 1;
+                    st->rejected = st->rejected + 1;
+                    double c = pow(tol * 0.8 / lte, 1.0 / ord);
+                    if (c < 0.01) c = 0.01;
+                    dT *= c;
+                    if (dT < dmin) dT = dmin;
+                    st->dT = dT;
+                    st->reject_flag = 1;
+                    st->need_restore = 1;
+                    st->primed = 0;
+                } else if (lte > 0) {
+                    double c = pow(tol * 0.8 / lte, 1.0 / ord);
+                    if (c > st->dT_incr) c = st->dT_incr;
+                    if (c < 0.01) c = 0.01;
+                    dT *= c;
+                    if (dT < dmin) dT = dmin;
+                    if (dT > dmax) dT = dmax;
+                    st->dT = dT;
+                }
+            }
+        }
+    }
+    st->lte_bits = 0ull;
+    st->blocks_done = 0u;
+    __threadfence();
+}
+
+template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
+{
+    int nt = 3 * a.rpb * a.px.tpl;
+    if (nt < 32) nt = 32;
+    if (nt > bm_lb<T>::v) return 201;
+    size_t smem = (size_t)3 * a.rpb * padded_len(a.LX) * sizeof(cpx<T>);
+    if (smem > 200 * 1024) return 202;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_stage<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    int nrows = a.ny * a.nz;
+    dim3 grid((nrows + a.rpb - 1) / a.rpb);
+    k_stage<T><<<grid, nt, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+template int launch_stage<float>(const StageArgs<float> &, cudaStream_t);
+template int launch_stage<double>(const StageArgs<double> &, cudaStream_t);

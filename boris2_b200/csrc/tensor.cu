@@ -1,0 +1,285 @@
+// FP64 demagnetising-tensor build and its transform into the real kernel spectra.
+//
+// Follows the reference's kernel construction:
+//   Newell f, g               Boris/DemagTFunc_fg.cpp:10,45 (written here with asinh/atan directly)
+//   27-point differences      Boris/DemagTFunc_L.cpp:8,59
+//   octant fill + parity      Boris/DemagTFunc.cpp:21,95,172,237 (D = -N, "minus" = true)
+//   switch to far field       ASYMPTOTIC_DISTANCE = 40 cells (Boris/DemagTFunc_Defs.h:9)
+//   spectra                   Boris/DemagKernel.cpp:171,317: real parts of the DFT over the
+//                             (Nx/2+1)(Ny/2+1)(Nz/2+1) octant, h normalised by max(h)
+// The far field is this project's own expansion: the double cell average of
+// (V / 4pi) d_i d_j (1/R), expanded with prod_k (1 + h_k^2 d_k^2/12 + h_k^4 d_k^4/360 + h_k^6 d_k^6/20160)
+// to total derivative order 8; the polynomial coefficients are built on the host
+// (tensor_host.cpp) and evaluated here in FP64.
+#include "common.cuh"
+#include "fft.cuh"
+#include "kernels.h"
+
+#define BM_ASYMPT_DIST 40
+
+__device__ __forceinline__ double csum_d(const double *v, int n)
+{
+    double s = 0.0, c = 0.0;
+    for (int i = 0; i < n; i++) {
+        double t = s + v[i];
+        if (fabs(s) >= fabs(v[i])) c += (s - t) + v[i];
+        else c += (v[i] - t) + s;
+        s = t;
+    }
+    return s + c;
+}
+
+__device__ double nf(double x, double y, double z)
+{
+    double x2 = x * x, y2 = y * y, z2 = z * z;
+    double R = sqrt(x2 + y2 + z2);
+    double t[4] = {0, 0, 0, 0};
+    t[0] = (2.0 * x2 - y2 - z2) * R / 6.0;
+    double rxz = sqrt(x2 + z2), rxy = sqrt(x2 + y2);
+    if (rxz > 0.0) t[1] = 0.5 * y * (z2 - x2) * asinh(y / rxz);
+    if (rxy > 0.0) t[2] = 0.5 * z * (y2 - x2) * asinh(z / rxy);
+    if (x != 0.0 && R > 0.0) t[3] = -x * y * z * atan(y * z / (x * R));
+    return csum_d(t, 4);
+}
+
+__device__ double ng(double x, double y, double z)
+{
+    double x2 = x * x, y2 = y * y, z2 = z * z;
+    double R = sqrt(x2 + y2 + z2);
+    double t[7] = {0, 0, 0, 0, 0, 0, 0};
+    t[0] = -x * y * R / 3.0;
+    double rxy = sqrt(x2 + y2), ryz = sqrt(y2 + z2), rxz = sqrt(x2 + z2);
+    if (rxy > 0.0) t[1] = x * y * z * asinh(z / rxy);
+    if (ryz > 0.0) t[2] = y * (3.0 * z2 - y2) * asinh(x / ryz) / 6.0;
+    if (rxz > 0.0) t[3] = x * (3.0 * z2 - x2) * asinh(y / rxz) / 6.0;
+    if (z != 0.0 && R > 0.0) t[4] = -z2 * z * atan(x * y / (z * R)) / 6.0;
+    if (y != 0.0 && R > 0.0) t[5] = -y2 * z * atan(x * z / (y * R)) / 2.0;
+    if (x != 0.0 && R > 0.0) t[6] = -x2 * z * atan(y * z / (x * R)) / 2.0;
+    return csum_d(t, 7);
+}
+
+template <bool G>
+__device__ double newellL(double x, double y, double z, double hx, double hy, double hz)
+{
+    double v[27];
+    int m = 0;
+    const double cw[3] = {-1.0, 2.0, -1.0};
+    for (int a = -1; a <= 1; a++)
+        for (int b = -1; b <= 1; b++)
+            for (int c = -1; c <= 1; c++) {
+                double w = cw[a + 1] * cw[b + 1] * cw[c + 1];
+                v[m++] = w * (G ? ng(x + a * hx, y + b * hy, z + c * hz) : nf(x + a * hx, y + b * hy, z + c * hz));
+            }
+    return csum_d(v, 27) / (4.0 * M_PI * hx * hy * hz);
+}
+
+// far field: D_c = V/(4 pi) sum_n Q_{c,n}(u,v,w) / R^(n+1), coefficient layout per comp c:
+// for n in {2,4,6,8}: monomials (i,j,k), i+j+k = n, ordered i descending then j descending
+__device__ double far_eval(const double *__restrict__ q, double u, double v, double w, double R)
+{
+    double pu[9], pv[9], pw[9];
+    pu[0] = pv[0] = pw[0] = 1.0;
+    for (int i = 1; i < 9; i++) { pu[i] = pu[i - 1] * u; pv[i] = pv[i - 1] * v; pw[i] = pw[i - 1] * w; }
+    double tot[4];
+    int off = 0;
+    for (int o = 0; o < 4; o++) {
+        int n = 2 + 2 * o;
+        double acc[45];
+        int m = 0;
+        for (int i = n; i >= 0; i--)
+            for (int j = n - i; j >= 0; j--) {
+                int k = n - i - j;
+                acc[m++] = q[off++] * pu[i] * pv[j] * pw[k];
+            }
+        tot[o] = csum_d(acc, m) / pow(R, n + 1);
+    }
+    return csum_d(tot, 4);
+}
+
+// octant values D(i,j,k), i<nx, j<ny, k<nz -> oct[((k*ny + j)*nx + i)*6 + c], c = xx,yy,zz,xy,xz,yz
+__global__ void k_tensor_octant(double *oct, int nx, int ny, int nz, double hx, double hy, double hz,
+                                const double *__restrict__ farq, int two_d)
+{
+    long long N = (long long)nx * ny * nz;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % nx);
+        int j = (int)((p / nx) % ny);
+        int k = (int)(p / ((long long)nx * ny));
+        double x = i * hx, y = j * hy, z = k * hz;
+        double v[6];
+        bool far = (i >= BM_ASYMPT_DIST || j >= BM_ASYMPT_DIST || k >= BM_ASYMPT_DIST ||
+                    (long long)i * i + (long long)j * j + (long long)k * k >= (long long)BM_ASYMPT_DIST * BM_ASYMPT_DIST);
+        if (far) {
+            double R = sqrt(x * x + y * y + z * z);
+            double u = x / R, vv = y / R, w = z / R;
+            double V = hx * hy * hz / (4.0 * M_PI);
+            for (int c = 0; c < 6; c++) v[c] = V * far_eval(farq + c * BM_FARQ_PER_COMP, u, vv, w, R);
+        } else {
+            v[0] = -newellL<false>(x, y, z, hx, hy, hz);
+            v[1] = -newellL<false>(y, x, z, hy, hx, hz);
+            v[2] = -newellL<false>(z, y, x, hz, hy, hx);
+            v[3] = -newellL<true>(x, y, z, hx, hy, hz);
+            v[4] = two_d ? 0.0 : -newellL<true>(x, z, y, hx, hz, hy);
+            v[5] = two_d ? 0.0 : -newellL<true>(y, z, x, hy, hz, hx);
+        }
+        for (int c = 0; c < 6; c++) oct[p * 6 + c] = v[c];
+    }
+}
+
+// fill one component on the full N grid (complex, imaginary zero) from the octant with parity
+__global__ void k_tensor_fill(cpx<double> *F, const double *__restrict__ oct, int comp, int nx, int ny, int nz,
+                              int Nx, int Ny, int Nz)
+{
+    long long Ntot = (long long)Nx * Ny * Nz;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < Ntot; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % Nx);
+        int j = (int)((p / Nx) % Ny);
+        int k = (int)(p / ((long long)Nx * Ny));
+        int ai = i <= Nx / 2 ? i : Nx - i, sx = i <= Nx / 2 ? 1 : -1;
+        int aj = j <= Ny / 2 ? j : Ny - j, sy = j <= Ny / 2 ? 1 : -1;
+        int ak = k <= Nz / 2 ? k : Nz - k, sz = k <= Nz / 2 ? 1 : -1;
+        double val = 0.0;
+        if (ai < nx && aj < ny && ak < nz) {
+            val = oct[(((long long)ak * ny + aj) * nx + ai) * 6 + comp];
+            if (comp == 3) val *= sx * sy;
+            else if (comp == 4) val *= sx * sz;
+            else if (comp == 5) val *= sy * sz;
+        }
+        F[p] = mk<double>(val, 0.0);
+    }
+}
+
+// extract Re on the octant into the kernel planes K[comp][(kz*Ky1 + ky)*Kx1 + kx] (type T)
+template <typename T>
+__global__ void k_tensor_extract(T *K, const cpx<double> *__restrict__ F, int comp, int Nx, int Ny, int Nz)
+{
+    int Kx1 = Nx / 2 + 1, Ky1 = Ny / 2 + 1, Kz1 = Nz / 2 + 1;
+    long long nk = (long long)Kx1 * Ky1 * Kz1;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nk; q += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(q % Kx1);
+        int j = (int)((q / Kx1) % Ky1);
+        int k = (int)(q / ((long long)Kx1 * Ky1));
+        K[comp * nk + q] = (T)F[(long long)i + (long long)j * Nx + (long long)k * Nx * Ny].x;
+    }
+}
+
+// Generic strided batched line FFT (setup path and tests): line li (0 <= li < ninner), outer index
+// blockIdx.y; element e at data[li * ls + e * es + blockIdx.y * os]. A block transforms W lines.
+template <typename T, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_fft_strided(cpx<T> *data, FFTPlan P, const cpx<T> *__restrict__ tw, long long es, long long ls,
+                              int ninner, int W, long long os)
+{
+    extern __shared__ unsigned char smraw[];
+    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
+    int L = P.L;
+    int li0 = blockIdx.x * W;
+    cpx<T> *g = data + (long long)blockIdx.y * os;
+    int nt = blockDim.x;
+    // load tile [e][w]
+    for (int idx = threadIdx.x; idx < L * W; idx += nt) {
+        int e, w;
+        if (es == 1) { w = idx / L; e = idx % L; }
+        else { e = idx / W; w = idx % W; }
+        int li = li0 + w;
+        sm[e * W + w] = (li < ninner) ? g[(long long)li * ls + (long long)e * es] : mk<T>(0, 0);
+    }
+    __syncthreads();
+    int l = threadIdx.x % W, t = threadIdx.x / W;
+    bool active = t < P.tpl;
+    fft_line<T, false, INV>(sm + l, W, t, active, P, tw);
+    for (int idx = threadIdx.x; idx < L * W; idx += nt) {
+        int e, w;
+        if (es == 1) { w = idx / L; e = idx % L; }
+        else { e = idx / W; w = idx % W; }
+        int li = li0 + w;
+        if (li < ninner) g[(long long)li * ls + (long long)e * es] = sm[e * W + w];
+    }
+}
+
+template <typename T>
+int launch_fft_strided(cpx<T> *data, const FFTPlan &P, const cpx<T> *tw, long long es, long long ls, int ninner,
+                       long long os, int nouter, bool inv, cudaStream_t s)
+{
+    int W = 1;
+    while (W < 8 && W < ninner) W *= 2;
+    size_t smem = (size_t)P.L * W * sizeof(cpx<T>);
+    while ((smem > 96 * 1024 || W * P.tpl > bm_lb<T>::v) && W > 1) { W /= 2; smem = (size_t)P.L * W * sizeof(cpx<T>); }
+    int nt = W * P.tpl;
+    if (nt < 32) nt = 32;
+    if (nt > bm_lb<T>::v) return 1;
+    dim3 grid((ninner + W - 1) / W, nouter);
+    if (inv) {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k_fft_strided<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_fft_strided<T, true><<<grid, nt, smem, s>>>(data, P, tw, es, ls, ninner, W, os);
+    } else {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k_fft_strided<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_fft_strided<T, false><<<grid, nt, smem, s>>>(data, P, tw, es, ls, ninner, W, os);
+    }
+    return (int)cudaGetLastError();
+}
+
+template int launch_fft_strided<float>(cpx<float> *, const FFTPlan &, const cpx<float> *, long long, long long, int, long long, int, bool, cudaStream_t);
+template int launch_fft_strided<double>(cpx<double> *, const FFTPlan &, const cpx<double> *, long long, long long, int, long long, int, bool, cudaStream_t);
+
+static int grid_for(long long n)
+{
+    long long b = (n + 255) / 256;
+    if (b > 148 * 32) b = 148 * 32;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// Build the kernel planes (6 components, type T) for one mesh on the device.
+// twx/twy/twz are FP64 tables of exp(-2 pi i m / N) for N = Nx, Ny, Nz.
+template <typename T>
+int build_kernels_device(T *K, int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz,
+                         const double *farq_dev, const cpx<double> *twx, const cpx<double> *twy,
+                         const cpx<double> *twz, cudaStream_t s)
+{
+    double hm = fmax(hx, fmax(hy, hz));
+    hx /= hm; hy /= hm; hz /= hm;
+    long long noct = (long long)nx * ny * nz;
+    long long Ntot = (long long)Nx * Ny * Nz;
+    double *oct = nullptr;
+    cpx<double> *F = nullptr;
+    if (cudaMalloc(&oct, sizeof(double) * 6 * noct) != cudaSuccess) return 2;
+    if (cudaMalloc(&F, sizeof(cpx<double>) * Ntot) != cudaSuccess) { cudaFree(oct); return 2; }
+    k_tensor_octant<<<grid_for(noct), 256, 0, s>>>(oct, nx, ny, nz, hx, hy, hz, farq_dev, nz == 1);
+    FFTPlan px, py, pz;
+    bm_make_plan(Nx, px); bm_make_plan(Ny, py); bm_make_plan(Nz, pz);
+    int rc = 0;
+    for (int c = 0; c < 6 && !rc; c++) {
+        if (nz == 1 && (c == 4 || c == 5)) {
+            cudaMemsetAsync(K + (long long)c * (Nx / 2 + 1) * (Ny / 2 + 1) * (Nz / 2 + 1), 0,
+                            sizeof(T) * (Nx / 2 + 1) * (Ny / 2 + 1) * (Nz / 2 + 1), s);
+            continue;
+        }
+        k_tensor_fill<<<grid_for(Ntot), 256, 0, s>>>(F, oct, c, nx, ny, nz, Nx, Ny, Nz);
+        // x lines: contiguous, Ny*Nz of them
+        if (Nx > 1) rc |= launch_fft_strided<double>(F, px, twx, 1, Nx, Ny * Nz, 0, 1, false, s);
+        // y lines: stride Nx, Nx lines per z plane
+        if (Ny > 1) rc |= launch_fft_strided<double>(F, py, twy, Nx, 1, Nx, (long long)Nx * Ny, Nz, false, s);
+        // z lines: stride Nx*Ny, Nx*Ny lines
+        if (Nz > 1) rc |= launch_fft_strided<double>(F, pz, twz, (long long)Nx * Ny, 1, Nx * Ny, 0, 1, false, s);
+        k_tensor_extract<T><<<grid_for((long long)(Nx / 2 + 1) * (Ny / 2 + 1) * (Nz / 2 + 1)), 256, 0, s>>>(K, F, c, Nx, Ny, Nz);
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFree(oct);
+    cudaFree(F);
+    if (e != cudaSuccess) return 3;
+    return rc ? 4 : (int)cudaGetLastError();
+}
+
+template int build_kernels_device<float>(float *, int, int, int, int, int, int, double, double, double, const double *,
+                                         const cpx<double> *, const cpx<double> *, const cpx<double> *, cudaStream_t);
+template int build_kernels_device<double>(double *, int, int, int, int, int, int, double, double, double, const double *,
+                                          const cpx<double> *, const cpx<double> *, const cpx<double> *, cudaStream_t);
+
+// raw tensor octant to host (tests)
+int tensor_octant_device(double *oct_dev, int nx, int ny, int nz, double hx, double hy, double hz, const double *farq_dev,
+                         cudaStream_t s)
+{
+    double hm = fmax(hx, fmax(hy, hz));
+    k_tensor_octant<<<grid_for((long long)nx * ny * nz), 256, 0, s>>>(oct_dev, nx, ny, nz, hx / hm, hy / hm, hz / hm, farq_dev, nz == 1);
+    return (int)cudaGetLastError();
+}

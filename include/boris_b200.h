@@ -1,0 +1,153 @@
+/*
+ * boris_b200 — C ABI of the B200-native micromagnetic field-and-integrate path.
+ *
+ * Plain C: opaque context, plain pointers and sizes, int status (0 = ok, otherwise an
+ * error code; bm_last_error() gives the text). Host arrays of vectors are AoS doubles
+ * (x, y, z per cell), cells ordered x fastest, then y, then z — the layout of the
+ * reference's VEC<DBL3> (BorisLib/VEC.h). One context per host thread; all work goes
+ * to one internal CUDA stream.
+ *
+ * Each entry point names the reference interface it replaces (paths in the reference tree).
+ */
+#ifndef BORIS_B200_H
+#define BORIS_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bm_ctx bm_ctx;
+
+/* modules (the reference's MOD_ values for the FM mesh modules on this path) */
+#define BM_DEMAG   1   /* Boris/Demag.h            MOD_DEMAG */
+#define BM_EXCH    2   /* Boris/Exchange.h         MOD_EXCHANGE (Exch_6ngbr_Neu) */
+#define BM_IDMI    4   /* Boris/iDMExchange.h      MOD_IDMEXCHANGE (replaces BM_EXCH) */
+#define BM_ANIUNI  8   /* Boris/Anisotropy.h       MOD_ANIUNI */
+#define BM_ZEEMAN 16   /* Boris/Zeeman.h           MOD_ZEEMAN */
+
+/* evaluation methods (Boris/DiffEq_Defs.h EVAL_RK4, EVAL_RKDP54) */
+#define BM_RK4    0
+#define BM_RKDP54 1
+
+/* precision */
+#define BM_FP64   0   /* plain form: every array and transform in FP64 */
+#define BM_MIXED  1   /* FP32 FFTs, convolution and stages; FP64 tensor build and RKDP54 error norm */
+
+/* error codes */
+#define BM_OK          0
+#define BM_EINVAL      1
+#define BM_ECUDA       2
+#define BM_ENOMEM      3
+#define BM_ESTATE      4
+#define BM_EUNSUPPORTED 5
+#define BM_ENONFINITE  6
+
+typedef struct {
+    long long accepted;    /* accepted steps since creation (the reference's iteration counter) */
+    long long rejected;    /* RKDP54 rejections */
+    long long attempts;    /* RKDP54 stage-0 evaluations */
+    double time;           /* simulated time, s */
+    double dT;             /* current time step, s */
+    double last_lte;       /* last RKDP54 error estimate (max over cells of |M - M4| / |M|) */
+} bm_stats;
+
+/* Context (one device). Replaces the reference's SuperMesh/ODECommon ownership of meshes
+ * (Boris/SuperMesh.h, Boris/DiffEq_CommonBase.h). */
+int bm_create(int device, bm_ctx **out);
+int bm_destroy(bm_ctx *ctx);
+const char *bm_last_error(void);
+int bm_version(void);
+
+/* Add a ferromagnetic mesh: n cells, cellsize h (m), origin (m).
+ * Replaces Mesh creation + MeshBase::n / h / meshRect (Boris/MeshBase.h). */
+int bm_add_mesh(bm_ctx *ctx, int nx, int ny, int nz, double hx, double hy, double hz,
+                double ox, double oy, double oz, int *mesh_id);
+
+/* Material parameters (Boris/MeshParams.h: Ms, A, D, alpha, grel, K1, K2, mcanis_ea1).
+ * grel is the relative gyromagnetic ratio (gamma / 2.212761569e5). */
+int bm_set_material(bm_ctx *ctx, int mesh, double Ms, double A, double alpha, double grel,
+                    double K1, double K2, const double *ea3, double D);
+
+/* Per-cell maps of Ms and K1 (absolute values, one per cell), or NULL for uniform.
+ * Replaces the spatial scaling of MaterialParameter (Boris/MaterialParameter.h:805,
+ * setparamvar) read through update_parameters_mcoarse (Boris/MeshParamsControl.h:56). */
+int bm_set_material_maps(bm_ctx *ctx, int mesh, const double *Ms_map, const double *K1_map);
+
+/* Module set for a mesh (bitmask of BM_*). Replaces MeshBase::AddModule / DelModule
+ * (Boris/MeshBaseModules.cpp); BM_IDMI and BM_EXCH are exclusive as in the reference
+ * (Boris/SimSharedData.cpp:179). */
+int bm_set_modules(bm_ctx *ctx, int mesh, int modules);
+
+/* Applied field: nsamples piecewise-constant 3-vectors (A/m) over [0, t_span); with
+ * nsamples == 1 the field is constant. Replaces Zeeman::SetField / H_equation
+ * (Boris/Zeeman.cpp:164); as there, the field is evaluated at the step start time. */
+int bm_set_field(bm_ctx *ctx, int mesh, const double *Ha, int nsamples, double t_span);
+
+/* ODE: evaluation method and time step. Replaces SetODE (Boris/DiffEq_Common.cpp:79,
+ * "setode LLG RK4|RKDP54") and SetdT ("setdt", Boris/Commands.cpp:1914). Selecting an
+ * evaluation method loads its defaults (Boris/DiffEq_CommonBase_Control.cpp:9). */
+int bm_set_ode(bm_ctx *ctx, int eval, double dt);
+
+/* Adaptive step control for RKDP54. Replaces SetAdaptiveTimeStepCtrl ("astepctrl",
+ * Boris/Commands.cpp:1931, Boris/DiffEq_CommonBase.h:236): err_fail = relative error
+ * tolerance, dT_incr = maximum increase factor, dT_min / dT_max = step limits. */
+int bm_set_astepctrl(bm_ctx *ctx, double err_fail, double dT_incr, double dT_min, double dT_max);
+
+/* Precision: BM_FP64 or BM_MIXED (default BM_MIXED). Must be set before the first run. */
+int bm_set_precision(bm_ctx *ctx, int precision);
+
+/* Magnetization M (A/m, |M| = Ms), AoS doubles, 3 * n values. Replaces writes/reads of
+ * MeshBase::M (VEC_VC<DBL3>, Boris/Mesh.h). Setting M un-primes RKDP54 as a restart does. */
+int bm_set_m(bm_ctx *ctx, int mesh, const double *M);
+int bm_get_m(bm_ctx *ctx, int mesh, double *M);
+
+/* Demagnetising field of the current M into H (3 * n doubles) and the demag energy
+ * density -mu0/(2 n) sum M.H. Replaces Demag::UpdateField (Boris/Demag.cpp:170) /
+ * DemagCUDA::UpdateField (Boris/DemagCUDA.cpp:106). */
+int bm_compute_hdemag(bm_ctx *ctx, int mesh, double *H, double *energy);
+
+/* Effective field of the current M with all modules of the mesh (Zeeman, demag,
+ * exchange / iDMI, anisotropy), as MeshBase::UpdateModules leaves Heff
+ * (Boris/MeshBaseModules.cpp:76). */
+int bm_compute_heff(bm_ctx *ctx, int mesh, double *H);
+
+/* Advance until `steps` more steps are accepted. Replaces the AdvanceTime loop
+ * (Boris/SuperMeshSimulation.cpp:84,122) over ODECommon_Base::Iterate[CUDA]
+ * (Boris/DiffEq_CommonBase_Iterate.cpp:63, Boris/DiffEq_CommonBase_IterateCUDA.cpp:13). */
+int bm_run(bm_ctx *ctx, int steps, bm_stats *out);
+int bm_get_stats(bm_ctx *ctx, bm_stats *out);
+
+/* Number of cells of a mesh and the FFT sizes its demag convolution uses. */
+int bm_mesh_info(bm_ctx *ctx, int mesh, int *n3, int *N3);
+
+/* Device-resident access for benchmarks and wrappers: the device pointer of the
+ * current M planes ([3][n] of float (BM_MIXED) or double (BM_FP64)) and a
+ * synchronisation point. */
+int bm_device_m(bm_ctx *ctx, int mesh, void **dptr, int *elem_bytes);
+int bm_sync(bm_ctx *ctx);
+/* Number of kernels one bm_run step enqueues (for launch accounting). */
+int bm_kernels_per_step(bm_ctx *ctx, int *count);
+
+/* bm_run with its device time (CUDA events on the context's stream around the whole run). */
+int bm_run_timed(bm_ctx *ctx, int steps, bm_stats *out, double *device_ms);
+
+/* Time each kernel of one field evaluation of a mesh separately (reps launches each, CUDA
+ * events on the context's stream) and report the average ms per launch and the algorithmic
+ * bytes each launch must move: index 0 = y/z pass 1 (2D: ymid2d, 3D: yfwd), 1 = zmid (3D),
+ * 2 = yinv (3D), 3 = fused stage kernel (inverse x FFT, fields, LLG, update, forward x FFT).
+ * Unused slots are 0. Leaves the spectrum buffers stale (the next run re-primes them). */
+int bm_time_kernels(bm_ctx *ctx, int mesh, int reps, double *ms4, double *bytes4);
+
+/* Test hooks (used by the test suite only). */
+/* FP64 demag kernel spectra (octant (Nx/2+1)(Ny/2+1)(Nz/2+1), 6 components xx,yy,zz,xy,xz,yz). */
+int bm_debug_kernels(bm_ctx *ctx, int mesh, double *K6);
+/* Raw FP64 tensor octant values D(i,j,k) for i<nx, j<ny, k<nz: 6 per point. */
+int bm_debug_tensor(int device, int nx, int ny, int nz, double hx, double hy, double hz, double *oct6);
+/* Batched complex FFT on the device of `howmany` contiguous lines of length L (in place,
+ * interleaved re/im doubles on the host); precision BM_FP64 or BM_MIXED; inverse != 0
+ * uses exp(+2 pi i ...), unnormalised. */
+int bm_debug_fft(int device, int L, int howmany, int precision, int inverse, double *data);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

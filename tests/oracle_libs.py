@@ -1,0 +1,208 @@
+"""ctypes access to the oracle (test infrastructure only).
+
+  liboracle.so    oracle/oracle.c — the project's FP64 CPU restatement of the path
+  libborisref.so  the reference's own CPU sources compiled by oracle/Makefile
+
+Both are built from oracle/Makefile when missing (the reference build only where the
+reference tree is present; its .so travels with the repository otherwise).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
+REF_SO = os.path.join(ORACLE_DIR, "_ref", "libborisref.so")
+REF_TREE = "/root/reference"
+
+P = ctypes.c_void_p
+D = ctypes.c_double
+I = ctypes.c_int
+DP = ctypes.POINTER(ctypes.c_double)
+
+_orc = None
+_ref = None
+
+
+def dp(a):
+    return a.ctypes.data_as(DP)
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("nx", I), ("ny", I), ("nz", I), ("hx", D), ("hy", D), ("hz", D),
+                ("Ms", D), ("A", D), ("D", D), ("alpha", D), ("grel", D), ("K1", D), ("K2", D),
+                ("ea", D * 3), ("Ms_map", DP), ("K1_map", DP), ("modules", I),
+                ("Ha", DP), ("nHa", I), ("Ha_tspan", D)]
+
+
+class OrcStats(ctypes.Structure):
+    _fields_ = [("accepted", ctypes.c_long), ("rejected", ctypes.c_long), ("evals", ctypes.c_long),
+                ("time", D), ("dT", D), ("last_lte", D)]
+
+
+def oracle():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_SO):
+            subprocess.run(["make", "-C", ORACLE_DIR, "oracle"], check=True, capture_output=True)
+        L = ctypes.CDLL(ORACLE_SO)
+        L.orc_demag_create.restype = P
+        L.orc_demag_create.argtypes = [I, I, I, D, D, D, I, I, I]
+        L.orc_demag_apply.restype = D
+        L.orc_demag_apply.argtypes = [P, DP, DP, I]
+        L.orc_demag_destroy.argtypes = [P]
+        L.orc_solver_create.restype = P
+        L.orc_solver_create.argtypes = [I, ctypes.POINTER(MeshDesc), I, D, D, D, D, D]
+        L.orc_set_m.argtypes = [P, I, DP]
+        L.orc_get_m.argtypes = [P, I, DP]
+        L.orc_compute_heff.argtypes = [P, I, DP]
+        L.orc_run.argtypes = [P, I, ctypes.POINTER(OrcStats)]
+        L.orc_solver_destroy.argtypes = [P]
+        L.orc_newell_f.restype = D
+        L.orc_newell_f.argtypes = [D, D, D]
+        L.orc_newell_g.restype = D
+        L.orc_newell_g.argtypes = [D, D, D]
+        L.orc_asymptotic.argtypes = [D, D, D, D, D, D, DP]
+        L.orc_selfdemag.argtypes = [D, D, D, DP]
+        L.orc_tensor.argtypes = [I, I, I, I, I, I, D, D, D, DP, DP]
+        L.orc_kernels.argtypes = [I, I, I, I, I, I, D, D, D, DP, DP]
+        L.orc_field_exchange.argtypes = [I, I, I, D, D, D, DP, D, DP, DP]
+        L.orc_field_idmi.argtypes = [I, I, I, D, D, D, DP, D, D, DP, DP]
+        L.orc_field_aniuni.argtypes = [I, DP, DP, DP, D, DP, DP]
+        L.bm_oracle_fft.argtypes = [I, DP, I]
+        _orc = L
+    return _orc
+
+
+def ref_available():
+    return os.path.exists(REF_SO) or os.path.isdir(REF_TREE)
+
+
+def reference():
+    """The reference's compiled CPU code (None when neither the .so nor the tree is present)."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            if not os.path.isdir(REF_TREE):
+                return None
+            subprocess.run(["make", "-C", ORACLE_DIR, "-j8", "ref"], check=True, capture_output=True)
+        L = ctypes.CDLL(REF_SO)
+        L.ref_selfdemag.argtypes = [D, D, D, DP]
+        L.ref_tensor.argtypes = [I, I, I, I, I, I, D, D, D, DP, DP]
+        L.ref_kernels.argtypes = [I, I, I, D, D, D, DP, DP]
+        L.ref_hdemag.argtypes = [I, I, I, D, D, D, DP, DP, DP]
+        L.ref_demag_create.restype = P
+        L.ref_demag_create.argtypes = [I, I, I, D, D, D]
+        L.ref_demag_eval.restype = D
+        L.ref_demag_eval.argtypes = [P, DP, DP]
+        L.ref_demag_destroy.argtypes = [P]
+        L.ref_exchange.argtypes = [I, I, I, D, D, D, DP, DP, DP, DP]
+        L.ref_idmi.argtypes = [I, I, I, D, D, D, DP, DP, DP, DP, DP]
+        _ref = L
+    return _ref
+
+
+# ---------------------------------------------------------------- convenience wrappers
+def orc_hdemag(M, n, h, N=None):
+    """FP64 demag field of M (n cells x 3) on mesh n with cellsize h (oracle)."""
+    nx, ny, nz = n
+    if N is None:
+        N = (2 * nx, 2 * ny, 2 * nz if nz > 1 else 1)
+    L = oracle()
+    d = L.orc_demag_create(nx, ny, nz, h[0], h[1], h[2], N[0], N[1], N[2])
+    Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+    H = np.zeros_like(Mf)
+    dot = L.orc_demag_apply(P(d), dp(Mf), dp(H), 0)
+    L.orc_demag_destroy(P(d))
+    return H.reshape(-1, 3), dot
+
+
+def ref_hdemag(M, n, h):
+    R = reference()
+    Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+    H = np.zeros_like(Mf)
+    e = np.zeros(1)
+    rc = R.ref_hdemag(n[0], n[1], n[2], h[0], h[1], h[2], dp(Mf), dp(H), dp(e))
+    assert rc == 0
+    return H.reshape(-1, 3), e[0]
+
+
+class OracleSolver:
+    """Oracle solver over one or more meshes (a common time step, like ODECommon)."""
+
+    def __init__(self, meshes, evaluation=0, dt=1e-13, tol=1e-4, dT_incr=2.0, dT_min=1e-15, dT_max=3e-12):
+        self._keep = []
+        arr = (MeshDesc * len(meshes))()
+        for i, m in enumerate(meshes):
+            d = arr[i]
+            d.nx, d.ny, d.nz = m["n"]
+            d.hx, d.hy, d.hz = m["h"]
+            d.Ms = m.get("Ms", 8e5); d.A = m.get("A", 1.3e-11); d.D = m.get("D", 0.0)
+            d.alpha = m.get("alpha", 0.5); d.grel = m.get("grel", 1.0)
+            d.K1 = m.get("K1", 0.0); d.K2 = m.get("K2", 0.0)
+            ea = m.get("ea", (0.0, 0.0, 1.0))
+            en = np.linalg.norm(ea)
+            for k in range(3):
+                d.ea[k] = ea[k] / en if en > 0 else 0.0
+            for key in ("Ms_map", "K1_map"):
+                if m.get(key) is not None:
+                    a = np.ascontiguousarray(np.asarray(m[key], dtype=np.float64).reshape(-1))
+                    self._keep.append(a)
+                    setattr(d, key, dp(a))
+            d.modules = m.get("modules", 1 | 2 | 16)
+            Ha = np.ascontiguousarray(np.asarray(m.get("Ha", (0.0, 0.0, 0.0)), dtype=np.float64).reshape(-1))
+            self._keep.append(Ha)
+            d.Ha = dp(Ha)
+            d.nHa = Ha.size // 3
+            d.Ha_tspan = m.get("Ha_tspan", 0.0)
+        self._arr = arr
+        self.n = [m["n"][0] * m["n"][1] * m["n"][2] for m in meshes]
+        self.h = oracle().orc_solver_create(len(meshes), arr, evaluation, dt, tol, dT_incr, dT_min, dT_max)
+
+    def set_m(self, M, mesh=0):
+        a = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+        oracle().orc_set_m(P(self.h), mesh, dp(a))
+
+    def get_m(self, mesh=0):
+        a = np.zeros(3 * self.n[mesh])
+        oracle().orc_get_m(P(self.h), mesh, dp(a))
+        return a.reshape(-1, 3)
+
+    def heff(self, mesh=0):
+        a = np.zeros(3 * self.n[mesh])
+        oracle().orc_compute_heff(P(self.h), mesh, dp(a))
+        return a.reshape(-1, 3)
+
+    def run(self, steps):
+        st = OrcStats()
+        rc = oracle().orc_run(P(self.h), steps, ctypes.byref(st))
+        assert rc == 0
+        return {k: getattr(st, k) for k, _ in OrcStats._fields_}
+
+    def close(self):
+        if self.h:
+            oracle().orc_solver_destroy(P(self.h))
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def sphere_random(n, seed, Ms=1.0):
+    """Per-cell unit vectors uniform on the sphere (seeded), scaled by Ms."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    return v * (np.asarray(Ms).reshape(-1, 1) if np.ndim(Ms) else Ms)
+
+
+def tilted_z(n, seed, max_deg=15.0, Ms=1.0):
+    """+z with per-cell tilts theta ~ U[0, max_deg], phi ~ U[0, 2 pi) (seeded)."""
+    rng = np.random.default_rng(seed)
+    th = np.deg2rad(rng.uniform(0.0, max_deg, n))
+    ph = rng.uniform(0.0, 2 * np.pi, n)
+    v = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=1)
+    return v * Ms
