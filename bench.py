@@ -108,7 +108,7 @@ class ClockSampler:
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
         mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]})
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and s[3 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
@@ -175,6 +175,7 @@ def main():
     ap.add_argument("--config", default="film3d_512x512x16", choices=sorted(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="timed steps only (for profiler launch lists)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     ncell = cfg["n"][0] * cfg["n"][1] * cfg["n"][2]
@@ -246,6 +247,11 @@ def main():
     steps_done = st["accepted"] - st0["accepted"]
     value = ncell * steps_done * ws / (ms * 1e-3) / 1e6
     attempts = st["attempts"] - st0["attempts"]
+    if args.no_extras:
+        if rank == 0:
+            print(json.dumps(dict(base, value=value, ms_per_step=ms / max(steps_done, 1), note="no extras")))
+        c.close()
+        return
     # e2e through the C ABI with host buffers (pinned), copies inside the timed region
     try:
         import torch
@@ -292,7 +298,8 @@ def main():
                          "launch_ms": kms[dom]},
                kernels={names[i]: {"ms": kms[i], "GB/s": (kbytes[i] / (kms[i] * 1e-3) / 1e9 if kms[i] > 0 else None)}
                         for i in range(4) if kms[i] > 0},
-               rkdp={"attempts": attempts, "accepted": steps_done, "dT": st["dT"]})
+               rkdp={"attempts": attempts, "accepted": steps_done, "dT": st["dT"]},
+               tiles=c.tiles(0))
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_reference_rate(cfg)

@@ -82,6 +82,7 @@ _SIGS = {
     "bm_kernels_per_step": (_I, [_P, _IP]),
     "bm_run_timed": (_I, [_P, _I, ctypes.POINTER(Stats), _DP]),
     "bm_time_kernels": (_I, [_P, _I, _I, _DP, _DP]),
+    "bm_tiles": (_I, [_P, _I, _IP]),
     "bm_debug_kernels": (_I, [_P, _I, _DP]),
     "bm_debug_tensor": (_I, [_I, _I, _I, _I, _D, _D, _D, _DP]),
     "bm_debug_fft": (_I, [_I, _I, _I, _I, _I, _DP]),
@@ -237,6 +238,12 @@ class Context:
         _check(lib().bm_time_kernels(self._h, mesh, int(reps), _dp(ms), _dp(by)))
         return ms, by
 
+    def tiles(self, mesh=0):
+        """Autotuned tile shapes: 2D y width, 3D y width, z width, stage rows per block."""
+        t = (ctypes.c_int * 4)()
+        _check(lib().bm_tiles(self._h, mesh, t))
+        return {"ymid2d_W": t[0], "ypass_W": t[1], "zmid_W": t[2], "stage_rows": t[3]}
+
     def stats(self):
         st = Stats()
         _check(lib().bm_get_stats(self._h, ctypes.byref(st)))
@@ -280,7 +287,7 @@ def debug_fft(x, precision=FP64, inverse=False, device=0):
     """Batched 1D complex FFT along the last axis on the GPU (unnormalised)."""
     x = np.asarray(x, dtype=np.complex128)
     L = x.shape[-1]
-    flat = np.ascontiguousarray(x.reshape(-1, L))
+    flat = np.array(x.reshape(-1, L), dtype=np.complex128, copy=True)
     buf = np.ascontiguousarray(flat.view(np.float64).reshape(-1))
     _check(lib().bm_debug_fft(device, L, flat.shape[0], int(precision), int(bool(inverse)), _dp(buf)))
     return buf.view(np.complex128).reshape(x.shape)

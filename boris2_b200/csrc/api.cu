@@ -96,6 +96,7 @@ struct bm_ctx {
     cudaGraph_t graph = nullptr;
     int graph_eval = -1;
     bool eval_chosen = false;
+    bool autotune = true;
     int kernels_per_step = 0;
     double *farq = nullptr;
     StepState host_st;
@@ -187,24 +188,25 @@ void choose_tiles(Mesh &m)
 {
     const size_t cs = sizeof(cpx<T>);
     const int lim = bm_lb<T>::v;
-    // 2D y pass: 3 components per block, transformed one after another
+    // 2D y pass: 3 components per block, transformed one after another; keep the grid at
+    // least one wave of the GPU where the mesh allows it
     {
         int W = 16;
-        while (W > 1 && ((size_t)3 * m.Ny * W * cs > 100 * 1024 || W * m.py.tpl > lim)) W /= 2;
+        while (W > 1 && (ymid2d_smem<T>(m.Ny, W) > 110 * 1024 || W * m.py.tpl > lim || (m.LX / W) < 148)) W /= 2;
         if (W > m.LX) W = pow2_floor(m.LX);
         m.W2 = W;
     }
-    // 3D y passes
+    // 3D y passes: small tiles so several blocks share an SM and overlap load and compute
     {
-        int W = 16;
+        int W = 4;
         while (W > 1 && ((size_t)m.Ny * W * cs > 100 * 1024 || W * m.py.tpl > lim)) W /= 2;
         if (W > m.LX) W = pow2_floor(m.LX);
         m.Wy = W;
     }
     // 3D z pass: two mirror pencils in parallel, components one after another
     {
-        int W = 64;
-        while (W > 1 && ((size_t)6 * m.Nz * W * cs > 100 * 1024 || 2 * W * m.pz.tpl > lim)) W /= 2;
+        int W = 32;
+        while (W > 1 && (zmid_smem<T>(m.Nz, W) > 72 * 1024 || 2 * W * m.pz.tpl > lim)) W /= 2;
         if (W > m.LX) W = pow2_floor(m.LX);
         m.Wz = W;
     }
@@ -324,12 +326,107 @@ int read_state(bm_ctx *c)
     return 0;
 }
 
+// ------------------------------------------------------------------ autotuner
+// Times candidate tile shapes of each pass on the mesh's own buffers (CUDA events, a few
+// launches each) and keeps the fastest. Runs once per geometry at setup; the spectrum
+// buffers it scribbles on are re-primed before the first step.
+template <typename T> YZArgs<T> yz_args(bm_ctx *c, Mesh &m, int gate);
+template <typename T> StageArgs<T> stage_args(bm_ctx *c, Mesh &m);
+
+template <typename F>
+float time_launches(cudaStream_t s, F launch, int reps)
+{
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    if (launch()) { cudaEventDestroy(e0); cudaEventDestroy(e1); cudaGetLastError(); return 1e30f; }
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps; r++) launch();
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cudaGetLastError() != cudaSuccess) return 1e30f;
+    return ms / reps;
+}
+
+template <typename T>
+int autotune_mesh(bm_ctx *c, Mesh &m)
+{
+    cudaStream_t s = c->stream;
+    const int lim = bm_lb<T>::v;
+    const size_t cs = sizeof(cpx<T>);
+    const int reps = 3;
+    if (m.modules & BM_DEMAG) {
+        YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
+        if (m.nz == 1) {
+            float best = 1e30f; int bw = m.W2;
+            for (int W = 1; W <= 16 && W <= m.LX; W *= 2) {
+                if (ymid2d_smem<T>(m.Ny, W) > 200 * 1024 || W * m.py.tpl > lim) continue;
+                a.W = W;
+                float t = time_launches(s, [&]() { return launch_ymid2d<T>(a, s); }, reps);
+                if (t < best) { best = t; bw = W; }
+            }
+            m.W2 = bw;
+        } else {
+            float best = 1e30f; int bw = m.Wy;
+            for (int W = 1; W <= 16 && W <= m.LX; W *= 2) {
+                if ((size_t)m.Ny * W * cs > 200 * 1024 || W * m.py.tpl > lim) continue;
+                a.W = W;
+                float t = time_launches(s, [&]() { return launch_yfwd<T>(a, s); }, reps) +
+                          time_launches(s, [&]() { return launch_yinv<T>(a, s); }, reps);
+                if (t < best) { best = t; bw = W; }
+            }
+            m.Wy = bw;
+            best = 1e30f; bw = m.Wz;
+            for (int W = 4; W <= 128 && W <= m.LX; W *= 2) {
+                if (zmid_smem<T>(m.Nz, W) > 200 * 1024 || 2 * W * m.pz.tpl > lim) continue;
+                a.W = W;
+                float t = time_launches(s, [&]() { return launch_zmid<T>(a, s); }, reps);
+                if (t < best) { best = t; bw = W; }
+            }
+            m.Wz = bw;
+        }
+    }
+    // stage kernel: rows per block
+    T *tmp = nullptr;
+    if (cudaMalloc(&tmp, sizeof(T) * 6 * m.n) != cudaSuccess) return 0;   // keep heuristic choice
+    {
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.st = nullptr;   // no step-state side effects while tuning
+        a.mode = BM_MODE_STAGE;
+        a.Min = (const T *)m.buf[0];
+        a.Mbase = (const T *)m.buf[0];
+        a.nev = 2;
+        a.ev[0] = (const T *)m.buf[0]; a.ev[1] = (const T *)m.buf[0];
+        a.ev_out = tmp;
+        a.Mout = tmp + 3 * m.n;
+        float best = 1e30f; int br = m.rpb;
+        int rows = m.ny * m.nz;
+        for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
+            if (3 * rpb * m.px.tpl > lim) break;
+            if ((size_t)3 * rpb * padded_len(m.LX) * cs > 200 * 1024) break;
+            a.rpb = rpb;
+            float t = time_launches(s, [&]() { return launch_stage<T>(a, s); }, reps);
+            if (t < best) { best = t; br = rpb; }
+        }
+        m.rpb = br;
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    cudaGetLastError();
+    return 0;
+}
+
 template <typename T>
 int prepare_T(bm_ctx *c)
 {
     for (auto &m : c->meshes) {
         int rc = prepare_mesh<T>(c, m);
         if (rc) { for (auto &mm : c->meshes) free_mesh(mm); return rc; }
+        if (c->autotune) autotune_mesh<T>(c, m);
     }
     return 0;
 }
@@ -1028,6 +1125,15 @@ int bm_time_kernels(bm_ctx *c, int mesh, int reps, double *ms4, double *bytes4)
     Mesh &m = c->meshes[mesh];
     return (c->precision == BM_FP64) ? time_kernels_T<double>(c, m, reps, ms4, bytes4)
                                      : time_kernels_T<float>(c, m, reps, ms4, bytes4);
+}
+
+int bm_tiles(bm_ctx *c, int mesh, int *tiles4)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!tiles4) return fail(BM_EINVAL, "null out");
+    Mesh &m = c->meshes[mesh];
+    tiles4[0] = m.W2; tiles4[1] = m.Wy; tiles4[2] = m.Wz; tiles4[3] = m.rpb;
+    return 0;
 }
 
 int bm_debug_kernels(bm_ctx *c, int mesh, double *K6)

@@ -20,6 +20,32 @@ template <typename T> BM_HD cpx<T> conj(cpx<T> a) { return mk<T>(a.x, -a.y); }
 template <typename T> BM_HD cpx<T> mul_i(cpx<T> a) { return mk<T>(-a.y, a.x); }
 template <typename T> BM_HD cpx<T> mul_mi(cpx<T> a) { return mk<T>(a.y, -a.x); }
 
+#ifdef __CUDACC__
+// Asynchronous global -> shared copy of one element (4, 8 or 16 bytes); when !valid the
+// destination is zero-filled and nothing is read (src must still be a mapped address).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_el(void *smem, const void *gmem, bool valid)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int src = valid ? BYTES : 0;
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+template <typename T>
+__device__ __forceinline__ void cp_async_cpx(cpx<T> *smem, const cpx<T> *gmem, bool valid)
+{
+    cp_async_el<sizeof(cpx<T>)>(smem, gmem, valid);
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_real(T *smem, const T *gmem, bool valid)
+{
+    cp_async_el<sizeof(T)>(smem, gmem, valid);
+}
+#endif
+
 // Physical constants (the reference's BorisLib/Funcs_Math_base.h:9,16)
 #define BM_MU0 1.256637061435916e-6
 #define BM_GAMMA 2.212761569e5

@@ -37,6 +37,14 @@ struct YZArgs {
     int gate;
 };
 
+template <typename T> size_t ymid2d_smem(int Ny, int W)
+{
+    return (size_t)3 * Ny * W * sizeof(cpx<T>) + (size_t)4 * (Ny / 2 + 1) * (W + 1) * sizeof(T);
+}
+template <typename T> size_t zmid_smem(int Nz, int W)
+{
+    return (size_t)6 * Nz * W * sizeof(cpx<T>) + (size_t)6 * (Nz / 2 + 1) * (W + 1) * sizeof(T);
+}
 template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_zmid(const YZArgs<T> &a, cudaStream_t s);

@@ -131,8 +131,9 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
     if (demag) {
         if (qact) {
             const cpx<T> *src = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
-            for (int m = t; m < LX; m += tpl) line[eaddr<true>(m, 1)] = src[m];
+            for (int m = t; m < LX; m += tpl) cp_async_cpx<T>(&line[eaddr<true>(m, 1)], &src[m], true);
         }
+        cp_async_wait_all();
         __syncthreads();
         xinv_pre<T>(line, LX, a.twx2, t, tpl, qact);
         fft_line<T, true, true>(line, 1, t, qact, a.px, a.twx);

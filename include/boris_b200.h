@@ -137,6 +137,10 @@ int bm_run_timed(bm_ctx *ctx, int steps, bm_stats *out, double *device_ms);
  * Unused slots are 0. Leaves the spectrum buffers stale (the next run re-primes them). */
 int bm_time_kernels(bm_ctx *ctx, int mesh, int reps, double *ms4, double *bytes4);
 
+/* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width,
+ * z-pass width, stage rows per block]. Valid after the first compute or run. */
+int bm_tiles(bm_ctx *ctx, int mesh, int *tiles4);
+
 /* Test hooks (used by the test suite only). */
 /* FP64 demag kernel spectra (octant (Nx/2+1)(Ny/2+1)(Nz/2+1), 6 components xx,yy,zz,xy,xz,yz). */
 int bm_debug_kernels(bm_ctx *ctx, int mesh, double *K6);
