@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <cstdio>
+#include <cstdlib>
 
 namespace {
 
@@ -198,21 +199,27 @@ void choose_tiles(Mesh &m)
     }
     // 3D y passes: small tiles so several blocks share an SM and overlap load and compute
     {
-        int W = 4;
-        while (W > 1 && ((size_t)m.Ny * W * cs > 100 * 1024 || W * m.py.tpl > lim)) W /= 2;
+        int W = 8;
+        if (ypass_has_reg(m.Ny))
+            while (W > 1 && ((size_t)m.Ny * W * cs > 100 * 1024 || ypass_reg_threads(m.Ny, W) > lim)) W /= 2;
+        else
+            while (W > 1 && ((size_t)m.Ny * W * cs > 100 * 1024 || W * m.py.tpl > lim)) W /= 2;
         if (W > m.LX) W = pow2_floor(m.LX);
         m.Wy = W;
     }
-    // 3D z pass: two mirror pencils in parallel, components one after another
+    // 3D z pass: register transforms (6 lines per column) or the generic shared-memory path
     {
         int W = 32;
-        while (W > 1 && (zmid_smem<T>(m.Nz, W) > 72 * 1024 || 2 * W * m.pz.tpl > lim)) W /= 2;
+        if (zmid_has_reg(m.Nz))
+            while (W > 1 && (zmid_reg_smem<T>(m.Nz, W) > 72 * 1024 || 6 * W > lim)) W /= 2;
+        else
+            while (W > 1 && (zmid_smem<T>(m.Nz, W) > 72 * 1024 || 2 * W * m.pz.tpl > lim)) W /= 2;
         if (W > m.LX) W = pow2_floor(m.LX);
         m.Wz = W;
     }
     // stage kernel rows per block
     {
-        int tpl = m.px.tpl;
+        int tpl = stage_reg_q(m.LX) ? stage_reg_q(m.LX) : m.px.tpl;
         int rpb = lim / (3 * tpl);
         if (rpb < 1) rpb = 1;
         while (rpb > 1 && (size_t)3 * rpb * padded_len(m.LX) * cs > 64 * 1024) rpb--;
@@ -372,8 +379,9 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
             m.W2 = bw;
         } else {
             float best = 1e30f; int bw = m.Wy;
-            for (int W = 1; W <= 16 && W <= m.LX; W *= 2) {
-                if ((size_t)m.Ny * W * cs > 200 * 1024 || W * m.py.tpl > lim) continue;
+            for (int W = 1; W <= 32 && W <= m.LX; W *= 2) {
+                if ((size_t)m.Ny * W * cs > 200 * 1024) continue;
+                if (ypass_has_reg(m.Ny) ? ypass_reg_threads(m.Ny, W) > lim : W * m.py.tpl > lim) continue;
                 a.W = W;
                 float t = time_launches(s, [&]() { return launch_yfwd<T>(a, s); }, reps) +
                           time_launches(s, [&]() { return launch_yinv<T>(a, s); }, reps);
@@ -382,7 +390,8 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
             m.Wy = bw;
             best = 1e30f; bw = m.Wz;
             for (int W = 4; W <= 128 && W <= m.LX; W *= 2) {
-                if (zmid_smem<T>(m.Nz, W) > 200 * 1024 || 2 * W * m.pz.tpl > lim) continue;
+                if (zmid_has_reg(m.Nz) ? (zmid_reg_smem<T>(m.Nz, W) > 200 * 1024 || 6 * W > lim)
+                                       : (zmid_smem<T>(m.Nz, W) > 200 * 1024 || 2 * W * m.pz.tpl > lim)) continue;
                 a.W = W;
                 float t = time_launches(s, [&]() { return launch_zmid<T>(a, s); }, reps);
                 if (t < best) { best = t; bw = W; }
@@ -405,8 +414,9 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
         a.Mout = tmp + 3 * m.n;
         float best = 1e30f; int br = m.rpb;
         int rows = m.ny * m.nz;
+        const int tpl = stage_reg_q(m.LX) ? stage_reg_q(m.LX) : m.px.tpl;
         for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
-            if (3 * rpb * m.px.tpl > lim) break;
+            if (3 * rpb * tpl > lim) break;
             if ((size_t)3 * rpb * padded_len(m.LX) * cs > 200 * 1024) break;
             a.rpb = rpb;
             float t = time_launches(s, [&]() { return launch_stage<T>(a, s); }, reps);
@@ -426,7 +436,12 @@ int prepare_T(bm_ctx *c)
     for (auto &m : c->meshes) {
         int rc = prepare_mesh<T>(c, m);
         if (rc) { for (auto &mm : c->meshes) free_mesh(mm); return rc; }
-        if (c->autotune) autotune_mesh<T>(c, m);
+        // BM_TILES="w2,wy,wz,rows" fixes the tile shapes (profiling runs); otherwise autotune
+        const char *ev = getenv("BM_TILES");
+        int t4[4];
+        if (ev && sscanf(ev, "%d,%d,%d,%d", &t4[0], &t4[1], &t4[2], &t4[3]) == 4) {
+            m.W2 = t4[0]; m.Wy = t4[1]; m.Wz = t4[2]; m.rpb = t4[3];
+        } else if (c->autotune) autotune_mesh<T>(c, m);
     }
     return 0;
 }

@@ -13,6 +13,7 @@
 //                zmid     z FFT over n.z nonzero planes, product, inverse, first n.z planes kept
 //                yinv     S2 -> S1 (first n.y rows kept)
 #include "kernels.h"
+#include "regfft.cuh"
 
 template <typename T>
 __device__ __forceinline__ bool gated_out(const StepState *st, int gate)
@@ -268,6 +269,274 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid(YZArgs<T> a)
     }
 }
 
+// ------------------------------------------------------------------------------ 3D z pass, register FFT
+// Compile-time Nz (<= 64): one thread owns one (component, pencil, column) line of Nz points in
+// registers. The upper half of the padded input is a compile-time zero and only the first
+// Nz/2 inverse outputs are stored, so the zero-padding work folds away. Shared memory only
+// carries the spectra across the 3x3 product; the kernel tile arrives by cp.async while the
+// forward transforms run. Thread (c, p, w): w fastest so global loads/stores coalesce.
+template <typename T, int NZ>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    extern __shared__ unsigned char smraw[];
+    const int W = a.W, Ny = a.Ny, nz = a.nz, LX = a.LX;
+    const int lw = __ffs(W) - 1;
+    constexpr int KZ1 = NZ / 2 + 1;
+    const int Kx1 = LX + 1, Ky1 = Ny / 2 + 1;
+    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
+    T *Ks = reinterpret_cast<T *>(sm + 6 * NZ * W);
+    T *Kn = Ks + 6 * KZ1 * W;
+    const int kx0 = blockIdx.x * W;
+    const int ky = blockIdx.y, kym = (Ny - ky) % Ny;
+    const bool single = (ky == kym);
+    const int np = single ? 1 : 2;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const long long nk = (long long)Kx1 * Ky1 * KZ1;
+    // kernel tile (async)
+    for (int idx = tid; idx < 6 * KZ1 * W; idx += nt) {
+        int w = idx & (W - 1), r = idx >> lw;
+        int kz = r % KZ1, c = r / KZ1;
+        int kx = kx0 + w;
+        bool ok = kx < LX;
+        cp_async_real<T>(&Ks[(c * KZ1 + kz) * W + w], ok ? &a.K[c * nk + ((long long)kz * Ky1 + ky) * Kx1 + kx] : a.K, ok);
+    }
+    if (kx0 == 0) {
+        for (int idx = tid; idx < 6 * KZ1; idx += nt) {
+            int kz = idx % KZ1, c = idx / KZ1;
+            cp_async_real<T>(&Kn[c * KZ1 + kz], &a.K[c * nk + ((long long)kz * Ky1 + ky) * Kx1 + LX], true);
+        }
+    }
+    // forward transforms in registers
+    const int w = tid & (W - 1);
+    const int p = (tid >> lw) & 1;
+    const int c = tid >> (lw + 1);
+    const int kx = kx0 + w;
+    const bool own = (c < 3) && (p < np) && (kx < LX);
+    const int kyp = p ? kym : ky;
+    const long long gbase = ((long long)c * nz * Ny + kyp) * LX + kx;   // + e * Ny * LX
+    const long long gstride = (long long)Ny * LX;
+    cpx<T> v[NZ];
+#pragma unroll
+    for (int e = 0; e < NZ; e++) v[e] = mk<T>(0, 0);
+    if (own) {
+#pragma unroll
+        for (int e = 0; e < NZ / 2; e++)
+            if (e < nz) v[e] = a.S2[gbase + e * gstride];
+    }
+    RegFFT<T, NZ, false>::run(v, a.twz, 1);
+    auto S = [&](int cc, int pp, int e, int ww) -> cpx<T> & { return sm[((cc * 2 + pp) * NZ + e) * W + ww]; };
+    if (c < 3) {
+#pragma unroll
+        for (int e = 0; e < NZ; e++) S(c, p, e, w) = v[e];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // 3x3 product with mirror signs (KernelMultiplication_3D_line, DemagKernel.cpp:85)
+    for (int idx = tid; idx < np * NZ * W; idx += nt) {
+        int ww = idx & (W - 1), r = idx >> lw;
+        int kz = r % NZ, pp = r / NZ;
+        if (kx0 + ww >= LX) continue;
+        int akz = kz <= NZ / 2 ? kz : NZ - kz;
+        T sz = kz <= NZ / 2 ? (T)1 : (T)-1;
+        if (kx0 + ww == 0) {
+            if (pp == 1) continue;
+            if (single && kz > NZ / 2) continue;
+            int pm = single ? 0 : 1;
+            int kzm = (NZ - kz) % NZ;
+            cpx<T> A[3], B[3], Ap[3], Bp[3];
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) {
+                cpx<T> C = S(cc, 0, kz, ww), cj = conj(S(cc, pm, kzm, ww));
+                A[cc] = cscale(C + cj, (T)0.5);
+                B[cc] = cscale(mul_mi(C - cj), (T)0.5);
+            }
+            T k0[6] = {Ks[(0 * KZ1 + akz) * W + ww], Ks[(1 * KZ1 + akz) * W + ww], Ks[(2 * KZ1 + akz) * W + ww],
+                       Ks[(3 * KZ1 + akz) * W + ww], sz * Ks[(4 * KZ1 + akz) * W + ww], sz * Ks[(5 * KZ1 + akz) * W + ww]};
+            T kn[6] = {Kn[0 * KZ1 + akz], Kn[1 * KZ1 + akz], Kn[2 * KZ1 + akz],
+                       Kn[3 * KZ1 + akz], sz * Kn[4 * KZ1 + akz], sz * Kn[5 * KZ1 + akz]};
+            kapply<T>(k0, A, Ap);
+            kapply<T>(kn, B, Bp);
+            bool self = single && (kzm == kz);
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) {
+                S(cc, 0, kz, ww) = Ap[cc] + mul_i(Bp[cc]);
+                if (!self) S(cc, pm, kzm, ww) = conj(Ap[cc]) + mul_i(conj(Bp[cc]));
+            }
+        } else {
+            T sy = (pp == 0) ? (T)1 : (T)-1;
+            T k[6] = {Ks[(0 * KZ1 + akz) * W + ww], Ks[(1 * KZ1 + akz) * W + ww], Ks[(2 * KZ1 + akz) * W + ww],
+                      sy * Ks[(3 * KZ1 + akz) * W + ww], sz * Ks[(4 * KZ1 + akz) * W + ww],
+                      sy * sz * Ks[(5 * KZ1 + akz) * W + ww]};
+            cpx<T> m[3], h[3];
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) m[cc] = S(cc, pp, kz, ww);
+            kapply<T>(k, m, h);
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) S(cc, pp, kz, ww) = h[cc];
+        }
+    }
+    __syncthreads();
+    if (c < 3) {
+#pragma unroll
+        for (int e = 0; e < NZ; e++) v[e] = S(c, p, e, w);
+    }
+    RegFFT<T, NZ, true>::run(v, a.twz, 1);
+    if (own) {
+#pragma unroll
+        for (int e = 0; e < NZ / 2; e++)
+            if (e < nz) a.S2[gbase + e * gstride] = v[e];
+    }
+}
+
+template <typename T, int NZ>
+static int launch_zmid_reg(const YZArgs<T> &a, cudaStream_t s)
+{
+    int nt = 6 * a.W;
+    if (nt < 32) nt = 32;
+    if (nt > bm_lb<T>::v) return 104;
+    size_t smem = zmid_reg_smem<T>(NZ, a.W);
+    if (smem > 200 * 1024) return 105;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_zmid_reg<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    dim3 grid((a.LX + a.W - 1) / a.W, a.Ny / 2 + 1);
+    k_zmid_reg<T, NZ><<<grid, nt, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+// lengths with a register z pass
+bool zmid_has_reg(int Nz)
+{
+    return Nz == 4 || Nz == 6 || Nz == 8 || Nz == 12 || Nz == 16 || Nz == 24 || Nz == 32 || Nz == 48 || Nz == 64;
+}
+
+// ------------------------------------------------------------------------------ 3D y passes, two-level register FFT
+// Ny = P * Q (P <= Q <= 32). Stage 1: thread (w, n1) holds x[n1 + P n2], n2 < Q, in registers,
+// does DFT_Q, twiddles by w_Ny^(n1 k2) and writes u[k2][n1] to shared memory. Stage 2: thread
+// (w, k2) reads u[k2][.], does DFT_P and owns X[k2 + Q k1]. Forward: the input rows >= ny are
+// compile-time zeros (n2 >= Q/2). Inverse: only rows < ny (k1 < P/2) are written. One shared
+// transpose per transform instead of one per radix pass; no runtime division.
+template <typename T, int P, int Q, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass_reg(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    extern __shared__ unsigned char smraw[];
+    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
+    constexpr int L = P * Q;
+    const int W = a.W, ny = a.ny, LX = a.LX, nz = a.nz;
+    const int lw = __ffs(W) - 1;
+    const int kx0 = blockIdx.x * W, z = blockIdx.y, c = blockIdx.z;
+    const int tid = threadIdx.x;
+    const int w = tid & (W - 1), r = tid >> lw;
+    const int kx = kx0 + w;
+    const bool colok = kx < LX;
+    const cpx<T> *src;
+    cpx<T> *dst;
+    if (!INV) {
+        src = a.S1 + ((long long)c * nz + z) * ny * LX + kx;
+        dst = a.S2 + ((long long)c * nz + z) * L * LX + kx;
+    } else {
+        src = a.S2 + ((long long)c * nz + z) * L * LX + kx;
+        dst = a.S1 + ((long long)c * nz + z) * ny * LX + kx;
+    }
+    cpx<T> v[Q];
+    if (r < P) {
+        const int n1 = r;
+#pragma unroll
+        for (int n2 = 0; n2 < Q; n2++) {
+            v[n2] = mk<T>(0, 0);
+            const int e = n1 + P * n2;
+            if (!INV) {
+                if (n2 < Q / 2 && colok && e < ny) v[n2] = src[(long long)e * LX];
+            } else {
+                if (colok) v[n2] = src[(long long)e * LX];
+            }
+        }
+        RegFFT<T, Q, INV>::run(v, a.twy, P);
+#pragma unroll
+        for (int k2 = 0; k2 < Q; k2++) {
+            cpx<T> t = v[k2];
+            if (k2 > 0 && n1 > 0) {
+                cpx<T> tw = a.twy[n1 * k2];
+                if (INV) tw.y = -tw.y;
+                t = cmul(t, tw);
+            }
+            sm[(k2 * P + n1) * W + w] = t;
+        }
+    }
+    __syncthreads();
+    if (r < Q) {
+        const int k2 = r;
+        cpx<T> u[P];
+#pragma unroll
+        for (int n1 = 0; n1 < P; n1++) u[n1] = sm[(k2 * P + n1) * W + w];
+        RegFFT<T, P, INV>::run(u, a.twy, Q);
+        if (colok) {
+#pragma unroll
+            for (int k1 = 0; k1 < P; k1++) {
+                const int e = k2 + Q * k1;
+                if (!INV) dst[(long long)e * LX] = u[k1];
+                else if (k1 < P / 2 && e < ny) dst[(long long)e * LX] = u[k1];
+            }
+        }
+    }
+}
+
+template <int L> struct ysplit {
+    // P <= Q, both <= 32
+    static constexpr int q = (L >= 1024) ? 32 : (L >= 256) ? 16 : (L >= 64) ? 8 : (L >= 16) ? 4 : 2;
+    static constexpr int p = L / q;
+};
+
+template <typename T, int L, bool INV>
+static int launch_ypass_reg(const YZArgs<T> &a, cudaStream_t s)
+{
+    constexpr int P = ysplit<L>::p, Q = ysplit<L>::q;
+    int nt = a.W * (P > Q ? P : Q);
+    if (nt > bm_lb<T>::v) return 106;
+    if (nt < 32) nt = 32;
+    size_t smem = (size_t)L * a.W * sizeof(cpx<T>);
+    if (smem > 200 * 1024) return 107;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_ypass_reg<T, P, Q, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    dim3 grid((a.LX + a.W - 1) / a.W, a.nz, 3);
+    k_ypass_reg<T, P, Q, INV><<<grid, nt, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+bool ypass_has_reg(int Ny)
+{
+    return Ny == 8 || Ny == 16 || Ny == 32 || Ny == 64 || Ny == 128 || Ny == 256 || Ny == 512 || Ny == 1024;
+}
+
+int ypass_reg_threads(int Ny, int W)
+{
+    int q = (Ny >= 1024) ? 32 : (Ny >= 256) ? 16 : (Ny >= 64) ? 8 : (Ny >= 16) ? 4 : 2;
+    int p = Ny / q;
+    return W * (p > q ? p : q);
+}
+
+template <typename T, bool INV>
+static int launch_ypass_dispatch(const YZArgs<T> &a, cudaStream_t s)
+{
+    if ((a.W & (a.W - 1)) != 0) return -1;
+    switch (a.Ny) {
+    case 8: return launch_ypass_reg<T, 8, INV>(a, s);
+    case 16: return launch_ypass_reg<T, 16, INV>(a, s);
+    case 32: return launch_ypass_reg<T, 32, INV>(a, s);
+    case 64: return launch_ypass_reg<T, 64, INV>(a, s);
+    case 128: return launch_ypass_reg<T, 128, INV>(a, s);
+    case 256: return launch_ypass_reg<T, 256, INV>(a, s);
+    case 512: return launch_ypass_reg<T, 512, INV>(a, s);
+    case 1024: return launch_ypass_reg<T, 1024, INV>(a, s);
+    default: return -1;
+    }
+}
+
 // ------------------------------------------------------------------------------ launchers
 template <typename KF>
 static int launch_common(KF kern, dim3 grid, int nt, size_t smem, cudaStream_t s)
@@ -296,6 +565,10 @@ template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s)
 
 template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s)
 {
+    {
+        int rc = launch_ypass_dispatch<T, false>(a, s);
+        if (rc >= 0) return rc;
+    }
     int nt = a.W * a.py.tpl;
     if (nt < 32) nt = 32;
     if (nt > bm_lb<T>::v) return 103;
@@ -309,6 +582,10 @@ template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s)
 
 template <typename T> int launch_yinv(const YZArgs<T> &a, cudaStream_t s)
 {
+    {
+        int rc = launch_ypass_dispatch<T, true>(a, s);
+        if (rc >= 0) return rc;
+    }
     int nt = a.W * a.py.tpl;
     if (nt < 32) nt = 32;
     if (nt > bm_lb<T>::v) return 103;
@@ -322,6 +599,20 @@ template <typename T> int launch_yinv(const YZArgs<T> &a, cudaStream_t s)
 
 template <typename T> int launch_zmid(const YZArgs<T> &a, cudaStream_t s)
 {
+    if ((a.W & (a.W - 1)) == 0) {
+        switch (a.Nz) {
+        case 4: return launch_zmid_reg<T, 4>(a, s);
+        case 6: return launch_zmid_reg<T, 6>(a, s);
+        case 8: return launch_zmid_reg<T, 8>(a, s);
+        case 12: return launch_zmid_reg<T, 12>(a, s);
+        case 16: return launch_zmid_reg<T, 16>(a, s);
+        case 24: return launch_zmid_reg<T, 24>(a, s);
+        case 32: return launch_zmid_reg<T, 32>(a, s);
+        case 48: return launch_zmid_reg<T, 48>(a, s);
+        case 64: return launch_zmid_reg<T, 64>(a, s);
+        default: break;
+        }
+    }
     int nt = 2 * a.W * a.pz.tpl;
     if (nt < 32) nt = 32;
     if (nt > bm_lb<T>::v) return 103;

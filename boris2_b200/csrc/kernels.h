@@ -45,6 +45,13 @@ template <typename T> size_t zmid_smem(int Nz, int W)
 {
     return (size_t)6 * Nz * W * sizeof(cpx<T>) + (size_t)6 * (Nz / 2 + 1) * (W + 1) * sizeof(T);
 }
+template <typename T> size_t zmid_reg_smem(int Nz, int W)
+{
+    return (size_t)6 * Nz * W * sizeof(cpx<T>) + (size_t)6 * (Nz / 2 + 1) * (W + 1) * sizeof(T);
+}
+bool zmid_has_reg(int Nz);
+bool ypass_has_reg(int Ny);
+int ypass_reg_threads(int Ny, int W);
 template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_zmid(const YZArgs<T> &a, cudaStream_t s);
@@ -90,4 +97,5 @@ struct StageArgs {
 };
 
 template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s);
+int stage_reg_q(int LX);   // threads per x line of the register stage kernel (0: generic kernel)
 int launch_scalar_reset(StepState *st, cudaStream_t s);

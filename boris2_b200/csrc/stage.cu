@@ -16,6 +16,7 @@
 // RK4 Boris/DiffEqFM_Evals_RK4.cpp, RKDP54 Boris/DiffEqFM_Evals_RKDP54.cpp, step control
 // Boris/DiffEq_CommonBase_Iterate.cpp:15 (SetAdaptiveTimeStep) and :1214 (prime / restore).
 #include "kernels.h"
+#include "regfft.cuh"
 
 template <typename T>
 __device__ __forceinline__ bool stage_gated_out(const StepState *st, int gate)
@@ -76,6 +77,50 @@ __device__ __forceinline__ void xinv_pre(cpx<T> *line, int LX, const cpx<T> *__r
     __syncthreads();
 }
 
+// versions of xfwd_post / xinv_pre with an element-address functor
+template <typename T, typename AddrF>
+__device__ __forceinline__ void xfwd_post_f(cpx<T> *line, int LX, const cpx<T> *__restrict__ tw2, int t, int tpl, bool act, AddrF A)
+{
+    if (act) {
+        for (int k = t; k <= LX / 2; k += tpl) {
+            if (k == 0) {
+                cpx<T> z0 = line[A(0)];
+                line[A(0)] = mk<T>(z0.x + z0.y, z0.x - z0.y);
+                continue;
+            }
+            int k2 = LX - k;
+            cpx<T> Av = line[A(k)], Bc = conj(line[A(k2)]);
+            cpx<T> E = cscale(Av + Bc, (T)0.5);
+            cpx<T> O = cscale(mul_mi(Av - Bc), (T)0.5);
+            cpx<T> wO = cmul(tw2[k], O);
+            line[A(k)] = E + wO;
+            if (k2 != k) line[A(k2)] = conj(E - wO);
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, typename AddrF>
+__device__ __forceinline__ void xinv_pre_f(cpx<T> *line, int LX, const cpx<T> *__restrict__ tw2, int t, int tpl, bool act, AddrF A)
+{
+    if (act) {
+        for (int k = t; k <= LX / 2; k += tpl) {
+            if (k == 0) {
+                cpx<T> p0 = line[A(0)];
+                line[A(0)] = mk<T>((p0.x + p0.y) * (T)0.5, (p0.x - p0.y) * (T)0.5);
+                continue;
+            }
+            int k2 = LX - k;
+            cpx<T> Xk = line[A(k)], Xk2c = conj(line[A(k2)]);
+            cpx<T> E = cscale(Xk + Xk2c, (T)0.5);
+            cpx<T> O = cscale(cmul(Xk - Xk2c, conj(tw2[k])), (T)0.5);
+            line[A(k)] = E + mul_i(O);
+            if (k2 != k) line[A(k2)] = conj(E) + mul_i(conj(O));
+        }
+    }
+    __syncthreads();
+}
+
 template <typename T>
 __device__ __forceinline__ void ld3(const T *P, long long n, long long i, T v[3])
 {
@@ -105,40 +150,18 @@ __device__ __forceinline__ void axis_stencil(const T m[3], const T *mp, const T 
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
+// Per-cell part of a stage: Heff, LLG, update. `lines` holds the 3 * rpb packed x lines of the
+// block (component-major), element e of line q at sm[q * LSP + addr(e)]; on entry it carries
+// the unscaled inverse-x result (H_demag / scale), on exit the new M (when do_xfwd).
+template <typename T, typename AddrF>
+__device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, int LSP, AddrF addr, int r0, double &lmax)
 {
-    if (stage_gated_out<T>(a.st, a.gate)) return;
-    extern __shared__ unsigned char smraw[];
-    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
-    __shared__ double red[32];
-    __shared__ int is_last;
-
-    const int LX = a.LX, nx = a.nx, ny = a.ny, nz = a.nz, rpb = a.rpb, tpl = a.px.tpl;
-    const int LSP = padded_len(LX);
+    const int nx = a.nx, ny = a.ny, nz = a.nz, rpb = a.rpb;
     const int nrows = ny * nz;
-    const int r0 = blockIdx.x * rpb;
     const int tid = threadIdx.x, nt = blockDim.x;
     const long long n = a.n;
-    const int q = tid / tpl, t = tid % tpl;
-    const int qc = q / rpb, qr = q % rpb;
-    const bool qact = (q < 3 * rpb) && (r0 + qr < nrows);
-    cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
-
     const bool fields = (a.mode != BM_MODE_UPDATE);
     const bool demag = fields && (a.modules & BM_MOD_DEMAG);
-
-    if (demag) {
-        if (qact) {
-            const cpx<T> *src = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
-            for (int m = t; m < LX; m += tpl) cp_async_cpx<T>(&line[eaddr<true>(m, 1)], &src[m], true);
-        }
-        cp_async_wait_all();
-        __syncthreads();
-        xinv_pre<T>(line, LX, a.twx2, t, tpl, qact);
-        fft_line<T, true, true>(line, 1, t, qact, a.px, a.twx);
-    }
-
     const double dT = a.st ? *((volatile double *)&a.st->dT) : 0.0;
     T Ha[3] = {0, 0, 0};
     if (fields && (a.modules & BM_MOD_ZEEMAN) && a.Ha && a.nHa > 0) {
@@ -157,8 +180,9 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
 #pragma unroll
     for (int i = 0; i < 6; i++) cev[i] = (T)(a.cev[i] * dT);
     const T crhs = (T)(a.crhs * dT);
-    double lmax = 0.0;
-
+    auto rp = [&](int q, int x) -> T * {
+        return reinterpret_cast<T *>(&sm[q * LSP + addr(x >> 1)]) + (x & 1);
+    };
     for (int ci = tid; ci < rpb * nx; ci += nt) {
         int r = ci / nx, x = ci - r * nx;
         int row = r0 + r;
@@ -172,7 +196,7 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
             T H[3] = {Ha[0], Ha[1], Ha[2]};
             if (demag) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) H[c] += a.scale * *rptr<T>(sm + (c * rpb + r) * LSP, x);
+                for (int c = 0; c < 3; c++) H[c] += a.scale * *rp(c * rpb + r, x);
             }
             if (exch) {
                 int y = row % ny, z = row / ny;
@@ -262,31 +286,21 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
         if (a.do_xfwd) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                cpx<T> *ln = sm + (c * rpb + r) * LSP;
-                *rptr<T>(ln, x) = mn[c];
-                if ((x & 1) == 0 && x == nx - 1) *rptr<T>(ln, x + 1) = 0;   // odd nx: zero the partner slot
+                *rp(c * rpb + r, x) = mn[c];
+                if ((x & 1) == 0 && x == nx - 1) *rp(c * rpb + r, x + 1) = 0;   // odd nx: zero the partner slot
             }
         }
     }
+}
 
-    if (a.do_xfwd) {
-        // zero padding beyond the mesh, then forward x transform and store
-        const int first_pad = (nx + 1) >> 1;
-        for (int idx = tid; idx < 3 * rpb * LX; idx += nt) {
-            int qq = idx / LX, mm = idx - qq * LX;
-            if (mm >= first_pad) sm[qq * LSP + eaddr<true>(mm, 1)] = mk<T>(0, 0);
-        }
-        __syncthreads();
-        fft_line<T, true, false>(line, 1, t, qact, a.px, a.twx);
-        xfwd_post<T>(line, LX, a.twx2, t, tpl, qact);
-        if (qact) {
-            cpx<T> *dst = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
-            for (int mm = t; mm < LX; mm += tpl) dst[mm] = line[eaddr<true>(mm, 1)];
-        }
-    }
-
+// LTE block reduction and the last-block bookkeeping (step finish / controller / restore flag)
+template <typename T>
+__device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax)
+{
+    __shared__ double red[32];
+    __shared__ int is_last;
+    const int tid = threadIdx.x, nt = blockDim.x;
     if (a.mode == BM_MODE_LTE) {
-        // block max -> device max (bit order of non-negative doubles)
         for (int o = 16; o > 0; o >>= 1) {
             double v = __shfl_xor_sync(0xffffffffu, lmax, o);
             if (v > lmax) lmax = v;
@@ -359,8 +373,200 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
     __threadfence();
 }
 
+// generic-length kernel (shared-memory Stockham x transforms)
+template <typename T>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
+{
+    if (stage_gated_out<T>(a.st, a.gate)) return;
+    extern __shared__ unsigned char smraw[];
+    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
+    const int LX = a.LX, rpb = a.rpb, tpl = a.px.tpl;
+    const int LSP = padded_len(LX);
+    const int nrows = a.ny * a.nz;
+    const int r0 = blockIdx.x * rpb;
+    const int tid = threadIdx.x;
+    const int q = tid / tpl, t = tid % tpl;
+    const int qc = q / rpb, qr = q % rpb;
+    const bool qact = (q < 3 * rpb) && (r0 + qr < nrows);
+    cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
+    const bool demag = (a.mode != BM_MODE_UPDATE) && (a.modules & BM_MOD_DEMAG);
+    if (demag) {
+        if (qact) {
+            const cpx<T> *src = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
+            for (int m = t; m < LX; m += tpl) cp_async_cpx<T>(&line[eaddr<true>(m, 1)], &src[m], true);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        xinv_pre<T>(line, LX, a.twx2, t, tpl, qact);
+        fft_line<T, true, true>(line, 1, t, qact, a.px, a.twx);
+    }
+    double lmax = 0.0;
+    stage_cells<T>(a, sm, LSP, [](int e) { return eaddr<true>(e, 1); }, r0, lmax);
+    if (a.do_xfwd) {
+        const int first_pad = (a.nx + 1) >> 1;
+        for (int idx = tid; idx < 3 * rpb * LX; idx += blockDim.x) {
+            int qq = idx / LX, mm = idx - qq * LX;
+            if (mm >= first_pad) sm[qq * LSP + eaddr<true>(mm, 1)] = mk<T>(0, 0);
+        }
+        __syncthreads();
+        fft_line<T, true, false>(line, 1, t, qact, a.px, a.twx);
+        xfwd_post<T>(line, LX, a.twx2, t, tpl, qact);
+        if (qact) {
+            cpx<T> *dst = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
+            for (int mm = t; mm < LX; mm += tpl) dst[mm] = line[eaddr<true>(mm, 1)];
+        }
+    }
+    stage_tail<T>(a, lmax);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Register kernel for LX = P * Q (P <= Q <= 32): each x line is transformed with one DFT_Q and
+// one DFT_P per thread in registers and one shared transpose (padded one slot per P elements, so
+// both access patterns are conflict-free). The packed-spectrum split (xinv_pre / xfwd_post) and
+// the per-cell work stay in shared memory in natural order.
+template <int P> struct addrP {
+    __device__ __forceinline__ int operator()(int e) const { return e + e / P; }
+};
+
+template <typename T, int P, int Q, bool INV>
+__device__ __forceinline__ void x_twolevel(cpx<T> *line, int t, bool act, const cpx<T> *__restrict__ tw, int nkeep)
+{
+    addrP<P> A;
+    cpx<T> v[Q];
+    if (act && t < P) {
+#pragma unroll
+        for (int n2 = 0; n2 < Q; n2++) {
+            if (!INV && n2 >= Q / 2) v[n2] = mk<T>(0, 0);   // forward input is zero beyond LX/2
+            else v[n2] = line[A(t + P * n2)];
+        }
+    }
+    __syncthreads();
+    if (act && t < P) {
+        RegFFT<T, Q, INV>::run(v, tw, P);
+#pragma unroll
+        for (int k2 = 0; k2 < Q; k2++) {
+            cpx<T> x = v[k2];
+            if (k2 > 0 && t > 0) {
+                cpx<T> w = tw[t * k2];
+                if (INV) w.y = -w.y;
+                x = cmul(x, w);
+            }
+            line[A(k2 * P + t)] = x;
+        }
+    }
+    __syncthreads();
+    cpx<T> u[P];
+    if (act && t < Q) {
+#pragma unroll
+        for (int n1 = 0; n1 < P; n1++) u[n1] = line[A(t * P + n1)];
+    }
+    __syncthreads();
+    if (act && t < Q) {
+        RegFFT<T, P, INV>::run(u, tw, Q);
+#pragma unroll
+        for (int k1 = 0; k1 < P; k1++) {
+            const int e = t + Q * k1;
+            if (!INV || e < nkeep) line[A(e)] = u[k1];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
+{
+    if (stage_gated_out<T>(a.st, a.gate)) return;
+    extern __shared__ unsigned char smraw[];
+    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
+    constexpr int LX = P * Q;
+    constexpr int LSP = LX + LX / P + 1;
+    addrP<P> A;
+    const int rpb = a.rpb;
+    const int nrows = a.ny * a.nz;
+    const int r0 = blockIdx.x * rpb;
+    const int tid = threadIdx.x;
+    const int q = tid / Q, t = tid % Q;
+    const int qc = q / rpb, qr = q % rpb;
+    const bool qact = (q < 3 * rpb) && (r0 + qr < nrows);
+    cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
+    const bool demag = (a.mode != BM_MODE_UPDATE) && (a.modules & BM_MOD_DEMAG);
+    const int half = (a.nx + 1) >> 1;   // packed elements that carry mesh cells
+    if (demag) {
+        if (qact) {
+            const cpx<T> *src = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
+#pragma unroll 4
+            for (int m = t; m < LX; m += Q) cp_async_cpx<T>(&line[A(m)], &src[m], true);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        xinv_pre_f<T>(line, LX, a.twx2, t, Q, qact, A);
+        x_twolevel<T, P, Q, true>(line, t, qact, a.twx, half);
+    }
+    double lmax = 0.0;
+    stage_cells<T>(a, sm, LSP, A, r0, lmax);
+    if (a.do_xfwd) {
+        for (int idx = tid; idx < 3 * rpb * (LX / 2); idx += blockDim.x) {
+            int qq = idx / (LX / 2), mm = idx - qq * (LX / 2);
+            if (mm >= half) sm[qq * LSP + A(mm)] = mk<T>(0, 0);
+        }
+        __syncthreads();
+        x_twolevel<T, P, Q, false>(line, t, qact, a.twx, LX);
+        xfwd_post_f<T>(line, LX, a.twx2, t, Q, qact, A);
+        if (qact) {
+            cpx<T> *dst = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
+#pragma unroll 4
+            for (int mm = t; mm < LX; mm += Q) dst[mm] = line[A(mm)];
+        }
+    }
+    stage_tail<T>(a, lmax);
+}
+
+template <typename T, int P, int Q>
+static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
+{
+    constexpr int LX = P * Q;
+    int nt = 3 * a.rpb * Q;
+    if (nt > bm_lb<T>::v) return 203;
+    if (nt < 32) nt = 32;
+    size_t smem = (size_t)3 * a.rpb * (LX + LX / P + 1) * sizeof(cpx<T>);
+    if (smem > 200 * 1024) return 204;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_stage_reg<T, P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    int nrows = a.ny * a.nz;
+    dim3 grid((nrows + a.rpb - 1) / a.rpb);
+    k_stage_reg<T, P, Q><<<grid, nt, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+// x lengths with a register kernel and their threads per line
+int stage_reg_q(int LX)
+{
+    switch (LX) {
+    case 16: return 4;
+    case 32: return 8;
+    case 64: return 8;
+    case 128: return 16;
+    case 256: return 16;
+    case 512: return 32;
+    case 1024: return 32;
+    default: return 0;
+    }
+}
+
 template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
 {
+    switch (a.LX) {
+    case 16: return launch_stage_reg<T, 4, 4>(a, s);
+    case 32: return launch_stage_reg<T, 4, 8>(a, s);
+    case 64: return launch_stage_reg<T, 8, 8>(a, s);
+    case 128: return launch_stage_reg<T, 8, 16>(a, s);
+    case 256: return launch_stage_reg<T, 16, 16>(a, s);
+    case 512: return launch_stage_reg<T, 16, 32>(a, s);
+    case 1024: return launch_stage_reg<T, 32, 32>(a, s);
+    default: break;
+    }
     int nt = 3 * a.rpb * a.px.tpl;
     if (nt < 32) nt = 32;
     if (nt > bm_lb<T>::v) return 201;

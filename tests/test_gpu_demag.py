@@ -79,6 +79,15 @@ DEMAG_CASES = [
     ((24, 20, 2), (2e-9, 2e-9, 1.5e-9)),
     ((64, 48, 1), (4e-9, 4e-9, 3e-9)),
     ((33, 17, 5), (3e-9, 2e-9, 2e-9)),
+    ((16, 16, 4), (2e-9, 2e-9, 2e-9)),      # power-of-two y: register y passes
+    ((20, 64, 2), (2e-9, 2e-9, 2e-9)),
+    ((8, 512, 3), (2e-9, 2e-9, 2e-9)),      # Ny = 1024 = 32 x 32 split
+    ((6, 5, 32), (2e-9, 2e-9, 2e-9)),       # Nz = 64 register z pass
+    ((100, 10, 3), (2e-9, 2e-9, 2e-9)),     # LX = 128 register x passes
+    ((200, 6, 1), (2e-9, 2e-9, 1e-9)),      # LX = 256
+    ((300, 3, 2), (2e-9, 2e-9, 1e-9)),      # LX = 384 (generic x kernel)
+    ((512, 4, 1), (2e-9, 2e-9, 1e-9)),      # LX = 512
+    ((1000, 2, 1), (2e-9, 2e-9, 1e-9)),     # LX = 1024
 ]
 
 

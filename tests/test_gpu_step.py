@@ -93,7 +93,7 @@ def test_zeeman_pulse_samples(bm):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_rkdp54_adaptive(bm, prec):
-    n = (16, 12, 2)
+    n = (16, 16, 2)
     N = n[0] * n[1] * n[2]
     mesh = dict(n=n, h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, D=1.5e-3, alpha=0.1, K1=5e5,
                 modules=1 | 4 | 8 | 16, Ha=(0, 0, 0))
