@@ -86,6 +86,7 @@ _SIGS = {
     "bm_debug_kernels": (_I, [_P, _I, _DP]),
     "bm_debug_tensor": (_I, [_I, _I, _I, _I, _D, _D, _D, _DP]),
     "bm_debug_fft": (_I, [_I, _I, _I, _I, _I, _DP]),
+    "bm_fft_noalloc": (_I, [_I, _I, _I, _I, _P, _P, _P]),
 }
 
 

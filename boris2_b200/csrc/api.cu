@@ -742,6 +742,9 @@ int check_mesh(bm_ctx *c, int mesh)
 
 }  // namespace
 
+// error text for entry points defined in other translation units
+int bm_set_error(int code, const std::string &msg) { return fail(code, msg); }
+
 // =============================================================================== C ABI
 extern "C" {
 

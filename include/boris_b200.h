@@ -151,6 +151,21 @@ int bm_debug_tensor(int device, int nx, int ny, int nz, double hx, double hy, do
  * uses exp(+2 pi i ...), unnormalised. */
 int bm_debug_fft(int device, int L, int howmany, int precision, int inverse, double *data);
 
+/* Allocation-free batched FFT, for callers that cannot allocate device memory when they need
+ * the transform (a host that has handed the rest of the GPU's memory to other work, or a
+ * solver in the middle of an asynchronous step where a cudaMalloc/cudaFree, which may
+ * synchronise the device, would stall it). This entry point has no counterpart in the
+ * reference. It transforms `howmany` contiguous lines of L complex FP64 values (interleaved
+ * re/im) from the device buffer `in` into the device buffer `out` (in == out transforms in
+ * place), on `stream` (a cudaStream_t; NULL for the default stream), unnormalised, with
+ * exp(+2 pi i ...) when inverse != 0. It calls no cudaMalloc/cudaFree: its only scratch, the
+ * twiddle table, lives in a fixed device array of 4096 complex doubles (64 KiB) that every GPU
+ * loading the library keeps until exit, so L is limited to 1..4096 (2^p or 3*2^p). The first
+ * call on a device looks up that array's device address; make that first call before any
+ * stream capture. The table is rewritten by every call, so calls that overlap on the GPU
+ * (different streams, or concurrent host threads) race on it and must be serialised. */
+int bm_fft_noalloc(int device, int L, int howmany, int inverse, const double *in, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
