@@ -68,7 +68,7 @@ struct Mesh {
     long long n = 0;
     int Nx = 1, Ny = 1, Nz = 1, LX = 1;
     FFTPlan px, py, pz;
-    int W2 = 1, Wy = 1, Wz = 1, rpb = 1;
+    int W2 = 1, Wy = 1, Wz = 1, rpb = 1, staged = 0;
     // device (element type depends on the context precision)
     void *buf[4] = {nullptr, nullptr, nullptr, nullptr};   // A (M), P (sM1), B, C
     void *ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -222,6 +222,7 @@ void choose_tiles(Mesh &m)
         int tpl = stage_reg_q(m.LX) ? stage_reg_q(m.LX) : m.px.tpl;
         int rpb = lim / (3 * tpl);
         if (rpb < 1) rpb = 1;
+        while (rpb > 1 && ((3 * rpb * tpl + 31) & ~31) > lim) rpb--;
         while (rpb > 1 && (size_t)3 * rpb * padded_len(m.LX) * cs > 64 * 1024) rpb--;
         int rows = m.ny * m.nz;
         if (rpb > rows) rpb = rows;
@@ -412,17 +413,22 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
         a.ev[0] = (const T *)m.buf[0]; a.ev[1] = (const T *)m.buf[0];
         a.ev_out = tmp;
         a.Mout = tmp + 3 * m.n;
-        float best = 1e30f; int br = m.rpb;
+        float best = 1e30f; int br = m.rpb, bs = 0;
         int rows = m.ny * m.nz;
         const int tpl = stage_reg_q(m.LX) ? stage_reg_q(m.LX) : m.px.tpl;
-        for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
-            if (3 * rpb * tpl > lim) break;
-            if ((size_t)3 * rpb * padded_len(m.LX) * cs > 200 * 1024) break;
-            a.rpb = rpb;
-            float t = time_launches(s, [&]() { return launch_stage<T>(a, s); }, reps);
-            if (t < best) { best = t; br = rpb; }
-        }
+        // rows per block x (per-cell rows prefetched to shared memory or read from global);
+        // staging applies to the register kernel only
+        for (int stg = 0; stg <= (stage_reg_q(m.LX) ? 1 : 0); stg++)
+            for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
+                if (((3 * rpb * tpl + 31) & ~31) > lim) break;
+                if ((size_t)3 * rpb * padded_len(m.LX) * cs > 200 * 1024) break;
+                a.rpb = rpb;
+                a.staged = stg;
+                float t = time_launches(s, [&]() { return launch_stage<T>(a, s); }, reps);
+                if (t < best) { best = t; br = rpb; bs = stg; }
+            }
         m.rpb = br;
+        m.staged = bs;
     }
     cudaStreamSynchronize(s);
     cudaFree(tmp);
@@ -441,6 +447,8 @@ int prepare_T(bm_ctx *c)
         int t4[4];
         if (ev && sscanf(ev, "%d,%d,%d,%d", &t4[0], &t4[1], &t4[2], &t4[3]) == 4) {
             m.W2 = t4[0]; m.Wy = t4[1]; m.Wz = t4[2]; m.rpb = t4[3];
+            const char *sr = getenv("BM_STAGE_ROWS");
+            m.staged = (sr && sr[0] == '1') ? 1 : 0;
         } else if (c->autotune) autotune_mesh<T>(c, m);
     }
     return 0;
@@ -513,6 +521,7 @@ StageArgs<T> stage_args(bm_ctx *c, Mesh &m)
     a.st = c->st;
     a.n = m.n;
     a.do_xfwd = (m.modules & BM_DEMAG) ? 1 : 0;
+    a.staged = m.staged;
     return a;
 }
 
@@ -1150,7 +1159,7 @@ int bm_tiles(bm_ctx *c, int mesh, int *tiles4)
     if (int rc = check_mesh(c, mesh)) return rc;
     if (!tiles4) return fail(BM_EINVAL, "null out");
     Mesh &m = c->meshes[mesh];
-    tiles4[0] = m.W2; tiles4[1] = m.Wy; tiles4[2] = m.Wz; tiles4[3] = m.rpb;
+    tiles4[0] = m.W2; tiles4[1] = m.Wy; tiles4[2] = m.Wz; tiles4[3] = m.staged ? -m.rpb : m.rpb;
     return 0;
 }
 

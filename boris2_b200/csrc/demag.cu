@@ -392,8 +392,7 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
 template <typename T, int NZ>
 static int launch_zmid_reg(const YZArgs<T> &a, cudaStream_t s)
 {
-    int nt = 6 * a.W;
-    if (nt < 32) nt = 32;
+    int nt = (6 * a.W + 31) & ~31;
     if (nt > bm_lb<T>::v) return 104;
     size_t smem = zmid_reg_smem<T>(NZ, a.W);
     if (smem > 200 * 1024) return 105;

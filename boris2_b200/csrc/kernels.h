@@ -94,7 +94,27 @@ struct StageArgs {
     double crhs;
     int renorm, mode, do_xfwd, last_kind, gate;
     long long n;         // cells
+    int staged;          // prefetch the per-cell input rows into shared memory (register kernel)
 };
+
+// Shared-memory row staging of the register stage kernel: per block row, kr rows of nx values:
+// 3*ns rows of M (slot 0 the row itself, 1/2 the y-1/y+1 rows, 3/4 the z-1/z+1 rows, each x,y,z),
+// 3 rows of the update base (when it differs from M), 3 per earlier stage evaluation, then the
+// Ms map row and the K1 map row when present and used.
+struct StageLayout {
+    int ns, mb, ms, k1, kr;
+};
+template <typename T> __host__ __device__ inline StageLayout stage_layout(const StageArgs<T> &a)
+{
+    StageLayout L;
+    const bool fields = a.mode != BM_MODE_UPDATE;
+    L.ns = (fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI))) ? 5 : 1;
+    L.mb = (a.mode != BM_MODE_HEFF && a.Mbase && a.Mbase != a.Min) ? 1 : 0;
+    L.ms = a.Ms_map ? 1 : 0;
+    L.k1 = (a.K1_map && fields && (a.modules & BM_MOD_ANIUNI)) ? 1 : 0;
+    L.kr = 3 * L.ns + 3 * L.mb + 3 * (a.mode == BM_MODE_HEFF ? 0 : a.nev) + L.ms + L.k1;
+    return L;
+}
 
 template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s);
 int stage_reg_q(int LX);   // threads per x line of the register stage kernel (0: generic kernel)

@@ -153,8 +153,37 @@ __device__ __forceinline__ void axis_stencil(const T m[3], const T *mp, const T 
 // Per-cell part of a stage: Heff, LLG, update. `lines` holds the 3 * rpb packed x lines of the
 // block (component-major), element e of line q at sm[q * LSP + addr(e)]; on entry it carries
 // the unscaled inverse-x result (H_demag / scale), on exit the new M (when do_xfwd).
-template <typename T, typename AddrF>
-__device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, int LSP, AddrF addr, int r0, double &lmax)
+// Per-cell input accessors. AccGlobal reads the device arrays; AccStaged reads the rows the
+// register kernel prefetched into shared memory (layout: stage_layout in kernels.h).
+template <typename T> struct AccGlobal {
+    const StageArgs<T> *a;
+    long long n, off[5];
+    __device__ AccGlobal(const StageArgs<T> &aa) : a(&aa), n(aa.n)
+    {
+        long long nxy = (long long)aa.nx * aa.ny;
+        off[0] = 0; off[1] = -aa.nx; off[2] = aa.nx; off[3] = -nxy; off[4] = nxy;
+    }
+    __device__ __forceinline__ T m(int, int slot, int c, int, long long cell) const { return a->Min[c * n + cell + off[slot]]; }
+    __device__ __forceinline__ T mb(int, int c, int, long long cell) const { return a->Mbase[c * n + cell]; }
+    __device__ __forceinline__ T ev(int i, int, int c, int, long long cell) const { return a->ev[i][c * n + cell]; }
+    __device__ __forceinline__ T ms(int, int, long long cell) const { return a->Ms_map[cell]; }
+    __device__ __forceinline__ T k1(int, int, long long cell) const { return a->K1_map[cell]; }
+};
+
+template <typename T> struct AccStaged {
+    const T *R;
+    int nx, kr, ns3, hasmb, evo, mso, k1o;
+    __device__ __forceinline__ const T *row(int r, int k) const { return R + ((long long)r * kr + k) * nx; }
+    __device__ __forceinline__ T m(int r, int slot, int c, int x, long long) const { return row(r, slot * 3 + c)[x]; }
+    __device__ __forceinline__ T mb(int r, int c, int x, long long) const { return row(r, hasmb ? ns3 + c : c)[x]; }
+    __device__ __forceinline__ T ev(int i, int r, int c, int x, long long) const { return row(r, evo + 3 * i + c)[x]; }
+    __device__ __forceinline__ T ms(int r, int x, long long) const { return row(r, mso)[x]; }
+    __device__ __forceinline__ T k1(int r, int x, long long) const { return row(r, k1o)[x]; }
+};
+
+template <typename T, typename AddrF, typename Acc>
+__device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, int LSP, AddrF addr, int r0, double &lmax,
+                                            const Acc &acc)
 {
     const int nx = a.nx, ny = a.ny, nz = a.nz, rpb = a.rpb;
     const int nrows = ny * nz;
@@ -189,8 +218,9 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         if (row >= nrows) continue;
         long long cell = (long long)row * nx + x;
         T m[3];
-        ld3(a.Min, n, cell, m);
-        T Ms = a.Ms_map ? a.Ms_map[cell] : a.Ms;
+#pragma unroll
+        for (int c = 0; c < 3; c++) m[c] = acc.m(r, 0, c, x, cell);
+        T Ms = a.Ms_map ? acc.ms(r, x, cell) : a.Ms;
         T rhs[3] = {0, 0, 0};
         if (fields) {
             T H[3] = {Ha[0], Ha[1], Ha[2]};
@@ -202,12 +232,15 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 int y = row % ny, z = row / ny;
                 T mxp[3], mxm[3], myp[3], mym[3], mzp[3], mzm[3];
                 bool hxp = x + 1 < nx, hxm = x > 0, hyp = y + 1 < ny, hym = y > 0, hzp = z + 1 < nz, hzm = z > 0;
-                if (hxp) ld3(a.Min, n, cell + 1, mxp);
-                if (hxm) ld3(a.Min, n, cell - 1, mxm);
-                if (hyp) ld3(a.Min, n, cell + nx, myp);
-                if (hym) ld3(a.Min, n, cell - nx, mym);
-                if (hzp) ld3(a.Min, n, cell + (long long)nx * ny, mzp);
-                if (hzm) ld3(a.Min, n, cell - (long long)nx * ny, mzm);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    mxp[c] = hxp ? acc.m(r, 0, c, x + 1, cell + 1) : (T)0;
+                    mxm[c] = hxm ? acc.m(r, 0, c, x - 1, cell - 1) : (T)0;
+                    mym[c] = hym ? acc.m(r, 1, c, x, cell) : (T)0;
+                    myp[c] = hyp ? acc.m(r, 2, c, x, cell) : (T)0;
+                    mzm[c] = hzm ? acc.m(r, 3, c, x, cell) : (T)0;
+                    mzp[c] = hzp ? acc.m(r, 4, c, x, cell) : (T)0;
+                }
                 T rr = (a.A != (T)0) ? Dv / (2 * a.A) : (T)0;
                 T bx[3] = {rr * m[2], 0, -rr * m[0]};
                 T by[3] = {0, rr * m[2], -rr * m[1]};
@@ -223,7 +256,7 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 for (int c = 0; c < 3; c++) H[c] += Ac * (dx[c] + dy[c] + dz[c]) + Dc * hd[c];
             }
             if (a.modules & BM_MOD_ANIUNI) {
-                T K1 = a.K1_map ? a.K1_map[cell] : a.K1;
+                T K1 = a.K1_map ? acc.k1(r, x, cell) : a.K1;
                 T dp = (m[0] * a.ea[0] + m[1] * a.ea[1] + m[2] * a.ea[2]) / Ms;
                 T s = (2 / ((T)BM_MU0 * Ms)) * dp * (K1 + 2 * a.K2 * (1 - dp * dp));
 #pragma unroll
@@ -246,9 +279,9 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             double d2 = 0.0, m2 = 0.0;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                double acc = 0.0;
-                for (int i = 0; i < a.nev; i++) acc += a.cev[i] * (double)a.ev[i][c * n + cell];
-                double pred = (double)a.Mbase[c * n + cell] + dT * (acc + a.crhs * (double)rhs[c]);
+                double sum = 0.0;
+                for (int i = 0; i < a.nev; i++) sum += a.cev[i] * (double)acc.ev(i, r, c, x, cell);
+                double pred = (double)acc.mb(r, c, x, cell) + dT * (sum + a.crhs * (double)rhs[c]);
                 double d = (double)m[c] - pred;
                 d2 += d * d;
                 m2 += (double)m[c] * (double)m[c];
@@ -263,9 +296,9 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         T mn[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            T acc = crhs * rhs[c];
-            for (int i = 0; i < a.nev; i++) acc += cev[i] * a.ev[i][c * n + cell];
-            mn[c] = a.Mbase[c * n + cell] + acc;
+            T sum = crhs * rhs[c];
+            for (int i = 0; i < a.nev; i++) sum += cev[i] * acc.ev(i, r, c, x, cell);
+            mn[c] = acc.mb(r, c, x, cell) + sum;
         }
         if (a.renorm) {
             T f = Ms / sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
@@ -401,7 +434,7 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
         fft_line<T, true, true>(line, 1, t, qact, a.px, a.twx);
     }
     double lmax = 0.0;
-    stage_cells<T>(a, sm, LSP, [](int e) { return eaddr<true>(e, 1); }, r0, lmax);
+    stage_cells<T>(a, sm, LSP, [](int e) { return eaddr<true>(e, 1); }, r0, lmax, AccGlobal<T>(a));
     if (a.do_xfwd) {
         const int first_pad = (a.nx + 1) >> 1;
         for (int idx = tid; idx < 3 * rpb * LX; idx += blockDim.x) {
@@ -491,19 +524,75 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
     cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
     const bool demag = (a.mode != BM_MODE_UPDATE) && (a.modules & BM_MOD_DEMAG);
     const int half = (a.nx + 1) >> 1;   // packed elements that carry mesh cells
-    if (demag) {
-        if (qact) {
-            const cpx<T> *src = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
+    // group 1: the spectrum rows
+    if (demag && qact) {
+        const cpx<T> *src = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
 #pragma unroll 4
-            for (int m = t; m < LX; m += Q) cp_async_cpx<T>(&line[A(m)], &src[m], true);
+        for (int m = t; m < LX; m += Q) cp_async_cpx<T>(&line[A(m)], &src[m], true);
+    }
+    cp_async_commit();
+    // group 2: the per-cell input rows, arriving while the inverse transform runs
+    AccStaged<T> st;
+    if (a.staged) {
+        const StageLayout L = stage_layout(a);
+        const int nx = a.nx, ny = a.ny, nz = a.nz;
+        const long long n = a.n;
+        size_t lbytes = ((size_t)3 * rpb * LSP * sizeof(cpx<T>) + 15) & ~(size_t)15;
+        T *R = reinterpret_cast<T *>(smraw + lbytes);
+        st.R = R; st.nx = nx; st.kr = L.kr; st.ns3 = 3 * L.ns; st.hasmb = L.mb;
+        st.evo = 3 * L.ns + 3 * L.mb;
+        st.mso = st.evo + 3 * (a.mode == BM_MODE_HEFF ? 0 : a.nev);
+        st.k1o = st.mso + L.ms;
+        const bool chunk = ((nx * (int)sizeof(T)) % 16) == 0;
+        const int per16 = 16 / (int)sizeof(T);
+        const int CH = chunk ? nx / per16 : nx;
+        const int lane = tid & 31, warp = tid >> 5, nwarp = (blockDim.x + 31) >> 5;
+        const int wsz = min(32, (int)blockDim.x - warp * 32);   // lanes present in this warp
+        for (int job = warp; job < rpb * L.kr; job += nwarp) {
+            const int r = job / L.kr, kk = job - r * L.kr;
+            const int row = r0 + r;
+            if (row >= nrows) continue;
+            const int y = row % ny, z = row / ny;
+            const T *src = nullptr;
+            if (kk < 3 * L.ns) {
+                const int slot = kk / 3, c = kk - 3 * slot;
+                long long srow = -1;
+                if (slot == 0) srow = row;
+                else if (slot == 1) srow = (y > 0) ? row - 1 : -1;
+                else if (slot == 2) srow = (y + 1 < ny) ? row + 1 : -1;
+                else if (slot == 3) srow = (z > 0) ? row - ny : -1;
+                else srow = (z + 1 < nz) ? row + ny : -1;
+                if (srow >= 0) src = a.Min + c * n + srow * nx;
+            } else if (kk < st.evo) {
+                src = a.Mbase + (kk - 3 * L.ns) * n + (long long)row * nx;
+            } else if (kk < st.mso) {
+                const int i = (kk - st.evo) / 3, c = (kk - st.evo) - 3 * i;
+                src = a.ev[i] + c * n + (long long)row * nx;
+            } else if (kk < st.k1o) {
+                src = a.Ms_map + (long long)row * nx;
+            } else {
+                src = a.K1_map + (long long)row * nx;
+            }
+            if (!src) continue;
+            T *dst = R + ((long long)r * L.kr + kk) * nx;
+            if (chunk)
+                for (int i = lane; i < CH; i += wsz) cp_async_el<16>(dst + i * per16, src + i * per16, true);
+            else
+                for (int i = lane; i < CH; i += wsz) cp_async_real<T>(dst + i, src + i, true);
         }
-        cp_async_wait_all();
+    }
+    cp_async_commit();
+    if (demag) {
+        cp_async_wait_group<1>();
         __syncthreads();
         xinv_pre_f<T>(line, LX, a.twx2, t, Q, qact, A);
         x_twolevel<T, P, Q, true>(line, t, qact, a.twx, half);
     }
+    cp_async_wait_group<0>();
+    __syncthreads();
     double lmax = 0.0;
-    stage_cells<T>(a, sm, LSP, A, r0, lmax);
+    if (a.staged) stage_cells<T>(a, sm, LSP, A, r0, lmax, st);
+    else stage_cells<T>(a, sm, LSP, A, r0, lmax, AccGlobal<T>(a));
     if (a.do_xfwd) {
         for (int idx = tid; idx < 3 * rpb * (LX / 2); idx += blockDim.x) {
             int qq = idx / (LX / 2), mm = idx - qq * (LX / 2);
@@ -525,18 +614,25 @@ template <typename T, int P, int Q>
 static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
 {
     constexpr int LX = P * Q;
-    int nt = 3 * a.rpb * Q;
+    int nt = (3 * a.rpb * Q + 31) & ~31;   // whole warps: the error-norm reduction shuffles full warps
     if (nt > bm_lb<T>::v) return 203;
-    if (nt < 32) nt = 32;
     size_t smem = (size_t)3 * a.rpb * (LX + LX / P + 1) * sizeof(cpx<T>);
     if (smem > 200 * 1024) return 204;
+    StageArgs<T> b = a;
+    if (b.staged) {
+        // stage the per-cell rows when they fit; otherwise read them from global memory
+        size_t lb = (smem + 15) & ~(size_t)15;
+        size_t rb = (size_t)b.rpb * stage_layout(b).kr * b.nx * sizeof(T);
+        if (lb + rb <= 200 * 1024) smem = lb + rb;
+        else b.staged = 0;
+    }
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_stage_reg<T, P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
     }
     int nrows = a.ny * a.nz;
     dim3 grid((nrows + a.rpb - 1) / a.rpb);
-    k_stage_reg<T, P, Q><<<grid, nt, smem, s>>>(a);
+    k_stage_reg<T, P, Q><<<grid, nt, smem, s>>>(b);
     return (int)cudaGetLastError();
 }
 
@@ -567,8 +663,7 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
     case 1024: return launch_stage_reg<T, 32, 32>(a, s);
     default: break;
     }
-    int nt = 3 * a.rpb * a.px.tpl;
-    if (nt < 32) nt = 32;
+    int nt = (3 * a.rpb * a.px.tpl + 31) & ~31;   // whole warps
     if (nt > bm_lb<T>::v) return 201;
     size_t smem = (size_t)3 * a.rpb * padded_len(a.LX) * sizeof(cpx<T>);
     if (smem > 200 * 1024) return 202;

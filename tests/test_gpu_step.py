@@ -155,3 +155,32 @@ def test_norm_preserved_and_energy_decreases(bm):
     c.close()
     assert np.abs(np.linalg.norm(m, axis=1) / 8e5 - 1).max() < 1e-5
     assert e1 < e0
+
+
+@pytest.mark.parametrize("staged", ["0", "1"])
+@pytest.mark.parametrize("rows", [1, 3])
+def test_stage_kernel_variants(bm, staged, rows, monkeypatch):
+    """Both stage-kernel variants (per-cell rows prefetched into shared memory or read from
+    global memory) and several rows per block, forced through BM_TILES / BM_STAGE_ROWS, give the
+    oracle's RKDP54 trajectory (exchange + iDMI + anisotropy + demag, 3D, LX = 128 and 64)."""
+    monkeypatch.setenv("BM_TILES", "1,4,8,%d" % rows)
+    monkeypatch.setenv("BM_STAGE_ROWS", staged)
+    for n in [(100, 10, 3), (64, 12, 2)]:
+        N = n[0] * n[1] * n[2]
+        rng = np.random.default_rng(5)
+        Ms_map = 1.1e6 * (1 + 0.05 * rng.normal(size=N))
+        mesh = dict(n=n, h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, D=1.5e-3, alpha=0.1, K1=5e5,
+                    modules=1 | 4 | 8 | 16, Ha=(1e3, 0, 0), Ms_map=Ms_map)
+        M = tilted_z(N, seed=23) * Ms_map[:, None]
+        s = OracleSolver([mesh], evaluation=1, dt=1e-14, tol=1e-5, dT_incr=2.0, dT_min=1e-15, dT_max=3e-12)
+        s.set_m(M)
+        sr = s.run(8)
+        mref = s.get_m() / Ms_map[:, None]
+        c = _make(bm, "fp64", mesh, M, "RKDP54", 1e-14, (1e-5, 2.0, 1e-15, 3e-12))
+        st = c.run(8)
+        t = c.tiles()
+        m = c.get_m() / Ms_map[:, None]
+        c.close()
+        assert abs(t["stage_rows"]) == rows and (t["stage_rows"] < 0) == (staged == "1")
+        assert st["rejected"] == sr["rejected"]
+        assert np.abs(m - mref).max() < 1e-8
