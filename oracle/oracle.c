@@ -414,6 +414,527 @@ double orc_demag_apply(orc_demag *d, const double *M, double *H, int add)
     return dot;
 }
 
+/* ------------------------------------------------------------------ multilayered convolution */
+
+/* Geometry of the multilayered convolution (SDemag multilayer mode):
+ *   n_common        SDemag::set_default_n_common (Boris/SDemag.cpp:173), Set_n_common (:362),
+ *                   Set_2D_Multilayered_Convolution (:341)
+ *   layer rects     SDemag::set_Rect_collection (Boris/SDemag.cpp:215), Rect::get_zlayer
+ *                   (BorisLib/Types_Rect.h:485) in 2D-layered mode
+ *   h_max           SDemag::get_maximum_cellsize (Boris/SDemag.cpp:297): the meshes' own cellsizes
+ *   transfer        SDemag_Demag::Initialize (Boris/SDemag_Demag.cpp:349-361) and the weighted
+ *                   mesh transfer of BorisLib/VEC_MeshTransfer.h (:306 build_meshcells_weights,
+ *                   :396 build_supermeshcells_weights, :901 initialize_transfer_in_weighted,
+ *                   :1221 initialize_transfer_out)
+ *   kernels         DemagKernelCollection::Calculate_Demag_Kernels and KernelAlreadyComputed
+ *                   (Boris/DemagKernelCollection_Calc.cpp:9,114); tensors from
+ *                   DemagTFunc_Shifted.cpp (3D and regular 2D) and DemagTFunc_Irregular.cpp
+ *                   (2D with source and destination thickness differing), including the
+ *                   thickness roles and far-field scaling those functions use
+ *   evaluation      SDemag::UpdateField multilayer branch (Boris/SDemag.cpp:786-900)
+ * Spectra here are plain full complex 3D DFTs of the real-space tensors (no symmetry storage). */
+
+#define ML_EPS 1e-12          /* BorisLib/Funcs_Aux_base.h:9 EPSILON_POSITIVE */
+#define ML_EPS_ROUND 1e-4     /* BorisLib/Funcs_Aux_base.h:13 EPSILON_ROUNDING */
+
+typedef struct { double x, y, z; } d3;
+typedef struct { d3 s, e; } rect3;
+
+static int isz(double v) { return v < ML_EPS && v > -ML_EPS; }
+static int iszop(double v) { return v > 0 || isz(v); }
+static int d3eq(d3 a, d3 b) { return isz(a.x - b.x) && isz(a.y - b.y) && isz(a.z - b.z); }
+static d3 d3m(double x, double y, double z) { d3 r = {x, y, z}; return r; }
+static d3 d3sub(d3 a, d3 b) { return d3m(a.x - b.x, a.y - b.y, a.z - b.z); }
+static d3 d3add(d3 a, d3 b) { return d3m(a.x + b.x, a.y + b.y, a.z + b.z); }
+static double d3norm(d3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+static d3 rsize(rect3 r) { return d3sub(r.e, r.s); }
+static int recteq(rect3 a, rect3 b) { return d3eq(a.s, b.s) && d3eq(a.e, b.e); }
+static double floor_eps(double v) { return floor(v + ML_EPS_ROUND); }
+static double ceil_eps(double v) { return ceil(v - ML_EPS_ROUND); }
+
+/* Rect::get_intersection and intersects (BorisLib/Types_Rect.h:494,361) */
+static int rect_intersection(rect3 a, rect3 b, rect3 *out)
+{
+    d3 st = d3m(b.s.x > a.s.x ? b.s.x : a.s.x, b.s.y > a.s.y ? b.s.y : a.s.y, b.s.z > a.s.z ? b.s.z : a.s.z);
+    d3 en = d3m(b.e.x < a.e.x ? b.e.x : a.e.x, b.e.y < a.e.y ? b.e.y : a.e.y, b.e.z < a.e.z ? b.e.z : a.e.z);
+    rect3 r = {{0, 0, 0}, {0, 0, 0}};
+    if (iszop(en.x - st.x) && iszop(en.y - st.y) && iszop(en.z - st.z)) { r.s = st; r.e = en; }
+    *out = r;
+    /* intersects: the intersection differs from the null rect */
+    return !(isz(r.s.x) && isz(r.s.y) && isz(r.s.z) && isz(r.e.x) && isz(r.e.y) && isz(r.e.z));
+}
+static int rect_isplane(rect3 r)
+{
+    double dx = r.s.x - r.e.x, dy = r.s.y - r.e.y, dz = r.s.z - r.e.z;
+    return (isz(dx) && !isz(dy) && !isz(dz)) || (isz(dy) && !isz(dx) && !isz(dz)) || (isz(dz) && !isz(dx) && !isz(dy));
+}
+static int rect_ispoint(rect3 r) { return d3eq(r.s, r.e); }
+
+typedef struct { int n; int *idx; double *w; } wlist;   /* one cell's contributions */
+
+static void wl_push(wlist *l, int idx, double w)
+{
+    l->idx = (int *)realloc(l->idx, sizeof(int) * (l->n + 1));
+    l->w = (double *)realloc(l->w, sizeof(double) * (l->n + 1));
+    l->idx[l->n] = idx; l->w[l->n] = w; l->n++;
+}
+
+/* cells of grid (n, h, origin rs) within the index box of rect rc, with reciprocal-distance weights */
+static double recip_weights(wlist *l, rect3 rc, const int n[3], d3 h, d3 rs)
+{
+    d3 coord = d3sub(d3m((rc.e.x + rc.s.x) / 2, (rc.e.y + rc.s.y) / 2, (rc.e.z + rc.s.z) / 2), rs);
+    d3 pll = d3sub(rc.s, rs), pur = d3sub(rc.e, rs);
+    int ll[3] = {(int)floor_eps(pll.x / h.x), (int)floor_eps(pll.y / h.y), (int)floor_eps(pll.z / h.z)};
+    int ur[3] = {(int)ceil_eps(pur.x / h.x), (int)ceil_eps(pur.y / h.y), (int)ceil_eps(pur.z / h.z)};
+    d3 sz = rsize(rc);
+    double dmax = d3norm(d3m(sz.x / 2 + h.x / 2, sz.y / 2 + h.y / 2, sz.z / 2 + h.z / 2));
+    double tot = 0.0;
+    for (int ii = ll[0] >= 0 ? ll[0] : 0; ii < (ur[0] < n[0] ? ur[0] : n[0]); ii++)
+        for (int jj = ll[1] >= 0 ? ll[1] : 0; jj < (ur[1] < n[1] ? ur[1] : n[1]); jj++)
+            for (int kk = ll[2] >= 0 ? ll[2] : 0; kk < (ur[2] < n[2] ? ur[2] : n[2]); kk++) {
+                d3 cc = d3m((ii + 0.5) * h.x, (jj + 0.5) * h.y, (kk + 0.5) * h.z);
+                double dr = dmax - d3norm(d3sub(cc, coord));
+                tot += dr;
+                wl_push(l, ii + jj * n[0] + kk * n[0] * n[1], dr);
+            }
+    return tot;
+}
+
+typedef struct {
+    int type;       /* 0 regular (same cellsize), 1 irregular 2D (source / destination thickness differ) */
+    d3 hs, hd, shift;   /* normalised by h_max */
+    double *F;      /* 6 full complex spectra, component-major, each Nx*Ny*Nz complex */
+} ml_kernel;
+
+typedef struct {
+    int mesh, transfer;
+    rect3 rect;
+    d3 hc;                      /* convolution cellsize (rect / n_common) */
+    wlist *tin;                 /* per common cell */
+    wlist *tout;                /* per mesh cell */
+    int *kidx, *kinv;           /* per source: kernel index, inverse z-shift flag */
+    int *kkind;                 /* per source: 1 self, 2 z-shifted, 3 inverse z-shifted, 4 full */
+} ml_layer;
+
+struct orc_ml {
+    int nmesh, L;
+    int (*mn)[3];
+    d3 *mh;
+    rect3 *mrect;
+    size_t *moff;               /* first cell of each mesh in the concatenated arrays */
+    int nc[3], N[3], force2d;
+    double h_max;
+    ml_layer *lay;
+    ml_kernel *ker;
+    int nker;
+};
+
+/* one tensor point D = -N (xx,yy,zz,xy,xz,yz) at grid offset (i,j,k) for a kernel */
+static void ml_tensor_point(const ml_kernel *K, int i, int j, int k, int two_d, double out[6])
+{
+    const d3 h = (K->type == 1) ? K->hd : K->hs;
+    const d3 sh = K->shift;
+    double is = fabs(i + sh.x / h.x), js = fabs(j + sh.y / h.y), ks = fabs(k + sh.z / h.z);
+    int far = ((int)floor_eps(is) >= ASYMPT_DIST || (int)floor_eps(js) >= ASYMPT_DIST || (int)floor_eps(ks) >= ASYMPT_DIST ||
+               (int)floor_eps(is * is + js * js + ks * ks) >= ASYMPT_DIST * ASYMPT_DIST);
+    double x = i * h.x + sh.x, y = j * h.y + sh.y, z = k * h.z + sh.z;
+    if (far) {
+        orc_asymptotic(h.x, h.y, h.z, x, y, z, out);
+        /* irregular: the reference scales the destination-cell expansion by the source thickness
+         * (DemagTFunc_Irregular.cpp:52-56) */
+        if (K->type == 1) for (int c = 0; c < 6; c++) out[c] *= K->hs.z;
+    } else if (K->type == 0) {
+        out[0] = -newell_L(orc_newell_f, x, y, z, h.x, h.y, h.z);
+        out[1] = -newell_L(orc_newell_f, y, x, z, h.y, h.x, h.z);
+        out[2] = -newell_L(orc_newell_f, z, y, x, h.z, h.y, h.x);
+        out[3] = -newell_L(orc_newell_g, x, y, z, h.x, h.y, h.z);
+        out[4] = -newell_L(orc_newell_g, x, z, y, h.x, h.z, h.y);
+        out[5] = -newell_L(orc_newell_g, y, z, x, h.y, h.z, h.x);
+    } else {
+        /* 36-point sums: (-1,2,-1) along the two in-plane axes, four z points along the axis
+         * carrying the shift. xx, yy use z in {D-s, D, D+d, D+d-s}; zz, xy, xz, yz use
+         * z in {D-d, D, D+s, D+s-d} (D the shift, s / d the source / destination thickness),
+         * as fill_f_vals_zshifted_irregular / fill_g_vals_zshifted_irregular
+         * (DemagTFunc_fg.cpp:507,560) and DemagTFunc_L.cpp:377-814 combine them. */
+        const double s = K->hs.z, d = K->hd.z;
+        const double zA[4] = {z - s, z, z + d, z + d - s}, zB[4] = {z - d, z, z + s, z + s - d};
+        const double wz[4] = {-1.0, 1.0, -1.0, 1.0};
+        const double cw[3] = {-1.0, 2.0, -1.0};
+        const double tau = h.x * h.y * h.z;
+        for (int c = 0; c < 6; c++) {
+            double v[36];
+            int m = 0;
+            for (int a = -1; a <= 1; a++)
+                for (int b = -1; b <= 1; b++)
+                    for (int q = 0; q < 4; q++) {
+                        double w = cw[a + 1] * cw[b + 1] * wz[q], val;
+                        switch (c) {
+                        case 0: val = orc_newell_f(x + a * h.x, y + b * h.y, zA[q]); break;
+                        case 1: val = orc_newell_f(y + a * h.y, x + b * h.x, zA[q]); break;
+                        case 2: val = orc_newell_f(zB[q], y + a * h.y, x + b * h.x); break;
+                        case 3: val = orc_newell_g(x + a * h.x, y + b * h.y, zB[q]); break;
+                        case 4: val = orc_newell_g(x + a * h.x, zB[q], y + b * h.y); break;
+                        default: val = orc_newell_g(y + a * h.y, zB[q], x + b * h.x); break;
+                        }
+                        v[m++] = w * val;
+                    }
+            out[c] = -csum(v, 36) / (4.0 * M_PI * tau);
+        }
+    }
+    /* 2D self kernel: only Dxy is computed off the diagonal (CalcOffDiagTens2D) */
+    if (two_d && sh.x == 0.0 && sh.y == 0.0 && sh.z == 0.0) { out[4] = 0.0; out[5] = 0.0; }
+}
+
+static void ml_build_kernel(const struct orc_ml *s, ml_kernel *K)
+{
+    const int Nx = s->N[0], Ny = s->N[1], Nz = s->N[2];
+    const int nx = s->nc[0], ny = s->nc[1], nz = s->nc[2];
+    const int two_d = (nz == 1);
+    size_t np = (size_t)Nx * Ny * Nz;
+    K->F = (double *)calloc(6 * 2 * np, sizeof(double));
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int k = -nz + 1; k < nz; k++)
+        for (int j = -ny + 1; j < ny; j++)
+            for (int i = -nx + 1; i < nx; i++) {
+                double v[6];
+                ml_tensor_point(K, i, j, k, two_d, v);
+                size_t p = (size_t)((i + Nx) % Nx) + (size_t)((j + Ny) % Ny) * Nx + (size_t)((k + Nz) % Nz) * Nx * Ny;
+                for (int c = 0; c < 6; c++) K->F[2 * (c * np + p)] = v[c];
+            }
+    for (int c = 0; c < 6; c++) dft3(K->F + 2 * c * np, Nx, Ny, Nz, -1);
+}
+
+void orc_ml_destroy(orc_ml *s)
+{
+    if (!s) return;
+    for (int l = 0; l < s->L; l++) {
+        ml_layer *y = &s->lay[l];
+        if (y->tin) {
+            size_t ncell = (size_t)s->nc[0] * s->nc[1] * s->nc[2];
+            for (size_t i = 0; i < ncell; i++) { free(y->tin[i].idx); free(y->tin[i].w); }
+            free(y->tin);
+        }
+        if (y->tout) {
+            int m = y->mesh;
+            size_t n = (size_t)s->mn[m][0] * s->mn[m][1] * s->mn[m][2];
+            for (size_t i = 0; i < n; i++) { free(y->tout[i].idx); free(y->tout[i].w); }
+            free(y->tout);
+        }
+        free(y->kidx); free(y->kinv); free(y->kkind);
+    }
+    for (int q = 0; q < s->nker; q++) free(s->ker[q].F);
+    free(s->ker); free(s->lay); free(s->mn); free(s->mh); free(s->mrect); free(s->moff);
+    free(s);
+}
+
+orc_ml *orc_ml_create(int nmesh, const int *n3, const double *h3, const double *o3, int mode, const int *ncommon)
+{
+    orc_ml *s = (orc_ml *)calloc(1, sizeof(orc_ml));
+    s->nmesh = nmesh;
+    s->mn = calloc(nmesh, sizeof(*s->mn));
+    s->mh = (d3 *)calloc(nmesh, sizeof(d3));
+    s->mrect = (rect3 *)calloc(nmesh, sizeof(rect3));
+    s->moff = (size_t *)calloc(nmesh + 1, sizeof(size_t));
+    for (int m = 0; m < nmesh; m++) {
+        for (int a = 0; a < 3; a++) s->mn[m][a] = n3[3 * m + a];
+        s->mh[m] = d3m(h3[3 * m], h3[3 * m + 1], h3[3 * m + 2]);
+        s->mrect[m].s = d3m(o3[3 * m], o3[3 * m + 1], o3[3 * m + 2]);
+        s->mrect[m].e = d3add(s->mrect[m].s, d3m(s->mh[m].x * s->mn[m][0], s->mh[m].y * s->mn[m][1], s->mh[m].z * s->mn[m][2]));
+        s->moff[m + 1] = s->moff[m] + (size_t)s->mn[m][0] * s->mn[m][1] * s->mn[m][2];
+    }
+    /* n_common and the 2D mode */
+    int force2d = mode;
+    if (ncommon) {
+        for (int a = 0; a < 3; a++) s->nc[a] = ncommon[a];
+        if (force2d == 0 && s->nc[2] == 1) force2d = 1;
+    } else {
+        int all2d = 1;
+        s->nc[0] = s->nc[1] = s->nc[2] = 1;
+        for (int m = 0; m < nmesh; m++) {
+            if (s->mn[m][2] != 1) all2d = 0;
+            for (int a = 0; a < 3; a++) if (s->nc[a] < s->mn[m][a]) s->nc[a] = s->mn[m][a];
+        }
+        if (all2d) s->nc[2] = 1;
+    }
+    if (force2d) s->nc[2] = 1;
+    s->force2d = force2d;
+    for (int a = 0; a < 3; a++) s->N[a] = s->nc[a] > 1 ? 2 * s->nc[a] : 1;
+    /* layers and the raw rect collection */
+    int L = 0;
+    for (int m = 0; m < nmesh; m++) L += (force2d == 2) ? s->mn[m][2] : 1;
+    s->L = L;
+    s->lay = (ml_layer *)calloc(L, sizeof(ml_layer));
+    int li = 0;
+    for (int m = 0; m < nmesh; m++) {
+        int nl = (force2d == 2) ? s->mn[m][2] : 1;
+        for (int q = 0; q < nl; q++, li++) {
+            rect3 r = s->mrect[m];
+            if (force2d == 2) {
+                double t = s->mh[m].z;
+                /* Rect::get_zlayer */
+                if (!(q * t < 0 || (q + 1) * t > (r.e.z - r.s.z))) { r.s.z = s->mrect[m].s.z + q * t; r.e.z = s->mrect[m].s.z + (q + 1) * t; }
+            }
+            s->lay[li].mesh = m;
+            s->lay[li].rect = r;
+        }
+    }
+    /* enlarge to common sizes */
+    d3 mx = d3m(0, 0, 0);
+    double minx = s->lay[0].rect.s.x, miny = s->lay[0].rect.s.y, minz = s->lay[0].rect.s.z;
+    for (int l = 0; l < L; l++) {
+        d3 sz = rsize(s->lay[l].rect);
+        if (mx.x < sz.x) mx.x = sz.x;
+        if (mx.y < sz.y) mx.y = sz.y;
+        if (mx.z < sz.z) mx.z = sz.z;
+        if (s->lay[l].rect.s.x < minx) minx = s->lay[l].rect.s.x;
+        if (s->lay[l].rect.s.y < miny) miny = s->lay[l].rect.s.y;
+        if (s->lay[l].rect.s.z < minz) minz = s->lay[l].rect.s.z;
+    }
+    for (int l = 0; l < L; l++) {
+        rect3 *r = &s->lay[l].rect;
+        if (r->e.x - mx.x < minx) { r->s.x = minx; r->e.x = r->s.x + mx.x; } else r->s.x = r->e.x - mx.x;
+        if (r->e.y - mx.y < miny) { r->s.y = miny; r->e.y = r->s.y + mx.y; } else r->s.y = r->e.y - mx.y;
+        if (s->nc[2] != 1) {
+            if (r->e.z - mx.z < minz) { r->s.z = minz; r->e.z = r->s.z + mx.z; } else r->s.z = r->e.z - mx.z;
+        }
+    }
+    s->h_max = 0.0;
+    for (int l = 0; l < L; l++) {
+        d3 h = s->mh[s->lay[l].mesh];
+        double hm = h.x > h.y ? h.x : h.y;
+        if (h.z > hm) hm = h.z;
+        if (s->h_max < hm) s->h_max = hm;
+    }
+    for (int l = 0; l < L; l++) {
+        ml_layer *y = &s->lay[l];
+        d3 sz = rsize(y->rect);
+        y->hc = d3m(sz.x / s->nc[0], sz.y / s->nc[1], sz.z / s->nc[2]);
+    }
+    /* kernels: dedup by (shift, h_src, h_dst); in 2D a kernel computed for the opposite z shift
+     * is reused with the xz, yz signs flipped */
+    s->ker = (ml_kernel *)calloc(L * L, sizeof(ml_kernel));
+    typedef struct { d3 shift, hs, hd; int computed; } kdesc;
+    kdesc *kd = (kdesc *)calloc(L * L, sizeof(kdesc));
+    int *slot = (int *)malloc(sizeof(int) * L * L);   /* per (dest, src): index into s->ker or -1 */
+    for (int i = 0; i < L * L; i++) slot[i] = -1;
+    for (int l = 0; l < L; l++) {
+        ml_layer *y = &s->lay[l];
+        y->kidx = (int *)calloc(L, sizeof(int));
+        y->kinv = (int *)calloc(L, sizeof(int));
+        y->kkind = (int *)calloc(L, sizeof(int));
+    }
+    for (int d = 0; d < L; d++) {
+        ml_layer *y = &s->lay[d];
+        for (int q = 0; q < L; q++) {
+            d3 shift = d3sub(y->rect.s, s->lay[q].rect.s);
+            d3 hsrc = s->lay[q].hc, hdst = y->hc;
+            int found = -1, inv = 0;
+            /* search every collection in order, each over its kernels in order */
+            for (int c2 = 0; c2 < L && found < 0; c2++)
+                for (int k2 = 0; k2 < L && found < 0; k2++) {
+                    int kk = slot[c2 * L + k2];
+                    if (kk < 0 || !kd[kk].computed) continue;
+                    if (!(d3eq(kd[kk].hs, hsrc) && d3eq(kd[kk].hd, hdst))) continue;
+                    if (d3eq(kd[kk].shift, shift)) found = kk;
+                    else if (s->N[2] == 1 && isz(shift.x) && isz(shift.y) && isz(kd[kk].shift.x) && isz(kd[kk].shift.y) &&
+                             isz(shift.z + kd[kk].shift.z)) found = kk;
+                }
+            int self = recteq(s->lay[q].rect, y->rect);
+            if (found >= 0) {
+                if (isz(shift.x) && isz(shift.y) && !isz(shift.z) && isz(shift.z + kd[found].shift.z)) inv = 1;
+                slot[d * L + q] = found;
+            } else {
+                int kk = s->nker++;
+                ml_kernel *K = &s->ker[kk];
+                if (self) {
+                    kd[kk].shift = d3m(0, 0, 0); kd[kk].hs = hdst; kd[kk].hd = hdst;
+                    K->type = 0;
+                    K->hs = K->hd = d3m(hdst.x / s->h_max, hdst.y / s->h_max, hdst.z / s->h_max);
+                    K->shift = d3m(0, 0, 0);
+                } else {
+                    kd[kk].shift = shift; kd[kk].hs = hsrc; kd[kk].hd = hdst;
+                    K->shift = d3m(shift.x / s->h_max, shift.y / s->h_max, shift.z / s->h_max);
+                    if (s->nc[2] == 1) {
+                        /* 2D: irregular unless s * 1e-9 == d * 1e-9 (DemagTFunc_Irregular.cpp:12) */
+                        d3 a = d3m(hsrc.x / s->h_max, hsrc.y / s->h_max, hsrc.z / s->h_max);
+                        d3 b = d3m(hdst.x / s->h_max, hdst.y / s->h_max, hdst.z / s->h_max);
+                        K->hs = a; K->hd = b;
+                        K->type = d3eq(d3m(a.x * 1e-9, a.y * 1e-9, a.z * 1e-9), d3m(b.x * 1e-9, b.y * 1e-9, b.z * 1e-9)) ? 0 : 1;
+                    } else {
+                        /* 3D uses the destination cellsize for both (DemagKernelCollection_Calc.cpp:921) */
+                        K->type = 0;
+                        K->hs = K->hd = d3m(hdst.x / s->h_max, hdst.y / s->h_max, hdst.z / s->h_max);
+                    }
+                }
+                kd[kk].computed = 1;
+                slot[d * L + q] = kk;
+                found = kk;
+            }
+            y->kidx[q] = found;
+            y->kinv[q] = inv;
+            if (self) y->kkind[q] = 1;
+            else if (isz(kd[found].shift.x) && isz(kd[found].shift.y) && !isz(kd[found].shift.z)) y->kkind[q] = inv ? 3 : 2;
+            else y->kkind[q] = recteq(s->lay[q].rect, y->rect) ? 1 : 4;
+        }
+    }
+    free(kd); free(slot);
+    for (int k = 0; k < s->nker; k++) ml_build_kernel(s, &s->ker[k]);
+    /* transfers */
+    size_t ncell = (size_t)s->nc[0] * s->nc[1] * s->nc[2];
+    for (int l = 0; l < L; l++) {
+        ml_layer *y = &s->lay[l];
+        int m = y->mesh;
+        y->transfer = !(recteq(y->rect, s->mrect[m]) && d3eq(y->hc, s->mh[m]));
+        if (!y->transfer) continue;
+        y->tin = (wlist *)calloc(ncell, sizeof(wlist));
+        for (size_t c = 0; c < ncell; c++) {
+            int ii = (int)(c % s->nc[0]), jj = (int)((c / s->nc[0]) % s->nc[1]), kk = (int)(c / ((size_t)s->nc[0] * s->nc[1]));
+            rect3 rc;
+            rc.s = d3add(y->rect.s, d3m(y->hc.x * ii, y->hc.y * jj, y->hc.z * kk));
+            rc.e = d3add(rc.s, y->hc);
+            rect3 ri;
+            double tot = 0.0, cov = 0.0;
+            if (rect_intersection(s->mrect[m], rc, &ri) && !rect_isplane(ri) && !rect_ispoint(ri)) {
+                d3 si = rsize(ri), sc = rsize(rc);
+                cov += (si.x / sc.x) * (si.y / sc.y) * (si.z / sc.z);
+                tot += recip_weights(&y->tin[c], rc, s->mn[m], s->mh[m], s->mrect[m].s);
+            }
+            if (tot > 0) for (int q = 0; q < y->tin[c].n; q++) y->tin[c].w[q] *= cov / tot;
+        }
+        size_t n = (size_t)s->mn[m][0] * s->mn[m][1] * s->mn[m][2];
+        y->tout = (wlist *)calloc(n, sizeof(wlist));
+        for (size_t c = 0; c < n; c++) {
+            int ii = (int)(c % s->mn[m][0]), jj = (int)((c / s->mn[m][0]) % s->mn[m][1]);
+            int kk = (int)(c / ((size_t)s->mn[m][0] * s->mn[m][1]));
+            rect3 rc;
+            rc.s = d3add(s->mrect[m].s, d3m(s->mh[m].x * ii, s->mh[m].y * jj, s->mh[m].z * kk));
+            rc.e = d3add(rc.s, s->mh[m]);
+            double tot = recip_weights(&y->tout[c], rc, s->nc, y->hc, y->rect.s);
+            if (tot > 0) for (int q = 0; q < y->tout[c].n; q++) y->tout[c].w[q] *= 1.0 / tot;
+        }
+    }
+    return s;
+}
+
+int orc_ml_info(orc_ml *s, int *L, int *nc3, int *layer_mesh, int *do_transfer, double *rects6, int *kinds)
+{
+    if (L) *L = s->L;
+    if (nc3) for (int a = 0; a < 3; a++) nc3[a] = s->nc[a];
+    for (int l = 0; l < s->L; l++) {
+        ml_layer *y = &s->lay[l];
+        if (layer_mesh) layer_mesh[l] = y->mesh;
+        if (do_transfer) do_transfer[l] = y->transfer;
+        if (rects6) {
+            rects6[6 * l] = y->rect.s.x; rects6[6 * l + 1] = y->rect.s.y; rects6[6 * l + 2] = y->rect.s.z;
+            rects6[6 * l + 3] = y->rect.e.x; rects6[6 * l + 4] = y->rect.e.y; rects6[6 * l + 5] = y->rect.e.z;
+        }
+        if (kinds) for (int q = 0; q < s->L; q++) kinds[l * s->L + q] = y->kkind[q];
+    }
+    return 0;
+}
+
+/* H_demag of every mesh (AoS, meshes concatenated) from M of every mesh */
+int orc_ml_eval(orc_ml *s, const double *M, double *H)
+{
+    const int Nx = s->N[0], Ny = s->N[1], Nz = s->N[2];
+    const int nx = s->nc[0], ny = s->nc[1], nz = s->nc[2];
+    const size_t np = (size_t)Nx * Ny * Nz, ncell = (size_t)nx * ny * nz;
+    const int L = s->L;
+    double **F = (double **)calloc(L, sizeof(double *));
+    double *tmp = (double *)malloc(sizeof(double) * 3 * ncell);
+    memset(H, 0, sizeof(double) * 3 * s->moff[s->nmesh]);
+    for (int l = 0; l < L; l++) {
+        ml_layer *y = &s->lay[l];
+        const double *Mm = M + 3 * s->moff[y->mesh];
+        if (y->transfer) {
+            for (size_t c = 0; c < ncell; c++) {
+                double v[3] = {0, 0, 0};
+                for (int q = 0; q < y->tin[c].n; q++)
+                    for (int a = 0; a < 3; a++) v[a] += Mm[3 * (size_t)y->tin[c].idx[q] + a] * y->tin[c].w[q];
+                for (int a = 0; a < 3; a++) tmp[3 * c + a] = v[a];
+            }
+        } else memcpy(tmp, Mm, sizeof(double) * 3 * ncell);
+        F[l] = (double *)calloc(3 * 2 * np, sizeof(double));
+        for (int a = 0; a < 3; a++) {
+            double *Fa = F[l] + 2 * a * np;
+            for (int k = 0; k < nz; k++)
+                for (int j = 0; j < ny; j++)
+                    for (int i = 0; i < nx; i++)
+                        Fa[2 * ((size_t)i + (size_t)j * Nx + (size_t)k * Nx * Ny)] = tmp[3 * ((size_t)i + (size_t)j * nx + (size_t)k * nx * ny) + a];
+            dft3(Fa, Nx, Ny, Nz, -1);
+        }
+    }
+    double *O = (double *)malloc(sizeof(double) * 3 * 2 * np);
+    static const int cmap[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+    for (int d = 0; d < L; d++) {
+        ml_layer *y = &s->lay[d];
+        memset(O, 0, sizeof(double) * 3 * 2 * np);
+        for (int q = 0; q < L; q++) {
+            const ml_kernel *K = &s->ker[y->kidx[q]];
+            const int inv = y->kinv[q];
+#pragma omp parallel for
+            for (long p = 0; p < (long)np; p++) {
+                for (int a = 0; a < 3; a++) {
+                    double re = 0.0, im = 0.0;
+                    for (int b = 0; b < 3; b++) {
+                        int c = cmap[a][b];
+                        double sg = (inv && (c == 4 || c == 5)) ? -1.0 : 1.0;
+                        double kr = sg * K->F[2 * (c * np + p)], ki = sg * K->F[2 * (c * np + p) + 1];
+                        double mr = F[q][2 * (b * np + p)], mi = F[q][2 * (b * np + p) + 1];
+                        re += kr * mr - ki * mi;
+                        im += kr * mi + ki * mr;
+                    }
+                    O[2 * (a * np + p)] += re;
+                    O[2 * (a * np + p) + 1] += im;
+                }
+            }
+        }
+        for (int a = 0; a < 3; a++) {
+            double *Oa = O + 2 * a * np;
+            dft3(Oa, Nx, Ny, Nz, +1);
+            for (size_t c = 0; c < ncell; c++) {
+                int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+                tmp[3 * c + a] = Oa[2 * ((size_t)i + (size_t)j * Nx + (size_t)k * Nx * Ny)] / (double)np;
+            }
+        }
+        double *Hm = H + 3 * s->moff[y->mesh];
+        size_t n = s->moff[y->mesh + 1] - s->moff[y->mesh];
+        if (y->transfer) {
+            for (size_t c = 0; c < n; c++)
+                for (int q = 0; q < y->tout[c].n; q++)
+                    for (int a = 0; a < 3; a++) Hm[3 * c + a] += tmp[3 * (size_t)y->tout[c].idx[q] + a] * y->tout[c].w[q];
+        } else {
+            for (size_t c = 0; c < 3 * n; c++) Hm[c] += tmp[c];
+        }
+    }
+    for (int l = 0; l < L; l++) free(F[l]);
+    free(F); free(tmp); free(O);
+    return 0;
+}
+
+/* the transfer of one layer alone (tests): Mc = transfer_in(M), Hmesh = transfer_out(Hc) */
+int orc_ml_transfer(orc_ml *s, int l, const double *M, double *Mc, const double *Hc, double *Hmesh)
+{
+    if (l < 0 || l >= s->L || !s->lay[l].transfer) return 1;
+    ml_layer *y = &s->lay[l];
+    const double *Mm = M + 3 * s->moff[y->mesh];
+    size_t ncell = (size_t)s->nc[0] * s->nc[1] * s->nc[2];
+    for (size_t c = 0; c < ncell; c++) {
+        double v[3] = {0, 0, 0};
+        for (int q = 0; q < y->tin[c].n; q++)
+            for (int a = 0; a < 3; a++) v[a] += Mm[3 * (size_t)y->tin[c].idx[q] + a] * y->tin[c].w[q];
+        for (int a = 0; a < 3; a++) Mc[3 * c + a] = v[a];
+    }
+    size_t n = s->moff[y->mesh + 1] - s->moff[y->mesh];
+    for (size_t c = 0; c < n; c++) {
+        double v[3] = {0, 0, 0};
+        for (int q = 0; q < y->tout[c].n; q++)
+            for (int a = 0; a < 3; a++) v[a] += Hc[3 * (size_t)y->tout[c].idx[q] + a] * y->tout[c].w[q];
+        for (int a = 0; a < 3; a++) Hmesh[3 * c + a] = v[a];
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------ field terms */
 
 static double ms_at(const double *Ms_cell, size_t i) { return Ms_cell[i]; }
@@ -515,6 +1036,10 @@ typedef struct {
 struct orc_solver {
     int nmesh;
     orc_mesh *m;
+    orc_ml *ml;          /* multilayered convolution over the meshes with demag, or NULL */
+    int *ml_mesh;        /* solver mesh of each multilayer mesh */
+    int ml_nmesh;
+    double *ml_M, *ml_H; /* concatenated M and H_demag of the multilayer meshes */
     int eval;
     double dT, tol, dT_incr, dT_min, dT_max;
     double time, stagetime;
@@ -555,9 +1080,39 @@ orc_solver *orc_solver_create(int nmesh, const orc_mesh_desc *desc, int eval, do
     return s;
 }
 
+/* Replace the per-mesh demag of every mesh with ORC_DEMAG by one multilayered convolution
+ * (SDemag in multilayer mode); origins give the meshes' positions. */
+int orc_solver_set_multilayer(orc_solver *s, const double *o3, int mode, const int *ncommon)
+{
+    int cnt = 0;
+    for (int q = 0; q < s->nmesh; q++) if (s->m[q].d.modules & ORC_DEMAG) cnt++;
+    if (!cnt) return 1;
+    int *n3 = (int *)malloc(sizeof(int) * 3 * cnt);
+    double *h3 = (double *)malloc(sizeof(double) * 3 * cnt), *oo = (double *)malloc(sizeof(double) * 3 * cnt);
+    s->ml_mesh = (int *)malloc(sizeof(int) * cnt);
+    size_t tot = 0;
+    int k = 0;
+    for (int q = 0; q < s->nmesh; q++) {
+        const orc_mesh_desc *d = &s->m[q].d;
+        if (!(d->modules & ORC_DEMAG)) continue;
+        n3[3 * k] = d->nx; n3[3 * k + 1] = d->ny; n3[3 * k + 2] = d->nz;
+        h3[3 * k] = d->hx; h3[3 * k + 1] = d->hy; h3[3 * k + 2] = d->hz;
+        for (int a = 0; a < 3; a++) oo[3 * k + a] = o3[3 * q + a];
+        s->ml_mesh[k++] = q;
+        tot += (size_t)s->m[q].n;
+    }
+    s->ml_nmesh = cnt;
+    s->ml = orc_ml_create(cnt, n3, h3, oo, mode, ncommon);
+    s->ml_M = (double *)calloc(3 * tot, sizeof(double));
+    s->ml_H = (double *)calloc(3 * tot, sizeof(double));
+    free(n3); free(h3); free(oo);
+    return s->ml ? 0 : 2;
+}
+
 void orc_solver_destroy(orc_solver *s)
 {
     if (!s) return;
+    if (s->ml) { orc_ml_destroy(s->ml); free(s->ml_mesh); free(s->ml_M); free(s->ml_H); }
     for (int q = 0; q < s->nmesh; q++) {
         orc_mesh *m = &s->m[q];
         free(m->Ms); free(m->K1); free(m->M); free(m->H); free(m->sM1);
@@ -596,6 +1151,18 @@ static void applied_field(const orc_mesh_desc *d, double t, double *Ha)
 
 /* module order Zeeman (sets) -> Demag -> Exchange/iDMI -> Anisotropy (MeshModules.cpp:131,
  * Mesh_Ferromagnetic.h:152) */
+/* multilayered convolution of all multilayer meshes into s->ml_H */
+static void update_ml(orc_solver *s)
+{
+    size_t off = 0;
+    for (int k = 0; k < s->ml_nmesh; k++) {
+        orc_mesh *m = &s->m[s->ml_mesh[k]];
+        memcpy(s->ml_M + 3 * off, m->M, sizeof(double) * 3 * m->n);
+        off += (size_t)m->n;
+    }
+    orc_ml_eval(s->ml, s->ml_M, s->ml_H);
+}
+
 static void update_fields(orc_solver *s, orc_mesh *m)
 {
     const orc_mesh_desc *d = &m->d;
@@ -603,7 +1170,14 @@ static void update_fields(orc_solver *s, orc_mesh *m)
     double Ha[3];
     applied_field(d, s->stagetime, Ha);
     for (size_t i = 0; i < n; i++) { m->H[3 * i] = Ha[0]; m->H[3 * i + 1] = Ha[1]; m->H[3 * i + 2] = Ha[2]; }
-    if (d->modules & ORC_DEMAG) orc_demag_apply(m->dm, m->M, m->H, 1);
+    if ((d->modules & ORC_DEMAG) && s->ml) {
+        size_t off = 0;
+        for (int k = 0; k < s->ml_nmesh; k++) {
+            orc_mesh *mk = &s->m[s->ml_mesh[k]];
+            if (mk == m) { for (size_t i = 0; i < 3 * n; i++) m->H[i] += s->ml_H[3 * off + i]; break; }
+            off += (size_t)mk->n;
+        }
+    } else if (d->modules & ORC_DEMAG) orc_demag_apply(m->dm, m->M, m->H, 1);
     if (d->modules & ORC_IDMI) orc_field_idmi(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, m->M, d->A, d->D, m->Ms, m->H);
     else if (d->modules & ORC_EXCH) orc_field_exchange(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, m->M, d->A, m->Ms, m->H);
     if (d->modules & ORC_ANIUNI) orc_field_aniuni(m->n, m->M, m->Ms, m->K1, d->K2, d->ea, m->H);
@@ -611,12 +1185,14 @@ static void update_fields(orc_solver *s, orc_mesh *m)
 
 static void update_all_fields(orc_solver *s)
 {
+    if (s->ml) update_ml(s);
     for (int q = 0; q < s->nmesh; q++) update_fields(s, &s->m[q]);
     s->evals++;
 }
 
 int orc_compute_heff(orc_solver *s, int q, double *H)
 {
+    if (s->ml) update_ml(s);
     update_fields(s, &s->m[q]);
     memcpy(H, s->m[q].H, sizeof(double) * 3 * s->m[q].n);
     return 0;

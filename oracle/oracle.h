@@ -67,6 +67,7 @@ typedef struct {
     double time, dT, last_lte;
 } orc_stats;
 
+typedef struct orc_ml orc_ml;
 typedef struct orc_solver orc_solver;
 #define ORC_RK4 0
 #define ORC_RKDP54 1
@@ -74,11 +75,28 @@ orc_solver *orc_solver_create(int nmesh, const orc_mesh_desc *desc, int eval, do
                               double dT_incr, double dT_min, double dT_max);
 int orc_set_m(orc_solver *s, int mesh, const double *M);
 int orc_get_m(orc_solver *s, int mesh, double *M);
+/* one multilayered convolution (orc_ml, below) replaces the per-mesh demag of every mesh with
+ * ORC_DEMAG; o3 = origin of every solver mesh (3 per mesh) */
+int orc_solver_set_multilayer(orc_solver *s, const double *o3, int mode, const int *ncommon);
 /* effective field at the current M and time; H has 3n doubles */
 int orc_compute_heff(orc_solver *s, int mesh, double *H);
 /* advance until `steps` more steps are accepted */
 int orc_run(orc_solver *s, int steps, orc_stats *st);
 void orc_solver_destroy(orc_solver *s);
+
+/* ---- multilayered convolution (SDemag multilayer mode) ----
+ * meshes: n3, h3 (cellsize), o3 (origin), 3 per mesh; mode 0: 3D (2D when every mesh is one cell
+ * thick or ncommon[2] == 1), 1: 2D, 2: 2D with every z cell layer its own layer; ncommon: NULL for
+ * the largest n of the meshes per axis. */
+orc_ml *orc_ml_create(int nmesh, const int *n3, const double *h3, const double *o3, int mode, const int *ncommon);
+/* layer count, n_common, per layer: mesh, transfer flag, rect (s, e), kernel kind per source
+ * (1 self, 2 z-shifted, 3 inverse z-shifted, 4 full complex) */
+int orc_ml_info(orc_ml *s, int *L, int *nc3, int *layer_mesh, int *do_transfer, double *rects6, int *kinds);
+/* H_demag of every mesh (AoS, meshes concatenated in order) from M of every mesh */
+int orc_ml_eval(orc_ml *s, const double *M, double *H);
+/* one layer's mesh transfer alone: Mc = transfer in of M, Hmesh = transfer out of Hc */
+int orc_ml_transfer(orc_ml *s, int layer, const double *M, double *Mc, const double *Hc, double *Hmesh);
+void orc_ml_destroy(orc_ml *s);
 
 /* FP64 in-place complex DFT (fftw_shim.c) */
 void bm_oracle_fft(int n, double *data, int sign);

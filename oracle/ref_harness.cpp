@@ -15,11 +15,18 @@
  *   ref_idmi           VEC_VC<DBL3>::delsq_nneu/grad_nneu/grad_neu (BorisLib/VEC_VC_Del.h:141,
  *                      BorisLib/VEC_VC_Grad.h:10,139) with the field formula of
  *                      iDMExchange::UpdateField (Boris/iDMExchange.cpp:97)
+ *   ref_tensor_shifted DemagTFunc::Calc{Diag,OffDiag}Tens3D_Shifted (Boris/DemagTFunc_Shifted.cpp:6,...)
+ *                      and Calc{Diag,OffDiag}Tens2D_Shifted_Irregular (Boris/DemagTFunc_Irregular.cpp:4,121)
+ *   ref_ml_*           the multilayered convolution: one Convolution<., DemagKernelCollection> per
+ *                      layer with the rectangle rules of SDemag (Boris/SDemag.cpp:173,215,441), the
+ *                      weighted mesh transfer of SDemag_Demag (Boris/SDemag_Demag.cpp:64,349) and the
+ *                      evaluation order of SDemag::UpdateField (Boris/SDemag.cpp:786-900)
  * All arrays are AoS (x,y,z per cell), cells ordered x fastest, then y, then z.
  */
 #include "stdafx.h"
 #include "DemagTFunc.h"
 #include "DemagKernel.h"
+#include "DemagKernelCollection.h"
 #include "Convolution.h"
 
 #include <vector>
@@ -34,6 +41,27 @@ struct OracleDemag : public Convolution<OracleDemag, DemagKernel> {
     SZ3 get_n(void) const { return n; }
     bool create_failed(void) { return (bool)Convolution_Error_on_Create(); }
     double convolute(VEC<DBL3> &In, VEC<DBL3> &Out) { return Convolute(In, Out, true); }
+};
+
+/* one layer of the multilayered convolution (the Convolution part of SDemag_Demag) */
+struct OracleMLConv : public Convolution<OracleMLConv, DemagKernelCollection> {
+    OracleMLConv() : Convolution<OracleMLConv, DemagKernelCollection>() {}
+    BError setdims(SZ3 n_, DBL3 h_) { return SetDimensions(n_, h_, false); }
+    BError setrects(std::vector<Rect> &rc, Rect r, double hmax, int idx) { return Set_Rect_Collection(rc, r, hmax, idx); }
+    BError calc(std::vector<DemagKernelCollection *> &kc) { return Calculate_Demag_Kernels(kc); }
+    VEC<ReIm3> *in_space(void) { return Get_Input_Scratch_Space(); }
+    void fwd(VEC<DBL3> &In) { ForwardFFT(In); }
+    void mult(std::vector<VEC<ReIm3> *> &F) { KernelMultiplication_MultipleInputs(F); }
+    double inv(VEC<DBL3> &In, VEC<DBL3> &Out, bool clear) { return InverseFFT(In, Out, clear); }
+    SZ3 get_N(void) const { return N; }
+    int kernel_kind(int idx)
+    {
+        std::shared_ptr<KerType> k = Get_Kernel(idx);
+        if (!k) return -1;
+        if (k->zshifted) return is_inverse_shifted(idx) ? 3 : 2;
+        if (k->Kdiag_cmpl.linear_size()) return 4;
+        return 1;
+    }
 };
 
 }
@@ -196,6 +224,250 @@ int ref_idmi(int nx, int ny, int nz, double hx, double hy, double hz, const doub
         DBL3 Ht = HA + HD;
         H[3 * idx] = Ht.x; H[3 * idx + 1] = Ht.y; H[3 * idx + 2] = Ht.z;
     }
+    return 0;
+}
+
+
+/* Shifted real-space tensors D = -N on the N grid (AoS, 3 doubles per point).
+ * kind 0: Calc{Diag,OffDiag}Tens3D_Shifted(n, N, hs, shift)
+ * kind 1: Calc{Diag,OffDiag}Tens2D_Shifted_Irregular(n, N, s = hs, d = hd, shift)
+ * Cellsizes and shift are given already normalised (the reference divides them by h_max).
+ * asympt is the asymptotic distance in cells (40 is the reference value; 0 uses the exact
+ * Newell sums everywhere). */
+int ref_tensor_shifted(int kind, int nx, int ny, int nz, int Nx, int Ny, int Nz, const double *hs, const double *hd,
+                       const double *shift, int asympt, double *diag, double *odiag)
+{
+    DemagTFunc dtf;
+    VEC<DBL3> D;
+    INT3 n(nx, ny, nz), N(Nx, Ny, Nz);
+    if (!D.resize(SZ3(Nx, Ny, Nz))) return 1;
+    size_t np = (size_t)Nx * Ny * Nz;
+    DBL3 s(hs[0], hs[1], hs[2]), d(hd[0], hd[1], hd[2]), sh(shift[0], shift[1], shift[2]);
+    if (kind == 0) {
+        if (!dtf.CalcDiagTens3D_Shifted(D, n, N, s, sh, true, asympt)) return 2;
+        memcpy(diag, D.data(), sizeof(double) * 3 * np);
+        if (!dtf.CalcOffDiagTens3D_Shifted(D, n, N, s, sh, true, asympt)) return 3;
+        memcpy(odiag, D.data(), sizeof(double) * 3 * np);
+    }
+    else {
+        if (!dtf.CalcDiagTens2D_Shifted_Irregular(D, n, N, s, d, sh, true, asympt)) return 2;
+        memcpy(diag, D.data(), sizeof(double) * 3 * np);
+        if (!dtf.CalcOffDiagTens2D_Shifted_Irregular(D, n, N, s, d, sh, true, asympt)) return 3;
+        memcpy(odiag, D.data(), sizeof(double) * 3 * np);
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------- multilayered convolution
+ * Meshes are given by n, h and origin o (rect = [o, o + n h]); all are ferromagnetic with
+ * demag. force2d follows SDemag::force_2d_convolution (0: 3D unless every mesh is one cell
+ * thick, 1: 2D with each mesh one layer, 2: 2D with every z cell layer its own layer);
+ * ncommon (optional) is the user's n_common (Set_n_common, SDemag.cpp:362); n_common.z is 1
+ * whenever a 2D mode is on (Set_2D_Multilayered_Convolution, SDemag.cpp:341). */
+struct ref_ml_s {
+    int nmesh = 0, L = 0;
+    std::vector<VEC<DBL3> *> M, Heff;
+    std::vector<OracleMLConv *> conv;
+    std::vector<VEC<DBL3> *> transfer;
+    std::vector<int> layer_mesh;
+    std::vector<int> do_transfer;
+    std::vector<Rect> rects;
+    std::vector<VEC<ReIm3> *> F;
+    std::vector<DemagKernelCollection *> kc;
+    SZ3 n_common;
+    double h_max = 0.0;
+};
+
+void ref_ml_destroy(void *hp)
+{
+    ref_ml_s *s = (ref_ml_s *)hp;
+    if (!s) return;
+    for (auto p : s->conv) delete p;
+    for (auto p : s->transfer) delete p;
+    for (auto p : s->M) delete p;
+    for (auto p : s->Heff) delete p;
+    delete s;
+}
+
+void *ref_ml_create(int nmesh, const int *n3, const double *h3, const double *o3, int force2d, const int *ncommon)
+{
+    ref_ml_s *s = new ref_ml_s();
+    s->nmesh = nmesh;
+    std::vector<Rect> mrect(nmesh);
+    std::vector<DBL3> mh(nmesh);
+    std::vector<INT3> mn(nmesh);
+    for (int m = 0; m < nmesh; m++) {
+        mn[m] = INT3(n3[3 * m], n3[3 * m + 1], n3[3 * m + 2]);
+        mh[m] = DBL3(h3[3 * m], h3[3 * m + 1], h3[3 * m + 2]);
+        DBL3 o(o3[3 * m], o3[3 * m + 1], o3[3 * m + 2]);
+        mrect[m] = Rect(o, o + (mh[m] & DBL3(mn[m].x, mn[m].y, mn[m].z)));
+        VEC<DBL3> *M = new VEC<DBL3>(), *H = new VEC<DBL3>();
+        M->resize(mh[m], mrect[m]);
+        H->resize(mh[m], mrect[m]);
+        s->M.push_back(M);
+        s->Heff.push_back(H);
+    }
+    // n_common (SDemag::set_default_n_common, SDemag.cpp:173; Set_n_common, :362)
+    SZ3 nc(1, 1, 1);
+    if (ncommon) {
+        nc = SZ3(ncommon[0], ncommon[1], ncommon[2]);
+        if (force2d == 0 && nc.z == 1) force2d = 1;
+    }
+    else {
+        bool all2d = true;
+        for (int m = 0; m < nmesh; m++) if (mn[m].z != 1) all2d = false;
+        for (int m = 0; m < nmesh; m++) {
+            if (nc.x < mn[m].x) nc.x = mn[m].x;
+            if (nc.y < mn[m].y) nc.y = mn[m].y;
+            if (nc.z < mn[m].z) nc.z = mn[m].z;
+        }
+        if (all2d || force2d) nc.z = 1;
+    }
+    if (force2d) nc.z = 1;
+    s->n_common = nc;
+    // layers and the raw rectangle collection (SDemag::set_Rect_collection, SDemag.cpp:215)
+    std::vector<Rect> rc;
+    for (int m = 0; m < nmesh; m++) {
+        int nl = (force2d == 2) ? mn[m].z : 1;
+        for (int l = 0; l < nl; l++) {
+            rc.push_back(force2d == 2 ? mrect[m].get_zlayer(l, mh[m].z) : mrect[m]);
+            s->layer_mesh.push_back(m);
+        }
+    }
+    DBL3 max_sizes;
+    double min_x = rc[0].s.x, min_y = rc[0].s.y, min_z = rc[0].s.z;
+    for (size_t i = 0; i < rc.size(); i++) {
+        if (max_sizes.x < rc[i].size().x) max_sizes.x = rc[i].size().x;
+        if (max_sizes.y < rc[i].size().y) max_sizes.y = rc[i].size().y;
+        if (max_sizes.z < rc[i].size().z) max_sizes.z = rc[i].size().z;
+        if (rc[i].s.x < min_x) min_x = rc[i].s.x;
+        if (rc[i].s.y < min_y) min_y = rc[i].s.y;
+        if (rc[i].s.z < min_z) min_z = rc[i].s.z;
+    }
+    for (size_t i = 0; i < rc.size(); i++) {
+        if (rc[i].e.x - max_sizes.x < min_x) { rc[i].s.x = min_x; rc[i].e.x = rc[i].s.x + max_sizes.x; }
+        else rc[i].s.x = rc[i].e.x - max_sizes.x;
+        if (rc[i].e.y - max_sizes.y < min_y) { rc[i].s.y = min_y; rc[i].e.y = rc[i].s.y + max_sizes.y; }
+        else rc[i].s.y = rc[i].e.y - max_sizes.y;
+        if (nc.z != 1) {
+            if (rc[i].e.z - max_sizes.z < min_z) { rc[i].s.z = min_z; rc[i].e.z = rc[i].s.z + max_sizes.z; }
+            else rc[i].s.z = rc[i].e.z - max_sizes.z;
+        }
+    }
+    s->rects = rc;
+    s->L = (int)rc.size();
+    // h_max over the meshes' own cellsizes (SDemag::get_maximum_cellsize, SDemag.cpp:297)
+    for (int i = 0; i < s->L; i++) {
+        double hm = mh[s->layer_mesh[i]].maxdim();
+        if (s->h_max < hm) s->h_max = hm;
+    }
+    // convolution objects (SDemag::Initialize, SDemag.cpp:456-486)
+    for (int i = 0; i < s->L; i++) {
+        OracleMLConv *c = new OracleMLConv();
+        DBL3 hconv = rc[i] / nc;
+        if (c->setdims(nc, hconv)) { s->conv.push_back(c); ref_ml_destroy(s); return nullptr; }
+        s->conv.push_back(c);
+    }
+    for (int i = 0; i < s->L; i++) {
+        if (s->conv[i]->setrects(rc, rc[i], s->h_max, i)) { ref_ml_destroy(s); return nullptr; }
+        s->kc.push_back(s->conv[i]);
+        s->F.push_back(s->conv[i]->in_space());
+    }
+    // kernels and transfers (SDemag_Demag::Initialize, SDemag_Demag.cpp:306-366)
+    for (int i = 0; i < s->L; i++) {
+        if (s->conv[i]->calc(s->kc)) { ref_ml_destroy(s); return nullptr; }
+        int m = s->layer_mesh[i];
+        DBL3 hconv = rc[i] / nc;
+        VEC<DBL3> *t = new VEC<DBL3>();
+        s->transfer.push_back(t);
+        if (rc[i] == mrect[m] && hconv == mh[m]) s->do_transfer.push_back(0);
+        else {
+            s->do_transfer.push_back(1);
+            if (!t->resize(hconv, rc[i])) { ref_ml_destroy(s); return nullptr; }
+            if (!t->Initialize_MeshTransfer({s->M[m]}, {s->Heff[m]}, MESHTRANSFERTYPE_WEIGHTED)) { ref_ml_destroy(s); return nullptr; }
+        }
+    }
+    return s;
+}
+
+/* layer count, n_common, and per layer: mesh, transfer flag, rect (s, e), kernel kinds per
+ * source (1 self/regular real, 2 z-shifted, 3 inverse z-shifted, 4 complex full) */
+int ref_ml_info(void *hp, int *L, int *nc3, int *layer_mesh, int *do_transfer, double *rects6, int *kinds)
+{
+    ref_ml_s *s = (ref_ml_s *)hp;
+    if (L) *L = s->L;
+    if (nc3) { nc3[0] = s->n_common.x; nc3[1] = s->n_common.y; nc3[2] = s->n_common.z; }
+    for (int i = 0; i < s->L; i++) {
+        if (layer_mesh) layer_mesh[i] = s->layer_mesh[i];
+        if (do_transfer) do_transfer[i] = s->do_transfer[i];
+        if (rects6) {
+            rects6[6 * i + 0] = s->rects[i].s.x; rects6[6 * i + 1] = s->rects[i].s.y; rects6[6 * i + 2] = s->rects[i].s.z;
+            rects6[6 * i + 3] = s->rects[i].e.x; rects6[6 * i + 4] = s->rects[i].e.y; rects6[6 * i + 5] = s->rects[i].e.z;
+        }
+        if (kinds) for (int j = 0; j < s->L; j++) kinds[i * s->L + j] = s->conv[i]->kernel_kind(j);
+    }
+    return 0;
+}
+
+/* H_demag of every mesh from M of every mesh (AoS, meshes concatenated in order), as
+ * SDemag::UpdateField computes it in multilayered mode (no evaluation speedup). */
+int ref_ml_eval(void *hp, const double *M, double *H)
+{
+    ref_ml_s *s = (ref_ml_s *)hp;
+    size_t off = 0;
+    for (int m = 0; m < s->nmesh; m++) {
+        size_t n = s->M[m]->linear_size();
+        memcpy(s->M[m]->data(), M + 3 * off, sizeof(double) * 3 * n);
+        s->Heff[m]->set(DBL3());
+        off += n;
+    }
+    for (int i = 0; i < s->L; i++) {
+        int m = s->layer_mesh[i];
+        if (s->do_transfer[i]) {
+            s->transfer[i]->transfer_in();
+            s->conv[i]->fwd(*s->transfer[i]);
+        }
+        else s->conv[i]->fwd(*s->M[m]);
+    }
+    for (int i = s->L - 1; i >= 0; i--) s->conv[i]->mult(s->F);
+    for (int i = 0; i < s->L; i++) {
+        int m = s->layer_mesh[i];
+        if (s->do_transfer[i]) {
+            s->conv[i]->inv(*s->transfer[i], *s->transfer[i], true);
+            s->transfer[i]->transfer_out();
+        }
+        else s->conv[i]->inv(*s->M[m], *s->Heff[m], false);
+    }
+    off = 0;
+    for (int m = 0; m < s->nmesh; m++) {
+        size_t n = s->Heff[m]->linear_size();
+        memcpy(H + 3 * off, s->Heff[m]->data(), sizeof(double) * 3 * n);
+        off += n;
+    }
+    return 0;
+}
+
+/* transfer only (tests of the mesh-transfer rules): for layer i, the common-grid input
+ * transfer_in() builds from M (AoS, all meshes), and the mesh H that transfer_out() adds from
+ * a given common-grid field Hc. */
+int ref_ml_transfer(void *hp, int layer, const double *M, double *Mc, const double *Hc, double *Hmesh)
+{
+    ref_ml_s *s = (ref_ml_s *)hp;
+    if (layer < 0 || layer >= s->L || !s->do_transfer[layer]) return 1;
+    size_t off = 0;
+    for (int m = 0; m < s->nmesh; m++) {
+        size_t n = s->M[m]->linear_size();
+        memcpy(s->M[m]->data(), M + 3 * off, sizeof(double) * 3 * n);
+        s->Heff[m]->set(DBL3());
+        off += n;
+    }
+    VEC<DBL3> &t = *s->transfer[layer];
+    t.transfer_in();
+    memcpy(Mc, t.data(), sizeof(double) * 3 * t.linear_size());
+    memcpy(t.data(), Hc, sizeof(double) * 3 * t.linear_size());
+    t.transfer_out();
+    int m = s->layer_mesh[layer];
+    memcpy(Hmesh, s->Heff[m]->data(), sizeof(double) * 3 * s->Heff[m]->linear_size());
     return 0;
 }
 

@@ -22,6 +22,7 @@ P = ctypes.c_void_p
 D = ctypes.c_double
 I = ctypes.c_int
 DP = ctypes.POINTER(ctypes.c_double)
+IP = ctypes.POINTER(ctypes.c_int)
 
 _orc = None
 _ref = None
@@ -73,6 +74,13 @@ def oracle():
         L.orc_field_idmi.argtypes = [I, I, I, D, D, D, DP, D, D, DP, DP]
         L.orc_field_aniuni.argtypes = [I, DP, DP, DP, D, DP, DP]
         L.bm_oracle_fft.argtypes = [I, DP, I]
+        L.orc_ml_create.restype = P
+        L.orc_ml_create.argtypes = [I, IP, DP, DP, I, IP]
+        L.orc_ml_info.argtypes = [P, IP, IP, IP, IP, DP, IP]
+        L.orc_ml_eval.argtypes = [P, DP, DP]
+        L.orc_ml_transfer.argtypes = [P, I, DP, DP, DP, DP]
+        L.orc_ml_destroy.argtypes = [P]
+        L.orc_solver_set_multilayer.argtypes = [P, DP, I, IP]
         _orc = L
     return _orc
 
@@ -101,6 +109,13 @@ def reference():
         L.ref_demag_destroy.argtypes = [P]
         L.ref_exchange.argtypes = [I, I, I, D, D, D, DP, DP, DP, DP]
         L.ref_idmi.argtypes = [I, I, I, D, D, D, DP, DP, DP, DP, DP]
+        L.ref_tensor_shifted.argtypes = [I, I, I, I, I, I, I, DP, DP, DP, I, DP, DP]
+        L.ref_ml_create.restype = P
+        L.ref_ml_create.argtypes = [I, IP, DP, DP, I, IP]
+        L.ref_ml_info.argtypes = [P, IP, IP, IP, IP, DP, IP]
+        L.ref_ml_eval.argtypes = [P, DP, DP]
+        L.ref_ml_transfer.argtypes = [P, I, DP, DP, DP, DP]
+        L.ref_ml_destroy.argtypes = [P]
         _ref = L
     return _ref
 
@@ -118,6 +133,65 @@ def orc_hdemag(M, n, h, N=None):
     dot = L.orc_demag_apply(P(d), dp(Mf), dp(H), 0)
     L.orc_demag_destroy(P(d))
     return H.reshape(-1, 3), dot
+
+
+def ip(a):
+    return a.ctypes.data_as(IP)
+
+
+class MultiLayer:
+    """The multilayered convolution of the oracle (which="oracle") or of the reference build
+    (which="reference"). meshes: list of (n, h, origin); mode 0 3D, 1 2D, 2 2D-layered."""
+
+    def __init__(self, meshes, mode=0, ncommon=None, which="oracle"):
+        self.lib = oracle() if which == "oracle" else reference()
+        self.pre = "orc_" if which == "oracle" else "ref_"
+        self.meshes = meshes
+        n3 = np.array([m[0] for m in meshes], dtype=np.int32).reshape(-1)
+        h3 = np.array([m[1] for m in meshes], dtype=np.float64).reshape(-1)
+        o3 = np.array([m[2] for m in meshes], dtype=np.float64).reshape(-1)
+        self._nc = np.array(ncommon, dtype=np.int32) if ncommon is not None else None
+        self.h = getattr(self.lib, self.pre + "ml_create")(len(meshes), ip(n3), dp(h3), dp(o3), mode,
+                                                          ip(self._nc) if self._nc is not None else None)
+        assert self.h
+        self.ncell = [int(np.prod(m[0])) for m in meshes]
+
+    def info(self):
+        L = np.zeros(1, np.int32)
+        nc = np.zeros(3, np.int32)
+        lm = np.zeros(256, np.int32)
+        tr = np.zeros(256, np.int32)
+        rc = np.zeros(256 * 6)
+        kk = np.zeros(256 * 256, np.int32)
+        getattr(self.lib, self.pre + "ml_info")(P(self.h), ip(L), ip(nc), ip(lm), ip(tr), dp(rc), ip(kk))
+        n = int(L[0])
+        return {"L": n, "n_common": tuple(int(v) for v in nc), "layer_mesh": lm[:n].tolist(),
+                "transfer": tr[:n].tolist(), "rects": rc[:6 * n].reshape(n, 6).copy(),
+                "kinds": kk[:n * n].reshape(n, n).copy()}
+
+    def eval(self, M):
+        Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+        H = np.zeros_like(Mf)
+        getattr(self.lib, self.pre + "ml_eval")(P(self.h), dp(Mf), dp(H))
+        return H.reshape(-1, 3)
+
+    def transfer(self, layer, M, Hc, ncommon_cells):
+        Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+        Hcf = np.ascontiguousarray(np.asarray(Hc, dtype=np.float64).reshape(-1))
+        Mc = np.zeros(3 * ncommon_cells)
+        m = self.info()["layer_mesh"][layer]
+        Hm = np.zeros(3 * self.ncell[m])
+        rc = getattr(self.lib, self.pre + "ml_transfer")(P(self.h), layer, dp(Mf), dp(Mc), dp(Hcf), dp(Hm))
+        assert rc == 0
+        return Mc.reshape(-1, 3), Hm.reshape(-1, 3)
+
+    def close(self):
+        if self.h:
+            getattr(self.lib, self.pre + "ml_destroy")(P(self.h))
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def ref_hdemag(M, n, h):
@@ -161,6 +235,14 @@ class OracleSolver:
         self._arr = arr
         self.n = [m["n"][0] * m["n"][1] * m["n"][2] for m in meshes]
         self.h = oracle().orc_solver_create(len(meshes), arr, evaluation, dt, tol, dT_incr, dT_min, dT_max)
+
+    def multilayer(self, origins, mode=0, ncommon=None):
+        """Demag of all meshes with the demag bit as one multilayered convolution."""
+        o3 = np.ascontiguousarray(np.asarray(origins, dtype=np.float64).reshape(-1))
+        nc = np.array(ncommon, dtype=np.int32) if ncommon is not None else None
+        self._keep += [o3, nc]
+        rc = oracle().orc_solver_set_multilayer(P(self.h), dp(o3), mode, ip(nc) if nc is not None else None)
+        assert rc == 0
 
     def set_m(self, M, mesh=0):
         a = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
