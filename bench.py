@@ -40,8 +40,33 @@ CONFIGS = {
                           init="sphere"),
     "film2d_256x256": dict(n=(256, 256, 1), h=(4e-9, 4e-9, 3e-9), Ms=8e5, A=1.3e-11, K1=1e5, D=0.0, alpha=0.02,
                            modules=1 | 2 | 8 | 16, Ha=(0, 0, 0), eval="RK4", dt=1e-13, init="sphere"),
+    # three stacked meshes with different cellsizes, 1 nm spacers, one multilayered convolution
+    # (3D common grid n = (1024, 1024, 2), FFT 2048 x 2048 x 4)
+    "multilayer_stack3": dict(meshes=[dict(n=(1024, 1024, 1), h=(2e-9, 2e-9, 1e-9), o=(0, 0, 0), Ms=1.4e6, K1=0.0,
+                                           modules=1 | 2),
+                                      dict(n=(512, 512, 2), h=(4e-9, 4e-9, 2e-9), o=(0, 0, 2e-9), Ms=6e5, K1=0.0,
+                                           modules=1 | 2),
+                                      dict(n=(1024, 1024, 1), h=(2e-9, 2e-9, 1.5e-9), o=(0, 0, 7e-9), Ms=1.1e6,
+                                           K1=3e5, modules=1 | 2 | 8)],
+                              A=1.5e-11, D=0.0, alpha=0.05, eval="RKDP54", dt=1e-14, tol=1e-5, init="sphere",
+                              multilayer=0),
 }
 MU0 = 1.256637061435916e-6
+
+
+def mesh_list(cfg):
+    """The meshes of a workload as dicts with n, h, o, Ms, K1, modules."""
+    if "meshes" in cfg:
+        return cfg["meshes"]
+    return [dict(n=cfg["n"], h=cfg["h"], o=(0, 0, 0), Ms=cfg["Ms"], K1=cfg["K1"], modules=cfg["modules"])]
+
+
+def total_cells(cfg):
+    return sum(m["n"][0] * m["n"][1] * m["n"][2] for m in mesh_list(cfg))
+
+
+def init_all(cfg, seed):
+    return [init_m(dict(cfg, n=m["n"], Ms=m["Ms"]), seed + 101 * q) for q, m in enumerate(mesh_list(cfg))]
 
 
 def init_m(cfg, seed):
@@ -59,11 +84,14 @@ def init_m(cfg, seed):
 
 def make_ctx(bm, cfg, device, precision):
     c = bm.Context(device=device, precision=precision)
-    c.add_mesh(cfg["n"], cfg["h"])
-    c.set_material(0, Ms=cfg["Ms"], A=cfg["A"], alpha=cfg["alpha"], grel=cfg.get("grel", 1.0), K1=cfg["K1"],
-                   ea=(0, 0, 1), D=cfg["D"])
-    c.set_modules(0, cfg["modules"])
-    c.set_field(0, cfg.get("Ha", (0, 0, 0)))
+    for q, m in enumerate(mesh_list(cfg)):
+        c.add_mesh(m["n"], m["h"], m["o"])
+        c.set_material(q, Ms=m["Ms"], A=cfg["A"], alpha=cfg["alpha"], grel=cfg.get("grel", 1.0), K1=m["K1"],
+                       ea=(0, 0, 1), D=cfg["D"])
+        c.set_modules(q, m["modules"])
+        c.set_field(q, cfg.get("Ha", (0, 0, 0)))
+    if "multilayer" in cfg:
+        c.multiconvolution(cfg["multilayer"])
     c.setode(cfg["eval"], cfg["dt"])
     if cfg["eval"] == "RKDP54":
         c.astepctrl(cfg["tol"], 2.0, 1e-15, 3e-12)
@@ -122,6 +150,37 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def ml_sample(cfg, shrink=4):
+    """A bounded CPU sample of a multilayer workload: every mesh shrunk in-plane by `shrink`."""
+    out = []
+    for m in cfg["meshes"]:
+        out.append(((m["n"][0] // shrink, m["n"][1] // shrink, m["n"][2]), tuple(m["h"]), tuple(m["o"])))
+    return out
+
+
+def cpu_reference_ml(cfg, warmup, evals):
+    """Seconds per H_demag evaluation of the reference's multilayered convolution
+    (DemagKernelCollection + VEC mesh transfer, compiled CPU build) on the shrunk sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_libs import reference, MultiLayer
+    if reference() is None:
+        return None, None
+    sample = ml_sample(cfg)
+    ml = MultiLayer(sample, cfg["multilayer"], which="reference")
+    n = sum(a[0][0] * a[0][1] * a[0][2] for a in sample)
+    rng = np.random.default_rng(7)
+    M = rng.normal(size=(n, 3))
+    M = M / np.linalg.norm(M, axis=1)[:, None] * 1e6
+    times = []
+    for i in range(warmup + evals):
+        t0 = time.perf_counter()
+        ml.eval(M)
+        if i >= warmup:
+            times.append(time.perf_counter() - t0)
+    ml.close()
+    return float(np.mean(times)), sample
+
+
 def cpu_reference_rate(cfg, sample_n=(256, 256, 16), evals=2, threads=None):
     """Mcell-steps/s of the reference's compiled CPU demag (6 evaluations per RKDP54 step)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -131,6 +190,15 @@ def cpu_reference_rate(cfg, sample_n=(256, 256, 16), evals=2, threads=None):
     R = reference()
     if R is None:
         return None
+    if "meshes" in cfg:
+        dt, sample = cpu_reference_ml(cfg, 1, evals)
+        n = sum(a[0][0] * a[0][1] * a[0][2] for a in sample)
+        per_step = 6 if cfg["eval"] == "RKDP54" else 4
+        return {"value": n / (per_step * dt) / 1e6, "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "reference CPU multilayered convolution (SDemag multilayer: DemagKernelCollection + weighted "
+                          "mesh transfer, project FFTW-API shim) on the meshes shrunk 4x in-plane %s, %d evaluations, "
+                          "%d per step; other field terms not timed" % ([a[0] for a in sample], evals, per_step),
+                "sec_per_eval": dt}
     nz = min(sample_n[2], cfg["n"][2])
     sn = (min(sample_n[0], cfg["n"][0]), min(sample_n[1], cfg["n"][1]), nz)
     ncell = sn[0] * sn[1] * sn[2]
@@ -178,13 +246,15 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="timed steps only (for profiler launch lists)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
-    ncell = cfg["n"][0] * cfg["n"][1] * cfg["n"][2]
+    ncell = total_cells(cfg)
     rank, ws, local, dist = dist_setup()
     base = {"metric": "Mcell-steps/s", "unit": "Mcell-steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "data": "synthetic (seeded initial magnetization, random-init state of the named film)",
-            "config": {"workload": args.config, "cells": list(cfg["n"]), "cellsize_m": list(cfg["h"]),
-                       "evaluation": cfg["eval"], "modules": cfg["modules"], "parallelism": "replicas x%d" % ws,
+            "config": {"workload": args.config, "cells": [list(m["n"]) for m in mesh_list(cfg)],
+                       "cellsize_m": [list(m["h"]) for m in mesh_list(cfg)],
+                       "evaluation": cfg["eval"], "modules": [m["modules"] for m in mesh_list(cfg)],
+                       "parallelism": "replicas x%d" % ws,
                        "l2": "working set above L2 (126 MB) every step"}}
 
     if args.impl == "reference":
@@ -200,12 +270,23 @@ def main():
         if R is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not present"}))
             return
+        per_step = 6 if cfg["eval"] == "RKDP54" else 4
+        if "meshes" in cfg:
+            dt, sample = cpu_reference_ml(cfg, args.warmup, args.steps)
+            nsc = sum(a[0][0] * a[0][1] * a[0][2] for a in sample)
+            v = nsc / (dt * per_step) / 1e6
+            out = dict(base, impl="reference", value=v, ms_per_step=dt * per_step * 1e3, dtype="f64",
+                       cpu_baseline={"value": v, "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                                     "sample": "each step = %d evaluations of the reference CPU multilayered convolution "
+                                               "on the meshes shrunk 4x in-plane %s" % (per_step, [a[0] for a in sample])},
+                       e2e={"value": v, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+            print(json.dumps(out))
+            return
         sn = (256, 256, min(16, cfg["n"][2])) if ncell > 256 * 256 * 16 else cfg["n"]
         sub = dict(cfg, n=sn)
         M = np.ascontiguousarray(init_m(sub, 7).reshape(-1))
         H = np.zeros_like(M)
         h = R.ref_demag_create(sn[0], sn[1], sn[2], cfg["h"][0], cfg["h"][1], cfg["h"][2])
-        per_step = 6 if cfg["eval"] == "RKDP54" else 4
         for i in range(args.warmup + args.steps):
             t0 = time.perf_counter()
             R.ref_demag_eval(P(h), dp(M), dp(H))
@@ -227,8 +308,9 @@ def main():
     import boris2_b200 as bm
     prec = bm.MIXED if args.precision == "mixed" else bm.FP64
     c = make_ctx(bm, cfg, local, prec)
-    M0 = init_m(cfg, 1234 + rank)
-    c.set_m(M0)
+    M0 = init_all(cfg, 1234 + rank)
+    for q, Mq in enumerate(M0):
+        c.set_m(Mq, q)
     # warm-up (also builds kernels and the CUDA graph)
     c.run(args.warmup)
     c.sync()
@@ -253,23 +335,25 @@ def main():
         c.close()
         return
     # e2e through the C ABI with host buffers (pinned), copies inside the timed region
-    try:
-        import torch
-        Mpin = torch.from_numpy(M0.reshape(-1).copy()).pin_memory()
-        Mout = torch.empty_like(Mpin).pin_memory()
-        Min_np = Mpin.numpy()
-        Mout_np = Mout.numpy()
-    except Exception:
-        Min_np = M0.reshape(-1).copy()
-        Mout_np = np.empty_like(Min_np)
+    bufs = []
+    for Mq in M0:
+        try:
+            import torch
+            Mpin = torch.from_numpy(Mq.reshape(-1).copy()).pin_memory()
+            Mout = torch.empty_like(Mpin).pin_memory()
+            bufs.append((Mpin.numpy(), Mout.numpy(), Mpin, Mout))
+        except Exception:
+            bufs.append((Mq.reshape(-1).copy(), np.empty(Mq.size), None, None))
     c.sync()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    c.set_m(Min_np)
+    for q, bq in enumerate(bufs):
+        c.set_m(bq[0], q)
     st1 = c.stats()
     st2 = c.run(args.steps)
-    c.get_m(out=Mout_np)
+    for q, bq in enumerate(bufs):
+        c.get_m(q, out=bq[1])
     e2e_s = time.perf_counter() - t0
     if dist:
         import torch
@@ -278,13 +362,24 @@ def main():
         e2e_s = float(t.item())
     e2e_steps = st2["accepted"] - st1["accepted"]
     e2e = ncell * e2e_steps * ws / e2e_s / 1e6
-    # kernel timing for the roofline
-    kms, kbytes = c.time_kernels(0, reps=20)
-    names = ["ymid2d" if cfg["n"][2] == 1 else "yfwd", "zmid", "yinv", "stage"]
-    # dominant kernel: largest share of one field evaluation
-    share = kms.copy()
-    dom = int(np.argmax(share))
+    # kernel timing for the roofline: dominant kernel of one field evaluation
     peak, peak_kind = peaks()
+    ml = "multilayer" in cfg
+    if ml:
+        kms, kbytes = c.ml_time_kernels(reps=10)
+        names = ["ml_transfer_in_xfwd", "ml_yfwd", "ml_zmid", "ml_yinv", "ml_xinv_transfer_out"]
+        dom = int(np.argmax(kms[:5]))
+        kernels = {names[i]: {"ms": kms[i], "GB/s": kbytes[i] / (kms[i] * 1e-3) / 1e9} for i in range(5) if kms[i] > 0}
+        kernels["demag_evaluation"] = {"ms": kms[5], "GB/s": kbytes[5] / (kms[5] * 1e-3) / 1e9,
+                                       "frac": kbytes[5] / (kms[5] * 1e-3) / 1e9 / peak}
+        tiles = None
+    else:
+        kms, kbytes = c.time_kernels(0, reps=20)
+        names = ["ymid2d" if cfg["n"][2] == 1 else "yfwd", "zmid", "yinv", "stage"]
+        dom = int(np.argmax(kms))
+        kernels = {names[i]: {"ms": kms[i], "GB/s": (kbytes[i] / (kms[i] * 1e-3) / 1e9 if kms[i] > 0 else None)}
+                   for i in range(4) if kms[i] > 0}
+        tiles = c.tiles(0)
     achieved = kbytes[dom] / (kms[dom] * 1e-3) / 1e9
     kpe = c.kernels_per_step()
     out = dict(base, value=value, ms_per_step=ms / max(steps_done, 1), dtype="f32" if prec == bm.MIXED else "f64",
@@ -296,21 +391,64 @@ def main():
                          "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "algorithmic_bytes_per_launch": kbytes[dom],
                          "launch_ms": kms[dom]},
-               kernels={names[i]: {"ms": kms[i], "GB/s": (kbytes[i] / (kms[i] * 1e-3) / 1e9 if kms[i] > 0 else None)}
-                        for i in range(4) if kms[i] > 0},
-               rkdp={"attempts": attempts, "accepted": steps_done, "dT": st["dT"]},
-               tiles=c.tiles(0))
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        try:
-            out["cpu_baseline"] = cpu_reference_rate(cfg)
-        except Exception as e:  # reported, not fatal
-            out["cpu_baseline"] = {"error": str(e)}
+               kernels=kernels,
+               rkdp={"attempts": attempts, "accepted": steps_done, "dT": st["dT"]})
+    if tiles:
+        out["tiles"] = tiles
     c.close()
+    if rank == 0 and ws == 1:
+        extra_steps = max(3, min(args.steps, 10))
+        # the same workload in the FP64 plain form
+        if prec == bm.MIXED:
+            try:
+                f = quick_rate(bm, cfg, bm.FP64, extra_steps, args.warmup, local)
+                out["fp64_plain"] = dict(f, speedup_mixed_over_fp64=value / f["value"])
+            except Exception as e:
+                out["fp64_plain"] = {"error": str(e)}
+        # the multilayered convolution workload (three stacked meshes), mixed and FP64
+        if not ml and args.config == "film3d_512x512x16":
+            try:
+                mcfg = CONFIGS["multilayer_stack3"]
+                mx = quick_rate(bm, mcfg, bm.MIXED, extra_steps, args.warmup, local, ml_timing=True)
+                f64 = quick_rate(bm, mcfg, bm.FP64, extra_steps, args.warmup, local, ml_timing=True)
+                out["multilayer"] = {"workload": "multilayer_stack3", "cells": total_cells(mcfg), "mixed": mx,
+                                     "fp64_plain": f64, "speedup_mixed_over_fp64": mx["value"] / f64["value"],
+                                     "peak_GB/s": peak}
+            except Exception as e:
+                out["multilayer"] = {"error": str(e)}
+        if not args.no_cpu_baseline:
+            try:
+                out["cpu_baseline"] = cpu_reference_rate(cfg)
+            except Exception as e:  # reported, not fatal
+                out["cpu_baseline"] = {"error": str(e)}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def quick_rate(bm, cfg, prec, steps, warmup, device, ml_timing=False):
+    """Mcell-steps/s of a workload over a short device-timed run (plus the multilayer demag
+    evaluation time and algorithmic GB/s when asked)."""
+    c = make_ctx(bm, cfg, device, prec)
+    for q, Mq in enumerate(init_all(cfg, 4321)):
+        c.set_m(Mq, q)
+    c.run(warmup)
+    c.sync()
+    st0 = c.stats()
+    st, ms = c.run_timed(steps)
+    done = st["accepted"] - st0["accepted"]
+    r = {"value": total_cells(cfg) * done / (ms * 1e-3) / 1e6, "ms_per_step": ms / max(done, 1), "steps": done,
+         "attempts": st["attempts"] - st0["attempts"]}
+    if ml_timing:
+        kms, kb = c.ml_time_kernels(reps=5)
+        r["demag_evaluation_ms"] = kms[5]
+        r["demag_GB/s"] = kb[5] / (kms[5] * 1e-3) / 1e9
+        r["zmid_ml_ms"] = kms[2]
+        r["zmid_ml_GB/s"] = kb[2] / (kms[2] * 1e-3) / 1e9
+    c.close()
+    return r
 
 
 if __name__ == "__main__":

@@ -17,6 +17,7 @@ this module            reference (Boris2)
 ``update_field``       Module::UpdateField / MeshBase::UpdateModules (Heff)
 ``demag_field``        Demag::UpdateField (Boris/Demag.cpp:170)
 ``run``                AdvanceTime over ODECommon_Base::Iterate
+``multiconvolution``   multiconvolution / 2dmulticonvolution / ncommon (SDemag multilayer)
 =====================  ============================================================
 
 Errors from the library raise :class:`BorisError` with the library's message, the
@@ -34,6 +35,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libboris_b200.so")
 DEMAG, EXCH, IDMI, ANIUNI, ZEEMAN = 1, 2, 4, 8, 16
 RK4, RKDP54 = 0, 1
 FP64, MIXED = 0, 1
+ML_OFF, ML_3D, ML_2D, ML_2D_LAYERED = -1, 0, 1, 2
 
 _lib = None
 
@@ -87,6 +89,10 @@ _SIGS = {
     "bm_debug_tensor": (_I, [_I, _I, _I, _I, _D, _D, _D, _DP]),
     "bm_debug_fft": (_I, [_I, _I, _I, _I, _I, _DP]),
     "bm_fft_noalloc": (_I, [_I, _I, _I, _I, _P, _P, _P]),
+    "bm_set_multiconvolution": (_I, [_P, _I, _IP]),
+    "bm_ml_info": (_I, [_P, _IP, _IP, _IP, _IP, _DP, _IP]),
+    "bm_prepare": (_I, [_P]),
+    "bm_ml_time_kernels": (_I, [_P, _I, _DP, _DP]),
 }
 
 
@@ -180,6 +186,38 @@ class Context:
 
     def set_precision(self, precision):
         _check(lib().bm_set_precision(self._h, int(precision)))
+
+    def multiconvolution(self, mode=ML_3D, ncommon=None):
+        """Multilayered demag over all meshes with the demag module (ML_OFF turns it off):
+        ML_3D = ``multiconvolution 1``, ML_2D / ML_2D_LAYERED = ``2dmulticonvolution 1 / 2``;
+        ncommon = ``ncommon nx ny nz`` (None: ``ncommonauto``)."""
+        nc = None if ncommon is None else (ctypes.c_int * 3)(*[int(v) for v in ncommon])
+        _check(lib().bm_set_multiconvolution(self._h, int(mode), nc))
+
+    def ml_info(self):
+        """Layers of the multilayered convolution: count, n_common, mesh and transfer flag per
+        layer, rectangles (start, end) and kernel kinds per (layer, source)."""
+        L = _I()
+        nc = (ctypes.c_int * 3)()
+        lm = (ctypes.c_int * 8)()
+        tr = (ctypes.c_int * 8)()
+        rc = np.zeros(48)
+        kk = (ctypes.c_int * 64)()
+        _check(lib().bm_ml_info(self._h, ctypes.byref(L), nc, lm, tr, _dp(rc), kk))
+        n = L.value
+        return {"L": n, "n_common": tuple(nc), "layer_mesh": list(lm)[:n], "transfer": list(tr)[:n],
+                "rects": rc[:6 * n].reshape(n, 6).copy(), "kinds": np.array(list(kk)[:n * n]).reshape(n, n)}
+
+    def prepare(self):
+        _check(lib().bm_prepare(self._h))
+
+    def ml_time_kernels(self, reps=10):
+        """ms and algorithmic bytes of the parts of one multilayer demag evaluation: transfer
+        in + x forward, y forward, z pass + products, y inverse, x inverse + transfer out, all."""
+        ms = np.zeros(6)
+        by = np.zeros(6)
+        _check(lib().bm_ml_time_kernels(self._h, int(reps), _dp(ms), _dp(by)))
+        return ms, by
 
     # ------------------------------------------------------------------ ODE
     def setode(self, evaluation="RK4", dt=None):

@@ -13,6 +13,7 @@
 // except one read of the accepted-step counter per batch of graph launches.
 #include "../../include/boris_b200.h"
 #include "kernels.h"
+#include "ml.h"
 #include "util.h"
 #include <vector>
 #include <string>
@@ -77,6 +78,28 @@ struct Mesh {
     void *Msd = nullptr, *K1d = nullptr, *Hout = nullptr;
     double *Had = nullptr, *stage64 = nullptr;
     int nHa = 1;
+    // multilayered convolution: 0 not in one, 1 its grid is the common grid (spectra in S1/S2),
+    // 2 mesh transfer to and from the common grid (demag field arrives in Hd)
+    int ml_role = 0;
+    void *Hd = nullptr;         // demag field of the mesh (role 2)
+    void *Hc = nullptr;         // common-grid demag fields of the mesh's layers, [layer][c][cell]
+    int *out_ptr = nullptr, *out_idx = nullptr;
+    void *out_w = nullptr;
+};
+
+// multilayered convolution state of a context
+struct MLRun {
+    MLGeom g;
+    std::vector<int> mesh_of;       // multilayer mesh -> context mesh
+    std::vector<Mesh> grids;        // per layer: the common grid of a transfer layer
+    std::vector<int> direct;        // per layer: context mesh whose grid is the common grid, or -1
+    std::vector<int> block;         // per layer: block of the layer in its mesh's Hc
+    std::vector<int *> in_ptr, in_idx;
+    std::vector<void *> in_w;
+    void *K = nullptr;
+    void *twz = nullptr;
+    int W = 8;
+    long long ncc = 0;
 };
 
 }  // namespace
@@ -101,6 +124,10 @@ struct bm_ctx {
     int kernels_per_step = 0;
     double *farq = nullptr;
     StepState host_st;
+    int ml_mode = -1;           // -1 off; 0 3D, 1 2D, 2 2D layered
+    bool ml_nc_set = false;
+    int ml_nc[3] = {1, 1, 1};
+    MLRun *ml = nullptr;
 };
 
 namespace {
@@ -117,6 +144,26 @@ void free_mesh(Mesh &m)
     m.Had = nullptr;
     if (m.stage64) cudaFree(m.stage64);
     m.stage64 = nullptr;
+    void **pm[] = {&m.Hd, &m.Hc, &m.out_w};
+    for (auto pp : pm) { if (*pp) cudaFree(*pp); *pp = nullptr; }
+    if (m.out_ptr) cudaFree(m.out_ptr);
+    if (m.out_idx) cudaFree(m.out_idx);
+    m.out_ptr = m.out_idx = nullptr;
+    m.ml_role = 0;
+}
+
+void free_ml(bm_ctx *c)
+{
+    if (!c->ml) return;
+    MLRun &r = *c->ml;
+    for (auto &g : r.grids) free_mesh(g);
+    for (auto p : r.in_ptr) if (p) cudaFree(p);
+    for (auto p : r.in_idx) if (p) cudaFree(p);
+    for (auto p : r.in_w) if (p) cudaFree(p);
+    if (r.K) cudaFree(r.K);
+    if (r.twz) cudaFree(r.twz);
+    delete c->ml;
+    c->ml = nullptr;
 }
 
 void drop_graph(bm_ctx *c)
@@ -150,6 +197,7 @@ void unprepare(bm_ctx *c)
         }
         free_mesh(m);
     }
+    free_ml(c);
     c->ready = false;
     c->s1_dirty = true;
 }
@@ -255,21 +303,29 @@ int prepare_mesh(bm_ctx *c, Mesh &m)
     }
     if (cudaMalloc(&m.Hout, v3) != cudaSuccess) return fail(BM_ENOMEM, "H buffer");
     if (cudaMalloc(&m.stage64, sizeof(double) * 3 * m.n) != cudaSuccess) return fail(BM_ENOMEM, "staging buffer");
-    if (m.modules & BM_DEMAG) {
+    if (m.ml_role == 2) {
+        if (cudaMalloc(&m.Hd, v3) != cudaSuccess) return fail(BM_ENOMEM, "multilayer demag field");
+        cudaMemsetAsync(m.Hd, 0, v3, s);
+    }
+    if ((m.modules & BM_DEMAG) && m.ml_role != 2) {
         size_t s1 = sizeof(cpx<T>) * 3 * (size_t)m.nz * m.ny * m.LX;
         if (cudaMalloc(&m.S1, s1) != cudaSuccess) return fail(BM_ENOMEM, "S1");
         cudaMemsetAsync(m.S1, 0, s1, s);
-        if (m.nz > 1) {
+        if (m.nz > 1 || m.ml_role == 1) {
             size_t s2 = sizeof(cpx<T>) * 3 * (size_t)m.nz * m.Ny * m.LX;
             if (cudaMalloc(&m.S2, s2) != cudaSuccess) return fail(BM_ENOMEM, "S2");
+            cudaMemsetAsync(m.S2, 0, s2, s);
         }
-        size_t nk = (size_t)(m.Nx / 2 + 1) * (m.Ny / 2 + 1) * (m.Nz / 2 + 1);
-        if (cudaMalloc(&m.K, sizeof(T) * 6 * nk) != cudaSuccess) return fail(BM_ENOMEM, "kernel spectra");
         int rc;
         if ((rc = upload_table<T>(&m.twx, m.LX, false, s))) return rc;
         if ((rc = upload_table<T>(&m.twx2, m.Nx, false, s))) return rc;
         if ((rc = upload_table<T>(&m.twy, m.Ny, false, s))) return rc;
         if ((rc = upload_table<T>(&m.twz, m.Nz, false, s))) return rc;
+    }
+    if ((m.modules & BM_DEMAG) && m.ml_role == 0) {
+        int rc;
+        size_t nk = (size_t)(m.Nx / 2 + 1) * (m.Ny / 2 + 1) * (m.Nz / 2 + 1);
+        if (cudaMalloc(&m.K, sizeof(T) * 6 * nk) != cudaSuccess) return fail(BM_ENOMEM, "kernel spectra");
         void *tx = nullptr, *ty = nullptr, *tz = nullptr;
         if ((rc = upload_table<double>(&tx, m.Nx, true, s))) return rc;
         if ((rc = upload_table<double>(&ty, m.Ny, true, s))) return rc;
@@ -367,7 +423,7 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
     const int lim = bm_lb<T>::v;
     const size_t cs = sizeof(cpx<T>);
     const int reps = 3;
-    if (m.modules & BM_DEMAG) {
+    if ((m.modules & BM_DEMAG) && m.ml_role == 0) {
         YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
         if (m.nz == 1) {
             float best = 1e30f; int bw = m.W2;
@@ -436,12 +492,163 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
     return 0;
 }
 
+// ------------------------------------------------------------------ multilayered convolution setup
+// Geometry and roles (host only, before the meshes allocate): every mesh with the demag module
+// takes part; a layer whose grid is its mesh's grid keeps its spectra in the mesh's S1/S2,
+// every other layer gets a common-grid buffer set and the weighted transfers.
+int ml_plan(bm_ctx *c)
+{
+    if (c->ml_mode < 0) return 0;
+    std::vector<MLMeshIn> in;
+    std::vector<int> of;
+    for (int i = 0; i < (int)c->meshes.size(); i++) {
+        Mesh &m = c->meshes[i];
+        if (!(m.modules & BM_DEMAG)) continue;
+        MLMeshIn x;
+        x.n[0] = m.nx; x.n[1] = m.ny; x.n[2] = m.nz;
+        for (int a = 0; a < 3; a++) { x.h[a] = m.h[a]; x.o[a] = m.o[a]; }
+        in.push_back(x);
+        of.push_back(i);
+    }
+    if (in.empty()) return 0;
+    MLRun *r = new MLRun();
+    c->ml = r;
+    r->mesh_of = of;
+    std::string err;
+    if (ml_build_geometry(in, c->ml_mode, c->ml_nc_set ? c->ml_nc : nullptr, r->g, err)) return fail(BM_EINVAL, err);
+    if (!zmid_ml_supported(r->g.N[2])) return fail(BM_EUNSUPPORTED, "multilayer: common n.z above 32 is not supported");
+    for (int l = 0; l < r->g.L; l++) c->meshes[of[r->g.layers[l].mesh]].ml_role = r->g.layers[l].transfer ? 2 : 1;
+    return 0;
+}
+
+template <typename T>
+int prepare_grid(bm_ctx *c, Mesh &g)
+{
+    cudaStream_t s = c->stream;
+    g.n = (long long)g.nx * g.ny * g.nz;
+    g.Nx = 2 * nice_size(g.nx);
+    g.Ny = 2 * nice_size(g.ny);
+    g.Nz = g.nz > 1 ? 2 * nice_size(g.nz) : 1;
+    g.LX = g.Nx / 2;
+    if (!bm_make_plan(g.LX, g.px) || !bm_make_plan(g.Ny, g.py) || !bm_make_plan(g.Nz, g.pz))
+        return fail(BM_EUNSUPPORTED, "unsupported FFT size");
+    choose_tiles<T>(g);
+    size_t v3 = sizeof(T) * 3 * (size_t)g.n;
+    if (cudaMalloc(&g.buf[0], v3) != cudaSuccess) return fail(BM_ENOMEM, "multilayer grid M");
+    cudaMemsetAsync(g.buf[0], 0, v3, s);
+    size_t s1 = sizeof(cpx<T>) * 3 * (size_t)g.nz * g.ny * g.LX, s2 = sizeof(cpx<T>) * 3 * (size_t)g.nz * g.Ny * g.LX;
+    if (cudaMalloc(&g.S1, s1) != cudaSuccess) return fail(BM_ENOMEM, "multilayer S1");
+    if (cudaMalloc(&g.S2, s2) != cudaSuccess) return fail(BM_ENOMEM, "multilayer S2");
+    cudaMemsetAsync(g.S1, 0, s1, s);
+    cudaMemsetAsync(g.S2, 0, s2, s);
+    int rc;
+    if ((rc = upload_table<T>(&g.twx, g.LX, false, s))) return rc;
+    if ((rc = upload_table<T>(&g.twx2, g.Nx, false, s))) return rc;
+    if ((rc = upload_table<T>(&g.twy, g.Ny, false, s))) return rc;
+    if ((rc = upload_table<T>(&g.twz, g.Nz, false, s))) return rc;
+    return 0;
+}
+
+template <typename T>
+int upload_vec(void **dst, const std::vector<T> &v, cudaStream_t s)
+{
+    size_t bytes = sizeof(T) * (v.empty() ? 1 : v.size());
+    if (cudaMalloc(dst, bytes) != cudaSuccess) return fail(BM_ENOMEM, "multilayer transfer lists");
+    if (!v.empty()) CK(cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+template <typename T>
+std::vector<T> as_type(const std::vector<double> &v)
+{
+    std::vector<T> o(v.size());
+    for (size_t i = 0; i < v.size(); i++) o[i] = (T)v[i];
+    return o;
+}
+
+template <typename T>
+int prepare_ml(bm_ctx *c)
+{
+    if (!c->ml) return 0;
+    MLRun &r = *c->ml;
+    MLGeom &g = r.g;
+    cudaStream_t s = c->stream;
+    const int L = g.L;
+    r.ncc = (long long)g.nc[0] * g.nc[1] * g.nc[2];
+    r.grids.assign(L, Mesh());
+    r.direct.assign(L, -1);
+    r.block.assign(L, -1);
+    r.in_ptr.assign(L, nullptr);
+    r.in_idx.assign(L, nullptr);
+    r.in_w.assign(L, nullptr);
+    int rc;
+    for (int l = 0; l < L; l++) {
+        const MLLayerGeom &y = g.layers[l];
+        if (!y.transfer) { r.direct[l] = r.mesh_of[y.mesh]; continue; }
+        Mesh &G = r.grids[l];
+        G.nx = g.nc[0]; G.ny = g.nc[1]; G.nz = g.nc[2];
+        for (int a = 0; a < 3; a++) { G.h[a] = y.hc[a]; G.o[a] = y.rs[a]; }
+        G.modules = BM_DEMAG;
+        if ((rc = prepare_grid<T>(c, G))) return rc;
+        if ((rc = upload_vec<int>((void **)&r.in_ptr[l], y.in_ptr, s))) return rc;
+        if ((rc = upload_vec<int>((void **)&r.in_idx[l], y.in_idx, s))) return rc;
+        if ((rc = upload_vec<T>(&r.in_w[l], as_type<T>(y.in_w), s))) return rc;
+    }
+    for (size_t k = 0; k < g.out.size(); k++) {
+        const MLMeshOut &o = g.out[k];
+        if (o.layers.empty()) continue;
+        Mesh &m = c->meshes[r.mesh_of[k]];
+        if ((rc = upload_vec<int>((void **)&m.out_ptr, o.ptr, s))) return rc;
+        if ((rc = upload_vec<int>((void **)&m.out_idx, o.idx, s))) return rc;
+        if ((rc = upload_vec<T>(&m.out_w, as_type<T>(o.w), s))) return rc;
+        size_t hb = sizeof(T) * 3 * (size_t)r.ncc * o.layers.size();
+        if (cudaMalloc(&m.Hc, hb) != cudaSuccess) return fail(BM_ENOMEM, "multilayer common-grid fields");
+        cudaMemsetAsync(m.Hc, 0, hb, s);
+        for (size_t b = 0; b < o.layers.size(); b++) r.block[o.layers[b]] = (int)b;
+    }
+    // kernel collection
+    size_t total = 0;
+    for (auto &K : g.kernels) total = std::max(total, K.off + ((K.count + 31) & ~(size_t)31));
+    if (cudaMalloc(&r.K, sizeof(T) * total) != cudaSuccess) return fail(BM_ENOMEM, "multilayer kernels");
+    void *tx = nullptr, *ty = nullptr, *tz = nullptr;
+    if ((rc = upload_table<double>(&tx, g.N[0], true, s)) || (rc = upload_table<double>(&ty, g.N[1], true, s)) ||
+        (rc = upload_table<double>(&tz, g.N[2], true, s))) return rc;
+    for (auto &K : g.kernels) {
+        double hq[3];
+        if (K.kind == BM_MLK_SELF) {
+            double hm = std::fmax(K.hd[0], std::fmax(K.hd[1], K.hd[2]));
+            for (int a = 0; a < 3; a++) hq[a] = K.hd[a] / hm;
+        } else {
+            for (int a = 0; a < 3; a++) hq[a] = K.irregular ? K.hd[a] : K.hs[a];
+        }
+        std::vector<double> fq(6 * BM_FARQ_PER_COMP);
+        bm_far_coeffs(hq[0], hq[1], hq[2], fq.data());
+        CK(cudaMemcpyAsync(c->farq, fq.data(), sizeof(double) * fq.size(), cudaMemcpyHostToDevice, s));
+        rc = build_ml_kernel_device<T>((T *)r.K + K.off, K, g.nc, g.N, c->farq, (const cpx<double> *)tx,
+                                       (const cpx<double> *)ty, (const cpx<double> *)tz, s);
+        if (rc) break;
+    }
+    cudaFree(tx); cudaFree(ty); cudaFree(tz);
+    if (rc) return fail(BM_ECUDA, "multilayer kernel build failed (" + std::to_string(rc) + ")");
+    if ((rc = upload_table<T>(&r.twz, g.N[2], false, s))) return rc;
+    // z pass tile: columns per block
+    const int lim = bm_lb<T>::v, LX = g.N[0] / 2;
+    int W = 16;
+    while (W > 1 && (6 * L * W > lim || zmid_ml_smem<T>(L, g.N[2], W) > 96 * 1024)) W /= 2;
+    while (W > 1 && W > LX) W /= 2;
+    r.W = W;
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
 template <typename T>
 int prepare_T(bm_ctx *c)
 {
+    if (int rc = ml_plan(c)) { free_ml(c); for (auto &mm : c->meshes) mm.ml_role = 0; return rc; }
     for (auto &m : c->meshes) {
         int rc = prepare_mesh<T>(c, m);
-        if (rc) { for (auto &mm : c->meshes) free_mesh(mm); return rc; }
+        if (rc) { for (auto &mm : c->meshes) free_mesh(mm); free_ml(c); return rc; }
         // BM_TILES="w2,wy,wz,rows" fixes the tile shapes (profiling runs); otherwise autotune
         const char *ev = getenv("BM_TILES");
         int t4[4];
@@ -451,6 +658,7 @@ int prepare_T(bm_ctx *c)
             m.staged = (sr && sr[0] == '1') ? 1 : 0;
         } else if (c->autotune) autotune_mesh<T>(c, m);
     }
+    if (int rc = prepare_ml<T>(c)) { for (auto &mm : c->meshes) free_mesh(mm); free_ml(c); return rc; }
     return 0;
 }
 
@@ -522,18 +730,130 @@ StageArgs<T> stage_args(bm_ctx *c, Mesh &m)
     a.n = m.n;
     a.do_xfwd = (m.modules & BM_DEMAG) ? 1 : 0;
     a.staged = m.staged;
+    if (m.ml_role == 2) {
+        // multilayer with mesh transfer: the demag field arrives in Hd, no x transforms here
+        a.modules &= ~BM_DEMAG;
+        a.do_xfwd = 0;
+        a.S1 = nullptr;
+        a.Hd = (const T *)m.Hd;
+    }
     return a;
 }
 
 template <typename T> T *B(Mesh &m, int i) { return (T *)m.buf[i]; }
 template <typename T> T *E(Mesh &m, int i) { return (T *)m.ev[i]; }
 
+Mesh &ml_grid(bm_ctx *c, int l)
+{
+    return c->ml->direct[l] >= 0 ? c->meshes[c->ml->direct[l]] : c->ml->grids[l];
+}
+
+// Demag spectra -> fields for one effective-field evaluation whose stage kernels read
+// M from buffer bi of every mesh. Without a multilayered convolution: each mesh's own y/z
+// passes. With one: transfer in and x FFT of the transfer layers, y passes of every layer, the
+// fused z pass with the L x L products, inverse y, then inverse x and transfer out into Hd.
+// multilayer parts: 0 transfer in + x forward, 1 y forward, 2 z pass + products, 3 y inverse,
+// 4 x inverse + transfer out
+template <typename T>
+int ml_enqueue_part(bm_ctx *c, int part, int gate, int bi, int *count)
+{
+    MLRun &r = *c->ml;
+    const MLGeom &g = r.g;
+    const int L = g.L;
+    cudaStream_t s = c->stream;
+    if (part == 0) for (int l = 0; l < L; l++) {
+        if (r.direct[l] >= 0) continue;
+        Mesh &G = r.grids[l];
+        Mesh &M = c->meshes[r.mesh_of[g.layers[l].mesh]];
+        CKL(launch_ml_gather<T>(B<T>(G, 0), r.ncc, r.ncc, B<T>(M, bi), M.n, r.in_ptr[l], r.in_idx[l], (const T *)r.in_w[l],
+                                c->st, gate, s), "multilayer transfer in");
+        StageArgs<T> a = stage_args<T>(c, G);
+        a.mode = BM_MODE_UPDATE;
+        a.gate = gate;
+        a.Min = B<T>(G, 0); a.Mbase = B<T>(G, 0);
+        a.nev = 0;
+        CKL(launch_stage<T>(a, s), "multilayer x forward");
+        (*count) += 2;
+    }
+    if (part == 1) for (int l = 0; l < L; l++) {
+        Mesh &G = ml_grid(c, l);
+        YZArgs<T> a = yz_args<T>(c, G, gate);
+        a.W = G.Wy;
+        CKL(launch_yfwd<T>(a, s), "multilayer y forward");
+        (*count)++;
+    }
+    if (part == 2) {
+        MLZArgs<T> z;
+        memset(&z, 0, sizeof(z));
+        for (int l = 0; l < L; l++) z.S2[l] = (cpx<T> *)ml_grid(c, l).S2;
+        z.K = (const T *)r.K;
+        for (int d = 0; d < L; d++)
+            for (int q = 0; q < L; q++) {
+                const MLKernelSpec &K = g.kernels[g.pair_kernel[d * L + q]];
+                z.kd[d * L + q].kind = K.kind;
+                z.kd[d * L + q].inv = g.pair_inv[d * L + q];
+                z.kd[d * L + q].off = (long long)K.off;
+            }
+        z.twz = (const cpx<T> *)r.twz;
+        z.L = L; z.nz = g.nc[2]; z.Ny = g.N[1]; z.Nz = g.N[2]; z.LX = g.N[0] / 2; z.W = r.W;
+        z.st = c->st; z.gate = gate;
+        CKL(launch_zmid_ml<T>(z, s), "multilayer z pass");
+        (*count)++;
+    }
+    if (part == 3) for (int l = 0; l < L; l++) {
+        Mesh &G = ml_grid(c, l);
+        YZArgs<T> a = yz_args<T>(c, G, gate);
+        a.W = G.Wy;
+        CKL(launch_yinv<T>(a, s), "multilayer y inverse");
+        (*count)++;
+    }
+    if (part == 4) for (int l = 0; l < L; l++) {
+        if (r.direct[l] >= 0) continue;
+        Mesh &G = r.grids[l];
+        Mesh &M = c->meshes[r.mesh_of[g.layers[l].mesh]];
+        StageArgs<T> a = stage_args<T>(c, G);
+        a.mode = BM_MODE_HEFF;
+        a.modules = BM_DEMAG;
+        a.do_xfwd = 0;
+        a.gate = gate;
+        a.Min = B<T>(G, 0);
+        a.Hout = (T *)M.Hc + (size_t)r.block[l] * 3 * r.ncc;
+        CKL(launch_stage<T>(a, s), "multilayer x inverse");
+        (*count)++;
+    }
+    if (part == 4) for (size_t k = 0; k < g.out.size(); k++) {
+        if (g.out[k].layers.empty()) continue;
+        Mesh &M = c->meshes[r.mesh_of[k]];
+        CKL(launch_ml_gather<T>((T *)M.Hd, M.n, M.n, (const T *)M.Hc, r.ncc, M.out_ptr, M.out_idx, (const T *)M.out_w, c->st,
+                                gate, s), "multilayer transfer out");
+        (*count)++;
+    }
+    return 0;
+}
+
+template <typename T>
+int enqueue_fields(bm_ctx *c, int gate, int bi, int *count)
+{
+    if (!c->ml) {
+        for (auto &m : c->meshes) {
+            int rc = enqueue_yz<T>(c, m, gate, count);
+            if (rc) return rc;
+        }
+        return 0;
+    }
+    for (int part = 0; part < 5; part++) {
+        int rc = ml_enqueue_part<T>(c, part, gate, bi, count);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
 // S1 = x-FFT(M) for every mesh (after set_m, compute_* or a fresh start)
 template <typename T>
 int enqueue_prime(bm_ctx *c, int *count)
 {
     for (auto &m : c->meshes) {
-        if (!(m.modules & BM_DEMAG)) continue;
+        if (!(m.modules & BM_DEMAG) || m.ml_role == 2) continue;
         StageArgs<T> a = stage_args<T>(c, m);
         a.mode = BM_MODE_UPDATE;
         a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0);
@@ -549,9 +869,10 @@ int enqueue_rk4_step(bm_ctx *c, int *count)
 {
     // buffers: 0 = M (step start, sM1), 2 = B, 3 = C ; evals 0..2
     const int nm = (int)c->meshes.size();
+    static const int min_buf[4] = {0, 2, 3, 2};
     for (int s = 0; s < 4; s++) {
-        for (int i = 0; i < nm; i++) {
-            int rc = enqueue_yz<T>(c, c->meshes[i], BM_GATE_ALWAYS, count);
+        {
+            int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count);
             if (rc) return rc;
         }
         for (int i = 0; i < nm; i++) {
@@ -596,8 +917,8 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
         (*count)++;
     }
     // evaluation 0: FSAL rhs + error of the previous step + controller
-    for (int i = 0; i < nm; i++) {
-        int rc = enqueue_yz<T>(c, c->meshes[i], BM_GATE_ALWAYS, count);
+    {
+        int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, 0, count);
         if (rc) return rc;
     }
     static const double bs[5] = {5179.0 / 57600, 7571.0 / 16695, 393.0 / 640, -92097.0 / 339200, 187.0 / 2100};
@@ -636,8 +957,8 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
         {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656},
         {35.0 / 384, 0.0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
     for (int s = 1; s <= 5; s++) {
-        for (int i = 0; i < nm; i++) {
-            int rc = enqueue_yz<T>(c, c->meshes[i], BM_GATE_ACCEPTED, count);
+        {
+            int rc = enqueue_fields<T>(c, BM_GATE_ACCEPTED, (s % 2 == 1) ? 2 : 3, count);
             if (rc) return rc;
         }
         for (int i = 0; i < nm; i++) {
@@ -719,7 +1040,18 @@ template <typename T>
 int compute_field_T(bm_ctx *c, Mesh &m, int modules_mask, double *H)
 {
     int cnt = 0;
-    if (m.modules & BM_DEMAG) {
+    if ((m.modules & BM_DEMAG) && m.ml_role) {
+        // x transforms of the layers that live on their mesh's grid, then the whole convolution
+        for (auto &mm : c->meshes) {
+            if (mm.ml_role != 1) continue;
+            StageArgs<T> a = stage_args<T>(c, mm);
+            a.mode = BM_MODE_UPDATE;
+            a.Min = B<T>(mm, 0); a.Mbase = B<T>(mm, 0);
+            CKL(launch_stage<T>(a, c->stream), "xfwd");
+        }
+        int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, 0, &cnt);
+        if (rc) return rc;
+    } else if (m.modules & BM_DEMAG) {
         StageArgs<T> a = stage_args<T>(c, m);
         a.mode = BM_MODE_UPDATE;
         a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0);
@@ -731,6 +1063,10 @@ int compute_field_T(bm_ctx *c, Mesh &m, int modules_mask, double *H)
     a.mode = BM_MODE_HEFF;
     a.modules = m.modules & modules_mask;
     a.do_xfwd = 0;
+    if (m.ml_role == 2) {
+        a.modules &= ~BM_DEMAG;
+        a.Hd = (modules_mask & BM_DEMAG) ? (const T *)m.Hd : nullptr;
+    }
     a.Min = B<T>(m, 0);
     a.Hout = (T *)m.Hout;
     CKL(launch_stage<T>(a, c->stream), "heff");
@@ -911,6 +1247,46 @@ int bm_set_precision(bm_ctx *c, int precision)
     return 0;
 }
 
+int bm_set_multiconvolution(bm_ctx *c, int mode, const int *n_common)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (mode < BM_ML_OFF || mode > BM_ML_2D_LAYERED) return fail(BM_EINVAL, "multiconvolution mode");
+    if (n_common && (n_common[0] < 1 || n_common[1] < 1 || n_common[2] < 1)) return fail(BM_EINVAL, "n_common must be >= 1");
+    if (n_common && (nice_size(n_common[0]) > 4096 || nice_size(n_common[1]) > 4096 || n_common[2] > 32))
+        return fail(BM_EUNSUPPORTED, "n_common above the supported FFT size");
+    unprepare(c);
+    c->ml_mode = mode;
+    c->ml_nc_set = n_common != nullptr;
+    if (n_common) for (int a = 0; a < 3; a++) c->ml_nc[a] = n_common[a];
+    return 0;
+}
+
+int bm_ml_info(bm_ctx *c, int *L, int *nc3, int *layer_mesh, int *transfer, double *rects6, int *kinds)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (c->ml_mode < 0) return fail(BM_ESTATE, "multilayered convolution is off");
+    if (int rc = prepare(c)) return rc;
+    if (!c->ml) return fail(BM_ESTATE, "no mesh with demag in the multilayered convolution");
+    const MLRun &r = *c->ml;
+    const MLGeom &g = r.g;
+    if (L) *L = g.L;
+    if (nc3) for (int a = 0; a < 3; a++) nc3[a] = g.nc[a];
+    for (int l = 0; l < g.L; l++) {
+        if (layer_mesh) layer_mesh[l] = r.mesh_of[g.layers[l].mesh];
+        if (transfer) transfer[l] = g.layers[l].transfer;
+        if (rects6)
+            for (int a = 0; a < 3; a++) { rects6[6 * l + a] = g.layers[l].rs[a]; rects6[6 * l + 3 + a] = g.layers[l].re[a]; }
+        if (kinds) for (int q = 0; q < g.L; q++) kinds[l * g.L + q] = g.pair_kind[l * g.L + q];
+    }
+    return 0;
+}
+
+int bm_prepare(bm_ctx *c)
+{
+    if (int rc = check_ctx(c)) return rc;
+    return prepare(c);
+}
+
 int bm_set_m(bm_ctx *c, int mesh, const double *M)
 {
     if (int rc = check_mesh(c, mesh)) return rc;
@@ -1079,6 +1455,7 @@ template <typename T>
 int time_kernels_T(bm_ctx *c, Mesh &m, int reps, double *ms4, double *bytes4)
 {
     for (int i = 0; i < 4; i++) { ms4[i] = 0.0; bytes4[i] = 0.0; }
+    if (m.ml_role) return fail(BM_EUNSUPPORTED, "per-mesh kernel timing of a multilayer mesh");
     cudaStream_t s = c->stream;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -1099,7 +1476,7 @@ int time_kernels_T(bm_ctx *c, Mesh &m, int reps, double *ms4, double *bytes4)
         return 0;
     };
     int rc = 0;
-    if (m.modules & BM_DEMAG) {
+    if ((m.modules & BM_DEMAG) && m.ml_role == 0) {
         YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
         if (m.nz == 1) {
             rc = timeit([&]() { return launch_ymid2d<T>(a, s); }, 0, 2.0 * s1 + 4.0 / 6.0 * kb);
@@ -1141,7 +1518,80 @@ int time_kernels_T(bm_ctx *c, Mesh &m, int reps, double *ms4, double *bytes4)
 }
 }  // namespace
 
+namespace {
+// Times the parts of one multilayer demag evaluation (CUDA events, reps launches each after two
+// warm-ups) and returns their algorithmic bytes: slots 0..4 as ml_enqueue_part, slot 5 the
+// whole evaluation. Algorithmic bytes per evaluation: every layer's native M read and field
+// write (2 R n_mesh), its spectra through the y passes and the z pass (4 C S1 + 4 C S2, C the
+// complex3 size, S1 = LX ny nz, S2 = LX Ny nz on the common grid) and every unique kernel once.
+template <typename T>
+int ml_time_T(bm_ctx *c, int reps, double *ms6, double *bytes6)
+{
+    MLRun &r = *c->ml;
+    const MLGeom &g = r.g;
+    cudaStream_t s = c->stream;
+    const double R3 = 3.0 * sizeof(T), C3 = 6.0 * sizeof(T);
+    const double LX = g.N[0] / 2, S1 = LX * g.nc[1] * g.nc[2], S2 = LX * g.N[1] * g.nc[2];
+    double kbytes = 0.0;
+    for (auto &K : g.kernels) kbytes += (double)K.count * sizeof(T);
+    double bin = 0.0, bout = 0.0;
+    for (int l = 0; l < g.L; l++) {
+        const Mesh &M = c->meshes[r.mesh_of[g.layers[l].mesh]];
+        double nm = (double)M.n;
+        if (g.force2d == 2) nm /= M.nz;   // a z layer of the mesh
+        bin += R3 * nm + C3 * S1;
+        bout += R3 * nm + C3 * S1;
+    }
+    bytes6[0] = bin;
+    bytes6[1] = g.L * C3 * (S1 + S2);
+    bytes6[2] = g.L * 2.0 * C3 * S2 + kbytes;
+    bytes6[3] = g.L * C3 * (S1 + S2);
+    bytes6[4] = bout;
+    bytes6[5] = bytes6[0] + bytes6[1] + bytes6[2] + bytes6[3] + bytes6[4];
+    // the x forward of direct layers happens in their stage kernels; prime it once
+    int cnt = 0;
+    for (auto &mm : c->meshes) {
+        if (mm.ml_role != 1) continue;
+        StageArgs<T> a = stage_args<T>(c, mm);
+        a.mode = BM_MODE_UPDATE;
+        a.Min = B<T>(mm, 0); a.Mbase = B<T>(mm, 0);
+        CKL(launch_stage<T>(a, s), "xfwd");
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int part = 0; part <= 5; part++) {
+        auto go = [&]() -> int {
+            if (part < 5) return ml_enqueue_part<T>(c, part, BM_GATE_ALWAYS, 0, &cnt);
+            return enqueue_fields<T>(c, BM_GATE_ALWAYS, 0, &cnt);
+        };
+        for (int w = 0; w < 2; w++) if (int rc = go()) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+        cudaEventRecord(e0, s);
+        for (int q = 0; q < reps; q++) if (int rc = go()) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms6[part] = ms / reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->s1_dirty = true;
+    return 0;
+}
+}  // namespace
+
 extern "C" {
+
+int bm_ml_time_kernels(bm_ctx *c, int reps, double *ms6, double *bytes6)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (!ms6 || !bytes6 || reps < 1) return fail(BM_EINVAL, "args");
+    if (int rc = prepare(c)) return rc;
+    if (!c->ml) return fail(BM_ESTATE, "multilayered convolution is off");
+    cudaSetDevice(c->device);
+    return (c->precision == BM_FP64) ? ml_time_T<double>(c, reps, ms6, bytes6) : ml_time_T<float>(c, reps, ms6, bytes6);
+}
 
 int bm_time_kernels(bm_ctx *c, int mesh, int reps, double *ms4, double *bytes4)
 {

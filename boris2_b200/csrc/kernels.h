@@ -88,6 +88,7 @@ struct StageArgs {
     StepState *st;
     const T *Min, *Mbase;
     T *Mout, *copy_to, *ev_out, *Hout;
+    const T *Hd;         // demag field per cell from a multilayered convolution (added when set)
     int nev;
     const T *ev[6];
     double cev[6];

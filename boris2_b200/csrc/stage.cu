@@ -228,6 +228,10 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
                 for (int c = 0; c < 3; c++) H[c] += a.scale * *rp(c * rpb + r, x);
             }
+            if (a.Hd) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) H[c] += a.Hd[c * n + cell];
+            }
             if (exch) {
                 int y = row % ny, z = row / ny;
                 T mxp[3], mxm[3], myp[3], mym[3], mzp[3], mzm[3];

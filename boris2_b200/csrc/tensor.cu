@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 #include "kernels.h"
+#include "ml.h"
 
 #define BM_ASYMPT_DIST 40
 
@@ -283,3 +284,152 @@ int tensor_octant_device(double *oct_dev, int nx, int ny, int nz, double hx, dou
     k_tensor_octant<<<grid_for((long long)nx * ny * nz), 256, 0, s>>>(oct_dev, nx, ny, nz, hx / hm, hy / hm, hz / hm, farq_dev, nz == 1);
     return (int)cudaGetLastError();
 }
+
+// ============================================================================ multilayer kernels
+// Shifted kernels of the multilayered convolution (Boris/DemagKernelCollection_Calc.cpp):
+//   regular cells (3D, or 2D with equal thickness)  Boris/DemagTFunc_Shifted.cpp:6,120,235,343
+//   2D, source and destination thickness differ    Boris/DemagTFunc_Irregular.cpp:4,121
+// evaluated per grid offset (i, j, k) in (-n, n) on each axis with the shift added, near field
+// by exact Newell sums, far field (beyond 40 cells, measured with the shift) by this project's
+// expansion. The irregular sums follow the reference's combination: xx, yy take z in
+// {D-s, D, D+d, D+d-s}, zz, xy, xz, yz take z in {D-d, D, D+s, D+s-d} (D the shift, s and d the
+// source and destination thickness); the irregular far field is the destination-cell
+// expansion at z = D scaled by the source thickness, as the reference computes it.
+struct MLTP {
+    double hs[3], hd[3], sh[3];
+    int irregular;
+};
+
+__device__ __forceinline__ double floor_r(double v) { return floor(v + 1e-4); }
+
+// 36-point irregular sum for one component (c: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz)
+__device__ double ml_irregular(int c, double x, double y, double z, const MLTP &P)
+{
+    const double hx = P.hd[0], hy = P.hd[1], s = P.hs[2], d = P.hd[2];
+    const bool setA = (c < 2);
+    const double zq[4] = {setA ? z - s : z - d, z, setA ? z + d : z + s, setA ? z + d - s : z + s - d};
+    const double wz[4] = {-1.0, 1.0, -1.0, 1.0};
+    const double cw[3] = {-1.0, 2.0, -1.0};
+    double v[36];
+    int m = 0;
+    for (int a = -1; a <= 1; a++)
+        for (int b = -1; b <= 1; b++)
+            for (int q = 0; q < 4; q++) {
+                double w = cw[a + 1] * cw[b + 1] * wz[q], val;
+                switch (c) {
+                case 0: val = nf(x + a * hx, y + b * hy, zq[q]); break;
+                case 1: val = nf(y + a * hy, x + b * hx, zq[q]); break;
+                case 2: val = nf(zq[q], y + a * hy, x + b * hx); break;
+                case 3: val = ng(x + a * hx, y + b * hy, zq[q]); break;
+                case 4: val = ng(x + a * hx, zq[q], y + b * hy); break;
+                default: val = ng(y + a * hy, zq[q], x + b * hx); break;
+                }
+                v[m++] = w * val;
+            }
+    return -csum_d(v, 36) / (4.0 * M_PI * hx * hy * d);
+}
+
+// D6[c * np + p] for the (2n-1)^3 box of offsets, p the position on the N grid
+__global__ void k_ml_tensor(double *D6, long long np, MLTP P, int nx, int ny, int nz, int Nx, int Ny, int Nz,
+                            const double *__restrict__ farq)
+{
+    const long long bx = 2 * nx - 1, by = 2 * ny - 1, bz = 2 * nz - 1;
+    const long long nb = bx * by * bz;
+    const bool two_d = (nz == 1);
+    const double *h = P.irregular ? P.hd : P.hs;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t % bx) - (nx - 1);
+        int j = (int)((t / bx) % by) - (ny - 1);
+        int k = (int)(t / (bx * by)) - (nz - 1);
+        double is = fabs(i + P.sh[0] / h[0]), js = fabs(j + P.sh[1] / h[1]), ks = fabs(k + P.sh[2] / h[2]);
+        bool far = ((int)floor_r(is) >= BM_ASYMPT_DIST || (int)floor_r(js) >= BM_ASYMPT_DIST || (int)floor_r(ks) >= BM_ASYMPT_DIST ||
+                    (int)floor_r(is * is + js * js + ks * ks) >= BM_ASYMPT_DIST * BM_ASYMPT_DIST);
+        double x = i * h[0] + P.sh[0], y = j * h[1] + P.sh[1], z = k * h[2] + P.sh[2];
+        double v[6];
+        if (far) {
+            double R = sqrt(x * x + y * y + z * z);
+            double V = h[0] * h[1] * h[2] / (4.0 * M_PI);
+            if (P.irregular) V *= P.hs[2];
+            for (int c = 0; c < 6; c++) v[c] = V * far_eval(farq + c * BM_FARQ_PER_COMP, x / R, y / R, z / R, R);
+        } else if (!P.irregular) {
+            v[0] = -newellL<false>(x, y, z, h[0], h[1], h[2]);
+            v[1] = -newellL<false>(y, x, z, h[1], h[0], h[2]);
+            v[2] = -newellL<false>(z, y, x, h[2], h[1], h[0]);
+            v[3] = -newellL<true>(x, y, z, h[0], h[1], h[2]);
+            v[4] = -newellL<true>(x, z, y, h[0], h[2], h[1]);
+            v[5] = -newellL<true>(y, z, x, h[1], h[2], h[0]);
+        } else {
+            for (int c = 0; c < 6; c++) v[c] = ml_irregular(c, x, y, z, P);
+        }
+        if (two_d && P.sh[0] == 0.0 && P.sh[1] == 0.0 && P.sh[2] == 0.0) { v[4] = 0.0; v[5] = 0.0; }
+        long long p = (long long)((i + Nx) % Nx) + (long long)((j + Ny) % Ny) * Nx + (long long)((k + Nz) % Nz) * Nx * Ny;
+        for (int c = 0; c < 6; c++) D6[c * np + p] = v[c];
+    }
+}
+
+__global__ void k_ml_to_complex(cpx<double> *F, const double *__restrict__ D, long long np)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x)
+        F[p] = mk<double>(D[p], 0.0);
+}
+
+// complex spectra of one component: z-shifted kernels keep ky <= Ny/2, kz <= Nz/2 (the rest
+// follows from the x/y parity and the Hermitian symmetry); full kernels keep every ky, kz
+template <typename T>
+__global__ void k_ml_extract(cpx<T> *K, const cpx<double> *__restrict__ F, int kind, int Nx, int Ny, int Nz)
+{
+    const int Kx1 = Nx / 2 + 1;
+    const int ny = (kind == BM_MLK_ZSHIFT) ? Ny / 2 + 1 : Ny;
+    const int nzk = (kind == BM_MLK_ZSHIFT) ? Nz / 2 + 1 : Nz;
+    const long long nk = (long long)Kx1 * ny * nzk;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nk; q += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(q % Kx1);
+        int j = (int)((q / Kx1) % ny);
+        int k = (int)(q / ((long long)Kx1 * ny));
+        cpx<double> v = F[(long long)i + (long long)j * Nx + (long long)k * Nx * Ny];
+        K[q] = mk<T>((T)v.x, (T)v.y);
+    }
+}
+
+template <typename T>
+int build_ml_kernel_device(T *K, const MLKernelSpec &spec, const int *nc, const int *N, const double *farq_dev,
+                           const cpx<double> *twx, const cpx<double> *twy, const cpx<double> *twz, cudaStream_t s)
+{
+    const int Nx = N[0], Ny = N[1], Nz = N[2];
+    if (spec.kind == BM_MLK_SELF)
+        return build_kernels_device<T>(K, nc[0], nc[1], nc[2], Nx, Ny, Nz, spec.hd[0], spec.hd[1], spec.hd[2], farq_dev, twx,
+                                       twy, twz, s);
+    const long long np = (long long)Nx * Ny * Nz;
+    double *D6 = nullptr;
+    cpx<double> *F = nullptr;
+    if (cudaMalloc(&D6, sizeof(double) * 6 * np) != cudaSuccess) return 2;
+    if (cudaMalloc(&F, sizeof(cpx<double>) * np) != cudaSuccess) { cudaFree(D6); return 2; }
+    cudaMemsetAsync(D6, 0, sizeof(double) * 6 * np, s);
+    MLTP P;
+    for (int a = 0; a < 3; a++) { P.hs[a] = spec.hs[a]; P.hd[a] = spec.hd[a]; P.sh[a] = spec.shift[a]; }
+    P.irregular = spec.irregular;
+    long long nb = (long long)(2 * nc[0] - 1) * (2 * nc[1] - 1) * (2 * nc[2] - 1);
+    k_ml_tensor<<<grid_for(nb), 256, 0, s>>>(D6, np, P, nc[0], nc[1], nc[2], Nx, Ny, Nz, farq_dev);
+    FFTPlan px, py, pz;
+    bm_make_plan(Nx, px); bm_make_plan(Ny, py); bm_make_plan(Nz, pz);
+    const int Kx1 = Nx / 2 + 1;
+    const long long nk = (spec.kind == BM_MLK_ZSHIFT) ? (long long)Kx1 * (Ny / 2 + 1) * (Nz / 2 + 1) : (long long)Kx1 * Ny * Nz;
+    int rc = 0;
+    for (int c = 0; c < 6 && !rc; c++) {
+        k_ml_to_complex<<<grid_for(np), 256, 0, s>>>(F, D6 + c * np, np);
+        if (Nx > 1) rc |= launch_fft_strided<double>(F, px, twx, 1, Nx, Ny * Nz, 0, 1, false, s);
+        if (Ny > 1) rc |= launch_fft_strided<double>(F, py, twy, Nx, 1, Nx, (long long)Nx * Ny, Nz, false, s);
+        if (Nz > 1) rc |= launch_fft_strided<double>(F, pz, twz, (long long)Nx * Ny, 1, Nx * Ny, 0, 1, false, s);
+        k_ml_extract<T><<<grid_for(nk), 256, 0, s>>>(reinterpret_cast<cpx<T> *>(K) + c * nk, F, spec.kind, Nx, Ny, Nz);
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFree(D6);
+    cudaFree(F);
+    if (e != cudaSuccess) return 3;
+    return rc ? 4 : (int)cudaGetLastError();
+}
+
+template int build_ml_kernel_device<float>(float *, const MLKernelSpec &, const int *, const int *, const double *,
+                                           const cpx<double> *, const cpx<double> *, const cpx<double> *, cudaStream_t);
+template int build_ml_kernel_device<double>(double *, const MLKernelSpec &, const int *, const int *, const double *,
+                                            const cpx<double> *, const cpx<double> *, const cpx<double> *, cudaStream_t);

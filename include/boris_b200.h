@@ -95,6 +95,41 @@ int bm_set_astepctrl(bm_ctx *ctx, double err_fail, double dT_incr, double dT_min
 /* Precision: BM_FP64 or BM_MIXED (default BM_MIXED). Must be set before the first run. */
 int bm_set_precision(bm_ctx *ctx, int precision);
 
+/* Multilayered convolution (SDemag in multilayer mode). The demag modules of all meshes with
+ * BM_DEMAG become the layers of one convolution on a common grid: each layer's M is moved to the
+ * common grid by the reference's weighted mesh transfer, the layers' spectra are combined by an
+ * L x L set of kernels (self, z-shifted, full), and the field is moved back into every mesh.
+ * Mesh positions come from the origins given to bm_add_mesh.
+ *   mode BM_ML_OFF   every mesh its own demag convolution (default)
+ *        BM_ML_3D    `multiconvolution 1`: 3D common grid (2D when every mesh is one cell thick)
+ *        BM_ML_2D    `2dmulticonvolution 1`: n_common.z = 1, each mesh one layer
+ *        BM_ML_2D_LAYERED `2dmulticonvolution 2`: n_common.z = 1, every z cell layer its own layer
+ *   n_common NULL for the default (largest cell count of the meshes per axis, `ncommonauto`),
+ *        else 3 ints (`ncommon`; n_common.z = 1 then selects 2D).
+ * Replaces SDemag::Set_Multilayered_Convolution / Set_2D_Multilayered_Convolution / Set_n_common
+ * (Boris/SDemag.cpp:323,341,362; commands Boris/Commands.cpp:1704,1720). At most 8 layers;
+ * n_common.z at most 32. */
+#define BM_ML_OFF (-1)
+#define BM_ML_3D 0
+#define BM_ML_2D 1
+#define BM_ML_2D_LAYERED 2
+int bm_set_multiconvolution(bm_ctx *ctx, int mode, const int *n_common);
+
+/* Geometry of the multilayered convolution once prepared (after a run or field call, or
+ * bm_prepare): layer count, n_common, and per layer the mesh, whether it is moved by mesh
+ * transfer, the convolution rectangle (start, end; 6 doubles) and per (layer, source) pair the
+ * kernel kind (1 self, 2 z-shifted, 3 z-shifted reused for the opposite shift, 4 full). Arrays
+ * sized for 8 layers may be passed; any pointer may be NULL. */
+int bm_ml_info(bm_ctx *ctx, int *L, int *nc3, int *layer_mesh, int *transfer, double *rects6, int *kinds);
+
+/* Device time (ms per launch sequence, CUDA events) and algorithmic bytes of the parts of one
+ * multilayer demag evaluation: [0] transfer in + x forward, [1] y forward, [2] z pass with the
+ * L x L products, [3] y inverse, [4] x inverse + transfer out, [5] the whole evaluation. */
+int bm_ml_time_kernels(bm_ctx *ctx, int reps, double *ms6, double *bytes6);
+
+/* Allocate and build everything for the current configuration now (kernels, tiles). */
+int bm_prepare(bm_ctx *ctx);
+
 /* Magnetization M (A/m, |M| = Ms), AoS doubles, 3 * n values. Replaces writes/reads of
  * MeshBase::M (VEC_VC<DBL3>, Boris/Mesh.h). Setting M un-primes RKDP54 as a restart does. */
 int bm_set_m(bm_ctx *ctx, int mesh, const double *M);
