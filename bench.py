@@ -372,7 +372,7 @@ def main():
         kernels = {names[i]: {"ms": kms[i], "GB/s": kbytes[i] / (kms[i] * 1e-3) / 1e9} for i in range(5) if kms[i] > 0}
         kernels["demag_evaluation"] = {"ms": kms[5], "GB/s": kbytes[5] / (kms[5] * 1e-3) / 1e9,
                                        "frac": kbytes[5] / (kms[5] * 1e-3) / 1e9 / peak}
-        tiles = None
+        tiles = {"zmid_ml_W": c.ml_tile()}
     else:
         kms, kbytes = c.time_kernels(0, reps=20)
         names = ["ymid2d" if cfg["n"][2] == 1 else "yfwd", "zmid", "yinv", "stage"]

@@ -93,6 +93,7 @@ _SIGS = {
     "bm_ml_info": (_I, [_P, _IP, _IP, _IP, _IP, _DP, _IP]),
     "bm_prepare": (_I, [_P]),
     "bm_ml_time_kernels": (_I, [_P, _I, _DP, _DP]),
+    "bm_ml_tile": (_I, [_P, _IP]),
 }
 
 
@@ -210,6 +211,12 @@ class Context:
 
     def prepare(self):
         _check(lib().bm_prepare(self._h))
+
+    def ml_tile(self):
+        """Columns per block of the fused multilayer z pass."""
+        w = _I()
+        _check(lib().bm_ml_tile(self._h, ctypes.byref(w)))
+        return w.value
 
     def ml_time_kernels(self, reps=10):
         """ms and algorithmic bytes of the parts of one multilayer demag evaluation: transfer

@@ -567,6 +567,8 @@ std::vector<T> as_type(const std::vector<double> &v)
     return o;
 }
 
+template <typename T> MLZArgs<T> ml_zargs(bm_ctx *c, int W, int gate);
+
 template <typename T>
 int prepare_ml(bm_ctx *c)
 {
@@ -632,12 +634,28 @@ int prepare_ml(bm_ctx *c)
     cudaFree(tx); cudaFree(ty); cudaFree(tz);
     if (rc) return fail(BM_ECUDA, "multilayer kernel build failed (" + std::to_string(rc) + ")");
     if ((rc = upload_table<T>(&r.twz, g.N[2], false, s))) return rc;
-    // z pass tile: columns per block
+    CK(cudaStreamSynchronize(s));
+    // z pass tile: columns per block, the fastest of the widths that fit (timed on the layer
+    // spectra, which the first evaluation rewrites)
     const int lim = bm_lb<T>::v, LX = g.N[0] / 2;
-    int W = 16;
-    while (W > 1 && (6 * L * W > lim || zmid_ml_smem<T>(L, g.N[2], W) > 96 * 1024)) W /= 2;
-    while (W > 1 && W > LX) W /= 2;
-    r.W = W;
+    r.W = 0;
+    float best = 1e30f;
+    const char *fw = getenv("BM_ML_W");   // fixed width (profiling runs)
+    if (fw && atoi(fw) >= 1 && (atoi(fw) & (atoi(fw) - 1)) == 0) {
+        r.W = atoi(fw);
+        return 0;
+    }
+    for (int W = 1; W <= 32 && W <= LX; W *= 2) {
+        MLZArgs<T> z = ml_zargs<T>(c, W, BM_GATE_ALWAYS);
+        z.st = nullptr;
+        if (((6 * L * W + 31) & ~31) > lim || zmid_ml_smem<T>(L, g.N[2], W, z.ksm) > 200 * 1024) continue;
+        if (!r.W) r.W = W;
+        if (!c->autotune) continue;
+        float t = time_launches(s, [&]() { return launch_zmid_ml<T>(z, s); }, 3);
+        if (t < best) { best = t; r.W = W; }
+    }
+    if (!r.W) return fail(BM_EUNSUPPORTED, "multilayer: no z-pass tile fits");
+    cudaGetLastError();
     CK(cudaStreamSynchronize(s));
     return 0;
 }
@@ -752,6 +770,37 @@ Mesh &ml_grid(bm_ctx *c, int l)
 // M from buffer bi of every mesh. Without a multilayered convolution: each mesh's own y/z
 // passes. With one: transfer in and x FFT of the transfer layers, y passes of every layer, the
 // fused z pass with the L x L products, inverse y, then inverse x and transfer out into Hd.
+// arguments of the fused multilayer z pass for tile width W: layer spectra, the unique kernels
+// with their shared-memory tile offsets, and the (dest, src) -> kernel map
+template <typename T>
+MLZArgs<T> ml_zargs(bm_ctx *c, int W, int gate)
+{
+    MLRun &r = *c->ml;
+    const MLGeom &g = r.g;
+    const int L = g.L;
+    MLZArgs<T> z;
+    memset(&z, 0, sizeof(z));
+    for (int l = 0; l < L; l++) z.S2[l] = (cpx<T> *)ml_grid(c, l).S2;
+    z.K = (const T *)r.K;
+    int sm = 0;
+    z.nu = (int)g.kernels.size();
+    for (int u = 0; u < z.nu; u++) {
+        z.u[u].kind = g.kernels[u].kind;
+        z.u[u].off = (long long)g.kernels[u].off;
+        z.u[u].sm = sm;
+        sm += zmid_ml_tile_bytes<T>(g.kernels[u].kind, g.N[2], W);
+    }
+    z.ksm = sm;
+    for (int i = 0; i < L * L; i++) {
+        z.pu[i] = (unsigned char)g.pair_kernel[i];
+        z.pinv[i] = (unsigned char)g.pair_inv[i];
+    }
+    z.twz = (const cpx<T> *)r.twz;
+    z.L = L; z.nz = g.nc[2]; z.Ny = g.N[1]; z.Nz = g.N[2]; z.LX = g.N[0] / 2; z.W = W;
+    z.st = c->st; z.gate = gate;
+    return z;
+}
+
 // multilayer parts: 0 transfer in + x forward, 1 y forward, 2 z pass + products, 3 y inverse,
 // 4 x inverse + transfer out
 template <typename T>
@@ -783,20 +832,7 @@ int ml_enqueue_part(bm_ctx *c, int part, int gate, int bi, int *count)
         (*count)++;
     }
     if (part == 2) {
-        MLZArgs<T> z;
-        memset(&z, 0, sizeof(z));
-        for (int l = 0; l < L; l++) z.S2[l] = (cpx<T> *)ml_grid(c, l).S2;
-        z.K = (const T *)r.K;
-        for (int d = 0; d < L; d++)
-            for (int q = 0; q < L; q++) {
-                const MLKernelSpec &K = g.kernels[g.pair_kernel[d * L + q]];
-                z.kd[d * L + q].kind = K.kind;
-                z.kd[d * L + q].inv = g.pair_inv[d * L + q];
-                z.kd[d * L + q].off = (long long)K.off;
-            }
-        z.twz = (const cpx<T> *)r.twz;
-        z.L = L; z.nz = g.nc[2]; z.Ny = g.N[1]; z.Nz = g.N[2]; z.LX = g.N[0] / 2; z.W = r.W;
-        z.st = c->st; z.gate = gate;
+        MLZArgs<T> z = ml_zargs<T>(c, r.W, gate);
         CKL(launch_zmid_ml<T>(z, s), "multilayer z pass");
         (*count)++;
     }
@@ -1278,6 +1314,15 @@ int bm_ml_info(bm_ctx *c, int *L, int *nc3, int *layer_mesh, int *transfer, doub
             for (int a = 0; a < 3; a++) { rects6[6 * l + a] = g.layers[l].rs[a]; rects6[6 * l + 3 + a] = g.layers[l].re[a]; }
         if (kinds) for (int q = 0; q < g.L; q++) kinds[l * g.L + q] = g.pair_kind[l * g.L + q];
     }
+    return 0;
+}
+
+int bm_ml_tile(bm_ctx *c, int *W)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (int rc = prepare(c)) return rc;
+    if (!c->ml) return fail(BM_ESTATE, "multilayered convolution is off");
+    if (W) *W = c->ml->W;
     return 0;
 }
 

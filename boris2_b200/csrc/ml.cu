@@ -59,83 +59,131 @@ template int launch_ml_gather<float>(float *, long long, long long, const float 
 template int launch_ml_gather<double>(double *, long long, long long, const double *, long long, const int *, const int *,
                                       const double *, StepState *, int, cudaStream_t);
 
-// ------------------------------------------------------------------------------ kernel values
-// 6 complex components (xx, yy, zz, xy, xz, yz) of one kernel at frequency (kx, ky, kz),
-// kx in [0, Nx/2], ky in [0, Ny), kz in [0, Nz), expanded from the stored part:
-//   self     real; Kxy odd in ky, Kxz odd in kz, Kyz odd in ky and kz
-//   z-shift  Kxy, Kyz odd in ky; K(-kz) = conj(K(kz)) for xx, yy, zz, xy and -conj(K(kz)) for xz, yz
-//   full     stored as is
-// inv: the kernel was computed for the opposite z shift; Kxz and Kyz change sign.
-template <typename T>
-__device__ __forceinline__ void ml_kfetch(const T *__restrict__ K, const MLKDesc &d, int kx, int ky, int kz, int Kx1, int Ny,
-                                          int Nz, cpx<T> k[6])
-{
-    const int Ky1 = Ny / 2 + 1, Kz1 = Nz / 2 + 1;
-    const bool ylo = ky <= Ny / 2, zlo = kz <= Nz / 2;
-    const int aky = ylo ? ky : Ny - ky, akz = zlo ? kz : Nz - kz;
-    const T sy = ylo ? (T)1 : (T)-1, sz = zlo ? (T)1 : (T)-1;
-    if (d.kind == BM_MLK_SELF) {
-        const long long nk = (long long)Kx1 * Ky1 * Kz1;
-        const T *b = K + d.off + ((long long)akz * Ky1 + aky) * Kx1 + kx;
-#pragma unroll
-        for (int c = 0; c < 6; c++) k[c] = mk<T>(__ldg(b + c * nk), (T)0);
-        k[3].x *= sy;
-        k[4].x *= sz;
-        k[5].x *= sy * sz;
-    } else if (d.kind == BM_MLK_ZSHIFT) {
-        const long long nk = (long long)Kx1 * Ky1 * Kz1;
-        const cpx<T> *b = reinterpret_cast<const cpx<T> *>(K + d.off) + ((long long)akz * Ky1 + aky) * Kx1 + kx;
-#pragma unroll
-        for (int c = 0; c < 6; c++) {
-            cpx<T> v = b[c * nk];
-            if (!zlo) {
-                v = conj(v);
-                if (c >= 4) v = mk<T>(-v.x, -v.y);
-            }
-            if (c == 3 || c == 5) v = cscale(v, sy);
-            k[c] = v;
-        }
-    } else {
-        const long long nk = (long long)Kx1 * Ny * Nz;
-        const cpx<T> *b = reinterpret_cast<const cpx<T> *>(K + d.off) + ((long long)kz * Ny + ky) * Kx1 + kx;
-#pragma unroll
-        for (int c = 0; c < 6; c++) k[c] = b[c * nk];
-    }
-    if (d.inv) {
-        k[4] = mk<T>(-k[4].x, -k[4].y);
-        k[5] = mk<T>(-k[5].x, -k[5].y);
-    }
-}
-
-// h += K m for the symmetric complex 3x3 kernel
-template <typename T>
-__device__ __forceinline__ void ml_kmac(const cpx<T> k[6], const cpx<T> m[3], cpx<T> h[3])
-{
-    h[0] = h[0] + cmul(k[0], m[0]) + cmul(k[3], m[1]) + cmul(k[4], m[2]);
-    h[1] = h[1] + cmul(k[3], m[0]) + cmul(k[1], m[1]) + cmul(k[5], m[2]);
-    h[2] = h[2] + cmul(k[4], m[0]) + cmul(k[5], m[1]) + cmul(k[2], m[2]);
-}
-
 // ------------------------------------------------------------------------------ fused z pass
-// Block: W columns from kx0, the pencil pair ky / Ny - ky, every layer and component.
-// Thread (l, c, p, w), w fastest, owns one z line of NZ points in registers. Shared memory:
-// In [L][3][2][NZ][W] (forward spectra), Out [L][3][2][NZ][W] (products per destination).
+// Block: W columns from kx0, the pencil pair ky / Ny - ky (ky <= Ny/2), every layer and component.
+// Thread (l, c, p, w), w fastest, owns one z line of NZ points in registers: it loads layer l's
+// component c of pencil p, transforms it forward, and after the shared exchange computes layer
+// l's output of component c on that same line, row c of sum_s K_ls In_s, then transforms back.
+// Shared memory: In [L][3][2][NZ][W], then one tile per unique kernel with its stored values at
+// this block's columns (and at the x Nyquist column kx = Nx/2 that column 0 carries), copied by
+// cp.async while the forward transforms run. The stored part and the symmetries that give the
+// rest (true DFT values of the real-space tensors):
+//   self     ky <= Ny/2, kz <= Nz/2, real; Kxy odd in ky, Kxz odd in kz, Kyz odd in both
+//   z-shift  ky <= Ny/2, kz <= Nz/2; Kxy, Kyz odd in ky; K(-kz) = conj(K(kz)) for xx, yy, zz,
+//            xy and -conj(K(kz)) for xz, yz
+//   full     every ky and kz
+// pinv: the kernel was computed for the opposite z shift, so Kxz and Kyz change sign.
+// The symmetry signs are per (source, component) pairs of multipliers for the real and the
+// imaginary part, one for kz <= Nz/2 and one for kz > Nz/2, applied in the unrolled kz loop.
+
+// multipliers (re, im) of a stored self / z-shift value for kz <= Nz/2 (lo) and kz > Nz/2 (hi)
+template <typename T>
+__device__ __forceinline__ void ml_signs(int kind, int comp, bool ylo, bool inv, cpx<T> &lo, cpx<T> &hi)
+{
+    T sy = (!ylo && (comp == 3 || comp == 5)) ? (T)-1 : (T)1;
+    if (inv && comp >= 4) sy = -sy;
+    lo = mk<T>(sy, sy);
+    if (kind == BM_MLK_SELF) hi = mk<T>(comp >= 4 ? -sy : sy, (T)0);
+    else hi = (comp >= 4) ? mk<T>(-sy, sy) : mk<T>(sy, -sy);
+    if (kind == BM_MLK_SELF) lo.y = (T)0;
+}
+
+// one stored value of a kernel at (comp, kz, pencil) of column kxc (kxc = -1: Nyquist column)
 template <typename T, int NZ>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_ml(MLZArgs<T> a)
+__device__ __forceinline__ cpx<T> ml_tile_get(const unsigned char *tile, int kind, int comp, int kz, int p, bool ylo, bool inv,
+                                              int mainb, int w, int lw)
+{
+    if (kind == BM_MLK_FULL) {
+        const cpx<T> *t = reinterpret_cast<const cpx<T> *>(tile);
+        cpx<T> v = (w >= 0) ? t[(((comp * NZ + kz) * 2 + p) << lw) + w]
+                            : reinterpret_cast<const cpx<T> *>(tile + mainb)[(comp * NZ + kz) * 2 + p];
+        if (inv && comp >= 4) v = mk<T>(-v.x, -v.y);
+        return v;
+    }
+    constexpr int KZ1 = NZ / 2 + 1;
+    const int akz = kz <= NZ / 2 ? kz : NZ - kz;
+    const cpx<T> *t = reinterpret_cast<const cpx<T> *>(tile);
+    cpx<T> v = (w >= 0) ? t[((comp * KZ1 + akz) << lw) + w] : reinterpret_cast<const cpx<T> *>(tile + mainb)[comp * KZ1 + akz];
+    cpx<T> lo, hi;
+    ml_signs<T>(kind, comp, ylo, inv, lo, hi);
+    const cpx<T> sg = kz <= NZ / 2 ? lo : hi;
+    return mk<T>(v.x * sg.x, v.y * sg.y);
+}
+
+template <int NZ> struct zml_bounds {
+    static constexpr int blocks = NZ <= 16 ? 2 : 1;
+};
+
+template <typename T, int NZ>
+__global__ void __launch_bounds__(bm_lb<T>::v, zml_bounds<NZ>::blocks) k_zmid_ml(MLZArgs<T> a)
 {
     if (ml_gated_out<T>(a.st, a.gate)) return;
-    extern __shared__ unsigned char smraw[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    constexpr int KZ1 = NZ / 2 + 1;
     const int W = a.W, L = a.L, Ny = a.Ny, nz = a.nz, LX = a.LX;
     const int lw = __ffs(W) - 1;
-    const int Kx1 = LX + 1;
+    const int Kx1 = LX + 1, Ky1 = Ny / 2 + 1;
     cpx<T> *In = reinterpret_cast<cpx<T> *>(smraw);
-    cpx<T> *Out = In + (size_t)L * 6 * NZ * W;
+    unsigned char *Ks = smraw + (size_t)L * 6 * NZ * W * sizeof(cpx<T>);
     auto IDX = [&](int l, int c, int p, int e, int w) -> int { return ((((l * 3 + c) * 2 + p) * NZ + e) << lw) + w; };
     const int kx0 = blockIdx.x * W;
     const int ky = blockIdx.y, kym = (Ny - ky) % Ny;
     const bool single = (ky == kym);
     const int np = single ? 1 : 2;
     const int tid = threadIdx.x, nt = blockDim.x;
+    // kernel tiles (async)
+    for (int u = 0; u < a.nu; u++) {
+        const MLUDesc d = a.u[u];
+        cpx<T> *t = reinterpret_cast<cpx<T> *>(Ks + d.sm);
+        const int mainb = zmid_ml_tile_main<T>(d.kind, NZ, W);
+        cpx<T> *tn = reinterpret_cast<cpx<T> *>(Ks + d.sm + mainb);
+        if (d.kind == BM_MLK_FULL) {
+            const long long nk = (long long)Kx1 * Ny * NZ;
+            const cpx<T> *K = reinterpret_cast<const cpx<T> *>(a.K + d.off);
+            for (int i = tid; i < 12 * NZ * W; i += nt) {
+                const int w = i & (W - 1), r = i >> lw;
+                const int pp = r & 1, kz = (r >> 1) % NZ, comp = (r >> 1) / NZ;
+                const int kx = kx0 + w;
+                const bool ok = kx < LX && pp < np;
+                cp_async_cpx<T>(&t[i], ok ? &K[comp * nk + ((long long)kz * Ny + (pp ? kym : ky)) * Kx1 + kx] : K, ok);
+            }
+            if (kx0 == 0)
+                for (int i = tid; i < 12 * NZ; i += nt) {
+                    const int pp = i & 1, kz = (i >> 1) % NZ, comp = (i >> 1) / NZ;
+                    const bool ok = pp < np;
+                    cp_async_cpx<T>(&tn[i], ok ? &K[comp * nk + ((long long)kz * Ny + (pp ? kym : ky)) * Kx1 + LX] : K, ok);
+                }
+        } else {
+            const long long nk = (long long)Kx1 * Ky1 * KZ1;
+            const bool self = d.kind == BM_MLK_SELF;
+            for (int i = tid; i < 6 * KZ1 * W; i += nt) {
+                const int w = i & (W - 1), r = i >> lw, kz = r % KZ1, comp = r / KZ1;
+                const int kx = kx0 + w;
+                const long long q = comp * nk + ((long long)kz * Ky1 + ky) * Kx1 + kx;
+                if (self) {
+                    // real value into .x, zero into .y
+                    cp_async_real<T>(&t[i].x, kx < LX ? a.K + d.off + q : a.K, kx < LX);
+                    cp_async_real<T>(&t[i].y, a.K, false);
+                } else {
+                    const cpx<T> *K = reinterpret_cast<const cpx<T> *>(a.K + d.off);
+                    cp_async_cpx<T>(&t[i], kx < LX ? &K[q] : K, kx < LX);
+                }
+            }
+            if (kx0 == 0)
+                for (int i = tid; i < 6 * KZ1; i += nt) {
+                    const int kz = i % KZ1, comp = i / KZ1;
+                    const long long q = comp * nk + ((long long)kz * Ky1 + ky) * Kx1 + LX;
+                    if (self) {
+                        cp_async_real<T>(&tn[i].x, a.K + d.off + q, true);
+                        cp_async_real<T>(&tn[i].y, a.K, false);
+                    } else {
+                        cp_async_cpx<T>(&tn[i], reinterpret_cast<const cpx<T> *>(a.K + d.off) + q, true);
+                    }
+                }
+        }
+    }
+    cp_async_commit();
+    // forward transforms of the owned lines
     const int w = tid & (W - 1);
     const int p = (tid >> lw) & 1;
     const int lc = tid >> (lw + 1);
@@ -160,61 +208,80 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_ml(MLZArgs<T> a)
 #pragma unroll
         for (int e = 0; e < NZ; e++) In[IDX(l, c, p, e, w)] = v[e];
     }
+    cp_async_wait_all();
     __syncthreads();
-    // products for every destination
-    const int tot = L * np * NZ * W;
-    for (int t = tid; t < tot; t += nt) {
-        const int ww = t & (W - 1);
-        int r = t >> lw;
-        const int kz = r % NZ;
-        r /= NZ;
-        const int pp = r % np, d = r / np;
-        const int kxx = kx0 + ww;
-        if (kxx >= LX) continue;
-        if (kxx == 0) {
-            // packed DC / Nyquist column: pair (p = 0, kz) with (mirror pencil, -kz)
-            if (pp == 1) continue;
-            if (single && kz > NZ / 2) continue;
-            const int pm = single ? 0 : 1;
-            const int kzm = (NZ - kz) % NZ;
-            cpx<T> Ap[3] = {mk<T>(0, 0), mk<T>(0, 0), mk<T>(0, 0)}, Bp[3] = {mk<T>(0, 0), mk<T>(0, 0), mk<T>(0, 0)};
-            for (int s = 0; s < L; s++) {
-                cpx<T> A[3], B[3];
+    const int cmp[3] = {c == 0 ? 0 : (c == 1 ? 3 : 4), c == 0 ? 3 : (c == 1 ? 1 : 5), c == 0 ? 4 : (c == 1 ? 5 : 2)};
+    // row c of sum_s K_ls In_s on this line
+    if (own && kx != 0) {
+#pragma unroll
+        for (int e = 0; e < NZ; e++) v[e] = mk<T>(0, 0);
+        for (int s = 0; s < L; s++) {
+            const MLUDesc d = a.u[a.pu[l * L + s]];
+            const bool inv = a.pinv[l * L + s] != 0;
+            const cpx<T> *t = reinterpret_cast<const cpx<T> *>(Ks + d.sm);
+            if (d.kind == BM_MLK_FULL) {
 #pragma unroll
                 for (int cc = 0; cc < 3; cc++) {
-                    cpx<T> C = In[IDX(s, cc, 0, kz, ww)], cj = conj(In[IDX(s, cc, pm, kzm, ww)]);
-                    A[cc] = cscale(C + cj, (T)0.5);
-                    B[cc] = cscale(mul_mi(C - cj), (T)0.5);
+                    const T sg = (inv && cmp[cc] >= 4) ? (T)-1 : (T)1;
+                    const cpx<T> *row = t + ((cmp[cc] * NZ * 2 + p) << lw) + w;
+                    const cpx<T> *in = In + IDX(s, cc, p, 0, w);
+#pragma unroll
+                    for (int kz = 0; kz < NZ; kz++) v[kz] = v[kz] + cscale(cmul(row[(kz * 2) << lw], in[kz << lw]), sg);
                 }
-                cpx<T> k0[6], kn[6];
-                ml_kfetch<T>(a.K, a.kd[d * L + s], 0, ky, kz, Kx1, Ny, NZ, k0);
-                ml_kfetch<T>(a.K, a.kd[d * L + s], LX, ky, kz, Kx1, Ny, NZ, kn);
-                ml_kmac<T>(k0, A, Ap);
-                ml_kmac<T>(kn, B, Bp);
-            }
-            const bool self = single && (kzm == kz);
+            } else {
 #pragma unroll
-            for (int cc = 0; cc < 3; cc++) {
-                Out[IDX(d, cc, 0, kz, ww)] = Ap[cc] + mul_i(Bp[cc]);
-                if (!self) Out[IDX(d, cc, pm, kzm, ww)] = conj(Ap[cc]) + mul_i(conj(Bp[cc]));
-            }
-        } else {
-            const int kyq = pp ? kym : ky;
-            cpx<T> h[3] = {mk<T>(0, 0), mk<T>(0, 0), mk<T>(0, 0)};
-            for (int s = 0; s < L; s++) {
-                cpx<T> m[3] = {In[IDX(s, 0, pp, kz, ww)], In[IDX(s, 1, pp, kz, ww)], In[IDX(s, 2, pp, kz, ww)]};
-                cpx<T> k[6];
-                ml_kfetch<T>(a.K, a.kd[d * L + s], kxx, kyq, kz, Kx1, Ny, NZ, k);
-                ml_kmac<T>(k, m, h);
-            }
+                for (int cc = 0; cc < 3; cc++) {
+                    cpx<T> lo, hi;
+                    ml_signs<T>(d.kind, cmp[cc], p == 0, inv, lo, hi);
+                    const cpx<T> *row = t + ((cmp[cc] * KZ1) << lw) + w;
+                    const cpx<T> *in = In + IDX(s, cc, p, 0, w);
 #pragma unroll
-            for (int cc = 0; cc < 3; cc++) Out[IDX(d, cc, pp, kz, ww)] = h[cc];
+                    for (int kz = 0; kz < NZ; kz++) {
+                        const int akz = kz <= NZ / 2 ? kz : NZ - kz;
+                        const cpx<T> sg = kz <= NZ / 2 ? lo : hi;
+                        const cpx<T> kr = row[akz << lw];
+                        v[kz] = v[kz] + cmul(mk<T>(kr.x * sg.x, kr.y * sg.y), in[kz << lw]);
+                    }
+                }
+            }
         }
     }
-    __syncthreads();
-    if (line) {
+    if (kx0 == 0) {
+        // column 0 packs the DC (kx = 0) and Nyquist (kx = Nx/2) spectra; both are unpacked with
+        // the Hermitian mirror (pencil 0, kz) <-> (pencil pm, -kz), multiplied and re-packed. The
+        // results go through a small shared buffer after the tiles so that the kz loop can stay
+        // rolled (only the first block column runs this).
+        cpx<T> *O = reinterpret_cast<cpx<T> *>(Ks + a.ksm);
+        if (own && kx == 0) {
+            const int pm = single ? 0 : 1;
+            for (int kz = 0; kz < NZ; kz++) {
+                const int kr = p == 0 ? kz : (NZ - kz) % NZ;   // frequency in pencil-0 terms
+                const int krm = (NZ - kr) % NZ;
+                cpx<T> acc = mk<T>(0, 0);
+                for (int s = 0; s < L; s++) {
+                    const MLUDesc d = a.u[a.pu[l * L + s]];
+                    const bool inv = a.pinv[l * L + s] != 0;
+                    const unsigned char *tile = Ks + d.sm;
+                    const int mainb = zmid_ml_tile_main<T>(d.kind, NZ, W);
+                    cpx<T> ap = mk<T>(0, 0), bp = mk<T>(0, 0);
+                    for (int cc = 0; cc < 3; cc++) {
+                        const cpx<T> C = In[IDX(s, cc, 0, kr, 0)], cj = conj(In[IDX(s, cc, pm, krm, 0)]);
+                        const cpx<T> A = cscale(C + cj, (T)0.5), B = cscale(mul_mi(C - cj), (T)0.5);
+                        const cpx<T> k0 = ml_tile_get<T, NZ>(tile, d.kind, cmp[cc], kr, 0, true, inv, mainb, 0, lw);
+                        const cpx<T> kn = ml_tile_get<T, NZ>(tile, d.kind, cmp[cc], kr, 0, true, inv, mainb, -1, lw);
+                        ap = ap + cmul(k0, A);
+                        bp = bp + cmul(kn, B);
+                    }
+                    acc = acc + (p == 0 ? ap + mul_i(bp) : conj(ap) + mul_i(conj(bp)));
+                }
+                O[((l * 3 + c) * 2 + p) * NZ + kz] = acc;
+            }
+        }
+        __syncthreads();
+        if (own && kx == 0) {
 #pragma unroll
-        for (int e = 0; e < NZ; e++) v[e] = Out[IDX(l, c, p, e, w)];
+            for (int e = 0; e < NZ; e++) v[e] = O[((l * 3 + c) * 2 + p) * NZ + e];
+        }
     }
     RegFFT<T, NZ, true>::run(v, a.twz, 1);
     if (own) {
@@ -230,7 +297,7 @@ static int launch_zmid_ml_t(const MLZArgs<T> &a, cudaStream_t s)
 {
     int nt = (6 * a.L * a.W + 31) & ~31;
     if (nt > bm_lb<T>::v) return 304;
-    size_t smem = zmid_ml_smem<T>(a.L, NZ, a.W);
+    size_t smem = zmid_ml_smem<T>(a.L, NZ, a.W, a.ksm);
     if (smem > 200 * 1024) return 305;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_zmid_ml<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -72,8 +72,10 @@ struct MLGeom {
 int ml_build_geometry(const std::vector<MLMeshIn> &meshes, int mode, const int *nc_user, MLGeom &g, std::string &err);
 
 // ------------------------------------------------------------------------------ device arguments
-struct MLKDesc {
-    int kind, inv;
+// one unique kernel as the z pass sees it: storage kind, element offset in the kernel buffer,
+// byte offset of its staged tile in shared memory
+struct MLUDesc {
+    int kind, sm;
     long long off;
 };
 
@@ -81,15 +83,35 @@ template <typename T>
 struct MLZArgs {
     cpx<T> *S2[BM_ML_MAXL];   // per layer [3][nz][Ny][LX]
     const T *K;               // kernel buffer
-    MLKDesc kd[BM_ML_MAXL * BM_ML_MAXL];
+    MLUDesc u[BM_ML_MAXL * BM_ML_MAXL];
+    unsigned char pu[BM_ML_MAXL * BM_ML_MAXL];     // (dest, src) -> unique kernel
+    unsigned char pinv[BM_ML_MAXL * BM_ML_MAXL];   // (dest, src) reuses the opposite z shift
     const cpx<T> *twz;
-    int L, nz, Ny, Nz, LX, W;
+    int L, nu, nz, Ny, Nz, LX, W;
+    int ksm;                  // bytes of staged kernel tiles
     StepState *st;
     int gate;
 };
 
+// bytes of one unique kernel's staged tile at a block's columns (complex values, 16-aligned):
+//   self, z-shift  [comp][kz <= Nz/2][W] and the Nyquist column [comp][kz <= Nz/2]
+//   full           [comp][kz][pencil][W] and the Nyquist column [comp][kz][pencil]
+template <typename T> BM_HD int zmid_ml_tile_main(int kind, int Nz, int W)
+{
+    size_t b = (kind == BM_MLK_FULL) ? (size_t)12 * Nz * W * sizeof(cpx<T>) : (size_t)6 * (Nz / 2 + 1) * W * sizeof(cpx<T>);
+    return (int)((b + 15) & ~(size_t)15);
+}
+template <typename T> BM_HD int zmid_ml_tile_bytes(int kind, int Nz, int W)
+{
+    size_t nyq = (kind == BM_MLK_FULL) ? (size_t)12 * Nz * sizeof(cpx<T>) : (size_t)6 * (Nz / 2 + 1) * sizeof(cpx<T>);
+    return zmid_ml_tile_main<T>(kind, Nz, W) + (int)((nyq + 15) & ~(size_t)15);
+}
+template <typename T> size_t zmid_ml_smem(int L, int Nz, int W, int ksm)
+{
+    // In, the kernel tiles, and the column-0 results [L][3][2][Nz]
+    return (size_t)L * 3 * 2 * Nz * W * sizeof(cpx<T>) + (size_t)ksm + (size_t)L * 6 * Nz * sizeof(cpx<T>);
+}
 template <typename T> int launch_zmid_ml(const MLZArgs<T> &a, cudaStream_t s);
-template <typename T> size_t zmid_ml_smem(int L, int Nz, int W) { return (size_t)2 * L * 3 * 2 * Nz * W * sizeof(cpx<T>); }
 bool zmid_ml_supported(int Nz);
 
 // dst[c * dst_plane + i] = sum_q w[q] * src[idx[q] + c * src_plane], q in [ptr[i], ptr[i+1])

@@ -127,6 +127,9 @@ int bm_ml_info(bm_ctx *ctx, int *L, int *nc3, int *layer_mesh, int *transfer, do
  * L x L products, [3] y inverse, [4] x inverse + transfer out, [5] the whole evaluation. */
 int bm_ml_time_kernels(bm_ctx *ctx, int reps, double *ms6, double *bytes6);
 
+/* Columns per block of the fused multilayer z pass (chosen by timing at setup). */
+int bm_ml_tile(bm_ctx *ctx, int *W);
+
 /* Allocate and build everything for the current configuration now (kernels, tiles). */
 int bm_prepare(bm_ctx *ctx);
 
