@@ -35,6 +35,9 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     "film3d_512x512x16": dict(n=(512, 512, 16), h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, K1=5e5, D=1.5e-3,
                               alpha=0.1, modules=1 | 4 | 8 | 16, eval="RKDP54", dt=1e-14, tol=1e-5, init="tilt"),
+    # the same film at half thickness: the small case for full ncu captures of the stage kernel
+    "film3d_512x512x8": dict(n=(512, 512, 8), h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, K1=5e5, D=1.5e-3,
+                             alpha=0.1, modules=1 | 4 | 8 | 16, eval="RKDP54", dt=1e-14, tol=1e-5, init="tilt"),
     "film2d_128x64": dict(n=(128, 64, 1), h=(5e-9, 5e-9, 3e-9), Ms=8e5, A=1.3e-11, K1=0.0, D=0.0, alpha=0.5,
                           grel=2.211e5 / 2.212761569e5, modules=1 | 2 | 16, Ha=(1e3, 0, 0), eval="RK4", dt=1e-13,
                           init="sphere"),
@@ -50,8 +53,23 @@ CONFIGS = {
                                            K1=3e5, modules=1 | 2 | 8)],
                               A=1.5e-11, D=0.0, alpha=0.05, eval="RKDP54", dt=1e-14, tol=1e-5, init="sphere",
                               multilayer=0),
+    # the same stack at half the in-plane size (FFT 1024 x 1024 x 4): small case for ncu captures
+    "multilayer_stack3_512": dict(meshes=[dict(n=(512, 512, 1), h=(2e-9, 2e-9, 1e-9), o=(0, 0, 0), Ms=1.4e6, K1=0.0,
+                                               modules=1 | 2),
+                                          dict(n=(256, 256, 2), h=(4e-9, 4e-9, 2e-9), o=(0, 0, 2e-9), Ms=6e5, K1=0.0,
+                                               modules=1 | 2),
+                                          dict(n=(512, 512, 1), h=(2e-9, 2e-9, 1.5e-9), o=(0, 0, 7e-9), Ms=1.1e6,
+                                               K1=3e5, modules=1 | 2 | 8)],
+                                  A=1.5e-11, D=0.0, alpha=0.05, eval="RKDP54", dt=1e-14, tol=1e-5, init="sphere",
+                                  multilayer=0),
 }
 MU0 = 1.256637061435916e-6
+
+# DRAM traffic per cell of one launch of the roofline kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture on the half-size case, divided by its cells;
+# profiles/stage_film3d_512x512x8.md, profiles/zmid_ml_multilayer_stack3_512.md)
+TRAFFIC_PER_CELL = {("film3d", "stage"): 246.87e6 / (512 * 512 * 8),
+                    ("multilayer", "ml_zmid"): 383.30e6 / (512 * 512 + 256 * 256 * 2 + 512 * 512)}
 
 
 def mesh_list(cfg):
@@ -381,6 +399,8 @@ def main():
                    for i in range(4) if kms[i] > 0}
         tiles = c.tiles(0)
     achieved = kbytes[dom] / (kms[dom] * 1e-3) / 1e9
+    tpc = TRAFFIC_PER_CELL.get(("multilayer" if ml else "film3d", names[dom]))
+    traffic = tpc * ncell if (tpc and (ml or args.config.startswith("film3d"))) else None
     kpe = c.kernels_per_step()
     out = dict(base, value=value, ms_per_step=ms / max(steps_done, 1), dtype="f32" if prec == bm.MIXED else "f64",
                e2e={"value": e2e, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 3 * ncell * 8 / max(e2e_steps, 1),
@@ -389,7 +409,7 @@ def main():
                clocks=clocks,
                roofline={"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
                          "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "algorithmic_bytes_per_launch": kbytes[dom],
+                         "traffic": traffic, "algorithmic_bytes_per_launch": kbytes[dom],
                          "launch_ms": kms[dom]},
                kernels=kernels,
                rkdp={"attempts": attempts, "accepted": steps_done, "dT": st["dT"]})

@@ -397,7 +397,7 @@ static int launch_zmid_reg(const YZArgs<T> &a, cudaStream_t s)
     size_t smem = zmid_reg_smem<T>(NZ, a.W);
     if (smem > 200 * 1024) return 105;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_zmid_reg<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_zmid_reg<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     dim3 grid((a.LX + a.W - 1) / a.W, a.Ny / 2 + 1);
@@ -499,7 +499,7 @@ static int launch_ypass_reg(const YZArgs<T> &a, cudaStream_t s)
     size_t smem = (size_t)L * a.W * sizeof(cpx<T>);
     if (smem > 200 * 1024) return 107;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_ypass_reg<T, P, Q, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_ypass_reg<T, P, Q, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     dim3 grid((a.LX + a.W - 1) / a.W, a.nz, 3);
@@ -543,7 +543,7 @@ static int launch_common(KF kern, dim3 grid, int nt, size_t smem, cudaStream_t s
     if (nt > 1024 || nt < 1) return 101;
     if (smem > 227 * 1024) return 102;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     return 0;

@@ -8,6 +8,12 @@
 // Twiddles come from a table of exp(-2 pi i m / L) rounded from FP64 on the host.
 // A thread (l, t) works on line l; t indexes its butterflies j = t + i * TPL.
 #pragma once
+
+// Dynamic shared memory ceiling every kernel with more than 48 KB is opened to. The attribute is
+// per kernel function, not per launch: captured graph nodes of one kernel with different sizes all
+// launch against the last value set, so it is always set to this one ceiling (no launch here uses
+// more; the B200 limit per block is 227 KB).
+#define BM_SMEM_CAP (200 * 1024)
 #include "common.cuh"
 
 #define BM_FFT_MAXPASS 8

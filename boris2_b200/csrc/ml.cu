@@ -300,7 +300,7 @@ static int launch_zmid_ml_t(const MLZArgs<T> &a, cudaStream_t s)
     size_t smem = zmid_ml_smem<T>(a.L, NZ, a.W, a.ksm);
     if (smem > 200 * 1024) return 305;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_zmid_ml<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_zmid_ml<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     dim3 grid((a.LX + a.W - 1) / a.W, a.Ny / 2 + 1);

@@ -631,7 +631,7 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
         else b.staged = 0;
     }
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_stage_reg<T, P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_stage_reg<T, P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     int nrows = a.ny * a.nz;
@@ -672,7 +672,7 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
     size_t smem = (size_t)3 * a.rpb * padded_len(a.LX) * sizeof(cpx<T>);
     if (smem > 200 * 1024) return 202;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_stage<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_stage<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     int nrows = a.ny * a.nz;

@@ -162,10 +162,12 @@ def test_norm_preserved_and_energy_decreases(bm):
 def test_stage_kernel_variants(bm, staged, rows, monkeypatch):
     """Both stage-kernel variants (per-cell rows prefetched into shared memory or read from
     global memory) and several rows per block, forced through BM_TILES / BM_STAGE_ROWS, give the
-    oracle's RKDP54 trajectory (exchange + iDMI + anisotropy + demag, 3D, LX = 128 and 64)."""
+    oracle's RKDP54 trajectory (exchange + iDMI + anisotropy + demag, 3D, LX = 128, 64 and 256).
+    The 256-wide mesh makes the staged launches of one graph need different shared-memory sizes
+    above 48 KB (the error-estimate launch stages the most rows)."""
     monkeypatch.setenv("BM_TILES", "1,4,8,%d" % rows)
     monkeypatch.setenv("BM_STAGE_ROWS", staged)
-    for n in [(100, 10, 3), (64, 12, 2)]:
+    for n in [(100, 10, 3), (64, 12, 2), (256, 6, 2)]:
         N = n[0] * n[1] * n[2]
         rng = np.random.default_rng(5)
         Ms_map = 1.1e6 * (1 + 0.05 * rng.normal(size=N))
