@@ -32,6 +32,20 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+def batch_systems(nsys=256, seed=3):
+    """The batching workload: independent films with Nx, Ny drawn log-uniformly from
+    {64, 96, 128, 192, 256, 384, 512} (uniform over that log-spaced set), Nz from {1, 2, 4},
+    4 x 4 x 3 nm cells, Ms ~ U[4e5, 1.4e6], A ~ U[0.8e-11, 2e-11], alpha ~ U[0.01, 0.5] (seeded)."""
+    rng = np.random.default_rng(seed)
+    sizes = [64, 96, 128, 192, 256, 384, 512]
+    out = []
+    for q in range(nsys):
+        n = (int(rng.choice(sizes)), int(rng.choice(sizes)), int(rng.choice([1, 2, 4])))
+        out.append(dict(n=n, h=(4e-9, 4e-9, 3e-9), o=(0.0, 0.0, 0.0), Ms=float(rng.uniform(4e5, 1.4e6)), K1=0.0,
+                        A=float(rng.uniform(0.8e-11, 2e-11)), alpha=float(rng.uniform(0.01, 0.5)), modules=1 | 2))
+    return out
+
+
 CONFIGS = {
     "film3d_512x512x16": dict(n=(512, 512, 16), h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, K1=5e5, D=1.5e-3,
                               alpha=0.1, modules=1 | 4 | 8 | 16, eval="RKDP54", dt=1e-14, tol=1e-5, init="tilt"),
@@ -53,6 +67,9 @@ CONFIGS = {
                                            K1=3e5, modules=1 | 2 | 8)],
                               A=1.5e-11, D=0.0, alpha=0.05, eval="RKDP54", dt=1e-14, tol=1e-5, init="sphere",
                               multilayer=0),
+    # 256 independent films of uneven sizes advanced together, one launch per pass over all of them
+    "batch256": dict(meshes=batch_systems(), A=1.3e-11, D=0.0, alpha=0.1, eval="RK4", dt=5e-14, init="sphere",
+                     batched=True),
     # the same stack at half the in-plane size (FFT 1024 x 1024 x 4): small case for ncu captures
     "multilayer_stack3_512": dict(meshes=[dict(n=(512, 512, 1), h=(2e-9, 2e-9, 1e-9), o=(0, 0, 0), Ms=1.4e6, K1=0.0,
                                                modules=1 | 2),
@@ -65,11 +82,46 @@ CONFIGS = {
 }
 MU0 = 1.256637061435916e-6
 
+
+
 # DRAM traffic per cell of one launch of the roofline kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture on the half-size case, divided by its cells;
 # profiles/stage_film3d_512x512x8.md, profiles/zmid_ml_multilayer_stack3_512.md)
 TRAFFIC_PER_CELL = {("film3d", "stage"): 246.87e6 / (512 * 512 * 8),
                     ("multilayer", "ml_zmid"): 383.30e6 / (512 * 512 + 256 * 256 * 2 + 512 * 512)}
+
+
+def nice(n):
+    b = 1
+    while b < n:
+        b *= 2
+    t = 3
+    while t < b:
+        if t >= n:
+            return t
+        t *= 2
+    return b
+
+
+def rk4_step_bytes(cfg, p):
+    """Algorithmic bytes of one RK4 step over every mesh (p bytes per real): per evaluation the y
+    passes, z pass with its kernel read and the stage kernel's S1 rows (2D: the fused y pass), per
+    step 19 cell-vector reads/writes of the stage updates (M in, base, rhs out, M out each stage,
+    plus the three earlier rhs of the last stage)."""
+    R, C = 3 * p, 6 * p
+    tot = 0.0
+    for m in mesh_list(cfg):
+        nx, ny, nz = m["n"]
+        Nx, Ny = 2 * nice(nx), 2 * nice(ny)
+        Nz = 2 * nice(nz) if nz > 1 else 1
+        LX = Nx // 2
+        S1, S2 = LX * ny * nz, LX * Ny * nz
+        if nz > 1:
+            demag = 2 * C * (S1 + S2) + 2 * C * S2 + 6 * p * (LX + 1) * (Ny // 2 + 1) * (Nz // 2 + 1)
+        else:
+            demag = 2 * C * S1 + 4 * p * (LX + 1) * (Ny // 2 + 1)
+        tot += 4 * (demag + 2 * C * S1) + 19 * R * nx * ny * nz
+    return tot
 
 
 def mesh_list(cfg):
@@ -104,12 +156,14 @@ def make_ctx(bm, cfg, device, precision):
     c = bm.Context(device=device, precision=precision)
     for q, m in enumerate(mesh_list(cfg)):
         c.add_mesh(m["n"], m["h"], m["o"])
-        c.set_material(q, Ms=m["Ms"], A=cfg["A"], alpha=cfg["alpha"], grel=cfg.get("grel", 1.0), K1=m["K1"],
-                       ea=(0, 0, 1), D=cfg["D"])
+        c.set_material(q, Ms=m["Ms"], A=m.get("A", cfg["A"]), alpha=m.get("alpha", cfg["alpha"]),
+                       grel=cfg.get("grel", 1.0), K1=m["K1"], ea=(0, 0, 1), D=cfg["D"])
         c.set_modules(q, m["modules"])
         c.set_field(q, cfg.get("Ha", (0, 0, 0)))
     if "multilayer" in cfg:
         c.multiconvolution(cfg["multilayer"])
+    if cfg.get("batched"):
+        c.set_batched(True)
     c.setode(cfg["eval"], cfg["dt"])
     if cfg["eval"] == "RKDP54":
         c.astepctrl(cfg["tol"], 2.0, 1e-15, 3e-12)
@@ -383,7 +437,16 @@ def main():
     # kernel timing for the roofline: dominant kernel of one field evaluation
     peak, peak_kind = peaks()
     ml = "multilayer" in cfg
-    if ml:
+    if cfg.get("batched"):
+        # one launch per pass over every system: the roofline is that of the whole step
+        p = 4 if prec == bm.MIXED else 8
+        kbytes = np.array([rk4_step_bytes(cfg, p)])
+        kms = np.array([ms / max(steps_done, 1)])
+        names = ["batched RK4 step (all passes, all systems)"]
+        dom = 0
+        kernels = {names[0]: {"ms": kms[0], "GB/s": kbytes[0] / (kms[0] * 1e-3) / 1e9}}
+        tiles = None
+    elif ml:
         kms, kbytes = c.ml_time_kernels(reps=10)
         names = ["ml_transfer_in_xfwd", "ml_yfwd", "ml_zmid", "ml_yinv", "ml_xinv_transfer_out"]
         dom = int(np.argmax(kms[:5]))
@@ -436,6 +499,17 @@ def main():
                                      "peak_GB/s": peak}
             except Exception as e:
                 out["multilayer"] = {"error": str(e)}
+        # the batching workload (256 uneven films, one launch per pass over all of them)
+        if not ml and args.config == "film3d_512x512x16":
+            try:
+                bcfg = CONFIGS["batch256"]
+                bx = quick_rate(bm, bcfg, bm.MIXED, 5, 2, local)
+                pb = rk4_step_bytes(bcfg, 4)
+                out["batching"] = {"workload": "batch256", "systems": len(bcfg["meshes"]), "cells": total_cells(bcfg),
+                                   "mixed": bx, "step_GB/s": pb / (bx["ms_per_step"] * 1e-3) / 1e9,
+                                   "step_frac_of_peak": pb / (bx["ms_per_step"] * 1e-3) / 1e9 / peak}
+            except Exception as e:
+                out["batching"] = {"error": str(e)}
         if not args.no_cpu_baseline:
             try:
                 out["cpu_baseline"] = cpu_reference_rate(cfg)

@@ -94,6 +94,7 @@ _SIGS = {
     "bm_prepare": (_I, [_P]),
     "bm_ml_time_kernels": (_I, [_P, _I, _DP, _DP]),
     "bm_ml_tile": (_I, [_P, _IP]),
+    "bm_set_batched": (_I, [_P, _I]),
 }
 
 
@@ -187,6 +188,10 @@ class Context:
 
     def set_precision(self, precision):
         _check(lib().bm_set_precision(self._h, int(precision)))
+
+    def set_batched(self, on=True):
+        """Advance all meshes with one launch per pass over a (mesh, tile) work list."""
+        _check(lib().bm_set_batched(self._h, int(bool(on))))
 
     def multiconvolution(self, mode=ML_3D, ncommon=None):
         """Multilayered demag over all meshes with the demag module (ML_OFF turns it off):

@@ -102,6 +102,23 @@ struct MLRun {
     long long ncc = 0;
 };
 
+// Graphs of a context with many meshes per launch are built in two passes: the first collects
+// every batched launch's argument blocks and work list (host), they are uploaded in one buffer,
+// the second (under stream capture) launches them from the uploaded copies.
+struct BatchRec {
+    int kind;             // 0 stage, else BM_BATCH_*
+    size_t args_off, work_off;
+    int nwork, nt;
+    size_t smem;
+};
+struct BatchPlan {
+    bool collect = false;
+    std::vector<unsigned char> hbuf;
+    std::vector<BatchRec> recs;
+    size_t next = 0;
+    void *dbuf = nullptr;
+};
+
 }  // namespace
 
 struct bm_ctx {
@@ -124,6 +141,8 @@ struct bm_ctx {
     int kernels_per_step = 0;
     double *farq = nullptr;
     StepState host_st;
+    bool batched = false;       // many meshes per launch (work lists) instead of one launch per mesh
+    BatchPlan bp;
     int ml_mode = -1;           // -1 off; 0 3D, 1 2D, 2 2D layered
     bool ml_nc_set = false;
     int ml_nc[3] = {1, 1, 1};
@@ -173,6 +192,8 @@ void drop_graph(bm_ctx *c)
     c->gexec = nullptr;
     c->graph = nullptr;
     c->graph_eval = -1;
+    if (c->bp.dbuf) cudaFree(c->bp.dbuf);
+    c->bp = BatchPlan();
 }
 
 void unprepare(bm_ctx *c)
@@ -674,7 +695,7 @@ int prepare_T(bm_ctx *c)
             m.W2 = t4[0]; m.Wy = t4[1]; m.Wz = t4[2]; m.rpb = t4[3];
             const char *sr = getenv("BM_STAGE_ROWS");
             m.staged = (sr && sr[0] == '1') ? 1 : 0;
-        } else if (c->autotune) autotune_mesh<T>(c, m);
+        } else if (c->autotune && !c->batched) autotune_mesh<T>(c, m);
     }
     if (int rc = prepare_ml<T>(c)) { for (auto &mm : c->meshes) free_mesh(mm); free_ml(c); return rc; }
     return 0;
@@ -684,6 +705,7 @@ int prepare(bm_ctx *c)
 {
     if (c->ready) return 0;
     if (c->meshes.empty()) return fail(BM_ESTATE, "no mesh");
+    if (c->batched && c->ml_mode >= 0) return fail(BM_EUNSUPPORTED, "batched meshes with a multilayered convolution");
     CK(cudaSetDevice(c->device));
     int rc = (c->precision == BM_FP64) ? prepare_T<double>(c) : prepare_T<float>(c);
     if (rc) return rc;
@@ -760,6 +782,153 @@ StageArgs<T> stage_args(bm_ctx *c, Mesh &m)
 
 template <typename T> T *B(Mesh &m, int i) { return (T *)m.buf[i]; }
 template <typename T> T *E(Mesh &m, int i) { return (T *)m.ev[i]; }
+
+// ------------------------------------------------------------------ many meshes per launch
+size_t bp_append(BatchPlan &bp, const void *p, size_t bytes)
+{
+    size_t off = (bp.hbuf.size() + 255) & ~(size_t)255;
+    bp.hbuf.resize(off + bytes);
+    memcpy(bp.hbuf.data() + off, p, bytes);
+    return off;
+}
+
+// stage kernels of several meshes: per-mesh launches, or one launch over (mesh, row block) items
+// with the generic-length kernel (rows per block chosen so every mesh fills ~256 threads)
+template <typename T>
+int stage_multi(bm_ctx *c, std::vector<StageArgs<T>> &v, int *count)
+{
+    if (v.empty()) return 0;
+    if (!c->batched || v.size() == 1) {
+        for (auto &a : v) {
+            CKL(launch_stage<T>(a, c->stream), "stage");
+            (*count)++;
+        }
+        return 0;
+    }
+    BatchPlan &bp = c->bp;
+    if (bp.collect) {
+        int lk = BM_LAST_NONE;
+        for (auto &a : v) if (a.last_kind != BM_LAST_NONE) lk = a.last_kind;
+        std::vector<int2> work;
+        int nt = 32;
+        size_t smem = 0;
+        for (size_t i = 0; i < v.size(); i++) {
+            StageArgs<T> &a = v[i];
+            a.last_kind = lk;
+            a.staged = 0;
+            const int rows = a.ny * a.nz;
+            int rpb = 256 / (3 * a.px.tpl);
+            rpb = std::max(1, std::min(rpb, rows));
+            a.rpb = rpb;
+            for (int b = 0; b < (rows + rpb - 1) / rpb; b++) work.push_back(make_int2((int)i, b));
+            nt = std::max(nt, (3 * rpb * a.px.tpl + 31) & ~31);
+            smem = std::max(smem, (size_t)3 * rpb * padded_len(a.LX) * sizeof(cpx<T>));
+        }
+        BatchRec r;
+        r.kind = 0;
+        r.args_off = bp_append(bp, v.data(), sizeof(StageArgs<T>) * v.size());
+        r.work_off = bp_append(bp, work.data(), sizeof(int2) * work.size());
+        r.nwork = (int)work.size();
+        r.nt = nt;
+        r.smem = smem;
+        bp.recs.push_back(r);
+        return 0;
+    }
+    if (bp.next >= bp.recs.size()) return fail(BM_ESTATE, "batched launch plan out of step");
+    const BatchRec &r = bp.recs[bp.next++];
+    const char *base = (const char *)bp.dbuf;
+    CKL(launch_stage_batch<T>((const StageArgs<T> *)(base + r.args_off), (const int2 *)(base + r.work_off), r.nwork, r.nt,
+                              r.smem, c->stream), "stage batch");
+    (*count)++;
+    return 0;
+}
+
+// generic-kernel tile widths of a mesh for the batched y passes and z pass
+template <typename T>
+void batch_tiles(const Mesh &m, int &Wy, int &Wz)
+{
+    const int lim = 256;
+    Wy = 16;
+    while (Wy > 1 && (Wy * m.py.tpl > lim || (size_t)m.Ny * Wy * sizeof(cpx<T>) > 64 * 1024)) Wy /= 2;
+    Wz = 16;
+    while (Wz > 1 && (2 * Wz * m.pz.tpl > lim || zmid_smem<T>(m.Nz, Wz) > 64 * 1024)) Wz /= 2;
+    while (Wy > 1 && Wy > m.LX) Wy /= 2;
+    while (Wz > 1 && Wz > m.LX) Wz /= 2;
+}
+
+template <typename T>
+int yz_batch_one(bm_ctx *c, int kind, std::vector<YZArgs<T>> &v, int *count)
+{
+    if (v.empty()) return 0;
+    BatchPlan &bp = c->bp;
+    if (bp.collect) {
+        std::vector<int2> work;
+        int nt = 32;
+        size_t smem = 0;
+        for (size_t i = 0; i < v.size(); i++) {
+            const YZArgs<T> &a = v[i];
+            const int nbx = (a.LX + a.W - 1) / a.W;
+            int items = nbx;
+            if (kind == BM_BATCH_YFWD || kind == BM_BATCH_YINV) {
+                items = nbx * a.nz * 3;
+                nt = std::max(nt, (a.W * a.py.tpl + 31) & ~31);
+                smem = std::max(smem, (size_t)a.Ny * a.W * sizeof(cpx<T>));
+            } else if (kind == BM_BATCH_ZMID) {
+                items = nbx * (a.Ny / 2 + 1);
+                nt = std::max(nt, (2 * a.W * a.pz.tpl + 31) & ~31);
+                smem = std::max(smem, zmid_smem<T>(a.Nz, a.W));
+            } else {
+                nt = std::max(nt, (a.W * a.py.tpl + 31) & ~31);
+                smem = std::max(smem, ymid2d_smem<T>(a.Ny, a.W));
+            }
+            for (int b = 0; b < items; b++) work.push_back(make_int2((int)i, b));
+        }
+        BatchRec r;
+        r.kind = kind;
+        r.args_off = bp_append(bp, v.data(), sizeof(YZArgs<T>) * v.size());
+        r.work_off = bp_append(bp, work.data(), sizeof(int2) * work.size());
+        r.nwork = (int)work.size();
+        r.nt = nt;
+        r.smem = smem;
+        bp.recs.push_back(r);
+        return 0;
+    }
+    if (bp.next >= bp.recs.size()) return fail(BM_ESTATE, "batched launch plan out of step");
+    const BatchRec &r = bp.recs[bp.next++];
+    const char *base = (const char *)bp.dbuf;
+    CKL(launch_yz_batch<T>(r.kind, (const YZArgs<T> *)(base + r.args_off), (const int2 *)(base + r.work_off), r.nwork, r.nt,
+                           r.smem, c->stream), "y/z batch");
+    (*count)++;
+    return 0;
+}
+
+// y/z passes of every mesh with demag in four launches (2D y pass, y forward, z pass, y inverse)
+template <typename T>
+int yz_multi(bm_ctx *c, int gate, int *count)
+{
+    std::vector<YZArgs<T>> v2, vy, vz;
+    for (auto &m : c->meshes) {
+        if (!(m.modules & BM_DEMAG)) continue;
+        YZArgs<T> a = yz_args<T>(c, m, gate);
+        if (m.nz == 1) {
+            a.W = m.W2;
+            v2.push_back(a);
+        } else {
+            int Wy, Wz;
+            batch_tiles<T>(m, Wy, Wz);
+            a.W = Wy;
+            vy.push_back(a);
+            a.W = Wz;
+            vz.push_back(a);
+        }
+    }
+    int rc;
+    if ((rc = yz_batch_one<T>(c, BM_BATCH_YMID2D, v2, count))) return rc;
+    if ((rc = yz_batch_one<T>(c, BM_BATCH_YFWD, vy, count))) return rc;
+    if ((rc = yz_batch_one<T>(c, BM_BATCH_ZMID, vz, count))) return rc;
+    if ((rc = yz_batch_one<T>(c, BM_BATCH_YINV, vy, count))) return rc;
+    return 0;
+}
 
 Mesh &ml_grid(bm_ctx *c, int l)
 {
@@ -871,6 +1040,7 @@ template <typename T>
 int enqueue_fields(bm_ctx *c, int gate, int bi, int *count)
 {
     if (!c->ml) {
+        if (c->batched && c->meshes.size() > 1) return yz_multi<T>(c, gate, count);
         for (auto &m : c->meshes) {
             int rc = enqueue_yz<T>(c, m, gate, count);
             if (rc) return rc;
@@ -911,6 +1081,7 @@ int enqueue_rk4_step(bm_ctx *c, int *count)
             int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count);
             if (rc) return rc;
         }
+        std::vector<StageArgs<T>> v;
         for (int i = 0; i < nm; i++) {
             Mesh &m = c->meshes[i];
             StageArgs<T> a = stage_args<T>(c, m);
@@ -929,9 +1100,9 @@ int enqueue_rk4_step(bm_ctx *c, int *count)
                 a.renorm = 1;
                 if (i == nm - 1) a.last_kind = BM_LAST_FINISH;
             }
-            CKL(launch_stage<T>(a, c->stream), "stage");
-            (*count)++;
+            v.push_back(a);
         }
+        if (int rc = stage_multi<T>(c, v, count)) return rc;
     }
     return 0;
 }
@@ -942,15 +1113,18 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
     // buffers: 0 = M, 1 = P (sM1), 2 = B, 3 = C ; evals 0..5
     const int nm = (int)c->meshes.size();
     // restore after a rejection: M = sM1 and its x transform
-    for (int i = 0; i < nm; i++) {
-        Mesh &m = c->meshes[i];
-        StageArgs<T> a = stage_args<T>(c, m);
-        a.mode = BM_MODE_UPDATE;
-        a.gate = BM_GATE_RESTORE;
-        a.Min = B<T>(m, 1); a.Mbase = B<T>(m, 1); a.Mout = B<T>(m, 0);
-        if (i == nm - 1) a.last_kind = BM_LAST_RESTORED;
-        CKL(launch_stage<T>(a, c->stream), "restore");
-        (*count)++;
+    {
+        std::vector<StageArgs<T>> v;
+        for (int i = 0; i < nm; i++) {
+            Mesh &m = c->meshes[i];
+            StageArgs<T> a = stage_args<T>(c, m);
+            a.mode = BM_MODE_UPDATE;
+            a.gate = BM_GATE_RESTORE;
+            a.Min = B<T>(m, 1); a.Mbase = B<T>(m, 1); a.Mout = B<T>(m, 0);
+            if (i == nm - 1) a.last_kind = BM_LAST_RESTORED;
+            v.push_back(a);
+        }
+        if (int rc = stage_multi<T>(c, v, count)) return rc;
     }
     // evaluation 0: FSAL rhs + error of the previous step + controller
     {
@@ -958,32 +1132,38 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
         if (rc) return rc;
     }
     static const double bs[5] = {5179.0 / 57600, 7571.0 / 16695, 393.0 / 640, -92097.0 / 339200, 187.0 / 2100};
-    for (int i = 0; i < nm; i++) {
-        Mesh &m = c->meshes[i];
-        StageArgs<T> a = stage_args<T>(c, m);
-        a.mode = BM_MODE_LTE;
-        a.do_xfwd = 0;
-        a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 1);
-        a.nev = 5;
-        a.ev[0] = E<T>(m, 0); a.ev[1] = E<T>(m, 2); a.ev[2] = E<T>(m, 3); a.ev[3] = E<T>(m, 4); a.ev[4] = E<T>(m, 5);
-        for (int k = 0; k < 5; k++) a.cev[k] = bs[k];
-        a.crhs = 1.0 / 40;
-        a.ev_out = E<T>(m, 0);
-        if (i == nm - 1) a.last_kind = BM_LAST_CONTROL;
-        CKL(launch_stage<T>(a, c->stream), "rkdp eval0");
-        (*count)++;
+    {
+        std::vector<StageArgs<T>> v;
+        for (int i = 0; i < nm; i++) {
+            Mesh &m = c->meshes[i];
+            StageArgs<T> a = stage_args<T>(c, m);
+            a.mode = BM_MODE_LTE;
+            a.do_xfwd = 0;
+            a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 1);
+            a.nev = 5;
+            a.ev[0] = E<T>(m, 0); a.ev[1] = E<T>(m, 2); a.ev[2] = E<T>(m, 3); a.ev[3] = E<T>(m, 4); a.ev[4] = E<T>(m, 5);
+            for (int k = 0; k < 5; k++) a.cev[k] = bs[k];
+            a.crhs = 1.0 / 40;
+            a.ev_out = E<T>(m, 0);
+            if (i == nm - 1) a.last_kind = BM_LAST_CONTROL;
+            v.push_back(a);
+        }
+        if (int rc = stage_multi<T>(c, v, count)) return rc;
     }
     // advance: sM1 = M, M1 = M + dT/5 k0
-    for (int i = 0; i < nm; i++) {
-        Mesh &m = c->meshes[i];
-        StageArgs<T> a = stage_args<T>(c, m);
-        a.mode = BM_MODE_UPDATE;
-        a.gate = BM_GATE_ACCEPTED;
-        a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0); a.copy_to = B<T>(m, 1);
-        a.nev = 1; a.ev[0] = E<T>(m, 0); a.cev[0] = 0.2;
-        a.Mout = B<T>(m, 2);
-        CKL(launch_stage<T>(a, c->stream), "rkdp advance");
-        (*count)++;
+    {
+        std::vector<StageArgs<T>> v;
+        for (int i = 0; i < nm; i++) {
+            Mesh &m = c->meshes[i];
+            StageArgs<T> a = stage_args<T>(c, m);
+            a.mode = BM_MODE_UPDATE;
+            a.gate = BM_GATE_ACCEPTED;
+            a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0); a.copy_to = B<T>(m, 1);
+            a.nev = 1; a.ev[0] = E<T>(m, 0); a.cev[0] = 0.2;
+            a.Mout = B<T>(m, 2);
+            v.push_back(a);
+        }
+        if (int rc = stage_multi<T>(c, v, count)) return rc;
     }
     static const double av[6][6] = {
         {0},
@@ -997,6 +1177,7 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
             int rc = enqueue_fields<T>(c, BM_GATE_ACCEPTED, (s % 2 == 1) ? 2 : 3, count);
             if (rc) return rc;
         }
+        std::vector<StageArgs<T>> v;
         for (int i = 0; i < nm; i++) {
             Mesh &m = c->meshes[i];
             StageArgs<T> a = stage_args<T>(c, m);
@@ -1019,9 +1200,9 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
                 a.renorm = 1;
                 if (i == nm - 1) a.last_kind = BM_LAST_FINISH;
             }
-            CKL(launch_stage<T>(a, c->stream), "rkdp stage");
-            (*count)++;
+            v.push_back(a);
         }
+        if (int rc = stage_multi<T>(c, v, count)) return rc;
     }
     return 0;
 }
@@ -1031,6 +1212,20 @@ int build_graph(bm_ctx *c)
 {
     drop_graph(c);
     int count = 0;
+    if (c->batched && c->meshes.size() > 1) {
+        // pass 1: collect the batched launches' argument blocks and work lists, upload them
+        c->bp = BatchPlan();
+        c->bp.collect = true;
+        int rc = (c->eval == BM_RKDP54) ? enqueue_rkdp_attempt<T>(c, &count) : enqueue_rk4_step<T>(c, &count);
+        c->bp.collect = false;
+        if (rc) return rc;
+        if (!c->bp.hbuf.empty()) {
+            if (cudaMalloc(&c->bp.dbuf, c->bp.hbuf.size()) != cudaSuccess) return fail(BM_ENOMEM, "batched launch plan");
+            CK(cudaMemcpy(c->bp.dbuf, c->bp.hbuf.data(), c->bp.hbuf.size(), cudaMemcpyHostToDevice));
+        }
+        c->bp.next = 0;
+        count = 0;
+    }
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = (c->eval == BM_RKDP54) ? enqueue_rkdp_attempt<T>(c, &count) : enqueue_rk4_step<T>(c, &count);
     cudaGraph_t g = nullptr;
@@ -1271,6 +1466,14 @@ int bm_set_astepctrl(bm_ctx *c, double err_fail, double dT_incr, double dT_min, 
         c->dt = c->host_st.dT;
         return upload_state(c);
     }
+    return 0;
+}
+
+int bm_set_batched(bm_ctx *c, int on)
+{
+    if (int rc = check_ctx(c)) return rc;
+    unprepare(c);
+    c->batched = on != 0;
     return 0;
 }
 

@@ -35,16 +35,15 @@ __device__ __forceinline__ void kapply(const T k[6], const cpx<T> m[3], cpx<T> h
 // smem: data [3][Ny][W] complex, kernel tile [4][Ky1][W] real (xx, yy, zz, xy at kz = 0),
 // column-0 Nyquist kernel [4][Ky1] real. All tiles arrive by cp.async (one DRAM latency).
 template <typename T>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_ymid2d(YZArgs<T> a)
+__device__ __forceinline__ void ymid2d_body(const YZArgs<T> &a, int bx)
 {
-    if (gated_out<T>(a.st, a.gate)) return;
     extern __shared__ unsigned char smraw[];
     const int W = a.W, Ny = a.Ny, ny = a.ny, LX = a.LX;
     const int Ky1 = Ny / 2 + 1, Kx1 = LX + 1;
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
     T *Ks = reinterpret_cast<T *>(sm + 3 * Ny * W);
     T *Kn = Ks + 4 * Ky1 * W;
-    const int kx0 = blockIdx.x * W;
+    const int kx0 = bx * W;
     const int nt = blockDim.x, tid = threadIdx.x;
     const long long plane = (long long)ny * LX;   // one component (nz == 1)
     const long long nk = (long long)Kx1 * Ky1;
@@ -126,15 +125,34 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_ymid2d(YZArgs<T> a)
     }
 }
 
-// ------------------------------------------------------------------------------ 3D y passes
-template <typename T, bool INV>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass3d(YZArgs<T> a)
+template <typename T>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ymid2d(YZArgs<T> a)
 {
     if (gated_out<T>(a.st, a.gate)) return;
+    ymid2d_body<T>(a, blockIdx.x);
+}
+
+// many meshes in one launch: work item (mesh, column tile); every mesh shares the step state
+template <typename T>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ymid2d_batch(const YZArgs<T> *__restrict__ args, const int2 *__restrict__ work,
+                                                                 int nwork)
+{
+    if (gated_out<T>(args[0].st, args[0].gate)) return;
+    for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
+        const int2 it = work[i];
+        ymid2d_body<T>(args[it.x], it.y);
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------ 3D y passes
+template <typename T, bool INV>
+__device__ __forceinline__ void ypass3d_body(const YZArgs<T> &a, int bx, int z, int c)
+{
     extern __shared__ unsigned char smraw[];
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
     const int W = a.W, Ny = a.Ny, ny = a.ny, LX = a.LX, nz = a.nz;
-    const int kx0 = blockIdx.x * W, z = blockIdx.y, c = blockIdx.z;
+    const int kx0 = bx * W;
     const int nt = blockDim.x, tid = threadIdx.x;
     const cpx<T> *src;
     cpx<T> *dst;
@@ -162,22 +180,44 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_ypass3d(YZArgs<T> a)
     }
 }
 
+template <typename T, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass3d(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    ypass3d_body<T, INV>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// many meshes in one launch: work item (mesh, column tile + W-columns count * (z + nz * component))
+template <typename T, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass3d_batch(const YZArgs<T> *__restrict__ args, const int2 *__restrict__ work,
+                                                                  int nwork)
+{
+    if (gated_out<T>(args[0].st, args[0].gate)) return;
+    for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
+        const int2 it = work[i];
+        const YZArgs<T> &a = args[it.x];
+        const int nbx = (a.LX + a.W - 1) / a.W;
+        const int bx = it.y % nbx, r = it.y / nbx;
+        ypass3d_body<T, INV>(a, bx, r % a.nz, r / a.nz);
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------------------ 3D z pass + product
 // Block: W columns kx0.., the mirror pencils ky and Ny - ky (which share |ky|), 3 components.
 // smem: data [3][2][Nz][W] complex, kernel tile [6][Kz1][W] real at |ky|, column-0 Nyquist
 // kernel [6][Kz1] real.
 template <typename T>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid(YZArgs<T> a)
+__device__ __forceinline__ void zmid_body(const YZArgs<T> &a, int bx, int ky)
 {
-    if (gated_out<T>(a.st, a.gate)) return;
     extern __shared__ unsigned char smraw[];
     const int W = a.W, Ny = a.Ny, Nz = a.Nz, nz = a.nz, LX = a.LX;
     const int Kx1 = LX + 1, Ky1 = Ny / 2 + 1, Kz1 = Nz / 2 + 1;
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
     T *Ks = reinterpret_cast<T *>(sm + 6 * Nz * W);
     T *Kn = Ks + 6 * Kz1 * W;
-    const int kx0 = blockIdx.x * W;
-    const int ky = blockIdx.y, kym = (Ny - ky) % Ny;
+    const int kx0 = bx * W;
+    const int kym = (Ny - ky) % Ny;
     const bool single = (ky == kym);
     const int nt = blockDim.x, tid = threadIdx.x;
     const long long nk = (long long)Kx1 * Ky1 * Kz1;
@@ -266,6 +306,28 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid(YZArgs<T> a)
         int c = cp / np, p = cp % np;
         int kyp = p ? kym : ky, kx = kx0 + w;
         if (kx < LX) a.S2[(((long long)c * nz + e) * Ny + kyp) * LX + kx] = S(c, p, e, w);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    zmid_body<T>(a, blockIdx.x, blockIdx.y);
+}
+
+// many meshes in one launch: work item (mesh, column tile + W-columns count * ky)
+template <typename T>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_batch(const YZArgs<T> *__restrict__ args, const int2 *__restrict__ work,
+                                                               int nwork)
+{
+    if (gated_out<T>(args[0].st, args[0].gate)) return;
+    for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
+        const int2 it = work[i];
+        const YZArgs<T> &a = args[it.x];
+        const int nbx = (a.LX + a.W - 1) / a.W;
+        zmid_body<T>(a, it.y % nbx, it.y / nbx);
+        __syncthreads();
     }
 }
 
@@ -631,3 +693,51 @@ template int launch_yinv<float>(const YZArgs<float> &, cudaStream_t);
 template int launch_yinv<double>(const YZArgs<double> &, cudaStream_t);
 template int launch_zmid<float>(const YZArgs<float> &, cudaStream_t);
 template int launch_zmid<double>(const YZArgs<double> &, cudaStream_t);
+
+// ------------------------------------------------------------------------------ batched launchers
+// One launch over a work list of (mesh, tile) items; nt and smem are the maxima over the meshes,
+// the grid is one wave of resident blocks (each block loops over items).
+template <typename KF>
+static int launch_batch_common(KF kern, int nwork, int nt, size_t smem, int *grid)
+{
+    int rc = launch_common(kern, dim3(1), nt, smem, 0);
+    if (rc) return rc;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long long g = (long long)per_sm * nsm;
+    *grid = (int)(g < nwork ? g : nwork);
+    return 0;
+}
+
+template <typename T>
+int launch_yz_batch(int kind, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+{
+    if (nwork < 1) return 0;
+    int grid = 1, rc = 0;
+    switch (kind) {
+    case BM_BATCH_YMID2D:
+        if ((rc = launch_batch_common(k_ymid2d_batch<T>, nwork, nt, smem, &grid))) return rc;
+        k_ymid2d_batch<T><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+        break;
+    case BM_BATCH_YFWD:
+        if ((rc = launch_batch_common(k_ypass3d_batch<T, false>, nwork, nt, smem, &grid))) return rc;
+        k_ypass3d_batch<T, false><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+        break;
+    case BM_BATCH_YINV:
+        if ((rc = launch_batch_common(k_ypass3d_batch<T, true>, nwork, nt, smem, &grid))) return rc;
+        k_ypass3d_batch<T, true><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+        break;
+    case BM_BATCH_ZMID:
+        if ((rc = launch_batch_common(k_zmid_batch<T>, nwork, nt, smem, &grid))) return rc;
+        k_zmid_batch<T><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+        break;
+    default: return 110;
+    }
+    return (int)cudaGetLastError();
+}
+
+template int launch_yz_batch<float>(int, const YZArgs<float> *, const int2 *, int, int, size_t, cudaStream_t);
+template int launch_yz_batch<double>(int, const YZArgs<double> *, const int2 *, int, int, size_t, cudaStream_t);

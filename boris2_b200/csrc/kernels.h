@@ -118,5 +118,18 @@ template <typename T> __host__ __device__ inline StageLayout stage_layout(const 
 }
 
 template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s);
+
+// ---------------------------------------------------------------- many meshes per launch
+// Work items (mesh, tile index); the argument blocks and the work list live in device memory.
+// Tile index: stage = row block; ymid2d = column tile; y passes = column tile + tiles * (z + nz *
+// component); z pass = column tile + tiles * ky.
+#define BM_BATCH_YMID2D 1
+#define BM_BATCH_YFWD 2
+#define BM_BATCH_ZMID 3
+#define BM_BATCH_YINV 4
+template <typename T>
+int launch_yz_batch(int kind, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
+template <typename T>
+int launch_stage_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
 int stage_reg_q(int LX);   // threads per x line of the register stage kernel (0: generic kernel)
 int launch_scalar_reset(StepState *st, cudaStream_t s);

@@ -331,8 +331,9 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 }
 
 // LTE block reduction and the last-block bookkeeping (step finish / controller / restore flag)
+// total: launch items that each call the tail once (blocks, or work items of a batched launch)
 template <typename T>
-__device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax)
+__device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, unsigned int total)
 {
     __shared__ double red[32];
     __shared__ int is_last;
@@ -355,7 +356,7 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax)
     __syncthreads();
     if (tid == 0) {
         unsigned int tk = atomicAdd(&a.st->blocks_done, 1u);
-        is_last = (tk == gridDim.x - 1);
+        is_last = (tk == total - 1);
     }
     __syncthreads();
     if (!is_last || tid != 0) return;
@@ -410,17 +411,16 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax)
     __threadfence();
 }
 
-// generic-length kernel (shared-memory Stockham x transforms)
+// generic-length body (shared-memory Stockham x transforms) for row block bid
 template <typename T>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
+__device__ __forceinline__ void stage_generic_body(const StageArgs<T> &a, int bid, unsigned int total)
 {
-    if (stage_gated_out<T>(a.st, a.gate)) return;
     extern __shared__ unsigned char smraw[];
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
     const int LX = a.LX, rpb = a.rpb, tpl = a.px.tpl;
     const int LSP = padded_len(LX);
     const int nrows = a.ny * a.nz;
-    const int r0 = blockIdx.x * rpb;
+    const int r0 = bid * rpb;
     const int tid = threadIdx.x;
     const int q = tid / tpl, t = tid % tpl;
     const int qc = q / rpb, qr = q % rpb;
@@ -453,7 +453,29 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
             for (int mm = t; mm < LX; mm += tpl) dst[mm] = line[eaddr<true>(mm, 1)];
         }
     }
-    stage_tail<T>(a, lmax);
+    stage_tail<T>(a, lmax, total);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_stage(StageArgs<T> a)
+{
+    if (stage_gated_out<T>(a.st, a.gate)) return;
+    stage_generic_body<T>(a, blockIdx.x, gridDim.x);
+}
+
+// many meshes in one launch: work item (mesh, row block). The meshes share the step state; every
+// item takes part in the error-norm maximum and the last item finishes the step (last_kind is the
+// same for all meshes of the launch).
+template <typename T>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_stage_batch(const StageArgs<T> *__restrict__ args, const int2 *__restrict__ work,
+                                                                int nwork)
+{
+    if (stage_gated_out<T>(args[0].st, args[0].gate)) return;
+    for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
+        const int2 it = work[i];
+        stage_generic_body<T>(args[it.x], it.y, (unsigned int)nwork);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -611,7 +633,7 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
             for (int mm = t; mm < LX; mm += Q) dst[mm] = line[A(mm)];
         }
     }
-    stage_tail<T>(a, lmax);
+    stage_tail<T>(a, lmax, gridDim.x);
 }
 
 template <typename T, int P, int Q>
@@ -683,3 +705,27 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
 
 template int launch_stage<float>(const StageArgs<float> &, cudaStream_t);
 template int launch_stage<double>(const StageArgs<double> &, cudaStream_t);
+
+template <typename T>
+int launch_stage_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+{
+    if (nwork < 1) return 0;
+    if (nt > bm_lb<T>::v || nt < 32) return 211;
+    if (smem > 200 * 1024) return 212;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_stage_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        if (e != cudaSuccess) return (int)e;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_batch<T>, nt, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long long g = (long long)per_sm * nsm;
+    int grid = (int)(g < nwork ? g : nwork);
+    k_stage_batch<T><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+    return (int)cudaGetLastError();
+}
+
+template int launch_stage_batch<float>(const StageArgs<float> *, const int2 *, int, int, size_t, cudaStream_t);
+template int launch_stage_batch<double>(const StageArgs<double> *, const int2 *, int, int, size_t, cudaStream_t);

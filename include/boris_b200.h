@@ -92,6 +92,14 @@ int bm_set_ode(bm_ctx *ctx, int eval, double dt);
  * tolerance, dT_incr = maximum increase factor, dT_min / dT_max = step limits. */
 int bm_set_astepctrl(bm_ctx *ctx, double err_fail, double dT_incr, double dT_min, double dT_max);
 
+/* Many independent meshes per launch (batching): with on != 0, every pass of a field evaluation
+ * runs as one launch over a work list of (mesh, tile) items covering all meshes of the context
+ * (uneven sizes allowed), and a step is one CUDA graph of those launches. The meshes are
+ * independent systems sharing the time step, as meshes of one reference simulation do
+ * (ODECommon); without it every mesh gets its own launches. Not combined with
+ * bm_set_multiconvolution. */
+int bm_set_batched(bm_ctx *ctx, int on);
+
 /* Precision: BM_FP64 or BM_MIXED (default BM_MIXED). Must be set before the first run. */
 int bm_set_precision(bm_ctx *ctx, int precision);
 
