@@ -1365,3 +1365,217 @@ int orc_run(orc_solver *s, int steps, orc_stats *st)
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------ discrete adjoint of RK4 */
+/* Forward: the solver's RK4 step (DiffEqFM_Evals_RK4.cpp, renormalisation to Ms; the Zeeman sample
+ * is the one at the step start time, as the solver takes it), modules demag + exchange + uniaxial
+ * anisotropy (K2 = 0) + Zeeman, per-cell Ms and K1; the initial state is M0 = Ms m0.
+ * Loss: L = (1/n) sum_i |M_i(T)/Ms_i - target_i|^2.
+ * Backward: reverse mode through every stage of every step, the renormalisation and the field terms
+ * (the project's own derivation; the reference has no adjoint). The demag operator D and the
+ * Neumann Laplacian L are symmetric, so their transposes are themselves. States of every step are
+ * kept (test sizes); each step's stages are recomputed in the backward sweep. */
+
+typedef struct {
+    const orc_mesh_desc *d;
+    orc_demag *dm;
+    int n;
+    const double *Ms, *K1;
+    double *tmp;
+} adj_ctx;
+
+static void adj_fields(adj_ctx *a, const double *X, const double *Ha, double *H)
+{
+    const orc_mesh_desc *d = a->d;
+    for (int i = 0; i < a->n; i++) { H[3 * i] = Ha[0]; H[3 * i + 1] = Ha[1]; H[3 * i + 2] = Ha[2]; }
+    if (d->modules & ORC_DEMAG) orc_demag_apply(a->dm, X, H, 1);
+    if (d->modules & ORC_EXCH) orc_field_exchange(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, X, d->A, a->Ms, H);
+    if (d->modules & ORC_ANIUNI) orc_field_aniuni(a->n, X, a->Ms, a->K1, 0.0, d->ea, H);
+}
+
+/* out = L V per component (Neumann: only existing neighbours) */
+static void adj_lap(const orc_mesh_desc *d, const double *V, double *out)
+{
+    static const double zero[3] = {0, 0, 0};
+    int nx = d->nx, ny = d->ny, nz = d->nz;
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                size_t idx = (size_t)i + (size_t)j * nx + (size_t)k * nx * ny;
+                double dx[3], dy[3], dz[3], g[3];
+                axis_terms(V, idx, i, nx, 1, d->hx, zero, dx, g);
+                axis_terms(V, idx, j, ny, nx, d->hy, zero, dy, g);
+                axis_terms(V, idx, k, nz, (size_t)nx * ny, d->hz, zero, dz, g);
+                for (int c = 0; c < 3; c++) out[3 * idx + c] = dx[c] + dy[c] + dz[c];
+            }
+}
+
+/* one RK4 step from M0 at time t; stage inputs X[0..3], fields H[0..3], pre-normalisation Y */
+static void adj_step(adj_ctx *a, const double *M0, double t, double dt, double *X[4], double *H[4], double *Y, double *Mout)
+{
+    const orc_mesh_desc *d = a->d;
+    const int n = a->n;
+    double Ha[3];
+    applied_field(d, t, Ha);
+    double *k = a->tmp;   /* 4 x 3n */
+    static const double cx[4] = {0.0, 0.5, 0.5, 1.0};
+    for (int s = 0; s < 4; s++) {
+        if (s == 0) memcpy(X[0], M0, sizeof(double) * 3 * n);
+        else
+            for (int i = 0; i < 3 * n; i++) X[s][i] = M0[i] + cx[s] * dt * k[(size_t)(s - 1) * 3 * n + i];
+        adj_fields(a, X[s], Ha, H[s]);
+        for (int i = 0; i < n; i++) llg(X[s] + 3 * i, H[s] + 3 * i, a->Ms[i], d->alpha, d->grel, k + (size_t)s * 3 * n + 3 * i);
+    }
+    for (int i = 0; i < 3 * n; i++)
+        Y[i] = M0[i] + (k[i] + 2 * k[3 * n + i] + 2 * k[6 * n + i] + k[9 * n + i]) * (dt / 6);
+    for (int i = 0; i < n; i++) {
+        double *y = Y + 3 * i, nr = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+        for (int c = 0; c < 3; c++) Mout[3 * i + c] = a->Ms[i] * y[c] / nr;
+    }
+}
+
+/* gX = (d f / d X)^T mu for f = LLG(X, H(X)) at one stage; accumulates the parameter gradients */
+static void adj_vjp(adj_ctx *a, const double *X, const double *H, const double *mu, double t, double *gX, double *gMs,
+                    double *gK1, double *gHa)
+{
+    const orc_mesh_desc *d = a->d;
+    const int n = a->n;
+    double *gH = a->tmp + 12 * (size_t)n, *w = a->tmp + 15 * (size_t)n, *lx = a->tmp + 18 * (size_t)n;
+    const double al = d->alpha, pre = -ORC_GAMMA * d->grel / (1.0 + al * al);
+    for (int i = 0; i < n; i++) {
+        const double *x = X + 3 * i, *h = H + 3 * i, *m = mu + 3 * i;
+        const double Ms = a->Ms[i], b = pre * al / Ms;
+        double xh = x[0] * h[0] + x[1] * h[1] + x[2] * h[2];
+        double mx = m[0] * x[0] + m[1] * x[1] + m[2] * x[2];
+        double mh = m[0] * h[0] + m[1] * h[1] + m[2] * h[2];
+        double xx = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        double hxm[3] = {h[1] * m[2] - h[2] * m[1], h[2] * m[0] - h[0] * m[2], h[0] * m[1] - h[1] * m[0]};
+        double mxx[3] = {m[1] * x[2] - m[2] * x[1], m[2] * x[0] - m[0] * x[2], m[0] * x[1] - m[1] * x[0]};
+        for (int c = 0; c < 3; c++) {
+            gX[3 * i + c] = pre * hxm[c] + b * (xh * m[c] + mx * h[c] - 2.0 * mh * x[c]);
+            gH[3 * i + c] = pre * mxx[c] + b * (mx * x[c] - xx * m[c]);
+        }
+        /* d/dMs of (alpha/Ms) X x (X x H): mu . (X (X.H) - H |X|^2) times -alpha pre / Ms^2 */
+        gMs[i] += -pre * al / (Ms * Ms) * (mx * xh - mh * xx);
+    }
+    /* Zeeman */
+    if ((d->modules & ORC_ZEEMAN) && d->Ha && d->nHa > 0) {
+        int idx = 0;
+        if (d->nHa > 1 && d->Ha_tspan > 0.0) {
+            idx = (int)floor(t / d->Ha_tspan * d->nHa);
+            if (idx < 0) idx = 0;
+            if (idx >= d->nHa) idx = d->nHa - 1;
+        }
+        for (int i = 0; i < n; i++)
+            for (int c = 0; c < 3; c++) gHa[3 * idx + c] += gH[3 * i + c];
+    }
+    /* demag: D is symmetric */
+    if (d->modules & ORC_DEMAG) {
+        orc_demag_apply(a->dm, gH, w, 0);
+        for (int i = 0; i < 3 * n; i++) gX[i] += w[i];
+    }
+    /* exchange: H = c (L X), c_i = 2 A / (mu0 Ms_i^2) */
+    if (d->modules & ORC_EXCH) {
+        for (int i = 0; i < n; i++) {
+            double ci = 2.0 * d->A / (ORC_MU0 * a->Ms[i] * a->Ms[i]);
+            for (int c = 0; c < 3; c++) w[3 * i + c] = ci * gH[3 * i + c];
+        }
+        adj_lap(d, w, lx);
+        for (int i = 0; i < 3 * n; i++) gX[i] += lx[i];
+        adj_lap(d, X, lx);
+        for (int i = 0; i < n; i++) {
+            double ci = 2.0 * d->A / (ORC_MU0 * a->Ms[i] * a->Ms[i]);
+            double dot = gH[3 * i] * lx[3 * i] + gH[3 * i + 1] * lx[3 * i + 1] + gH[3 * i + 2] * lx[3 * i + 2];
+            gMs[i] += dot * (-2.0 * ci / a->Ms[i]);
+        }
+    }
+    /* uniaxial anisotropy: H = kappa (X.e) e, kappa_i = 2 K1_i / (mu0 Ms_i^2) */
+    if (d->modules & ORC_ANIUNI) {
+        const double *e = d->ea;
+        for (int i = 0; i < n; i++) {
+            double Ms = a->Ms[i], kap = 2.0 * a->K1[i] / (ORC_MU0 * Ms * Ms);
+            double xe = X[3 * i] * e[0] + X[3 * i + 1] * e[1] + X[3 * i + 2] * e[2];
+            double ge = gH[3 * i] * e[0] + gH[3 * i + 1] * e[1] + gH[3 * i + 2] * e[2];
+            for (int c = 0; c < 3; c++) gX[3 * i + c] += kap * ge * e[c];
+            gK1[i] += xe * ge * 2.0 / (ORC_MU0 * Ms * Ms);
+            gMs[i] += xe * ge * (-2.0 * kap / Ms);
+        }
+    }
+}
+
+int orc_adjoint_rk4(const orc_mesh_desc *d, const double *m0, const double *target, int steps, double dt,
+                    double *loss, double *gMs, double *gK1, double *gHa)
+{
+    adj_ctx a;
+    a.d = d;
+    a.n = d->nx * d->ny * d->nz;
+    const int n = a.n;
+    double *Ms = (double *)malloc(sizeof(double) * n), *K1 = (double *)malloc(sizeof(double) * n);
+    for (int i = 0; i < n; i++) {
+        Ms[i] = d->Ms_map ? d->Ms_map[i] : d->Ms;
+        K1[i] = d->K1_map ? d->K1_map[i] : d->K1;
+    }
+    a.Ms = Ms; a.K1 = K1;
+    a.dm = (d->modules & ORC_DEMAG) ? orc_demag_create(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, fft_size(d->nx),
+                                                       fft_size(d->ny), fft_size(d->nz)) : 0;
+    a.tmp = (double *)calloc(21 * (size_t)n, sizeof(double));
+    size_t v3 = 3 * (size_t)n;
+    double *Ms_hist = (double *)malloc(sizeof(double) * v3 * (steps + 1));
+    double *tm = (double *)malloc(sizeof(double) * (steps + 1));
+    double *X[4], *H[4];
+    for (int s = 0; s < 4; s++) { X[s] = (double *)malloc(sizeof(double) * v3); H[s] = (double *)malloc(sizeof(double) * v3); }
+    double *Y = (double *)malloc(sizeof(double) * v3);
+    /* forward */
+    for (int i = 0; i < n; i++)
+        for (int c = 0; c < 3; c++) Ms_hist[3 * i + c] = Ms[i] * m0[3 * i + c];
+    tm[0] = 0.0;
+    for (int st = 0; st < steps; st++) {
+        adj_step(&a, Ms_hist + st * v3, tm[st], dt, X, H, Y, Ms_hist + (st + 1) * v3);
+        tm[st + 1] = tm[st] + dt;
+    }
+    /* loss and its gradient at the final state */
+    for (int i = 0; i < n; i++) gMs[i] = 0.0, gK1[i] = 0.0;
+    if (gHa && d->nHa > 0) memset(gHa, 0, sizeof(double) * 3 * d->nHa);
+    double *lam = (double *)malloc(sizeof(double) * v3), *lY = (double *)malloc(sizeof(double) * v3);
+    double *mu = (double *)malloc(sizeof(double) * v3), *gX = (double *)malloc(sizeof(double) * v3);
+    const double *MT = Ms_hist + steps * v3;
+    double L = 0.0;
+    for (int i = 0; i < n; i++)
+        for (int c = 0; c < 3; c++) {
+            double m = MT[3 * i + c] / Ms[i], r = m - target[3 * i + c];
+            L += r * r;
+            lam[3 * i + c] = 2.0 / n * r / Ms[i];
+            gMs[i] += 2.0 / n * r * (-m / Ms[i]);
+        }
+    *loss = L / n;
+    double dummyHa[3 * 256];
+    double *gHa_use = gHa ? gHa : dummyHa;
+    /* backward */
+    for (int st = steps - 1; st >= 0; st--) {
+        adj_step(&a, Ms_hist + st * v3, tm[st], dt, X, H, Y, gX);   /* recompute the stages */
+        for (int i = 0; i < n; i++) {
+            double *y = Y + 3 * i, nr = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+            double yl = (y[0] * lam[3 * i] + y[1] * lam[3 * i + 1] + y[2] * lam[3 * i + 2]) / nr;
+            gMs[i] += yl;
+            for (int c = 0; c < 3; c++) lY[3 * i + c] = Ms[i] / nr * (lam[3 * i + c] - yl * y[c] / nr);
+        }
+        /* lam <- dL/dM_st */
+        memcpy(lam, lY, sizeof(double) * v3);
+        for (int i = 0; i < (int)v3; i++) mu[i] = dt / 6 * lY[i];
+        adj_vjp(&a, X[3], H[3], mu, tm[st], gX, gMs, gK1, gHa_use);
+        for (int i = 0; i < (int)v3; i++) { lam[i] += gX[i]; mu[i] = dt / 3 * lY[i] + dt * gX[i]; }
+        adj_vjp(&a, X[2], H[2], mu, tm[st], gX, gMs, gK1, gHa_use);
+        for (int i = 0; i < (int)v3; i++) { lam[i] += gX[i]; mu[i] = dt / 3 * lY[i] + dt / 2 * gX[i]; }
+        adj_vjp(&a, X[1], H[1], mu, tm[st], gX, gMs, gK1, gHa_use);
+        for (int i = 0; i < (int)v3; i++) { lam[i] += gX[i]; mu[i] = dt / 6 * lY[i] + dt / 2 * gX[i]; }
+        adj_vjp(&a, X[0], H[0], mu, tm[st], gX, gMs, gK1, gHa_use);
+        for (int i = 0; i < (int)v3; i++) lam[i] += gX[i];
+    }
+    /* initial state M0 = Ms m0 */
+    for (int i = 0; i < n; i++)
+        gMs[i] += m0[3 * i] * lam[3 * i] + m0[3 * i + 1] * lam[3 * i + 1] + m0[3 * i + 2] * lam[3 * i + 2];
+    for (int s = 0; s < 4; s++) { free(X[s]); free(H[s]); }
+    free(Y); free(lam); free(lY); free(mu); free(gX); free(Ms_hist); free(tm); free(a.tmp); free(Ms); free(K1);
+    orc_demag_destroy(a.dm);
+    return 0;
+}

@@ -98,6 +98,14 @@ int orc_ml_eval(orc_ml *s, const double *M, double *H);
 int orc_ml_transfer(orc_ml *s, int layer, const double *M, double *Mc, const double *Hc, double *Hmesh);
 void orc_ml_destroy(orc_ml *s);
 
+/* ---- discrete adjoint of RK4 (FP64) ----
+ * One mesh, modules demag / exchange / uniaxial anisotropy (K2 = 0) / Zeeman (piecewise-constant
+ * samples, the sample at each step's start time), per-cell Ms and K1 maps; initial state Ms * m0;
+ * loss (1/n) sum_i |M_i(T)/Ms_i - target_i|^2 after `steps` steps of dt. Returns the loss and its
+ * gradients with respect to the Ms map, the K1 map and the 3 * nHa field samples (gHa may be NULL). */
+int orc_adjoint_rk4(const orc_mesh_desc *d, const double *m0, const double *target, int steps, double dt,
+                    double *loss, double *gMs, double *gK1, double *gHa);
+
 /* FP64 in-place complex DFT (fftw_shim.c) */
 void bm_oracle_fft(int n, double *data, int sign);
 

@@ -81,6 +81,7 @@ def oracle():
         L.orc_ml_transfer.argtypes = [P, I, DP, DP, DP, DP]
         L.orc_ml_destroy.argtypes = [P]
         L.orc_solver_set_multilayer.argtypes = [P, DP, I, IP]
+        L.orc_adjoint_rk4.argtypes = [ctypes.POINTER(MeshDesc), DP, DP, I, D, DP, DP, DP, DP]
         _orc = L
     return _orc
 
@@ -288,3 +289,37 @@ def tilted_z(n, seed, max_deg=15.0, Ms=1.0):
     ph = rng.uniform(0.0, 2 * np.pi, n)
     v = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=1)
     return v * Ms
+
+
+def orc_adjoint(mesh, m0, target, steps, dt):
+    """FP64 loss and gradients (Ms map, K1 map, field samples) of the oracle's discrete RK4 adjoint.
+    mesh: dict with n, h, Ms_map, K1_map, A, alpha, ea, modules, Ha (nHa x 3), Ha_tspan."""
+    d = MeshDesc()
+    d.nx, d.ny, d.nz = mesh["n"]
+    d.hx, d.hy, d.hz = mesh["h"]
+    d.Ms = 8e5; d.A = mesh.get("A", 1.3e-11); d.D = 0.0; d.alpha = mesh.get("alpha", 0.02)
+    d.grel = mesh.get("grel", 1.0); d.K1 = 0.0; d.K2 = 0.0
+    ea = mesh.get("ea", (0.0, 0.0, 1.0))
+    for k in range(3):
+        d.ea[k] = ea[k]
+    keep = []
+    for key in ("Ms_map", "K1_map"):
+        a = np.ascontiguousarray(np.asarray(mesh[key], dtype=np.float64).reshape(-1))
+        keep.append(a)
+        setattr(d, key, dp(a))
+    Ha = np.ascontiguousarray(np.asarray(mesh["Ha"], dtype=np.float64).reshape(-1))
+    keep.append(Ha)
+    d.Ha = dp(Ha)
+    d.nHa = Ha.size // 3
+    d.Ha_tspan = mesh["Ha_tspan"]
+    d.modules = mesh.get("modules", 1 | 2 | 8 | 16)
+    n = int(np.prod(mesh["n"]))
+    m0a = np.ascontiguousarray(np.asarray(m0, dtype=np.float64).reshape(-1))
+    ta = np.ascontiguousarray(np.asarray(target, dtype=np.float64).reshape(-1))
+    loss = np.zeros(1)
+    gMs = np.zeros(n)
+    gK = np.zeros(n)
+    gHa = np.zeros(Ha.size)
+    rc = oracle().orc_adjoint_rk4(ctypes.byref(d), dp(m0a), dp(ta), steps, dt, dp(loss), dp(gMs), dp(gK), dp(gHa))
+    assert rc == 0
+    return loss[0], gMs, gK, gHa.reshape(-1, 3)
