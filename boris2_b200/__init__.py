@@ -95,6 +95,7 @@ _SIGS = {
     "bm_ml_time_kernels": (_I, [_P, _I, _DP, _DP]),
     "bm_ml_tile": (_I, [_P, _IP]),
     "bm_set_batched": (_I, [_P, _I]),
+    "bm_adjoint_rk4": (_I, [_P, _I, _I, _DP, _I, _DP, _DP, _DP, _DP, _DP]),
 }
 
 
@@ -136,6 +137,7 @@ class Context:
         self._h = _P()
         _check(lib().bm_create(int(device), ctypes.byref(self._h)))
         self.meshes = []
+        self._nHa = 1
         _check(lib().bm_set_precision(self._h, int(precision)))
 
     def close(self):
@@ -185,9 +187,27 @@ class Context:
     def set_field(self, mesh=0, Ha=(0.0, 0.0, 0.0), t_span=0.0):
         a = np.ascontiguousarray(np.asarray(Ha, dtype=np.float64).reshape(-1, 3))
         _check(lib().bm_set_field(self._h, mesh, _dp(a), a.shape[0], float(t_span)))
+        self._nHa = a.shape[0]
 
     def set_precision(self, precision):
         _check(lib().bm_set_precision(self._h, int(precision)))
+
+    def adjoint_rk4(self, target, steps, ckpt_every=100, m0_scales_with_Ms=True, nHa=None):
+        """Run `steps` RK4 steps from the current state and return (loss, dMs, dK1, dHa, times_ms):
+        the loss (1/n) sum |m(T) - target|^2 and its exact gradients with respect to the per-cell Ms
+        and K1 maps and the applied-field samples (reverse mode through every stage, checkpoints every
+        ckpt_every steps). times_ms = (forward run, backward sweep) device time."""
+        n = self.ncells(0)
+        t = _vec(target, n)
+        loss = ctypes.c_double(0.0)
+        dMs = np.zeros(n)
+        dK1 = np.zeros(n)
+        k = self._nHa if nHa is None else int(nHa)
+        dHa = np.zeros(3 * max(k, 1))
+        tm = np.zeros(2)
+        _check(lib().bm_adjoint_rk4(self._h, int(steps), int(ckpt_every), _dp(t), int(bool(m0_scales_with_Ms)),
+                                    ctypes.byref(loss), _dp(dMs), _dp(dK1), _dp(dHa), _dp(tm)))
+        return loss.value, dMs, dK1, dHa[:3 * k].reshape(-1, 3), tuple(tm)
 
     def set_batched(self, on=True):
         """Advance all meshes with one launch per pass over a (mesh, tile) work list."""

@@ -1071,9 +1071,11 @@ int enqueue_prime(bm_ctx *c, int *count)
 }
 
 template <typename T>
-int enqueue_rk4_step(bm_ctx *c, int *count)
+int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void *const *cacheH = nullptr, void *cacheY = nullptr)
 {
     // buffers: 0 = M (step start, sM1), 2 = B, 3 = C ; evals 0..2
+    // cacheX/cacheH/cacheY (adjoint recompute, one mesh): each stage's input M, its field, and the
+    // update before renormalisation are also written there
     const int nm = (int)c->meshes.size();
     static const int min_buf[4] = {0, 2, 3, 2};
     for (int s = 0; s < 4; s++) {
@@ -1099,6 +1101,11 @@ int enqueue_rk4_step(bm_ctx *c, int *count)
                 a.Mout = B<T>(m, 0);
                 a.renorm = 1;
                 if (i == nm - 1) a.last_kind = BM_LAST_FINISH;
+            }
+            if (cacheX) {
+                a.copy_to = (T *)cacheX[s];
+                a.Hsave = (T *)cacheH[s];
+                if (s == 3) a.Ysave = (T *)cacheY;
             }
             v.push_back(a);
         }
@@ -1305,6 +1312,196 @@ int compute_field_T(bm_ctx *c, Mesh &m, int modules_mask, double *H)
     CK(cudaMemcpyAsync(H, m.stage64, sizeof(double) * 3 * m.n, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->s1_dirty = true;
+    return 0;
+}
+
+// ------------------------------------------------------------------ discrete adjoint of RK4
+// Forward: the step graph with a checkpoint of M and the time every k steps. Backward, per segment
+// from the last: restore the checkpoint, replay a captured graph that recomputes the segment's k
+// steps with the fused stage kernels also writing each stage's input, field and pre-normalisation
+// update into a k-slot cache, then replay a captured graph that walks the k steps in reverse
+// (renormalisation VJP, then per stage the LLG / local-field VJP, the demag of gH through the
+// convolution pipeline, and the Laplacian / accumulation kernel). Gradients accumulate in FP64;
+// the Zeeman gradient of each step is summed per step and mapped to its sample on the host with
+// the step start time the device used.
+struct AdjBufs {
+    std::vector<void *> all;
+    void *get(size_t bytes, bool zero, cudaStream_t s)
+    {
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        if (zero) cudaMemsetAsync(p, 0, bytes, s);
+        all.push_back(p);
+        return p;
+    }
+    ~AdjBufs() { for (auto p : all) cudaFree(p); }
+};
+
+template <typename T>
+int adjoint_T(bm_ctx *c, int steps, int k, const double *target, int m0_scales, double *loss, double *gMs_h, double *gK1_h,
+              double *gHa_h, double *times2)
+{
+    Mesh &m = c->meshes[0];
+    cudaStream_t s = c->stream;
+    const long long n = m.n;
+    const size_t v3 = sizeof(T) * 3 * (size_t)n;
+    const int S = steps / k;
+    AdjBufs ab;
+    auto need = [&](void *p) { return p != nullptr; };
+    // forward with checkpoints
+    if (c->s1_dirty) {
+        int cnt = 0;
+        if (int rc = enqueue_prime<T>(c, &cnt)) return rc;
+        c->s1_dirty = false;
+    }
+    if (!c->gexec || c->graph_eval != c->eval) {
+        if (int rc = build_graph<T>(c)) return rc;
+    }
+    if (int rc = read_state(c)) return rc;
+    const StepState st0 = c->host_st;
+    void *ckM = ab.get(v3 * S, false, s), *ckT = ab.get(sizeof(double) * S, false, s);
+    if (!need(ckM) || !need(ckT)) return fail(BM_ENOMEM, "adjoint checkpoints");
+    cudaEvent_t e0, e1, e2, e3;
+    CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1)); CK(cudaEventCreate(&e2)); CK(cudaEventCreate(&e3));
+    CK(cudaEventRecord(e0, s));
+    for (int g = 0; g < S; g++) {
+        CK(cudaMemcpyAsync((char *)ckM + v3 * g, m.buf[0], v3, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync((double *)ckT + g, &c->st->time, sizeof(double), cudaMemcpyDeviceToDevice, s));
+        for (int q = 0; q < k; q++) CK(cudaGraphLaunch(c->gexec, s));
+    }
+    CK(cudaEventRecord(e1, s));
+    if (int rc = read_state(c)) return rc;
+    const StepState st_end = c->host_st;
+    std::vector<double> tck(S);
+    CK(cudaMemcpy(tck.data(), ckT, sizeof(double) * S, cudaMemcpyDeviceToHost));
+    // adjoint buffers
+    void *Mfin = ab.get(v3, false, s), *tgt = ab.get(sizeof(double) * 3 * n, false, s);
+    void *lam = ab.get(v3, true, s), *lamY = ab.get(v3, true, s), *mu = ab.get(v3, true, s), *gH = ab.get(v3, true, s);
+    void *gXd = ab.get(v3, true, s), *w = ab.get(v3, true, s), *gD = ab.get(v3, true, s);
+    void *gMs = ab.get(sizeof(double) * n, true, s), *gK1 = ab.get(sizeof(double) * n, true, s);
+    void *gHs = ab.get(sizeof(double) * 3 * k, true, s), *gHall = ab.get(sizeof(double) * 3 * (size_t)steps, true, s);
+    void *lossd = ab.get(sizeof(double), true, s);
+    void *cache = ab.get(v3 * 9 * (size_t)k, false, s);
+    for (void *p : {Mfin, tgt, lam, lamY, mu, gH, gXd, w, gD, gMs, gK1, gHs, gHall, lossd, cache})
+        if (!need(p)) return fail(BM_ENOMEM, "adjoint buffers");
+    auto slot = [&](int j, int q) -> void * { return (char *)cache + v3 * (9 * (size_t)j + q); };   // 0..3 X, 4..7 H, 8 Y
+    CK(cudaMemcpyAsync(Mfin, m.buf[0], v3, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(tgt, target, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    AdjArgs<T> aa;
+    memset(&aa, 0, sizeof(aa));
+    aa.nx = m.nx; aa.ny = m.ny; aa.nz = m.nz; aa.n = n;
+    aa.hx = (T)m.h[0]; aa.hy = (T)m.h[1]; aa.hz = (T)m.h[2];
+    aa.Ms_map = (const T *)m.Msd; aa.K1_map = (const T *)m.K1d;
+    aa.Ms = (T)m.Ms; aa.K1 = (T)m.K1; aa.A = (T)m.A; aa.alpha = (T)m.alpha; aa.grel = (T)m.grel;
+    double en = std::sqrt(m.ea[0] * m.ea[0] + m.ea[1] * m.ea[1] + m.ea[2] * m.ea[2]);
+    for (int q = 0; q < 3; q++) aa.ea[q] = (T)(en > 0 ? m.ea[q] / en : 0.0);
+    aa.modules = m.modules;
+    const double dt = c->dt;
+    // the two segment graphs
+    cudaGraph_t gr = nullptr, gb = nullptr;
+    cudaGraphExec_t xr = nullptr, xb = nullptr;
+    int cnt = 0, rc = 0;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue_prime<T>(c, &cnt);
+    for (int j = 0; j < k && !rc; j++) {
+        void *cx[4] = {slot(j, 0), slot(j, 1), slot(j, 2), slot(j, 3)}, *ch[4] = {slot(j, 4), slot(j, 5), slot(j, 6), slot(j, 7)};
+        rc = enqueue_rk4_step<T>(c, &cnt, cx, ch, slot(j, 8));
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &gr);
+    if (rc || ce != cudaSuccess) { if (gr) cudaGraphDestroy(gr); return rc ? rc : fail(BM_ECUDA, "adjoint recompute capture"); }
+    CK(cudaGraphInstantiate(&xr, gr, 0));
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    static const double cYs[4] = {0.0, 1.0 / 6, 1.0 / 3, 1.0 / 3}, cXs[4] = {0.0, 0.5, 0.5, 1.0};
+    for (int j = k - 1; j >= 0 && !rc; j--) {
+        rc = launch_adj_renorm<T>(aa, (T *)lam, (const T *)slot(j, 8), (T *)lamY, (T *)mu, dt, (double *)gMs, s);
+        for (int q = 3; q >= 0 && !rc; q--) {
+            rc = launch_adj_vjp_a<T>(aa, (const T *)slot(j, q), (const T *)slot(j, 4 + q), (const T *)mu, (T *)gH, (T *)gXd,
+                                     (T *)w, (double *)gMs, (double *)gK1, (double *)gHs + 3 * j, s);
+            if (!rc && (m.modules & BM_DEMAG)) {
+                // gD = D gH through the convolution pipeline
+                StageArgs<T> a = stage_args<T>(c, m);
+                a.mode = BM_MODE_UPDATE;
+                a.Min = (const T *)gH; a.Mbase = (const T *)gH;
+                a.st = nullptr;
+                rc = launch_stage<T>(a, s);
+                if (!rc) rc = enqueue_yz<T>(c, m, BM_GATE_ALWAYS, &cnt);
+                if (!rc) {
+                    StageArgs<T> b = stage_args<T>(c, m);
+                    b.mode = BM_MODE_HEFF;
+                    b.modules = BM_DEMAG;
+                    b.do_xfwd = 0;
+                    b.st = nullptr;
+                    b.Min = (const T *)gH;
+                    b.Hout = (T *)gD;
+                    rc = launch_stage<T>(b, s);
+                }
+            }
+            if (!rc)
+                rc = launch_adj_vjp_c<T>(aa, (const T *)gXd, (const T *)w, (m.modules & BM_DEMAG) ? (const T *)gD : nullptr,
+                                         (const T *)lamY, (T *)lam, (T *)mu, cYs[q] * dt, cXs[q] * dt, q > 0 ? 1 : 0, s);
+        }
+    }
+    ce = cudaStreamEndCapture(s, &gb);
+    if (rc || ce != cudaSuccess) {
+        if (gb) cudaGraphDestroy(gb);
+        cudaGraphExecDestroy(xr); cudaGraphDestroy(gr);
+        return rc ? fail(BM_ECUDA, "adjoint backward launch failed (" + std::to_string(rc) + ")") : fail(BM_ECUDA, "adjoint capture");
+    }
+    cudaError_t ie = cudaGraphInstantiate(&xb, gb, 0);
+    if (ie != cudaSuccess) { cudaGraphDestroy(gb); cudaGraphExecDestroy(xr); cudaGraphDestroy(gr); return fail(BM_ECUDA, "adjoint instantiate"); }
+    // backward sweep
+    CK(cudaEventRecord(e2, s));
+    rc = launch_adj_loss<T>(aa, (const T *)Mfin, (const double *)tgt, (T *)lam, (double *)gMs, (double *)lossd, s);
+    for (int g = S - 1; g >= 0 && !rc; g--) {
+        CK(cudaMemcpyAsync(m.buf[0], (char *)ckM + v3 * g, v3, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(&c->st->time, (double *)ckT + g, sizeof(double), cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(&c->st->stagetime, (double *)ckT + g, sizeof(double), cudaMemcpyDeviceToDevice, s));
+        CK(cudaGraphLaunch(xr, s));
+        CK(cudaGraphLaunch(xb, s));
+        CK(cudaMemcpyAsync((double *)gHall + 3 * (size_t)k * g, gHs, sizeof(double) * 3 * k, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemsetAsync(gHs, 0, sizeof(double) * 3 * k, s));
+    }
+    if (!rc && m0_scales) rc = launch_adj_m0<T>(aa, (const T *)ckM, (const T *)lam, (double *)gMs, s);
+    CK(cudaEventRecord(e3, s));
+    CK(cudaStreamSynchronize(s));
+    cudaGraphExecDestroy(xb); cudaGraphDestroy(gb);
+    cudaGraphExecDestroy(xr); cudaGraphDestroy(gr);
+    if (rc) return fail(BM_ECUDA, "adjoint launch failed (" + std::to_string(rc) + ")");
+    float f_ms = 0.f, b_ms = 0.f;
+    cudaEventElapsedTime(&f_ms, e0, e1);
+    cudaEventElapsedTime(&b_ms, e2, e3);
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
+    if (times2) { times2[0] = f_ms; times2[1] = b_ms; }
+    // results
+    CK(cudaMemcpy(loss, lossd, sizeof(double), cudaMemcpyDeviceToHost));
+    if (gMs_h) CK(cudaMemcpy(gMs_h, gMs, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (gK1_h) CK(cudaMemcpy(gK1_h, gK1, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (gHa_h) {
+        const int nHa = m.nHa;
+        for (int q = 0; q < 3 * nHa; q++) gHa_h[q] = 0.0;
+        if ((m.modules & BM_ZEEMAN) && nHa > 0) {
+            std::vector<double> gall(3 * (size_t)steps);
+            CK(cudaMemcpy(gall.data(), gHall, sizeof(double) * 3 * steps, cudaMemcpyDeviceToHost));
+            for (int g = 0; g < S; g++) {
+                double t = tck[g];
+                for (int j = 0; j < k; j++) {
+                    int hi = 0;
+                    if (nHa > 1 && m.Ha_tspan > 0.0) {
+                        hi = (int)std::floor(t / m.Ha_tspan * nHa);
+                        hi = hi < 0 ? 0 : (hi >= nHa ? nHa - 1 : hi);
+                    }
+                    for (int q = 0; q < 3; q++) gHa_h[3 * hi + q] += gall[3 * ((size_t)g * k + j) + q];
+                    t = t + dt;
+                }
+            }
+        }
+    }
+    // leave the context at the end of the forward run
+    CK(cudaMemcpy(m.buf[0], Mfin, v3, cudaMemcpyDeviceToDevice));
+    c->host_st = st_end;
+    CK(cudaMemcpy(c->st, &c->host_st, sizeof(StepState), cudaMemcpyHostToDevice));
+    c->s1_dirty = true;
+    (void)st0;
     return 0;
 }
 
@@ -1527,6 +1724,25 @@ int bm_ml_tile(bm_ctx *c, int *W)
     if (!c->ml) return fail(BM_ESTATE, "multilayered convolution is off");
     if (W) *W = c->ml->W;
     return 0;
+}
+
+int bm_adjoint_rk4(bm_ctx *c, int steps, int ckpt_every, const double *target, int m0_scales_with_Ms, double *loss,
+                   double *dMs, double *dK1, double *dHa, double *times_ms)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (!target || !loss) return fail(BM_EINVAL, "null target or loss");
+    if (c->meshes.size() != 1) return fail(BM_EUNSUPPORTED, "adjoint: one mesh");
+    if (c->eval != BM_RK4) return fail(BM_EUNSUPPORTED, "adjoint: RK4 only");
+    if (c->ml_mode >= 0 || c->batched) return fail(BM_EUNSUPPORTED, "adjoint: no multilayer or batching");
+    if (ckpt_every < 1 || steps < 1 || steps % ckpt_every) return fail(BM_EINVAL, "adjoint: steps must be a positive multiple of ckpt_every");
+    const Mesh &m0 = c->meshes[0];
+    if (m0.modules & ~(BM_DEMAG | BM_EXCH | BM_ANIUNI | BM_ZEEMAN)) return fail(BM_EUNSUPPORTED, "adjoint: demag, exchange, anisotropy, Zeeman only");
+    if (m0.K2 != 0.0) return fail(BM_EUNSUPPORTED, "adjoint: K2 must be 0");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    return (c->precision == BM_FP64)
+               ? adjoint_T<double>(c, steps, ckpt_every, target, m0_scales_with_Ms, loss, dMs, dK1, dHa, times_ms)
+               : adjoint_T<float>(c, steps, ckpt_every, target, m0_scales_with_Ms, loss, dMs, dK1, dHa, times_ms);
 }
 
 int bm_prepare(bm_ctx *c)

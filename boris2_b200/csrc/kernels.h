@@ -89,6 +89,7 @@ struct StageArgs {
     const T *Min, *Mbase;
     T *Mout, *copy_to, *ev_out, *Hout;
     const T *Hd;         // demag field per cell from a multilayered convolution (added when set)
+    T *Hsave, *Ysave;    // adjoint stage cache: the field used by LLG, the update before renormalisation
     int nev;
     const T *ev[6];
     double cev[6];
@@ -133,3 +134,28 @@ template <typename T>
 int launch_stage_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
 int stage_reg_q(int LX);   // threads per x line of the register stage kernel (0: generic kernel)
 int launch_scalar_reset(StepState *st, cudaStream_t s);
+
+// ---------------------------------------------------------------- discrete adjoint of RK4
+// Per-cell material of the adjoint kernels (single mesh): Ms and K1 maps or constants.
+template <typename T>
+struct AdjArgs {
+    int nx, ny, nz;
+    long long n;
+    T hx, hy, hz;
+    const T *Ms_map, *K1_map;
+    T Ms, K1, A, alpha, grel;
+    T ea[3];
+    int modules;
+};
+template <typename T>
+int launch_adj_loss(const AdjArgs<T> &a, const T *M, const double *target, T *lam, double *gMs, double *loss, cudaStream_t s);
+template <typename T>
+int launch_adj_renorm(const AdjArgs<T> &a, T *lam, const T *Y, T *lamY, T *mu, double dt, double *gMs, cudaStream_t s);
+template <typename T>
+int launch_adj_vjp_a(const AdjArgs<T> &a, const T *X, const T *H, const T *mu, T *gH, T *gXd, T *w, double *gMs, double *gK1,
+                     double *gHa3, cudaStream_t s);
+template <typename T>
+int launch_adj_vjp_c(const AdjArgs<T> &a, const T *gXd, const T *w, const T *gD, const T *lamY, T *lam, T *mu, double cY,
+                     double cX, int write_mu, cudaStream_t s);
+template <typename T>
+int launch_adj_m0(const AdjArgs<T> &a, const T *M0, const T *lam, double *gMs, cudaStream_t s);

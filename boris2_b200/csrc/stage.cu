@@ -271,6 +271,10 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 for (int c = 0; c < 3; c++) a.Hout[c * n + cell] = H[c];
                 continue;
             }
+            if (a.Hsave) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.Hsave[c * n + cell] = H[c];
+            }
             T mxh[3] = {m[1] * H[2] - m[2] * H[1], m[2] * H[0] - m[0] * H[2], m[0] * H[1] - m[1] * H[0]};
             T mu[3] = {m[0] / Ms, m[1] / Ms, m[2] / Ms};
             T mmxh[3] = {mu[1] * mxh[2] - mu[2] * mxh[1], mu[2] * mxh[0] - mu[0] * mxh[2], mu[0] * mxh[1] - mu[1] * mxh[0]};
@@ -303,6 +307,10 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             T sum = crhs * rhs[c];
             for (int i = 0; i < a.nev; i++) sum += cev[i] * acc.ev(i, r, c, x, cell);
             mn[c] = acc.mb(r, c, x, cell) + sum;
+        }
+        if (a.Ysave) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.Ysave[c * n + cell] = mn[c];
         }
         if (a.renorm) {
             T f = Ms / sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);

@@ -138,6 +138,18 @@ int bm_ml_time_kernels(bm_ctx *ctx, int reps, double *ms6, double *bytes6);
 /* Columns per block of the fused multilayer z pass (chosen by timing at setup). */
 int bm_ml_tile(bm_ctx *ctx, int *W);
 
+/* Discrete adjoint of RK4 (no counterpart in the reference): from the current state, run `steps`
+ * RK4 steps (a checkpoint of M every ckpt_every steps), evaluate the loss
+ * L = (1/n) sum_i |M_i(T)/Ms_i - target_i|^2 (target: AoS unit vectors, 3n doubles) and its exact
+ * gradients by reverse mode through every stage: dMs (n, per-cell Ms), dK1 (n, per-cell K1 of the
+ * uniaxial anisotropy) and dHa (3 * nsamples of bm_set_field). m0_scales_with_Ms: the initial M is
+ * Ms * m0, so L also depends on Ms through it. One mesh; modules demag, exchange, anisotropy
+ * (K2 = 0) and Zeeman; steps a multiple of ckpt_every. times_ms (optional, 2 doubles): device time
+ * of the forward run and of the backward sweep. The context is left at the end of the run.
+ * Any output pointer except loss may be NULL. */
+int bm_adjoint_rk4(bm_ctx *ctx, int steps, int ckpt_every, const double *target, int m0_scales_with_Ms, double *loss,
+                   double *dMs, double *dK1, double *dHa, double *times_ms);
+
 /* Allocate and build everything for the current configuration now (kernels, tiles). */
 int bm_prepare(bm_ctx *ctx);
 
