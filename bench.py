@@ -91,6 +91,59 @@ TRAFFIC_PER_CELL = {("film3d", "stage"): 246.87e6 / (512 * 512 * 8),
                     ("multilayer", "ml_zmid"): 383.30e6 / (512 * 512 + 256 * 256 * 2 + 512 * 512)}
 
 
+def adjoint_problem(seed=4):
+    """The differentiation workload: film 256 x 256 x 1 of 4 x 4 x 3 nm; Ms map 8e5 (1 + 0.1 g), g a
+    unit-variance Gaussian random field of 20 nm correlation length (white noise filtered by
+    exp(-k^2 l^2 / 4) in Fourier space, seeded); K1 map ~ U[0, 2e5] along z; A = 1.3e-11, alpha = 0.02;
+    64 piecewise-constant field samples ~ N(0, 5e3^2) per component over 1 ns; m0 = +z tilted by up
+    to 15 degrees; target = random unit vectors (seeded); RK4 dt = 1e-13, 10000 steps, checkpoint
+    every 100."""
+    rng = np.random.default_rng(seed)
+    nx = ny = 256
+    h = 4e-9
+    white = rng.normal(size=(ny, nx))
+    kx = 2 * np.pi * np.fft.fftfreq(nx, d=h)
+    ky = 2 * np.pi * np.fft.fftfreq(ny, d=h)
+    k2 = ky[:, None] ** 2 + kx[None, :] ** 2
+    g = np.real(np.fft.ifft2(np.fft.fft2(white) * np.exp(-k2 * (20e-9) ** 2 / 4)))
+    g = (g - g.mean()) / g.std()
+    Ms = 8e5 * (1 + 0.1 * g.reshape(-1))
+    K1 = rng.uniform(0, 2e5, nx * ny)
+    Ha = rng.normal(0, 5e3, (64, 3))
+    th = np.deg2rad(rng.uniform(0, 15.0, nx * ny))
+    ph = rng.uniform(0, 2 * np.pi, nx * ny)
+    m0 = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=1)
+    t = rng.normal(size=(nx * ny, 3))
+    t /= np.linalg.norm(t, axis=1)[:, None]
+    return dict(n=(nx, ny, 1), h=(h, h, 3e-9), Ms=Ms, K1=K1, Ha=Ha, t_span=1e-9, m0=m0, target=t, A=1.3e-11,
+                alpha=0.02, dt=1e-13, steps=10000, ckpt=100)
+
+
+def adjoint_rate(bm, prec, device, steps=None):
+    """Forward and backward device time of the differentiation workload (gradients of the loss
+    with respect to the Ms map, K1 map and field samples)."""
+    p = adjoint_problem()
+    steps = steps or p["steps"]
+    c = bm.Context(device=device, precision=prec)
+    c.add_mesh(p["n"], p["h"])
+    c.set_material(0, Ms=8e5, A=p["A"], alpha=p["alpha"], ea=(0, 0, 1))
+    c.set_material_maps(0, Ms_map=p["Ms"], K1_map=p["K1"])
+    c.set_modules(0, 1 | 2 | 8 | 16)
+    c.set_field(0, p["Ha"], p["t_span"])
+    c.setode("RK4", p["dt"])
+    c.set_m(p["m0"] * p["Ms"][:, None])
+    c.run(2)                                   # warm-up: kernels, tiles, graph
+    c.set_m(p["m0"] * p["Ms"][:, None])
+    loss, dMs, dK1, dHa, (f_ms, b_ms) = c.adjoint_rk4(p["target"], steps, p["ckpt"], True, nHa=64)
+    c.close()
+    ncell = p["n"][0] * p["n"][1]
+    return {"workload": "adjoint_film256 (RK4, %d steps, checkpoint every %d)" % (steps, p["ckpt"]), "loss": loss,
+            "forward_ms": f_ms, "backward_ms": b_ms, "adjoint_over_forward": b_ms / f_ms,
+            "forward_Mcell_steps_per_s": ncell * steps / (f_ms * 1e-3) / 1e6,
+            "grad_norms": {"Ms": float(np.linalg.norm(dMs)), "K1": float(np.linalg.norm(dK1)),
+                           "Ha": float(np.linalg.norm(dHa))}}
+
+
 def nice(n):
     b = 1
     while b < n:
@@ -510,6 +563,12 @@ def main():
                                    "step_frac_of_peak": pb / (bx["ms_per_step"] * 1e-3) / 1e9 / peak}
             except Exception as e:
                 out["batching"] = {"error": str(e)}
+        # the differentiation workload: adjoint / forward device time
+        if not ml and args.config == "film3d_512x512x16":
+            try:
+                out["adjoint"] = adjoint_rate(bm, bm.MIXED, local)
+            except Exception as e:
+                out["adjoint"] = {"error": str(e)}
         if not args.no_cpu_baseline:
             try:
                 out["cpu_baseline"] = cpu_reference_rate(cfg)
