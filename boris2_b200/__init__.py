@@ -96,6 +96,7 @@ _SIGS = {
     "bm_ml_tile": (_I, [_P, _IP]),
     "bm_set_batched": (_I, [_P, _I]),
     "bm_adjoint_rk4": (_I, [_P, _I, _I, _DP, _I, _DP, _DP, _DP, _DP, _DP]),
+    "bm_debug_time_stage": (_I, [_P, _I, _I, _I, _I, _DP]),
 }
 
 

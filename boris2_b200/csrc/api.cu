@@ -2068,6 +2068,48 @@ int bm_time_kernels(bm_ctx *c, int mesh, int reps, double *ms4, double *bytes4)
                                      : time_kernels_T<float>(c, m, reps, ms4, bytes4);
 }
 
+// device time (ms per launch) of the stage kernel in one mode on the mesh's own buffers
+// (diagnostics): mode 0 stage update with nev earlier evaluations, 1 x forward only (UPDATE,
+// nev = 0), 2 fields only (HEFF: x inverse + field terms)
+int bm_debug_time_stage(bm_ctx *c, int mesh, int mode, int nev, int reps, double *ms)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!ms || reps < 1 || nev < 0 || nev > 5) return fail(BM_EINVAL, "args");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    Mesh &m = c->meshes[mesh];
+    auto run = [&](auto tag) -> int {
+        using T = decltype(tag);
+        T *tmp = nullptr;
+        if (cudaMalloc(&tmp, sizeof(T) * 9 * m.n) != cudaSuccess) return fail(BM_ENOMEM, "tmp");
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.st = nullptr;
+        a.Min = (const T *)m.buf[0];
+        a.Mbase = (const T *)m.buf[0];
+        if (mode == 0) {
+            a.mode = BM_MODE_STAGE;
+            a.nev = nev;
+            for (int i = 0; i < nev; i++) a.ev[i] = (const T *)m.buf[0];
+            a.ev_out = tmp;
+            a.Mout = tmp + 3 * m.n;
+        } else if (mode == 1) {
+            a.mode = BM_MODE_UPDATE;
+            a.nev = 0;
+        } else {
+            a.mode = BM_MODE_HEFF;
+            a.do_xfwd = 0;
+            a.Hout = tmp + 6 * m.n;
+        }
+        float t = time_launches(c->stream, [&]() { return launch_stage<T>(a, c->stream); }, reps);
+        cudaStreamSynchronize(c->stream);
+        cudaFree(tmp);
+        c->s1_dirty = true;
+        *ms = t;
+        return t > 1e29f ? fail(BM_ECUDA, "launch failed") : 0;
+    };
+    return (c->precision == BM_FP64) ? run(double()) : run(float());
+}
+
 int bm_tiles(bm_ctx *c, int mesh, int *tiles4)
 {
     if (int rc = check_mesh(c, mesh)) return rc;

@@ -203,6 +203,9 @@ int bm_tiles(bm_ctx *ctx, int mesh, int *tiles4);
 /* Test hooks (used by the test suite only). */
 /* FP64 demag kernel spectra (octant (Nx/2+1)(Ny/2+1)(Nz/2+1), 6 components xx,yy,zz,xy,xz,yz). */
 int bm_debug_kernels(bm_ctx *ctx, int mesh, double *K6);
+/* Device time of the stage kernel alone in one mode (0 stage update with nev evaluations, 1 x
+ * forward only, 2 x inverse + field terms), ms per launch. */
+int bm_debug_time_stage(bm_ctx *ctx, int mesh, int mode, int nev, int reps, double *ms);
 /* Raw FP64 tensor octant values D(i,j,k) for i<nx, j<ny, k<nz: 6 per point. */
 int bm_debug_tensor(int device, int nx, int ny, int nz, double hx, double hy, double hz, double *oct6);
 /* Batched complex FFT on the device of `howmany` contiguous lines of length L (in place,
