@@ -311,10 +311,13 @@ class Context:
         return ms, by
 
     def tiles(self, mesh=0):
-        """Autotuned tile shapes: 2D y width, 3D y width, z width, stage rows per block."""
+        """Autotuned tile shapes: 2D y width, 3D y width, z width, stage rows per block (negative
+        when the per-cell rows are prefetched), stage x-transform variant (1: radix-8 Stockham)."""
         t = (ctypes.c_int * 4)()
         _check(lib().bm_tiles(self._h, mesh, t))
-        return {"ymid2d_W": t[0], "ypass_W": t[1], "zmid_W": t[2], "stage_rows": t[3]}
+        sgn = -1 if t[3] < 0 else 1
+        return {"ymid2d_W": t[0], "ypass_W": t[1], "zmid_W": t[2], "stage_rows": sgn * (abs(t[3]) % 100),
+                "stage_xv": abs(t[3]) // 100}
 
     def stats(self):
         st = Stats()

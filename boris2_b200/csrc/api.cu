@@ -69,7 +69,7 @@ struct Mesh {
     long long n = 0;
     int Nx = 1, Ny = 1, Nz = 1, LX = 1;
     FFTPlan px, py, pz;
-    int W2 = 1, Wy = 1, Wz = 1, rpb = 1, staged = 0;
+    int W2 = 1, Wy = 1, Wz = 1, rpb = 1, staged = 0, xv = 0;
     // device (element type depends on the context precision)
     void *buf[4] = {nullptr, nullptr, nullptr, nullptr};   // A (M), P (sM1), B, C
     void *ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -288,7 +288,7 @@ void choose_tiles(Mesh &m)
     }
     // stage kernel rows per block
     {
-        int tpl = stage_reg_q(m.LX) ? stage_reg_q(m.LX) : m.px.tpl;
+        int tpl = stage_reg_q(m.LX, m.xv) ? stage_reg_q(m.LX, m.xv) : m.px.tpl;
         int rpb = lim / (3 * tpl);
         if (rpb < 1) rpb = 1;
         while (rpb > 1 && ((3 * rpb * tpl + 31) & ~31) > lim) rpb--;
@@ -490,22 +490,26 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
         a.ev[0] = (const T *)m.buf[0]; a.ev[1] = (const T *)m.buf[0];
         a.ev_out = tmp;
         a.Mout = tmp + 3 * m.n;
-        float best = 1e30f; int br = m.rpb, bs = 0;
+        float best = 1e30f; int br = m.rpb, bs = 0, bx = 0;
         int rows = m.ny * m.nz;
-        const int tpl = stage_reg_q(m.LX) ? stage_reg_q(m.LX) : m.px.tpl;
-        // rows per block x (per-cell rows prefetched to shared memory or read from global);
-        // staging applies to the register kernel only
-        for (int stg = 0; stg <= (stage_reg_q(m.LX) ? 1 : 0); stg++)
-            for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
-                if (((3 * rpb * tpl + 31) & ~31) > lim) break;
-                if ((size_t)3 * rpb * padded_len(m.LX) * cs > 200 * 1024) break;
-                a.rpb = rpb;
-                a.staged = stg;
-                float t = time_launches(s, [&]() { return launch_stage<T>(a, s); }, reps);
-                if (t < best) { best = t; br = rpb; bs = stg; }
-            }
+        const bool reg = stage_reg_q(m.LX) != 0;
+        // x-transform variant x rows per block x (per-cell rows prefetched to shared memory or
+        // read from global); variants and staging apply to the register kernels only
+        for (int xv = 0; xv <= (reg ? 1 : 0); xv++)
+            for (int stg = 0; stg <= (reg ? 1 : 0); stg++)
+                for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
+                    const int tpl = reg ? stage_reg_q(m.LX, xv) : m.px.tpl;
+                    if (((3 * rpb * tpl + 31) & ~31) > lim) break;
+                    if ((size_t)3 * rpb * padded_len(m.LX) * cs > 200 * 1024) break;
+                    a.rpb = rpb;
+                    a.staged = stg;
+                    a.xv = xv;
+                    float t = time_launches(s, [&]() { return launch_stage<T>(a, s); }, reps);
+                    if (t < best) { best = t; br = rpb; bs = stg; bx = xv; }
+                }
         m.rpb = br;
         m.staged = bs;
+        m.xv = bx;
     }
     cudaStreamSynchronize(s);
     cudaFree(tmp);
@@ -695,6 +699,8 @@ int prepare_T(bm_ctx *c)
             m.W2 = t4[0]; m.Wy = t4[1]; m.Wz = t4[2]; m.rpb = t4[3];
             const char *sr = getenv("BM_STAGE_ROWS");
             m.staged = (sr && sr[0] == '1') ? 1 : 0;
+            const char *sx = getenv("BM_STAGE_XV");
+            m.xv = (sx && sx[0] == '1' && stage_reg_q(m.LX)) ? 1 : 0;
         } else if (c->autotune && !c->batched) autotune_mesh<T>(c, m);
     }
     if (int rc = prepare_ml<T>(c)) { for (auto &mm : c->meshes) free_mesh(mm); free_ml(c); return rc; }
@@ -770,6 +776,7 @@ StageArgs<T> stage_args(bm_ctx *c, Mesh &m)
     a.n = m.n;
     a.do_xfwd = (m.modules & BM_DEMAG) ? 1 : 0;
     a.staged = m.staged;
+    a.xv = m.xv;
     if (m.ml_role == 2) {
         // multilayer with mesh transfer: the demag field arrives in Hd, no x transforms here
         a.modules &= ~BM_DEMAG;
@@ -2115,7 +2122,7 @@ int bm_tiles(bm_ctx *c, int mesh, int *tiles4)
     if (int rc = check_mesh(c, mesh)) return rc;
     if (!tiles4) return fail(BM_EINVAL, "null out");
     Mesh &m = c->meshes[mesh];
-    tiles4[0] = m.W2; tiles4[1] = m.Wy; tiles4[2] = m.Wz; tiles4[3] = m.staged ? -m.rpb : m.rpb;
+    tiles4[0] = m.W2; tiles4[1] = m.Wy; tiles4[2] = m.Wz; tiles4[3] = (m.staged ? -1 : 1) * (m.rpb + 100 * m.xv);
     return 0;
 }
 

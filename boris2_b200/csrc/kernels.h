@@ -97,6 +97,7 @@ struct StageArgs {
     int renorm, mode, do_xfwd, last_kind, gate;
     long long n;         // cells
     int staged;          // prefetch the per-cell input rows into shared memory (register kernel)
+    int xv;              // register x transform: 0 two-level P x Q, 1 radix-8 Stockham at 64 (FP32) registers
 };
 
 // Shared-memory row staging of the register stage kernel: per block row, kr rows of nx values:
@@ -132,7 +133,7 @@ template <typename T>
 int launch_yz_batch(int kind, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
 template <typename T>
 int launch_stage_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
-int stage_reg_q(int LX);   // threads per x line of the register stage kernel (0: generic kernel)
+int stage_reg_q(int LX, int xv = 0);   // threads per x line of the register stage kernel, variant xv (0: generic kernel)
 int launch_scalar_reset(StepState *st, cudaStream_t s);
 
 // ---------------------------------------------------------------- discrete adjoint of RK4

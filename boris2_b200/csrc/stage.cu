@@ -487,12 +487,28 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_batch(const StageArgs<T> 
 }
 
 // ---------------------------------------------------------------------------------------------
-// Register kernel for LX = P * Q (P <= Q <= 32): each x line is transformed with one DFT_Q and
-// one DFT_P per thread in registers and one shared transpose (padded one slot per P elements, so
-// both access patterns are conflict-free). The packed-spectrum split (xinv_pre / xfwd_post) and
-// the per-cell work stay in shared memory in natural order.
+// Register kernels for power-of-two LX (16 .. 1024). Two x-transform variants:
+//   xv 0: LX = P * Q (P <= Q <= 32): one DFT_Q and one DFT_P per thread in registers around one
+//         shared transpose (line padded one slot per P elements, so both access patterns are
+//         conflict-free); Q threads per line.
+//   xv 1: radix-8 Stockham (the last pass takes the remaining radix 2 or 4), LX / 8 threads per
+//         line each holding 8 values per pass, line padded one slot per 16 elements; compiled
+//         with a register cap (64 FP32, 128 FP64) so that more rows are resident per SM.
+// The packed-spectrum split (xinv_pre / xfwd_post) and the per-cell work stay in shared memory
+// in natural order.
 template <int P> struct addrP {
     __device__ __forceinline__ int operator()(int e) const { return e + e / P; }
+};
+
+template <int LX> struct xr_pq {
+    static constexpr int P = LX == 16 ? 4 : LX == 32 ? 4 : LX == 64 ? 8 : LX == 128 ? 8 : LX == 256 ? 16 : LX == 512 ? 16 : 32;
+    static constexpr int Q = LX / P;
+};
+
+template <int LX, int XV> struct xr_cfg {
+    static constexpr int PAD = XV == 0 ? xr_pq<LX>::P : 16;      // one padding slot per PAD elements
+    static constexpr int TPL = XV == 0 ? xr_pq<LX>::Q : LX / 8;  // threads per line
+    static constexpr int LSP = LX + LX / PAD + 1;                // padded line length
 };
 
 template <typename T, int P, int Q, bool INV>
@@ -539,20 +555,77 @@ __device__ __forceinline__ void x_twolevel(cpx<T> *line, int t, bool act, const 
     __syncthreads();
 }
 
-template <typename T, int P, int Q>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
+// One Stockham pass of stride NS (radix R = min(8, L / NS)) and the passes after it. Butterfly j
+// reads elements j + r * L / R, twiddles them by w_L^(r k L / (NS R)) (k = j mod NS), and writes
+// the R-point DFT to (j - k) R + k + r NS. ZHALF: the input is zero beyond L / 2 (only the first
+// pass reads it: there element j + r L / R >= L / 2 exactly when r >= R / 2). The last inverse
+// pass stores only elements below nkeep.
+template <typename T, int L, int NS, bool INV, bool ZHALF>
+__device__ __forceinline__ void x_stockham(cpx<T> *line, int t, bool act, const cpx<T> *__restrict__ tw, int nkeep)
+{
+    constexpr int TPL = L / 8;
+    constexpr int R = (L / NS) >= 8 ? 8 : L / NS;
+    constexpr int LR = L / R, BPT = LR / TPL, TWS = L / (NS * R);
+    constexpr bool LAST = NS * R == L;
+    addrP<16> A;
+    cpx<T> v[BPT][R];
+    if (act) {
+#pragma unroll
+        for (int b = 0; b < BPT; b++)
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                if (ZHALF && 2 * r >= R) v[b][r] = mk<T>(0, 0);
+                else v[b][r] = line[A(t + b * TPL + r * LR)];
+            }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int b = 0; b < BPT; b++) {
+            const int j = t + b * TPL;
+            const int k = j & (NS - 1);
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    cpx<T> w = tw[r * k * TWS];
+                    if (INV) w.y = -w.y;
+                    v[b][r] = cmul(v[b][r], w);
+                }
+            }
+            dftR<T, R, INV>(v[b]);
+            const int d = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int e = d + r * NS;
+                if (!INV || !LAST || e < nkeep) line[A(e)] = v[b][r];
+            }
+        }
+    }
+    __syncthreads();
+    if constexpr (!LAST) x_stockham<T, L, NS * R, INV, false>(line, t, act, tw, nkeep);
+}
+
+template <typename T, int LX, int XV, bool INV>
+__device__ __forceinline__ void x_reg(cpx<T> *line, int t, bool act, const cpx<T> *__restrict__ tw, int nkeep)
+{
+    if constexpr (XV == 0) x_twolevel<T, xr_pq<LX>::P, xr_pq<LX>::Q, INV>(line, t, act, tw, nkeep);
+    else x_stockham<T, LX, 1, INV, !INV>(line, t, act, tw, nkeep);
+}
+
+template <typename T, int LX, int XV>
+__device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a)
 {
     if (stage_gated_out<T>(a.st, a.gate)) return;
     extern __shared__ unsigned char smraw[];
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
-    constexpr int LX = P * Q;
-    constexpr int LSP = LX + LX / P + 1;
-    addrP<P> A;
+    using C = xr_cfg<LX, XV>;
+    constexpr int TPL = C::TPL, LSP = C::LSP;
+    addrP<C::PAD> A;
     const int rpb = a.rpb;
     const int nrows = a.ny * a.nz;
     const int r0 = blockIdx.x * rpb;
     const int tid = threadIdx.x;
-    const int q = tid / Q, t = tid % Q;
+    const int q = tid / TPL, t = tid % TPL;
     const int qc = q / rpb, qr = q % rpb;
     const bool qact = (q < 3 * rpb) && (r0 + qr < nrows);
     cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
@@ -562,7 +635,7 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
     if (demag && qact) {
         const cpx<T> *src = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
 #pragma unroll 4
-        for (int m = t; m < LX; m += Q) cp_async_cpx<T>(&line[A(m)], &src[m], true);
+        for (int m = t; m < LX; m += TPL) cp_async_cpx<T>(&line[A(m)], &src[m], true);
     }
     cp_async_commit();
     // group 2: the per-cell input rows, arriving while the inverse transform runs
@@ -619,8 +692,8 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
     if (demag) {
         cp_async_wait_group<1>();
         __syncthreads();
-        xinv_pre_f<T>(line, LX, a.twx2, t, Q, qact, A);
-        x_twolevel<T, P, Q, true>(line, t, qact, a.twx, half);
+        xinv_pre_f<T>(line, LX, a.twx2, t, TPL, qact, A);
+        x_reg<T, LX, XV, true>(line, t, qact, a.twx, half);
     }
     cp_async_wait_group<0>();
     __syncthreads();
@@ -633,24 +706,36 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
             if (mm >= half) sm[qq * LSP + A(mm)] = mk<T>(0, 0);
         }
         __syncthreads();
-        x_twolevel<T, P, Q, false>(line, t, qact, a.twx, LX);
-        xfwd_post_f<T>(line, LX, a.twx2, t, Q, qact, A);
+        x_reg<T, LX, XV, false>(line, t, qact, a.twx, LX);
+        xfwd_post_f<T>(line, LX, a.twx2, t, TPL, qact, A);
         if (qact) {
             cpx<T> *dst = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
 #pragma unroll 4
-            for (int mm = t; mm < LX; mm += Q) dst[mm] = line[A(mm)];
+            for (int mm = t; mm < LX; mm += TPL) dst[mm] = line[A(mm)];
         }
     }
     stage_tail<T>(a, lmax, gridDim.x);
 }
 
-template <typename T, int P, int Q>
+template <typename T, int LX>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
+{
+    stage_reg_body<T, LX, 0>(a);
+}
+
+template <typename T, int LX>
+__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : 64) k_stage_rx(StageArgs<T> a)
+{
+    stage_reg_body<T, LX, 1>(a);
+}
+
+template <typename T, int LX, int XV>
 static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
 {
-    constexpr int LX = P * Q;
-    int nt = (3 * a.rpb * Q + 31) & ~31;   // whole warps: the error-norm reduction shuffles full warps
+    using C = xr_cfg<LX, XV>;
+    int nt = (3 * a.rpb * C::TPL + 31) & ~31;   // whole warps: the error-norm reduction shuffles full warps
     if (nt > bm_lb<T>::v) return 203;
-    size_t smem = (size_t)3 * a.rpb * (LX + LX / P + 1) * sizeof(cpx<T>);
+    size_t smem = (size_t)3 * a.rpb * C::LSP * sizeof(cpx<T>);
     if (smem > 200 * 1024) return 204;
     StageArgs<T> b = a;
     if (b.staged) {
@@ -660,41 +745,47 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
         if (lb + rb <= 200 * 1024) smem = lb + rb;
         else b.staged = 0;
     }
+    auto kern = XV == 0 ? k_stage_reg<T, LX> : k_stage_rx<T, LX>;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_stage_reg<T, P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     int nrows = a.ny * a.nz;
     dim3 grid((nrows + a.rpb - 1) / a.rpb);
-    k_stage_reg<T, P, Q><<<grid, nt, smem, s>>>(b);
+    kern<<<grid, nt, smem, s>>>(b);
     return (int)cudaGetLastError();
 }
 
 // x lengths with a register kernel and their threads per line
-int stage_reg_q(int LX)
+int stage_reg_q(int LX, int xv)
 {
     switch (LX) {
-    case 16: return 4;
-    case 32: return 8;
+    case 16: return xv ? 2 : 4;
+    case 32: return xv ? 4 : 8;
     case 64: return 8;
     case 128: return 16;
-    case 256: return 16;
-    case 512: return 32;
-    case 1024: return 32;
+    case 256: return xv ? 32 : 16;
+    case 512: return xv ? 64 : 32;
+    case 1024: return xv ? 128 : 32;
     default: return 0;
     }
+}
+
+template <typename T, int LX> static int launch_stage_xv(const StageArgs<T> &a, cudaStream_t s)
+{
+    return a.xv ? launch_stage_reg<T, LX, 1>(a, s) : launch_stage_reg<T, LX, 0>(a, s);
 }
 
 template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
 {
     switch (a.LX) {
-    case 16: return launch_stage_reg<T, 4, 4>(a, s);
-    case 32: return launch_stage_reg<T, 4, 8>(a, s);
-    case 64: return launch_stage_reg<T, 8, 8>(a, s);
-    case 128: return launch_stage_reg<T, 8, 16>(a, s);
-    case 256: return launch_stage_reg<T, 16, 16>(a, s);
-    case 512: return launch_stage_reg<T, 16, 32>(a, s);
-    case 1024: return launch_stage_reg<T, 32, 32>(a, s);
+    case 16: return launch_stage_xv<T, 16>(a, s);
+    case 32: return launch_stage_xv<T, 32>(a, s);
+    case 64: return launch_stage_xv<T, 64>(a, s);
+    case 128: return launch_stage_xv<T, 128>(a, s);
+    case 256: return launch_stage_xv<T, 256>(a, s);
+    case 512: return launch_stage_xv<T, 512>(a, s);
+    case 1024: return launch_stage_xv<T, 1024>(a, s);
     default: break;
     }
     int nt = (3 * a.rpb * a.px.tpl + 31) & ~31;   // whole warps

@@ -196,8 +196,9 @@ int bm_run_timed(bm_ctx *ctx, int steps, bm_stats *out, double *device_ms);
 int bm_time_kernels(bm_ctx *ctx, int mesh, int reps, double *ms4, double *bytes4);
 
 /* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width,
- * z-pass width, stage rows per block (negative when the stage kernel prefetches its
- * per-cell rows into shared memory)]. Valid after the first compute or run. */
+ * z-pass width, stage rows per block (plus 100 when the stage kernel uses the radix-8
+ * Stockham x transform; negative when it prefetches its per-cell rows into shared
+ * memory)]. Valid after the first compute or run. */
 int bm_tiles(bm_ctx *ctx, int mesh, int *tiles4);
 
 /* Test hooks (used by the test suite only). */

@@ -157,16 +157,19 @@ def test_norm_preserved_and_energy_decreases(bm):
     assert e1 < e0
 
 
+@pytest.mark.parametrize("xv", ["0", "1"])
 @pytest.mark.parametrize("staged", ["0", "1"])
 @pytest.mark.parametrize("rows", [1, 3])
-def test_stage_kernel_variants(bm, staged, rows, monkeypatch):
-    """Both stage-kernel variants (per-cell rows prefetched into shared memory or read from
-    global memory) and several rows per block, forced through BM_TILES / BM_STAGE_ROWS, give the
-    oracle's RKDP54 trajectory (exchange + iDMI + anisotropy + demag, 3D, LX = 128, 64 and 256).
-    The 256-wide mesh makes the staged launches of one graph need different shared-memory sizes
-    above 48 KB (the error-estimate launch stages the most rows)."""
+def test_stage_kernel_variants(bm, staged, rows, xv, monkeypatch):
+    """Every stage-kernel variant (per-cell rows prefetched into shared memory or read from global
+    memory; two-level or radix-8 Stockham x transform) and several rows per block, forced through
+    BM_TILES / BM_STAGE_ROWS / BM_STAGE_XV, give the oracle's RKDP54 trajectory (exchange + iDMI +
+    anisotropy + demag, 3D, LX = 128, 64 and 256). The 256-wide mesh makes the staged launches of
+    one graph need different shared-memory sizes above 48 KB (the error-estimate launch stages the
+    most rows)."""
     monkeypatch.setenv("BM_TILES", "1,4,8,%d" % rows)
     monkeypatch.setenv("BM_STAGE_ROWS", staged)
+    monkeypatch.setenv("BM_STAGE_XV", xv)
     for n in [(100, 10, 3), (64, 12, 2), (256, 6, 2)]:
         N = n[0] * n[1] * n[2]
         rng = np.random.default_rng(5)
@@ -184,5 +187,30 @@ def test_stage_kernel_variants(bm, staged, rows, monkeypatch):
         m = c.get_m() / Ms_map[:, None]
         c.close()
         assert abs(t["stage_rows"]) == rows and (t["stage_rows"] < 0) == (staged == "1")
+        assert t["stage_xv"] == int(xv)
         assert st["rejected"] == sr["rejected"]
         assert np.abs(m - mref).max() < 1e-8
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+@pytest.mark.parametrize("nx", [16, 32, 64, 128, 256, 512, 1024])
+def test_stage_xv_every_length(bm, nx, prec, tol, monkeypatch):
+    """The radix-8 Stockham x transform at every register length (radix tails 8x2, 8x4, 8x8,
+    8x8x2, 8x8x4, 8x8x8, 8x8x8x2; odd nx leaves a zero partner slot) against the oracle's RK4
+    trajectory with demag, exchange and Zeeman."""
+    monkeypatch.setenv("BM_TILES", "1,4,8,1")
+    monkeypatch.setenv("BM_STAGE_XV", "1")
+    for n in [(nx, 3, 2), (nx - 1, 2, 1)]:
+        N = n[0] * n[1] * n[2]
+        mesh = dict(n=n, h=(3e-9, 3e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(2e3, 1e3, 0))
+        M = sphere_random(N, seed=nx, Ms=8e5)
+        s = OracleSolver([mesh], evaluation=0, dt=2e-14)
+        s.set_m(M)
+        s.run(10)
+        c = _make(bm, prec, mesh, M, "RK4", 2e-14)
+        c.run(10)
+        t = c.tiles()
+        m = c.get_m()
+        c.close()
+        assert t["stage_xv"] == 1
+        assert np.abs(m - s.get_m()).max() / 8e5 < tol
