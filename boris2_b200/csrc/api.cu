@@ -777,6 +777,7 @@ StageArgs<T> stage_args(bm_ctx *c, Mesh &m)
     a.do_xfwd = (m.modules & BM_DEMAG) ? 1 : 0;
     a.staged = m.staged;
     a.xv = m.xv;
+    stage_derive(a);
     if (m.ml_role == 2) {
         // multilayer with mesh transfer: the demag field arrives in Hd, no x transforms here
         a.modules &= ~BM_DEMAG;

@@ -137,12 +137,9 @@ template <typename T>
 __global__ void __launch_bounds__(bm_lb<T>::v) k_ymid2d_batch(const YZArgs<T> *__restrict__ args, const int2 *__restrict__ work,
                                                                  int nwork)
 {
-    if (gated_out<T>(args[0].st, args[0].gate)) return;
-    for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
-        const int2 it = work[i];
-        ymid2d_body<T>(args[it.x], it.y);
-        __syncthreads();
-    }
+    if (gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    ymid2d_body<T>(args[it.x], it.y);
 }
 
 // ------------------------------------------------------------------------------ 3D y passes
@@ -192,15 +189,12 @@ template <typename T, bool INV>
 __global__ void __launch_bounds__(bm_lb<T>::v) k_ypass3d_batch(const YZArgs<T> *__restrict__ args, const int2 *__restrict__ work,
                                                                   int nwork)
 {
-    if (gated_out<T>(args[0].st, args[0].gate)) return;
-    for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
-        const int2 it = work[i];
-        const YZArgs<T> &a = args[it.x];
-        const int nbx = (a.LX + a.W - 1) / a.W;
-        const int bx = it.y % nbx, r = it.y / nbx;
-        ypass3d_body<T, INV>(a, bx, r % a.nz, r / a.nz);
-        __syncthreads();
-    }
+    if (gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    const YZArgs<T> &a = args[it.x];
+    const int nbx = (a.LX + a.W - 1) / a.W;
+    const int bx = it.y % nbx, r = it.y / nbx;
+    ypass3d_body<T, INV>(a, bx, r % a.nz, r / a.nz);
 }
 
 // ------------------------------------------------------------------------------ 3D z pass + product
@@ -321,14 +315,11 @@ template <typename T>
 __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_batch(const YZArgs<T> *__restrict__ args, const int2 *__restrict__ work,
                                                                int nwork)
 {
-    if (gated_out<T>(args[0].st, args[0].gate)) return;
-    for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
-        const int2 it = work[i];
-        const YZArgs<T> &a = args[it.x];
-        const int nbx = (a.LX + a.W - 1) / a.W;
-        zmid_body<T>(a, it.y % nbx, it.y / nbx);
-        __syncthreads();
-    }
+    if (gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    const YZArgs<T> &a = args[it.x];
+    const int nbx = (a.LX + a.W - 1) / a.W;
+    zmid_body<T>(a, it.y % nbx, it.y / nbx);
 }
 
 // ------------------------------------------------------------------------------ 3D z pass, register FFT
@@ -695,20 +686,16 @@ template int launch_zmid<float>(const YZArgs<float> &, cudaStream_t);
 template int launch_zmid<double>(const YZArgs<double> &, cudaStream_t);
 
 // ------------------------------------------------------------------------------ batched launchers
-// One launch over a work list of (mesh, tile) items; nt and smem are the maxima over the meshes,
-// the grid is one wave of resident blocks (each block loops over items).
+// One launch over a work list of (mesh, tile) items, one block per item; nt and smem are the
+// maxima over the meshes. (A grid-stride loop over the items around the FFT bodies made the
+// compiler fall back to 32 registers with kilobytes of per-thread stack, so each block takes one
+// item and the hardware block scheduler balances the uneven items.)
 template <typename KF>
 static int launch_batch_common(KF kern, int nwork, int nt, size_t smem, int *grid)
 {
     int rc = launch_common(kern, dim3(1), nt, smem, 0);
     if (rc) return rc;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    long long g = (long long)per_sm * nsm;
-    *grid = (int)(g < nwork ? g : nwork);
+    *grid = nwork;
     return 0;
 }
 

@@ -98,7 +98,32 @@ struct StageArgs {
     long long n;         // cells
     int staged;          // prefetch the per-cell input rows into shared memory (register kernel)
     int xv;              // register x transform: 0 two-level P x Q, 1 radix-8 Stockham at 64 (FP32) registers
+    // derived per-launch constants (products replace per-cell divisions)
+    T hh[3], ih[3], ih2[3];   // h, 1 / h, 1 / h^2
+    T iMs;                    // 1 / Ms (uniform Ms)
+    T rrD;                    // D / (2 A): iDMI boundary condition slope factor (0 when A = 0)
+    T exA, exD;               // 2 A / mu0, -2 D / mu0 (times 1 / Ms^2 per cell)
+    T two_mu0;                // 2 / mu0
+    T llg_pre;                // -gamma grel / (1 + alpha^2)
 };
+
+// fills the derived constants of a StageArgs from its material and cellsize fields
+template <typename T> inline void stage_derive(StageArgs<T> &a)
+{
+    const double h[3] = {a.hx, a.hy, a.hz};
+    for (int i = 0; i < 3; i++) {
+        a.hh[i] = (T)h[i];
+        a.ih[i] = (T)(1.0 / h[i]);
+        a.ih2[i] = (T)(1.0 / (h[i] * h[i]));
+    }
+    const double Ms = (double)a.Ms, A = (double)a.A, D = (double)a.D, al = (double)a.alpha;
+    a.iMs = (T)(Ms != 0.0 ? 1.0 / Ms : 0.0);
+    a.rrD = (T)(A != 0.0 ? D / (2.0 * A) : 0.0);
+    a.exA = (T)(2.0 * A / BM_MU0);
+    a.exD = (T)(-2.0 * D / BM_MU0);
+    a.two_mu0 = (T)(2.0 / BM_MU0);
+    a.llg_pre = (T)(-BM_GAMMA * (double)a.grel / (1.0 + al * al));
+}
 
 // Shared-memory row staging of the register stage kernel: per block row, kr rows of nx values:
 // 3*ns rows of M (slot 0 the row itself, 1/2 the y-1/y+1 rows, 3/4 the z-1/z+1 rows, each x,y,z),

@@ -128,21 +128,22 @@ __device__ __forceinline__ void ld3(const T *P, long long n, long long i, T v[3]
 }
 
 // one axis of the Neumann / non-homogeneous Neumann stencils for a full rectangular mesh
+// (ih = 1 / h, ih2 = 1 / h^2, products instead of divisions)
 template <typename T>
-__device__ __forceinline__ void axis_stencil(const T m[3], const T *mp, const T *mm, bool hp, bool hm, T h, const T bd[3],
-                                             T d2[3], T g[3])
+__device__ __forceinline__ void axis_stencil(const T m[3], const T *mp, const T *mm, bool hp, bool hm, T h, T ih, T ih2,
+                                             const T bd[3], T d2[3], T g[3])
 {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         if (hp && hm) {
-            d2[c] = (mp[c] + mm[c] - 2 * m[c]) / (h * h);
-            g[c] = (mp[c] - mm[c]) / (2 * h);
+            d2[c] = (mp[c] + mm[c] - 2 * m[c]) * ih2;
+            g[c] = (mp[c] - mm[c]) * ((T)0.5 * ih);
         } else if (hp) {
-            d2[c] = ((mp[c] - m[c]) - bd[c] * h) / (h * h);
-            g[c] = (T)0.5 * ((mp[c] - m[c]) / h + bd[c]);
+            d2[c] = ((mp[c] - m[c]) - bd[c] * h) * ih2;
+            g[c] = (T)0.5 * ((mp[c] - m[c]) * ih + bd[c]);
         } else if (hm) {
-            d2[c] = ((mm[c] - m[c]) + bd[c] * h) / (h * h);
-            g[c] = (T)0.5 * ((m[c] - mm[c]) / h + bd[c]);
+            d2[c] = ((mm[c] - m[c]) + bd[c] * h) * ih2;
+            g[c] = (T)0.5 * ((m[c] - mm[c]) * ih + bd[c]);
         } else {
             d2[c] = 0;
             g[c] = 0;
@@ -203,8 +204,8 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         Ha[0] = (T)a.Ha[3 * hi]; Ha[1] = (T)a.Ha[3 * hi + 1]; Ha[2] = (T)a.Ha[3 * hi + 2];
     }
     const bool exch = fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
-    const T Dv = (a.modules & BM_MOD_IDMI) ? a.D : (T)0;
-    const T hx = (T)a.hx, hy = (T)a.hy, hz = (T)a.hz;
+    const bool idmi = (a.modules & BM_MOD_IDMI) != 0;
+    const int nev = a.nev;
     T cev[6];
 #pragma unroll
     for (int i = 0; i < 6; i++) cev[i] = (T)(a.cev[i] * dT);
@@ -212,15 +213,21 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
     auto rp = [&](int q, int x) -> T * {
         return reinterpret_cast<T *>(&sm[q * LSP + addr(x >> 1)]) + (x & 1);
     };
-    for (int ci = tid; ci < rpb * nx; ci += nt) {
-        int r = ci / nx, x = ci - r * nx;
-        int row = r0 + r;
-        if (row >= nrows) continue;
-        long long cell = (long long)row * nx + x;
+    // (r, x) of cell index ci = r * nx + x, advanced by nt per iteration without divisions
+    const int dr = nt / nx, dx = nt - dr * nx;
+    int r = tid / nx, x = tid - r * nx;
+    int yrow = -1, y = 0, z = 0;
+    for (; r < rpb; x += dx, r += dr) {
+        if (x >= nx) { x -= nx; r++; if (r >= rpb) break; }
+        const int row = r0 + r;
+        if (row >= nrows) break;
+        if (row != yrow) { yrow = row; z = row / ny; y = row - z * ny; }
+        const long long cell = (long long)row * nx + x;
         T m[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) m[c] = acc.m(r, 0, c, x, cell);
-        T Ms = a.Ms_map ? acc.ms(r, x, cell) : a.Ms;
+        const T Ms = a.Ms_map ? acc.ms(r, x, cell) : a.Ms;
+        const T iMs = a.Ms_map ? (T)1 / Ms : a.iMs;
         T rhs[3] = {0, 0, 0};
         if (fields) {
             T H[3] = {Ha[0], Ha[1], Ha[2]};
@@ -233,9 +240,8 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 for (int c = 0; c < 3; c++) H[c] += a.Hd[c * n + cell];
             }
             if (exch) {
-                int y = row % ny, z = row / ny;
                 T mxp[3], mxm[3], myp[3], mym[3], mzp[3], mzm[3];
-                bool hxp = x + 1 < nx, hxm = x > 0, hyp = y + 1 < ny, hym = y > 0, hzp = z + 1 < nz, hzm = z > 0;
+                const bool hxp = x + 1 < nx, hxm = x > 0, hyp = y + 1 < ny, hym = y > 0, hzp = z + 1 < nz, hzm = z > 0;
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     mxp[c] = hxp ? acc.m(r, 0, c, x + 1, cell + 1) : (T)0;
@@ -245,24 +251,25 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                     mzm[c] = hzm ? acc.m(r, 3, c, x, cell) : (T)0;
                     mzp[c] = hzp ? acc.m(r, 4, c, x, cell) : (T)0;
                 }
-                T rr = (a.A != (T)0) ? Dv / (2 * a.A) : (T)0;
+                const T rr = idmi ? a.rrD : (T)0;
                 T bx[3] = {rr * m[2], 0, -rr * m[0]};
                 T by[3] = {0, rr * m[2], -rr * m[1]};
                 T bz[3] = {0, 0, 0};
-                T dx[3], dy[3], dz[3], gx[3], gy[3], gz[3];
-                axis_stencil<T>(m, mxp, mxm, hxp, hxm, hx, bx, dx, gx);
-                axis_stencil<T>(m, myp, mym, hyp, hym, hy, by, dy, gy);
-                axis_stencil<T>(m, mzp, mzm, hzp, hzm, hz, bz, dz, gz);
-                T Ac = 2 * a.A / ((T)BM_MU0 * Ms * Ms);
-                T Dc = -2 * Dv / ((T)BM_MU0 * Ms * Ms);
+                T dx2[3], dy2[3], dz2[3], gx[3], gy[3], gz[3];
+                axis_stencil<T>(m, mxp, mxm, hxp, hxm, a.hh[0], a.ih[0], a.ih2[0], bx, dx2, gx);
+                axis_stencil<T>(m, myp, mym, hyp, hym, a.hh[1], a.ih[1], a.ih2[1], by, dy2, gy);
+                axis_stencil<T>(m, mzp, mzm, hzp, hzm, a.hh[2], a.ih[2], a.ih2[2], bz, dz2, gz);
+                const T iMs2 = iMs * iMs;
+                const T Ac = a.exA * iMs2;
+                const T Dc = idmi ? a.exD * iMs2 : (T)0;
                 T hd[3] = {gx[2], gy[2], -gx[0] - gy[1]};
 #pragma unroll
-                for (int c = 0; c < 3; c++) H[c] += Ac * (dx[c] + dy[c] + dz[c]) + Dc * hd[c];
+                for (int c = 0; c < 3; c++) H[c] += Ac * (dx2[c] + dy2[c] + dz2[c]) + Dc * hd[c];
             }
             if (a.modules & BM_MOD_ANIUNI) {
                 T K1 = a.K1_map ? acc.k1(r, x, cell) : a.K1;
-                T dp = (m[0] * a.ea[0] + m[1] * a.ea[1] + m[2] * a.ea[2]) / Ms;
-                T s = (2 / ((T)BM_MU0 * Ms)) * dp * (K1 + 2 * a.K2 * (1 - dp * dp));
+                T dp = (m[0] * a.ea[0] + m[1] * a.ea[1] + m[2] * a.ea[2]) * iMs;
+                T s = (a.two_mu0 * iMs) * dp * (K1 + 2 * a.K2 * (1 - dp * dp));
 #pragma unroll
                 for (int c = 0; c < 3; c++) H[c] += s * a.ea[c];
             }
@@ -276,11 +283,10 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 for (int c = 0; c < 3; c++) a.Hsave[c * n + cell] = H[c];
             }
             T mxh[3] = {m[1] * H[2] - m[2] * H[1], m[2] * H[0] - m[0] * H[2], m[0] * H[1] - m[1] * H[0]};
-            T mu[3] = {m[0] / Ms, m[1] / Ms, m[2] / Ms};
+            T mu[3] = {m[0] * iMs, m[1] * iMs, m[2] * iMs};
             T mmxh[3] = {mu[1] * mxh[2] - mu[2] * mxh[1], mu[2] * mxh[0] - mu[0] * mxh[2], mu[0] * mxh[1] - mu[1] * mxh[0]};
-            T pre = -(T)BM_GAMMA * a.grel / (1 + a.alpha * a.alpha);
 #pragma unroll
-            for (int c = 0; c < 3; c++) rhs[c] = pre * (mxh[c] + a.alpha * mmxh[c]);
+            for (int c = 0; c < 3; c++) rhs[c] = a.llg_pre * (mxh[c] + a.alpha * mmxh[c]);
         }
         if (a.mode == BM_MODE_LTE) {
             // 4th-order prediction from the previous step's stages (FSAL), error in FP64
@@ -288,7 +294,9 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 double sum = 0.0;
-                for (int i = 0; i < a.nev; i++) sum += a.cev[i] * (double)acc.ev(i, r, c, x, cell);
+#pragma unroll
+                for (int i = 0; i < 6; i++)
+                    if (i < nev) sum += a.cev[i] * (double)acc.ev(i, r, c, x, cell);
                 double pred = (double)acc.mb(r, c, x, cell) + dT * (sum + a.crhs * (double)rhs[c]);
                 double d = (double)m[c] - pred;
                 d2 += d * d;
@@ -305,7 +313,9 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             T sum = crhs * rhs[c];
-            for (int i = 0; i < a.nev; i++) sum += cev[i] * acc.ev(i, r, c, x, cell);
+#pragma unroll
+            for (int i = 0; i < 6; i++)
+                if (i < nev) sum += cev[i] * acc.ev(i, r, c, x, cell);
             mn[c] = acc.mb(r, c, x, cell) + sum;
         }
         if (a.Ysave) {
@@ -478,12 +488,9 @@ template <typename T>
 __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_batch(const StageArgs<T> *__restrict__ args, const int2 *__restrict__ work,
                                                                 int nwork)
 {
-    if (stage_gated_out<T>(args[0].st, args[0].gate)) return;
-    for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
-        const int2 it = work[i];
-        stage_generic_body<T>(args[it.x], it.y, (unsigned int)nwork);
-        __syncthreads();
-    }
+    if (stage_gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    stage_generic_body<T>(args[it.x], it.y, (unsigned int)nwork);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -815,14 +822,7 @@ int launch_stage_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, 
         cudaError_t e = cudaFuncSetAttribute(k_stage_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_batch<T>, nt, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    long long g = (long long)per_sm * nsm;
-    int grid = (int)(g < nwork ? g : nwork);
-    k_stage_batch<T><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+    k_stage_batch<T><<<nwork, nt, smem, s>>>(dargs, dwork, nwork);
     return (int)cudaGetLastError();
 }
 
