@@ -326,8 +326,11 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_batch(const YZArgs<T> *__r
 // Compile-time Nz (<= 64): one thread owns one (component, pencil, column) line of Nz points in
 // registers. The upper half of the padded input is a compile-time zero and only the first
 // Nz/2 inverse outputs are stored, so the zero-padding work folds away. Shared memory only
-// carries the spectra across the 3x3 product; the kernel tile arrives by cp.async while the
-// forward transforms run. Thread (c, p, w): w fastest so global loads/stores coalesce.
+// carries the forward spectra to the 3x3 product: each thread reads the three components of its
+// own (pencil, column) and forms its own output component in registers, so one barrier separates
+// the transforms. The kernel tile arrives by cp.async while the forward transforms run (thread
+// row j < 6 copies kernel component j for every kz). Thread (c, p, w): w fastest so global loads
+// and stores coalesce.
 template <typename T, int NZ>
 __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
 {
@@ -346,25 +349,26 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
     const int np = single ? 1 : 2;
     const int tid = threadIdx.x, nt = blockDim.x;
     const long long nk = (long long)Kx1 * Ky1 * KZ1;
+    const long long kzs = (long long)Ky1 * Kx1;   // kz stride of a kernel component
+    const int w = tid & (W - 1);
+    const int j = tid >> lw;
+    const int kx = kx0 + w;
     // kernel tile (async)
-    for (int idx = tid; idx < 6 * KZ1 * W; idx += nt) {
-        int w = idx & (W - 1), r = idx >> lw;
-        int kz = r % KZ1, c = r / KZ1;
-        int kx = kx0 + w;
-        bool ok = kx < LX;
-        cp_async_real<T>(&Ks[(c * KZ1 + kz) * W + w], ok ? &a.K[c * nk + ((long long)kz * Ky1 + ky) * Kx1 + kx] : a.K, ok);
+    if (j < 6) {
+        const bool ok = kx < LX;
+        const T *src = a.K + j * nk + (long long)ky * Kx1 + (ok ? kx : 0);
+#pragma unroll
+        for (int kz = 0; kz < KZ1; kz++) cp_async_real<T>(&Ks[(j * KZ1 + kz) * W + w], src + kz * kzs, ok);
     }
     if (kx0 == 0) {
         for (int idx = tid; idx < 6 * KZ1; idx += nt) {
             int kz = idx % KZ1, c = idx / KZ1;
-            cp_async_real<T>(&Kn[c * KZ1 + kz], &a.K[c * nk + ((long long)kz * Ky1 + ky) * Kx1 + LX], true);
+            cp_async_real<T>(&Kn[c * KZ1 + kz], &a.K[c * nk + kz * kzs + (long long)ky * Kx1 + LX], true);
         }
     }
     // forward transforms in registers
-    const int w = tid & (W - 1);
-    const int p = (tid >> lw) & 1;
-    const int c = tid >> (lw + 1);
-    const int kx = kx0 + w;
+    const int p = j & 1;
+    const int c = j >> 1;
     const bool own = (c < 3) && (p < np) && (kx < LX);
     const int kyp = p ? kym : ky;
     const long long gbase = ((long long)c * nz * Ny + kyp) * LX + kx;   // + e * Ny * LX
@@ -378,68 +382,72 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
             if (e < nz) v[e] = a.S2[gbase + e * gstride];
     }
     RegFFT<T, NZ, false>::run(v, a.twz, 1);
-    auto S = [&](int cc, int pp, int e, int ww) -> cpx<T> & { return sm[((cc * 2 + pp) * NZ + e) * W + ww]; };
+    auto S = [&](int cc, int pp, int e) -> cpx<T> { return sm[((cc * 2 + pp) * NZ + e) * W + w]; };
     if (c < 3) {
 #pragma unroll
-        for (int e = 0; e < NZ; e++) S(c, p, e, w) = v[e];
+        for (int e = 0; e < NZ; e++) sm[((c * 2 + p) * NZ + e) * W + w] = v[e];
     }
     cp_async_wait_all();
     __syncthreads();
-    // 3x3 product with mirror signs (KernelMultiplication_3D_line, DemagKernel.cpp:85)
-    for (int idx = tid; idx < np * NZ * W; idx += nt) {
-        int ww = idx & (W - 1), r = idx >> lw;
-        int kz = r % NZ, pp = r / NZ;
-        if (kx0 + ww >= LX) continue;
-        int akz = kz <= NZ / 2 ? kz : NZ - kz;
-        T sz = kz <= NZ / 2 ? (T)1 : (T)-1;
-        if (kx0 + ww == 0) {
-            if (pp == 1) continue;
-            if (single && kz > NZ / 2) continue;
-            int pm = single ? 0 : 1;
-            int kzm = (NZ - kz) % NZ;
-            cpx<T> A[3], B[3], Ap[3], Bp[3];
+    if (!own) return;
+    // row c of the symmetric 3x3 kernel in (xx, yy, zz, xy, xz, yz) order, with the mirror signs
+    // of KernelMultiplication_3D_line (DemagKernel.cpp:85): xy odd in y, xz odd in z, yz odd in both
+    const int q0 = c == 0 ? 0 : c == 1 ? 3 : 4;
+    const int q1 = c == 0 ? 3 : c == 1 ? 1 : 5;
+    const int q2 = c == 0 ? 4 : c == 1 ? 5 : 2;
+    auto has_y = [](int q) { return q == 3 || q == 5; };
+    auto has_z = [](int q) { return q == 4 || q == 5; };
+    if (kx != 0) {
+        const T sy = p ? (T)-1 : (T)1;
+        const T y0 = has_y(q0) ? sy : (T)1, y1 = has_y(q1) ? sy : (T)1, y2 = has_y(q2) ? sy : (T)1;
+        const T z0 = has_z(q0) ? (T)-1 : (T)1, z1 = has_z(q1) ? (T)-1 : (T)1, z2 = has_z(q2) ? (T)-1 : (T)1;
+#pragma unroll
+        for (int kz = 0; kz < NZ; kz++) {
+            const int akz = kz <= NZ / 2 ? kz : NZ - kz;
+            const bool neg = kz > NZ / 2;
+            const T a0 = (neg ? y0 * z0 : y0) * Ks[(q0 * KZ1 + akz) * W + w];
+            const T a1 = (neg ? y1 * z1 : y1) * Ks[(q1 * KZ1 + akz) * W + w];
+            const T a2 = (neg ? y2 * z2 : y2) * Ks[(q2 * KZ1 + akz) * W + w];
+            const cpx<T> m0 = S(0, p, kz), m1 = S(1, p, kz), m2 = S(2, p, kz);
+            v[kz] = mk<T>(a0 * m0.x + a1 * m1.x + a2 * m2.x, a0 * m0.y + a1 * m1.y + a2 * m2.y);
+        }
+    } else {
+        // packed column: DC (kernel column 0) + i Nyquist (kernel column LX); the x-odd entries
+        // vanish there, and the z sign follows the line's primary kz (p = 0 pencil, kz <= Nz/2
+        // for a self-mirrored pencil) so that both mirror halves see the same kernel values. Only
+        // the column-0 threads take this path: a rolled loop through their own slots of O keeps it
+        // from adding registers to the unrolled path above.
+        cpx<T> *O = sm + 6 * NZ * W + ((6 * KZ1 * (W + 1) * sizeof(T) + sizeof(cpx<T>) - 1) / sizeof(cpx<T>)) + (c * 2 + p) * NZ;
+        const int pm = single ? 0 : 1 - p;
+        const T zq0 = has_z(q0) ? (T)-1 : (T)1, zq1 = has_z(q1) ? (T)-1 : (T)1, zq2 = has_z(q2) ? (T)-1 : (T)1;
+#pragma unroll 1
+        for (int kz = 0; kz < NZ; kz++) {
+            const int kzm = (NZ - kz) % NZ;
+            const int akz = kz <= NZ / 2 ? kz : NZ - kz;
+            const int kq = single ? (kz <= NZ / 2 ? kz : kzm) : (p == 0 ? kz : kzm);
+            const bool neg = kq > NZ / 2;
+            cpx<T> A[3], B[3];
 #pragma unroll
             for (int cc = 0; cc < 3; cc++) {
-                cpx<T> C = S(cc, 0, kz, ww), cj = conj(S(cc, pm, kzm, ww));
+                const cpx<T> C = S(cc, p, kz), cj = conj(S(cc, pm, kzm));
                 A[cc] = cscale(C + cj, (T)0.5);
                 B[cc] = cscale(mul_mi(C - cj), (T)0.5);
             }
-            T k0[6] = {Ks[(0 * KZ1 + akz) * W + ww], Ks[(1 * KZ1 + akz) * W + ww], Ks[(2 * KZ1 + akz) * W + ww],
-                       Ks[(3 * KZ1 + akz) * W + ww], sz * Ks[(4 * KZ1 + akz) * W + ww], sz * Ks[(5 * KZ1 + akz) * W + ww]};
-            T kn[6] = {Kn[0 * KZ1 + akz], Kn[1 * KZ1 + akz], Kn[2 * KZ1 + akz],
-                       Kn[3 * KZ1 + akz], sz * Kn[4 * KZ1 + akz], sz * Kn[5 * KZ1 + akz]};
-            kapply<T>(k0, A, Ap);
-            kapply<T>(kn, B, Bp);
-            bool self = single && (kzm == kz);
-#pragma unroll
-            for (int cc = 0; cc < 3; cc++) {
-                S(cc, 0, kz, ww) = Ap[cc] + mul_i(Bp[cc]);
-                if (!self) S(cc, pm, kzm, ww) = conj(Ap[cc]) + mul_i(conj(Bp[cc]));
-            }
-        } else {
-            T sy = (pp == 0) ? (T)1 : (T)-1;
-            T k[6] = {Ks[(0 * KZ1 + akz) * W + ww], Ks[(1 * KZ1 + akz) * W + ww], Ks[(2 * KZ1 + akz) * W + ww],
-                      sy * Ks[(3 * KZ1 + akz) * W + ww], sz * Ks[(4 * KZ1 + akz) * W + ww],
-                      sy * sz * Ks[(5 * KZ1 + akz) * W + ww]};
-            cpx<T> m[3], h[3];
-#pragma unroll
-            for (int cc = 0; cc < 3; cc++) m[cc] = S(cc, pp, kz, ww);
-            kapply<T>(k, m, h);
-#pragma unroll
-            for (int cc = 0; cc < 3; cc++) S(cc, pp, kz, ww) = h[cc];
+            const T s0 = neg ? zq0 : (T)1, s1 = neg ? zq1 : (T)1, s2 = neg ? zq2 : (T)1;
+            const T a0 = s0 * Ks[(q0 * KZ1 + akz) * W + w], a1 = s1 * Ks[(q1 * KZ1 + akz) * W + w],
+                    a2 = s2 * Ks[(q2 * KZ1 + akz) * W + w];
+            const T b0 = s0 * Kn[q0 * KZ1 + akz], b1 = s1 * Kn[q1 * KZ1 + akz], b2 = s2 * Kn[q2 * KZ1 + akz];
+            const cpx<T> Ap = mk<T>(a0 * A[0].x + a1 * A[1].x + a2 * A[2].x, a0 * A[0].y + a1 * A[1].y + a2 * A[2].y);
+            const cpx<T> Bp = mk<T>(b0 * B[0].x + b1 * B[1].x + b2 * B[2].x, b0 * B[0].y + b1 * B[1].y + b2 * B[2].y);
+            O[kz] = Ap + mul_i(Bp);
         }
-    }
-    __syncthreads();
-    if (c < 3) {
 #pragma unroll
-        for (int e = 0; e < NZ; e++) v[e] = S(c, p, e, w);
+        for (int kz = 0; kz < NZ; kz++) v[kz] = O[kz];
     }
     RegFFT<T, NZ, true>::run(v, a.twz, 1);
-    if (own) {
 #pragma unroll
-        for (int e = 0; e < NZ / 2; e++)
-            if (e < nz) a.S2[gbase + e * gstride] = v[e];
-    }
+    for (int e = 0; e < NZ / 2; e++)
+        if (e < nz) a.S2[gbase + e * gstride] = v[e];
 }
 
 template <typename T, int NZ>

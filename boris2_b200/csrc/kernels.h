@@ -47,7 +47,10 @@ template <typename T> size_t zmid_smem(int Nz, int W)
 }
 template <typename T> size_t zmid_reg_smem(int Nz, int W)
 {
-    return (size_t)6 * Nz * W * sizeof(cpx<T>) + (size_t)6 * (Nz / 2 + 1) * (W + 1) * sizeof(T);
+    // spectra [3][2][Nz][W], kernel tile + Nyquist column, column-0 outputs [3][2][Nz]
+    size_t kb = (size_t)6 * (Nz / 2 + 1) * (W + 1) * sizeof(T);
+    kb = (kb + sizeof(cpx<T>) - 1) / sizeof(cpx<T>) * sizeof(cpx<T>);
+    return (size_t)6 * Nz * W * sizeof(cpx<T>) + kb + (size_t)6 * Nz * sizeof(cpx<T>);
 }
 bool zmid_has_reg(int Nz);
 bool ypass_has_reg(int Ny);
