@@ -96,7 +96,6 @@ _SIGS = {
     "bm_ml_tile": (_I, [_P, _IP]),
     "bm_set_batched": (_I, [_P, _I]),
     "bm_adjoint_rk4": (_I, [_P, _I, _I, _DP, _I, _DP, _DP, _DP, _DP, _DP]),
-    "bm_debug_time_stage": (_I, [_P, _I, _I, _I, _I, _DP]),
 }
 
 
@@ -311,13 +310,14 @@ class Context:
         return ms, by
 
     def tiles(self, mesh=0):
-        """Autotuned tile shapes: 2D y width, 3D y width, z width, stage rows per block (negative
-        when the per-cell rows are prefetched), stage x-transform variant (1: radix-8 Stockham)."""
+        """Autotuned tile shapes: 2D y width, 3D y width and variant (1: radix-16 Stockham), z width,
+        stage rows per block (negative when the per-cell rows are prefetched), stage x-transform
+        variant (1: radix-8 Stockham)."""
         t = (ctypes.c_int * 4)()
         _check(lib().bm_tiles(self._h, mesh, t))
         sgn = -1 if t[3] < 0 else 1
-        return {"ymid2d_W": t[0], "ypass_W": t[1], "zmid_W": t[2], "stage_rows": sgn * (abs(t[3]) % 100),
-                "stage_xv": abs(t[3]) // 100}
+        return {"ymid2d_W": t[0], "ypass_W": t[1] % 100, "ypass_yv": t[1] // 100, "zmid_W": t[2],
+                "stage_rows": sgn * (abs(t[3]) % 100), "stage_xv": abs(t[3]) // 100}
 
     def stats(self):
         st = Stats()

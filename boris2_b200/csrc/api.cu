@@ -69,7 +69,7 @@ struct Mesh {
     long long n = 0;
     int Nx = 1, Ny = 1, Nz = 1, LX = 1;
     FFTPlan px, py, pz;
-    int W2 = 1, Wy = 1, Wz = 1, rpb = 1, staged = 0, xv = 0;
+    int W2 = 1, Wy = 1, Wz = 1, rpb = 1, staged = 0, xv = 0, yv = 0;
     // device (element type depends on the context precision)
     void *buf[4] = {nullptr, nullptr, nullptr, nullptr};   // A (M), P (sM1), B, C
     void *ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -456,16 +456,26 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
             }
             m.W2 = bw;
         } else {
-            float best = 1e30f; int bw = m.Wy;
-            for (int W = 1; W <= 32 && W <= m.LX; W *= 2) {
-                if ((size_t)m.Ny * W * cs > 200 * 1024) continue;
-                if (ypass_has_reg(m.Ny) ? ypass_reg_threads(m.Ny, W) > lim : W * m.py.tpl > lim) continue;
-                a.W = W;
-                float t = time_launches(s, [&]() { return launch_yfwd<T>(a, s); }, reps) +
-                          time_launches(s, [&]() { return launch_yinv<T>(a, s); }, reps);
-                if (t < best) { best = t; bw = W; }
-            }
+            float best = 1e30f; int bw = m.Wy, byv = 0;
+            // y transform variant (two-level register / radix-16 Stockham) x column tile width
+            for (int yv = 0; yv <= (ypass_has_st(m.Ny) ? 1 : 0); yv++)
+                for (int W = 1; W <= 32 && W <= m.LX; W *= 2) {
+                    if ((size_t)m.Ny * W * cs > 200 * 1024) continue;
+                    if (yv) {
+                        const int nt = ypass_st_threads(m.Ny, W);
+                        if (nt > lim || nt % 32) continue;
+                    } else if (ypass_has_reg(m.Ny) ? ypass_reg_threads(m.Ny, W) > lim : W * m.py.tpl > lim) {
+                        continue;
+                    }
+                    a.W = W;
+                    a.yv = yv;
+                    float t = time_launches(s, [&]() { return launch_yfwd<T>(a, s); }, reps) +
+                              time_launches(s, [&]() { return launch_yinv<T>(a, s); }, reps);
+                    if (t < best) { best = t; bw = W; byv = yv; }
+                }
             m.Wy = bw;
+            m.yv = byv;
+            a.yv = byv;
             best = 1e30f; bw = m.Wz;
             for (int W = 4; W <= 128 && W <= m.LX; W *= 2) {
                 if (zmid_has_reg(m.Nz) ? (zmid_reg_smem<T>(m.Nz, W) > 200 * 1024 || 6 * W > lim)
@@ -701,6 +711,8 @@ int prepare_T(bm_ctx *c)
             m.staged = (sr && sr[0] == '1') ? 1 : 0;
             const char *sx = getenv("BM_STAGE_XV");
             m.xv = (sx && sx[0] == '1' && stage_reg_q(m.LX)) ? 1 : 0;
+            const char *sy = getenv("BM_Y_XV");
+            m.yv = (sy && sy[0] == '1' && ypass_has_st(m.Ny) && m.nz > 1 && ypass_st_threads(m.Ny, m.Wy) % 32 == 0) ? 1 : 0;
         } else if (c->autotune && !c->batched) autotune_mesh<T>(c, m);
     }
     if (int rc = prepare_ml<T>(c)) { for (auto &mm : c->meshes) free_mesh(mm); free_ml(c); return rc; }
@@ -731,6 +743,7 @@ YZArgs<T> yz_args(bm_ctx *c, Mesh &m, int gate)
     a.nx = m.nx; a.ny = m.ny; a.nz = m.nz; a.LX = m.LX; a.Ny = m.Ny; a.Nz = m.Nz;
     a.W = m.nz > 1 ? m.Wy : m.W2;
     a.st = c->st; a.gate = gate;
+    a.yv = m.yv;
     return a;
 }
 
@@ -2076,54 +2089,12 @@ int bm_time_kernels(bm_ctx *c, int mesh, int reps, double *ms4, double *bytes4)
                                      : time_kernels_T<float>(c, m, reps, ms4, bytes4);
 }
 
-// device time (ms per launch) of the stage kernel in one mode on the mesh's own buffers
-// (diagnostics): mode 0 stage update with nev earlier evaluations, 1 x forward only (UPDATE,
-// nev = 0), 2 fields only (HEFF: x inverse + field terms)
-int bm_debug_time_stage(bm_ctx *c, int mesh, int mode, int nev, int reps, double *ms)
-{
-    if (int rc = check_mesh(c, mesh)) return rc;
-    if (!ms || reps < 1 || nev < 0 || nev > 5) return fail(BM_EINVAL, "args");
-    if (int rc = prepare(c)) return rc;
-    cudaSetDevice(c->device);
-    Mesh &m = c->meshes[mesh];
-    auto run = [&](auto tag) -> int {
-        using T = decltype(tag);
-        T *tmp = nullptr;
-        if (cudaMalloc(&tmp, sizeof(T) * 9 * m.n) != cudaSuccess) return fail(BM_ENOMEM, "tmp");
-        StageArgs<T> a = stage_args<T>(c, m);
-        a.st = nullptr;
-        a.Min = (const T *)m.buf[0];
-        a.Mbase = (const T *)m.buf[0];
-        if (mode == 0) {
-            a.mode = BM_MODE_STAGE;
-            a.nev = nev;
-            for (int i = 0; i < nev; i++) a.ev[i] = (const T *)m.buf[0];
-            a.ev_out = tmp;
-            a.Mout = tmp + 3 * m.n;
-        } else if (mode == 1) {
-            a.mode = BM_MODE_UPDATE;
-            a.nev = 0;
-        } else {
-            a.mode = BM_MODE_HEFF;
-            a.do_xfwd = 0;
-            a.Hout = tmp + 6 * m.n;
-        }
-        float t = time_launches(c->stream, [&]() { return launch_stage<T>(a, c->stream); }, reps);
-        cudaStreamSynchronize(c->stream);
-        cudaFree(tmp);
-        c->s1_dirty = true;
-        *ms = t;
-        return t > 1e29f ? fail(BM_ECUDA, "launch failed") : 0;
-    };
-    return (c->precision == BM_FP64) ? run(double()) : run(float());
-}
-
 int bm_tiles(bm_ctx *c, int mesh, int *tiles4)
 {
     if (int rc = check_mesh(c, mesh)) return rc;
     if (!tiles4) return fail(BM_EINVAL, "null out");
     Mesh &m = c->meshes[mesh];
-    tiles4[0] = m.W2; tiles4[1] = m.Wy; tiles4[2] = m.Wz; tiles4[3] = (m.staged ? -1 : 1) * (m.rpb + 100 * m.xv);
+    tiles4[0] = m.W2; tiles4[1] = m.Wy + 100 * m.yv; tiles4[2] = m.Wz; tiles4[3] = (m.staged ? -1 : 1) * (m.rpb + 100 * m.xv);
     return 0;
 }
 

@@ -597,6 +597,126 @@ static int launch_ypass_dispatch(const YZArgs<T> &a, cudaStream_t s)
     }
 }
 
+// ------------------------------------------------------------------------------ 3D y passes, radix-16 Stockham
+// Ny = 256 .. 2048. Block: W columns x Ny / 16 threads per column (w fastest), 16 values per
+// thread in every pass. The first pass reads its butterfly inputs straight from global memory
+// (forward: rows >= ny are zeros, and those >= Ny / 2 fold away at compile time) and the last
+// pass writes straight to global memory (inverse: rows < ny only); the passes in between go
+// through a shared tile [Ny][W] skewed by 8 elements per 16 rows, so that the stride-16 stores
+// of the first pass and the unit-stride accesses of the others are both conflict-free.
+__device__ __forceinline__ int ysk(int e, int w, int W) { return e * W + w + ((e >> 4) << 3); }
+
+template <typename T, int L, int NS, bool INV>
+__device__ __forceinline__ void ypass_st_pass(cpx<T> *tile, const cpx<T> *src, cpx<T> *dst, int ld, int ny, int t, int w,
+                                              int W, bool colok, const cpx<T> *__restrict__ tw)
+{
+    constexpr int TPL = L / 16;
+    constexpr int R = (L / NS) >= 16 ? 16 : L / NS;
+    constexpr int LR = L / R, BPT = LR / TPL, TWS = L / (NS * R);
+    constexpr bool FIRST = NS == 1, LAST = NS * R == L;
+    cpx<T> v[BPT][R];
+#pragma unroll
+    for (int b = 0; b < BPT; b++)
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int e = t + b * TPL + r * LR;
+            if (FIRST) {
+                if (!INV) v[b][r] = (2 * r < R && colok && e < ny) ? src[(long long)e * ld] : mk<T>(0, 0);
+                else v[b][r] = colok ? src[(long long)e * ld] : mk<T>(0, 0);
+            } else {
+                v[b][r] = tile[ysk(e, w, W)];
+            }
+        }
+    if (!FIRST && !LAST) __syncthreads();   // every load of this pass before any store into the tile
+#pragma unroll
+    for (int b = 0; b < BPT; b++) {
+        const int j = t + b * TPL;
+        const int k = j & (NS - 1);
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                cpx<T> wv = tw[r * k * TWS];
+                if (INV) wv.y = -wv.y;
+                v[b][r] = cmul(v[b][r], wv);
+            }
+        }
+        dftR<T, R, INV>(v[b]);
+        const int d = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int e = d + r * NS;
+            if (LAST) {
+                if (colok && (!INV || e < ny)) dst[(long long)e * ld] = v[b][r];
+            } else {
+                tile[ysk(e, w, W)] = v[b][r];
+            }
+        }
+    }
+    if constexpr (!LAST) {
+        __syncthreads();
+        ypass_st_pass<T, L, NS * R, INV>(tile, src, dst, ld, ny, t, w, W, colok, tw);
+    }
+}
+
+template <typename T, int L, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v, sizeof(T) == 4 ? 2 : 1) k_ypass_st(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    extern __shared__ unsigned char smraw[];
+    cpx<T> *tile = reinterpret_cast<cpx<T> *>(smraw);
+    const int W = a.W, ny = a.ny, LX = a.LX, nz = a.nz;
+    const int lw = __ffs(W) - 1;
+    const int kx0 = blockIdx.x * W, z = blockIdx.y, c = blockIdx.z;
+    const int tid = threadIdx.x;
+    const int w = tid & (W - 1), t = tid >> lw;
+    const int kx = kx0 + w;
+    const bool colok = kx < LX;
+    const cpx<T> *src;
+    cpx<T> *dst;
+    if (!INV) {
+        src = a.S1 + ((long long)c * nz + z) * ny * LX + (colok ? kx : 0);
+        dst = a.S2 + ((long long)c * nz + z) * L * LX + kx;
+    } else {
+        src = a.S2 + ((long long)c * nz + z) * L * LX + (colok ? kx : 0);
+        dst = a.S1 + ((long long)c * nz + z) * ny * LX + kx;
+    }
+    ypass_st_pass<T, L, 1, INV>(tile, src, dst, LX, ny, t, w, W, colok, a.twy);
+}
+
+bool ypass_has_st(int Ny) { return Ny == 256 || Ny == 512 || Ny == 1024 || Ny == 2048; }
+int ypass_st_threads(int Ny, int W) { return W * (Ny / 16); }
+template <typename T> size_t ypass_st_smem(int Ny, int W) { return ((size_t)Ny * W + (size_t)(Ny / 16) * 8) * sizeof(cpx<T>); }
+
+template <typename T, int L, bool INV>
+static int launch_ypass_st(const YZArgs<T> &a, cudaStream_t s)
+{
+    int nt = a.W * (L / 16);
+    if (nt > bm_lb<T>::v) return 108;
+    if (nt % 32) return 108;
+    size_t smem = ypass_st_smem<T>(L, a.W);
+    if (smem > 200 * 1024) return 109;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_ypass_st<T, L, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        if (e != cudaSuccess) return (int)e;
+    }
+    dim3 grid((a.LX + a.W - 1) / a.W, a.nz, 3);
+    k_ypass_st<T, L, INV><<<grid, nt, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, bool INV>
+static int launch_ypass_st_dispatch(const YZArgs<T> &a, cudaStream_t s)
+{
+    if ((a.W & (a.W - 1)) != 0) return -1;
+    switch (a.Ny) {
+    case 256: return launch_ypass_st<T, 256, INV>(a, s);
+    case 512: return launch_ypass_st<T, 512, INV>(a, s);
+    case 1024: return launch_ypass_st<T, 1024, INV>(a, s);
+    case 2048: return launch_ypass_st<T, 2048, INV>(a, s);
+    default: return -1;
+    }
+}
+
 // ------------------------------------------------------------------------------ launchers
 template <typename KF>
 static int launch_common(KF kern, dim3 grid, int nt, size_t smem, cudaStream_t s)
@@ -625,6 +745,10 @@ template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s)
 
 template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s)
 {
+    if (a.yv) {
+        int rc = launch_ypass_st_dispatch<T, false>(a, s);
+        if (rc >= 0) return rc;
+    }
     {
         int rc = launch_ypass_dispatch<T, false>(a, s);
         if (rc >= 0) return rc;
@@ -642,6 +766,10 @@ template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s)
 
 template <typename T> int launch_yinv(const YZArgs<T> &a, cudaStream_t s)
 {
+    if (a.yv) {
+        int rc = launch_ypass_st_dispatch<T, true>(a, s);
+        if (rc >= 0) return rc;
+    }
     {
         int rc = launch_ypass_dispatch<T, true>(a, s);
         if (rc >= 0) return rc;

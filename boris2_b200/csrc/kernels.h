@@ -35,6 +35,7 @@ struct YZArgs {
     int W;               // column tile width
     StepState *st;
     int gate;
+    int yv;              // 3D y transform: 0 two-level register kernel, 1 radix-16 Stockham (Ny >= 256)
 };
 
 template <typename T> size_t ymid2d_smem(int Ny, int W)
@@ -54,6 +55,8 @@ template <typename T> size_t zmid_reg_smem(int Nz, int W)
 }
 bool zmid_has_reg(int Nz);
 bool ypass_has_reg(int Ny);
+bool ypass_has_st(int Ny);            // lengths with the radix-16 Stockham y transform
+int ypass_st_threads(int Ny, int W);
 int ypass_reg_threads(int Ny, int W);
 template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s);

@@ -157,18 +157,21 @@ __device__ __forceinline__ void axis_stencil(const T m[3], const T *mp, const T 
 // Per-cell input accessors. AccGlobal reads the device arrays; AccStaged reads the rows the
 // register kernel prefetched into shared memory (layout: stage_layout in kernels.h).
 template <typename T> struct AccGlobal {
-    const StageArgs<T> *a;
+    // pointers copied out of the argument block so each access is (per-cell base)[uniform offset]
+    const T *Mn, *Mb, *E[6], *Msm, *K1m;
     long long n, off[5];
-    __device__ AccGlobal(const StageArgs<T> &aa) : a(&aa), n(aa.n)
+    __device__ AccGlobal(const StageArgs<T> &aa) : Mn(aa.Min), Mb(aa.Mbase), Msm(aa.Ms_map), K1m(aa.K1_map), n(aa.n)
     {
+#pragma unroll
+        for (int i = 0; i < 6; i++) E[i] = aa.ev[i];
         long long nxy = (long long)aa.nx * aa.ny;
         off[0] = 0; off[1] = -aa.nx; off[2] = aa.nx; off[3] = -nxy; off[4] = nxy;
     }
-    __device__ __forceinline__ T m(int, int slot, int c, int, long long cell) const { return a->Min[c * n + cell + off[slot]]; }
-    __device__ __forceinline__ T mb(int, int c, int, long long cell) const { return a->Mbase[c * n + cell]; }
-    __device__ __forceinline__ T ev(int i, int, int c, int, long long cell) const { return a->ev[i][c * n + cell]; }
-    __device__ __forceinline__ T ms(int, int, long long cell) const { return a->Ms_map[cell]; }
-    __device__ __forceinline__ T k1(int, int, long long cell) const { return a->K1_map[cell]; }
+    __device__ __forceinline__ T m(int, int slot, int c, int, long long cell) const { return (Mn + cell)[c * n + off[slot]]; }
+    __device__ __forceinline__ T mb(int, int c, int, long long cell) const { return (Mb + cell)[c * n]; }
+    __device__ __forceinline__ T ev(int i, int, int c, int, long long cell) const { return (E[i] + cell)[c * n]; }
+    __device__ __forceinline__ T ms(int, int, long long cell) const { return Msm[cell]; }
+    __device__ __forceinline__ T k1(int, int, long long cell) const { return K1m[cell]; }
 };
 
 template <typename T> struct AccStaged {
@@ -181,6 +184,26 @@ template <typename T> struct AccStaged {
     __device__ __forceinline__ T ms(int r, int x, long long) const { return row(r, mso)[x]; }
     __device__ __forceinline__ T k1(int r, int x, long long) const { return row(r, k1o)[x]; }
 };
+
+// sum[c] += sum_{i < NEV} cev[i] * ev_i[c] (component by component, i ascending)
+template <int NEV, typename T, typename Acc>
+__device__ __forceinline__ void ev_acc(const Acc &acc, const T *cev, int r, int x, long long cell, T sum[3])
+{
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int i = 0; i < NEV; i++) sum[c] += cev[i] * acc.ev(i, r, c, x, cell);
+}
+
+// sum_{i < NEV} cev[i] * ev_i[c] in FP64 (error estimate)
+template <int NEV, typename Acc>
+__device__ __forceinline__ double ev_sum_d(const Acc &acc, const double *cev, int r, int c, int x, long long cell)
+{
+    double sum = 0.0;
+#pragma unroll
+    for (int i = 0; i < NEV; i++) sum += cev[i] * (double)acc.ev(i, r, c, x, cell);
+    return sum;
+}
 
 template <typename T, typename AddrF, typename Acc>
 __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, int LSP, AddrF addr, int r0, double &lmax,
@@ -205,14 +228,13 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
     }
     const bool exch = fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
     const bool idmi = (a.modules & BM_MOD_IDMI) != 0;
+    const bool zflat = (nz == 1);
     const int nev = a.nev;
     T cev[6];
 #pragma unroll
     for (int i = 0; i < 6; i++) cev[i] = (T)(a.cev[i] * dT);
     const T crhs = (T)(a.crhs * dT);
-    auto rp = [&](int q, int x) -> T * {
-        return reinterpret_cast<T *>(&sm[q * LSP + addr(x >> 1)]) + (x & 1);
-    };
+    const int cstride = 2 * rpb * LSP;   // T elements between the component lines of one row
     // (r, x) of cell index ci = r * nx + x, advanced by nt per iteration without divisions
     const int dr = nt / nx, dx = nt - dr * nx;
     int r = tid / nx, x = tid - r * nx;
@@ -223,6 +245,7 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         if (row >= nrows) break;
         if (row != yrow) { yrow = row; z = row / ny; y = row - z * ny; }
         const long long cell = (long long)row * nx + x;
+        T *sp = reinterpret_cast<T *>(&sm[r * LSP + addr(x >> 1)]) + (x & 1);   // packed line slot of x
         T m[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) m[c] = acc.m(r, 0, c, x, cell);
@@ -233,15 +256,45 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             T H[3] = {Ha[0], Ha[1], Ha[2]};
             if (demag) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) H[c] += a.scale * *rp(c * rpb + r, x);
+                for (int c = 0; c < 3; c++) H[c] += a.scale * sp[c * cstride];
             }
             if (a.Hd) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) H[c] += a.Hd[c * n + cell];
+                for (int c = 0; c < 3; c++) H[c] += (a.Hd + cell)[c * n];
             }
-            if (exch) {
+            const bool hxp = x + 1 < nx, hxm = x > 0, hyp = y + 1 < ny, hym = y > 0, hzp = z + 1 < nz, hzm = z > 0;
+            if (exch && hxp && hxm && hyp && hym && (zflat || (hzp && hzm))) {
+                // interior cell: both neighbours on every axis (the first branch of axis_stencil;
+                // a one-cell-thick mesh has no z terms)
+                const T iMs2 = iMs * iMs;
+                const T Ac = a.exA * iMs2;
+                T lap[3], gxv[3], gyv[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const T mxp = acc.m(r, 0, c, x + 1, cell + 1), mxm = acc.m(r, 0, c, x - 1, cell - 1);
+                    const T mym = acc.m(r, 1, c, x, cell), myp = acc.m(r, 2, c, x, cell);
+                    const T dx2 = (mxp + mxm - 2 * m[c]) * a.ih2[0];
+                    const T dy2 = (myp + mym - 2 * m[c]) * a.ih2[1];
+                    T dz2 = 0;
+                    if (!zflat) {
+                        const T mzm = acc.m(r, 3, c, x, cell), mzp = acc.m(r, 4, c, x, cell);
+                        dz2 = (mzp + mzm - 2 * m[c]) * a.ih2[2];
+                    }
+                    lap[c] = dx2 + dy2 + dz2;
+                    gxv[c] = (mxp - mxm) * ((T)0.5 * a.ih[0]);
+                    gyv[c] = (myp - mym) * ((T)0.5 * a.ih[1]);
+                }
+                if (idmi) {
+                    const T Dc = a.exD * iMs2;
+                    const T hd[3] = {gxv[2], gyv[2], -gxv[0] - gyv[1]};
+#pragma unroll
+                    for (int c = 0; c < 3; c++) H[c] += Ac * lap[c] + Dc * hd[c];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) H[c] += Ac * lap[c];
+                }
+            } else if (exch) {
                 T mxp[3], mxm[3], myp[3], mym[3], mzp[3], mzm[3];
-                const bool hxp = x + 1 < nx, hxm = x > 0, hyp = y + 1 < ny, hym = y > 0, hzp = z + 1 < nz, hzm = z > 0;
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     mxp[c] = hxp ? acc.m(r, 0, c, x + 1, cell + 1) : (T)0;
@@ -275,12 +328,12 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             }
             if (a.mode == BM_MODE_HEFF) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) a.Hout[c * n + cell] = H[c];
+                for (int c = 0; c < 3; c++) (a.Hout + cell)[c * n] = H[c];
                 continue;
             }
             if (a.Hsave) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) a.Hsave[c * n + cell] = H[c];
+                for (int c = 0; c < 3; c++) (a.Hsave + cell)[c * n] = H[c];
             }
             T mxh[3] = {m[1] * H[2] - m[2] * H[1], m[2] * H[0] - m[0] * H[2], m[0] * H[1] - m[1] * H[0]};
             T mu[3] = {m[0] * iMs, m[1] * iMs, m[2] * iMs};
@@ -294,9 +347,15 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 double sum = 0.0;
-#pragma unroll
-                for (int i = 0; i < 6; i++)
-                    if (i < nev) sum += a.cev[i] * (double)acc.ev(i, r, c, x, cell);
+                switch (nev) {   // block-uniform: unrolled sums without predicated loads
+                case 6: sum = ev_sum_d<6>(acc, a.cev, r, c, x, cell); break;
+                case 5: sum = ev_sum_d<5>(acc, a.cev, r, c, x, cell); break;
+                case 4: sum = ev_sum_d<4>(acc, a.cev, r, c, x, cell); break;
+                case 3: sum = ev_sum_d<3>(acc, a.cev, r, c, x, cell); break;
+                case 2: sum = ev_sum_d<2>(acc, a.cev, r, c, x, cell); break;
+                case 1: sum = ev_sum_d<1>(acc, a.cev, r, c, x, cell); break;
+                default: break;
+                }
                 double pred = (double)acc.mb(r, c, x, cell) + dT * (sum + a.crhs * (double)rhs[c]);
                 double d = (double)m[c] - pred;
                 d2 += d * d;
@@ -306,21 +365,27 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             if (l != l) l = 1e300;   // NaN counts as a huge error so the step is rejected
             if (l > lmax) lmax = l;
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.ev_out[c * n + cell] = rhs[c];
+            for (int c = 0; c < 3; c++) (a.ev_out + cell)[c * n] = rhs[c];
             continue;
         }
         T mn[3];
+        {
+            T sum[3] = {crhs * rhs[0], crhs * rhs[1], crhs * rhs[2]};
+            switch (nev) {   // block-uniform: unrolled sums without predicated loads
+            case 6: ev_acc<6>(acc, cev, r, x, cell, sum); break;
+            case 5: ev_acc<5>(acc, cev, r, x, cell, sum); break;
+            case 4: ev_acc<4>(acc, cev, r, x, cell, sum); break;
+            case 3: ev_acc<3>(acc, cev, r, x, cell, sum); break;
+            case 2: ev_acc<2>(acc, cev, r, x, cell, sum); break;
+            case 1: ev_acc<1>(acc, cev, r, x, cell, sum); break;
+            default: break;
+            }
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            T sum = crhs * rhs[c];
-#pragma unroll
-            for (int i = 0; i < 6; i++)
-                if (i < nev) sum += cev[i] * acc.ev(i, r, c, x, cell);
-            mn[c] = acc.mb(r, c, x, cell) + sum;
+            for (int c = 0; c < 3; c++) mn[c] = acc.mb(r, c, x, cell) + sum[c];
         }
         if (a.Ysave) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.Ysave[c * n + cell] = mn[c];
+            for (int c = 0; c < 3; c++) (a.Ysave + cell)[c * n] = mn[c];
         }
         if (a.renorm) {
             T f = Ms / sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
@@ -328,21 +393,21 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         }
         if (a.ev_out) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.ev_out[c * n + cell] = rhs[c];
+            for (int c = 0; c < 3; c++) (a.ev_out + cell)[c * n] = rhs[c];
         }
         if (a.copy_to) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.copy_to[c * n + cell] = m[c];
+            for (int c = 0; c < 3; c++) (a.copy_to + cell)[c * n] = m[c];
         }
         if (a.Mout) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.Mout[c * n + cell] = mn[c];
+            for (int c = 0; c < 3; c++) (a.Mout + cell)[c * n] = mn[c];
         }
         if (a.do_xfwd) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                *rp(c * rpb + r, x) = mn[c];
-                if ((x & 1) == 0 && x == nx - 1) *rp(c * rpb + r, x + 1) = 0;   // odd nx: zero the partner slot
+                sp[c * cstride] = mn[c];
+                if ((x & 1) == 0 && x == nx - 1) sp[c * cstride + 1] = 0;   // odd nx: zero the partner slot
             }
         }
     }
@@ -575,15 +640,21 @@ __device__ __forceinline__ void x_stockham(cpx<T> *line, int t, bool act, const 
     constexpr int LR = L / R, BPT = LR / TPL, TWS = L / (NS * R);
     constexpr bool LAST = NS * R == L;
     addrP<16> A;
+    // padded addresses: A(e + 16 q) = A(e) + 17 q, so strides that are multiples of 16 become
+    // compile-time offsets from one runtime base
+    constexpr bool LRP = (LR % 16) == 0, TPP = (TPL % 16) == 0, NSP = (NS % 16) == 0;
     cpx<T> v[BPT][R];
     if (act) {
+        const int at = A(t);
 #pragma unroll
-        for (int b = 0; b < BPT; b++)
+        for (int b = 0; b < BPT; b++) {
+            const int ab = TPP ? at + b * (TPL + TPL / 16) : A(t + b * TPL);
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 if (ZHALF && 2 * r >= R) v[b][r] = mk<T>(0, 0);
-                else v[b][r] = line[A(t + b * TPL + r * LR)];
+                else v[b][r] = line[LRP ? ab + r * (LR + LR / 16) : A(t + b * TPL + r * LR)];
             }
+        }
     }
     __syncthreads();
     if (act) {
@@ -592,19 +663,23 @@ __device__ __forceinline__ void x_stockham(cpx<T> *line, int t, bool act, const 
             const int j = t + b * TPL;
             const int k = j & (NS - 1);
             if (NS > 1) {
+                const int step = k * TWS;
+                const cpx<T> *tp = tw;
 #pragma unroll
                 for (int r = 1; r < R; r++) {
-                    cpx<T> w = tw[r * k * TWS];
+                    tp += step;
+                    cpx<T> w = *tp;
                     if (INV) w.y = -w.y;
                     v[b][r] = cmul(v[b][r], w);
                 }
             }
             dftR<T, R, INV>(v[b]);
             const int d = (j - k) * R + k;
+            const int ad = A(d);
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int e = d + r * NS;
-                if (!INV || !LAST || e < nkeep) line[A(e)] = v[b][r];
+                if (!INV || !LAST || e < nkeep) line[NSP ? ad + r * (NS + NS / 16) : A(e)] = v[b][r];
             }
         }
     }

@@ -195,7 +195,8 @@ int bm_run_timed(bm_ctx *ctx, int steps, bm_stats *out, double *device_ms);
  * Unused slots are 0. Leaves the spectrum buffers stale (the next run re-primes them). */
 int bm_time_kernels(bm_ctx *ctx, int mesh, int reps, double *ms4, double *bytes4);
 
-/* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width,
+/* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width (plus 100
+ * when the 3D y passes use the radix-16 Stockham transform),
  * z-pass width, stage rows per block (plus 100 when the stage kernel uses the radix-8
  * Stockham x transform; negative when it prefetches its per-cell rows into shared
  * memory)]. Valid after the first compute or run. */
@@ -204,9 +205,6 @@ int bm_tiles(bm_ctx *ctx, int mesh, int *tiles4);
 /* Test hooks (used by the test suite only). */
 /* FP64 demag kernel spectra (octant (Nx/2+1)(Ny/2+1)(Nz/2+1), 6 components xx,yy,zz,xy,xz,yz). */
 int bm_debug_kernels(bm_ctx *ctx, int mesh, double *K6);
-/* Device time of the stage kernel alone in one mode (0 stage update with nev evaluations, 1 x
- * forward only, 2 x inverse + field terms), ms per launch. */
-int bm_debug_time_stage(bm_ctx *ctx, int mesh, int mode, int nev, int reps, double *ms);
 /* Raw FP64 tensor octant values D(i,j,k) for i<nx, j<ny, k<nz: 6 per point. */
 int bm_debug_tensor(int device, int nx, int ny, int nz, double hx, double hy, double hz, double *oct6);
 /* Batched complex FFT on the device of `howmany` contiguous lines of length L (in place,

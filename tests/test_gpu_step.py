@@ -214,3 +214,27 @@ def test_stage_xv_every_length(bm, nx, prec, tol, monkeypatch):
         c.close()
         assert t["stage_xv"] == 1
         assert np.abs(m - s.get_m()).max() / 8e5 < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+@pytest.mark.parametrize("ny,W", [(128, 4), (256, 4), (512, 4), (1024, 2)])
+def test_ypass_stockham_every_length(bm, ny, W, prec, tol, monkeypatch):
+    """The radix-16 Stockham y transform (3D, Ny = 256 .. 2048: radix tails 16x16, 16x16x2,
+    16x16x4, 16x16x8) against the oracle's RK4 trajectory with demag, exchange and Zeeman, for a
+    power-of-two ny and one that leaves zero rows below Ny / 2."""
+    monkeypatch.setenv("BM_TILES", "1,%d,8,1" % W)
+    monkeypatch.setenv("BM_Y_XV", "1")
+    for n in [(8, ny, 2), (6, ny - 3, 3)]:
+        N = n[0] * n[1] * n[2]
+        mesh = dict(n=n, h=(3e-9, 3e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(2e3, 1e3, 0))
+        M = sphere_random(N, seed=ny, Ms=8e5)
+        s = OracleSolver([mesh], evaluation=0, dt=2e-14)
+        s.set_m(M)
+        s.run(10)
+        c = _make(bm, prec, mesh, M, "RK4", 2e-14)
+        c.run(10)
+        t = c.tiles()
+        m = c.get_m()
+        c.close()
+        assert t["ypass_yv"] == 1 and t["ypass_W"] == W
+        assert np.abs(m - s.get_m()).max() / 8e5 < tol
