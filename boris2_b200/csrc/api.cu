@@ -437,6 +437,82 @@ float time_launches(cudaStream_t s, F launch, int reps)
     return ms / reps;
 }
 
+// 3D y passes of one grid: transform variant (two-level register / radix-16 Stockham) x column
+// tile width, timed as a forward + inverse pair on the grid's own spectra
+template <typename T>
+void tune_ypass(bm_ctx *c, Mesh &m)
+{
+    cudaStream_t s = c->stream;
+    const int lim = bm_lb<T>::v;
+    const size_t cs = sizeof(cpx<T>);
+    YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
+    float best = 1e30f; int bw = m.Wy, byv = m.yv;
+    for (int yv = 0; yv <= (ypass_has_st(m.Ny) ? 1 : 0); yv++)
+        for (int W = 1; W <= 32 && W <= m.LX; W *= 2) {
+            if ((size_t)m.Ny * W * cs > 200 * 1024) continue;
+            if (yv) {
+                const int nt = ypass_st_threads(m.Ny, W);
+                if (nt > lim || nt % 32) continue;
+            } else if (ypass_has_reg(m.Ny) ? ypass_reg_threads(m.Ny, W) > lim : W * m.py.tpl > lim) {
+                continue;
+            }
+            a.W = W;
+            a.yv = yv;
+            float t = time_launches(s, [&]() { return launch_yfwd<T>(a, s); }, 3) +
+                      time_launches(s, [&]() { return launch_yinv<T>(a, s); }, 3);
+            if (t < best) { best = t; bw = W; byv = yv; }
+        }
+    m.Wy = bw;
+    m.yv = byv;
+}
+
+template <typename T> T *B(Mesh &m, int i);
+
+// x transforms of a multilayer common grid (x forward after the transfer in, x inverse before the
+// transfer out): register variant x rows per block, timed on the grid's own buffers
+template <typename T>
+int tune_grid_x(bm_ctx *c, Mesh &G)
+{
+    cudaStream_t s = c->stream;
+    const int lim = bm_lb<T>::v;
+    const size_t cs = sizeof(cpx<T>);
+    if (!stage_reg_q(G.LX)) return 0;
+    T *tmp = nullptr;
+    if (cudaMalloc(&tmp, sizeof(T) * 3 * G.n) != cudaSuccess) return 0;   // keep the heuristic choice
+    StageArgs<T> f = stage_args<T>(c, G);
+    f.st = nullptr;
+    f.mode = BM_MODE_UPDATE;
+    f.Min = B<T>(G, 0); f.Mbase = B<T>(G, 0);
+    f.nev = 0;
+    StageArgs<T> h = stage_args<T>(c, G);
+    h.st = nullptr;
+    h.mode = BM_MODE_HEFF;
+    h.modules = BM_DEMAG;
+    h.do_xfwd = 0;
+    h.Min = B<T>(G, 0);
+    h.Hout = tmp;
+    float best = 1e30f; int br = G.rpb, bx = G.xv;
+    const int rows = G.ny * G.nz;
+    for (int xv = 0; xv <= 1; xv++)
+        for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
+            if (((3 * rpb * stage_reg_q(G.LX, xv) + 31) & ~31) > lim) break;
+            if ((size_t)3 * rpb * padded_len(G.LX) * cs > 200 * 1024) break;
+            f.rpb = h.rpb = rpb;
+            f.xv = h.xv = xv;
+            f.staged = h.staged = 0;
+            float t = time_launches(s, [&]() { return launch_stage<T>(f, s); }, 3) +
+                      time_launches(s, [&]() { return launch_stage<T>(h, s); }, 3);
+            if (t < best) { best = t; br = rpb; bx = xv; }
+        }
+    G.rpb = br;
+    G.xv = bx;
+    G.staged = 0;
+    cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    cudaGetLastError();
+    return 0;
+}
+
 template <typename T>
 int autotune_mesh(bm_ctx *c, Mesh &m)
 {
@@ -444,6 +520,7 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
     const int lim = bm_lb<T>::v;
     const size_t cs = sizeof(cpx<T>);
     const int reps = 3;
+    if ((m.modules & BM_DEMAG) && m.ml_role == 1) tune_ypass<T>(c, m);   // its y passes feed the multilayer z pass
     if ((m.modules & BM_DEMAG) && m.ml_role == 0) {
         YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
         if (m.nz == 1) {
@@ -456,27 +533,9 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
             }
             m.W2 = bw;
         } else {
-            float best = 1e30f; int bw = m.Wy, byv = 0;
-            // y transform variant (two-level register / radix-16 Stockham) x column tile width
-            for (int yv = 0; yv <= (ypass_has_st(m.Ny) ? 1 : 0); yv++)
-                for (int W = 1; W <= 32 && W <= m.LX; W *= 2) {
-                    if ((size_t)m.Ny * W * cs > 200 * 1024) continue;
-                    if (yv) {
-                        const int nt = ypass_st_threads(m.Ny, W);
-                        if (nt > lim || nt % 32) continue;
-                    } else if (ypass_has_reg(m.Ny) ? ypass_reg_threads(m.Ny, W) > lim : W * m.py.tpl > lim) {
-                        continue;
-                    }
-                    a.W = W;
-                    a.yv = yv;
-                    float t = time_launches(s, [&]() { return launch_yfwd<T>(a, s); }, reps) +
-                              time_launches(s, [&]() { return launch_yinv<T>(a, s); }, reps);
-                    if (t < best) { best = t; bw = W; byv = yv; }
-                }
-            m.Wy = bw;
-            m.yv = byv;
-            a.yv = byv;
-            best = 1e30f; bw = m.Wz;
+            tune_ypass<T>(c, m);
+            a.yv = m.yv;
+            float best = 1e30f; int bw = m.Wz;
             for (int W = 4; W <= 128 && W <= m.LX; W *= 2) {
                 if (zmid_has_reg(m.Nz) ? (zmid_reg_smem<T>(m.Nz, W) > 200 * 1024 || 6 * W > lim)
                                        : (zmid_smem<T>(m.Nz, W) > 200 * 1024 || 2 * W * m.pz.tpl > lim)) continue;
@@ -670,6 +729,13 @@ int prepare_ml(bm_ctx *c)
     if (rc) return fail(BM_ECUDA, "multilayer kernel build failed (" + std::to_string(rc) + ")");
     if ((rc = upload_table<T>(&r.twz, g.N[2], false, s))) return rc;
     CK(cudaStreamSynchronize(s));
+    // common grids: y-pass variant and width, x-transform variant and rows per block
+    if (c->autotune)
+        for (int l = 0; l < L; l++) {
+            if (r.direct[l] >= 0) continue;
+            tune_ypass<T>(c, r.grids[l]);
+            if ((rc = tune_grid_x<T>(c, r.grids[l]))) return rc;
+        }
     // z pass tile: columns per block, the fastest of the widths that fit (timed on the layer
     // spectra, which the first evaluation rewrites)
     const int lim = bm_lb<T>::v, LX = g.N[0] / 2;
