@@ -88,7 +88,7 @@ __device__ __forceinline__ void ml_signs(int kind, int comp, bool ylo, bool inv,
     if (kind == BM_MLK_SELF) lo.y = (T)0;
 }
 
-// one stored value of a kernel at (comp, kz, pencil) of column kxc (kxc = -1: Nyquist column)
+// one stored value of a kernel at (comp, kz, pencil) of column w (w = -1: Nyquist column)
 template <typename T, int NZ>
 __device__ __forceinline__ cpx<T> ml_tile_get(const unsigned char *tile, int kind, int comp, int kz, int p, bool ylo, bool inv,
                                               int mainb, int w, int lw)
@@ -102,8 +102,14 @@ __device__ __forceinline__ cpx<T> ml_tile_get(const unsigned char *tile, int kin
     }
     constexpr int KZ1 = NZ / 2 + 1;
     const int akz = kz <= NZ / 2 ? kz : NZ - kz;
-    const cpx<T> *t = reinterpret_cast<const cpx<T> *>(tile);
-    cpx<T> v = (w >= 0) ? t[((comp * KZ1 + akz) << lw) + w] : reinterpret_cast<const cpx<T> *>(tile + mainb)[comp * KZ1 + akz];
+    cpx<T> v;
+    if (kind == BM_MLK_SELF) {
+        const T *t = reinterpret_cast<const T *>(tile);
+        v = mk<T>((w >= 0) ? t[((comp * KZ1 + akz) << lw) + w] : reinterpret_cast<const T *>(tile + mainb)[comp * KZ1 + akz], (T)0);
+    } else {
+        const cpx<T> *t = reinterpret_cast<const cpx<T> *>(tile);
+        v = (w >= 0) ? t[((comp * KZ1 + akz) << lw) + w] : reinterpret_cast<const cpx<T> *>(tile + mainb)[comp * KZ1 + akz];
+    }
     cpx<T> lo, hi;
     ml_signs<T>(kind, comp, ylo, inv, lo, hi);
     const cpx<T> sg = kz <= NZ / 2 ? lo : hi;
@@ -131,55 +137,51 @@ __global__ void __launch_bounds__(bm_lb<T>::v, zml_bounds<NZ>::blocks) k_zmid_ml
     const bool single = (ky == kym);
     const int np = single ? 1 : 2;
     const int tid = threadIdx.x, nt = blockDim.x;
-    // kernel tiles (async)
-    for (int u = 0; u < a.nu; u++) {
-        const MLUDesc d = a.u[u];
-        cpx<T> *t = reinterpret_cast<cpx<T> *>(Ks + d.sm);
-        const int mainb = zmid_ml_tile_main<T>(d.kind, NZ, W);
-        cpx<T> *tn = reinterpret_cast<cpx<T> *>(Ks + d.sm + mainb);
-        if (d.kind == BM_MLK_FULL) {
-            const long long nk = (long long)Kx1 * Ny * NZ;
-            const cpx<T> *K = reinterpret_cast<const cpx<T> *>(a.K + d.off);
-            for (int i = tid; i < 12 * NZ * W; i += nt) {
-                const int w = i & (W - 1), r = i >> lw;
-                const int pp = r & 1, kz = (r >> 1) % NZ, comp = (r >> 1) / NZ;
-                const int kx = kx0 + w;
-                const bool ok = kx < LX && pp < np;
-                cp_async_cpx<T>(&t[i], ok ? &K[comp * nk + ((long long)kz * Ny + (pp ? kym : ky)) * Kx1 + kx] : K, ok);
+    // kernel tiles (async): thread group g (W threads, one column each) copies rows g, g + ng, ...
+    // of every unique kernel, one address computation per element
+    {
+        const int w = tid & (W - 1), g = tid >> lw, ng = nt >> lw;
+        const int kx = kx0 + w;
+        const bool okx = kx < LX;
+        for (int u = 0; u < a.nu; u++) {
+            const MLUDesc d = a.u[u];
+            unsigned char *tb = Ks + d.sm;
+            const int mainb = zmid_ml_tile_main<T>(d.kind, NZ, W);
+            if (d.kind == BM_MLK_FULL) {
+                const long long nk = (long long)Kx1 * Ny * NZ;
+                const cpx<T> *K = reinterpret_cast<const cpx<T> *>(a.K + d.off);
+                cpx<T> *t = reinterpret_cast<cpx<T> *>(tb);
+                cpx<T> *tn = reinterpret_cast<cpx<T> *>(tb + mainb);
+                for (int j = g; j < 12 * NZ; j += ng) {
+                    const int pp = j & 1, kz = (j >> 1) % NZ, comp = (j >> 1) / NZ;
+                    const bool ok = okx && pp < np;
+                    const long long q = comp * nk + ((long long)kz * Ny + (pp ? kym : ky)) * Kx1;
+                    cp_async_cpx<T>(&t[(j << lw) + w], ok ? &K[q + kx] : K, ok);
+                    if (kx0 == 0 && w == 0) cp_async_cpx<T>(&tn[j], pp < np ? &K[q + LX] : K, pp < np);
+                }
+            } else if (d.kind == BM_MLK_SELF) {
+                const long long nk = (long long)Kx1 * Ky1 * KZ1;
+                const T *K = a.K + d.off;
+                T *t = reinterpret_cast<T *>(tb);
+                T *tn = reinterpret_cast<T *>(tb + mainb);
+                for (int j = g; j < 6 * KZ1; j += ng) {
+                    const int kz = j % KZ1, comp = j / KZ1;
+                    const long long q = comp * nk + ((long long)kz * Ky1 + ky) * Kx1;
+                    cp_async_real<T>(&t[(j << lw) + w], okx ? &K[q + kx] : K, okx);
+                    if (kx0 == 0 && w == 0) cp_async_real<T>(&tn[j], &K[q + LX], true);
+                }
+            } else {
+                const long long nk = (long long)Kx1 * Ky1 * KZ1;
+                const cpx<T> *K = reinterpret_cast<const cpx<T> *>(a.K + d.off);
+                cpx<T> *t = reinterpret_cast<cpx<T> *>(tb);
+                cpx<T> *tn = reinterpret_cast<cpx<T> *>(tb + mainb);
+                for (int j = g; j < 6 * KZ1; j += ng) {
+                    const int kz = j % KZ1, comp = j / KZ1;
+                    const long long q = comp * nk + ((long long)kz * Ky1 + ky) * Kx1;
+                    cp_async_cpx<T>(&t[(j << lw) + w], okx ? &K[q + kx] : K, okx);
+                    if (kx0 == 0 && w == 0) cp_async_cpx<T>(&tn[j], &K[q + LX], true);
+                }
             }
-            if (kx0 == 0)
-                for (int i = tid; i < 12 * NZ; i += nt) {
-                    const int pp = i & 1, kz = (i >> 1) % NZ, comp = (i >> 1) / NZ;
-                    const bool ok = pp < np;
-                    cp_async_cpx<T>(&tn[i], ok ? &K[comp * nk + ((long long)kz * Ny + (pp ? kym : ky)) * Kx1 + LX] : K, ok);
-                }
-        } else {
-            const long long nk = (long long)Kx1 * Ky1 * KZ1;
-            const bool self = d.kind == BM_MLK_SELF;
-            for (int i = tid; i < 6 * KZ1 * W; i += nt) {
-                const int w = i & (W - 1), r = i >> lw, kz = r % KZ1, comp = r / KZ1;
-                const int kx = kx0 + w;
-                const long long q = comp * nk + ((long long)kz * Ky1 + ky) * Kx1 + kx;
-                if (self) {
-                    // real value into .x, zero into .y
-                    cp_async_real<T>(&t[i].x, kx < LX ? a.K + d.off + q : a.K, kx < LX);
-                    cp_async_real<T>(&t[i].y, a.K, false);
-                } else {
-                    const cpx<T> *K = reinterpret_cast<const cpx<T> *>(a.K + d.off);
-                    cp_async_cpx<T>(&t[i], kx < LX ? &K[q] : K, kx < LX);
-                }
-            }
-            if (kx0 == 0)
-                for (int i = tid; i < 6 * KZ1; i += nt) {
-                    const int kz = i % KZ1, comp = i / KZ1;
-                    const long long q = comp * nk + ((long long)kz * Ky1 + ky) * Kx1 + LX;
-                    if (self) {
-                        cp_async_real<T>(&tn[i].x, a.K + d.off + q, true);
-                        cp_async_real<T>(&tn[i].y, a.K, false);
-                    } else {
-                        cp_async_cpx<T>(&tn[i], reinterpret_cast<const cpx<T> *>(a.K + d.off) + q, true);
-                    }
-                }
         }
     }
     cp_async_commit();
@@ -227,6 +229,21 @@ __global__ void __launch_bounds__(bm_lb<T>::v, zml_bounds<NZ>::blocks) k_zmid_ml
                     const cpx<T> *in = In + IDX(s, cc, p, 0, w);
 #pragma unroll
                     for (int kz = 0; kz < NZ; kz++) v[kz] = v[kz] + cscale(cmul(row[(kz * 2) << lw], in[kz << lw]), sg);
+                }
+            } else if (d.kind == BM_MLK_SELF) {
+#pragma unroll
+                for (int cc = 0; cc < 3; cc++) {
+                    cpx<T> lo, hi;
+                    ml_signs<T>(d.kind, cmp[cc], p == 0, inv, lo, hi);
+                    const T *row = reinterpret_cast<const T *>(Ks + d.sm) + ((cmp[cc] * KZ1) << lw) + w;
+                    const cpx<T> *in = In + IDX(s, cc, p, 0, w);
+#pragma unroll
+                    for (int kz = 0; kz < NZ; kz++) {
+                        const int akz = kz <= NZ / 2 ? kz : NZ - kz;
+                        const T kr = (kz <= NZ / 2 ? lo.x : hi.x) * row[akz << lw];
+                        const cpx<T> x = in[kz << lw];
+                        v[kz] = mk<T>(v[kz].x + kr * x.x, v[kz].y + kr * x.y);
+                    }
                 }
             } else {
 #pragma unroll

@@ -93,17 +93,22 @@ struct MLZArgs {
     int gate;
 };
 
-// bytes of one unique kernel's staged tile at a block's columns (complex values, 16-aligned):
-//   self, z-shift  [comp][kz <= Nz/2][W] and the Nyquist column [comp][kz <= Nz/2]
-//   full           [comp][kz][pencil][W] and the Nyquist column [comp][kz][pencil]
+// bytes of one unique kernel's staged tile at a block's columns (16-aligned):
+//   self     [comp][kz <= Nz/2][W] real and the Nyquist column [comp][kz <= Nz/2] real
+//   z-shift  [comp][kz <= Nz/2][W] complex and the Nyquist column [comp][kz <= Nz/2] complex
+//   full     [comp][kz][pencil][W] complex and the Nyquist column [comp][kz][pencil] complex
 template <typename T> BM_HD int zmid_ml_tile_main(int kind, int Nz, int W)
 {
-    size_t b = (kind == BM_MLK_FULL) ? (size_t)12 * Nz * W * sizeof(cpx<T>) : (size_t)6 * (Nz / 2 + 1) * W * sizeof(cpx<T>);
+    size_t b = (kind == BM_MLK_FULL) ? (size_t)12 * Nz * W * sizeof(cpx<T>)
+             : (kind == BM_MLK_SELF) ? (size_t)6 * (Nz / 2 + 1) * W * sizeof(T)
+                                     : (size_t)6 * (Nz / 2 + 1) * W * sizeof(cpx<T>);
     return (int)((b + 15) & ~(size_t)15);
 }
 template <typename T> BM_HD int zmid_ml_tile_bytes(int kind, int Nz, int W)
 {
-    size_t nyq = (kind == BM_MLK_FULL) ? (size_t)12 * Nz * sizeof(cpx<T>) : (size_t)6 * (Nz / 2 + 1) * sizeof(cpx<T>);
+    size_t nyq = (kind == BM_MLK_FULL) ? (size_t)12 * Nz * sizeof(cpx<T>)
+               : (kind == BM_MLK_SELF) ? (size_t)6 * (Nz / 2 + 1) * sizeof(T)
+                                       : (size_t)6 * (Nz / 2 + 1) * sizeof(cpx<T>);
     return zmid_ml_tile_main<T>(kind, Nz, W) + (int)((nyq + 15) & ~(size_t)15);
 }
 template <typename T> size_t zmid_ml_smem(int L, int Nz, int W, int ksm)
