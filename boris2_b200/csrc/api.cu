@@ -16,6 +16,7 @@
 #include "ml.h"
 #include "util.h"
 #include <vector>
+#include <map>
 #include <string>
 #include <cmath>
 #include <cstring>
@@ -107,6 +108,7 @@ struct MLRun {
 // the second (under stream capture) launches them from the uploaded copies.
 struct BatchRec {
     int kind;             // 0 stage, else BM_BATCH_*
+    int key;              // register-kernel length of the launch (0: generic-length kernel)
     size_t args_off, work_off;
     int nwork, nt;
     size_t smem;
@@ -881,38 +883,34 @@ size_t bp_append(BatchPlan &bp, const void *p, size_t bytes)
 
 // stage kernels of several meshes: per-mesh launches, or one launch over (mesh, row block) items
 // with the generic-length kernel (rows per block chosen so every mesh fills ~256 threads)
+// stage kernels of every mesh: one launch per x length with a radix-8 register kernel, one for
+// the remaining lengths (generic kernel). Only the last launch finishes the step (error-norm
+// controller, time advance); the earlier ones only add to the error-norm maximum.
 template <typename T>
-int stage_multi(bm_ctx *c, std::vector<StageArgs<T>> &v, int *count)
+int stage_batch_one(bm_ctx *c, int key, std::vector<StageArgs<T>> &v, int *count)
 {
-    if (v.empty()) return 0;
-    if (!c->batched || v.size() == 1) {
-        for (auto &a : v) {
-            CKL(launch_stage<T>(a, c->stream), "stage");
-            (*count)++;
-        }
-        return 0;
-    }
     BatchPlan &bp = c->bp;
     if (bp.collect) {
-        int lk = BM_LAST_NONE;
-        for (auto &a : v) if (a.last_kind != BM_LAST_NONE) lk = a.last_kind;
         std::vector<int2> work;
         int nt = 32;
         size_t smem = 0;
         for (size_t i = 0; i < v.size(); i++) {
             StageArgs<T> &a = v[i];
-            a.last_kind = lk;
             a.staged = 0;
             const int rows = a.ny * a.nz;
-            int rpb = 256 / (3 * a.px.tpl);
+            const int tpl = key ? stage_reg_q(a.LX, 1) : a.px.tpl;
+            int rpb = 256 / (3 * tpl);
             rpb = std::max(1, std::min(rpb, rows));
             a.rpb = rpb;
+            a.xv = key ? 1 : 0;
             for (int b = 0; b < (rows + rpb - 1) / rpb; b++) work.push_back(make_int2((int)i, b));
-            nt = std::max(nt, (3 * rpb * a.px.tpl + 31) & ~31);
-            smem = std::max(smem, (size_t)3 * rpb * padded_len(a.LX) * sizeof(cpx<T>));
+            nt = std::max(nt, (3 * rpb * tpl + 31) & ~31);
+            const size_t lsp = key ? (size_t)(a.LX + a.LX / 16 + 1) : (size_t)padded_len(a.LX);
+            smem = std::max(smem, (size_t)3 * rpb * lsp * sizeof(cpx<T>));
         }
         BatchRec r;
         r.kind = 0;
+        r.key = key;
         r.args_off = bp_append(bp, v.data(), sizeof(StageArgs<T>) * v.size());
         r.work_off = bp_append(bp, work.data(), sizeof(int2) * work.size());
         r.nwork = (int)work.size();
@@ -924,13 +922,36 @@ int stage_multi(bm_ctx *c, std::vector<StageArgs<T>> &v, int *count)
     if (bp.next >= bp.recs.size()) return fail(BM_ESTATE, "batched launch plan out of step");
     const BatchRec &r = bp.recs[bp.next++];
     const char *base = (const char *)bp.dbuf;
-    CKL(launch_stage_batch<T>((const StageArgs<T> *)(base + r.args_off), (const int2 *)(base + r.work_off), r.nwork, r.nt,
-                              r.smem, c->stream), "stage batch");
+    CKL(launch_stage_batch<T>(r.key, (const StageArgs<T> *)(base + r.args_off), (const int2 *)(base + r.work_off), r.nwork,
+                              r.nt, r.smem, c->stream), "stage batch");
     (*count)++;
     return 0;
 }
 
-// generic-kernel tile widths of a mesh for the batched y passes and z pass
+template <typename T>
+int stage_multi(bm_ctx *c, std::vector<StageArgs<T>> &v, int *count)
+{
+    if (v.empty()) return 0;
+    if (!c->batched || v.size() == 1) {
+        for (auto &a : v) {
+            CKL(launch_stage<T>(a, c->stream), "stage");
+            (*count)++;
+        }
+        return 0;
+    }
+    int lk = BM_LAST_NONE;
+    for (auto &a : v) if (a.last_kind != BM_LAST_NONE) lk = a.last_kind;
+    std::map<int, std::vector<StageArgs<T>>> groups;   // x length with a register kernel, or 0
+    for (auto &a : v) groups[stage_reg_q(a.LX, 1) ? a.LX : 0].push_back(a);
+    size_t gi = 0;
+    for (auto &kv : groups) {
+        const bool last = (++gi == groups.size());
+        for (auto &a : kv.second) a.last_kind = last ? lk : BM_LAST_NONE;
+        if (int rc = stage_batch_one<T>(c, kv.first, kv.second, count)) return rc;
+    }
+    return 0;
+}
+
 template <typename T>
 void batch_tiles(const Mesh &m, int &Wy, int &Wz)
 {
@@ -944,7 +965,7 @@ void batch_tiles(const Mesh &m, int &Wy, int &Wz)
 }
 
 template <typename T>
-int yz_batch_one(bm_ctx *c, int kind, std::vector<YZArgs<T>> &v, int *count)
+int yz_batch_one(bm_ctx *c, int kind, int key, std::vector<YZArgs<T>> &v, int *count)
 {
     if (v.empty()) return 0;
     BatchPlan &bp = c->bp;
@@ -956,7 +977,15 @@ int yz_batch_one(bm_ctx *c, int kind, std::vector<YZArgs<T>> &v, int *count)
             const YZArgs<T> &a = v[i];
             const int nbx = (a.LX + a.W - 1) / a.W;
             int items = nbx;
-            if (kind == BM_BATCH_YFWD || kind == BM_BATCH_YINV) {
+            if (kind == BM_BATCH_YFWD_REG || kind == BM_BATCH_YINV_REG) {
+                items = nbx * a.nz * 3;
+                nt = std::max(nt, (ypass_reg_threads(a.Ny, a.W) + 31) & ~31);
+                smem = std::max(smem, (size_t)a.Ny * a.W * sizeof(cpx<T>));
+            } else if (kind == BM_BATCH_ZMID_REG) {
+                items = nbx * (a.Ny / 2 + 1);
+                nt = std::max(nt, (6 * a.W + 31) & ~31);
+                smem = std::max(smem, zmid_reg_smem<T>(a.Nz, a.W));
+            } else if (kind == BM_BATCH_YFWD || kind == BM_BATCH_YINV) {
                 items = nbx * a.nz * 3;
                 nt = std::max(nt, (a.W * a.py.tpl + 31) & ~31);
                 smem = std::max(smem, (size_t)a.Ny * a.W * sizeof(cpx<T>));
@@ -972,6 +1001,7 @@ int yz_batch_one(bm_ctx *c, int kind, std::vector<YZArgs<T>> &v, int *count)
         }
         BatchRec r;
         r.kind = kind;
+        r.key = key;
         r.args_off = bp_append(bp, v.data(), sizeof(YZArgs<T>) * v.size());
         r.work_off = bp_append(bp, work.data(), sizeof(int2) * work.size());
         r.nwork = (int)work.size();
@@ -983,37 +1013,58 @@ int yz_batch_one(bm_ctx *c, int kind, std::vector<YZArgs<T>> &v, int *count)
     if (bp.next >= bp.recs.size()) return fail(BM_ESTATE, "batched launch plan out of step");
     const BatchRec &r = bp.recs[bp.next++];
     const char *base = (const char *)bp.dbuf;
-    CKL(launch_yz_batch<T>(r.kind, (const YZArgs<T> *)(base + r.args_off), (const int2 *)(base + r.work_off), r.nwork, r.nt,
-                           r.smem, c->stream), "y/z batch");
+    CKL(launch_yz_batch<T>(r.kind, r.key, (const YZArgs<T> *)(base + r.args_off), (const int2 *)(base + r.work_off), r.nwork,
+                           r.nt, r.smem, c->stream), "y/z batch");
     (*count)++;
     return 0;
 }
 
-// y/z passes of every mesh with demag in four launches (2D y pass, y forward, z pass, y inverse)
+// y/z passes of every mesh with demag: the 2D y pass in one launch; the 3D y forward, z pass and
+// y inverse each in one launch per transform length with a register kernel plus one launch for the
+// remaining lengths (generic kernels)
 template <typename T>
 int yz_multi(bm_ctx *c, int gate, int *count)
 {
-    std::vector<YZArgs<T>> v2, vy, vz;
+    const int lim = 256;
+    std::vector<YZArgs<T>> v2;
+    std::map<int, std::vector<YZArgs<T>>> gy, gz;   // key Ny / Nz with a register kernel, or 0
     for (auto &m : c->meshes) {
         if (!(m.modules & BM_DEMAG)) continue;
         YZArgs<T> a = yz_args<T>(c, m, gate);
         if (m.nz == 1) {
             a.W = m.W2;
             v2.push_back(a);
+            continue;
+        }
+        int Wy, Wz;
+        batch_tiles<T>(m, Wy, Wz);
+        if (ypass_has_reg(m.Ny)) {
+            int W = 16;
+            while (W > 1 && (ypass_reg_threads(m.Ny, W) > lim || (size_t)m.Ny * W * sizeof(cpx<T>) > 64 * 1024 || W > m.LX)) W /= 2;
+            a.W = W;
+            gy[m.Ny].push_back(a);
         } else {
-            int Wy, Wz;
-            batch_tiles<T>(m, Wy, Wz);
             a.W = Wy;
-            vy.push_back(a);
+            gy[0].push_back(a);
+        }
+        if (zmid_has_reg(m.Nz)) {
+            int W = 16;
+            while (W > 1 && (6 * W > lim || zmid_reg_smem<T>(m.Nz, W) > 64 * 1024 || W > m.LX)) W /= 2;
+            a.W = W;
+            gz[m.Nz].push_back(a);
+        } else {
             a.W = Wz;
-            vz.push_back(a);
+            gz[0].push_back(a);
         }
     }
     int rc;
-    if ((rc = yz_batch_one<T>(c, BM_BATCH_YMID2D, v2, count))) return rc;
-    if ((rc = yz_batch_one<T>(c, BM_BATCH_YFWD, vy, count))) return rc;
-    if ((rc = yz_batch_one<T>(c, BM_BATCH_ZMID, vz, count))) return rc;
-    if ((rc = yz_batch_one<T>(c, BM_BATCH_YINV, vy, count))) return rc;
+    if ((rc = yz_batch_one<T>(c, BM_BATCH_YMID2D, 0, v2, count))) return rc;
+    for (auto &kv : gy)
+        if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_YFWD_REG : BM_BATCH_YFWD, kv.first, kv.second, count))) return rc;
+    for (auto &kv : gz)
+        if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_ZMID_REG : BM_BATCH_ZMID, kv.first, kv.second, count))) return rc;
+    for (auto &kv : gy)
+        if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_YINV_REG : BM_BATCH_YINV, kv.first, kv.second, count))) return rc;
     return 0;
 }
 

@@ -332,9 +332,8 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_batch(const YZArgs<T> *__r
 // row j < 6 copies kernel component j for every kz). Thread (c, p, w): w fastest so global loads
 // and stores coalesce.
 template <typename T, int NZ>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
+__device__ __forceinline__ void zmid_reg_body(const YZArgs<T> &a, int bx, int ky)
 {
-    if (gated_out<T>(a.st, a.gate)) return;
     extern __shared__ unsigned char smraw[];
     const int W = a.W, Ny = a.Ny, nz = a.nz, LX = a.LX;
     const int lw = __ffs(W) - 1;
@@ -343,8 +342,8 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
     T *Ks = reinterpret_cast<T *>(sm + 6 * NZ * W);
     T *Kn = Ks + 6 * KZ1 * W;
-    const int kx0 = blockIdx.x * W;
-    const int ky = blockIdx.y, kym = (Ny - ky) % Ny;
+    const int kx0 = bx * W;
+    const int kym = (Ny - ky) % Ny;
     const bool single = (ky == kym);
     const int np = single ? 1 : 2;
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -451,6 +450,25 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
 }
 
 template <typename T, int NZ>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    zmid_reg_body<T, NZ>(a, blockIdx.x, blockIdx.y);
+}
+
+// many meshes with the same Nz in one launch: work item (mesh, column tile + W-columns count * ky)
+template <typename T, int NZ>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg_batch(const YZArgs<T> *__restrict__ args,
+                                                                   const int2 *__restrict__ work, int nwork)
+{
+    if (gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    const YZArgs<T> &a = args[it.x];
+    const int nbx = (a.LX + a.W - 1) / a.W;
+    zmid_reg_body<T, NZ>(a, it.y % nbx, it.y / nbx);
+}
+
+template <typename T, int NZ>
 static int launch_zmid_reg(const YZArgs<T> &a, cudaStream_t s)
 {
     int nt = (6 * a.W + 31) & ~31;
@@ -479,15 +497,14 @@ bool zmid_has_reg(int Nz)
 // compile-time zeros (n2 >= Q/2). Inverse: only rows < ny (k1 < P/2) are written. One shared
 // transpose per transform instead of one per radix pass; no runtime division.
 template <typename T, int P, int Q, bool INV>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass_reg(YZArgs<T> a)
+__device__ __forceinline__ void ypass_reg_body(const YZArgs<T> &a, int bx, int z, int c)
 {
-    if (gated_out<T>(a.st, a.gate)) return;
     extern __shared__ unsigned char smraw[];
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
     constexpr int L = P * Q;
     const int W = a.W, ny = a.ny, LX = a.LX, nz = a.nz;
     const int lw = __ffs(W) - 1;
-    const int kx0 = blockIdx.x * W, z = blockIdx.y, c = blockIdx.z;
+    const int kx0 = bx * W;
     const int tid = threadIdx.x;
     const int w = tid & (W - 1), r = tid >> lw;
     const int kx = kx0 + w;
@@ -542,6 +559,27 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_ypass_reg(YZArgs<T> a)
             }
         }
     }
+}
+
+template <typename T, int P, int Q, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass_reg(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    ypass_reg_body<T, P, Q, INV>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// many meshes with the same Ny in one launch: work item (mesh, column tile + W-columns count *
+// (z + nz * component))
+template <typename T, int P, int Q, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass_reg_batch(const YZArgs<T> *__restrict__ args,
+                                                                    const int2 *__restrict__ work, int nwork)
+{
+    if (gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    const YZArgs<T> &a = args[it.x];
+    const int nbx = (a.LX + a.W - 1) / a.W;
+    const int bx = it.y % nbx, r = it.y / nbx;
+    ypass_reg_body<T, P, Q, INV>(a, bx, r % a.nz, r / a.nz);
 }
 
 template <int L> struct ysplit {
@@ -835,8 +873,45 @@ static int launch_batch_common(KF kern, int nwork, int nt, size_t smem, int *gri
     return 0;
 }
 
+template <typename T, int NZ>
+static int launch_zmid_reg_batch(const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+{
+    int grid = 1, rc = launch_batch_common(k_zmid_reg_batch<T, NZ>, nwork, nt, smem, &grid);
+    if (rc) return rc;
+    k_zmid_reg_batch<T, NZ><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, int L, bool INV>
+static int launch_ypass_reg_batch(const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+{
+    constexpr int P = ysplit<L>::p, Q = ysplit<L>::q;
+    int grid = 1, rc = launch_batch_common(k_ypass_reg_batch<T, P, Q, INV>, nwork, nt, smem, &grid);
+    if (rc) return rc;
+    k_ypass_reg_batch<T, P, Q, INV><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, bool INV>
+static int ypass_reg_batch_dispatch(int Ny, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem,
+                                    cudaStream_t s)
+{
+    switch (Ny) {
+    case 8: return launch_ypass_reg_batch<T, 8, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 16: return launch_ypass_reg_batch<T, 16, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 32: return launch_ypass_reg_batch<T, 32, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 64: return launch_ypass_reg_batch<T, 64, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 128: return launch_ypass_reg_batch<T, 128, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 256: return launch_ypass_reg_batch<T, 256, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 512: return launch_ypass_reg_batch<T, 512, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 1024: return launch_ypass_reg_batch<T, 1024, INV>(dargs, dwork, nwork, nt, smem, s);
+    default: return 111;
+    }
+}
+
 template <typename T>
-int launch_yz_batch(int kind, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+int launch_yz_batch(int kind, int key, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem,
+                    cudaStream_t s)
 {
     if (nwork < 1) return 0;
     int grid = 1, rc = 0;
@@ -857,10 +932,25 @@ int launch_yz_batch(int kind, const YZArgs<T> *dargs, const int2 *dwork, int nwo
         if ((rc = launch_batch_common(k_zmid_batch<T>, nwork, nt, smem, &grid))) return rc;
         k_zmid_batch<T><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
         break;
+    case BM_BATCH_ZMID_REG:
+        switch (key) {
+        case 4: return launch_zmid_reg_batch<T, 4>(dargs, dwork, nwork, nt, smem, s);
+        case 6: return launch_zmid_reg_batch<T, 6>(dargs, dwork, nwork, nt, smem, s);
+        case 8: return launch_zmid_reg_batch<T, 8>(dargs, dwork, nwork, nt, smem, s);
+        case 12: return launch_zmid_reg_batch<T, 12>(dargs, dwork, nwork, nt, smem, s);
+        case 16: return launch_zmid_reg_batch<T, 16>(dargs, dwork, nwork, nt, smem, s);
+        case 24: return launch_zmid_reg_batch<T, 24>(dargs, dwork, nwork, nt, smem, s);
+        case 32: return launch_zmid_reg_batch<T, 32>(dargs, dwork, nwork, nt, smem, s);
+        case 48: return launch_zmid_reg_batch<T, 48>(dargs, dwork, nwork, nt, smem, s);
+        case 64: return launch_zmid_reg_batch<T, 64>(dargs, dwork, nwork, nt, smem, s);
+        default: return 111;
+        }
+    case BM_BATCH_YFWD_REG: return ypass_reg_batch_dispatch<T, false>(key, dargs, dwork, nwork, nt, smem, s);
+    case BM_BATCH_YINV_REG: return ypass_reg_batch_dispatch<T, true>(key, dargs, dwork, nwork, nt, smem, s);
     default: return 110;
     }
     return (int)cudaGetLastError();
 }
 
-template int launch_yz_batch<float>(int, const YZArgs<float> *, const int2 *, int, int, size_t, cudaStream_t);
-template int launch_yz_batch<double>(int, const YZArgs<double> *, const int2 *, int, int, size_t, cudaStream_t);
+template int launch_yz_batch<float>(int, int, const YZArgs<float> *, const int2 *, int, int, size_t, cudaStream_t);
+template int launch_yz_batch<double>(int, int, const YZArgs<double> *, const int2 *, int, int, size_t, cudaStream_t);

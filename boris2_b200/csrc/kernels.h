@@ -160,10 +160,16 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s);
 #define BM_BATCH_YFWD 2
 #define BM_BATCH_ZMID 3
 #define BM_BATCH_YINV 4
+// register-kernel buckets: every mesh of the launch has the same transform length (key)
+#define BM_BATCH_ZMID_REG 5   // key Nz
+#define BM_BATCH_YFWD_REG 6   // key Ny
+#define BM_BATCH_YINV_REG 7   // key Ny
 template <typename T>
-int launch_yz_batch(int kind, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
+int launch_yz_batch(int kind, int key, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem,
+                    cudaStream_t s);
+// key 0: generic-length stage kernel; key LX: the radix-8 register kernel of that length
 template <typename T>
-int launch_stage_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
+int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
 int stage_reg_q(int LX, int xv = 0);   // threads per x line of the register stage kernel, variant xv (0: generic kernel)
 int launch_scalar_reset(StepState *st, cudaStream_t s);
 

@@ -695,9 +695,8 @@ __device__ __forceinline__ void x_reg(cpx<T> *line, int t, bool act, const cpx<T
 }
 
 template <typename T, int LX, int XV>
-__device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a)
+__device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, unsigned int total)
 {
-    if (stage_gated_out<T>(a.st, a.gate)) return;
     extern __shared__ unsigned char smraw[];
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
     using C = xr_cfg<LX, XV>;
@@ -705,7 +704,7 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a)
     addrP<C::PAD> A;
     const int rpb = a.rpb;
     const int nrows = a.ny * a.nz;
-    const int r0 = blockIdx.x * rpb;
+    const int r0 = bid * rpb;
     const int tid = threadIdx.x;
     const int q = tid / TPL, t = tid % TPL;
     const int qc = q / rpb, qr = q % rpb;
@@ -796,19 +795,32 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a)
             for (int mm = t; mm < LX; mm += TPL) dst[mm] = line[A(mm)];
         }
     }
-    stage_tail<T>(a, lmax, gridDim.x);
+    stage_tail<T>(a, lmax, total);
 }
 
 template <typename T, int LX>
 __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
 {
-    stage_reg_body<T, LX, 0>(a);
+    if (stage_gated_out<T>(a.st, a.gate)) return;
+    stage_reg_body<T, LX, 0>(a, blockIdx.x, gridDim.x);
 }
 
 template <typename T, int LX>
 __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : 64) k_stage_rx(StageArgs<T> a)
 {
-    stage_reg_body<T, LX, 1>(a);
+    if (stage_gated_out<T>(a.st, a.gate)) return;
+    stage_reg_body<T, LX, 1>(a, blockIdx.x, gridDim.x);
+}
+
+// many meshes with the same x length in one launch (radix-8 transform): work item (mesh, row
+// block); the error-norm maximum and the step bookkeeping follow k_stage_batch
+template <typename T, int LX>
+__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : 64) k_stage_rx_batch(const StageArgs<T> *__restrict__ args,
+                                                                         const int2 *__restrict__ work, int nwork)
+{
+    if (stage_gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    stage_reg_body<T, LX, 1>(args[it.x], it.y, (unsigned int)nwork);
 }
 
 template <typename T, int LX, int XV>
@@ -887,12 +899,34 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
 template int launch_stage<float>(const StageArgs<float> &, cudaStream_t);
 template int launch_stage<double>(const StageArgs<double> &, cudaStream_t);
 
+template <typename T, int LX>
+static int launch_stage_rx_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+{
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_stage_rx_batch<T, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        if (e != cudaSuccess) return (int)e;
+    }
+    k_stage_rx_batch<T, LX><<<nwork, nt, smem, s>>>(dargs, dwork, nwork);
+    return (int)cudaGetLastError();
+}
+
 template <typename T>
-int launch_stage_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
 {
     if (nwork < 1) return 0;
     if (nt > bm_lb<T>::v || nt < 32) return 211;
     if (smem > 200 * 1024) return 212;
+    switch (key) {
+    case 0: break;
+    case 16: return launch_stage_rx_batch<T, 16>(dargs, dwork, nwork, nt, smem, s);
+    case 32: return launch_stage_rx_batch<T, 32>(dargs, dwork, nwork, nt, smem, s);
+    case 64: return launch_stage_rx_batch<T, 64>(dargs, dwork, nwork, nt, smem, s);
+    case 128: return launch_stage_rx_batch<T, 128>(dargs, dwork, nwork, nt, smem, s);
+    case 256: return launch_stage_rx_batch<T, 256>(dargs, dwork, nwork, nt, smem, s);
+    case 512: return launch_stage_rx_batch<T, 512>(dargs, dwork, nwork, nt, smem, s);
+    case 1024: return launch_stage_rx_batch<T, 1024>(dargs, dwork, nwork, nt, smem, s);
+    default: return 213;
+    }
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_stage_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
@@ -901,5 +935,5 @@ int launch_stage_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, 
     return (int)cudaGetLastError();
 }
 
-template int launch_stage_batch<float>(const StageArgs<float> *, const int2 *, int, int, size_t, cudaStream_t);
-template int launch_stage_batch<double>(const StageArgs<double> *, const int2 *, int, int, size_t, cudaStream_t);
+template int launch_stage_batch<float>(int, const StageArgs<float> *, const int2 *, int, int, size_t, cudaStream_t);
+template int launch_stage_batch<double>(int, const StageArgs<double> *, const int2 *, int, int, size_t, cudaStream_t);
