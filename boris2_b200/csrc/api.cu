@@ -478,7 +478,7 @@ int tune_grid_x(bm_ctx *c, Mesh &G)
     cudaStream_t s = c->stream;
     const int lim = bm_lb<T>::v;
     const size_t cs = sizeof(cpx<T>);
-    if (!stage_reg_q(G.LX)) return 0;
+    if (!stage_reg_q(G.LX, 1)) return 0;
     T *tmp = nullptr;
     if (cudaMalloc(&tmp, sizeof(T) * 3 * G.n) != cudaSuccess) return 0;   // keep the heuristic choice
     StageArgs<T> f = stage_args<T>(c, G);
@@ -497,7 +497,8 @@ int tune_grid_x(bm_ctx *c, Mesh &G)
     const int rows = G.ny * G.nz;
     for (int xv = 0; xv <= 1; xv++)
         for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
-            if (((3 * rpb * stage_reg_q(G.LX, xv) + 31) & ~31) > lim) break;
+            const int tpl = stage_reg_q(G.LX, xv) ? stage_reg_q(G.LX, xv) : G.px.tpl;
+            if (((3 * rpb * tpl + 31) & ~31) > lim) break;
             if ((size_t)3 * rpb * padded_len(G.LX) * cs > 200 * 1024) break;
             f.rpb = h.rpb = rpb;
             f.xv = h.xv = xv;
@@ -563,13 +564,13 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
         a.Mout = tmp + 3 * m.n;
         float best = 1e30f; int br = m.rpb, bs = 0, bx = 0;
         int rows = m.ny * m.nz;
-        const bool reg = stage_reg_q(m.LX) != 0;
+        const bool reg = stage_reg_q(m.LX, 1) != 0;
         // x-transform variant x rows per block x (per-cell rows prefetched to shared memory or
         // read from global); variants and staging apply to the register kernels only
         for (int xv = 0; xv <= (reg ? 1 : 0); xv++)
             for (int stg = 0; stg <= (reg ? 1 : 0); stg++)
                 for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
-                    const int tpl = reg ? stage_reg_q(m.LX, xv) : m.px.tpl;
+                    const int tpl = stage_reg_q(m.LX, xv) ? stage_reg_q(m.LX, xv) : m.px.tpl;
                     if (((3 * rpb * tpl + 31) & ~31) > lim) break;
                     if ((size_t)3 * rpb * padded_len(m.LX) * cs > 200 * 1024) break;
                     a.rpb = rpb;
@@ -778,7 +779,7 @@ int prepare_T(bm_ctx *c)
             const char *sr = getenv("BM_STAGE_ROWS");
             m.staged = (sr && sr[0] == '1') ? 1 : 0;
             const char *sx = getenv("BM_STAGE_XV");
-            m.xv = (sx && sx[0] == '1' && stage_reg_q(m.LX)) ? 1 : 0;
+            m.xv = (sx && sx[0] == '1' && stage_reg_q(m.LX, 1)) ? 1 : 0;
             const char *sy = getenv("BM_Y_XV");
             m.yv = (sy && sy[0] == '1' && ypass_has_st(m.Ny) && m.nz > 1 && ypass_st_threads(m.Ny, m.Wy) % 32 == 0) ? 1 : 0;
         } else if (c->autotune && !c->batched) autotune_mesh<T>(c, m);

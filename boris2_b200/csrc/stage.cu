@@ -577,10 +577,22 @@ template <int LX> struct xr_pq {
     static constexpr int Q = LX / P;
 };
 
+// Stockham shape: power-of-two L, 8 values per thread (radix 8, the last pass the remaining 2 or
+// 4); L = 3 * 2^k, 12 values per thread (radix 4, one radix 2 where the power of two is odd, then
+// the radix-3 pass last so that every earlier stride is a power of two)
+template <int L> struct xs_shape {
+    static constexpr int V = (L % 3 == 0) ? 12 : 8;
+    static constexpr int TPL = L / V;
+};
+template <int L, int NS> struct xs_radix {
+    static constexpr int M = L / NS;
+    static constexpr int v = (L % 3) ? (M >= 8 ? 8 : M) : ((M % 4 == 0 && M / 4 >= 3) ? 4 : (M % 2 == 0 && M / 2 >= 3) ? 2 : 3);
+};
+
 template <int LX, int XV> struct xr_cfg {
-    static constexpr int PAD = XV == 0 ? xr_pq<LX>::P : 16;      // one padding slot per PAD elements
-    static constexpr int TPL = XV == 0 ? xr_pq<LX>::Q : LX / 8;  // threads per line
-    static constexpr int LSP = LX + LX / PAD + 1;                // padded line length
+    static constexpr int PAD = XV == 0 ? xr_pq<LX>::P : 16;                // one padding slot per PAD elements
+    static constexpr int TPL = XV == 0 ? xr_pq<LX>::Q : xs_shape<LX>::TPL;  // threads per line
+    static constexpr int LSP = LX + LX / PAD + 1;                          // padded line length
 };
 
 template <typename T, int P, int Q, bool INV>
@@ -627,7 +639,7 @@ __device__ __forceinline__ void x_twolevel(cpx<T> *line, int t, bool act, const 
     __syncthreads();
 }
 
-// One Stockham pass of stride NS (radix R = min(8, L / NS)) and the passes after it. Butterfly j
+// One Stockham pass of stride NS (radix R from xs_radix) and the passes after it. Butterfly j
 // reads elements j + r * L / R, twiddles them by w_L^(r k L / (NS R)) (k = j mod NS), and writes
 // the R-point DFT to (j - k) R + k + r NS. ZHALF: the input is zero beyond L / 2 (only the first
 // pass reads it: there element j + r L / R >= L / 2 exactly when r >= R / 2). The last inverse
@@ -635,8 +647,8 @@ __device__ __forceinline__ void x_twolevel(cpx<T> *line, int t, bool act, const 
 template <typename T, int L, int NS, bool INV, bool ZHALF>
 __device__ __forceinline__ void x_stockham(cpx<T> *line, int t, bool act, const cpx<T> *__restrict__ tw, int nkeep)
 {
-    constexpr int TPL = L / 8;
-    constexpr int R = (L / NS) >= 8 ? 8 : L / NS;
+    constexpr int TPL = xs_shape<L>::TPL;
+    constexpr int R = xs_radix<L, NS>::v;
     constexpr int LR = L / R, BPT = LR / TPL, TWS = L / (NS * R);
     constexpr bool LAST = NS * R == L;
     addrP<16> A;
@@ -839,7 +851,9 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
         if (lb + rb <= 200 * 1024) smem = lb + rb;
         else b.staged = 0;
     }
-    auto kern = XV == 0 ? k_stage_reg<T, LX> : k_stage_rx<T, LX>;
+    void (*kern)(StageArgs<T>);
+    if constexpr (XV == 0) kern = k_stage_reg<T, LX>;
+    else kern = k_stage_rx<T, LX>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
@@ -861,6 +875,8 @@ int stage_reg_q(int LX, int xv)
     case 256: return xv ? 32 : 16;
     case 512: return xv ? 64 : 32;
     case 1024: return xv ? 128 : 32;
+    case 24: case 48: case 96: case 192: case 384: case 768:
+        return xv ? LX / 12 : 0;   // Stockham only
     default: return 0;
     }
 }
@@ -869,6 +885,7 @@ template <typename T, int LX> static int launch_stage_xv(const StageArgs<T> &a, 
 {
     return a.xv ? launch_stage_reg<T, LX, 1>(a, s) : launch_stage_reg<T, LX, 0>(a, s);
 }
+
 
 template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
 {
@@ -880,6 +897,12 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
     case 256: return launch_stage_xv<T, 256>(a, s);
     case 512: return launch_stage_xv<T, 512>(a, s);
     case 1024: return launch_stage_xv<T, 1024>(a, s);
+    case 24: if (a.xv) return launch_stage_reg<T, 24, 1>(a, s); break;
+    case 48: if (a.xv) return launch_stage_reg<T, 48, 1>(a, s); break;
+    case 96: if (a.xv) return launch_stage_reg<T, 96, 1>(a, s); break;
+    case 192: if (a.xv) return launch_stage_reg<T, 192, 1>(a, s); break;
+    case 384: if (a.xv) return launch_stage_reg<T, 384, 1>(a, s); break;
+    case 768: if (a.xv) return launch_stage_reg<T, 768, 1>(a, s); break;
     default: break;
     }
     int nt = (3 * a.rpb * a.px.tpl + 31) & ~31;   // whole warps
@@ -925,6 +948,12 @@ int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, in
     case 256: return launch_stage_rx_batch<T, 256>(dargs, dwork, nwork, nt, smem, s);
     case 512: return launch_stage_rx_batch<T, 512>(dargs, dwork, nwork, nt, smem, s);
     case 1024: return launch_stage_rx_batch<T, 1024>(dargs, dwork, nwork, nt, smem, s);
+    case 24: return launch_stage_rx_batch<T, 24>(dargs, dwork, nwork, nt, smem, s);
+    case 48: return launch_stage_rx_batch<T, 48>(dargs, dwork, nwork, nt, smem, s);
+    case 96: return launch_stage_rx_batch<T, 96>(dargs, dwork, nwork, nt, smem, s);
+    case 192: return launch_stage_rx_batch<T, 192>(dargs, dwork, nwork, nt, smem, s);
+    case 384: return launch_stage_rx_batch<T, 384>(dargs, dwork, nwork, nt, smem, s);
+    case 768: return launch_stage_rx_batch<T, 768>(dargs, dwork, nwork, nt, smem, s);
     default: return 213;
     }
     if (smem > 48 * 1024) {

@@ -55,8 +55,8 @@ def test_batched_rk4_matches_oracle(bm, prec, tol):
     err = max(np.abs(c.get_m(q) - s.get_m(q)).max() / d["Ms"] for q, d in enumerate(descs))
     # per RK stage: one 2D y pass; one launch per transform length with a register kernel plus one
     # for the other lengths: y forward and y inverse (Ny 48 generic, 32, 128), z pass (Nz 4, 8),
-    # stage (LX 24, 48, 96 generic, 32, 64) -> 1 + 3 + 2 + 3 + 3 launches
-    assert c.kernels_per_step() == 4 * 12
+    # stage (LX 24, 32, 48, 64, 96) -> 1 + 3 + 2 + 3 + 5 launches
+    assert c.kernels_per_step() == 4 * 14
     c.close()
     assert err < tol
 

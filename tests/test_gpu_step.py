@@ -193,11 +193,12 @@ def test_stage_kernel_variants(bm, staged, rows, xv, monkeypatch):
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
-@pytest.mark.parametrize("nx", [16, 32, 64, 128, 256, 512, 1024])
+@pytest.mark.parametrize("nx", [16, 32, 64, 128, 256, 512, 1024, 24, 48, 96, 192, 384, 768])
 def test_stage_xv_every_length(bm, nx, prec, tol, monkeypatch):
-    """The radix-8 Stockham x transform at every register length (radix tails 8x2, 8x4, 8x8,
-    8x8x2, 8x8x4, 8x8x8, 8x8x8x2; odd nx leaves a zero partner slot) against the oracle's RK4
-    trajectory with demag, exchange and Zeeman."""
+    """The Stockham x transform at every register length (power of two, radix 8 with tails 8x2,
+    8x4, 8x8, 8x8x2, 8x8x4, 8x8x8, 8x8x8x2; 3 * 2^k, radix 4 / 2 with a last radix-3 pass; odd nx
+    leaves a zero partner slot) against the oracle's RK4 trajectory with demag, exchange and
+    Zeeman."""
     monkeypatch.setenv("BM_TILES", "1,4,8,1")
     monkeypatch.setenv("BM_STAGE_XV", "1")
     for n in [(nx, 3, 2), (nx - 1, 2, 1)]:
