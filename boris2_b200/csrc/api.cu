@@ -1033,7 +1033,10 @@ int yz_multi(bm_ctx *c, int gate, int *count)
         if (!(m.modules & BM_DEMAG)) continue;
         YZArgs<T> a = yz_args<T>(c, m, gate);
         if (m.nz == 1) {
-            a.W = m.W2;
+            // batched launches take their parallelism from the many meshes: wide column tiles
+            int W = 16;
+            while (W > 1 && (W * m.py.tpl > lim || ymid2d_smem<T>(m.Ny, W) > 100 * 1024 || W > m.LX)) W /= 2;
+            a.W = W;
             v2.push_back(a);
             continue;
         }
