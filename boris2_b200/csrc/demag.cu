@@ -47,18 +47,18 @@ __device__ __forceinline__ void ymid2d_body(const YZArgs<T> &a, int bx)
     const int nt = blockDim.x, tid = threadIdx.x;
     const long long plane = (long long)ny * LX;   // one component (nz == 1)
     const long long nk = (long long)Kx1 * Ky1;
-    for (int idx = tid; idx < 3 * Ny * W; idx += nt) {
-        int w = idx % W, e = (idx / W) % Ny, c = idx / (W * Ny);
-        int kx = kx0 + w;
-        bool ok = (e < ny && kx < LX);
-        cp_async_cpx<T>(&sm[(c * Ny + e) * W + w], ok ? &a.S1[c * plane + (long long)e * LX + kx] : a.S1, ok);
-    }
-    for (int idx = tid; idx < 4 * Ky1 * W; idx += nt) {
-        int w = idx % W, ky = (idx / W) % Ky1, c = idx / (W * Ky1);
-        int kx = kx0 + w;
-        bool ok = kx < LX;
-        cp_async_real<T>(&Ks[(c * Ky1 + ky) * W + w], ok ? &a.K[c * nk + (long long)ky * Kx1 + kx] : a.K, ok);
-    }
+    // thread (column wq, row group g0): W is a power of two and divides the block size
+    const int lw = __ffs(W) - 1, wq = tid & (W - 1), g0 = tid >> lw, ng = nt >> lw;
+    const int kxq = kx0 + wq;
+    const bool okx = kxq < LX;
+    for (int c = 0; c < 3; c++)
+        for (int e = g0; e < Ny; e += ng) {
+            const bool ok = e < ny && okx;
+            cp_async_cpx<T>(&sm[(c * Ny + e) * W + wq], ok ? &a.S1[c * plane + (long long)e * LX + kxq] : a.S1, ok);
+        }
+    for (int c = 0; c < 4; c++)
+        for (int ky = g0; ky < Ky1; ky += ng)
+            cp_async_real<T>(&Ks[(c * Ky1 + ky) * W + wq], okx ? &a.K[c * nk + (long long)ky * Kx1 + kxq] : a.K, okx);
     if (kx0 == 0) {
         for (int idx = tid; idx < 4 * Ky1; idx += nt) {
             int ky = idx % Ky1, c = idx / Ky1;
@@ -68,15 +68,15 @@ __device__ __forceinline__ void ymid2d_body(const YZArgs<T> &a, int bx)
     cp_async_wait_all();
     __syncthreads();
     const int tpl = a.py.tpl;
-    const int l = tid % W, t = tid / W;
+    const int l = wq, t = g0;
     const bool act = t < tpl;
     // three explicit calls: a loop around fft_line defeats register allocation
     fft_line<T, false, false>(sm + 0 * Ny * W + l, W, t, act, a.py, a.twy);
     fft_line<T, false, false>(sm + 1 * Ny * W + l, W, t, act, a.py, a.twy);
     fft_line<T, false, false>(sm + 2 * Ny * W + l, W, t, act, a.py, a.twy);
     // product: Kxy odd in y (KernelMultiplication_2D_line, DemagKernel.cpp:42)
-    for (int idx = tid; idx < W * Ny; idx += nt) {
-        int w = idx % W, ky = idx / W, kx = kx0 + w;
+    for (int ky = g0; ky < Ny; ky += ng) {
+        const int w = wq, kx = kxq;
         if (kx >= LX) continue;
         if (kx == 0) {
             if (ky > Ny / 2) continue;
@@ -118,11 +118,9 @@ __device__ __forceinline__ void ymid2d_body(const YZArgs<T> &a, int bx)
     fft_line<T, false, true>(sm + 0 * Ny * W + l, W, t, act, a.py, a.twy);
     fft_line<T, false, true>(sm + 1 * Ny * W + l, W, t, act, a.py, a.twy);
     fft_line<T, false, true>(sm + 2 * Ny * W + l, W, t, act, a.py, a.twy);
-    for (int idx = tid; idx < 3 * ny * W; idx += nt) {
-        int w = idx % W, e = (idx / W) % ny, cc = idx / (W * ny);
-        int kx = kx0 + w;
-        if (kx < LX) a.S1[cc * plane + (long long)e * LX + kx] = sm[(cc * Ny + e) * W + w];
-    }
+    if (okx)
+        for (int cc = 0; cc < 3; cc++)
+            for (int e = g0; e < ny; e += ng) a.S1[cc * plane + (long long)e * LX + kxq] = sm[(cc * Ny + e) * W + wq];
 }
 
 template <typename T>
@@ -161,20 +159,20 @@ __device__ __forceinline__ void ypass3d_body(const YZArgs<T> &a, int bx, int z, 
         src = a.S2 + ((long long)c * nz + z) * Ny * LX; nin = Ny;
         dst = a.S1 + ((long long)c * nz + z) * ny * LX; nout = ny;
     }
-    for (int idx = tid; idx < Ny * W; idx += nt) {
-        int w = idx % W, e = idx / W, kx = kx0 + w;
-        bool ok = (e < nin && kx < LX);
-        cp_async_cpx<T>(&sm[e * W + w], ok ? &src[(long long)e * LX + kx] : src, ok);
+    // thread (column wq, row group g0): W is a power of two and divides the block size
+    const int lw = __ffs(W) - 1, wq = tid & (W - 1), g0 = tid >> lw, ng = nt >> lw;
+    const int kxq = kx0 + wq;
+    const bool okx = kxq < LX;
+    for (int e = g0; e < Ny; e += ng) {
+        const bool ok = e < nin && okx;
+        cp_async_cpx<T>(&sm[e * W + wq], ok ? &src[(long long)e * LX + kxq] : src, ok);
     }
     cp_async_wait_all();
     __syncthreads();
     const int tpl = a.py.tpl;
-    const int l = tid % W, t = tid / W;
-    fft_line<T, false, INV>(sm + l, W, t, t < tpl, a.py, a.twy);
-    for (int idx = tid; idx < nout * W; idx += nt) {
-        int w = idx % W, e = idx / W, kx = kx0 + w;
-        if (kx < LX) dst[(long long)e * LX + kx] = sm[e * W + w];
-    }
+    fft_line<T, false, INV>(sm + wq, W, g0, g0 < tpl, a.py, a.twy);
+    if (okx)
+        for (int e = g0; e < nout; e += ng) dst[(long long)e * LX + kxq] = sm[e * W + wq];
 }
 
 template <typename T, bool INV>
@@ -217,19 +215,21 @@ __device__ __forceinline__ void zmid_body(const YZArgs<T> &a, int bx, int ky)
     const long long nk = (long long)Kx1 * Ky1 * Kz1;
     auto S = [&](int c, int p, int e, int w) -> cpx<T> & { return sm[((c * 2 + p) * Nz + e) * W + w]; };
     const int np = single ? 1 : 2;
-    for (int idx = tid; idx < 3 * np * Nz * W; idx += nt) {
-        int w = idx % W, e = (idx / W) % Nz, cp = idx / (W * Nz);
-        int c = cp / np, p = cp % np;
-        int kyp = p ? kym : ky, kx = kx0 + w;
-        bool ok = (e < nz && kx < LX);
-        cp_async_cpx<T>(&S(c, p, e, w), ok ? &a.S2[(((long long)c * nz + e) * Ny + kyp) * LX + kx] : a.S2, ok);
-    }
-    for (int idx = tid; idx < 6 * Kz1 * W; idx += nt) {
-        int w = idx % W, kz = (idx / W) % Kz1, c = idx / (W * Kz1);
-        int kx = kx0 + w;
-        bool ok = kx < LX;
-        cp_async_real<T>(&Ks[(c * Kz1 + kz) * W + w], ok ? &a.K[c * nk + ((long long)kz * Ky1 + ky) * Kx1 + kx] : a.K, ok);
-    }
+    // thread (column wq, row group g0): W is a power of two and divides the block size
+    const int lw = __ffs(W) - 1, wq = tid & (W - 1), g0 = tid >> lw, ng = nt >> lw;
+    const int kxq = kx0 + wq;
+    const bool okx = kxq < LX;
+    for (int c = 0; c < 3; c++)
+        for (int p = 0; p < np; p++) {
+            const int kyp = p ? kym : ky;
+            for (int e = g0; e < Nz; e += ng) {
+                const bool ok = e < nz && okx;
+                cp_async_cpx<T>(&S(c, p, e, wq), ok ? &a.S2[(((long long)c * nz + e) * Ny + kyp) * LX + kxq] : a.S2, ok);
+            }
+        }
+    for (int c = 0; c < 6; c++)
+        for (int kz = g0; kz < Kz1; kz += ng)
+            cp_async_real<T>(&Ks[(c * Kz1 + kz) * W + wq], okx ? &a.K[c * nk + ((long long)kz * Ky1 + ky) * Kx1 + kxq] : a.K, okx);
     if (kx0 == 0) {
         for (int idx = tid; idx < 6 * Kz1; idx += nt) {
             int kz = idx % Kz1, c = idx / Kz1;
@@ -239,16 +239,16 @@ __device__ __forceinline__ void zmid_body(const YZArgs<T> &a, int bx, int ky)
     cp_async_wait_all();
     __syncthreads();
     const int tpl = a.pz.tpl;
-    const int gp = tid / (W * tpl), l = tid % W, t = (tid / W) % tpl;
+    const int gp = g0 / tpl, l = wq, t = g0 - gp * tpl;
     const bool act = gp < np;
     const int gq = act ? gp : 0;
     fft_line<T, false, false>(sm + ((0 * 2 + gq) * Nz) * W + l, W, t, act, a.pz, a.twz);
     fft_line<T, false, false>(sm + ((1 * 2 + gq) * Nz) * W + l, W, t, act, a.pz, a.twz);
     fft_line<T, false, false>(sm + ((2 * 2 + gq) * Nz) * W + l, W, t, act, a.pz, a.twz);
     // product with mirror signs (KernelMultiplication_3D_line, DemagKernel.cpp:85)
-    for (int idx = tid; idx < np * Nz * W; idx += nt) {
-        int w = idx % W, kz = (idx / W) % Nz, p = idx / (W * Nz);
-        int kx = kx0 + w;
+    for (int r = g0; r < np * Nz; r += ng) {
+        const int p = r >= Nz ? 1 : 0, kz = r - p * Nz;
+        const int w = wq, kx = kxq;
         if (kx >= LX) continue;
         int akz = kz <= Nz / 2 ? kz : Nz - kz;
         T sz = kz <= Nz / 2 ? (T)1 : (T)-1;
@@ -295,12 +295,12 @@ __device__ __forceinline__ void zmid_body(const YZArgs<T> &a, int bx, int ky)
     fft_line<T, false, true>(sm + ((0 * 2 + gq) * Nz) * W + l, W, t, act, a.pz, a.twz);
     fft_line<T, false, true>(sm + ((1 * 2 + gq) * Nz) * W + l, W, t, act, a.pz, a.twz);
     fft_line<T, false, true>(sm + ((2 * 2 + gq) * Nz) * W + l, W, t, act, a.pz, a.twz);
-    for (int idx = tid; idx < 3 * np * nz * W; idx += nt) {
-        int w = idx % W, e = (idx / W) % nz, cp = idx / (W * nz);
-        int c = cp / np, p = cp % np;
-        int kyp = p ? kym : ky, kx = kx0 + w;
-        if (kx < LX) a.S2[(((long long)c * nz + e) * Ny + kyp) * LX + kx] = S(c, p, e, w);
-    }
+    if (okx)
+        for (int c = 0; c < 3; c++)
+            for (int p = 0; p < np; p++) {
+                const int kyp = p ? kym : ky;
+                for (int e = g0; e < nz; e += ng) a.S2[(((long long)c * nz + e) * Ny + kyp) * LX + kxq] = S(c, p, e, wq);
+            }
 }
 
 template <typename T>

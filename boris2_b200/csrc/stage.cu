@@ -568,6 +568,11 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_batch(const StageArgs<T> 
 //         with a register cap (64 FP32, 128 FP64) so that more rows are resident per SM.
 // The packed-spectrum split (xinv_pre / xfwd_post) and the per-cell work stay in shared memory
 // in natural order.
+// register cap of the FP32 Stockham stage kernels (more resident rows per SM against spills)
+#ifndef BM_RX_MAXNREG_F
+#define BM_RX_MAXNREG_F 64
+#endif
+
 template <int P> struct addrP {
     __device__ __forceinline__ int operator()(int e) const { return e + e / P; }
 };
@@ -731,6 +736,33 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
         for (int m = t; m < LX; m += TPL) cp_async_cpx<T>(&line[A(m)], &src[m], true);
     }
     cp_async_commit();
+    // without staging: L2 prefetch of the rows the per-cell phase reads from DRAM (this row and the
+    // z + 1 row of M, the update base, the earlier stage evaluations, the material maps), so that
+    // they arrive while the inverse transform runs. Every prefetched address lies inside its row.
+    if (!a.staged && (a.mode != BM_MODE_UPDATE || a.Mbase != a.Min)) {
+        const int nx = a.nx, ny = a.ny, nz = a.nz;
+        const long long n = a.n;
+        const int lpr = (int)((nx * sizeof(T) + 127) / 128);   // 128-byte lines per row
+        const StageLayout L = stage_layout(a);
+        const int nzr = L.ns > 1 ? 3 : 0;                        // z + 1 rows of M
+        const int nev = (a.mode == BM_MODE_HEFF) ? 0 : a.nev;
+        const int o_mb = 3 + nzr, o_ev = o_mb + 3 * L.mb, o_ms = o_ev + 3 * nev, o_k1 = o_ms + L.ms;
+        const int nrow = o_k1 + L.k1;
+        for (int job = tid; job < rpb * nrow * lpr; job += blockDim.x) {
+            const int line_i = job % lpr, rk = job / lpr, r = rk / nrow, k = rk - r * nrow;
+            const int row = r0 + r;
+            if (row >= nrows) continue;
+            const long long ro = (long long)row * nx;
+            const T *src = nullptr;
+            if (k < 3) src = a.Min + k * n + ro;
+            else if (k < o_mb) src = (row / ny + 1 < nz) ? a.Min + (k - 3) * n + ro + (long long)ny * nx : nullptr;
+            else if (k < o_ev) src = a.Mbase + (k - o_mb) * n + ro;
+            else if (k < o_ms) src = a.ev[(k - o_ev) / 3] + ((k - o_ev) % 3) * n + ro;
+            else if (k < o_k1) src = a.Ms_map + ro;
+            else src = a.K1_map + ro;
+            if (src) asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(src) + 128 * line_i));
+        }
+    }
     // group 2: the per-cell input rows, arriving while the inverse transform runs
     AccStaged<T> st;
     if (a.staged) {
@@ -818,7 +850,7 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_reg(StageArgs<T> a)
 }
 
 template <typename T, int LX>
-__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : 64) k_stage_rx(StageArgs<T> a)
+__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx(StageArgs<T> a)
 {
     if (stage_gated_out<T>(a.st, a.gate)) return;
     stage_reg_body<T, LX, 1>(a, blockIdx.x, gridDim.x);
@@ -827,7 +859,7 @@ __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : 64) k_stage_rx(StageArgs<T> a
 // many meshes with the same x length in one launch (radix-8 transform): work item (mesh, row
 // block); the error-norm maximum and the step bookkeeping follow k_stage_batch
 template <typename T, int LX>
-__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : 64) k_stage_rx_batch(const StageArgs<T> *__restrict__ args,
+__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx_batch(const StageArgs<T> *__restrict__ args,
                                                                          const int2 *__restrict__ work, int nwork)
 {
     if (stage_gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
