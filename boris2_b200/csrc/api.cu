@@ -272,7 +272,7 @@ void choose_tiles(Mesh &m)
     {
         int W = 8;
         if (ypass_has_reg(m.Ny))
-            while (W > 1 && ((size_t)m.Ny * W * cs > 100 * 1024 || ypass_reg_threads(m.Ny, W) > lim)) W /= 2;
+            while (W > 1 && ((size_t)m.Ny * W * cs > 100 * 1024 || ypass_reg_threads(m.Ny, W) > yreg_maxt<T>::v)) W /= 2;
         else
             while (W > 1 && ((size_t)m.Ny * W * cs > 100 * 1024 || W * m.py.tpl > lim)) W /= 2;
         if (W > m.LX) W = pow2_floor(m.LX);
@@ -455,7 +455,7 @@ void tune_ypass(bm_ctx *c, Mesh &m)
             if (yv) {
                 const int nt = ypass_st_threads(m.Ny, W);
                 if (nt > lim || nt % 32) continue;
-            } else if (ypass_has_reg(m.Ny) ? ypass_reg_threads(m.Ny, W) > lim : W * m.py.tpl > lim) {
+            } else if (ypass_has_reg(m.Ny) ? ypass_reg_threads(m.Ny, W) > yreg_maxt<T>::v : W * m.py.tpl > lim) {
                 continue;
             }
             a.W = W;
@@ -1044,7 +1044,8 @@ int yz_multi(bm_ctx *c, int gate, int *count)
         batch_tiles<T>(m, Wy, Wz);
         if (ypass_has_reg(m.Ny)) {
             int W = 16;
-            while (W > 1 && (ypass_reg_threads(m.Ny, W) > lim || (size_t)m.Ny * W * sizeof(cpx<T>) > 64 * 1024 || W > m.LX)) W /= 2;
+            while (W > 1 && (ypass_reg_threads(m.Ny, W) > std::min(lim, yreg_maxt<T>::v) || (size_t)m.Ny * W * sizeof(cpx<T>) > 64 * 1024 ||
+                             W > m.LX)) W /= 2;
             a.W = W;
             gy[m.Ny].push_back(a);
         } else {

@@ -562,7 +562,7 @@ __device__ __forceinline__ void ypass_reg_body(const YZArgs<T> &a, int bx, int z
 }
 
 template <typename T, int P, int Q, bool INV>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass_reg(YZArgs<T> a)
+__global__ void __launch_bounds__(yreg_maxt<T>::v) k_ypass_reg(YZArgs<T> a)
 {
     if (gated_out<T>(a.st, a.gate)) return;
     ypass_reg_body<T, P, Q, INV>(a, blockIdx.x, blockIdx.y, blockIdx.z);
@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_ypass_reg(YZArgs<T> a)
 // many meshes with the same Ny in one launch: work item (mesh, column tile + W-columns count *
 // (z + nz * component))
 template <typename T, int P, int Q, bool INV>
-__global__ void __launch_bounds__(bm_lb<T>::v) k_ypass_reg_batch(const YZArgs<T> *__restrict__ args,
+__global__ void __launch_bounds__(yreg_maxt<T>::v) k_ypass_reg_batch(const YZArgs<T> *__restrict__ args,
                                                                     const int2 *__restrict__ work, int nwork)
 {
     if (gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
@@ -593,7 +593,7 @@ static int launch_ypass_reg(const YZArgs<T> &a, cudaStream_t s)
 {
     constexpr int P = ysplit<L>::p, Q = ysplit<L>::q;
     int nt = a.W * (P > Q ? P : Q);
-    if (nt > bm_lb<T>::v) return 106;
+    if (nt > yreg_maxt<T>::v) return 106;
     if (nt < 32) nt = 32;
     size_t smem = (size_t)L * a.W * sizeof(cpx<T>);
     if (smem > 200 * 1024) return 107;

@@ -55,6 +55,9 @@ template <typename T> size_t zmid_reg_smem(int Nz, int W)
 }
 bool zmid_has_reg(int Nz);
 bool ypass_has_reg(int Ny);
+// block-size ceiling of the two-level register y kernel: FP64 lines of 32 values need the registers
+// a 256-thread bound allows
+template <typename T> struct yreg_maxt { static constexpr int v = sizeof(T) == 8 ? 256 : bm_lb<T>::v; };
 bool ypass_has_st(int Ny);            // lengths with the radix-16 Stockham y transform
 int ypass_st_threads(int Ny, int W);
 int ypass_reg_threads(int Ny, int W);
