@@ -331,12 +331,14 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_batch(const YZArgs<T> *__r
 // the transforms. The kernel tile arrives by cp.async while the forward transforms run (thread
 // row j < 6 copies kernel component j for every kz). Thread (c, p, w): w fastest so global loads
 // and stores coalesce.
-template <typename T, int NZ>
+// WC: the tile width as a compile-time constant (0: a.W at run time), so that every shared-memory
+// address of the product becomes a base plus an immediate offset
+template <typename T, int NZ, int WC>
 __device__ __forceinline__ void zmid_reg_body(const YZArgs<T> &a, int bx, int ky)
 {
     extern __shared__ unsigned char smraw[];
-    const int W = a.W, Ny = a.Ny, nz = a.nz, LX = a.LX;
-    const int lw = __ffs(W) - 1;
+    const int W = WC ? WC : a.W, Ny = a.Ny, nz = a.nz, LX = a.LX;
+    const int lw = WC ? (WC == 32 ? 5 : WC == 16 ? 4 : WC == 8 ? 3 : WC == 4 ? 2 : WC == 2 ? 1 : 0) : __ffs(W) - 1;
     constexpr int KZ1 = NZ / 2 + 1;
     const int Kx1 = LX + 1, Ky1 = Ny / 2 + 1;
     cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
@@ -449,11 +451,11 @@ __device__ __forceinline__ void zmid_reg_body(const YZArgs<T> &a, int bx, int ky
         if (e < nz) a.S2[gbase + e * gstride] = v[e];
 }
 
-template <typename T, int NZ>
+template <typename T, int NZ, int WC>
 __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
 {
     if (gated_out<T>(a.st, a.gate)) return;
-    zmid_reg_body<T, NZ>(a, blockIdx.x, blockIdx.y);
+    zmid_reg_body<T, NZ, WC>(a, blockIdx.x, blockIdx.y);
 }
 
 // many meshes with the same Nz in one launch: work item (mesh, column tile + W-columns count * ky)
@@ -465,23 +467,29 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg_batch(const YZArgs<T> 
     const int2 it = work[blockIdx.x];
     const YZArgs<T> &a = args[it.x];
     const int nbx = (a.LX + a.W - 1) / a.W;
-    zmid_reg_body<T, NZ>(a, it.y % nbx, it.y / nbx);
+    zmid_reg_body<T, NZ, 0>(a, it.y % nbx, it.y / nbx);
 }
 
-template <typename T, int NZ>
-static int launch_zmid_reg(const YZArgs<T> &a, cudaStream_t s)
+template <typename T, int NZ, int WC>
+static int launch_zmid_reg_w(const YZArgs<T> &a, cudaStream_t s)
 {
     int nt = (6 * a.W + 31) & ~31;
     if (nt > bm_lb<T>::v) return 104;
     size_t smem = zmid_reg_smem<T>(NZ, a.W);
     if (smem > 200 * 1024) return 105;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_zmid_reg<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        cudaError_t e = cudaFuncSetAttribute(k_zmid_reg<T, NZ, WC>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     dim3 grid((a.LX + a.W - 1) / a.W, a.Ny / 2 + 1);
-    k_zmid_reg<T, NZ><<<grid, nt, smem, s>>>(a);
+    k_zmid_reg<T, NZ, WC><<<grid, nt, smem, s>>>(a);
     return (int)cudaGetLastError();
+}
+
+template <typename T, int NZ>
+static int launch_zmid_reg(const YZArgs<T> &a, cudaStream_t s)
+{
+    return a.W == 16 ? launch_zmid_reg_w<T, NZ, 16>(a, s) : launch_zmid_reg_w<T, NZ, 0>(a, s);
 }
 
 // lengths with a register z pass

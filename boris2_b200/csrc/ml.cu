@@ -120,14 +120,16 @@ template <int NZ> struct zml_bounds {
     static constexpr int blocks = NZ <= 16 ? 2 : 1;
 };
 
-template <typename T, int NZ>
+// WC: the tile width as a compile-time constant (0: a.W at run time), so that the shared-memory
+// addresses of the products become a base plus an immediate offset
+template <typename T, int NZ, int WC>
 __global__ void __launch_bounds__(bm_lb<T>::v, zml_bounds<NZ>::blocks) k_zmid_ml(MLZArgs<T> a)
 {
     if (ml_gated_out<T>(a.st, a.gate)) return;
     extern __shared__ __align__(16) unsigned char smraw[];
     constexpr int KZ1 = NZ / 2 + 1;
-    const int W = a.W, L = a.L, Ny = a.Ny, nz = a.nz, LX = a.LX;
-    const int lw = __ffs(W) - 1;
+    const int W = WC ? WC : a.W, L = a.L, Ny = a.Ny, nz = a.nz, LX = a.LX;
+    const int lw = WC ? (WC == 32 ? 5 : WC == 16 ? 4 : WC == 8 ? 3 : WC == 4 ? 2 : WC == 2 ? 1 : 0) : __ffs(W) - 1;
     const int Kx1 = LX + 1, Ky1 = Ny / 2 + 1;
     cpx<T> *In = reinterpret_cast<cpx<T> *>(smraw);
     unsigned char *Ks = smraw + (size_t)L * 6 * NZ * W * sizeof(cpx<T>);
@@ -309,20 +311,26 @@ __global__ void __launch_bounds__(bm_lb<T>::v, zml_bounds<NZ>::blocks) k_zmid_ml
     }
 }
 
-template <typename T, int NZ>
-static int launch_zmid_ml_t(const MLZArgs<T> &a, cudaStream_t s)
+template <typename T, int NZ, int WC>
+static int launch_zmid_ml_w(const MLZArgs<T> &a, cudaStream_t s)
 {
     int nt = (6 * a.L * a.W + 31) & ~31;
     if (nt > bm_lb<T>::v) return 304;
     size_t smem = zmid_ml_smem<T>(a.L, NZ, a.W, a.ksm);
     if (smem > 200 * 1024) return 305;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_zmid_ml<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        cudaError_t e = cudaFuncSetAttribute(k_zmid_ml<T, NZ, WC>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
     dim3 grid((a.LX + a.W - 1) / a.W, a.Ny / 2 + 1);
-    k_zmid_ml<T, NZ><<<grid, nt, smem, s>>>(a);
+    k_zmid_ml<T, NZ, WC><<<grid, nt, smem, s>>>(a);
     return (int)cudaGetLastError();
+}
+
+template <typename T, int NZ>
+static int launch_zmid_ml_t(const MLZArgs<T> &a, cudaStream_t s)
+{
+    return a.W == 16 ? launch_zmid_ml_w<T, NZ, 16>(a, s) : launch_zmid_ml_w<T, NZ, 0>(a, s);
 }
 
 bool zmid_ml_supported(int Nz)
