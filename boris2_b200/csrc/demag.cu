@@ -477,7 +477,7 @@ static int launch_zmid_reg_w(const YZArgs<T> &a, cudaStream_t s)
     if (nt > bm_lb<T>::v) return 104;
     size_t smem = zmid_reg_smem<T>(NZ, a.W);
     if (smem > 200 * 1024) return 105;
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(k_zmid_reg<T, NZ, WC>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
@@ -605,7 +605,7 @@ static int launch_ypass_reg(const YZArgs<T> &a, cudaStream_t s)
     if (nt < 32) nt = 32;
     size_t smem = (size_t)L * a.W * sizeof(cpx<T>);
     if (smem > 200 * 1024) return 107;
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(k_ypass_reg<T, P, Q, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
@@ -741,7 +741,7 @@ static int launch_ypass_st(const YZArgs<T> &a, cudaStream_t s)
     if (nt % 32) return 108;
     size_t smem = ypass_st_smem<T>(L, a.W);
     if (smem > 200 * 1024) return 109;
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(k_ypass_st<T, L, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
@@ -769,7 +769,7 @@ static int launch_common(KF kern, dim3 grid, int nt, size_t smem, cudaStream_t s
 {
     if (nt > 1024 || nt < 1) return 101;
     if (smem > 227 * 1024) return 102;
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }

@@ -14,6 +14,9 @@
 // launch against the last value set, so it is always set to this one ceiling (no launch here uses
 // more; the B200 limit per block is 227 KB).
 #define BM_SMEM_CAP (200 * 1024)
+// dynamic shared memory above which a launch opens its kernel to BM_SMEM_CAP: the 48 KB default
+// covers static plus dynamic shared memory, so the threshold leaves room for the static part
+#define BM_SMEM_DEFAULT_SAFE (40 * 1024)
 #include "common.cuh"
 
 #define BM_FFT_MAXPASS 8

@@ -318,7 +318,7 @@ static int launch_zmid_ml_w(const MLZArgs<T> &a, cudaStream_t s)
     if (nt > bm_lb<T>::v) return 304;
     size_t smem = zmid_ml_smem<T>(a.L, NZ, a.W, a.ksm);
     if (smem > 200 * 1024) return 305;
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(k_zmid_ml<T, NZ, WC>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }

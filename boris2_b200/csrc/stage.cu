@@ -886,9 +886,9 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
     void (*kern)(StageArgs<T>);
     if constexpr (XV == 0) kern = k_stage_reg<T, LX>;
     else kern = k_stage_rx<T, LX>;
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
-        if (e != cudaSuccess) return (int)e;
+        if (e != cudaSuccess) return 2000 + (int)e;   // the shared-memory ceiling was refused
     }
     int nrows = a.ny * a.nz;
     dim3 grid((nrows + a.rpb - 1) / a.rpb);
@@ -941,7 +941,7 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
     if (nt > bm_lb<T>::v) return 201;
     size_t smem = (size_t)3 * a.rpb * padded_len(a.LX) * sizeof(cpx<T>);
     if (smem > 200 * 1024) return 202;
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(k_stage<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
@@ -957,7 +957,7 @@ template int launch_stage<double>(const StageArgs<double> &, cudaStream_t);
 template <typename T, int LX>
 static int launch_stage_rx_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
 {
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(k_stage_rx_batch<T, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
@@ -988,7 +988,7 @@ int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, in
     case 768: return launch_stage_rx_batch<T, 768>(dargs, dwork, nwork, nt, smem, s);
     default: return 213;
     }
-    if (smem > 48 * 1024) {
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(k_stage_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }

@@ -210,10 +210,10 @@ int launch_fft_strided(cpx<T> *data, const FFTPlan &P, const cpx<T> *tw, long lo
     if (nt > bm_lb<T>::v) return 1;
     dim3 grid((ninner + W - 1) / W, nouter);
     if (inv) {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(k_fft_strided<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        if (smem > BM_SMEM_DEFAULT_SAFE) cudaFuncSetAttribute(k_fft_strided<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         k_fft_strided<T, true><<<grid, nt, smem, s>>>(data, P, tw, es, ls, ninner, W, os);
     } else {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(k_fft_strided<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        if (smem > BM_SMEM_DEFAULT_SAFE) cudaFuncSetAttribute(k_fft_strided<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         k_fft_strided<T, false><<<grid, nt, smem, s>>>(data, P, tw, es, ls, ninner, W, os);
     }
     return (int)cudaGetLastError();
