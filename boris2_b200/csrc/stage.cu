@@ -832,11 +832,24 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
         }
         __syncthreads();
         x_reg<T, LX, XV, false>(line, t, qact, a.twx, LX);
-        xfwd_post_f<T>(line, LX, a.twx2, t, TPL, qact, A);
+        // split into the packed half spectrum pairwise (k, LX - k) straight into the S1 row
+        // (xfwd_post)
         if (qact) {
             cpx<T> *dst = a.S1 + ((long long)qc * nrows + r0 + qr) * LX;
-#pragma unroll 4
-            for (int mm = t; mm < LX; mm += TPL) dst[mm] = line[A(mm)];
+            for (int k = t; k <= LX / 2; k += TPL) {
+                if (k == 0) {
+                    const cpx<T> z0 = line[A(0)];
+                    dst[0] = mk<T>(z0.x + z0.y, z0.x - z0.y);
+                    continue;
+                }
+                const int k2 = LX - k;
+                const cpx<T> Av = line[A(k)], Bc = conj(line[A(k2)]);
+                const cpx<T> E = cscale(Av + Bc, (T)0.5);
+                const cpx<T> O = cscale(mul_mi(Av - Bc), (T)0.5);
+                const cpx<T> wO = cmul(a.twx2[k], O);
+                dst[k] = E + wO;
+                if (k2 != k) dst[k2] = conj(E - wO);
+            }
         }
     }
     stage_tail<T>(a, lmax, total);
