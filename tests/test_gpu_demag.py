@@ -88,6 +88,10 @@ DEMAG_CASES = [
     ((300, 3, 2), (2e-9, 2e-9, 1e-9)),      # LX = 384 (generic x kernel)
     ((512, 4, 1), (2e-9, 2e-9, 1e-9)),      # LX = 512
     ((1000, 2, 1), (2e-9, 2e-9, 1e-9)),     # LX = 1024
+    ((1100, 2, 1), (2e-9, 2e-9, 1e-9)),     # LX = 1536 (beyond the register x kernels: generic)
+    ((2000, 1, 1), (2e-9, 2e-9, 1e-9)),     # LX = 2048 (generic)
+    ((4, 1024, 2), (2e-9, 2e-9, 2e-9)),     # Ny = 2048 (radix-16 Stockham or generic y passes)
+    ((4, 3, 64), (2e-9, 2e-9, 2e-9)),       # Nz = 128 (generic z pass)
 ]
 
 
