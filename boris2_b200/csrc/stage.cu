@@ -221,8 +221,12 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         double tm = a.st ? *((volatile double *)&a.st->stagetime) : 0.0;
         int hi = 0;
         if (a.nHa > 1 && a.Ha_tspan > 0.0) {
-            hi = (int)floor(tm / a.Ha_tspan * a.nHa);
-            hi = hi < 0 ? 0 : (hi >= a.nHa ? a.nHa - 1 : hi);
+            // one FP64 division per warp, broadcast (every launch runs whole warps)
+            if ((threadIdx.x & 31) == 0) {
+                hi = (int)floor(tm / a.Ha_tspan * a.nHa);
+                hi = hi < 0 ? 0 : (hi >= a.nHa ? a.nHa - 1 : hi);
+            }
+            hi = __shfl_sync(0xffffffffu, hi, 0);
         }
         Ha[0] = (T)a.Ha[3 * hi]; Ha[1] = (T)a.Ha[3 * hi + 1]; Ha[2] = (T)a.Ha[3 * hi + 2];
     }
@@ -236,8 +240,11 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
     const T crhs = (T)(a.crhs * dT);
     const int cstride = 2 * rpb * LSP;   // T elements between the component lines of one row
     // (r, x) of cell index ci = r * nx + x, advanced by nt per iteration without divisions
-    const int dr = nt / nx, dx = nt - dr * nx;
-    int r = tid / nx, x = tid - r * nx;
+    int dr = 0, dx = nt, r = 0, x = tid;   // a block no wider than a row: no divisions
+    if (nt > nx) {
+        dr = nt / nx; dx = nt - dr * nx;
+        r = tid / nx; x = tid - r * nx;
+    }
     int yrow = -1, y = 0, z = 0;
     for (; r < rpb; x += dx, r += dr) {
         if (x >= nx) { x -= nx; r++; if (r >= rpb) break; }
@@ -724,7 +731,7 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
     const int r0 = bid * rpb;
     const int tid = threadIdx.x;
     const int q = tid / TPL, t = tid % TPL;
-    const int qc = q / rpb, qr = q % rpb;
+    const int qc = rpb == 1 ? q : q / rpb, qr = q - qc * rpb;
     const bool qact = (q < 3 * rpb) && (r0 + qr < nrows);
     cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
     const bool demag = (a.mode != BM_MODE_UPDATE) && (a.modules & BM_MOD_DEMAG);
@@ -748,14 +755,17 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
         const int nev = (a.mode == BM_MODE_HEFF) ? 0 : a.nev;
         const int o_mb = 3 + nzr, o_ev = o_mb + 3 * L.mb, o_ms = o_ev + 3 * nev, o_k1 = o_ms + L.ms;
         const int nrow = o_k1 + L.k1;
-        for (int job = tid; job < rpb * nrow * lpr; job += blockDim.x) {
-            const int line_i = job % lpr, rk = job / lpr, r = rk / nrow, k = rk - r * nrow;
+        const int lsh = 32 - __clz(lpr - 1), lpr2 = 1 << lsh;   // lines per row rounded up to a power of two
+        for (int job = tid; job < rpb * nrow * lpr2; job += blockDim.x) {
+            const int line_i = job & (lpr2 - 1), rk = job >> lsh;
+            if (line_i >= lpr) continue;
+            const int r = rpb == 1 ? 0 : rk / nrow, k = rk - r * nrow;
             const int row = r0 + r;
             if (row >= nrows) continue;
             const long long ro = (long long)row * nx;
             const T *src = nullptr;
             if (k < 3) src = a.Min + k * n + ro;
-            else if (k < o_mb) src = (row / ny + 1 < nz) ? a.Min + (k - 3) * n + ro + (long long)ny * nx : nullptr;
+            else if (k < o_mb) src = (row + ny < nrows) ? a.Min + (k - 3) * n + ro + (long long)ny * nx : nullptr;
             else if (k < o_ev) src = a.Mbase + (k - o_mb) * n + ro;
             else if (k < o_ms) src = a.ev[(k - o_ev) / 3] + ((k - o_ev) % 3) * n + ro;
             else if (k < o_k1) src = a.Ms_map + ro;
