@@ -982,6 +982,9 @@ int yz_batch_one(bm_ctx *c, int kind, int key, std::vector<YZArgs<T>> &v, int *c
                 items = nbx * a.nz * 3;
                 nt = std::max(nt, (ypass_reg_threads(a.Ny, a.W) + 31) & ~31);
                 smem = std::max(smem, (size_t)a.Ny * a.W * sizeof(cpx<T>));
+            } else if (kind == BM_BATCH_YMID2D_REG) {
+                nt = std::max(nt, (ymid2d_reg_threads(a.Ny, a.W) + 31) & ~31);
+                smem = std::max(smem, ymid2d_smem<T>(a.Ny, a.W));
             } else if (kind == BM_BATCH_ZMID_REG) {
                 items = nbx * (a.Ny / 2 + 1);
                 nt = std::max(nt, (6 * a.W + 31) & ~31);
@@ -1027,17 +1030,22 @@ template <typename T>
 int yz_multi(bm_ctx *c, int gate, int *count)
 {
     const int lim = 256;
-    std::vector<YZArgs<T>> v2;
-    std::map<int, std::vector<YZArgs<T>>> gy, gz;   // key Ny / Nz with a register kernel, or 0
+    std::map<int, std::vector<YZArgs<T>>> g2, gy, gz;   // key Ny / Nz with a register kernel, or 0
     for (auto &m : c->meshes) {
         if (!(m.modules & BM_DEMAG)) continue;
         YZArgs<T> a = yz_args<T>(c, m, gate);
         if (m.nz == 1) {
             // batched launches take their parallelism from the many meshes: wide column tiles
             int W = 16;
-            while (W > 1 && (W * m.py.tpl > lim || ymid2d_smem<T>(m.Ny, W) > 100 * 1024 || W > m.LX)) W /= 2;
-            a.W = W;
-            v2.push_back(a);
+            if (ypass_has_reg(m.Ny)) {
+                while (W > 1 && (ymid2d_reg_threads(m.Ny, W) > 384 || ymid2d_smem<T>(m.Ny, W) > 100 * 1024 || W > m.LX)) W /= 2;
+                a.W = W;
+                g2[m.Ny].push_back(a);
+            } else {
+                while (W > 1 && (W * m.py.tpl > lim || ymid2d_smem<T>(m.Ny, W) > 100 * 1024 || W > m.LX)) W /= 2;
+                a.W = W;
+                g2[0].push_back(a);
+            }
             continue;
         }
         int Wy, Wz;
@@ -1063,7 +1071,8 @@ int yz_multi(bm_ctx *c, int gate, int *count)
         }
     }
     int rc;
-    if ((rc = yz_batch_one<T>(c, BM_BATCH_YMID2D, 0, v2, count))) return rc;
+    for (auto &kv : g2)
+        if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_YMID2D_REG : BM_BATCH_YMID2D, kv.first, kv.second, count))) return rc;
     for (auto &kv : gy)
         if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_YFWD_REG : BM_BATCH_YFWD, kv.first, kv.second, count))) return rc;
     for (auto &kv : gz)

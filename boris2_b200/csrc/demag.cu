@@ -614,6 +614,179 @@ static int launch_ypass_reg(const YZArgs<T> &a, cudaStream_t s)
     return (int)cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------ 2D y pass, two-level register FFT
+// Ny = P * Q (as k_ypass_reg). Block: W columns x 3 components x R = max(P, Q) threads, w fastest.
+// Forward: stage 1 reads the S1 rows straight from global memory (rows >= ny are zeros, those >=
+// Ny / 2 fold away), one shared transpose, stage 2 leaves the spectrum in the shared tile
+// [3][Ny][W] in natural order. The 2D kernel product runs on the tile exactly as in the generic
+// kernel (KernelMultiplication_2D_line, DemagKernel.cpp:42). Inverse: stage 1 from the tile, one
+// shared transpose, stage 2 writes rows < ny to S1.
+// stage 1 of the two-level y transform on values already in registers: DFT_Q of x[n1 + P n2],
+// twiddle, and the transposed store u[k2][n1] into this component's tile column (col = tile + w)
+template <typename T, int P, int Q, bool INV>
+__device__ __forceinline__ void y2d_stage1(const YZArgs<T> &a, cpx<T> *col, cpx<T> (&v)[Q], int n1, int W)
+{
+    RegFFT<T, Q, INV>::run(v, a.twy, P);
+#pragma unroll
+    for (int k2 = 0; k2 < Q; k2++) {
+        cpx<T> t = v[k2];
+        if (k2 > 0 && n1 > 0) {
+            cpx<T> tw = a.twy[n1 * k2];
+            if (INV) tw.y = -tw.y;
+            t = cmul(t, tw);
+        }
+        col[(k2 * P + n1) * W] = t;
+    }
+}
+
+template <typename T, int P, int Q>
+__device__ __forceinline__ void ymid2d_reg_body(const YZArgs<T> &a, int bx)
+{
+    extern __shared__ unsigned char smraw[];
+    constexpr int Ny = P * Q, R = P > Q ? P : Q, Ky1 = Ny / 2 + 1;
+    const int W = a.W, ny = a.ny, LX = a.LX;
+    const int Kx1 = LX + 1;
+    const int lw = __ffs(W) - 1;
+    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
+    T *Ks = reinterpret_cast<T *>(sm + 3 * Ny * W);
+    T *Kn = Ks + 4 * Ky1 * W;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int kx0 = bx * W;
+    const int w = tid & (W - 1), g = tid >> lw, ng = nt >> lw;
+    const int r = g % R, c = g / R;   // line component and row thread
+    const int kx = kx0 + w;
+    const bool colok = kx < LX;
+    const long long plane = (long long)ny * LX;
+    const long long nk = (long long)Kx1 * Ky1;
+    // kernel tiles (async)
+    for (int cc = 0; cc < 4; cc++)
+        for (int ky = g; ky < Ky1; ky += ng)
+            cp_async_real<T>(&Ks[(cc * Ky1 + ky) * W + w], colok ? &a.K[cc * nk + (long long)ky * Kx1 + kx] : a.K, colok);
+    if (kx0 == 0)
+        for (int i = tid; i < 4 * Ky1; i += nt) {
+            const int ky = i % Ky1, cc = i / Ky1;
+            cp_async_real<T>(&Kn[cc * Ky1 + ky], &a.K[cc * nk + (long long)ky * Kx1 + LX], true);
+        }
+    cp_async_commit();
+    cpx<T> *col = sm + (c < 3 ? c : 0) * Ny * W + w;
+    const bool line = c < 3;
+    // forward stage 1 from the S1 rows (rows >= ny read as zeros; n2 >= Q / 2 are rows >= Ny / 2)
+    if (line && r < P) {
+        const cpx<T> *src = a.S1 + c * plane + kx;
+        cpx<T> v[Q];
+#pragma unroll
+        for (int n2 = 0; n2 < Q; n2++) {
+            const int e = r + P * n2;
+            v[n2] = (n2 < Q / 2 && colok && e < ny) ? src[(long long)e * LX] : mk<T>(0, 0);
+        }
+        y2d_stage1<T, P, Q, false>(a, col, v, r, W);
+    }
+    __syncthreads();
+    {
+        cpx<T> u[P];
+        if (line && r < Q) {
+#pragma unroll
+            for (int n1 = 0; n1 < P; n1++) u[n1] = col[(r * P + n1) * W];
+            RegFFT<T, P, false>::run(u, a.twy, Q);
+        }
+        __syncthreads();
+        if (line && r < Q) {
+#pragma unroll
+            for (int k1 = 0; k1 < P; k1++) col[(r + Q * k1) * W] = u[k1];
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // product: Kxy odd in y (KernelMultiplication_2D_line, DemagKernel.cpp:42)
+    for (int ky = g; ky < Ny; ky += ng) {
+        if (kx >= LX) continue;
+        if (kx == 0) {
+            if (ky > Ny / 2) continue;
+            const int kym = (Ny - ky) % Ny;
+            cpx<T> A[3], B[3];
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) {
+                const cpx<T> C = sm[(cc * Ny + ky) * W + w], cj = conj(sm[(cc * Ny + kym) * W + w]);
+                A[cc] = cscale(C + cj, (T)0.5);
+                B[cc] = cscale(mul_mi(C - cj), (T)0.5);
+            }
+            T k0[6] = {Ks[(0 * Ky1 + ky) * W + w], Ks[(1 * Ky1 + ky) * W + w], Ks[(2 * Ky1 + ky) * W + w],
+                       Ks[(3 * Ky1 + ky) * W + w], (T)0, (T)0};
+            T kn[6] = {Kn[0 * Ky1 + ky], Kn[1 * Ky1 + ky], Kn[2 * Ky1 + ky], Kn[3 * Ky1 + ky], (T)0, (T)0};
+            cpx<T> Ap[3], Bp[3];
+            kapply<T>(k0, A, Ap);
+            kapply<T>(kn, B, Bp);
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) {
+                sm[(cc * Ny + ky) * W + w] = Ap[cc] + mul_i(Bp[cc]);
+                if (kym != ky) sm[(cc * Ny + kym) * W + w] = conj(Ap[cc]) + mul_i(conj(Bp[cc]));
+            }
+        } else {
+            const int aky = ky <= Ny / 2 ? ky : Ny - ky;
+            const T sy = ky <= Ny / 2 ? (T)1 : (T)-1;
+            T k[6] = {Ks[(0 * Ky1 + aky) * W + w], Ks[(1 * Ky1 + aky) * W + w], Ks[(2 * Ky1 + aky) * W + w],
+                      sy * Ks[(3 * Ky1 + aky) * W + w], (T)0, (T)0};
+            cpx<T> m[3], h[3];
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) m[cc] = sm[(cc * Ny + ky) * W + w];
+            kapply<T>(k, m, h);
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) sm[(cc * Ny + ky) * W + w] = h[cc];
+        }
+    }
+    __syncthreads();
+    // inverse stage 1: every thread reads its tile values, then the tile is rewritten
+    {
+        cpx<T> v[Q];
+        if (line && r < P) {
+#pragma unroll
+            for (int n2 = 0; n2 < Q; n2++) v[n2] = col[(r + P * n2) * W];
+        }
+        __syncthreads();
+        if (line && r < P) y2d_stage1<T, P, Q, true>(a, col, v, r, W);
+    }
+    __syncthreads();
+    if (line && r < Q) {
+        cpx<T> u[P];
+#pragma unroll
+        for (int n1 = 0; n1 < P; n1++) u[n1] = col[(r * P + n1) * W];
+        RegFFT<T, P, true>::run(u, a.twy, Q);
+        if (colok) {
+            cpx<T> *dst = a.S1 + c * plane + kx;
+#pragma unroll
+            for (int k1 = 0; k1 < P / 2; k1++) {
+                const int e = r + Q * k1;
+                if (e < ny) dst[(long long)e * LX] = u[k1];
+            }
+        }
+    }
+}
+
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ymid2d_reg(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    ymid2d_reg_body<T, P, Q>(a, blockIdx.x);
+}
+
+// many meshes with the same Ny in one launch: work item (mesh, column tile)
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_ymid2d_reg_batch(const YZArgs<T> *__restrict__ args,
+                                                                     const int2 *__restrict__ work, int nwork)
+{
+    if (gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    ymid2d_reg_body<T, P, Q>(args[it.x], it.y);
+}
+
+template <typename T> size_t ymid2d_reg_smem(int Ny, int W) { return ymid2d_smem<T>(Ny, W); }
+int ymid2d_reg_threads(int Ny, int W)
+{
+    int q = (Ny >= 1024) ? 32 : (Ny >= 256) ? 16 : (Ny >= 64) ? 8 : (Ny >= 16) ? 4 : 2;
+    int p = Ny / q;
+    return 3 * W * (p > q ? p : q);
+}
+
 bool ypass_has_reg(int Ny)
 {
     return Ny == 8 || Ny == 16 || Ny == 32 || Ny == 64 || Ny == 128 || Ny == 256 || Ny == 512 || Ny == 1024;
@@ -776,8 +949,46 @@ static int launch_common(KF kern, dim3 grid, int nt, size_t smem, cudaStream_t s
     return 0;
 }
 
+template <typename T, int L>
+static int launch_ymid2d_reg(const YZArgs<T> &a, cudaStream_t s)
+{
+    constexpr int P = ysplit<L>::p, Q = ysplit<L>::q;
+    int nt = (ymid2d_reg_threads(L, a.W) + 31) & ~31;
+    if (nt > bm_lb<T>::v) return 112;
+    size_t smem = ymid2d_smem<T>(L, a.W);
+    if (smem > 200 * 1024) return 113;
+    dim3 grid((a.LX + a.W - 1) / a.W);
+    int rc = launch_common(k_ymid2d_reg<T, P, Q>, grid, nt, smem, s);
+    if (rc) return rc;
+    k_ymid2d_reg<T, P, Q><<<grid, nt, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+// the register 2D y pass for this tile width, or -1 when it does not apply
+template <typename T>
+static int launch_ymid2d_reg_dispatch(const YZArgs<T> &a, cudaStream_t s)
+{
+    if ((a.W & (a.W - 1)) != 0 || !ypass_has_reg(a.Ny)) return -1;
+    if (((ymid2d_reg_threads(a.Ny, a.W) + 31) & ~31) > bm_lb<T>::v || ymid2d_smem<T>(a.Ny, a.W) > 200 * 1024) return -1;
+    switch (a.Ny) {
+    case 8: return launch_ymid2d_reg<T, 8>(a, s);
+    case 16: return launch_ymid2d_reg<T, 16>(a, s);
+    case 32: return launch_ymid2d_reg<T, 32>(a, s);
+    case 64: return launch_ymid2d_reg<T, 64>(a, s);
+    case 128: return launch_ymid2d_reg<T, 128>(a, s);
+    case 256: return launch_ymid2d_reg<T, 256>(a, s);
+    case 512: return launch_ymid2d_reg<T, 512>(a, s);
+    case 1024: return launch_ymid2d_reg<T, 1024>(a, s);
+    default: return -1;
+    }
+}
+
 template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s)
 {
+    {
+        int rc = launch_ymid2d_reg_dispatch<T>(a, s);
+        if (rc >= 0) return rc;
+    }
     int nt = a.W * a.py.tpl;
     if (nt < 32) nt = 32;
     if (nt > bm_lb<T>::v) return 103;
@@ -890,6 +1101,16 @@ static int launch_zmid_reg_batch(const YZArgs<T> *dargs, const int2 *dwork, int 
     return (int)cudaGetLastError();
 }
 
+template <typename T, int L>
+static int launch_ymid2d_reg_batch(const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+{
+    constexpr int P = ysplit<L>::p, Q = ysplit<L>::q;
+    int grid = 1, rc = launch_batch_common(k_ymid2d_reg_batch<T, P, Q>, nwork, nt, smem, &grid);
+    if (rc) return rc;
+    k_ymid2d_reg_batch<T, P, Q><<<grid, nt, smem, s>>>(dargs, dwork, nwork);
+    return (int)cudaGetLastError();
+}
+
 template <typename T, int L, bool INV>
 static int launch_ypass_reg_batch(const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
 {
@@ -951,6 +1172,18 @@ int launch_yz_batch(int kind, int key, const YZArgs<T> *dargs, const int2 *dwork
         case 32: return launch_zmid_reg_batch<T, 32>(dargs, dwork, nwork, nt, smem, s);
         case 48: return launch_zmid_reg_batch<T, 48>(dargs, dwork, nwork, nt, smem, s);
         case 64: return launch_zmid_reg_batch<T, 64>(dargs, dwork, nwork, nt, smem, s);
+        default: return 111;
+        }
+    case BM_BATCH_YMID2D_REG:
+        switch (key) {
+        case 8: return launch_ymid2d_reg_batch<T, 8>(dargs, dwork, nwork, nt, smem, s);
+        case 16: return launch_ymid2d_reg_batch<T, 16>(dargs, dwork, nwork, nt, smem, s);
+        case 32: return launch_ymid2d_reg_batch<T, 32>(dargs, dwork, nwork, nt, smem, s);
+        case 64: return launch_ymid2d_reg_batch<T, 64>(dargs, dwork, nwork, nt, smem, s);
+        case 128: return launch_ymid2d_reg_batch<T, 128>(dargs, dwork, nwork, nt, smem, s);
+        case 256: return launch_ymid2d_reg_batch<T, 256>(dargs, dwork, nwork, nt, smem, s);
+        case 512: return launch_ymid2d_reg_batch<T, 512>(dargs, dwork, nwork, nt, smem, s);
+        case 1024: return launch_ymid2d_reg_batch<T, 1024>(dargs, dwork, nwork, nt, smem, s);
         default: return 111;
         }
     case BM_BATCH_YFWD_REG: return ypass_reg_batch_dispatch<T, false>(key, dargs, dwork, nwork, nt, smem, s);

@@ -60,6 +60,7 @@ bool ypass_has_reg(int Ny);
 template <typename T> struct yreg_maxt { static constexpr int v = sizeof(T) == 8 ? 256 : bm_lb<T>::v; };
 bool ypass_has_st(int Ny);            // lengths with the radix-16 Stockham y transform
 int ypass_st_threads(int Ny, int W);
+int ymid2d_reg_threads(int Ny, int W);   // block size of the register 2D y pass
 int ypass_reg_threads(int Ny, int W);
 template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s);
@@ -167,6 +168,7 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s);
 #define BM_BATCH_ZMID_REG 5   // key Nz
 #define BM_BATCH_YFWD_REG 6   // key Ny
 #define BM_BATCH_YINV_REG 7   // key Ny
+#define BM_BATCH_YMID2D_REG 8 // key Ny
 template <typename T>
 int launch_yz_batch(int kind, int key, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem,
                     cudaStream_t s);

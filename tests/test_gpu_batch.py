@@ -53,10 +53,10 @@ def test_batched_rk4_matches_oracle(bm, prec, tol):
     st = c.run(20)
     assert st["accepted"] == 20
     err = max(np.abs(c.get_m(q) - s.get_m(q)).max() / d["Ms"] for q, d in enumerate(descs))
-    # per RK stage: one 2D y pass; one launch per transform length with a register kernel plus one
-    # for the other lengths: y forward and y inverse (Ny 48 generic, 32, 128), z pass (Nz 4, 8),
-    # stage (LX 24, 32, 48, 64, 96) -> 1 + 3 + 2 + 3 + 5 launches
-    assert c.kernels_per_step() == 4 * 14
+    # per RK stage: one launch per transform length with a register kernel plus one for the other
+    # lengths: 2D y pass (Ny 64; 192 and 48 generic), y forward and y inverse (Ny 48 generic, 32,
+    # 128), z pass (Nz 4, 8), stage (LX 24, 32, 48, 64, 96) -> 2 + 3 + 2 + 3 + 5 launches
+    assert c.kernels_per_step() == 4 * 15
     c.close()
     assert err < tol
 

@@ -239,3 +239,24 @@ def test_ypass_stockham_every_length(bm, ny, W, prec, tol, monkeypatch):
         c.close()
         assert t["ypass_yv"] == 1 and t["ypass_W"] == W
         assert np.abs(m - s.get_m()).max() / 8e5 < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+@pytest.mark.parametrize("ny,W", [(4, 8), (8, 8), (16, 8), (32, 4), (64, 4), (128, 4), (256, 4), (512, 2)])
+def test_ymid2d_register_every_length(bm, ny, W, prec, tol, monkeypatch):
+    """The two-level register 2D y pass (forward, fused 2D kernel product, inverse) at every
+    register length Ny = 8 .. 1024, with a power-of-two ny and one that leaves zero rows, against
+    the oracle's RK4 trajectory with demag, exchange and Zeeman."""
+    monkeypatch.setenv("BM_TILES", "%d,4,8,1" % W)
+    for n in [(12, ny, 1), (9, max(ny - 1, 1), 1)]:
+        N = n[0] * n[1] * n[2]
+        mesh = dict(n=n, h=(3e-9, 3e-9, 2e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(2e3, 1e3, 0))
+        M = sphere_random(N, seed=ny + 3, Ms=8e5)
+        s = OracleSolver([mesh], evaluation=0, dt=2e-14)
+        s.set_m(M)
+        s.run(10)
+        c = _make(bm, prec, mesh, M, "RK4", 2e-14)
+        c.run(10)
+        m = c.get_m()
+        c.close()
+        assert np.abs(m - s.get_m()).max() / 8e5 < tol
