@@ -978,7 +978,11 @@ int yz_batch_one(bm_ctx *c, int kind, int key, std::vector<YZArgs<T>> &v, int *c
             const YZArgs<T> &a = v[i];
             const int nbx = (a.LX + a.W - 1) / a.W;
             int items = nbx;
-            if (kind == BM_BATCH_YFWD_REG || kind == BM_BATCH_YINV_REG) {
+            if (kind == BM_BATCH_YFWD_ST || kind == BM_BATCH_YINV_ST) {
+                items = nbx * a.nz * 3;
+                nt = std::max(nt, (ypass_st_threads(a.Ny, a.W) + 31) & ~31);
+                smem = std::max(smem, ((size_t)a.Ny * a.W + (size_t)(a.Ny / 16) * 8) * sizeof(cpx<T>));
+            } else if (kind == BM_BATCH_YFWD_REG || kind == BM_BATCH_YINV_REG) {
                 items = nbx * a.nz * 3;
                 nt = std::max(nt, (ypass_reg_threads(a.Ny, a.W) + 31) & ~31);
                 smem = std::max(smem, (size_t)a.Ny * a.W * sizeof(cpx<T>));
@@ -1056,6 +1060,12 @@ int yz_multi(bm_ctx *c, int gate, int *count)
                              W > m.LX)) W /= 2;
             a.W = W;
             gy[m.Ny].push_back(a);
+        } else if (ypass_has_st(m.Ny)) {
+            // Stockham (3 * 2^k lengths), keyed negative to keep it apart from the register groups
+            int W = 16;
+            while (W > 2 && (ypass_st_threads(m.Ny, W) > lim || (size_t)m.Ny * W * sizeof(cpx<T>) > 64 * 1024 || W > m.LX)) W /= 2;
+            a.W = W;
+            gy[-m.Ny].push_back(a);
         } else {
             a.W = Wy;
             gy[0].push_back(a);
@@ -1073,12 +1083,16 @@ int yz_multi(bm_ctx *c, int gate, int *count)
     int rc;
     for (auto &kv : g2)
         if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_YMID2D_REG : BM_BATCH_YMID2D, kv.first, kv.second, count))) return rc;
+    auto ykind = [](int key, bool inv) {
+        return key > 0 ? (inv ? BM_BATCH_YINV_REG : BM_BATCH_YFWD_REG) : key < 0 ? (inv ? BM_BATCH_YINV_ST : BM_BATCH_YFWD_ST)
+                                                                            : (inv ? BM_BATCH_YINV : BM_BATCH_YFWD);
+    };
     for (auto &kv : gy)
-        if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_YFWD_REG : BM_BATCH_YFWD, kv.first, kv.second, count))) return rc;
+        if ((rc = yz_batch_one<T>(c, ykind(kv.first, false), kv.first < 0 ? -kv.first : kv.first, kv.second, count))) return rc;
     for (auto &kv : gz)
         if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_ZMID_REG : BM_BATCH_ZMID, kv.first, kv.second, count))) return rc;
     for (auto &kv : gy)
-        if ((rc = yz_batch_one<T>(c, kv.first ? BM_BATCH_YINV_REG : BM_BATCH_YINV, kv.first, kv.second, count))) return rc;
+        if ((rc = yz_batch_one<T>(c, ykind(kv.first, true), kv.first < 0 ? -kv.first : kv.first, kv.second, count))) return rc;
     return 0;
 }
 

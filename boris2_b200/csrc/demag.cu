@@ -825,28 +825,42 @@ static int launch_ypass_dispatch(const YZArgs<T> &a, cudaStream_t s)
 // of the first pass and the unit-stride accesses of the others are both conflict-free.
 __device__ __forceinline__ int ysk(int e, int w, int W) { return e * W + w + ((e >> 4) << 3); }
 
+// Stockham shape of the y transform: power-of-two Ny, 16 values per thread (radix 16, then the rest);
+// Ny = 3 * 2^k, 12 values per thread (radix 4, one radix 2 where the power of two is odd, radix 3 last)
+template <int L> struct ys_shape {
+    static constexpr int V = (L % 3 == 0) ? 12 : 16;
+    static constexpr int TPL = L / V;
+};
+template <int L, int NS> struct ys_radix {
+    static constexpr int M = L / NS;
+    static constexpr int v = (L % 3) ? (M >= 16 ? 16 : M) : ((M % 4 == 0 && M / 4 >= 3) ? 4 : (M % 2 == 0 && M / 2 >= 3) ? 2 : 3);
+};
+
 template <typename T, int L, int NS, bool INV>
 __device__ __forceinline__ void ypass_st_pass(cpx<T> *tile, const cpx<T> *src, cpx<T> *dst, int ld, int ny, int t, int w,
-                                              int W, bool colok, const cpx<T> *__restrict__ tw)
+                                              int W, bool colok, bool act, const cpx<T> *__restrict__ tw)
 {
-    constexpr int TPL = L / 16;
-    constexpr int R = (L / NS) >= 16 ? 16 : L / NS;
+    constexpr int TPL = ys_shape<L>::TPL;
+    constexpr int R = ys_radix<L, NS>::v;
     constexpr int LR = L / R, BPT = LR / TPL, TWS = L / (NS * R);
     constexpr bool FIRST = NS == 1, LAST = NS * R == L;
     cpx<T> v[BPT][R];
+    if (act) {
 #pragma unroll
-    for (int b = 0; b < BPT; b++)
+        for (int b = 0; b < BPT; b++)
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int e = t + b * TPL + r * LR;
-            if (FIRST) {
-                if (!INV) v[b][r] = (2 * r < R && colok && e < ny) ? src[(long long)e * ld] : mk<T>(0, 0);
-                else v[b][r] = colok ? src[(long long)e * ld] : mk<T>(0, 0);
-            } else {
-                v[b][r] = tile[ysk(e, w, W)];
+            for (int r = 0; r < R; r++) {
+                const int e = t + b * TPL + r * LR;
+                if (FIRST) {
+                    if (!INV) v[b][r] = (2 * r < R && colok && e < ny) ? src[(long long)e * ld] : mk<T>(0, 0);
+                    else v[b][r] = colok ? src[(long long)e * ld] : mk<T>(0, 0);
+                } else {
+                    v[b][r] = tile[ysk(e, w, W)];
+                }
             }
-        }
+    }
     if (!FIRST && !LAST) __syncthreads();   // every load of this pass before any store into the tile
+    if (act)
 #pragma unroll
     for (int b = 0; b < BPT; b++) {
         const int j = t + b * TPL;
@@ -873,21 +887,21 @@ __device__ __forceinline__ void ypass_st_pass(cpx<T> *tile, const cpx<T> *src, c
     }
     if constexpr (!LAST) {
         __syncthreads();
-        ypass_st_pass<T, L, NS * R, INV>(tile, src, dst, ld, ny, t, w, W, colok, tw);
+        ypass_st_pass<T, L, NS * R, INV>(tile, src, dst, ld, ny, t, w, W, colok, act, tw);
     }
 }
 
 template <typename T, int L, bool INV>
-__global__ void __launch_bounds__(bm_lb<T>::v, sizeof(T) == 4 ? 2 : 1) k_ypass_st(YZArgs<T> a)
+__device__ __forceinline__ void ypass_st_body(const YZArgs<T> &a, int bx, int z, int c)
 {
-    if (gated_out<T>(a.st, a.gate)) return;
     extern __shared__ unsigned char smraw[];
     cpx<T> *tile = reinterpret_cast<cpx<T> *>(smraw);
     const int W = a.W, ny = a.ny, LX = a.LX, nz = a.nz;
     const int lw = __ffs(W) - 1;
-    const int kx0 = blockIdx.x * W, z = blockIdx.y, c = blockIdx.z;
+    const int kx0 = bx * W;
     const int tid = threadIdx.x;
     const int w = tid & (W - 1), t = tid >> lw;
+    const bool act = t < ys_shape<L>::TPL;
     const int kx = kx0 + w;
     const bool colok = kx < LX;
     const cpx<T> *src;
@@ -899,17 +913,41 @@ __global__ void __launch_bounds__(bm_lb<T>::v, sizeof(T) == 4 ? 2 : 1) k_ypass_s
         src = a.S2 + ((long long)c * nz + z) * L * LX + (colok ? kx : 0);
         dst = a.S1 + ((long long)c * nz + z) * ny * LX + kx;
     }
-    ypass_st_pass<T, L, 1, INV>(tile, src, dst, LX, ny, t, w, W, colok, a.twy);
+    ypass_st_pass<T, L, 1, INV>(tile, src, dst, LX, ny, t, w, W, colok, act, a.twy);
 }
 
-bool ypass_has_st(int Ny) { return Ny == 256 || Ny == 512 || Ny == 1024 || Ny == 2048; }
-int ypass_st_threads(int Ny, int W) { return W * (Ny / 16); }
+template <typename T, int L, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v, sizeof(T) == 4 ? 2 : 1) k_ypass_st(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    ypass_st_body<T, L, INV>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// many meshes with the same Ny in one launch: work item (mesh, column tile + W-columns count *
+// (z + nz * component))
+template <typename T, int L, bool INV>
+__global__ void __launch_bounds__(bm_lb<T>::v, sizeof(T) == 4 ? 2 : 1) k_ypass_st_batch(const YZArgs<T> *__restrict__ args,
+                                                                                       const int2 *__restrict__ work, int nwork)
+{
+    if (gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    const YZArgs<T> &a = args[it.x];
+    const int nbx = (a.LX + a.W - 1) / a.W;
+    const int bx = it.y % nbx, r = it.y / nbx;
+    ypass_st_body<T, L, INV>(a, bx, r % a.nz, r / a.nz);
+}
+
+bool ypass_has_st(int Ny)
+{
+    return Ny == 256 || Ny == 512 || Ny == 1024 || Ny == 2048 || Ny == 192 || Ny == 384 || Ny == 768 || Ny == 1536;
+}
+int ypass_st_threads(int Ny, int W) { return W * (Ny / (Ny % 3 ? 16 : 12)); }
 template <typename T> size_t ypass_st_smem(int Ny, int W) { return ((size_t)Ny * W + (size_t)(Ny / 16) * 8) * sizeof(cpx<T>); }
 
 template <typename T, int L, bool INV>
 static int launch_ypass_st(const YZArgs<T> &a, cudaStream_t s)
 {
-    int nt = a.W * (L / 16);
+    int nt = a.W * ys_shape<L>::TPL;
     if (nt > bm_lb<T>::v) return 108;
     if (nt % 32) return 108;
     size_t smem = ypass_st_smem<T>(L, a.W);
@@ -932,7 +970,39 @@ static int launch_ypass_st_dispatch(const YZArgs<T> &a, cudaStream_t s)
     case 512: return launch_ypass_st<T, 512, INV>(a, s);
     case 1024: return launch_ypass_st<T, 1024, INV>(a, s);
     case 2048: return launch_ypass_st<T, 2048, INV>(a, s);
+    case 192: return launch_ypass_st<T, 192, INV>(a, s);
+    case 384: return launch_ypass_st<T, 384, INV>(a, s);
+    case 768: return launch_ypass_st<T, 768, INV>(a, s);
+    case 1536: return launch_ypass_st<T, 1536, INV>(a, s);
     default: return -1;
+    }
+}
+
+template <typename T, int L, bool INV>
+static int launch_ypass_st_batch(const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+{
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
+        cudaError_t e = cudaFuncSetAttribute(k_ypass_st_batch<T, L, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        if (e != cudaSuccess) return 2000 + (int)e;
+    }
+    k_ypass_st_batch<T, L, INV><<<nwork, nt, smem, s>>>(dargs, dwork, nwork);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, bool INV>
+static int ypass_st_batch_dispatch(int Ny, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem,
+                                   cudaStream_t s)
+{
+    switch (Ny) {
+    case 256: return launch_ypass_st_batch<T, 256, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 512: return launch_ypass_st_batch<T, 512, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 1024: return launch_ypass_st_batch<T, 1024, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 2048: return launch_ypass_st_batch<T, 2048, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 192: return launch_ypass_st_batch<T, 192, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 384: return launch_ypass_st_batch<T, 384, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 768: return launch_ypass_st_batch<T, 768, INV>(dargs, dwork, nwork, nt, smem, s);
+    case 1536: return launch_ypass_st_batch<T, 1536, INV>(dargs, dwork, nwork, nt, smem, s);
+    default: return 111;
     }
 }
 
@@ -1186,6 +1256,8 @@ int launch_yz_batch(int kind, int key, const YZArgs<T> *dargs, const int2 *dwork
         case 1024: return launch_ymid2d_reg_batch<T, 1024>(dargs, dwork, nwork, nt, smem, s);
         default: return 111;
         }
+    case BM_BATCH_YFWD_ST: return ypass_st_batch_dispatch<T, false>(key, dargs, dwork, nwork, nt, smem, s);
+    case BM_BATCH_YINV_ST: return ypass_st_batch_dispatch<T, true>(key, dargs, dwork, nwork, nt, smem, s);
     case BM_BATCH_YFWD_REG: return ypass_reg_batch_dispatch<T, false>(key, dargs, dwork, nwork, nt, smem, s);
     case BM_BATCH_YINV_REG: return ypass_reg_batch_dispatch<T, true>(key, dargs, dwork, nwork, nt, smem, s);
     default: return 110;

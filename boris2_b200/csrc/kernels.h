@@ -58,7 +58,7 @@ bool ypass_has_reg(int Ny);
 // block-size ceiling of the two-level register y kernel: FP64 lines of 32 values need the registers
 // a 256-thread bound allows
 template <typename T> struct yreg_maxt { static constexpr int v = sizeof(T) == 8 ? 256 : bm_lb<T>::v; };
-bool ypass_has_st(int Ny);            // lengths with the radix-16 Stockham y transform
+bool ypass_has_st(int Ny);            // lengths with the Stockham y transform (radix 16, or radix 4/2/3 for 3 * 2^k)
 int ypass_st_threads(int Ny, int W);
 int ymid2d_reg_threads(int Ny, int W);   // block size of the register 2D y pass
 int ypass_reg_threads(int Ny, int W);
@@ -169,6 +169,8 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s);
 #define BM_BATCH_YFWD_REG 6   // key Ny
 #define BM_BATCH_YINV_REG 7   // key Ny
 #define BM_BATCH_YMID2D_REG 8 // key Ny
+#define BM_BATCH_YFWD_ST 9    // key Ny (Stockham y transform)
+#define BM_BATCH_YINV_ST 10   // key Ny
 template <typename T>
 int launch_yz_batch(int kind, int key, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem,
                     cudaStream_t s);

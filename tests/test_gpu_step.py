@@ -218,11 +218,12 @@ def test_stage_xv_every_length(bm, nx, prec, tol, monkeypatch):
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
-@pytest.mark.parametrize("ny,W", [(128, 4), (256, 4), (512, 4), (1024, 2)])
+@pytest.mark.parametrize("ny,W", [(128, 4), (256, 4), (512, 4), (1024, 2), (96, 2), (192, 1), (384, 1), (768, 1)])
 def test_ypass_stockham_every_length(bm, ny, W, prec, tol, monkeypatch):
-    """The radix-16 Stockham y transform (3D, Ny = 256 .. 2048: radix tails 16x16, 16x16x2,
-    16x16x4, 16x16x8) against the oracle's RK4 trajectory with demag, exchange and Zeeman, for a
-    power-of-two ny and one that leaves zero rows below Ny / 2."""
+    """The Stockham y transform (3D; Ny = 256 .. 2048 with radix 16 and tails 16x16, 16x16x2,
+    16x16x4, 16x16x8; Ny = 192 .. 1536 with radix 4 / 2 and a last radix-3 pass) against the
+    oracle's RK4 trajectory with demag, exchange and Zeeman, for a ny that fills Ny / 2 and one that
+    leaves zero rows below Ny / 2."""
     monkeypatch.setenv("BM_TILES", "1,%d,8,1" % W)
     monkeypatch.setenv("BM_Y_XV", "1")
     for n in [(8, ny, 2), (6, ny - 3, 3)]:
