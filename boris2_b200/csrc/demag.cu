@@ -489,7 +489,12 @@ static int launch_zmid_reg_w(const YZArgs<T> &a, cudaStream_t s)
 template <typename T, int NZ>
 static int launch_zmid_reg(const YZArgs<T> &a, cudaStream_t s)
 {
-    return a.W == 16 ? launch_zmid_reg_w<T, NZ, 16>(a, s) : launch_zmid_reg_w<T, NZ, 0>(a, s);
+    switch (a.W) {
+    case 8: return launch_zmid_reg_w<T, NZ, 8>(a, s);
+    case 16: return launch_zmid_reg_w<T, NZ, 16>(a, s);
+    case 32: return launch_zmid_reg_w<T, NZ, 32>(a, s);
+    default: return launch_zmid_reg_w<T, NZ, 0>(a, s);
+    }
 }
 
 // lengths with a register z pass
