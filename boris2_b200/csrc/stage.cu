@@ -592,19 +592,21 @@ template <int LX> struct xr_pq {
 // Stockham shape: power-of-two L, 8 values per thread (radix 8, the last pass the remaining 2 or
 // 4); L = 3 * 2^k, 12 values per thread (radix 4, one radix 2 where the power of two is odd, then
 // the radix-3 pass last so that every earlier stride is a power of two)
-template <int L> struct xs_shape {
-    static constexpr int V = (L % 3 == 0) ? 12 : 8;
+// (VW = 16: the radix-16 variant of the power-of-two shape, 16 values per thread and half the
+// threads per line, so each thread carries twice the cells of the per-cell phase)
+template <int L, int VW = 8> struct xs_shape {
+    static constexpr int V = (L % 3 == 0) ? 12 : VW;
     static constexpr int TPL = L / V;
 };
-template <int L, int NS> struct xs_radix {
+template <int L, int NS, int VW = 8> struct xs_radix {
     static constexpr int M = L / NS;
-    static constexpr int v = (L % 3) ? (M >= 8 ? 8 : M) : ((M % 4 == 0 && M / 4 >= 3) ? 4 : (M % 2 == 0 && M / 2 >= 3) ? 2 : 3);
+    static constexpr int v = (L % 3) ? (M >= VW ? VW : M) : ((M % 4 == 0 && M / 4 >= 3) ? 4 : (M % 2 == 0 && M / 2 >= 3) ? 2 : 3);
 };
 
 template <int LX, int XV> struct xr_cfg {
-    static constexpr int PAD = XV == 0 ? xr_pq<LX>::P : 16;                // one padding slot per PAD elements
-    static constexpr int TPL = XV == 0 ? xr_pq<LX>::Q : xs_shape<LX>::TPL;  // threads per line
-    static constexpr int LSP = LX + LX / PAD + 1;                          // padded line length
+    static constexpr int PAD = XV == 0 ? xr_pq<LX>::P : 16;   // one padding slot per PAD elements
+    static constexpr int TPL = XV == 0 ? xr_pq<LX>::Q : xs_shape<LX, XV == 2 ? 16 : 8>::TPL;   // threads per line
+    static constexpr int LSP = LX + LX / PAD + 1;             // padded line length
 };
 
 template <typename T, int P, int Q, bool INV>
@@ -656,11 +658,11 @@ __device__ __forceinline__ void x_twolevel(cpx<T> *line, int t, bool act, const 
 // the R-point DFT to (j - k) R + k + r NS. ZHALF: the input is zero beyond L / 2 (only the first
 // pass reads it: there element j + r L / R >= L / 2 exactly when r >= R / 2). The last inverse
 // pass stores only elements below nkeep.
-template <typename T, int L, int NS, bool INV, bool ZHALF>
+template <typename T, int L, int NS, bool INV, bool ZHALF, int VW = 8>
 __device__ __forceinline__ void x_stockham(cpx<T> *line, int t, bool act, const cpx<T> *__restrict__ tw, int nkeep)
 {
-    constexpr int TPL = xs_shape<L>::TPL;
-    constexpr int R = xs_radix<L, NS>::v;
+    constexpr int TPL = xs_shape<L, VW>::TPL;
+    constexpr int R = xs_radix<L, NS, VW>::v;
     constexpr int LR = L / R, BPT = LR / TPL, TWS = L / (NS * R);
     constexpr bool LAST = NS * R == L;
     addrP<16> A;
@@ -708,14 +710,15 @@ __device__ __forceinline__ void x_stockham(cpx<T> *line, int t, bool act, const 
         }
     }
     __syncthreads();
-    if constexpr (!LAST) x_stockham<T, L, NS * R, INV, false>(line, t, act, tw, nkeep);
+    if constexpr (!LAST) x_stockham<T, L, NS * R, INV, false, VW>(line, t, act, tw, nkeep);
 }
 
 template <typename T, int LX, int XV, bool INV>
 __device__ __forceinline__ void x_reg(cpx<T> *line, int t, bool act, const cpx<T> *__restrict__ tw, int nkeep)
 {
     if constexpr (XV == 0) x_twolevel<T, xr_pq<LX>::P, xr_pq<LX>::Q, INV>(line, t, act, tw, nkeep);
-    else x_stockham<T, LX, 1, INV, !INV>(line, t, act, tw, nkeep);
+    else if constexpr (XV == 1) x_stockham<T, LX, 1, INV, !INV>(line, t, act, tw, nkeep);
+    else x_stockham<T, LX, 1, INV, !INV, 16>(line, t, act, tw, nkeep);
 }
 
 template <typename T, int LX, int XV>
@@ -879,6 +882,13 @@ __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx(S
     stage_reg_body<T, LX, 1>(a, blockIdx.x, gridDim.x);
 }
 
+template <typename T, int LX>
+__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx16(StageArgs<T> a)
+{
+    if (stage_gated_out<T>(a.st, a.gate)) return;
+    stage_reg_body<T, LX, 2>(a, blockIdx.x, gridDim.x);
+}
+
 // many meshes with the same x length in one launch (radix-8 transform): work item (mesh, row
 // block); the error-norm maximum and the step bookkeeping follow k_stage_batch
 template <typename T, int LX>
@@ -908,7 +918,8 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
     }
     void (*kern)(StageArgs<T>);
     if constexpr (XV == 0) kern = k_stage_reg<T, LX>;
-    else kern = k_stage_rx<T, LX>;
+    else if constexpr (XV == 1) kern = k_stage_rx<T, LX>;
+    else kern = k_stage_rx16<T, LX>;
     if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return 2000 + (int)e;   // the shared-memory ceiling was refused
@@ -923,21 +934,24 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
 int stage_reg_q(int LX, int xv)
 {
     switch (LX) {
-    case 16: return xv ? 2 : 4;
-    case 32: return xv ? 4 : 8;
-    case 64: return 8;
-    case 128: return 16;
-    case 256: return xv ? 32 : 16;
-    case 512: return xv ? 64 : 32;
-    case 1024: return xv ? 128 : 32;
+    case 16: return xv == 2 ? 0 : xv ? 2 : 4;
+    case 32: return xv == 2 ? 0 : xv ? 4 : 8;
+    case 64: return xv == 2 ? 0 : 8;
+    case 128: return xv == 2 ? 0 : 16;
+    case 256: return xv == 2 ? 16 : xv ? 32 : 16;
+    case 512: return xv == 2 ? 32 : xv ? 64 : 32;
+    case 1024: return xv == 2 ? 64 : xv ? 128 : 32;
     case 24: case 48: case 96: case 192: case 384: case 768:
-        return xv ? LX / 12 : 0;   // Stockham only
+        return xv == 1 ? LX / 12 : 0;   // Stockham only
     default: return 0;
     }
 }
 
 template <typename T, int LX> static int launch_stage_xv(const StageArgs<T> &a, cudaStream_t s)
 {
+    if constexpr (LX >= 256) {
+        if (a.xv == 2) return launch_stage_reg<T, LX, 2>(a, s);
+    }
     return a.xv ? launch_stage_reg<T, LX, 1>(a, s) : launch_stage_reg<T, LX, 0>(a, s);
 }
 

@@ -261,3 +261,33 @@ def test_ymid2d_register_every_length(bm, ny, W, prec, tol, monkeypatch):
         m = c.get_m()
         c.close()
         assert np.abs(m - s.get_m()).max() / 8e5 < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+@pytest.mark.parametrize("nx", [256, 512, 1024])
+def test_stage_radix16_lengths(bm, nx, prec, tol, monkeypatch):
+    """The radix-16 Stockham x transform of the stage kernel (16 values and half the threads per
+    line; radix tails 16x16, 16x16x2, 16x16x4) against the oracle with demag, exchange, iDMI,
+    anisotropy and Zeeman, for a power-of-two nx and an odd one: RKDP54 with step control in FP64,
+    fixed-step RK4 in mixed precision (an FP32 adaptive trajectory may choose other steps)."""
+    monkeypatch.setenv("BM_TILES", "1,4,8,1")
+    monkeypatch.setenv("BM_STAGE_XV", "2")
+    for n in [(nx, 3, 2), (nx - 1, 2, 2)]:
+        N = n[0] * n[1] * n[2]
+        mesh = dict(n=n, h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, D=1.5e-3, alpha=0.1, K1=5e5,
+                    modules=1 | 4 | 8 | 16, Ha=(1e3, 0, 0))
+        M = tilted_z(N, seed=nx) * 1.1e6
+        if prec == "fp64":
+            s = OracleSolver([mesh], evaluation=1, dt=1e-14, tol=1e-5, dT_incr=2.0, dT_min=1e-15, dT_max=3e-12)
+            c = _make(bm, prec, mesh, M, "RKDP54", 1e-14, (1e-5, 2.0, 1e-15, 3e-12))
+        else:
+            s = OracleSolver([mesh], evaluation=0, dt=2e-14)
+            c = _make(bm, prec, mesh, M, "RK4", 2e-14)
+        s.set_m(M)
+        s.run(6)
+        c.run(6)
+        t = c.tiles()
+        m = c.get_m()
+        c.close()
+        assert t["stage_xv"] == 2
+        assert np.abs(m - s.get_m()).max() / 1.1e6 < tol
