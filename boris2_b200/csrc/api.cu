@@ -899,11 +899,13 @@ int stage_batch_one(bm_ctx *c, int key, std::vector<StageArgs<T>> &v, int *count
             StageArgs<T> &a = v[i];
             a.staged = 0;
             const int rows = a.ny * a.nz;
-            const int tpl = key ? stage_reg_q(a.LX, 1) : a.px.tpl;
+            // register groups: the radix-16 variant where it exists (x 256 .. 1024), else radix 8 / 4-3
+            const int xvb = stage_reg_q(a.LX, 2) ? 2 : 1;
+            const int tpl = key ? stage_reg_q(a.LX, xvb) : a.px.tpl;
             int rpb = 256 / (3 * tpl);
             rpb = std::max(1, std::min(rpb, rows));
             a.rpb = rpb;
-            a.xv = key ? 1 : 0;
+            a.xv = key ? xvb : 0;
             for (int b = 0; b < (rows + rpb - 1) / rpb; b++) work.push_back(make_int2((int)i, b));
             nt = std::max(nt, (3 * rpb * tpl + 31) & ~31);
             const size_t lsp = key ? (size_t)(a.LX + a.LX / 16 + 1) : (size_t)padded_len(a.LX);

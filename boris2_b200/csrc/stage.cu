@@ -991,9 +991,27 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
 template int launch_stage<float>(const StageArgs<float> &, cudaStream_t);
 template int launch_stage<double>(const StageArgs<double> &, cudaStream_t);
 
+// radix-16 variant (x lengths 256 .. 1024)
+template <typename T, int LX>
+__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx16_batch(const StageArgs<T> *__restrict__ args,
+                                                                                       const int2 *__restrict__ work, int nwork)
+{
+    if (stage_gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
+    const int2 it = work[blockIdx.x];
+    stage_reg_body<T, LX, 2>(args[it.x], it.y, (unsigned int)nwork);
+}
+
 template <typename T, int LX>
 static int launch_stage_rx_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
 {
+    if constexpr (LX >= 256 && (LX % 3) != 0) {
+        if (smem > BM_SMEM_DEFAULT_SAFE) {
+            cudaError_t e = cudaFuncSetAttribute(k_stage_rx16_batch<T, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+            if (e != cudaSuccess) return 2000 + (int)e;
+        }
+        k_stage_rx16_batch<T, LX><<<nwork, nt, smem, s>>>(dargs, dwork, nwork);
+        return (int)cudaGetLastError();
+    }
     if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(k_stage_rx_batch<T, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;

@@ -96,3 +96,21 @@ def test_batched_rkdp54_matches_oracle(bm, prec, tol):
         assert sg["accepted"] == so["accepted"] and sg["rejected"] == so["rejected"]
         assert abs(sg["time"] - so["time"]) <= 1e-9 * so["time"]
     assert err < tol
+
+
+def test_batched_wide_systems_equal_per_mesh(bm):
+    """Systems 256 and 512 cells wide (the batched radix-16 stage kernel) and 384 wide (radix 4/3):
+    batched and per-mesh FP64 runs agree to 1e-11 of Ms."""
+    descs = [dict(n=n, h=H, Ms=Ms, A=1.3e-11, alpha=0.2, modules=1 | 2)
+             for n, Ms in [((256, 24, 1), 8e5), ((512, 16, 2), 1.1e6), ((384, 12, 2), 6e5)]]
+    M0 = _init(descs, "sphere")
+    out = []
+    for batched in (False, True):
+        c = _ctx(bm, "fp64", batched, descs, "RK4", 5e-14)
+        for q, M in enumerate(M0):
+            c.set_m(M, q)
+        c.run(6)
+        out.append([c.get_m(q) for q in range(len(descs))])
+        c.close()
+    err = max(np.abs(a - b).max() / d["Ms"] for a, b, d in zip(out[0], out[1], descs))
+    assert err < 1e-11
