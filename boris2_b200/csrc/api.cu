@@ -460,8 +460,12 @@ void tune_ypass(bm_ctx *c, Mesh &m)
             }
             a.W = W;
             a.yv = yv;
-            float t = time_launches(s, [&]() { return launch_yfwd<T>(a, s); }, 3) +
-                      time_launches(s, [&]() { return launch_yinv<T>(a, s); }, 3);
+            // the better of two timings of 5 launches each (single short timings mis-ranked the
+            // Stockham and generic kernels of large multilayer grids)
+            float t = 1e30f;
+            for (int trial = 0; trial < 2; trial++)
+                t = std::min(t, time_launches(s, [&]() { return launch_yfwd<T>(a, s); }, 5) +
+                                    time_launches(s, [&]() { return launch_yinv<T>(a, s); }, 5));
             if (t < best) { best = t; bw = W; byv = yv; }
         }
     m.Wy = bw;
