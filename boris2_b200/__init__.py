@@ -96,6 +96,12 @@ _SIGS = {
     "bm_ml_tile": (_I, [_P, _IP]),
     "bm_set_batched": (_I, [_P, _I]),
     "bm_adjoint_rk4": (_I, [_P, _I, _I, _DP, _I, _DP, _DP, _DP, _DP, _DP]),
+    "bm_ovf2_read": (_I, [ctypes.c_char_p, _IP, _DP, _DP, _DP, ctypes.c_longlong]),
+    "bm_ovf2_write": (_I, [ctypes.c_char_p, _IP, _DP, _DP, _DP, ctypes.c_char_p, _D]),
+    "bm_map_cells": (_I, [_DP, _IP, _DP, _IP]),
+    "bm_renormalize": (_I, [_DP, ctypes.c_longlong, _D]),
+    "bm_load_ovf2_mag": (_I, [_P, _I, ctypes.c_char_p, _D]),
+    "bm_save_ovf2_mag": (_I, [_P, _I, ctypes.c_char_p, ctypes.c_char_p, _I]),
 }
 
 
@@ -128,6 +134,45 @@ def _vec(a, n):
     if a.size != 3 * n:
         raise ValueError("expected %d values (3 per cell), got %d" % (3 * n, a.size))
     return a
+
+
+def ovf2_read(path):
+    """Read an OOMMF OVF 2.0 vector file (host only): dict with n (nodes), h (cellsize, m),
+    rect (xmin, ymin, zmin, xmax, ymax, zmax, m) and data ((n cells, 3), x fastest)."""
+    n3 = (ctypes.c_int * 3)()
+    h3 = np.empty(3)
+    r6 = np.empty(6)
+    p = os.fsencode(path)
+    _check(lib().bm_ovf2_read(p, n3, _dp(h3), _dp(r6), None, 0))
+    n = tuple(n3)
+    data = np.empty(3 * n[0] * n[1] * n[2])
+    _check(lib().bm_ovf2_read(p, None, None, None, _dp(data), data.size))
+    return {"n": n, "h": tuple(h3), "rect": tuple(r6), "data": data.reshape(-1, 3)}
+
+
+def ovf2_write(path, data, n, h, origin=(0.0, 0.0, 0.0), data_type="bin8", norm=1.0):
+    """Write an OOMMF OVF 2.0 vector file (host only); data_type "bin4", "bin8" or "text",
+    every value divided by norm."""
+    n3 = (ctypes.c_int * 3)(*[int(v) for v in n])
+    a = _vec(data, int(n[0]) * int(n[1]) * int(n[2]))
+    h3 = np.asarray(h, dtype=np.float64)
+    o3 = np.asarray(origin, dtype=np.float64)
+    _check(lib().bm_ovf2_write(os.fsencode(path), n3, _dp(h3), _dp(o3), _dp(a), data_type.encode(), float(norm)))
+
+
+def map_cells(data, src_n, dst_n):
+    """Nearest-cell remap of (cells, 3) vectors from src_n to dst_n cells (host only)."""
+    a = _vec(data, int(np.prod(src_n)))
+    out = np.empty(3 * int(np.prod(dst_n)))
+    _check(lib().bm_map_cells(_dp(a), (ctypes.c_int * 3)(*src_n), _dp(out), (ctypes.c_int * 3)(*dst_n)))
+    return out.reshape(-1, 3)
+
+
+def renormalize(data, length):
+    """Scale every vector longer than 1e-12 to `length` (host only); returns a new array."""
+    a = np.array(np.asarray(data, dtype=np.float64).reshape(-1), copy=True)
+    _check(lib().bm_renormalize(_dp(a), a.size // 3, float(length)))
+    return a.reshape(-1, 3)
 
 
 class Context:
@@ -275,6 +320,15 @@ class Context:
         out = np.empty(3 * n) if out is None else out
         _check(lib().bm_get_m(self._h, mesh, _dp(out)))
         return out.reshape(n, 3)
+
+    def loadovf2mag(self, path, mesh=0, renormalize=0.0):
+        """The reference's loadovf2mag: M from an OVF 2.0 file, mapped to this mesh's cells and
+        renormalised to `renormalize` when it is non-zero."""
+        _check(lib().bm_load_ovf2_mag(self._h, mesh, os.fsencode(path), float(renormalize)))
+
+    def saveovf2mag(self, path, mesh=0, data_type="bin8", normalize=False):
+        """The reference's saveovf2mag: M to an OVF 2.0 file, divided by Ms when normalize."""
+        _check(lib().bm_save_ovf2_mag(self._h, mesh, os.fsencode(path), data_type.encode(), int(bool(normalize))))
 
     def demag_field(self, mesh=0, with_energy=False):
         n = self.ncells(mesh)

@@ -1961,6 +1961,38 @@ int bm_get_m(bm_ctx *c, int mesh, double *M)
     return 0;
 }
 
+int bm_load_ovf2_mag(bm_ctx *c, int mesh, const char *path, double renormalize)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    int n3[3];
+    if (int rc = bm_ovf2_read(path, n3, nullptr, nullptr, nullptr, 0)) return rc;
+    std::vector<double> src(3 * (size_t)n3[0] * n3[1] * n3[2]);
+    if (int rc = bm_ovf2_read(path, nullptr, nullptr, nullptr, src.data(), (long long)src.size())) return rc;
+    if (std::fabs(renormalize) > 1e-12) bm_renormalize(src.data(), (long long)(src.size() / 3), renormalize);
+    Mesh &m = c->meshes[mesh];
+    int dn[3] = {m.nx, m.ny, m.nz};
+    std::vector<double> dst(3 * (size_t)m.n);
+    if (int rc = bm_map_cells(src.data(), n3, dst.data(), dn)) return rc;
+    // the reference marks zero-length cells empty (VEC_VC::copy_values); this path has no empty cells
+    for (long long i = 0; i < m.n; i++) {
+        const double *v = dst.data() + 3 * i;
+        if (!(v[0] * v[0] + v[1] * v[1] + v[2] * v[2] > 0.0))
+            return fail(BM_EUNSUPPORTED, "bm_load_ovf2_mag: cell " + std::to_string(i) +
+                                             " has a zero-length value (empty cells are not supported)");
+    }
+    return bm_set_m(c, mesh, dst.data());
+}
+
+int bm_save_ovf2_mag(bm_ctx *c, int mesh, const char *path, const char *data_type, int normalize)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    Mesh &m = c->meshes[mesh];
+    std::vector<double> M(3 * (size_t)m.n);
+    if (int rc = bm_get_m(c, mesh, M.data())) return rc;
+    int n3[3] = {m.nx, m.ny, m.nz};
+    return bm_ovf2_write(path, n3, m.h, m.o, M.data(), data_type, normalize ? m.Ms : 1.0);
+}
+
 int bm_compute_hdemag(bm_ctx *c, int mesh, double *H, double *energy)
 {
     if (int rc = check_mesh(c, mesh)) return rc;

@@ -158,6 +158,30 @@ int bm_prepare(bm_ctx *ctx);
 int bm_set_m(bm_ctx *ctx, int mesh, const double *M);
 int bm_get_m(bm_ctx *ctx, int mesh, double *M);
 
+/* OOMMF OVF 2.0 files of vector data (rectangular, valuedim 3; "binary 4", "binary 8" or "text").
+ * bm_ovf2_read replaces OVF2::Read_OVF2_VEC (Boris/OVF2_Handlers.cpp:364): it fills n3 (nodes),
+ * h3 (cellsize, m), rect6 (xmin, ymin, zmin, xmax, ymax, zmax, m) where given, and, when data is
+ * not NULL, 3 * n values (AoS, x fastest) into data, which must hold `capacity` >= 3 * n doubles
+ * (call once with data = NULL to learn n). A file whose first line is not "# OOMMF OVF 2.0" gives
+ * BM_EUNSUPPORTED; a malformed or truncated file BM_EINVAL.
+ * bm_ovf2_write replaces OVF2::Write_OVF2_VEC (Boris/OVF2_Handlers.cpp:701): data_type "bin4",
+ * "bin8" or "text", every value divided by norm, the rectangle from origin3 (NULL: 0) and n3 * h3. */
+int bm_ovf2_read(const char *path, int *n3, double *h3, double *rect6, double *data, long long capacity);
+int bm_ovf2_write(const char *path, const int *n3, const double *h3, const double *origin3, const double *data,
+                  const char *data_type, double norm);
+/* Nearest-cell remap of AoS vectors from src_n3 to dst_n3 cells: VEC::mapmesh_newdims
+ * (BorisLib/VEC_mng.h:9). Scale every vector longer than 1e-12 to `length`: VEC::renormalize
+ * (BorisLib/VEC_oper.h:45). */
+int bm_map_cells(const double *src, const int *src_n3, double *dst, const int *dst_n3);
+int bm_renormalize(double *data, long long ncell, double length);
+/* The reference's loadovf2mag / saveovf2mag commands (Boris/Commands.cpp:5025, 5192): load a file
+ * into a mesh's M, renormalised to `renormalize` when it is non-zero, mapped to the mesh's cell
+ * counts; save a mesh's M with the mesh's origin and cellsize, divided by the mesh's Ms when
+ * normalize != 0. A file that puts a zero-length value on a cell (an empty cell of the reference's
+ * mesh shape) gives BM_EUNSUPPORTED: every cell here carries Ms > 0. */
+int bm_load_ovf2_mag(bm_ctx *ctx, int mesh, const char *path, double renormalize);
+int bm_save_ovf2_mag(bm_ctx *ctx, int mesh, const char *path, const char *data_type, int normalize);
+
 /* Demagnetising field of the current M into H (3 * n doubles) and the demag energy
  * density -mu0/(2 n) sum M.H. Replaces Demag::UpdateField (Boris/Demag.cpp:170) /
  * DemagCUDA::UpdateField (Boris/DemagCUDA.cpp:106). */

@@ -21,6 +21,11 @@
  *                      layer with the rectangle rules of SDemag (Boris/SDemag.cpp:173,215,441), the
  *                      weighted mesh transfer of SDemag_Demag (Boris/SDemag_Demag.cpp:64,349) and the
  *                      evaluation order of SDemag::UpdateField (Boris/SDemag.cpp:786-900)
+ *   ref_ovf2_read      OVF2::Read_OVF2_VEC                  (Boris/OVF2_Handlers.cpp:364)
+ *   ref_ovf2_write     OVF2::Write_OVF2_VEC                 (Boris/OVF2_Handlers.cpp:701)
+ *   ref_ovf2_load      the loadovf2mag command's data path (Boris/Commands.cpp:5025): read,
+ *                      VEC::renormalize when the value is non-zero, VEC::resize(SZ3) to the mesh's
+ *                      cell counts (BorisLib/VEC_mng.h:9,118)
  * All arrays are AoS (x,y,z per cell), cells ordered x fastest, then y, then z.
  */
 #include "stdafx.h"
@@ -28,6 +33,7 @@
 #include "DemagKernel.h"
 #include "DemagKernelCollection.h"
 #include "Convolution.h"
+#include "OVF2_Handlers.h"
 
 #include <vector>
 #include <cstring>
@@ -468,6 +474,48 @@ int ref_ml_transfer(void *hp, int layer, const double *M, double *Mc, const doub
     t.transfer_out();
     int m = s->layer_mesh[layer];
     memcpy(Hmesh, s->Heff[m]->data(), sizeof(double) * 3 * s->Heff[m]->linear_size());
+    return 0;
+}
+
+/* Header of an OVF 2.0 file (n, h, rect) and, when data != NULL, its values; 0 on success,
+ * 1 when the reference's reader returns an error. */
+int ref_ovf2_read(const char *path, int *n3, double *h3, double *rect6, double *data)
+{
+    VEC<DBL3> v;
+    OVF2 ovf2;
+    BError err = ovf2.Read_OVF2_VEC(std::string(path), v);
+    if (err) return 1;
+    n3[0] = v.n.x; n3[1] = v.n.y; n3[2] = v.n.z;
+    h3[0] = v.h.x; h3[1] = v.h.y; h3[2] = v.h.z;
+    rect6[0] = v.rect.s.x; rect6[1] = v.rect.s.y; rect6[2] = v.rect.s.z;
+    rect6[3] = v.rect.e.x; rect6[4] = v.rect.e.y; rect6[5] = v.rect.e.z;
+    if (data) memcpy(data, v.data(), sizeof(double) * 3 * v.linear_size());
+    return 0;
+}
+
+int ref_ovf2_write(const char *path, const int *n3, const double *h3, const double *origin3, const double *data,
+                   const char *data_type, double norm)
+{
+    DBL3 h(h3[0], h3[1], h3[2]);
+    DBL3 s(origin3[0], origin3[1], origin3[2]);
+    Rect r(s, s + DBL3(n3[0] * h3[0], n3[1] * h3[1], n3[2] * h3[2]));
+    VEC<DBL3> v(h, r);
+    if (v.n.x != n3[0] || v.n.y != n3[1] || v.n.z != n3[2]) return 2;
+    memcpy(v.data(), data, sizeof(double) * 3 * v.linear_size());
+    OVF2 ovf2;
+    BError err = ovf2.Write_OVF2_VEC(std::string(path), v, std::string(data_type), norm);
+    return err ? 1 : 0;
+}
+
+int ref_ovf2_load(const char *path, double renormalize, const int *dst_n3, double *out)
+{
+    VEC<DBL3> v;
+    OVF2 ovf2;
+    BError err = ovf2.Read_OVF2_VEC(std::string(path), v);
+    if (err) return 1;
+    if (IsNZ(renormalize)) v.renormalize(renormalize);
+    if (!v.resize(SZ3(dst_n3[0], dst_n3[1], dst_n3[2]))) return 2;
+    memcpy(out, v.data(), sizeof(double) * 3 * v.linear_size());
     return 0;
 }
 

@@ -1,7 +1,8 @@
 """ctypes access to the oracle (test infrastructure only).
 
   liboracle.so    oracle/oracle.c — the project's FP64 CPU restatement of the path
-  libborisref.so  the reference's own CPU sources compiled by oracle/Makefile
+  libborisref.so  the reference's own CPU sources compiled by oracle/Makefile (demag,
+                  stencils, multilayer convolution, OVF 2.0 reader and writer)
 
 Both are built from oracle/Makefile when missing (the reference build only where the
 reference tree is present; its .so travels with the repository otherwise).
@@ -94,10 +95,11 @@ def reference():
     """The reference's compiled CPU code (None when neither the .so nor the tree is present)."""
     global _ref
     if _ref is None:
-        if not os.path.exists(REF_SO):
-            if not os.path.isdir(REF_TREE):
-                return None
+        if os.path.isdir(REF_TREE):
+            # incremental: rebuilds only what changed since the last build
             subprocess.run(["make", "-C", ORACLE_DIR, "-j8", "ref"], check=True, capture_output=True)
+        elif not os.path.exists(REF_SO):
+            return None
         L = ctypes.CDLL(REF_SO)
         L.ref_selfdemag.argtypes = [D, D, D, DP]
         L.ref_tensor.argtypes = [I, I, I, I, I, I, D, D, D, DP, DP]
@@ -117,6 +119,9 @@ def reference():
         L.ref_ml_eval.argtypes = [P, DP, DP]
         L.ref_ml_transfer.argtypes = [P, I, DP, DP, DP, DP]
         L.ref_ml_destroy.argtypes = [P]
+        L.ref_ovf2_read.argtypes = [ctypes.c_char_p, IP, DP, DP, DP]
+        L.ref_ovf2_write.argtypes = [ctypes.c_char_p, IP, DP, DP, DP, ctypes.c_char_p, D]
+        L.ref_ovf2_load.argtypes = [ctypes.c_char_p, D, IP, DP]
         _ref = L
     return _ref
 
