@@ -96,6 +96,8 @@ _SIGS = {
     "bm_ml_tile": (_I, [_P, _IP]),
     "bm_set_batched": (_I, [_P, _I]),
     "bm_adjoint_rk4": (_I, [_P, _I, _I, _DP, _I, _DP, _DP, _DP, _DP, _DP]),
+    "bm_set_evalspeedup": (_I, [_P, _I]),
+    "bm_self_demag": (_I, [_D, _D, _D, _DP]),
     "bm_ovf2_read": (_I, [ctypes.c_char_p, _IP, _DP, _DP, _DP, ctypes.c_longlong]),
     "bm_ovf2_write": (_I, [ctypes.c_char_p, _IP, _DP, _DP, _DP, ctypes.c_char_p, _D]),
     "bm_map_cells": (_I, [_DP, _IP, _DP, _IP]),
@@ -134,6 +136,13 @@ def _vec(a, n):
     if a.size != 3 * n:
         raise ValueError("expected %d values (3 per cell), got %d" % (3 * n, a.size))
     return a
+
+
+def self_demag(h):
+    """Self-demagnetising coefficients -N of a cell of size h (host only)."""
+    out = np.empty(3)
+    _check(lib().bm_self_demag(float(h[0]), float(h[1]), float(h[2]), _dp(out)))
+    return out
 
 
 def ovf2_read(path):
@@ -306,6 +315,11 @@ class Context:
 
     def setdt(self, dt):
         _check(lib().bm_set_ode(self._h, getattr(self, "_eval", RK4), float(dt)))
+
+    def evalspeedup(self, level):
+        """The reference's evalspeedup: 0 off, 1 step .. 6 quintic extrapolation of the demag field
+        between RK4 steps."""
+        _check(lib().bm_set_evalspeedup(self._h, int(level)))
 
     def astepctrl(self, err_fail, dT_incr, dT_min, dT_max):
         _check(lib().bm_set_astepctrl(self._h, float(err_fail), float(dT_incr), float(dT_min), float(dT_max)))

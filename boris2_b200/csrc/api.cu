@@ -77,6 +77,8 @@ struct Mesh {
     void *S1 = nullptr, *S2 = nullptr, *K = nullptr;
     void *twx = nullptr, *twx2 = nullptr, *twy = nullptr, *twz = nullptr;
     void *Msd = nullptr, *K1d = nullptr, *Hout = nullptr;
+    void *G = nullptr;          // evaluation speedup: es_level saved spectra (3 planes each)
+    double es_cs[3] = {0, 0, 0};
     double *Had = nullptr, *stage64 = nullptr;
     int nHa = 1;
     // multilayered convolution: 0 not in one, 1 its grid is the common grid (spectra in S1/S2),
@@ -149,6 +151,8 @@ struct bm_ctx {
     bool ml_nc_set = false;
     int ml_nc[3] = {1, 1, 1};
     MLRun *ml = nullptr;
+    int es_level = 0;           // evaluation speedup level (0 off, 1..6)
+    bool es_reset = true;       // clear the saved fields at the next state upload
 };
 
 namespace {
@@ -159,7 +163,7 @@ void free_mesh(Mesh &m)
 {
     for (auto &p : m.buf) { if (p) cudaFree(p); p = nullptr; }
     for (auto &p : m.ev) { if (p) cudaFree(p); p = nullptr; }
-    void **ps[] = {&m.S1, &m.S2, &m.K, &m.twx, &m.twx2, &m.twy, &m.twz, &m.Msd, &m.K1d, &m.Hout};
+    void **ps[] = {&m.S1, &m.S2, &m.K, &m.twx, &m.twx2, &m.twy, &m.twz, &m.Msd, &m.K1d, &m.Hout, &m.G};
     for (auto pp : ps) { if (*pp) cudaFree(*pp); *pp = nullptr; }
     if (m.Had) cudaFree(m.Had);
     m.Had = nullptr;
@@ -334,6 +338,13 @@ int prepare_mesh(bm_ctx *c, Mesh &m)
         size_t s1 = sizeof(cpx<T>) * 3 * (size_t)m.nz * m.ny * m.LX;
         if (cudaMalloc(&m.S1, s1) != cudaSuccess) return fail(BM_ENOMEM, "S1");
         cudaMemsetAsync(m.S1, 0, s1, s);
+        if (c->es_level > 0) {
+            if (cudaMalloc(&m.G, s1 * c->es_level) != cudaSuccess) return fail(BM_ENOMEM, "evaluation speedup slots");
+            cudaMemsetAsync(m.G, 0, s1 * c->es_level, s);
+            double S[3];
+            self_demag_host(m.h[0], m.h[1], m.h[2], S);
+            for (int k = 0; k < 3; k++) m.es_cs[k] = S[k] * (double)m.Ny * (double)m.Nz;
+        }
         if (m.nz > 1 || m.ml_role == 1) {
             size_t s2 = sizeof(cpx<T>) * 3 * (size_t)m.nz * m.Ny * m.LX;
             if (cudaMalloc(&m.S2, s2) != cudaSuccess) return fail(BM_ENOMEM, "S2");
@@ -396,6 +407,12 @@ int upload_state(bm_ctx *c)
     h.dT_min = c->dT_min;
     h.dT_max = c->dT_max;
     h.eval_order = (c->eval == BM_RKDP54) ? 5 : 4;
+    h.es_K = c->es_level;
+    if (c->es_reset) {
+        h.es_saved = 0;
+        for (int k = 0; k < 6; k++) h.es_t[k] = 0.0;
+        c->es_reset = false;
+    }
     h.reject_flag = 0;
     h.need_restore = 0;
     h.lte_bits = 0;
@@ -797,11 +814,14 @@ int prepare(bm_ctx *c)
     if (c->ready) return 0;
     if (c->meshes.empty()) return fail(BM_ESTATE, "no mesh");
     if (c->batched && c->ml_mode >= 0) return fail(BM_EUNSUPPORTED, "batched meshes with a multilayered convolution");
+    if (c->es_level > 0 && (c->ml_mode >= 0 || (c->batched && c->meshes.size() > 1)))
+        return fail(BM_EUNSUPPORTED, "evaluation speedup with a multilayered convolution or batched meshes");
     CK(cudaSetDevice(c->device));
     int rc = (c->precision == BM_FP64) ? prepare_T<double>(c) : prepare_T<float>(c);
     if (rc) return rc;
     c->ready = true;
     c->s1_dirty = true;
+    c->es_reset = true;
     return upload_state(c);
 }
 
@@ -1242,6 +1262,8 @@ int enqueue_prime(bm_ctx *c, int *count)
     return 0;
 }
 
+long long es_plane(const Mesh &m) { return (long long)m.nz * m.ny * m.LX; }
+
 template <typename T>
 int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void *const *cacheH = nullptr, void *cacheY = nullptr)
 {
@@ -1250,8 +1272,33 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
     // update before renormalisation are also written there
     const int nm = (int)c->meshes.size();
     static const int min_buf[4] = {0, 2, 3, 2};
+    static const double c_eval[4] = {0.0, 0.5, 0.5, 1.0};   // RK4 evaluation times (Get_EvalStep_Time)
     for (int s = 0; s < 4; s++) {
-        {
+        if (c->es_level > 0 && s == 0) {
+            // evaluation speedup: compute and save the field at the first evaluation of the step
+            for (auto &m : c->meshes) {
+                if (!(m.modules & BM_DEMAG)) continue;
+                CKL(launch_es_pre<T>((const cpx<T> *)m.S1, (cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c->stream), "es_pre");
+                (*count)++;
+            }
+            if (int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count)) return rc;
+            for (auto &m : c->meshes) {
+                if (!(m.modules & BM_DEMAG)) continue;
+                CKL(launch_es_post<T>((const cpx<T> *)m.S1, (cpx<T> *)m.G, es_plane(m), c->st, c->stream), "es_post");
+                (*count)++;
+            }
+            CKL(launch_es_commit(c->st, c->stream), "es_commit");
+            (*count)++;
+        } else if (c->es_level > 0) {
+            // full field while too few are saved, else the extrapolation
+            if (int rc = enqueue_fields<T>(c, BM_GATE_ES_FULL, min_buf[s], count)) return rc;
+            for (auto &m : c->meshes) {
+                if (!(m.modules & BM_DEMAG)) continue;
+                CKL(launch_es_extrap<T>((cpx<T> *)m.S1, (const cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c_eval[s],
+                                        c->stream), "es_extrap");
+                (*count)++;
+            }
+        } else {
             int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count);
             if (rc) return rc;
         }
@@ -1824,6 +1871,17 @@ int bm_set_ode(bm_ctx *c, int eval, double dt)
     return 0;
 }
 
+int bm_set_evalspeedup(bm_ctx *c, int level)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (level < 0 || level > 6) return fail(BM_EINVAL, "evaluation speedup level must be 0..6");
+    if (level == c->es_level) return 0;
+    unprepare(c);
+    c->es_level = level;
+    c->es_reset = true;
+    return 0;
+}
+
 int bm_set_astepctrl(bm_ctx *c, double err_fail, double dT_incr, double dT_min, double dT_max)
 {
     if (int rc = check_ctx(c)) return rc;
@@ -1906,6 +1964,7 @@ int bm_adjoint_rk4(bm_ctx *c, int steps, int ckpt_every, const double *target, i
     if (c->meshes.size() != 1) return fail(BM_EUNSUPPORTED, "adjoint: one mesh");
     if (c->eval != BM_RK4) return fail(BM_EUNSUPPORTED, "adjoint: RK4 only");
     if (c->ml_mode >= 0 || c->batched) return fail(BM_EUNSUPPORTED, "adjoint: no multilayer or batching");
+    if (c->es_level > 0) return fail(BM_EUNSUPPORTED, "adjoint: no evaluation speedup");
     if (ckpt_every < 1 || steps < 1 || steps % ckpt_every) return fail(BM_EINVAL, "adjoint: steps must be a positive multiple of ckpt_every");
     const Mesh &m0 = c->meshes[0];
     if (m0.modules & ~(BM_DEMAG | BM_EXCH | BM_ANIUNI | BM_ZEEMAN)) return fail(BM_EUNSUPPORTED, "adjoint: demag, exchange, anisotropy, Zeeman only");
@@ -1937,9 +1996,11 @@ int bm_set_m(bm_ctx *c, int mesh, const double *M)
     if (c->precision == BM_FP64) CKL(launch_aos_to_planes<double>((double *)m.buf[0], m.stage64, m.n, c->stream), "aos_to_planes");
     else CKL(launch_aos_to_planes<float>((float *)m.buf[0], m.stage64, m.n, c->stream), "aos_to_planes");
     c->s1_dirty = true;
-    // a new M un-primes the RKDP54 error estimate, as a restart of the reference solver does
+    // a new M un-primes the RKDP54 error estimate, as a restart of the reference solver does, and
+    // drops the fields saved for the evaluation speedup
     if (int rc = read_state(c)) return rc;
     c->host_st.primed = 0;
+    c->es_reset = true;
     c->dt = c->host_st.dT;
     return upload_state(c);
 }
@@ -2027,6 +2088,7 @@ int bm_run(bm_ctx *c, int steps, bm_stats *out)
 {
     if (int rc = check_ctx(c)) return rc;
     if (steps < 0) return fail(BM_EINVAL, "steps < 0");
+    if (c->es_level > 0 && c->eval != BM_RK4) return fail(BM_EUNSUPPORTED, "evaluation speedup needs RK4");
     if (int rc = prepare(c)) return rc;
     cudaSetDevice(c->device);
     if (steps > 0) {
@@ -2092,6 +2154,7 @@ int bm_kernels_per_step(bm_ctx *c, int *count)
 int bm_run_timed(bm_ctx *c, int steps, bm_stats *out, double *device_ms)
 {
     if (int rc = check_ctx(c)) return rc;
+    if (c->es_level > 0 && c->eval != BM_RK4) return fail(BM_EUNSUPPORTED, "evaluation speedup needs RK4");
     if (int rc = prepare(c)) return rc;
     cudaSetDevice(c->device);
     if (c->s1_dirty) {

@@ -72,4 +72,7 @@ struct StepState {
     unsigned int restore_done;
     int eval_order;
     int pad_;
+    // evaluation speedup: fields saved so far (<= es_K) and the times they were saved at
+    int es_saved, es_K;
+    double es_t[6];
 };

@@ -1,0 +1,141 @@
+// Evaluation speedup of RK4 (the reference's `evalspeedup` levels 1..6: step, linear, quadratic,
+// cubic, quartic, quintic), following DemagCUDA::UpdateField (Boris/DemagCUDA.cpp:106-470) with
+// ODECommon_Base::Check_Step_Update / Get_EvalStep_Time (Boris/DiffEq_CommonBase_Iterate.cpp:1536,1639;
+// dTspeedup linked to dT, so the field is computed at the first evaluation of every step):
+//   - the first evaluation of a step computes the demag field and saves H - S M (S the self-demag
+//     coefficients, Demag_EvalSpeedup_AddField_SubSelf, Boris/DemagCUDA.cu:46) in the next free slot,
+//     then in the slot holding the earliest time;
+//   - the other evaluations compute the field in full until es_K fields are saved, then use
+//     sum_k a_k (H_k - S M_k) + S M with the Lagrange weights a_k of the saved times at the
+//     evaluation time (Demag_EvalSpeedup_AddExtrapField_AddSelf, Boris/DemagCUDA.cu:64-265).
+// The reference does this on the real-space field; here it is done on S1, the x spectrum the y/z
+// passes consume and produce. Every step of it is linear and S is diagonal, so the field the stage
+// kernel transforms back is the same: an extrapolating evaluation replaces the y forward, z and y
+// inverse passes with one pass over S1 and the saved slots.
+#include "kernels.h"
+
+namespace {
+
+__device__ __forceinline__ int es_slot(const StepState *st)
+{
+    int K = st->es_K, saved = st->es_saved;
+    if (saved < K) return saved;
+    int slot = 0;
+    for (int k = 1; k < K; k++)
+        if (st->es_t[k] < st->es_t[slot]) slot = k;
+    return slot;
+}
+
+int es_grid(long long n)
+{
+    long long b = (n + 255) / 256;
+    long long cap = 148LL * 8;
+    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+template <typename T>
+__global__ void k_es_pre(const cpx<T> *__restrict__ S1, cpx<T> *__restrict__ G, long long plane, double c0, double c1,
+                         double c2, const StepState *st)
+{
+    cpx<T> *g = G + (long long)es_slot(st) * 3 * plane;
+    const long long n = 3 * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int c = (int)(i / plane);
+        T f = (T)(c == 0 ? c0 : (c == 1 ? c1 : c2));
+        cpx<T> v = S1[i];
+        g[i] = mk<T>(f * v.x, f * v.y);
+    }
+}
+
+template <typename T>
+__global__ void k_es_post(const cpx<T> *__restrict__ S1, cpx<T> *__restrict__ G, long long plane, const StepState *st)
+{
+    cpx<T> *g = G + (long long)es_slot(st) * 3 * plane;
+    const long long n = 3 * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        cpx<T> h = S1[i], s = g[i];
+        g[i] = mk<T>(h.x - s.x, h.y - s.y);
+    }
+}
+
+__global__ void k_es_commit(StepState *st)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        int slot = es_slot(st);
+        st->es_t[slot] = st->time;
+        if (st->es_saved < st->es_K) st->es_saved++;
+    }
+}
+
+template <typename T>
+__global__ void k_es_extrap(cpx<T> *__restrict__ S1, const cpx<T> *__restrict__ G, long long plane, double c0, double c1,
+                            double c2, const StepState *st, double c_eval)
+{
+    const int K = st->es_K;
+    if (st->es_saved < K) return;
+    // Lagrange weights of the saved times at the evaluation time
+    const double t = st->time + c_eval * st->dT;
+    T a[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        double w = 0.0;
+        if (k < K) {
+            w = 1.0;
+            for (int j = 0; j < K; j++)
+                if (j != k) w *= (t - st->es_t[j]) / (st->es_t[k] - st->es_t[j]);
+        }
+        a[k] = (T)w;
+    }
+    const long long n = 3 * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int c = (int)(i / plane);
+        T f = (T)(c == 0 ? c0 : (c == 1 ? c1 : c2));
+        cpx<T> m = S1[i];
+        T x = f * m.x, y = f * m.y;
+        for (int k = 0; k < K; k++) {
+            cpx<T> g = G[(long long)k * n + i];
+            x += a[k] * g.x;
+            y += a[k] * g.y;
+        }
+        S1[i] = mk<T>(x, y);
+    }
+}
+
+}  // namespace
+
+template <typename T>
+int launch_es_pre(const cpx<T> *S1, cpx<T> *G, long long plane, const double *cs, const StepState *st, cudaStream_t s)
+{
+    k_es_pre<T><<<es_grid(3 * plane), 256, 0, s>>>(S1, G, plane, cs[0], cs[1], cs[2], st);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+int launch_es_post(const cpx<T> *S1, cpx<T> *G, long long plane, const StepState *st, cudaStream_t s)
+{
+    k_es_post<T><<<es_grid(3 * plane), 256, 0, s>>>(S1, G, plane, st);
+    return (int)cudaGetLastError();
+}
+
+int launch_es_commit(StepState *st, cudaStream_t s)
+{
+    k_es_commit<<<1, 32, 0, s>>>(st);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+int launch_es_extrap(cpx<T> *S1, const cpx<T> *G, long long plane, const double *cs, const StepState *st, double c_eval,
+                     cudaStream_t s)
+{
+    k_es_extrap<T><<<es_grid(3 * plane), 256, 0, s>>>(S1, G, plane, cs[0], cs[1], cs[2], st, c_eval);
+    return (int)cudaGetLastError();
+}
+
+template int launch_es_pre<float>(const cpx<float> *, cpx<float> *, long long, const double *, const StepState *, cudaStream_t);
+template int launch_es_pre<double>(const cpx<double> *, cpx<double> *, long long, const double *, const StepState *, cudaStream_t);
+template int launch_es_post<float>(const cpx<float> *, cpx<float> *, long long, const StepState *, cudaStream_t);
+template int launch_es_post<double>(const cpx<double> *, cpx<double> *, long long, const StepState *, cudaStream_t);
+template int launch_es_extrap<float>(cpx<float> *, const cpx<float> *, long long, const double *, const StepState *, double,
+                                     cudaStream_t);
+template int launch_es_extrap<double>(cpx<double> *, const cpx<double> *, long long, const double *, const StepState *,
+                                      double, cudaStream_t);

@@ -22,6 +22,7 @@ void bm_far_coeffs(double hx, double hy, double hz, double *out);
 #define BM_GATE_ALWAYS 0
 #define BM_GATE_ACCEPTED 1      // skip when the current attempt was rejected
 #define BM_GATE_RESTORE 2       // run only when a restore is pending
+#define BM_GATE_ES_FULL 3       // evaluation speedup: run only while fewer than es_K fields are saved
 
 // ---------------------------------------------------------------- y / z passes
 template <typename T>
@@ -204,3 +205,18 @@ int launch_adj_vjp_c(const AdjArgs<T> &a, const T *gXd, const T *w, const T *gD,
                      double cX, int write_mu, cudaStream_t s);
 template <typename T>
 int launch_adj_m0(const AdjArgs<T> &a, const T *M0, const T *lam, double *gMs, cudaStream_t s);
+
+// ---------------------------------------------------------------- evaluation speedup (RK4)
+void self_demag_host(double hx, double hy, double hz, double out3[3]);   // -N of one cell (tensor.cu)
+// Demag extrapolation in the x-spectrum domain S1[c][z][y][kx] (plane = nz ny LX complex values per
+// component). G holds es_K slots of 3 planes: the saved field minus its self term. cs[c] is the
+// self-demag coefficient (-N_c) times Ny Nz, the factor between the x-spectrum of M the stage kernel
+// writes and the x-spectrum of H the y inverse pass leaves.
+template <typename T>
+int launch_es_pre(const cpx<T> *S1, cpx<T> *G, long long plane, const double *cs, const StepState *st, cudaStream_t s);
+template <typename T>
+int launch_es_post(const cpx<T> *S1, cpx<T> *G, long long plane, const StepState *st, cudaStream_t s);
+int launch_es_commit(StepState *st, cudaStream_t s);
+template <typename T>
+int launch_es_extrap(cpx<T> *S1, const cpx<T> *G, long long plane, const double *cs, const StepState *st, double c_eval,
+                     cudaStream_t s);

@@ -15,10 +15,14 @@
 #include "fft.cuh"
 #include "kernels.h"
 #include "ml.h"
+#include "boris_b200.h"
+
+#include <string>
+int bm_set_error(int code, const std::string &msg);
 
 #define BM_ASYMPT_DIST 40
 
-__device__ __forceinline__ double csum_d(const double *v, int n)
+__host__ __device__ __forceinline__ double csum_d(const double *v, int n)
 {
     double s = 0.0, c = 0.0;
     for (int i = 0; i < n; i++) {
@@ -30,7 +34,7 @@ __device__ __forceinline__ double csum_d(const double *v, int n)
     return s + c;
 }
 
-__device__ double nf(double x, double y, double z)
+__host__ __device__ double nf(double x, double y, double z)
 {
     double x2 = x * x, y2 = y * y, z2 = z * z;
     double R = sqrt(x2 + y2 + z2);
@@ -43,7 +47,7 @@ __device__ double nf(double x, double y, double z)
     return csum_d(t, 4);
 }
 
-__device__ double ng(double x, double y, double z)
+__host__ __device__ double ng(double x, double y, double z)
 {
     double x2 = x * x, y2 = y * y, z2 = z * z;
     double R = sqrt(x2 + y2 + z2);
@@ -60,7 +64,7 @@ __device__ double ng(double x, double y, double z)
 }
 
 template <bool G>
-__device__ double newellL(double x, double y, double z, double hx, double hy, double hz)
+__host__ __device__ double newellL(double x, double y, double z, double hx, double hy, double hz)
 {
     double v[27];
     int m = 0;
@@ -72,6 +76,24 @@ __device__ double newellL(double x, double y, double z, double hx, double hy, do
                 v[m++] = w * (G ? ng(x + a * hx, y + b * hy, z + c * hz) : nf(x + a * hx, y + b * hy, z + c * hz));
             }
     return csum_d(v, 27) / (4.0 * M_PI * hx * hy * hz);
+}
+
+// Self-demagnetising coefficients -N (the tensor's diagonal at the origin, DemagTFunc::SelfDemag,
+// Boris/DemagTFunc_Self.cpp:6 with "minus"), on the host, cellsizes normalised by the largest.
+void self_demag_host(double hx, double hy, double hz, double out3[3])
+{
+    double hm = fmax(hx, fmax(hy, hz));
+    hx /= hm; hy /= hm; hz /= hm;
+    out3[0] = -newellL<false>(0.0, 0.0, 0.0, hx, hy, hz);
+    out3[1] = -newellL<false>(0.0, 0.0, 0.0, hy, hx, hz);
+    out3[2] = -newellL<false>(0.0, 0.0, 0.0, hz, hy, hx);
+}
+
+extern "C" int bm_self_demag(double hx, double hy, double hz, double *out3)
+{
+    if (!out3 || !(hx > 0) || !(hy > 0) || !(hz > 0)) return bm_set_error(BM_EINVAL, "bm_self_demag: cellsizes must be > 0");
+    self_demag_host(hx, hy, hz, out3);
+    return 0;
 }
 
 // far field: D_c = V/(4 pi) sum_n Q_{c,n}(u,v,w) / R^(n+1), coefficient layout per comp c:

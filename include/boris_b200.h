@@ -153,6 +153,18 @@ int bm_adjoint_rk4(bm_ctx *ctx, int steps, int ckpt_every, const double *target,
 /* Allocate and build everything for the current configuration now (kernels, tiles). */
 int bm_prepare(bm_ctx *ctx);
 
+/* Evaluation speedup, the reference's `evalspeedup` command (Boris/Simulation.cpp:551,
+ * Boris/DemagCUDA.cpp:106): level 0 off, 1 step, 2 linear, 3 quadratic, 4 cubic, 5 quartic,
+ * 6 quintic. The demag field is computed at the first evaluation of every RK4 step and saved
+ * without its self term; the other evaluations extrapolate it from the last `level` saved fields
+ * (polynomial in time) plus the self term of the current M, once that many are saved. RK4 only
+ * (bm_run gives BM_EUNSUPPORTED with RKDP54), one mesh per launch (no multilayered convolution or
+ * batching). Setting M drops the saved fields. */
+int bm_set_evalspeedup(bm_ctx *ctx, int level);
+/* Self-demagnetising coefficients -N (x, y, z) of one cell of size hx, hy, hz (DemagTFunc::SelfDemag,
+ * Boris/DemagTFunc_Self.cpp:6); host only. */
+int bm_self_demag(double hx, double hy, double hz, double *out3);
+
 /* Magnetization M (A/m, |M| = Ms), AoS doubles, 3 * n values. Replaces writes/reads of
  * MeshBase::M (VEC_VC<DBL3>, Boris/Mesh.h). Setting M un-primes RKDP54 as a restart does. */
 int bm_set_m(bm_ctx *ctx, int mesh, const double *M);

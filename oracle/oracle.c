@@ -29,6 +29,8 @@
  *   RKDP54                     Boris/DiffEqFM_Evals_RKDP54.cpp:9-260,
  *                              Boris/DiffEq_CommonBase_Iterate.cpp:1214 (FSAL, prime/restore)
  *   step control               Boris/DiffEq_CommonBase_Iterate.cpp:15 (SetAdaptiveTimeStep)
+ *   evaluation speedup (RK4)   Boris/DemagCUDA.cpp:106-470, Boris/DemagCUDA.cu:29-265,
+ *                              Boris/DiffEq_CommonBase_Iterate.cpp:1536,1639
  */
 #include "oracle.h"
 #include <stdlib.h>
@@ -1031,6 +1033,8 @@ typedef struct {
     double *Ms, *K1;         /* per-cell */
     double *M, *H, *sM1, *sEval[6];
     orc_demag *dm;
+    double *Hs[6];           /* evaluation speedup: saved demag fields minus the self term */
+    double self[3];          /* self-demag coefficients (-N) */
 } orc_mesh;
 
 struct orc_solver {
@@ -1046,6 +1050,10 @@ struct orc_solver {
     int primed;
     long accepted, rejected, evals;
     double last_lte;
+    /* evaluation speedup (DemagCUDA::UpdateField, Boris/DemagCUDA.cpp:106): level K = number of
+       saved fields, es_mode of the current evaluation (0 full, 1 full + save, 2 extrapolate) */
+    int es_level, es_saved, es_mode, es_slot;
+    double es_t[6], es_a[6];
 };
 
 static int fft_size(int n) { return n > 1 ? 2 * n : 1; }
@@ -1116,7 +1124,7 @@ void orc_solver_destroy(orc_solver *s)
     for (int q = 0; q < s->nmesh; q++) {
         orc_mesh *m = &s->m[q];
         free(m->Ms); free(m->K1); free(m->M); free(m->H); free(m->sM1);
-        for (int e = 0; e < 6; e++) free(m->sEval[e]);
+        for (int e = 0; e < 6; e++) { free(m->sEval[e]); free(m->Hs[e]); }
         orc_demag_destroy(m->dm);
     }
     free(s->m);
@@ -1176,6 +1184,20 @@ static void update_fields(orc_solver *s, orc_mesh *m)
             orc_mesh *mk = &s->m[s->ml_mesh[k]];
             if (mk == m) { for (size_t i = 0; i < 3 * n; i++) m->H[i] += s->ml_H[3 * off + i]; break; }
             off += (size_t)mk->n;
+        }
+    } else if ((d->modules & ORC_DEMAG) && s->es_mode == 1) {
+        /* Demag_EvalSpeedup_AddField_SubSelf (Boris/DemagCUDA.cu:46): add the new field, keep it
+           minus the self term */
+        double *Hs = m->Hs[s->es_slot];
+        memset(Hs, 0, sizeof(double) * 3 * n);
+        orc_demag_apply(m->dm, m->M, Hs, 1);
+        for (size_t i = 0; i < 3 * n; i++) { m->H[i] += Hs[i]; Hs[i] -= m->self[i % 3] * m->M[i]; }
+    } else if ((d->modules & ORC_DEMAG) && s->es_mode == 2) {
+        /* Demag_EvalSpeedup_AddExtrapField_AddSelf (Boris/DemagCUDA.cu:64-265) */
+        for (size_t i = 0; i < 3 * n; i++) {
+            double v = m->self[i % 3] * m->M[i];
+            for (int k = 0; k < s->es_level; k++) v += s->es_a[k] * m->Hs[k][i];
+            m->H[i] += v;
         }
     } else if (d->modules & ORC_DEMAG) orc_demag_apply(m->dm, m->M, m->H, 1);
     if (d->modules & ORC_IDMI) orc_field_idmi(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, m->M, d->A, d->D, m->Ms, m->H);
@@ -1240,10 +1262,58 @@ static int adaptive_dt(orc_solver *s, double lte)
     return 1;
 }
 
+/* Evaluation speedup for one RK4 evaluation (DemagCUDA::UpdateField, Boris/DemagCUDA.cpp:106-470,
+   with ODECommon_Base::Check_Step_Update / Get_EvalStep_Time, Boris/DiffEq_CommonBase_Iterate.cpp:
+   1536,1639, dTspeedup linked to dT): the first evaluation of a step computes the field and saves it
+   (into the next free slot, then into the slot holding the earliest time); the others compute it in
+   full until `level` fields are saved, then extrapolate with the Lagrange polynomial through the
+   saved times. */
+static void es_prepare(orc_solver *s, int stage)
+{
+    static const double c_rk4[4] = {0.0, 0.5, 0.5, 1.0};
+    s->es_mode = 0;
+    if (!s->es_level) return;
+    int K = s->es_level;
+    double t = s->time + s->dT * c_rk4[stage];
+    if (stage == 0) {
+        int slot = 0;
+        if (s->es_saved < K) slot = s->es_saved++;
+        else for (int k = 1; k < K; k++) if (s->es_t[k] < s->es_t[slot]) slot = k;
+        s->es_t[slot] = t;
+        s->es_slot = slot;
+        s->es_mode = 1;
+    } else if (s->es_saved >= K) {
+        for (int k = 0; k < K; k++) {
+            double a = 1.0;
+            for (int j = 0; j < K; j++)
+                if (j != k) a *= (t - s->es_t[j]) / (s->es_t[k] - s->es_t[j]);
+            s->es_a[k] = a;
+        }
+        s->es_mode = 2;
+    }
+}
+
+int orc_solver_set_evalspeedup(orc_solver *s, int level)
+{
+    if (level < 0 || level > 6 || s->ml) return 1;
+    s->es_level = level;
+    s->es_saved = 0;
+    for (int q = 0; q < s->nmesh; q++) {
+        orc_mesh *m = &s->m[q];
+        orc_selfdemag(m->d.hx, m->d.hy, m->d.hz, m->self);
+        for (int k = 0; k < 6; k++) {
+            free(m->Hs[k]);
+            m->Hs[k] = k < level ? (double *)calloc(3 * (size_t)m->n, sizeof(double)) : NULL;
+        }
+    }
+    return 0;
+}
+
 static void rk4_step(orc_solver *s)
 {
     double dT = s->dT;
     for (int stage = 0; stage < 4; stage++) {
+        es_prepare(s, stage);
         update_all_fields(s);
         for (int q = 0; q < s->nmesh; q++) {
             orc_mesh *m = &s->m[q];

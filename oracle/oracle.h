@@ -78,6 +78,8 @@ int orc_get_m(orc_solver *s, int mesh, double *M);
 /* one multilayered convolution (orc_ml, below) replaces the per-mesh demag of every mesh with
  * ORC_DEMAG; o3 = origin of every solver mesh (3 per mesh) */
 int orc_solver_set_multilayer(orc_solver *s, const double *o3, int mode, const int *ncommon);
+/* Evaluation speedup of RK4 (level 0 off, 1 step .. 6 quintic): demag extrapolated from saved fields. */
+int orc_solver_set_evalspeedup(orc_solver *s, int level);
 /* effective field at the current M and time; H has 3n doubles */
 int orc_compute_heff(orc_solver *s, int mesh, double *H);
 /* advance until `steps` more steps are accepted */

@@ -82,6 +82,7 @@ def oracle():
         L.orc_ml_transfer.argtypes = [P, I, DP, DP, DP, DP]
         L.orc_ml_destroy.argtypes = [P]
         L.orc_solver_set_multilayer.argtypes = [P, DP, I, IP]
+        L.orc_solver_set_evalspeedup.argtypes = [P, I]
         L.orc_adjoint_rk4.argtypes = [ctypes.POINTER(MeshDesc), DP, DP, I, D, DP, DP, DP, DP]
         _orc = L
     return _orc
@@ -249,6 +250,9 @@ class OracleSolver:
         self._keep += [o3, nc]
         rc = oracle().orc_solver_set_multilayer(P(self.h), dp(o3), mode, ip(nc) if nc is not None else None)
         assert rc == 0
+
+    def evalspeedup(self, level):
+        assert oracle().orc_solver_set_evalspeedup(P(self.h), int(level)) == 0
 
     def set_m(self, M, mesh=0):
         a = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
