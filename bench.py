@@ -220,6 +220,8 @@ def make_ctx(bm, cfg, device, precision):
     c.setode(cfg["eval"], cfg["dt"])
     if cfg["eval"] == "RKDP54":
         c.astepctrl(cfg["tol"], 2.0, 1e-15, 3e-12)
+    if cfg.get("evalspeedup"):
+        c.evalspeedup(cfg["evalspeedup"])
     return c
 
 
@@ -563,6 +565,17 @@ def main():
                                    "step_frac_of_peak": pb / (bx["ms_per_step"] * 1e-3) / 1e9 / peak}
             except Exception as e:
                 out["batching"] = {"error": str(e)}
+        # evaluation speedup: the same film under RK4 (dt 1e-14), plain and with the demag field
+        # extrapolated quadratically between steps
+        if not ml and args.config == "film3d_512x512x16":
+            try:
+                rk = dict(cfg, eval="RK4")
+                plain = quick_rate(bm, rk, bm.MIXED, extra_steps, args.warmup, local)
+                es3 = quick_rate(bm, dict(rk, evalspeedup=3), bm.MIXED, extra_steps + 3, args.warmup, local)
+                out["evalspeedup"] = {"workload": "film3d_512x512x16 RK4 dt 1e-14", "rk4_plain": plain,
+                                      "rk4_quadratic": es3, "speedup": es3["value"] / plain["value"]}
+            except Exception as e:
+                out["evalspeedup"] = {"error": str(e)}
         # the differentiation workload: adjoint / forward device time
         if not ml and args.config == "film3d_512x512x16":
             try:

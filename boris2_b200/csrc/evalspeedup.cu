@@ -26,34 +26,42 @@ __device__ __forceinline__ int es_slot(const StepState *st)
     return slot;
 }
 
-int es_grid(long long n)
+// grid: x covers one component plane (capped, grid-stride), y = the 3 components
+dim3 es_grid(long long plane)
 {
-    long long b = (n + 255) / 256;
-    long long cap = 148LL * 8;
-    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+    long long b = (plane + 255) / 256;
+    long long cap = 148LL * 4;
+    return dim3((unsigned)(b < cap ? (b < 1 ? 1 : b) : cap), 3);
+}
+
+__device__ __forceinline__ double es_coef(int c, double c0, double c1, double c2)
+{
+    return c == 0 ? c0 : (c == 1 ? c1 : c2);
 }
 
 template <typename T>
-__global__ void k_es_pre(const cpx<T> *__restrict__ S1, cpx<T> *__restrict__ G, long long plane, double c0, double c1,
-                         double c2, const StepState *st)
+__global__ void __launch_bounds__(256) k_es_pre(const cpx<T> *__restrict__ S1, cpx<T> *__restrict__ G, long long plane,
+                                                double c0, double c1, double c2, const StepState *st)
 {
-    cpx<T> *g = G + (long long)es_slot(st) * 3 * plane;
-    const long long n = 3 * plane;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int c = (int)(i / plane);
-        T f = (T)(c == 0 ? c0 : (c == 1 ? c1 : c2));
-        cpx<T> v = S1[i];
+    const int c = blockIdx.y;
+    const T f = (T)es_coef(c, c0, c1, c2);
+    const cpx<T> *src = S1 + c * plane;
+    cpx<T> *g = G + ((long long)es_slot(st) * 3 + c) * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+        cpx<T> v = src[i];
         g[i] = mk<T>(f * v.x, f * v.y);
     }
 }
 
 template <typename T>
-__global__ void k_es_post(const cpx<T> *__restrict__ S1, cpx<T> *__restrict__ G, long long plane, const StepState *st)
+__global__ void __launch_bounds__(256) k_es_post(const cpx<T> *__restrict__ S1, cpx<T> *__restrict__ G, long long plane,
+                                                 const StepState *st)
 {
-    cpx<T> *g = G + (long long)es_slot(st) * 3 * plane;
-    const long long n = 3 * plane;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        cpx<T> h = S1[i], s = g[i];
+    const int c = blockIdx.y;
+    const cpx<T> *src = S1 + c * plane;
+    cpx<T> *g = G + ((long long)es_slot(st) * 3 + c) * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+        cpx<T> h = src[i], s = g[i];
         g[i] = mk<T>(h.x - s.x, h.y - s.y);
     }
 }
@@ -68,8 +76,8 @@ __global__ void k_es_commit(StepState *st)
 }
 
 template <typename T>
-__global__ void k_es_extrap(cpx<T> *__restrict__ S1, const cpx<T> *__restrict__ G, long long plane, double c0, double c1,
-                            double c2, const StepState *st, double c_eval)
+__global__ void __launch_bounds__(256) k_es_extrap(cpx<T> *__restrict__ S1, const cpx<T> *__restrict__ G, long long plane,
+                                                   double c0, double c1, double c2, const StepState *st, double c_eval)
 {
     const int K = st->es_K;
     if (st->es_saved < K) return;
@@ -86,18 +94,23 @@ __global__ void k_es_extrap(cpx<T> *__restrict__ S1, const cpx<T> *__restrict__ 
         }
         a[k] = (T)w;
     }
-    const long long n = 3 * plane;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int c = (int)(i / plane);
-        T f = (T)(c == 0 ? c0 : (c == 1 ? c1 : c2));
-        cpx<T> m = S1[i];
+    const int c = blockIdx.y;
+    const T f = (T)es_coef(c, c0, c1, c2);
+    cpx<T> *dst = S1 + c * plane;
+    const long long slot_stride = 3 * plane;
+    const cpx<T> *g = G + c * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+        cpx<T> m = dst[i];
         T x = f * m.x, y = f * m.y;
-        for (int k = 0; k < K; k++) {
-            cpx<T> g = G[(long long)k * n + i];
-            x += a[k] * g.x;
-            y += a[k] * g.y;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            if (k < K) {
+                cpx<T> v = g[k * slot_stride + i];
+                x += a[k] * v.x;
+                y += a[k] * v.y;
+            }
         }
-        S1[i] = mk<T>(x, y);
+        dst[i] = mk<T>(x, y);
     }
 }
 
@@ -106,14 +119,14 @@ __global__ void k_es_extrap(cpx<T> *__restrict__ S1, const cpx<T> *__restrict__ 
 template <typename T>
 int launch_es_pre(const cpx<T> *S1, cpx<T> *G, long long plane, const double *cs, const StepState *st, cudaStream_t s)
 {
-    k_es_pre<T><<<es_grid(3 * plane), 256, 0, s>>>(S1, G, plane, cs[0], cs[1], cs[2], st);
+    k_es_pre<T><<<es_grid(plane), 256, 0, s>>>(S1, G, plane, cs[0], cs[1], cs[2], st);
     return (int)cudaGetLastError();
 }
 
 template <typename T>
 int launch_es_post(const cpx<T> *S1, cpx<T> *G, long long plane, const StepState *st, cudaStream_t s)
 {
-    k_es_post<T><<<es_grid(3 * plane), 256, 0, s>>>(S1, G, plane, st);
+    k_es_post<T><<<es_grid(plane), 256, 0, s>>>(S1, G, plane, st);
     return (int)cudaGetLastError();
 }
 
@@ -127,7 +140,7 @@ template <typename T>
 int launch_es_extrap(cpx<T> *S1, const cpx<T> *G, long long plane, const double *cs, const StepState *st, double c_eval,
                      cudaStream_t s)
 {
-    k_es_extrap<T><<<es_grid(3 * plane), 256, 0, s>>>(S1, G, plane, cs[0], cs[1], cs[2], st, c_eval);
+    k_es_extrap<T><<<es_grid(plane), 256, 0, s>>>(S1, G, plane, cs[0], cs[1], cs[2], st, c_eval);
     return (int)cudaGetLastError();
 }
 
