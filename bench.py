@@ -49,6 +49,10 @@ def batch_systems(nsys=256, seed=3):
 CONFIGS = {
     "film3d_512x512x16": dict(n=(512, 512, 16), h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, K1=5e5, D=1.5e-3,
                               alpha=0.1, modules=1 | 4 | 8 | 16, eval="RKDP54", dt=1e-14, tol=1e-5, init="tilt"),
+    # the same film under RK4 with the demag field extrapolated quadratically between steps
+    "film3d_512x512x16_rk4_es3": dict(n=(512, 512, 16), h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, K1=5e5,
+                                      D=1.5e-3, alpha=0.1, modules=1 | 4 | 8 | 16, eval="RK4", dt=1e-14,
+                                      tol=1e-5, init="tilt", evalspeedup=3),
     # the same film at half thickness: the small case for full ncu captures of the stage kernel
     "film3d_512x512x8": dict(n=(512, 512, 8), h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, K1=5e5, D=1.5e-3,
                              alpha=0.1, modules=1 | 4 | 8 | 16, eval="RKDP54", dt=1e-14, tol=1e-5, init="tilt"),

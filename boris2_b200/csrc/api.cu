@@ -152,6 +152,9 @@ struct bm_ctx {
     int ml_nc[3] = {1, 1, 1};
     MLRun *ml = nullptr;
     int es_level = 0;           // evaluation speedup level (0 off, 1..6)
+    int es_phase = 0;           // step being captured: 1 while fields are still being saved, 2 extrapolating
+    cudaGraphExec_t gexec_es = nullptr;   // evaluation speedup: the extrapolating step (gexec saves)
+    cudaGraph_t graph_es = nullptr;
     bool es_reset = true;       // clear the saved fields at the next state upload
 };
 
@@ -195,8 +198,12 @@ void drop_graph(bm_ctx *c)
 {
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->gexec_es) cudaGraphExecDestroy(c->gexec_es);
+    if (c->graph_es) cudaGraphDestroy(c->graph_es);
     c->gexec = nullptr;
     c->graph = nullptr;
+    c->gexec_es = nullptr;
+    c->graph_es = nullptr;
     c->graph_eval = -1;
     if (c->bp.dbuf) cudaFree(c->bp.dbuf);
     c->bp = BatchPlan();
@@ -1289,9 +1296,11 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
             }
             CKL(launch_es_commit(c->st, c->stream), "es_commit");
             (*count)++;
+        } else if (c->es_level > 0 && c->es_phase != 2) {
+            // too few fields saved yet: the full field
+            if (int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count)) return rc;
         } else if (c->es_level > 0) {
-            // full field while too few are saved, else the extrapolation
-            if (int rc = enqueue_fields<T>(c, BM_GATE_ES_FULL, min_buf[s], count)) return rc;
+            // the extrapolation in place of the y/z passes
             for (auto &m : c->meshes) {
                 if (!(m.modules & BM_DEMAG)) continue;
                 CKL(launch_es_extrap<T>((cpx<T> *)m.S1, (const cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c_eval[s],
@@ -1452,14 +1461,26 @@ int build_graph(bm_ctx *c)
         c->bp.next = 0;
         count = 0;
     }
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = (c->eval == BM_RKDP54) ? enqueue_rkdp_attempt<T>(c, &count) : enqueue_rk4_step<T>(c, &count);
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-    if (e != cudaSuccess) return fail(BM_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    c->graph = g;
-    CK(cudaGraphInstantiate(&c->gexec, g, 0));
+    // evaluation speedup: one graph for the steps that still save fields, one for the extrapolating steps
+    const bool es = c->es_level > 0 && c->eval == BM_RK4;
+    for (int phase = 1; phase <= (es ? 2 : 1); phase++) {
+        c->es_phase = es ? phase : 0;
+        count = 0;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = (c->eval == BM_RKDP54) ? enqueue_rkdp_attempt<T>(c, &count) : enqueue_rk4_step<T>(c, &count);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->es_phase = 0;
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return fail(BM_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        if (phase == 1) {
+            c->graph = g;
+            CK(cudaGraphInstantiate(&c->gexec, g, 0));
+        } else {
+            c->graph_es = g;
+            CK(cudaGraphInstantiate(&c->gexec_es, g, 0));
+        }
+    }
     c->graph_eval = c->eval;
     c->kernels_per_step = count;
     return 0;
@@ -1484,7 +1505,16 @@ int run_T(bm_ctx *c, int steps)
     long long guard = 0;
     while (c->host_st.accepted < target) {
         long long k = target - c->host_st.accepted;
-        for (long long i = 0; i < k; i++) CK(cudaGraphLaunch(c->gexec, c->stream));
+        // evaluation speedup: every step saves one more field (up to es_K) at its first evaluation;
+        // a step whose save brings the count to es_K already extrapolates its other evaluations, so
+        // gexec (full evaluations) runs while fewer than es_K - 1 are saved at the step start
+        long long warm = k;
+        if (c->gexec_es) {
+            long long need = (long long)c->host_st.es_K - 1 - c->host_st.es_saved;
+            warm = need > 0 ? (need < k ? need : k) : 0;
+        }
+        for (long long i = 0; i < warm; i++) CK(cudaGraphLaunch(c->gexec, c->stream));
+        for (long long i = warm; i < k; i++) CK(cudaGraphLaunch(c->gexec_es, c->stream));
         guard += k;
         if ((rc = read_state(c))) return rc;
         if (c->eval == BM_RK4) break;

@@ -20,7 +20,6 @@ __device__ __forceinline__ bool gated_out(const StepState *st, int gate)
 {
     if (gate == BM_GATE_ALWAYS || st == nullptr) return false;
     if (gate == BM_GATE_ACCEPTED) return *((volatile const int *)&st->reject_flag) != 0;
-    if (gate == BM_GATE_ES_FULL) return *((volatile const int *)&st->es_saved) >= st->es_K;
     return *((volatile const int *)&st->need_restore) == 0;
 }
 

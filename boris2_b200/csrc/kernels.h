@@ -22,7 +22,6 @@ void bm_far_coeffs(double hx, double hy, double hz, double *out);
 #define BM_GATE_ALWAYS 0
 #define BM_GATE_ACCEPTED 1      // skip when the current attempt was rejected
 #define BM_GATE_RESTORE 2       // run only when a restore is pending
-#define BM_GATE_ES_FULL 3       // evaluation speedup: run only while fewer than es_K fields are saved
 
 // ---------------------------------------------------------------- y / z passes
 template <typename T>
