@@ -74,6 +74,9 @@ CONFIGS = {
     # 256 independent films of uneven sizes advanced together, one launch per pass over all of them
     "batch256": dict(meshes=batch_systems(), A=1.3e-11, D=0.0, alpha=0.1, eval="RK4", dt=5e-14, init="sphere",
                      batched=True),
+    # the batching workload with the demag field extrapolated quadratically between steps
+    "batch256_es3": dict(meshes=batch_systems(), A=1.3e-11, D=0.0, alpha=0.1, eval="RK4", dt=5e-14, init="sphere",
+                         batched=True, evalspeedup=3),
     # the same stack at half the in-plane size (FFT 1024 x 1024 x 4): small case for ncu captures
     "multilayer_stack3_512": dict(meshes=[dict(n=(512, 512, 1), h=(2e-9, 2e-9, 1e-9), o=(0, 0, 0), Ms=1.4e6, K1=0.0,
                                                modules=1 | 2),

@@ -821,8 +821,8 @@ int prepare(bm_ctx *c)
     if (c->ready) return 0;
     if (c->meshes.empty()) return fail(BM_ESTATE, "no mesh");
     if (c->batched && c->ml_mode >= 0) return fail(BM_EUNSUPPORTED, "batched meshes with a multilayered convolution");
-    if (c->es_level > 0 && (c->ml_mode >= 0 || (c->batched && c->meshes.size() > 1)))
-        return fail(BM_EUNSUPPORTED, "evaluation speedup with a multilayered convolution or batched meshes");
+    if (c->es_level > 0 && c->ml_mode >= 0)
+        return fail(BM_EUNSUPPORTED, "evaluation speedup with a multilayered convolution");
     CK(cudaSetDevice(c->device));
     int rc = (c->precision == BM_FP64) ? prepare_T<double>(c) : prepare_T<float>(c);
     if (rc) return rc;
@@ -1281,28 +1281,33 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
     static const int min_buf[4] = {0, 2, 3, 2};
     static const double c_eval[4] = {0.0, 0.5, 0.5, 1.0};   // RK4 evaluation times (Get_EvalStep_Time)
     for (int s = 0; s < 4; s++) {
+        // the evaluation-speedup kernels are not batched: nothing to record in the batched plan's
+        // collect pass (which must launch nothing)
+        const bool es_launch = !c->bp.collect;
         if (c->es_level > 0 && s == 0) {
             // evaluation speedup: compute and save the field at the first evaluation of the step
             for (auto &m : c->meshes) {
-                if (!(m.modules & BM_DEMAG)) continue;
+                if (!(m.modules & BM_DEMAG) || !es_launch) continue;
                 CKL(launch_es_pre<T>((const cpx<T> *)m.S1, (cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c->stream), "es_pre");
                 (*count)++;
             }
             if (int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count)) return rc;
             for (auto &m : c->meshes) {
-                if (!(m.modules & BM_DEMAG)) continue;
+                if (!(m.modules & BM_DEMAG) || !es_launch) continue;
                 CKL(launch_es_post<T>((const cpx<T> *)m.S1, (cpx<T> *)m.G, es_plane(m), c->st, c->stream), "es_post");
                 (*count)++;
             }
-            CKL(launch_es_commit(c->st, c->stream), "es_commit");
-            (*count)++;
+            if (es_launch) {
+                CKL(launch_es_commit(c->st, c->stream), "es_commit");
+                (*count)++;
+            }
         } else if (c->es_level > 0 && c->es_phase != 2) {
             // too few fields saved yet: the full field
             if (int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count)) return rc;
         } else if (c->es_level > 0) {
             // the extrapolation in place of the y/z passes
             for (auto &m : c->meshes) {
-                if (!(m.modules & BM_DEMAG)) continue;
+                if (!(m.modules & BM_DEMAG) || !es_launch) continue;
                 CKL(launch_es_extrap<T>((cpx<T> *)m.S1, (const cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c_eval[s],
                                         c->stream), "es_extrap");
                 (*count)++;
@@ -1447,11 +1452,19 @@ int build_graph(bm_ctx *c)
 {
     drop_graph(c);
     int count = 0;
+    // evaluation speedup: one graph for the steps that still save fields, one for the extrapolating steps
+    const bool es = c->es_level > 0 && c->eval == BM_RK4;
     if (c->batched && c->meshes.size() > 1) {
-        // pass 1: collect the batched launches' argument blocks and work lists, upload them
+        // pass 1: collect the batched launches' argument blocks and work lists (of both steps, in
+        // capture order, with evaluation speedup), upload them
         c->bp = BatchPlan();
         c->bp.collect = true;
-        int rc = (c->eval == BM_RKDP54) ? enqueue_rkdp_attempt<T>(c, &count) : enqueue_rk4_step<T>(c, &count);
+        int rc = 0;
+        for (int phase = 1; phase <= (es ? 2 : 1) && !rc; phase++) {
+            c->es_phase = es ? phase : 0;
+            rc = (c->eval == BM_RKDP54) ? enqueue_rkdp_attempt<T>(c, &count) : enqueue_rk4_step<T>(c, &count);
+        }
+        c->es_phase = 0;
         c->bp.collect = false;
         if (rc) return rc;
         if (!c->bp.hbuf.empty()) {
@@ -1461,8 +1474,6 @@ int build_graph(bm_ctx *c)
         c->bp.next = 0;
         count = 0;
     }
-    // evaluation speedup: one graph for the steps that still save fields, one for the extrapolating steps
-    const bool es = c->es_level > 0 && c->eval == BM_RK4;
     for (int phase = 1; phase <= (es ? 2 : 1); phase++) {
         c->es_phase = es ? phase : 0;
         count = 0;

@@ -75,3 +75,30 @@ def test_evalspeedup_refusals(bm):
     c.evalspeedup(0)
     c.run(2)                                        # and the context stays usable
     c.close()
+
+
+def test_evalspeedup_batched_uneven_systems(bm):
+    """Batched uneven meshes (2D and 3D, 3 * 2^k FFT lengths) with quadratic extrapolation follow the
+    oracle (FP64, 1e-9 of each mesh's Ms) and the same meshes run one launch per mesh."""
+    from test_gpu_batch import _descs, _ctx, _init
+    descs = _descs(modules=1 | 2 | 16)
+    M0 = _init(descs, "sphere")
+    s = OracleSolver(descs, evaluation=0, dt=5e-14)
+    s.evalspeedup(3)
+    for q, M in enumerate(M0):
+        s.set_m(M, q)
+    s.run(12)
+    out = []
+    for batched in (True, False):
+        c = _ctx(bm, "fp64", batched, descs, "RK4", 5e-14)
+        c.evalspeedup(3)
+        for q, M in enumerate(M0):
+            c.set_m(M, q)
+        assert c.run(12)["accepted"] == 12
+        out.append([c.get_m(q) for q in range(len(descs))])
+        c.close()
+    err = max(np.abs(a - s.get_m(q)).max() / d["Ms"] for q, (a, d) in enumerate(zip(out[0], descs)))
+    assert err < 1e-9, err
+    same = max(np.abs(a - b).max() / d["Ms"] for a, b, d in zip(out[0], out[1], descs))
+    assert same < 1e-11, same
+
