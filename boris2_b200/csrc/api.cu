@@ -155,6 +155,9 @@ struct bm_ctx {
     int es_phase = 0;           // step being captured: 1 while fields are still being saved, 2 extrapolating
     cudaGraphExec_t gexec_es = nullptr;   // evaluation speedup: the extrapolating step (gexec saves)
     cudaGraph_t graph_es = nullptr;
+    EsMesh *es_tab = nullptr;   // batched meshes: device table for the one-launch extrapolation kernels
+    int es_nmesh = 0;
+    long long es_max_plane = 0;
     bool es_reset = true;       // clear the saved fields at the next state upload
 };
 
@@ -204,6 +207,10 @@ void drop_graph(bm_ctx *c)
     c->graph = nullptr;
     c->gexec_es = nullptr;
     c->graph_es = nullptr;
+    if (c->es_tab) cudaFree(c->es_tab);
+    c->es_tab = nullptr;
+    c->es_nmesh = 0;
+    c->es_max_plane = 0;
     c->graph_eval = -1;
     if (c->bp.dbuf) cudaFree(c->bp.dbuf);
     c->bp = BatchPlan();
@@ -1284,16 +1291,25 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
         // the evaluation-speedup kernels are not batched: nothing to record in the batched plan's
         // collect pass (which must launch nothing)
         const bool es_launch = !c->bp.collect;
+        const bool es_tab = c->es_tab != nullptr;
         if (c->es_level > 0 && s == 0) {
             // evaluation speedup: compute and save the field at the first evaluation of the step
+            if (es_tab && es_launch) {
+                CKL(launch_es_pre_batch<T>(c->es_tab, c->es_nmesh, c->es_max_plane, c->st, c->stream), "es_pre_batch");
+                (*count)++;
+            }
             for (auto &m : c->meshes) {
-                if (!(m.modules & BM_DEMAG) || !es_launch) continue;
+                if (!(m.modules & BM_DEMAG) || !es_launch || es_tab) continue;
                 CKL(launch_es_pre<T>((const cpx<T> *)m.S1, (cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c->stream), "es_pre");
                 (*count)++;
             }
             if (int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count)) return rc;
+            if (es_tab && es_launch) {
+                CKL(launch_es_post_batch<T>(c->es_tab, c->es_nmesh, c->es_max_plane, c->st, c->stream), "es_post_batch");
+                (*count)++;
+            }
             for (auto &m : c->meshes) {
-                if (!(m.modules & BM_DEMAG) || !es_launch) continue;
+                if (!(m.modules & BM_DEMAG) || !es_launch || es_tab) continue;
                 CKL(launch_es_post<T>((const cpx<T> *)m.S1, (cpx<T> *)m.G, es_plane(m), c->st, c->stream), "es_post");
                 (*count)++;
             }
@@ -1306,8 +1322,13 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
             if (int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count)) return rc;
         } else if (c->es_level > 0) {
             // the extrapolation in place of the y/z passes
+            if (es_tab && es_launch) {
+                CKL(launch_es_extrap_batch<T>(c->es_tab, c->es_nmesh, c->es_max_plane, c->st, c_eval[s], c->stream),
+                    "es_extrap_batch");
+                (*count)++;
+            }
             for (auto &m : c->meshes) {
-                if (!(m.modules & BM_DEMAG) || !es_launch) continue;
+                if (!(m.modules & BM_DEMAG) || !es_launch || es_tab) continue;
                 CKL(launch_es_extrap<T>((cpx<T> *)m.S1, (const cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c_eval[s],
                                         c->stream), "es_extrap");
                 (*count)++;
@@ -1454,6 +1475,22 @@ int build_graph(bm_ctx *c)
     int count = 0;
     // evaluation speedup: one graph for the steps that still save fields, one for the extrapolating steps
     const bool es = c->es_level > 0 && c->eval == BM_RK4;
+    if (es && c->batched && c->meshes.size() > 1) {
+        std::vector<EsMesh> tab;
+        for (auto &m : c->meshes) {
+            if (!(m.modules & BM_DEMAG)) continue;
+            EsMesh e;
+            e.S1 = m.S1; e.G = m.G; e.plane = es_plane(m);
+            for (int k = 0; k < 3; k++) e.cs[k] = m.es_cs[k];
+            tab.push_back(e);
+            if (e.plane > c->es_max_plane) c->es_max_plane = e.plane;
+        }
+        if (!tab.empty()) {
+            if (cudaMalloc(&c->es_tab, sizeof(EsMesh) * tab.size()) != cudaSuccess) return fail(BM_ENOMEM, "evaluation speedup table");
+            CK(cudaMemcpy(c->es_tab, tab.data(), sizeof(EsMesh) * tab.size(), cudaMemcpyHostToDevice));
+            c->es_nmesh = (int)tab.size();
+        }
+    }
     if (c->batched && c->meshes.size() > 1) {
         // pass 1: collect the batched launches' argument blocks and work lists (of both steps, in
         // capture order, with evaluation speedup), upload them

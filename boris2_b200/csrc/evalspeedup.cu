@@ -114,7 +114,113 @@ __global__ void __launch_bounds__(256) k_es_extrap(cpx<T> *__restrict__ S1, cons
     }
 }
 
+// batched: blockIdx.y = 3 * mesh + component; blocks beyond a mesh's plane do nothing
+dim3 es_grid_batch(long long max_plane, int nmesh)
+{
+    long long b = (max_plane + 255) / 256;
+    long long cap = 64;
+    return dim3((unsigned)(b < cap ? (b < 1 ? 1 : b) : cap), 3 * nmesh);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_es_pre_batch(const EsMesh *__restrict__ tab, const StepState *st)
+{
+    const EsMesh &e = tab[blockIdx.y / 3];
+    const int c = blockIdx.y % 3;
+    const long long plane = e.plane;
+    const T f = (T)e.cs[c];
+    const cpx<T> *src = (const cpx<T> *)e.S1 + c * plane;
+    cpx<T> *g = (cpx<T> *)e.G + ((long long)es_slot(st) * 3 + c) * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+        cpx<T> v = src[i];
+        g[i] = mk<T>(f * v.x, f * v.y);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_es_post_batch(const EsMesh *__restrict__ tab, const StepState *st)
+{
+    const EsMesh &e = tab[blockIdx.y / 3];
+    const int c = blockIdx.y % 3;
+    const long long plane = e.plane;
+    const cpx<T> *src = (const cpx<T> *)e.S1 + c * plane;
+    cpx<T> *g = (cpx<T> *)e.G + ((long long)es_slot(st) * 3 + c) * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+        cpx<T> h = src[i], s = g[i];
+        g[i] = mk<T>(h.x - s.x, h.y - s.y);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_es_extrap_batch(const EsMesh *__restrict__ tab, const StepState *st, double c_eval)
+{
+    const int K = st->es_K;
+    if (st->es_saved < K) return;
+    const double t = st->time + c_eval * st->dT;
+    T a[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        double w = 0.0;
+        if (k < K) {
+            w = 1.0;
+            for (int j = 0; j < K; j++)
+                if (j != k) w *= (t - st->es_t[j]) / (st->es_t[k] - st->es_t[j]);
+        }
+        a[k] = (T)w;
+    }
+    const EsMesh &e = tab[blockIdx.y / 3];
+    const int c = blockIdx.y % 3;
+    const long long plane = e.plane;
+    const T f = (T)e.cs[c];
+    cpx<T> *dst = (cpx<T> *)e.S1 + c * plane;
+    const long long slot_stride = 3 * plane;
+    const cpx<T> *g = (const cpx<T> *)e.G + c * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+        cpx<T> m = dst[i];
+        T x = f * m.x, y = f * m.y;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            if (k < K) {
+                cpx<T> v = g[k * slot_stride + i];
+                x += a[k] * v.x;
+                y += a[k] * v.y;
+            }
+        }
+        dst[i] = mk<T>(x, y);
+    }
+}
+
 }  // namespace
+
+template <typename T>
+int launch_es_pre_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, cudaStream_t s)
+{
+    k_es_pre_batch<T><<<es_grid_batch(max_plane, nmesh), 256, 0, s>>>(tab, st);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+int launch_es_post_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, cudaStream_t s)
+{
+    k_es_post_batch<T><<<es_grid_batch(max_plane, nmesh), 256, 0, s>>>(tab, st);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+int launch_es_extrap_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, double c_eval,
+                           cudaStream_t s)
+{
+    k_es_extrap_batch<T><<<es_grid_batch(max_plane, nmesh), 256, 0, s>>>(tab, st, c_eval);
+    return (int)cudaGetLastError();
+}
+
+template int launch_es_pre_batch<float>(const EsMesh *, int, long long, const StepState *, cudaStream_t);
+template int launch_es_pre_batch<double>(const EsMesh *, int, long long, const StepState *, cudaStream_t);
+template int launch_es_post_batch<float>(const EsMesh *, int, long long, const StepState *, cudaStream_t);
+template int launch_es_post_batch<double>(const EsMesh *, int, long long, const StepState *, cudaStream_t);
+template int launch_es_extrap_batch<float>(const EsMesh *, int, long long, const StepState *, double, cudaStream_t);
+template int launch_es_extrap_batch<double>(const EsMesh *, int, long long, const StepState *, double, cudaStream_t);
+
 
 template <typename T>
 int launch_es_pre(const cpx<T> *S1, cpx<T> *G, long long plane, const double *cs, const StepState *st, cudaStream_t s)

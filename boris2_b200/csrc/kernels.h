@@ -216,6 +216,19 @@ int launch_es_pre(const cpx<T> *S1, cpx<T> *G, long long plane, const double *cs
 template <typename T>
 int launch_es_post(const cpx<T> *S1, cpx<T> *G, long long plane, const StepState *st, cudaStream_t s);
 int launch_es_commit(StepState *st, cudaStream_t s);
+// all meshes of a batched context in one launch: a device table of one EsMesh per mesh with demag
+struct EsMesh {
+    void *S1, *G;
+    long long plane;
+    double cs[3];
+};
+template <typename T>
+int launch_es_pre_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, cudaStream_t s);
+template <typename T>
+int launch_es_post_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, cudaStream_t s);
+template <typename T>
+int launch_es_extrap_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, double c_eval,
+                           cudaStream_t s);
 template <typename T>
 int launch_es_extrap(cpx<T> *S1, const cpx<T> *G, long long plane, const double *cs, const StepState *st, double c_eval,
                      cudaStream_t s);

@@ -159,7 +159,8 @@ int bm_prepare(bm_ctx *ctx);
  * without its self term; the other evaluations extrapolate it from the last `level` saved fields
  * (polynomial in time) plus the self term of the current M, once that many are saved. RK4 only
  * (bm_run gives BM_EUNSUPPORTED with RKDP54), no multilayered convolution; with batched meshes the
- * y/z passes stay batched and the extrapolation runs per mesh. Setting M drops the saved fields. */
+ * y/z passes stay batched and the extrapolation covers every mesh in one launch. Setting M drops the
+ * saved fields. */
 int bm_set_evalspeedup(bm_ctx *ctx, int level);
 /* Self-demagnetising coefficients -N (x, y, z) of one cell of size hx, hy, hz (DemagTFunc::SelfDemag,
  * Boris/DemagTFunc_Self.cpp:6); host only. */
