@@ -88,6 +88,9 @@ CONFIGS = {
                                   multilayer=0),
 }
 MU0 = 1.256637061435916e-6
+# seconds of timed CPU-reference steps after which the reference arm stops (whole steps of the full
+# film take several seconds each on the host)
+REF_TIME_CAP = 150
 
 
 
@@ -315,43 +318,75 @@ def cpu_reference_ml(cfg, warmup, evals):
     return float(np.mean(times)), sample
 
 
-def cpu_reference_rate(cfg, sample_n=(256, 256, 16), evals=2, threads=None):
-    """Mcell-steps/s of the reference's compiled CPU demag (6 evaluations per RKDP54 step)."""
+def reference_film_solver(cfg, seed=7):
+    """The CPU reference of a single-film workload: the film's full field-and-integrate step with the
+    demag convolution and the exchange / iDMI stencils from the reference's own compiled sources
+    (oracle/_ref: Convolution<DemagKernel>, VEC_VC stencils, project FFTW-API shim) and Zeeman,
+    uniaxial anisotropy, LLG and the RK4 / RKDP54 stages and step control from the oracle
+    restatement (oracle/oracle.c), all OpenMP over the host's cores. Returns (solver, setup_s) or
+    (None, reason)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from oracle_libs import reference, dp, P
-    if threads:
-        os.environ["OMP_NUM_THREADS"] = str(threads)
-    R = reference()
-    if R is None:
-        return None
+    from oracle_libs import OracleSolver, reference
+    if reference() is None:
+        return None, "reference CPU build (oracle/_ref) not present"
+    t0 = time.perf_counter()
+    mesh = dict(n=cfg["n"], h=cfg["h"], Ms=cfg["Ms"], A=cfg["A"], D=cfg["D"], K1=cfg["K1"], alpha=cfg["alpha"],
+                grel=cfg.get("grel", 1.0), modules=cfg["modules"], Ha=cfg.get("Ha", (0, 0, 0)))
+    ev = 1 if cfg["eval"] == "RKDP54" else 0
+    s = OracleSolver([mesh], evaluation=ev, dt=cfg["dt"], tol=cfg.get("tol", 1e-5), dT_incr=2.0, dT_min=1e-15,
+                     dT_max=3e-12)
+    s.use_reference_fields(0)
+    s.set_m(init_m(cfg, seed))
+    return s, time.perf_counter() - t0
+
+
+def reference_film_steps(s, warmup, steps, time_cap):
+    """Time whole steps of the CPU reference solver: `warmup` untimed, then up to `steps` timed
+    ones, stopping early once `time_cap` seconds of timed steps have run. Returns (steps run,
+    seconds, field evaluations)."""
+    if warmup:
+        s.run(warmup)
+    st0 = s.run(0)
+    done, tsum = 0, 0.0
+    while done < steps and tsum < time_cap:
+        t0 = time.perf_counter()
+        s.run(1)
+        tsum += time.perf_counter() - t0
+        done += 1
+    st1 = s.run(0)
+    return done, tsum, st1["evals"] - st0["evals"]
+
+
+def cpu_reference_rate(cfg, steps=2):
+    """cpu_baseline of a single-film workload: whole steps of the CPU reference (reference_film_solver)
+    on the full film. Multilayer workloads: the reference's multilayered convolution alone on a
+    shrunk sample (cpu_reference_ml)."""
     if "meshes" in cfg:
-        dt, sample = cpu_reference_ml(cfg, 1, evals)
+        if "multilayer" not in cfg:
+            return {"error": "no CPU reference for batched independent meshes"}
+        dt, sample = cpu_reference_ml(cfg, 1, 2)
+        if dt is None:
+            return {"error": "reference CPU build (oracle/_ref) not present"}
         n = sum(a[0][0] * a[0][1] * a[0][2] for a in sample)
         per_step = 6 if cfg["eval"] == "RKDP54" else 4
         return {"value": n / (per_step * dt) / 1e6, "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": "reference CPU multilayered convolution (SDemag multilayer: DemagKernelCollection + weighted "
-                          "mesh transfer, project FFTW-API shim) on the meshes shrunk 4x in-plane %s, %d evaluations, "
-                          "%d per step; other field terms not timed" % ([a[0] for a in sample], evals, per_step),
-                "sec_per_eval": dt}
-    nz = min(sample_n[2], cfg["n"][2])
-    sn = (min(sample_n[0], cfg["n"][0]), min(sample_n[1], cfg["n"][1]), nz)
-    ncell = sn[0] * sn[1] * sn[2]
-    sub = dict(cfg, n=sn)
-    M = np.ascontiguousarray(init_m(sub, 7).reshape(-1))
-    H = np.zeros_like(M)
-    h = R.ref_demag_create(sn[0], sn[1], sn[2], cfg["h"][0], cfg["h"][1], cfg["h"][2])
-    R.ref_demag_eval(P(h), dp(M), dp(H))          # warm-up
-    t0 = time.perf_counter()
-    for _ in range(evals):
-        R.ref_demag_eval(P(h), dp(M), dp(H))
-    dt = (time.perf_counter() - t0) / evals
-    R.ref_demag_destroy(P(h))
-    per_step = 6 if cfg["eval"] == "RKDP54" else 4
-    return {"value": ncell / (per_step * dt) / 1e6, "unit": "Mcell-steps/s", "cores": os.cpu_count(),
-            "kind": "reference",
-            "sample": "reference CPU Convolution<DemagKernel> (project FFTW-API shim) on %dx%dx%d cells of the same film, "
-                      "%d H_demag evaluations, %d per step; other field terms not timed" % (sn + (evals, per_step)),
-            "sec_per_eval": dt}
+                "sample": "reference CPU multilayered convolution alone (SDemag multilayer: DemagKernelCollection + "
+                          "weighted mesh transfer, project FFTW-API shim) on the meshes shrunk 4x in-plane %s, 2 "
+                          "evaluations, counted as %d per step; other field terms and stages not timed"
+                          % ([a[0] for a in sample], per_step), "sec_per_eval": dt}
+    s, setup = reference_film_solver(cfg)
+    if s is None:
+        return {"error": setup}
+    done, tsum, evals = reference_film_steps(s, 0, steps, 1e9)
+    s.close()
+    ncell = total_cells(cfg)
+    return {"value": ncell * done / tsum / 1e6, "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": "%d whole %s steps (%d field evaluations) of the full %s film: demag convolution and %s "
+                      "stencils from the reference's compiled sources (project FFTW-API shim), Zeeman, "
+                      "anisotropy, LLG and stages from the oracle restatement; setup (kernel build) %.1f s "
+                      "not timed" % (done, cfg["eval"], evals, "x".join(map(str, cfg["n"])),
+                                     "iDMI+exchange" if cfg["modules"] & 4 else "exchange", setup),
+            "sec_per_step": tsum / done}
 
 
 def dist_setup():
@@ -416,25 +451,28 @@ def main():
                        e2e={"value": v, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
             print(json.dumps(out))
             return
-        sn = (256, 256, min(16, cfg["n"][2])) if ncell > 256 * 256 * 16 else cfg["n"]
-        sub = dict(cfg, n=sn)
-        M = np.ascontiguousarray(init_m(sub, 7).reshape(-1))
-        H = np.zeros_like(M)
-        h = R.ref_demag_create(sn[0], sn[1], sn[2], cfg["h"][0], cfg["h"][1], cfg["h"][2])
-        for i in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            R.ref_demag_eval(P(h), dp(M), dp(H))
-            dt = time.perf_counter() - t0
-            if i >= args.warmup:
-                vals.append(dt * per_step)
-        R.ref_demag_destroy(P(h))
-        nsc = sn[0] * sn[1] * sn[2]
-        tstep = float(np.mean(vals))
-        v = nsc / tstep / 1e6
-        out = dict(base, impl="reference", value=v, ms_per_step=tstep * 1e3, dtype="f64",
+        # the whole film, whole steps: the reference's compiled demag convolution and exchange / iDMI
+        # stencils with the restated Zeeman, anisotropy, LLG and RK stages (reference_film_solver).
+        # One warm-up step (the host path has no kernels or graphs to build); timed steps stop at
+        # --steps or after REF_TIME_CAP seconds, and "steps" reports the number actually run.
+        solver, setup = reference_film_solver(cfg)
+        if solver is None:
+            print(json.dumps({"impl": "reference", "unavailable": setup}))
+            return
+        done, tsum, evals = reference_film_steps(solver, min(args.warmup, 1), args.steps, REF_TIME_CAP)
+        solver.close()
+        tstep = tsum / done
+        v = ncell / tstep / 1e6
+        sample = ("each step = one whole %s step (%d field evaluations in %d steps) of the full %s film: demag "
+                  "convolution and %s stencils from the reference's compiled sources (project FFTW-API shim), "
+                  "Zeeman, uniaxial anisotropy, LLG and stage updates from the oracle restatement; %d timed steps "
+                  "of %d asked (time cap %d s); kernel build %.1f s not timed"
+                  % (cfg["eval"], evals, done, "x".join(map(str, cfg["n"])),
+                     "iDMI+exchange" if cfg["modules"] & 4 else "exchange", done, args.steps, REF_TIME_CAP, setup))
+        out = dict(base, impl="reference", value=v, ms_per_step=tstep * 1e3, dtype="f64", steps=done,
+                   steps_requested=args.steps, warmup=min(args.warmup, 1),
                    cpu_baseline={"value": v, "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
-                                 "sample": "each step = %d H_demag evaluations of the reference CPU build on %dx%dx%d "
-                                           "cells of the same film (project FFTW-API shim)" % ((per_step,) + tuple(sn))},
+                                 "sample": sample},
                    e2e={"value": v, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
         print(json.dumps(out))
         return
@@ -517,11 +555,21 @@ def main():
                                        "frac": kbytes[5] / (kms[5] * 1e-3) / 1e9 / peak}
         tiles = {"zmid_ml_W": c.ml_tile()}
     else:
-        kms, kbytes = c.time_kernels(0, reps=20)
-        names = ["ymid2d" if cfg["n"][2] == 1 else "yfwd", "zmid", "yinv", "stage"]
-        dom = int(np.argmax(kms))
-        kernels = {names[i]: {"ms": kms[i], "GB/s": (kbytes[i] / (kms[i] * 1e-3) / 1e9 if kms[i] > 0 else None)}
-                   for i in range(4) if kms[i] > 0}
+        # every launch of a few eager steps timed one by one (the step graph's launches, buffers and
+        # arguments), summed per kernel kind with each launch's algorithmic bytes
+        tk = c.time_step(steps=3)
+        names = [k for k in tk if k != "other"]
+        kms = np.array([tk[k]["ms"] / tk[k]["launches"] for k in names])
+        kbytes = np.array([tk[k]["bytes"] / tk[k]["launches"] for k in names])
+        dom = int(np.argmax([tk[k]["ms"] for k in names]))
+        kernels = {k: {"ms_per_launch": tk[k]["ms"] / tk[k]["launches"], "launches": tk[k]["launches"],
+                       "GB/s": (tk[k]["bytes"] / (tk[k]["ms"] * 1e-3) / 1e9 if tk[k]["bytes"] else None)}
+                   for k in tk}
+        tot_b = sum(tk[k]["bytes"] for k in tk)
+        tot_ms = sum(tk[k]["ms"] for k in tk)
+        kernels["all_launches"] = {"ms": tot_ms, "GB/s": tot_b / (tot_ms * 1e-3) / 1e9,
+                                   "frac": tot_b / (tot_ms * 1e-3) / 1e9 / peak,
+                                   "timing": "3 eager steps, CUDA event after every launch"}
         tiles = c.tiles(0)
     achieved = kbytes[dom] / (kms[dom] * 1e-3) / 1e9
     tpc = TRAFFIC_PER_CELL.get(("multilayer" if ml else "film3d", names[dom]))
@@ -535,7 +583,10 @@ def main():
                roofline={"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
                          "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "algorithmic_bytes_per_launch": kbytes[dom],
-                         "launch_ms": kms[dom]},
+                         "launch_ms": kms[dom],
+                         "timing": ("launches inside eager steps of the workload (CUDA events on the "
+                                    "context's stream between launches)" if not (ml or cfg.get("batched"))
+                                    else "per-part launches (multilayer) or whole steps (batched)")},
                kernels=kernels,
                rkdp={"attempts": attempts, "accepted": steps_done, "dT": st["dT"]})
     if tiles:
@@ -591,7 +642,17 @@ def main():
                 out["adjoint"] = adjoint_rate(bm, bm.MIXED, local)
             except Exception as e:
                 out["adjoint"] = {"error": str(e)}
-        if not args.no_cpu_baseline:
+        # precision against FP64: the GPU FP64 plain form and the reference's CPU build, on the
+        # same seeded M, at the workload's full size
+        if not ml and not cfg.get("batched"):
+            try:
+                out["precision"] = precision_film(bm, cfg, local, with_reference=not args.no_cpu_baseline)
+                cb = out["precision"].pop("_cpu_baseline", None)
+                if cb is not None:
+                    out["cpu_baseline"] = cb
+            except Exception as e:
+                out["precision"] = {"error": str(e)}
+        if not args.no_cpu_baseline and "cpu_baseline" not in out:
             try:
                 out["cpu_baseline"] = cpu_reference_rate(cfg)
             except Exception as e:  # reported, not fatal
@@ -601,6 +662,73 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def rel_err(a, ref):
+    """max and RMS over cells of |a - ref| / max |ref| (vector norms per cell)."""
+    d = np.linalg.norm(np.asarray(a).reshape(-1, 3) - np.asarray(ref).reshape(-1, 3), axis=1)
+    s = np.linalg.norm(np.asarray(ref).reshape(-1, 3), axis=1).max()
+    return {"max": float(d.max() / s), "rms": float(np.sqrt(np.mean(d * d)) / s)}
+
+
+def precision_film(bm, cfg, device, with_reference=True, ref_steps=2, gpu_steps=1000):
+    """Errors of the mixed-precision path (and of the GPU FP64 plain form) against FP64 on the
+    workload's full film, from one seeded M:
+      h_demag            H_demag of M: mixed and GPU FP64 against the reference's CPU build
+                         (Convolution<DemagKernel>), and mixed against GPU FP64; relative to max |H_ref|
+      m_after_ref_steps  m after `ref_steps` whole steps of the workload's stepper from M: mixed and GPU
+                         FP64 against the CPU reference solver (reference_film_solver); |dm| per cell
+      m_after_gpu_steps  m after `gpu_steps` steps: mixed against GPU FP64, and their simulated times
+    Tolerances stated by the workload: 1e-5 on H_demag, 1e-4 on |dm|. The CPU reference steps are also
+    timed and returned as the cpu_baseline (key _cpu_baseline)."""
+    M = init_m(cfg, 4321)
+    ms = cfg["Ms"]
+    res = {"tolerance": {"h_demag_rel": 1e-5, "dm_abs": 1e-4}, "seed_m": 4321}
+    Hd, mref, mgpu, tgpu = {}, {}, {}, {}
+    for name, prec in (("mixed", bm.MIXED), ("fp64", bm.FP64)):
+        c = make_ctx(bm, cfg, device, prec)
+        c.set_m(M)
+        Hd[name] = c.demag_field()
+        c.set_m(M)
+        c.run(ref_steps)
+        mref[name] = c.get_m() / ms
+        c.set_m(M)
+        st = c.run(gpu_steps)
+        mgpu[name] = c.get_m() / ms
+        tgpu[name] = st["time"]
+        c.close()
+    res["h_demag"] = {"mixed_vs_fp64_gpu": rel_err(Hd["mixed"], Hd["fp64"])}
+    dmg = np.linalg.norm(mgpu["mixed"] - mgpu["fp64"], axis=1)
+    res["m_after_gpu_steps"] = {"steps": gpu_steps, "evaluation": cfg["eval"],
+                                "mixed_vs_fp64_gpu": {"max": float(dmg.max()), "rms": float(np.sqrt(np.mean(dmg ** 2)))},
+                                "time_s": {"mixed": tgpu["mixed"], "fp64": tgpu["fp64"]}}
+    if with_reference:
+        solver, setup = reference_film_solver(dict(cfg), seed=0)
+        if solver is None:
+            res["reference"] = {"error": setup}
+            return res
+        Href = solver.reference_hdemag(M)
+        res["h_demag"]["mixed_vs_reference_cpu"] = rel_err(Hd["mixed"], Href)
+        res["h_demag"]["fp64_gpu_vs_reference_cpu"] = rel_err(Hd["fp64"], Href)
+        solver.set_m(M)
+        done, tsum, evals = reference_film_steps(solver, 0, ref_steps, 1e9)
+        mr = solver.get_m() / ms
+        solver.close()
+        blk = {"steps": done, "evaluation": cfg["eval"]}
+        for name in ("mixed", "fp64"):
+            d = np.linalg.norm(mref[name] - mr, axis=1)
+            blk[name + "_vs_reference_cpu"] = {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d * d)))}
+        res["m_after_ref_steps"] = blk
+        ncell = total_cells(cfg)
+        res["_cpu_baseline"] = {
+            "value": ncell * done / tsum / 1e6, "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": "%d whole %s steps (%d field evaluations) of the full %s film from the precision block's M: "
+                      "demag convolution and %s stencils from the reference's compiled sources (project FFTW-API "
+                      "shim), Zeeman, anisotropy, LLG and stages from the oracle restatement; kernel build %.1f s "
+                      "not timed" % (done, cfg["eval"], evals, "x".join(map(str, cfg["n"])),
+                                     "iDMI+exchange" if cfg["modules"] & 4 else "exchange", setup),
+            "sec_per_step": tsum / done}
+    return res
 
 
 def quick_rate(bm, cfg, prec, steps, warmup, device, ml_timing=False):

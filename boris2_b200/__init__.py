@@ -41,7 +41,14 @@ _lib = None
 
 
 class BorisError(RuntimeError):
-    """A non-zero status from the C ABI."""
+    """A non-zero status from the C ABI; ``code`` is the status (BM_EINVAL ... BM_ENONFINITE)."""
+
+    def __init__(self, msg, code=None):
+        super().__init__(msg)
+        self.code = code
+
+
+OK, EINVAL, ECUDA, ENOMEM, ESTATE, EUNSUPPORTED, ENONFINITE = 0, 1, 2, 3, 4, 5, 6
 
 
 class Stats(ctypes.Structure):
@@ -84,6 +91,7 @@ _SIGS = {
     "bm_kernels_per_step": (_I, [_P, _IP]),
     "bm_run_timed": (_I, [_P, _I, ctypes.POINTER(Stats), _DP]),
     "bm_time_kernels": (_I, [_P, _I, _I, _DP, _DP]),
+    "bm_time_step": (_I, [_P, _I, _DP, _DP, _IP]),
     "bm_tiles": (_I, [_P, _I, _IP]),
     "bm_debug_kernels": (_I, [_P, _I, _DP]),
     "bm_debug_tensor": (_I, [_I, _I, _I, _I, _D, _D, _D, _DP]),
@@ -95,6 +103,7 @@ _SIGS = {
     "bm_ml_time_kernels": (_I, [_P, _I, _DP, _DP]),
     "bm_ml_tile": (_I, [_P, _IP]),
     "bm_set_batched": (_I, [_P, _I]),
+    "bm_set_memory_limit": (_I, [_P, ctypes.c_longlong]),
     "bm_adjoint_rk4": (_I, [_P, _I, _I, _DP, _I, _DP, _DP, _DP, _DP, _DP]),
     "bm_set_evalspeedup": (_I, [_P, _I]),
     "bm_self_demag": (_I, [_D, _D, _D, _DP]),
@@ -124,7 +133,7 @@ def lib():
 
 def _check(rc):
     if rc != 0:
-        raise BorisError("boris_b200 error %d: %s" % (rc, lib().bm_last_error().decode()))
+        raise BorisError("boris_b200 error %d: %s" % (rc, lib().bm_last_error().decode()), rc)
 
 
 def _dp(a):
@@ -263,6 +272,11 @@ class Context:
                                     ctypes.byref(loss), _dp(dMs), _dp(dK1), _dp(dHa), _dp(tm)))
         return loss.value, dMs, dK1, dHa[:3 * k].reshape(-1, 3), tuple(tm)
 
+    def set_memory_limit(self, nbytes):
+        """Device bytes the context may use (0: the free device memory); set-up refuses with
+        ENOMEM before allocating when its meshes need more."""
+        _check(lib().bm_set_memory_limit(self._h, int(nbytes)))
+
     def set_batched(self, on=True):
         """Advance all meshes with one launch per pass over a (mesh, tile) work list."""
         _check(lib().bm_set_batched(self._h, int(bool(on))))
@@ -376,6 +390,19 @@ class Context:
         by = np.zeros(4)
         _check(lib().bm_time_kernels(self._h, mesh, int(reps), _dp(ms), _dp(by)))
         return ms, by
+
+    TIME_KINDS = ("stage", "yfwd", "zmid", "yinv", "ymid2d", "other")
+
+    def time_step(self, steps=3):
+        """Run `steps` steps eagerly (the step graph's launches, timed one by one with CUDA events)
+        and return {kind: {"ms": summed device ms, "bytes": summed algorithmic bytes, "launches": n}}
+        for the kinds in TIME_KINDS that launched. The simulation advances."""
+        ms = np.zeros(6)
+        by = np.zeros(6)
+        nl = (ctypes.c_int * 6)()
+        _check(lib().bm_time_step(self._h, int(steps), _dp(ms), _dp(by), nl))
+        return {k: {"ms": float(ms[i]), "bytes": float(by[i]), "launches": int(nl[i])}
+                for i, k in enumerate(self.TIME_KINDS) if nl[i] > 0}
 
     def tiles(self, mesh=0):
         """Autotuned tile shapes: 2D y width, 3D y width and variant (1: radix-16 Stockham), z width,

@@ -123,6 +123,21 @@ struct BatchPlan {
     void *dbuf = nullptr;
 };
 
+// Per-launch timing of an eagerly enqueued step (bm_time_step): an event after every launch, the
+// launch's kernel kind and its algorithmic bytes.
+#define BM_TK_STAGE 0
+#define BM_TK_YFWD 1
+#define BM_TK_ZMID 2
+#define BM_TK_YINV 3
+#define BM_TK_YMID2D 4
+#define BM_TK_OTHER 5
+#define BM_TK_COUNT 6
+struct LaunchTimer {
+    std::vector<cudaEvent_t> ev;   // ev[0] before the first launch, ev[i + 1] after launch i
+    std::vector<int> kind;
+    std::vector<double> bytes;
+};
+
 }  // namespace
 
 struct bm_ctx {
@@ -159,6 +174,8 @@ struct bm_ctx {
     int es_nmesh = 0;
     long long es_max_plane = 0;
     bool es_reset = true;       // clear the saved fields at the next state upload
+    LaunchTimer *lt = nullptr;  // set while bm_time_step enqueues its eager steps
+    size_t mem_limit = 0;       // bm_set_memory_limit (0: the free device memory is the limit)
 };
 
 namespace {
@@ -823,6 +840,30 @@ int prepare_T(bm_ctx *c)
     return 0;
 }
 
+// Device bytes a context's meshes need (their own buffers; a multilayered convolution's common
+// grids and kernels come on top), and the largest transient scratch of a kernel-spectrum build.
+void plan_bytes(const bm_ctx *c, size_t elem, double *persistent, double *transient)
+{
+    double per = 0.0, tr = 0.0;
+    for (const Mesh &m : c->meshes) {
+        const double n = (double)m.nx * m.ny * m.nz;
+        const double Nx = 2.0 * nice_size(m.nx), Ny = 2.0 * nice_size(m.ny), Nz = m.nz > 1 ? 2.0 * nice_size(m.nz) : 1.0;
+        const double LX = Nx / 2, v3 = 3.0 * elem * n;
+        per += (4 + (c->eval == BM_RKDP54 ? 6 : 3) + 1) * v3 + 24.0 * n;
+        if (!m.Ms_map.empty()) per += elem * n;
+        if (!m.K1_map.empty()) per += elem * n;
+        if (m.modules & BM_DEMAG) {
+            const double s1 = 6.0 * elem * m.nz * m.ny * LX;
+            per += s1 * (1 + c->es_level);
+            if (m.nz > 1) per += 6.0 * elem * m.nz * Ny * LX;
+            per += 6.0 * elem * (LX + 1) * (Ny / 2 + 1) * (Nz / 2 + 1);
+            tr = std::max(tr, 48.0 * n + 16.0 * Nx * Ny * Nz);   // tensor octant + one FP64 transform grid
+        }
+    }
+    *persistent = per;
+    *transient = tr;
+}
+
 int prepare(bm_ctx *c)
 {
     if (c->ready) return 0;
@@ -831,12 +872,85 @@ int prepare(bm_ctx *c)
     if (c->es_level > 0 && c->ml_mode >= 0)
         return fail(BM_EUNSUPPORTED, "evaluation speedup with a multilayered convolution");
     CK(cudaSetDevice(c->device));
+    // refuse up front, before any allocation, when the meshes cannot fit: the free device memory,
+    // or the context's own limit (bm_set_memory_limit) when it is lower
+    {
+        double per = 0.0, tr = 0.0;
+        plan_bytes(c, c->precision == BM_FP64 ? sizeof(double) : sizeof(float), &per, &tr);
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        double avail = (double)fr;
+        const char *what = "free device memory";
+        if (c->mem_limit > 0 && (double)c->mem_limit < avail) { avail = (double)c->mem_limit; what = "the context's memory limit"; }
+        if (per + tr > avail) {
+            char msg[256];
+            snprintf(msg, sizeof(msg), "the meshes need %.1f MB of device memory (%.1f MB more while the kernels are built); "
+                     "%s is %.1f MB", per / 1e6, tr / 1e6, what, avail / 1e6);
+            return fail(BM_ENOMEM, msg);
+        }
+    }
     int rc = (c->precision == BM_FP64) ? prepare_T<double>(c) : prepare_T<float>(c);
     if (rc) return rc;
     c->ready = true;
     c->s1_dirty = true;
     c->es_reset = true;
     return upload_state(c);
+}
+
+// ------------------------------------------------------------------ per-launch timing records
+// Records an event after a launch (when bm_time_step is collecting) with its kind and bytes.
+void lt_mark(bm_ctx *c, int kind, double bytes)
+{
+    if (!c->lt) return;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, c->stream);
+    c->lt->ev.push_back(e);
+    c->lt->kind.push_back(kind);
+    c->lt->bytes.push_back(bytes);
+}
+
+// Algorithmic bytes of one stage-kernel launch: every array it must read once and write once
+// (the exchange stencil's neighbour reads are re-reads of M), from its arguments.
+template <typename T>
+double stage_alg_bytes(const StageArgs<T> &a)
+{
+    const double p = sizeof(T), v = 3.0 * p * (double)a.n;
+    const double s1 = 3.0 * a.nz * a.ny * (double)a.LX * sizeof(cpx<T>);
+    const bool fields = a.mode != BM_MODE_UPDATE;
+    double b = v;                                                   // Min
+    if (a.mode != BM_MODE_HEFF) {
+        if (a.Mbase && a.Mbase != a.Min) b += v;
+        b += a.nev * v;
+    }
+    if (a.Ms_map) b += p * (double)a.n;
+    if (fields && a.K1_map && (a.modules & BM_MOD_ANIUNI)) b += p * (double)a.n;
+    if (fields && (a.modules & BM_MOD_DEMAG) && a.S1) b += s1;      // demag spectrum rows, inverse x
+    if (fields && a.Hd) b += v;
+    if (a.mode == BM_MODE_HEFF) return b + v;                       // Hout
+    if (a.Hsave) b += v;
+    if (a.ev_out) b += v;
+    if (a.mode == BM_MODE_LTE) return b;
+    if (a.Ysave) b += v;
+    if (a.copy_to) b += v;
+    if (a.Mout) b += v;
+    if (a.do_xfwd && a.S1) b += s1;                                 // forward x of the new M
+    return b;
+}
+
+// Algorithmic bytes of the y / z passes of one mesh: spectra read once and written once, the
+// kernel spectra read once.
+double yz_alg_bytes(const Mesh &m, int kind, size_t p)
+{
+    const double cs = 2.0 * p;
+    const double s1 = 3.0 * m.nz * m.ny * (double)m.LX * cs, s2 = 3.0 * m.nz * m.Ny * (double)m.LX * cs;
+    const double kb = 6.0 * (m.LX + 1) * (m.Ny / 2 + 1) * (double)(m.Nz / 2 + 1) * p;
+    switch (kind) {
+    case BM_TK_YFWD: case BM_TK_YINV: return s1 + s2;
+    case BM_TK_ZMID: return 2.0 * s2 + kb;
+    case BM_TK_YMID2D: return 2.0 * s1 + 4.0 / 6.0 * kb;
+    default: return 0.0;
+    }
 }
 
 // ------------------------------------------------------------------ kernel argument builders
@@ -861,13 +975,17 @@ int enqueue_yz(bm_ctx *c, Mesh &m, int gate, int *count)
     YZArgs<T> a = yz_args<T>(c, m, gate);
     if (m.nz == 1) {
         CKL(launch_ymid2d<T>(a, c->stream), "ymid2d");
+        lt_mark(c, BM_TK_YMID2D, yz_alg_bytes(m, BM_TK_YMID2D, sizeof(T)));
         (*count)++;
     } else {
         CKL(launch_yfwd<T>(a, c->stream), "yfwd");
+        lt_mark(c, BM_TK_YFWD, yz_alg_bytes(m, BM_TK_YFWD, sizeof(T)));
         a.W = m.Wz;
         CKL(launch_zmid<T>(a, c->stream), "zmid");
+        lt_mark(c, BM_TK_ZMID, yz_alg_bytes(m, BM_TK_ZMID, sizeof(T)));
         a.W = m.Wy;
         CKL(launch_yinv<T>(a, c->stream), "yinv");
+        lt_mark(c, BM_TK_YINV, yz_alg_bytes(m, BM_TK_YINV, sizeof(T)));
         (*count) += 3;
     }
     return 0;
@@ -976,6 +1094,9 @@ int stage_multi(bm_ctx *c, std::vector<StageArgs<T>> &v, int *count)
     if (!c->batched || v.size() == 1) {
         for (auto &a : v) {
             CKL(launch_stage<T>(a, c->stream), "stage");
+            // a restore launch only works after a rejection: timed under "other", no bytes credited
+            if (a.gate == BM_GATE_RESTORE) lt_mark(c, BM_TK_OTHER, 0.0);
+            else lt_mark(c, BM_TK_STAGE, stage_alg_bytes(a));
             (*count)++;
         }
         return 0;
@@ -1549,6 +1670,8 @@ int run_T(bm_ctx *c, int steps)
     }
     int rc = read_state(c);
     if (rc) return rc;
+    if (c->host_st.error & BM_ERR_NONFINITE)
+        return fail(BM_ENONFINITE, "the state is not finite (NaN or infinity): set a new M before running");
     long long target = c->host_st.accepted + steps;
     long long guard = 0;
     while (c->host_st.accepted < target) {
@@ -1565,6 +1688,10 @@ int run_T(bm_ctx *c, int steps)
         for (long long i = warm; i < k; i++) CK(cudaGraphLaunch(c->gexec_es, c->stream));
         guard += k;
         if ((rc = read_state(c))) return rc;
+        if (c->host_st.error & BM_ERR_NONFINITE)
+            return fail(BM_ENONFINITE, c->eval == BM_RK4
+                                           ? "a step produced a non-finite M (NaN or infinity); its steps are counted"
+                                           : "a step produced a non-finite M (NaN or infinity); it was not accepted");
         if (c->eval == BM_RK4) break;
         if (guard > 100LL * steps + 1000) return fail(BM_ESTATE, "step control did not converge");
     }
@@ -1974,6 +2101,14 @@ int bm_set_astepctrl(bm_ctx *c, double err_fail, double dT_incr, double dT_min, 
     return 0;
 }
 
+int bm_set_memory_limit(bm_ctx *c, long long bytes)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (bytes < 0) return fail(BM_EINVAL, "memory limit < 0");
+    c->mem_limit = (size_t)bytes;
+    return 0;
+}
+
 int bm_set_batched(bm_ctx *c, int on)
 {
     if (int rc = check_ctx(c)) return rc;
@@ -2078,6 +2213,7 @@ int bm_set_m(bm_ctx *c, int mesh, const double *M)
     // drops the fields saved for the evaluation speedup
     if (int rc = read_state(c)) return rc;
     c->host_st.primed = 0;
+    c->host_st.error = 0;   // a new M clears a non-finite state
     c->es_reset = true;
     c->dt = c->host_st.dT;
     return upload_state(c);
@@ -2260,6 +2396,46 @@ int bm_run_timed(bm_ctx *c, int steps, bm_stats *out, double *device_ms)
 }  // extern "C"
 
 namespace {
+// Eager steps with an event after every launch: the launches, buffers and arguments of the
+// captured step graph, timed one by one on the context's stream.
+template <typename T>
+int time_step_T(bm_ctx *c, int steps, double *ms6, double *bytes6, int *launches6)
+{
+    for (int k = 0; k < BM_TK_COUNT; k++) { ms6[k] = 0.0; bytes6[k] = 0.0; launches6[k] = 0; }
+    if (c->batched && c->meshes.size() > 1) return fail(BM_EUNSUPPORTED, "bm_time_step: batched meshes are timed per step only");
+    if (c->ml) return fail(BM_EUNSUPPORTED, "bm_time_step: the multilayered convolution has bm_ml_time_kernels");
+    if (c->es_level > 0) return fail(BM_EUNSUPPORTED, "bm_time_step: evaluation speedup steps are timed per step only");
+    if (c->s1_dirty) {
+        int cnt = 0;
+        if (int rc = enqueue_prime<T>(c, &cnt)) return rc;
+        c->s1_dirty = false;
+    }
+    LaunchTimer lt;
+    cudaEvent_t e0 = nullptr;
+    CK(cudaEventCreate(&e0));
+    lt.ev.push_back(e0);
+    CK(cudaEventRecord(e0, c->stream));
+    c->lt = &lt;
+    int count = 0, rc = 0;
+    for (int i = 0; i < steps && !rc; i++)
+        rc = (c->eval == BM_RKDP54) ? enqueue_rkdp_attempt<T>(c, &count) : enqueue_rk4_step<T>(c, &count);
+    c->lt = nullptr;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (!rc && e == cudaSuccess) {
+        for (size_t i = 0; i < lt.kind.size(); i++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, lt.ev[i], lt.ev[i + 1]);
+            ms6[lt.kind[i]] += t;
+            bytes6[lt.kind[i]] += lt.bytes[i];
+            launches6[lt.kind[i]]++;
+        }
+    }
+    for (auto ev : lt.ev) cudaEventDestroy(ev);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(BM_ECUDA, std::string("bm_time_step: ") + cudaGetErrorString(e));
+    return read_state(c);
+}
+
 template <typename T>
 int time_kernels_T(bm_ctx *c, Mesh &m, int reps, double *ms4, double *bytes4)
 {
@@ -2298,20 +2474,24 @@ int time_kernels_T(bm_ctx *c, Mesh &m, int reps, double *ms4, double *bytes4)
             if (!rc) rc = timeit([&]() { return launch_yinv<T>(a, s); }, 2, s1 + s2);
         }
     }
-    // the stage kernel as RKDP54 stage 3 uses it: 3 earlier evaluations, writes rhs and next M
+    // the stage kernel as RKDP54 stage 3 uses it: stage input, step base and 3 earlier evaluations
+    // in five distinct arrays (copies of M), writes rhs and next M into two more
     T *tmp = nullptr;
-    if (!rc && cudaMalloc(&tmp, sizeof(T) * 6 * m.n) != cudaSuccess) rc = BM_ENOMEM;
+    if (!rc && cudaMalloc(&tmp, sizeof(T) * 3 * 7 * m.n) != cudaSuccess) rc = BM_ENOMEM;
+    for (int k = 0; k < 5 && !rc; k++)
+        if (cudaMemcpyAsync(tmp + 3 * k * m.n, m.buf[0], sizeof(T) * 3 * m.n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            rc = BM_ECUDA;
     if (!rc) {
         StageArgs<T> a = stage_args<T>(c, m);
         a.mode = BM_MODE_STAGE;
-        a.Min = (const T *)m.buf[0];
-        a.Mbase = (const T *)m.buf[0];
+        a.Min = tmp;
+        a.Mbase = tmp + 3 * m.n;
         a.nev = 3;
-        a.ev[0] = (const T *)m.buf[0]; a.ev[1] = (const T *)m.buf[0]; a.ev[2] = (const T *)m.buf[0];
+        a.ev[0] = tmp + 6 * m.n; a.ev[1] = tmp + 9 * m.n; a.ev[2] = tmp + 12 * m.n;
         a.cev[0] = a.cev[1] = a.cev[2] = 0.0;
         a.crhs = 0.0;
-        a.ev_out = tmp;
-        a.Mout = tmp + 3 * m.n;
+        a.ev_out = tmp + 15 * m.n;
+        a.Mout = tmp + 18 * m.n;
         double bytes = 3.0 * m.n * rs * (1 + 1 + 3 + 1 + 1);
         if (m.modules & BM_DEMAG) bytes += 2.0 * s1;
         if (a.Ms_map) bytes += m.n * rs;
@@ -2400,6 +2580,16 @@ int bm_ml_time_kernels(bm_ctx *c, int reps, double *ms6, double *bytes6)
     if (!c->ml) return fail(BM_ESTATE, "multilayered convolution is off");
     cudaSetDevice(c->device);
     return (c->precision == BM_FP64) ? ml_time_T<double>(c, reps, ms6, bytes6) : ml_time_T<float>(c, reps, ms6, bytes6);
+}
+
+int bm_time_step(bm_ctx *c, int steps, double *ms6, double *bytes6, int *launches6)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (!ms6 || !bytes6 || !launches6 || steps < 1) return fail(BM_EINVAL, "bm_time_step: bad arguments");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    return c->precision == BM_FP64 ? time_step_T<double>(c, steps, ms6, bytes6, launches6)
+                                   : time_step_T<float>(c, steps, ms6, bytes6, launches6);
 }
 
 int bm_time_kernels(bm_ctx *c, int mesh, int reps, double *ms4, double *bytes4)

@@ -60,6 +60,9 @@ __device__ __forceinline__ void cp_async_real(T *smem, const T *gmem, bool valid
 #define BM_MOD_ANIUNI 8
 #define BM_MOD_ZEEMAN 16
 
+// StepState.error bits (sticky until the next bm_set_m)
+#define BM_ERR_NONFINITE 1   // a stage produced a NaN or infinite M or error estimate
+
 // device-resident step state shared by all kernels of a solver
 struct StepState {
     double time, stagetime, dT, dT_last;

@@ -369,7 +369,10 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 m2 += (double)m[c] * (double)m[c];
             }
             double l = sqrt(d2) / sqrt(m2);
-            if (l != l) l = 1e300;   // NaN counts as a huge error so the step is rejected
+            if (!(l <= 1e300)) {     // NaN or infinite: a non-finite state, never accepted
+                l = 1e300;
+                atomicOr(&a.st->error, BM_ERR_NONFINITE);
+            }
             if (l > lmax) lmax = l;
 #pragma unroll
             for (int c = 0; c < 3; c++) (a.ev_out + cell)[c * n] = rhs[c];
@@ -397,6 +400,8 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         if (a.renorm) {
             T f = Ms / sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
             mn[0] *= f; mn[1] *= f; mn[2] *= f;
+            // the step's new state must be finite (the sum is non-finite if any component is)
+            if (!isfinite(mn[0] + mn[1] + mn[2]) && a.st) atomicOr(&a.st->error, BM_ERR_NONFINITE);
         }
         if (a.ev_out) {
 #pragma unroll
@@ -462,7 +467,19 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, u
         double lte = __longlong_as_double((long long)atomicAdd(&a.st->lte_bits, 0ull));
         st->attempts = st->attempts + 1;
         st->reject_flag = 0;
-        if (!st->primed) {
+        if (st->error) {
+            // a non-finite state: the step that produced it is taken back (restored at the next
+            // attempt) and the rest of this attempt is skipped, whatever dT is; the host stops
+            if (st->primed) {
+                st->time = st->time - st->dT;
+                st->stagetime = st->stagetime - st->dT;
+                st->accepted = st->accepted - 1;
+                st->rejected = st->rejected + 1;
+                st->need_restore = 1;
+            }
+            st->primed = 0;
+            st->reject_flag = 1;
+        } else if (!st->primed) {
             st->primed = 1;
         } else {
             st->dT_last = st->dT;

@@ -100,6 +100,15 @@ int bm_set_astepctrl(bm_ctx *ctx, double err_fail, double dT_incr, double dT_min
  * bm_set_multiconvolution. */
 int bm_set_batched(bm_ctx *ctx, int on);
 
+/* Device-memory limit of the context, in bytes (0, the default: the free device memory). Before it
+ * allocates anything, the set-up of a context compares the bytes its meshes need (every buffer plus
+ * the scratch of the kernel-spectrum build) with the lower of this limit and the free device memory
+ * and refuses with BM_ENOMEM, naming both figures, when they do not fit; the context stays usable
+ * (raise the limit or shrink the meshes and call again). The reference checks for room before it
+ * builds its kernels on the GPU and falls back to a CPU build (Boris/DemagKernelCUDA.cpp:357-369);
+ * this path has no CPU fallback, so it refuses. */
+int bm_set_memory_limit(bm_ctx *ctx, long long bytes);
+
 /* Precision: BM_FP64 or BM_MIXED (default BM_MIXED). Must be set before the first run. */
 int bm_set_precision(bm_ctx *ctx, int precision);
 
@@ -207,7 +216,12 @@ int bm_compute_heff(bm_ctx *ctx, int mesh, double *H);
 
 /* Advance until `steps` more steps are accepted. Replaces the AdvanceTime loop
  * (Boris/SuperMeshSimulation.cpp:84,122) over ODECommon_Base::Iterate[CUDA]
- * (Boris/DiffEq_CommonBase_Iterate.cpp:63, Boris/DiffEq_CommonBase_IterateCUDA.cpp:13). */
+ * (Boris/DiffEq_CommonBase_Iterate.cpp:63, Boris/DiffEq_CommonBase_IterateCUDA.cpp:13).
+ * A stage that produces a NaN or infinite M (or RKDP54 error estimate) sets a device flag that is
+ * read after every batch of steps: bm_run then returns BM_ENONFINITE. Under RKDP54 the step that
+ * produced the state is not accepted, whatever dT is; under RK4 the steps of the batch are counted.
+ * The flag stays set, and bm_run refuses, until bm_set_m gives a new M. (The reference has no such
+ * check: a NaN state propagates.) */
 int bm_run(bm_ctx *ctx, int steps, bm_stats *out);
 int bm_get_stats(bm_ctx *ctx, bm_stats *out);
 
@@ -231,6 +245,15 @@ int bm_run_timed(bm_ctx *ctx, int steps, bm_stats *out, double *device_ms);
  * 2 = yinv (3D), 3 = fused stage kernel (inverse x FFT, fields, LLG, update, forward x FFT).
  * Unused slots are 0. Leaves the spectrum buffers stale (the next run re-primes them). */
 int bm_time_kernels(bm_ctx *ctx, int mesh, int reps, double *ms4, double *bytes4);
+
+/* Run `steps` steps (RKDP54: attempts) of every mesh eagerly, with the launches, buffers and
+ * arguments of the captured step graph, recording a CUDA event after every launch, and report
+ * per kernel kind the summed device ms, the summed algorithmic bytes (what each launch must read
+ * and write once, from its arguments) and the launch count: [0] fused stage kernel, [1] y forward,
+ * [2] z pass, [3] y inverse, [4] 2D y pass, [5] other (restore launches, timed, no bytes). The
+ * simulation advances. Not for batched meshes, the multilayered convolution or the evaluation
+ * speedup (BM_EUNSUPPORTED). No counterpart in the reference (measurement). */
+int bm_time_step(bm_ctx *ctx, int steps, double *ms6, double *bytes6, int *launches6);
 
 /* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width (plus 100
  * when the 3D y passes use the radix-16 Stockham transform),
@@ -258,10 +281,12 @@ int bm_debug_fft(int device, int L, int howmany, int precision, int inverse, dou
  * place), on `stream` (a cudaStream_t; NULL for the default stream), unnormalised, with
  * exp(+2 pi i ...) when inverse != 0. It calls no cudaMalloc/cudaFree: its only scratch, the
  * twiddle table, lives in a fixed device array of 4096 complex doubles (64 KiB) that every GPU
- * loading the library keeps until exit, so L is limited to 1..4096 (2^p or 3*2^p). The first
- * call on a device looks up that array's device address; make that first call before any
- * stream capture. The table is rewritten by every call, so calls that overlap on the GPU
- * (different streams, or concurrent host threads) race on it and must be serialised. */
+ * loading the library keeps until exit, so L is limited to 1..4096 (2^p or 3*2^p). Every call
+ * made outside stream capture looks up that array's device address on `device`; a call under
+ * capture reuses the address of the last uncaptured call, so make the first call on a device
+ * before any stream capture (a captured first call gives BM_ESTATE). The caller's current
+ * device is restored on return. The table is rewritten by every call, so calls that overlap on
+ * the GPU (different streams, or concurrent host threads) race on it and must be serialised. */
 int bm_fft_noalloc(int device, int L, int howmany, int inverse, const double *in, double *out, void *stream);
 
 #ifdef __cplusplus

@@ -1035,6 +1035,8 @@ typedef struct {
     orc_demag *dm;
     double *Hs[6];           /* evaluation speedup: saved demag fields minus the self term */
     double self[3];          /* self-demag coefficients (-N) */
+    orc_field_fn hook;       /* caller's demag + exchange/iDMI terms, or NULL */
+    void *hook_user;
 } orc_mesh;
 
 struct orc_solver {
@@ -1177,7 +1179,13 @@ static void update_fields(orc_solver *s, orc_mesh *m)
     size_t n = (size_t)m->n;
     double Ha[3];
     applied_field(d, s->stagetime, Ha);
-    for (size_t i = 0; i < n; i++) { m->H[3 * i] = Ha[0]; m->H[3 * i + 1] = Ha[1]; m->H[3 * i + 2] = Ha[2]; }
+#pragma omp parallel for
+    for (long i = 0; i < (long)n; i++) { m->H[3 * i] = Ha[0]; m->H[3 * i + 1] = Ha[1]; m->H[3 * i + 2] = Ha[2]; }
+    if (m->hook) {
+        m->hook(m->hook_user, m->M, m->H);
+        if (d->modules & ORC_ANIUNI) orc_field_aniuni(m->n, m->M, m->Ms, m->K1, d->K2, d->ea, m->H);
+        return;
+    }
     if ((d->modules & ORC_DEMAG) && s->ml) {
         size_t off = 0;
         for (int k = 0; k < s->ml_nmesh; k++) {
@@ -1210,6 +1218,14 @@ static void update_all_fields(orc_solver *s)
     if (s->ml) update_ml(s);
     for (int q = 0; q < s->nmesh; q++) update_fields(s, &s->m[q]);
     s->evals++;
+}
+
+int orc_solver_set_field_hook(orc_solver *s, int q, orc_field_fn fn, void *user)
+{
+    if (q < 0 || q >= s->nmesh || s->ml || s->es_level) return 1;
+    s->m[q].hook = fn;
+    s->m[q].hook_user = user;
+    return 0;
 }
 
 int orc_compute_heff(orc_solver *s, int q, double *H)
@@ -1382,7 +1398,8 @@ static int rkdp_attempt(orc_solver *s)
     double dT = s->dT;
     for (int q = 0; q < s->nmesh; q++) {
         orc_mesh *m = &s->m[q];
-        for (size_t o = 0; o < 3 * (size_t)m->n; o++) {
+#pragma omp parallel for
+        for (long o = 0; o < 3 * (long)m->n; o++) {
             m->sM1[o] = m->M[o];
             m->M[o] += m->sEval[0][o] * (dT / 5);
         }

@@ -80,6 +80,12 @@ int orc_get_m(orc_solver *s, int mesh, double *M);
 int orc_solver_set_multilayer(orc_solver *s, const double *o3, int mode, const int *ncommon);
 /* Evaluation speedup of RK4 (level 0 off, 1 step .. 6 quintic): demag extrapolated from saved fields. */
 int orc_solver_set_evalspeedup(orc_solver *s, int level);
+/* Replace the demag and exchange / iDMI terms of one mesh by a caller's function that adds them
+ * into H (3n doubles) for the mesh's M; Zeeman, anisotropy, LLG and the stages stay the solver's.
+ * Used to drive the reference's own compiled field code (oracle/ref_harness.cpp) with this
+ * integrator for the CPU baseline. fn NULL restores the solver's own terms. */
+typedef void (*orc_field_fn)(void *user, const double *M, double *H);
+int orc_solver_set_field_hook(orc_solver *s, int mesh, orc_field_fn fn, void *user);
 /* effective field at the current M and time; H has 3n doubles */
 int orc_compute_heff(orc_solver *s, int mesh, double *H);
 /* advance until `steps` more steps are accepted */

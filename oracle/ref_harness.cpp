@@ -15,6 +15,11 @@
  *   ref_idmi           VEC_VC<DBL3>::delsq_nneu/grad_nneu/grad_neu (BorisLib/VEC_VC_Del.h:141,
  *                      BorisLib/VEC_VC_Grad.h:10,139) with the field formula of
  *                      iDMExchange::UpdateField (Boris/iDMExchange.cpp:97)
+ *   ref_film_fields_*  a persistent demag + exchange / iDMI field of one film for the CPU baseline:
+ *                      Convolution<.,DemagKernel>::Convolute (Boris/Convolution.h:659) added into H,
+ *                      then the stencils of ref_exchange / ref_idmi with uniform A, D, Ms over an
+ *                      OpenMP loop as Exch_6ngbr_Neu / iDMExchange::UpdateField run theirs
+ *                      (Boris/Exchange.cpp:108, Boris/iDMExchange.cpp:97)
  *   ref_tensor_shifted DemagTFunc::Calc{Diag,OffDiag}Tens3D_Shifted (Boris/DemagTFunc_Shifted.cpp:6,...)
  *                      and Calc{Diag,OffDiag}Tens2D_Shifted_Irregular (Boris/DemagTFunc_Irregular.cpp:4,121)
  *   ref_ml_*           the multilayered convolution: one Convolution<., DemagKernelCollection> per
@@ -233,6 +238,99 @@ int ref_idmi(int nx, int ny, int nz, double hx, double hy, double hz, const doub
     return 0;
 }
 
+
+/* The demag and exchange / iDMI terms of one film, kept across evaluations (kernels built once).
+ * modules: bit 1 demag, 2 exchange, 4 iDMI (exchange + DMI). ref_film_fields_add adds the terms
+ * into H for M (AoS), with the signature the oracle solver's field hook takes. */
+struct ref_film_s {
+    OracleDemag *od = nullptr;
+    VEC<DBL3> In, Out;
+    VEC_VC<DBL3> V;
+    int n = 0, modules = 0;
+    double A = 0, D = 0, Ms = 1;
+};
+
+void *ref_film_fields_create(int nx, int ny, int nz, double hx, double hy, double hz, int modules, double Ms, double A,
+                             double D)
+{
+    ref_film_s *s = new ref_film_s();
+    s->n = nx * ny * nz;
+    s->modules = modules;
+    s->A = A; s->D = D; s->Ms = Ms;
+    Rect r(DBL3(0, 0, 0), DBL3(hx * nx, hy * ny, hz * nz));
+    if (modules & 1) {
+        s->od = new OracleDemag(INT3(nx, ny, nz), DBL3(hx, hy, hz));
+        if (s->od->create_failed() || s->od->calc()) { delete s->od; delete s; return nullptr; }
+        s->In.resize(DBL3(hx, hy, hz), r);
+        s->Out.resize(DBL3(hx, hy, hz), r);
+    }
+    if (modules & 6) s->V.assign(DBL3(hx, hy, hz), r, DBL3(1, 0, 0));
+    return s;
+}
+
+void ref_film_fields_add(void *h, const double *M, double *H)
+{
+    ref_film_s *s = (ref_film_s *)h;
+    const int n = s->n;
+    if (s->od) {
+        memcpy(s->In.data(), M, sizeof(double) * 3 * n);
+        s->od->convolute(s->In, s->Out);
+        const double *o = (const double *)s->Out.data();
+#pragma omp parallel for
+        for (long i = 0; i < 3L * n; i++) H[i] += o[i];
+    }
+    if (!(s->modules & 6)) return;
+    VEC_VC<DBL3> &V = s->V;
+    memcpy(V.data(), M, sizeof(double) * 3 * n);
+    const double Aconst = 2 * s->A / (MU0 * s->Ms * s->Ms);
+    if (!(s->modules & 4)) {
+#pragma omp parallel for
+        for (int i = 0; i < n; i++) {
+            DBL3 d = V.delsq_neu(i);
+            H[3 * i] += Aconst * d.x; H[3 * i + 1] += Aconst * d.y; H[3 * i + 2] += Aconst * d.z;
+        }
+        return;
+    }
+    const double Dconst = -2 * s->D / (MU0 * s->Ms * s->Ms);
+    const double rr = s->D / (2 * s->A);
+#pragma omp parallel for
+    for (int idx = 0; idx < n; idx++) {
+        DBL3 HA, HD;
+        if (V.is_plane_interior(idx)) {
+            HA = Aconst * V.delsq_neu(idx);
+            DBL33 Md = V.grad_neu(idx);
+            HD = Dconst * DBL3(Md.x.z, Md.y.z, -Md.x.x - Md.y.y);
+        }
+        else {
+            DBL3 bx = rr * DBL3(V[idx].z, 0, -V[idx].x);
+            DBL3 by = rr * DBL3(0, V[idx].z, -V[idx].y);
+            DBL33 bnd(bx, by, DBL3());
+            HA = Aconst * V.delsq_nneu(idx, bnd);
+            DBL33 Md = V.grad_nneu(idx, bnd);
+            HD = Dconst * DBL3(Md.x.z, Md.y.z, -Md.x.x - Md.y.y);
+        }
+        H[3 * idx] += HA.x + HD.x; H[3 * idx + 1] += HA.y + HD.y; H[3 * idx + 2] += HA.z + HD.z;
+    }
+}
+
+/* The demag field alone (H = D * M, H overwritten) of a film object built with the demag bit. */
+int ref_film_fields_demag(void *h, const double *M, double *H)
+{
+    ref_film_s *s = (ref_film_s *)h;
+    if (!s->od) return 1;
+    memcpy(s->In.data(), M, sizeof(double) * 3 * s->n);
+    s->od->convolute(s->In, s->Out);
+    memcpy(H, s->Out.data(), sizeof(double) * 3 * s->n);
+    return 0;
+}
+
+void ref_film_fields_destroy(void *h)
+{
+    ref_film_s *s = (ref_film_s *)h;
+    if (!s) return;
+    delete s->od;
+    delete s;
+}
 
 /* Shifted real-space tensors D = -N on the N grid (AoS, 3 doubles per point).
  * kind 0: Calc{Diag,OffDiag}Tens3D_Shifted(n, N, hs, shift)

@@ -9,6 +9,7 @@ reference tree is present; its .so travels with the repository otherwise).
 """
 import ctypes
 import os
+import re
 import subprocess
 
 import numpy as np
@@ -17,7 +18,26 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
 REF_SO = os.path.join(ORACLE_DIR, "_ref", "libborisref.so")
-REF_TREE = "/root/reference"
+
+
+def _reference_tree():
+    """Root of the reference source tree: $BORIS2_REFERENCE, else the default of oracle/Makefile's
+    REF variable (the one recipe that names where the reference is mounted)."""
+    env = os.environ.get("BORIS2_REFERENCE")
+    if env:
+        return env
+    try:
+        with open(os.path.join(ORACLE_DIR, "Makefile")) as f:
+            for line in f:
+                m = re.match(r"\s*REF\s*\?=\s*(\S+)", line)
+                if m:
+                    return m.group(1)
+    except OSError:
+        pass
+    return ""
+
+
+REF_TREE = _reference_tree()
 
 P = ctypes.c_void_p
 D = ctypes.c_double
@@ -84,6 +104,7 @@ def oracle():
         L.orc_solver_set_multilayer.argtypes = [P, DP, I, IP]
         L.orc_solver_set_evalspeedup.argtypes = [P, I]
         L.orc_adjoint_rk4.argtypes = [ctypes.POINTER(MeshDesc), DP, DP, I, D, DP, DP, DP, DP]
+        L.orc_solver_set_field_hook.argtypes = [P, I, P, P]
         _orc = L
     return _orc
 
@@ -98,7 +119,7 @@ def reference():
     if _ref is None:
         if os.path.isdir(REF_TREE):
             # incremental: rebuilds only what changed since the last build
-            subprocess.run(["make", "-C", ORACLE_DIR, "-j8", "ref"], check=True, capture_output=True)
+            subprocess.run(["make", "-C", ORACLE_DIR, "-j8", "ref", "REF=" + REF_TREE], check=True, capture_output=True)
         elif not os.path.exists(REF_SO):
             return None
         L = ctypes.CDLL(REF_SO)
@@ -120,6 +141,11 @@ def reference():
         L.ref_ml_eval.argtypes = [P, DP, DP]
         L.ref_ml_transfer.argtypes = [P, I, DP, DP, DP, DP]
         L.ref_ml_destroy.argtypes = [P]
+        L.ref_film_fields_create.restype = P
+        L.ref_film_fields_create.argtypes = [I, I, I, D, D, D, I, D, D, D]
+        L.ref_film_fields_add.argtypes = [P, DP, DP]
+        L.ref_film_fields_destroy.argtypes = [P]
+        L.ref_film_fields_demag.argtypes = [P, DP, DP]
         L.ref_ovf2_read.argtypes = [ctypes.c_char_p, IP, DP, DP, DP]
         L.ref_ovf2_write.argtypes = [ctypes.c_char_p, IP, DP, DP, DP, ctypes.c_char_p, D]
         L.ref_ovf2_load.argtypes = [ctypes.c_char_p, D, IP, DP]
@@ -240,6 +266,8 @@ class OracleSolver:
             d.nHa = Ha.size // 3
             d.Ha_tspan = m.get("Ha_tspan", 0.0)
         self._arr = arr
+        self._meshes = meshes
+        self._ref_fields = []
         self.n = [m["n"][0] * m["n"][1] * m["n"][2] for m in meshes]
         self.h = oracle().orc_solver_create(len(meshes), arr, evaluation, dt, tol, dT_incr, dT_min, dT_max)
 
@@ -253,6 +281,32 @@ class OracleSolver:
 
     def evalspeedup(self, level):
         assert oracle().orc_solver_set_evalspeedup(P(self.h), int(level)) == 0
+
+    def use_reference_fields(self, mesh=0):
+        """Take this mesh's demag and exchange / iDMI terms from the reference's own compiled code
+        (Convolution<DemagKernel> and the VEC_VC stencils, oracle/_ref); Zeeman, anisotropy, LLG
+        and the RK stages stay the restatement's. Returns False when the reference build is absent."""
+        R = reference()
+        if R is None:
+            return False
+        m = self._meshes[mesh]
+        mods = m.get("modules", 1 | 2 | 16) & (1 | 2 | 4)
+        hnd = R.ref_film_fields_create(m["n"][0], m["n"][1], m["n"][2], m["h"][0], m["h"][1], m["h"][2], mods,
+                                       m.get("Ms", 8e5), m.get("A", 1.3e-11), m.get("D", 0.0))
+        assert hnd, "reference field object could not be built"
+        self._ref_fields.append(hnd)
+        fn = ctypes.cast(R.ref_film_fields_add, ctypes.c_void_p)
+        assert oracle().orc_solver_set_field_hook(P(self.h), mesh, fn, P(hnd)) == 0
+        return True
+
+    def reference_hdemag(self, M, mesh=0):
+        """H_demag of M from the reference's compiled convolution held for this mesh by
+        use_reference_fields (kernels built once)."""
+        hnd = self._ref_fields[mesh]
+        Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+        H = np.zeros_like(Mf)
+        assert reference().ref_film_fields_demag(P(hnd), dp(Mf), dp(H)) == 0
+        return H.reshape(-1, 3)
 
     def set_m(self, M, mesh=0):
         a = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
@@ -278,6 +332,9 @@ class OracleSolver:
         if self.h:
             oracle().orc_solver_destroy(P(self.h))
             self.h = None
+        for hnd in getattr(self, "_ref_fields", []):
+            reference().ref_film_fields_destroy(P(hnd))
+        self._ref_fields = []
 
     def __del__(self):
         self.close()

@@ -1,0 +1,205 @@
+"""GPU parity at the full sizes of the benchmark workloads, against the reference's own CPU build.
+
+  film 128 x 64 x 1 of 5 x 5 x 3 nm, FP64 and mixed, RK4 dt 1e-13, 2000 steps: H_demag at step 0
+      against the reference's Convolution<DemagKernel> (Boris/Convolution.h:262), m after the 2000
+      steps against the CPU solver whose demag and exchange terms are the reference's compiled code
+      (Zeeman, LLG and RK4 restated, oracle/oracle.c)
+  film 512 x 512 x 16 of 2 nm cells (padded FFT 1024 x 1024 x 32), iDMI, uniaxial anisotropy, RKDP54
+      tolerance 1e-5: H_demag against the reference's Convolute_3D (Boris/Convolution.h:659), and m after
+      two adaptive steps against the same CPU solver (demag and iDMI stencils from the reference)
+  film 256 x 256 x 1 of 4 x 4 x 3 nm with Gaussian-random-field Ms map and K1 map, 64 applied-field
+      samples: H_demag against the reference, m after 200 RK4 steps against the oracle restatement
+
+Tolerances (the stated ones): H_demag max |H - H_ref| / max |H_ref| <= 1e-5 mixed, <= 1e-9 FP64;
+|m - m_ref| per cell <= 1e-4 mixed after the run, FP64 <= 1e-8.
+"""
+import numpy as np
+import pytest
+
+from oracle_libs import OracleSolver, reference, ref_hdemag, sphere_random, tilted_z
+
+pytestmark = pytest.mark.gpu
+
+GREL = 2.211e5 / 2.212761569e5
+FILM128 = dict(n=(128, 64, 1), h=(5e-9, 5e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.5, grel=GREL,
+               modules=1 | 2 | 16, Ha=(1e3, 0, 0))
+FILM512 = dict(n=(512, 512, 16), h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, D=1.5e-3, K1=5e5, alpha=0.1,
+               modules=1 | 4 | 8 | 16, Ha=(0, 0, 0))
+
+
+def _need_reference():
+    if reference() is None:
+        pytest.skip("reference CPU build (oracle/_ref) absent")
+
+
+def _ctx(bm, prec, mesh, M, evaluation, dt, ctrl=None):
+    c = bm.Context(precision=bm.FP64 if prec == "fp64" else bm.MIXED)
+    c.add_mesh(mesh["n"], mesh["h"])
+    c.set_material(0, Ms=mesh["Ms"], A=mesh["A"], alpha=mesh["alpha"], grel=mesh.get("grel", 1.0),
+                   K1=mesh.get("K1", 0.0), ea=(0, 0, 1), D=mesh.get("D", 0.0))
+    if mesh.get("Ms_map") is not None:
+        c.set_material_maps(0, Ms_map=mesh["Ms_map"], K1_map=mesh.get("K1_map"))
+    c.set_modules(0, mesh["modules"])
+    c.set_field(0, mesh.get("Ha", (0, 0, 0)), mesh.get("Ha_tspan", 0.0))
+    c.setode(evaluation, dt)
+    if ctrl:
+        c.astepctrl(*ctrl)
+    c.set_m(M)
+    return c
+
+
+def _hrel(H, Href):
+    d = np.linalg.norm(H - Href, axis=1)
+    s = np.linalg.norm(Href, axis=1).max()
+    return d.max() / s, np.sqrt(np.mean(d * d)) / s
+
+
+def _dm(m, mref):
+    return np.linalg.norm(m - mref, axis=1).max()
+
+
+# ------------------------------------------------------------------ film 128 x 64 x 1, RK4 2000 steps
+@pytest.fixture(scope="module")
+def film128_reference():
+    _need_reference()
+    M = sphere_random(128 * 64, seed=1234, Ms=8e5)
+    Href, e_ref = ref_hdemag(M, FILM128["n"], FILM128["h"])
+    s = OracleSolver([FILM128], evaluation=0, dt=1e-13)
+    assert s.use_reference_fields(0)
+    s.set_m(M)
+    st = s.run(2000)
+    m = s.get_m() / 8e5
+    s.close()
+    return M, Href, e_ref, m, st
+
+
+@pytest.mark.parametrize("prec,htol", [("fp64", 1e-9), ("mixed", 1e-5)])
+def test_film128_hdemag_step0(bm, film128_reference, prec, htol):
+    M, Href, e_ref, _, _ = film128_reference
+    c = _ctx(bm, prec, FILM128, M, "RK4", 1e-13)
+    H, e = c.demag_field(with_energy=True)
+    c.close()
+    emax, erms = _hrel(H, Href)
+    assert emax <= htol and erms <= htol, (emax, erms)
+    assert abs(e - e_ref) <= htol * abs(e_ref)
+
+
+@pytest.mark.parametrize("prec,mtol", [("fp64", 1e-8), ("mixed", 1e-4)])
+def test_film128_rk4_2000_steps(bm, film128_reference, prec, mtol):
+    M, _, _, mref, st_ref = film128_reference
+    c = _ctx(bm, prec, FILM128, M, "RK4", 1e-13)
+    st = c.run(2000)
+    m = c.get_m() / 8e5
+    c.close()
+    assert st["accepted"] == 2000 == st_ref["accepted"]
+    assert abs(st["time"] - st_ref["time"]) <= 1e-12 * st_ref["time"]
+    assert _dm(m, mref) <= mtol, _dm(m, mref)
+
+
+# ------------------------------------------------------------------ film 512 x 512 x 16, RKDP54
+@pytest.fixture(scope="module")
+def film512_reference():
+    _need_reference()
+    n = FILM512["n"]
+    M = tilted_z(n[0] * n[1] * n[2], seed=2345, Ms=1.1e6)
+    s = OracleSolver([FILM512], evaluation=1, dt=1e-14, tol=1e-5, dT_incr=2.0, dT_min=1e-15, dT_max=3e-12)
+    assert s.use_reference_fields(0)
+    Href = s.reference_hdemag(M)
+    s.set_m(M)
+    st = s.run(2)
+    m = s.get_m() / 1.1e6
+    s.close()
+    return M, Href, m, st
+
+
+@pytest.mark.parametrize("prec,htol", [("fp64", 1e-9), ("mixed", 1e-5)])
+def test_film512_hdemag(bm, film512_reference, prec, htol):
+    M, Href, _, _ = film512_reference
+    c = _ctx(bm, prec, FILM512, M, "RKDP54", 1e-14, (1e-5, 2.0, 1e-15, 3e-12))
+    H = c.demag_field()
+    c.close()
+    emax, erms = _hrel(H, Href)
+    assert emax <= htol and erms <= htol, (emax, erms)
+
+
+@pytest.mark.parametrize("prec,mtol", [("fp64", 1e-8), ("mixed", 1e-4)])
+def test_film512_rkdp54_steps(bm, film512_reference, prec, mtol):
+    M, _, mref, st_ref = film512_reference
+    c = _ctx(bm, prec, FILM512, M, "RKDP54", 1e-14, (1e-5, 2.0, 1e-15, 3e-12))
+    st = c.run(2)
+    m = c.get_m() / 1.1e6
+    c.close()
+    assert st["accepted"] == st_ref["accepted"] and st["rejected"] == st_ref["rejected"]
+    assert abs(st["time"] - st_ref["time"]) <= 1e-6 * st_ref["time"]
+    assert _dm(m, mref) <= mtol, _dm(m, mref)
+
+
+# ------------------------------------------------------------------ film 256 x 256 x 1 with maps
+def _film256():
+    rng = np.random.default_rng(4)
+    nx = ny = 256
+    h = 4e-9
+    white = rng.normal(size=(ny, nx))
+    kx = 2 * np.pi * np.fft.fftfreq(nx, d=h)
+    ky = 2 * np.pi * np.fft.fftfreq(ny, d=h)
+    k2 = ky[:, None] ** 2 + kx[None, :] ** 2
+    g = np.real(np.fft.ifft2(np.fft.fft2(white) * np.exp(-k2 * (20e-9) ** 2 / 4)))
+    g = (g - g.mean()) / g.std()
+    Ms = 8e5 * (1 + 0.1 * g.reshape(-1))
+    K1 = rng.uniform(0, 2e5, nx * ny)
+    Ha = rng.normal(0, 5e3, (64, 3))
+    mesh = dict(n=(nx, ny, 1), h=(h, h, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.02, K1=0.0, Ms_map=Ms, K1_map=K1,
+                modules=1 | 2 | 8 | 16, Ha=Ha, Ha_tspan=1e-9)
+    M = sphere_random(nx * ny, seed=6, Ms=Ms)
+    return mesh, M
+
+
+def test_film256_maps_hdemag_and_run(bm):
+    _need_reference()
+    mesh, M = _film256()
+    Ms = mesh["Ms_map"][:, None]
+    Href, _ = ref_hdemag(M, mesh["n"], mesh["h"])
+    s = OracleSolver([mesh], evaluation=0, dt=1e-13)
+    s.set_m(M)
+    s.run(200)
+    mref = s.get_m() / Ms
+    s.close()
+    for prec, htol, mtol in (("fp64", 1e-9, 1e-8), ("mixed", 1e-5, 1e-4)):
+        c = _ctx(bm, prec, mesh, M, "RK4", 1e-13)
+        emax, erms = _hrel(c.demag_field(), Href)
+        assert emax <= htol and erms <= htol, (prec, emax, erms)
+        c.set_m(M)
+        c.run(200)
+        assert _dm(c.get_m() / Ms, mref) <= mtol, prec
+        c.close()
+
+
+# ------------------------------------------------------------------ three stacked meshes, full size
+STACK3_FULL = [((1024, 1024, 1), (2e-9, 2e-9, 1e-9), (0.0, 0.0, 0.0)),
+               ((512, 512, 2), (4e-9, 4e-9, 2e-9), (0.0, 0.0, 2e-9)),
+               ((1024, 1024, 1), (2e-9, 2e-9, 1.5e-9), (0.0, 0.0, 7e-9))]
+
+
+def test_stack3_full_multilayer_hdemag(bm):
+    """The multilayered convolution of the three-mesh stack at full size (n_common 1024 x 1024 x 2,
+    FFT 2048 x 2048 x 4) against the reference's DemagKernelCollection build
+    (Boris/SDemag.cpp:735, Boris/DemagKernelCollection_Mult.cpp:457)."""
+    from oracle_libs import MultiLayer
+    _need_reference()
+    ms = (1.4e6, 6e5, 1.1e6)
+    Ms = [sphere_random(int(np.prod(m[0])), seed=40 + q, Ms=ms[q]) for q, m in enumerate(STACK3_FULL)]
+    ml = MultiLayer(STACK3_FULL, 0, which="reference")
+    Href = ml.eval(np.concatenate(Ms))
+    ml.close()
+    for prec, htol in (("fp64", 1e-9), ("mixed", 1e-5)):
+        c = bm.Context(precision=bm.FP64 if prec == "fp64" else bm.MIXED)
+        for n, h, o in STACK3_FULL:
+            c.add_mesh(n, h, o)
+        for q in range(3):
+            c.set_modules(q, bm.DEMAG)
+            c.set_m(Ms[q], q)
+        c.multiconvolution(bm.ML_3D)
+        H = np.concatenate([c.demag_field(q) for q in range(3)])
+        c.close()
+        emax, erms = _hrel(H, Href)
+        assert emax <= htol and erms <= htol, (prec, emax, erms)

@@ -223,3 +223,27 @@ def test_oracle_rkdp_rejects_and_recovers():
     st = s.run(20)
     assert st["accepted"] == 20 and st["rejected"] > 0
     assert np.abs(np.linalg.norm(s.get_m(), axis=1) / 8e5 - 1).max() < 1e-12
+
+
+@pytest.mark.parametrize("modules", [1 | 4 | 8 | 16, 1 | 2 | 16])
+def test_solver_with_reference_fields_matches_restatement(modules):
+    """The CPU baseline's solver (demag and exchange / iDMI from the reference's compiled code,
+    the rest restated) follows the pure restatement's RKDP54 trajectory to FP64 round-off."""
+    if reference() is None:
+        pytest.skip("reference build absent")
+    n, h = (24, 16, 4), (2e-9, 2e-9, 2e-9)
+    mesh = dict(n=n, h=h, Ms=1.1e6, A=1.5e-11, D=1.5e-3, K1=5e5, alpha=0.1, modules=modules, Ha=(1e3, 2e3, 0))
+    M = tilted_z(n[0] * n[1] * n[2], seed=5, Ms=1.1e6)
+    out = []
+    for use_ref in (False, True):
+        s = OracleSolver([mesh], evaluation=1, dt=1e-14, tol=1e-5, dT_incr=2.0, dT_min=1e-15, dT_max=3e-12)
+        if use_ref:
+            assert s.use_reference_fields(0)
+        s.set_m(M)
+        st = s.run(8)
+        out.append((s.get_m(), st))
+        s.close()
+    (m0, s0), (m1, s1) = out
+    assert s0["accepted"] == s1["accepted"] and s0["rejected"] == s1["rejected"]
+    assert abs(s0["time"] - s1["time"]) <= 1e-9 * s0["time"]
+    assert np.abs(m1 - m0).max() / 1.1e6 < 1e-9

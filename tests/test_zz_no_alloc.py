@@ -27,7 +27,9 @@ def test_fft_noalloc_matches_allocating_entry_point(bm):
     import torch
     L = bm.lib()
     rng = np.random.default_rng(2024)
-    for n, howmany, inverse in [(1024, 7, 0), (384, 5, 1)]:
+    # two calls in a row with different lengths and directions, then the longest line the scratch
+    # table holds (4096, whose transform needs more than 48 KB of shared memory) and a 3 * 2^k one
+    for n, howmany, inverse in [(1024, 7, 0), (384, 5, 1), (4096, 3, 0), (3072, 2, 1)]:
         x = rng.normal(size=(howmany, n)) + 1j * rng.normal(size=(howmany, n))
         ref = bm.debug_fft(x, precision=bm.FP64, inverse=bool(inverse))
         xin = torch.from_numpy(np.ascontiguousarray(x).view(np.float64).copy()).cuda()
@@ -41,6 +43,24 @@ def test_fft_noalloc_matches_allocating_entry_point(bm):
         assert _relmax(got, ref) < 1e-13
         # the input buffer is left untouched
         assert np.array_equal(xin.cpu().numpy().view(np.complex128).reshape(howmany, n), x)
+
+
+def test_fft_noalloc_in_place_and_device_kept(bm):
+    import torch
+    L = bm.lib()
+    rng = np.random.default_rng(77)
+    for n, howmany, inverse in [(4096, 2, 1), (512, 9, 0)]:
+        x = rng.normal(size=(howmany, n)) + 1j * rng.normal(size=(howmany, n))
+        ref = bm.debug_fft(x, precision=bm.FP64, inverse=bool(inverse))
+        buf = torch.from_numpy(np.ascontiguousarray(x).view(np.float64).copy()).cuda()
+        torch.cuda.synchronize()
+        rc = L.bm_fft_noalloc(0, n, howmany, inverse, ctypes.c_void_p(buf.data_ptr()),
+                              ctypes.c_void_p(buf.data_ptr()), None)
+        assert rc == 0, L.bm_last_error().decode()
+        torch.cuda.synchronize()
+        got = buf.cpu().numpy().view(np.complex128).reshape(howmany, n)
+        assert _relmax(got, ref) < 1e-13
+        assert torch.cuda.current_device() == 0
 
 
 def test_fft_noalloc_rejects_lines_beyond_scratch(bm):
