@@ -671,14 +671,15 @@ def rel_err(a, ref):
     return {"max": float(d.max() / s), "rms": float(np.sqrt(np.mean(d * d)) / s)}
 
 
-def precision_film(bm, cfg, device, with_reference=True, ref_steps=2, gpu_steps=1000):
+def precision_film(bm, cfg, device, with_reference=True, ref_steps=2, gpu_steps=5000):
     """Errors of the mixed-precision path (and of the GPU FP64 plain form) against FP64 on the
     workload's full film, from one seeded M:
       h_demag            H_demag of M: mixed and GPU FP64 against the reference's CPU build
                          (Convolution<DemagKernel>), and mixed against GPU FP64; relative to max |H_ref|
       m_after_ref_steps  m after `ref_steps` whole steps of the workload's stepper from M: mixed and GPU
                          FP64 against the CPU reference solver (reference_film_solver); |dm| per cell
-      m_after_gpu_steps  m after `gpu_steps` steps: mixed against GPU FP64, and their simulated times
+      m_after_gpu_steps  m after `gpu_steps` steps (the workload's run length): mixed against GPU FP64,
+                         and their simulated times
     Tolerances stated by the workload: 1e-5 on H_demag, 1e-4 on |dm|. The CPU reference steps are also
     timed and returned as the cpu_baseline (key _cpu_baseline)."""
     M = init_m(cfg, 4321)

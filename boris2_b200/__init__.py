@@ -391,15 +391,15 @@ class Context:
         _check(lib().bm_time_kernels(self._h, mesh, int(reps), _dp(ms), _dp(by)))
         return ms, by
 
-    TIME_KINDS = ("stage", "yfwd", "zmid", "yinv", "ymid2d", "other")
+    TIME_KINDS = ("stage", "yfwd", "zmid", "yinv", "ymid2d", "other", "yzy", "")
 
     def time_step(self, steps=3):
         """Run `steps` steps eagerly (the step graph's launches, timed one by one with CUDA events)
         and return {kind: {"ms": summed device ms, "bytes": summed algorithmic bytes, "launches": n}}
         for the kinds in TIME_KINDS that launched. The simulation advances."""
-        ms = np.zeros(6)
-        by = np.zeros(6)
-        nl = (ctypes.c_int * 6)()
+        ms = np.zeros(8)
+        by = np.zeros(8)
+        nl = (ctypes.c_int * 8)()
         _check(lib().bm_time_step(self._h, int(steps), _dp(ms), _dp(by), nl))
         return {k: {"ms": float(ms[i]), "bytes": float(by[i]), "launches": int(nl[i])}
                 for i, k in enumerate(self.TIME_KINDS) if nl[i] > 0}
@@ -407,12 +407,12 @@ class Context:
     def tiles(self, mesh=0):
         """Autotuned tile shapes: 2D y width, 3D y width and variant (1: radix-16 Stockham), z width,
         stage rows per block (negative when the per-cell rows are prefetched), stage x-transform
-        variant (1: radix-8 Stockham)."""
+        variant (1: radix-8 Stockham), yzy (1: the fused y -> z -> y cluster pass of a 3D mesh)."""
         t = (ctypes.c_int * 4)()
         _check(lib().bm_tiles(self._h, mesh, t))
         sgn = -1 if t[3] < 0 else 1
-        return {"ymid2d_W": t[0], "ypass_W": t[1] % 100, "ypass_yv": t[1] // 100, "zmid_W": t[2],
-                "stage_rows": sgn * (abs(t[3]) % 100), "stage_xv": abs(t[3]) // 100}
+        return {"ymid2d_W": t[0], "ypass_W": t[1] % 100, "ypass_yv": t[1] // 100, "zmid_W": t[2] % 1000,
+                "yzy": t[2] // 1000, "stage_rows": sgn * (abs(t[3]) % 100), "stage_xv": abs(t[3]) // 100}
 
     def stats(self):
         st = Stats()

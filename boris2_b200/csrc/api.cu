@@ -71,6 +71,7 @@ struct Mesh {
     int Nx = 1, Ny = 1, Nz = 1, LX = 1;
     FFTPlan px, py, pz;
     int W2 = 1, Wy = 1, Wz = 1, rpb = 1, staged = 0, xv = 0, yv = 0;
+    int yzy = 0;                // 3D: the fused y -> z -> y cluster pass instead of three launches
     // device (element type depends on the context precision)
     void *buf[4] = {nullptr, nullptr, nullptr, nullptr};   // A (M), P (sM1), B, C
     void *ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -131,7 +132,8 @@ struct BatchPlan {
 #define BM_TK_YINV 3
 #define BM_TK_YMID2D 4
 #define BM_TK_OTHER 5
-#define BM_TK_COUNT 6
+#define BM_TK_YZY 6
+#define BM_TK_COUNT 8
 struct LaunchTimer {
     std::vector<cudaEvent_t> ev;   // ev[0] before the first launch, ev[i + 1] after launch i
     std::vector<int> kind;
@@ -599,6 +601,20 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
                 if (t < best) { best = t; bw = W; }
             }
             m.Wz = bw;
+            // the fused cluster pass, where it applies, against the three tuned launches
+            // (BM_YZY=0 keeps the three launches)
+            const char *sz = getenv("BM_YZY");
+            m.yzy = 0;
+            YZArgs<T> f = yz_args<T>(c, m, BM_GATE_ALWAYS);
+            if (!(sz && sz[0] == '0') && yzy_available<T>(f) == 0) {
+                YZArgs<T> y = f, z = f;
+                y.W = m.Wy; z.W = m.Wz;
+                const float t3 = time_launches(s, [&]() { return launch_yfwd<T>(y, s); }, reps) +
+                                 time_launches(s, [&]() { return launch_zmid<T>(z, s); }, reps) +
+                                 time_launches(s, [&]() { return launch_yinv<T>(y, s); }, reps);
+                const float tf = time_launches(s, [&]() { return launch_yzy<T>(f, s); }, reps);
+                if (tf < t3) m.yzy = 1;
+            }
         }
     }
     // stage kernel: rows per block
@@ -834,6 +850,10 @@ int prepare_T(bm_ctx *c)
             m.xv = (sx && sx[0] == '1' && stage_reg_q(m.LX, 1)) ? 1 : (sx && sx[0] == '2' && stage_reg_q(m.LX, 2)) ? 2 : 0;
             const char *sy = getenv("BM_Y_XV");
             m.yv = (sy && sy[0] == '1' && ypass_has_st(m.Ny) && m.nz > 1 && ypass_st_threads(m.Ny, m.Wy) % 32 == 0) ? 1 : 0;
+            const char *sz = getenv("BM_YZY");
+            m.yzy = 0;
+            if (sz && sz[0] == '1' && m.nz > 1 && m.ml_role == 0 && (m.modules & BM_DEMAG) && !c->batched)
+                m.yzy = yzy_available<T>(yz_args<T>(c, m, BM_GATE_ALWAYS)) == 0 ? 1 : 0;
         } else if (c->autotune && !c->batched) autotune_mesh<T>(c, m);
     }
     if (int rc = prepare_ml<T>(c)) { for (auto &mm : c->meshes) free_mesh(mm); free_ml(c); return rc; }
@@ -949,6 +969,7 @@ double yz_alg_bytes(const Mesh &m, int kind, size_t p)
     case BM_TK_YFWD: case BM_TK_YINV: return s1 + s2;
     case BM_TK_ZMID: return 2.0 * s2 + kb;
     case BM_TK_YMID2D: return 2.0 * s1 + 4.0 / 6.0 * kb;
+    case BM_TK_YZY: return 2.0 * s1 + kb;
     default: return 0.0;
     }
 }
@@ -976,6 +997,10 @@ int enqueue_yz(bm_ctx *c, Mesh &m, int gate, int *count)
     if (m.nz == 1) {
         CKL(launch_ymid2d<T>(a, c->stream), "ymid2d");
         lt_mark(c, BM_TK_YMID2D, yz_alg_bytes(m, BM_TK_YMID2D, sizeof(T)));
+        (*count)++;
+    } else if (m.yzy) {
+        CKL(launch_yzy<T>(a, c->stream), "yzy");
+        lt_mark(c, BM_TK_YZY, yz_alg_bytes(m, BM_TK_YZY, sizeof(T)));
         (*count)++;
     } else {
         CKL(launch_yfwd<T>(a, c->stream), "yfwd");
@@ -1514,6 +1539,8 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
         if (rc) return rc;
     }
     static const double bs[5] = {5179.0 / 57600, 7571.0 / 16695, 393.0 / 640, -92097.0 / 339200, 187.0 / 2100};
+    // 5th-order weights of k0, k2, k3, k4, k5 (k1 has none)
+    static const double as5[5] = {35.0 / 384, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84};
     {
         std::vector<StageArgs<T>> v;
         for (int i = 0; i < nm; i++) {
@@ -1526,6 +1553,14 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
             a.ev[0] = E<T>(m, 0); a.ev[1] = E<T>(m, 2); a.ev[2] = E<T>(m, 3); a.ev[3] = E<T>(m, 4); a.ev[4] = E<T>(m, 5);
             for (int k = 0; k < 5; k++) a.cev[k] = bs[k];
             a.crhs = 1.0 / 40;
+            if (sizeof(T) == 4) {
+                // mixed precision: the reference's |M - prediction| (Boris/DiffEqFM_Evals_RKDP54.cpp:72-76)
+                // with M, the renormalised 5th-order solution, recomputed in FP64 from sM1 and the stage
+                // rhs; the FP32-stored M would add its rounding (~1e-7 relative), a floor under the error
+                // estimate that holds small steps back
+                for (int k = 0; k < 5; k++) a.cev5[k] = as5[k];
+                a.lte_embedded = 1;
+            }
             a.ev_out = E<T>(m, 0);
             if (i == nm - 1) a.last_kind = BM_LAST_CONTROL;
             v.push_back(a);
@@ -2465,6 +2500,8 @@ int time_kernels_T(bm_ctx *c, Mesh &m, int reps, double *ms4, double *bytes4)
         YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
         if (m.nz == 1) {
             rc = timeit([&]() { return launch_ymid2d<T>(a, s); }, 0, 2.0 * s1 + 4.0 / 6.0 * kb);
+        } else if (m.yzy) {
+            rc = timeit([&]() { return launch_yzy<T>(a, s); }, 0, 2.0 * s1 + kb);
         } else {
             a.W = m.Wy;
             rc = timeit([&]() { return launch_yfwd<T>(a, s); }, 0, s1 + s2);
@@ -2608,7 +2645,7 @@ int bm_tiles(bm_ctx *c, int mesh, int *tiles4)
     if (int rc = check_mesh(c, mesh)) return rc;
     if (!tiles4) return fail(BM_EINVAL, "null out");
     Mesh &m = c->meshes[mesh];
-    tiles4[0] = m.W2; tiles4[1] = m.Wy + 100 * m.yv; tiles4[2] = m.Wz; tiles4[3] = (m.staged ? -1 : 1) * (m.rpb + 100 * m.xv);
+    tiles4[0] = m.W2; tiles4[1] = m.Wy + 100 * m.yv; tiles4[2] = m.Wz + 1000 * m.yzy; tiles4[3] = (m.staged ? -1 : 1) * (m.rpb + 100 * m.xv);
     return 0;
 }
 

@@ -62,6 +62,10 @@ bool ypass_has_st(int Ny);            // lengths with the Stockham y transform (
 int ypass_st_threads(int Ny, int W);
 int ymid2d_reg_threads(int Ny, int W);   // block size of the register 2D y pass
 int ypass_reg_threads(int Ny, int W);
+// fused y -> z -> y pass of a 3D mesh in one thread-block-cluster kernel (yzy.cu): 0 when it
+// applies to the mesh (sizes, shared memory, the device's cluster occupancy)
+template <typename T> int yzy_available(const YZArgs<T> &a);
+template <typename T> int launch_yzy(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s);
 template <typename T> int launch_zmid(const YZArgs<T> &a, cudaStream_t s);
@@ -105,6 +109,8 @@ struct StageArgs {
     double cev[6];
     double crhs;
     int renorm, mode, do_xfwd, last_kind, gate;
+    int lte_embedded;    // LTE mode: the 5th-order solution recomputed in FP64 from the base and cev5 (nev 5)
+    double cev5[6];      // LTE mode with lte_embedded: 5th-order weights of the same stage rhs as cev
     long long n;         // cells
     int staged;          // prefetch the per-cell input rows into shared memory (register kernel)
     int xv;              // register x transform: 0 two-level P x Q, 1 radix-8 Stockham at 64 (FP32) registers

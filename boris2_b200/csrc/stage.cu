@@ -351,28 +351,54 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         if (a.mode == BM_MODE_LTE) {
             // 4th-order prediction from the previous step's stages (FSAL), error in FP64
             double d2 = 0.0, m2 = 0.0;
+            double sb[3], sa[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                double sum = 0.0;
+                sb[c] = 0.0;
+                sa[c] = 0.0;
                 switch (nev) {   // block-uniform: unrolled sums without predicated loads
-                case 6: sum = ev_sum_d<6>(acc, a.cev, r, c, x, cell); break;
-                case 5: sum = ev_sum_d<5>(acc, a.cev, r, c, x, cell); break;
-                case 4: sum = ev_sum_d<4>(acc, a.cev, r, c, x, cell); break;
-                case 3: sum = ev_sum_d<3>(acc, a.cev, r, c, x, cell); break;
-                case 2: sum = ev_sum_d<2>(acc, a.cev, r, c, x, cell); break;
-                case 1: sum = ev_sum_d<1>(acc, a.cev, r, c, x, cell); break;
+                case 6: sb[c] = ev_sum_d<6>(acc, a.cev, r, c, x, cell); break;
+                case 5: sb[c] = ev_sum_d<5>(acc, a.cev, r, c, x, cell); break;
+                case 4: sb[c] = ev_sum_d<4>(acc, a.cev, r, c, x, cell); break;
+                case 3: sb[c] = ev_sum_d<3>(acc, a.cev, r, c, x, cell); break;
+                case 2: sb[c] = ev_sum_d<2>(acc, a.cev, r, c, x, cell); break;
+                case 1: sb[c] = ev_sum_d<1>(acc, a.cev, r, c, x, cell); break;
                 default: break;
                 }
-                double pred = (double)acc.mb(r, c, x, cell) + dT * (sum + a.crhs * (double)rhs[c]);
-                double d = (double)m[c] - pred;
-                d2 += d * d;
-                m2 += (double)m[c] * (double)m[c];
+                if (a.lte_embedded && nev == 5) sa[c] = ev_sum_d<5>(acc, a.cev5, r, c, x, cell);
             }
+            if (a.lte_embedded) {
+                // the step's 5th-order solution recomputed in FP64 from its base and stage rhs,
+                // renormalised to Ms, against the 4th-order prediction: the reference's
+                // |M - prediction| without the rounding of the FP32-stored M
+                double m5[3], n5 = 0.0;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    m5[c] = (double)acc.mb(r, c, x, cell) + dT * sa[c];
+                    n5 += m5[c] * m5[c];
+                }
+                const double f = (double)Ms / sqrt(n5);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const double pred = (double)acc.mb(r, c, x, cell) + dT * (sb[c] + a.crhs * (double)rhs[c]);
+                    const double d = m5[c] * f - pred;
+                    d2 += d * d;
+                    m2 += (double)m[c] * (double)m[c];
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const double pred = (double)acc.mb(r, c, x, cell) + dT * (sb[c] + a.crhs * (double)rhs[c]);
+                    const double d = (double)m[c] - pred;
+                    d2 += d * d;
+                    m2 += (double)m[c] * (double)m[c];
+                }
+            }
+            // a non-finite current state (M or its rhs) is flagged, never accepted; a NaN error
+            // estimate from the stage buffers of an unprimed attempt only counts as a huge error
+            if (!isfinite(m[0] + m[1] + m[2] + rhs[0] + rhs[1] + rhs[2])) atomicOr(&a.st->error, BM_ERR_NONFINITE);
             double l = sqrt(d2) / sqrt(m2);
-            if (!(l <= 1e300)) {     // NaN or infinite: a non-finite state, never accepted
-                l = 1e300;
-                atomicOr(&a.st->error, BM_ERR_NONFINITE);
-            }
+            if (!(l <= 1e300)) l = 1e300;
             if (l > lmax) lmax = l;
 #pragma unroll
             for (int c = 0; c < 3; c++) (a.ev_out + cell)[c * n] = rhs[c];

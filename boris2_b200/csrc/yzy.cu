@@ -1,0 +1,452 @@
+// Fused y -> z -> y pass of the 3D demag convolution in one thread-block-cluster kernel.
+//
+// The three-kernel path (k_ypass_* forward, k_zmid_*, k_ypass_* inverse) moves the y-transformed
+// spectra S2 (twice the bytes of S1) through HBM four times per field evaluation. Here one cluster
+// of C = 8 CTAs owns a tile of W x-columns (kx0 .. kx0 + W) of all three components and keeps that
+// tile's whole y-transformed slab, 3 nz lines x Ny rows x W columns, in the cluster's distributed
+// shared memory. HBM then sees the S1 tile once in, once out, and the kernel spectra once.
+//
+// The y transform of length Ny = P * Q is the two-level split of the register y passes:
+//   stage 1 (over n2):  u[n1][k2] = w_Ny^(n1 k2) sum_n2 x[n1 + P n2] w_Q^(n2 k2)
+//   stage 2 (over n1):  X[k2 + Q k1] = sum_n1 u[n1][k2] w_P^(n1 k1)
+// Each CTA owns a set of k2 residues (S = Q / C of them) closed under k2 -> (Q - k2) mod Q, so a
+// wavenumber ky = k2 + Q k1 and its mirror (Ny - ky) mod Ny always live in the same CTA.
+//   A1  line owners (line = c nz + z, lines dealt round-robin over the cluster) read their S1
+//       columns from HBM into registers, do stage 1 and store u[.][k2] into the shared memory of
+//       the CTA owning k2 (distributed shared memory stores)                      -> cluster barrier
+//   A2  every CTA does stage 2 on its own k2 rows in shared memory                 -> block barrier
+//   B   every CTA runs the z pass on its pencils (ky, kx): the 2 Nz-point z transform split by
+//       output parity (two Nz/2-point transforms, the sparse input folded), the symmetric 3x3
+//       kernel product with the mirror signs of KernelMultiplication_3D_line
+//       (Boris/DemagKernel.cpp:85), the inverse, the first nz planes kept. The six (component,
+//       parity) halves of a pencil are six lanes of one warp and exchange spectra by shuffles.
+//       The packed column kx = 0 (DC in .x, Nyquist in .y) pairs ky with its mirror as the
+//       three-kernel z pass does.                                                  -> block barrier
+//   C1  inverse stage 2 on the own k2 rows, times w_Ny^(-n1 k2)                     -> cluster barrier
+//   C2  line owners load u[.][k2] from the owning CTAs (distributed shared memory loads), do the
+//       inverse stage 1 and write the first ny rows of their S1 columns            -> cluster barrier
+// The last barrier keeps every CTA's shared memory alive until the others have read it. All
+// barriers are hardware cluster / block barriers taken by every thread of every CTA (no spin waits).
+//
+// Supported: Ny = 32 * Q with Q in {16, 32} (Ny 512, 1024), Nz in {4, 8, 12, 16, 24, 32} (the parity
+// halves of a z line split evenly between the two lanes of a component), LX a multiple
+// of W, and a slab that fits one CTA's shared memory (3 nz S P W complex values per CTA).
+#include "kernels.h"
+#include "regfft.cuh"
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
+#define YZY_C 8       // CTAs per cluster
+#define YZY_NT 384    // threads per CTA (12 warps)
+
+template <typename T>
+__device__ __forceinline__ bool yzy_gated_out(const StepState *st, int gate)
+{
+    if (gate == BM_GATE_ALWAYS || st == nullptr) return false;
+    if (gate == BM_GATE_ACCEPTED) return *((volatile const int *)&st->reject_flag) != 0;
+    return *((volatile const int *)&st->need_restore) == 0;
+}
+
+// k2 residues owned by each CTA of the cluster (C = 8), closed under k2 -> (Q - k2) mod Q.
+// Q = 32: CTA 0 {0, 16, 8, 24}, CTA r >= 1 {r, 32 - r, 16 - r, 16 + r}
+// Q = 16: CTA 0 {0, 8},         CTA r >= 1 {r, 16 - r}
+template <int Q> struct YzyOwn;
+template <> struct YzyOwn<32> {
+    static constexpr int S = 4;
+    __device__ __forceinline__ static int k2_of(int r, int s)
+    {
+        if (r == 0) return s == 0 ? 0 : s == 1 ? 16 : s == 2 ? 8 : 24;
+        return s == 0 ? r : s == 1 ? 32 - r : s == 2 ? 16 - r : 16 + r;
+    }
+    __device__ __forceinline__ static void where(int k2, int &r, int &s)
+    {
+        if ((k2 & 7) == 0) { r = 0; s = k2 == 0 ? 0 : k2 == 16 ? 1 : k2 == 8 ? 2 : 3; return; }
+        const int a = k2 & 15;
+        r = a < 8 ? a : 16 - a;
+        s = k2 < 16 ? (k2 == r ? 0 : 2) : (k2 == 32 - r ? 1 : 3);
+    }
+};
+template <> struct YzyOwn<16> {
+    static constexpr int S = 2;
+    __device__ __forceinline__ static int k2_of(int r, int s)
+    {
+        if (r == 0) return s == 0 ? 0 : 8;
+        return s == 0 ? r : 16 - r;
+    }
+    __device__ __forceinline__ static void where(int k2, int &r, int &s)
+    {
+        if ((k2 & 7) == 0) { r = 0; s = k2 >> 3; return; }
+        r = k2 < 8 ? k2 : 16 - k2;
+        s = k2 < 8 ? 0 : 1;
+    }
+};
+
+// shared-memory slab of one CTA: [line = c nz + z][slot][j = n1 or k1][w], a padded row per
+// (line, slot) and a small offset per component block against bank conflicts between components
+template <int P, int W> struct YzyLayout {
+    static constexpr int ROW = P * W + 4;
+    static constexpr int CPAD = 5;
+};
+template <int P, int W, int S>
+__device__ __forceinline__ int yzy_idx(int c, int line, int slot, int j, int w)
+{
+    return (line * S + slot) * YzyLayout<P, W>::ROW + c * YzyLayout<P, W>::CPAD + j * W + w;
+}
+template <typename T, int P, int W, int S> __host__ __device__ inline size_t yzy_smem_bytes(int nz)
+{
+    return ((size_t)3 * nz * S * YzyLayout<P, W>::ROW + 3 * YzyLayout<P, W>::CPAD) * sizeof(cpx<T>);
+}
+
+template <typename T>
+__device__ __forceinline__ cpx<T> shfl_c(cpx<T> v, int src)
+{
+    return mk<T>(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// kernel-plane value of component q at (|kz|, |ky|, kx)
+template <typename T>
+__device__ __forceinline__ T kval(const T *__restrict__ K, long long nk, int q, int akz, int aky, int kx, int Ky1, int Kx1)
+{
+    return __ldg(K + q * nk + ((long long)akz * Ky1 + aky) * Kx1 + kx);
+}
+
+template <typename T, int P, int Q, int NZ, int W>
+__global__ void __launch_bounds__(YZY_NT, 1) k_yzy(YZArgs<T> a)
+{
+    using Own = YzyOwn<Q>;
+    constexpr int S = Own::S, L = P * Q, H = NZ / 2;
+    if (yzy_gated_out<T>(a.st, a.gate)) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cpx<T> *buf = reinterpret_cast<cpx<T> *>(smraw);
+    cg::cluster_group cluster = cg::this_cluster();
+    const int r = (int)cluster.block_rank();
+    const int tile = blockIdx.x / YZY_C;
+    const int kx0 = tile * W;
+    const int tid = threadIdx.x;
+    const int ny = a.ny, nz = a.nz, LX = a.LX, Ny = L;
+    const int nl = 3 * nz;
+    const int myl = (nl - r + YZY_C - 1) / YZY_C;        // lines owned by this CTA: r, r + C, ...
+
+    // ---------------- A1: stage 1 of the forward y transform, pushed to the k2 owners
+    for (int t = tid; t < myl * P * W; t += YZY_NT) {
+        const int w = t % W, n1 = (t / W) % P, i = t / (W * P);
+        const int line = r + YZY_C * i;
+        const int c = line / nz, z = line - c * nz;
+        const cpx<T> *src = a.S1 + ((long long)(c * nz + z) * ny) * LX + kx0 + w;
+        cpx<T> v[Q];
+#pragma unroll
+        for (int n2 = 0; n2 < Q; n2++) {
+            const int e = n1 + P * n2;
+            v[n2] = (n2 < Q / 2 && e < ny) ? src[(long long)e * LX] : mk<T>(0, 0);
+        }
+        RegFFT<T, Q, false>::run(v, a.twy, P);
+#pragma unroll
+        for (int k2 = 0; k2 < Q; k2++) {
+            cpx<T> u = v[k2];
+            if (k2 > 0 && n1 > 0) u = cmul(u, a.twy[n1 * k2]);
+            int ro, so;
+            Own::where(k2, ro, so);
+            cpx<T> *dst = cluster.map_shared_rank(buf, ro);
+            dst[yzy_idx<P, W, S>(c, line, so, n1, w)] = u;
+        }
+    }
+    cluster.sync();
+
+    // ---------------- A2: stage 2 on the own k2 rows (in place, n1 -> k1)
+    for (int t = tid; t < nl * S * W; t += YZY_NT) {
+        const int w = t % W, s = (t / W) % S, line = t / (W * S);
+        const int c = line / nz;
+        cpx<T> *row = buf + yzy_idx<P, W, S>(c, line, s, 0, w);
+        cpx<T> u[P];
+#pragma unroll
+        for (int j = 0; j < P; j++) u[j] = row[j * W];
+        RegFFT<T, P, false>::run(u, a.twy, Q);
+#pragma unroll
+        for (int j = 0; j < P; j++) row[j * W] = u[j];
+    }
+    __syncthreads();
+
+    // ---------------- B: z pass with the kernel product on the own pencils
+    {
+        const long long nk = (long long)(LX + 1) * (Ny / 2 + 1) * (H + 1);
+        const int Kx1 = LX + 1, Ky1 = Ny / 2 + 1;
+        const int lane = tid & 31, warp = tid >> 5;
+        const bool packed_tile = (kx0 == 0);
+        // main path: six lanes (component c, output parity par) per pencil, five pencils per warp
+        {
+            const int g = lane / 6, wi = lane - 6 * g;
+            const int c = wi >> 1, par = wi & 1, gb = lane - wi;
+            const int q0 = c == 0 ? 0 : c == 1 ? 3 : 4;
+            const int q1 = c == 0 ? 3 : c == 1 ? 1 : 5;
+            const int q2 = c == 0 ? 4 : c == 1 ? 5 : 2;
+            const bool y0 = (q0 == 3 || q0 == 5), y1 = (q1 == 3 || q1 == 5), y2 = (q2 == 3 || q2 == 5);
+            const bool z0 = (q0 == 4 || q0 == 5), z1 = (q1 == 4 || q1 == 5), z2 = (q2 == 4 || q2 == 5);
+            const int npen = S * P * W;
+            constexpr int PER_IT = (YZY_NT / 32) * 5;
+            for (int base = 0; base < npen; base += PER_IT) {
+                const int pen = base + warp * 5 + g;
+                const int w = pen % W, k1 = (pen / W) % P, s = pen / (W * P);
+                const bool valid = (g < 5) && (pen < npen) && !(packed_tile && w == 0);
+                const int ky = Own::k2_of(r, s) + Q * k1;
+                const int aky = ky <= Ny / 2 ? ky : Ny - ky;
+                const T sy = ky > Ny / 2 ? (T)-1 : (T)1;
+                const int kx = kx0 + w;
+                cpx<T> x[H];
+#pragma unroll
+                for (int m = 0; m < H; m++) {
+                    x[m] = mk<T>(0, 0);
+                    if (valid && m < nz) x[m] = buf[yzy_idx<P, W, S>(c, c * nz + m, s, k1, w)];
+                }
+                if (par) {
+#pragma unroll
+                    for (int m = 1; m < H; m++) x[m] = cmul(x[m], a.twz[m]);
+                }
+                RegFFT<T, H, false>::run(x, a.twz, 2);
+#pragma unroll
+                for (int m = 0; m < H; m++) {
+                    const int kz = 2 * m + par;
+                    const int akz = kz <= H ? kz : NZ - kz;
+                    const T sz = kz > H ? (T)-1 : (T)1;
+                    const cpx<T> M0 = shfl_c(x[m], gb + par), M1 = shfl_c(x[m], gb + 2 + par), M2 = shfl_c(x[m], gb + 4 + par);
+                    T k0 = 0, k1v = 0, k2v = 0;
+                    if (valid) {
+                        k0 = kval(a.K, nk, q0, akz, aky, kx, Ky1, Kx1);
+                        k1v = kval(a.K, nk, q1, akz, aky, kx, Ky1, Kx1);
+                        k2v = kval(a.K, nk, q2, akz, aky, kx, Ky1, Kx1);
+                    }
+                    if (y0) k0 *= sy;
+                    if (z0) k0 *= sz;
+                    if (y1) k1v *= sy;
+                    if (z1) k1v *= sz;
+                    if (y2) k2v *= sy;
+                    if (z2) k2v *= sz;
+                    x[m] = mk<T>(k0 * M0.x + k1v * M1.x + k2v * M2.x, k0 * M0.y + k1v * M1.y + k2v * M2.y);
+                }
+                RegFFT<T, H, true>::run(x, a.twz, 2);
+                if (par) {
+#pragma unroll
+                    for (int m = 1; m < H; m++) x[m] = cmul(x[m], conj(a.twz[m]));
+                }
+                // out[n] = x_even[n] + x_odd[n]: the even lane keeps n < H/2, the odd lane n >= H/2
+#pragma unroll
+                for (int i = 0; i < H / 2; i++) {
+                    const cpx<T> send = par ? x[i] : x[H / 2 + i];
+                    const cpx<T> recv = mk<T>(__shfl_xor_sync(0xffffffffu, send.x, 1), __shfl_xor_sync(0xffffffffu, send.y, 1));
+                    const cpx<T> mine = par ? x[H / 2 + i] : x[i];
+                    const int n = par ? H / 2 + i : i;
+                    if (valid && n < nz) buf[yzy_idx<P, W, S>(c, c * nz + n, s, k1, w)] = mine + recv;
+                }
+            }
+        }
+        // packed column kx = 0 (first tile only): (ky, mirror) pairs, twelve lanes (pencil p,
+        // component c, parity par) per pair, two pairs per warp
+        if (packed_tile) {
+            __syncthreads();
+            const int g = lane / 12, wi = lane - 12 * g;
+            const int p = wi / 6, c = (wi % 6) >> 1, par = wi & 1, gb = lane - wi;
+            const int q0 = c == 0 ? 0 : c == 1 ? 3 : 4;
+            const int q1 = c == 0 ? 3 : c == 1 ? 1 : 5;
+            const int q2 = c == 0 ? 4 : c == 1 ? 5 : 2;
+            const T zq0 = (q0 == 4 || q0 == 5) ? (T)-1 : (T)1, zq1 = (q1 == 4 || q1 == 5) ? (T)-1 : (T)1,
+                    zq2 = (q2 == 4 || q2 == 5) ? (T)-1 : (T)1;
+            // primary pencils: ky <= Ny / 2 among the own (slot, k1)
+            const int npen = S * P;
+            constexpr int PER_IT = (YZY_NT / 32) * 2;
+            for (int base = 0; base < npen; base += PER_IT) {
+                const int pen = base + warp * 2 + g;
+                const int k1 = pen % P, s = pen / P;
+                const int ky0 = Own::k2_of(r, s) + Q * k1;
+                const bool prim = (g < 2) && (pen < npen) && ky0 <= Ny / 2;
+                const int kym = (Ny - ky0) % Ny;
+                const bool single = (ky0 == kym);
+                const int kyp = p ? kym : ky0;
+                int sp = s, k1p = k1;
+                if (p) {
+                    int ro;
+                    Own::where(kym % Q, ro, sp);
+                    k1p = kym / Q;
+                }
+                const bool valid = prim && !(p && single);
+                cpx<T> x[H];
+#pragma unroll
+                for (int m = 0; m < H; m++) {
+                    x[m] = mk<T>(0, 0);
+                    if (valid && m < nz) x[m] = buf[yzy_idx<P, W, S>(c, c * nz + m, sp, k1p, 0)];
+                }
+                if (par) {
+#pragma unroll
+                    for (int m = 1; m < H; m++) x[m] = cmul(x[m], a.twz[m]);
+                }
+                RegFFT<T, H, false>::run(x, a.twz, 2);
+                const int pm = single ? p : 1 - p;
+                cpx<T> o[H];
+#pragma unroll
+                for (int m = 0; m < H; m++) {
+                    const int kz = 2 * m + par;
+                    const int kzm = (NZ - kz) % NZ;
+                    const int akz = kz <= H ? kz : NZ - kz;
+                    // the mirror value S(cc, pm, kzm) sits at index (kzm - par) / 2 of its lane
+                    const int mm_e = (H - m) % H, mm_o = H - 1 - m;   // for par 0 / par 1
+                    const cpx<T> xm = par ? x[mm_o] : x[mm_e];
+                    cpx<T> A[3], B[3];
+#pragma unroll
+                    for (int cc = 0; cc < 3; cc++) {
+                        const cpx<T> C = shfl_c(x[m], gb + 6 * p + 2 * cc + par);
+                        const cpx<T> cj = conj(shfl_c(xm, gb + 6 * pm + 2 * cc + par));
+                        A[cc] = cscale(C + cj, (T)0.5);
+                        B[cc] = cscale(mul_mi(C - cj), (T)0.5);
+                    }
+                    const int kq = single ? (kz <= H ? kz : kzm) : (p == 0 ? kz : kzm);
+                    const bool neg = kq > H;
+                    const T s0 = neg ? zq0 : (T)1, s1 = neg ? zq1 : (T)1, s2 = neg ? zq2 : (T)1;
+                    T a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
+                    if (prim) {
+                        a0 = s0 * kval(a.K, nk, q0, akz, ky0, 0, Ky1, Kx1);
+                        a1 = s1 * kval(a.K, nk, q1, akz, ky0, 0, Ky1, Kx1);
+                        a2 = s2 * kval(a.K, nk, q2, akz, ky0, 0, Ky1, Kx1);
+                        b0 = s0 * kval(a.K, nk, q0, akz, ky0, LX, Ky1, Kx1);
+                        b1 = s1 * kval(a.K, nk, q1, akz, ky0, LX, Ky1, Kx1);
+                        b2 = s2 * kval(a.K, nk, q2, akz, ky0, LX, Ky1, Kx1);
+                    }
+                    const cpx<T> Ap = mk<T>(a0 * A[0].x + a1 * A[1].x + a2 * A[2].x, a0 * A[0].y + a1 * A[1].y + a2 * A[2].y);
+                    const cpx<T> Bp = mk<T>(b0 * B[0].x + b1 * B[1].x + b2 * B[2].x, b0 * B[0].y + b1 * B[1].y + b2 * B[2].y);
+                    o[m] = Ap + mul_i(Bp);
+                }
+                RegFFT<T, H, true>::run(o, a.twz, 2);
+                if (par) {
+#pragma unroll
+                    for (int m = 1; m < H; m++) o[m] = cmul(o[m], conj(a.twz[m]));
+                }
+                // both pencils of the pair have been read by every lane of the pair (the shuffles
+                // above), so the results can go back in place
+#pragma unroll
+                for (int i = 0; i < H / 2; i++) {
+                    const cpx<T> send = par ? o[i] : o[H / 2 + i];
+                    const cpx<T> recv = mk<T>(__shfl_xor_sync(0xffffffffu, send.x, 1), __shfl_xor_sync(0xffffffffu, send.y, 1));
+                    const cpx<T> mine = par ? o[H / 2 + i] : o[i];
+                    const int n = par ? H / 2 + i : i;
+                    if (valid && n < nz) buf[yzy_idx<P, W, S>(c, c * nz + n, sp, k1p, 0)] = mine + recv;
+                }
+                (void)kyp;
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---------------- C1: inverse stage 2 on the own k2 rows (k1 -> n1), times w_Ny^(-n1 k2)
+    for (int t = tid; t < nl * S * W; t += YZY_NT) {
+        const int w = t % W, s = (t / W) % S, line = t / (W * S);
+        const int c = line / nz;
+        const int k2 = Own::k2_of(r, s);
+        cpx<T> *row = buf + yzy_idx<P, W, S>(c, line, s, 0, w);
+        cpx<T> u[P];
+#pragma unroll
+        for (int j = 0; j < P; j++) u[j] = row[j * W];
+        RegFFT<T, P, true>::run(u, a.twy, Q);
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+            cpx<T> v = u[j];
+            if (j > 0 && k2 > 0) v = cmul(v, conj(a.twy[j * k2]));
+            row[j * W] = v;
+        }
+    }
+    cluster.sync();
+
+    // ---------------- C2: inverse stage 1 from the k2 owners, first ny rows to S1
+    for (int t = tid; t < myl * P * W; t += YZY_NT) {
+        const int w = t % W, n1 = (t / W) % P, i = t / (W * P);
+        const int line = r + YZY_C * i;
+        const int c = line / nz, z = line - c * nz;
+        cpx<T> v[Q];
+#pragma unroll
+        for (int k2 = 0; k2 < Q; k2++) {
+            int ro, so;
+            Own::where(k2, ro, so);
+            const cpx<T> *srcb = cluster.map_shared_rank(buf, ro);
+            v[k2] = srcb[yzy_idx<P, W, S>(c, line, so, n1, w)];
+        }
+        RegFFT<T, Q, true>::run(v, a.twy, P);
+        cpx<T> *dst = a.S1 + ((long long)(c * nz + z) * ny) * LX + kx0 + w;
+#pragma unroll
+        for (int n2 = 0; n2 < Q / 2; n2++) {
+            const int e = n1 + P * n2;
+            if (e < ny) dst[(long long)e * LX] = v[n2];
+        }
+    }
+    cluster.sync();
+}
+
+// ------------------------------------------------------------------------------ host side
+template <typename T> struct yzy_w { static constexpr int v = sizeof(T) == 4 ? 4 : 2; };
+
+template <typename T, int P, int Q, int NZ>
+static int launch_yzy_t(const YZArgs<T> &a, cudaStream_t s, bool check_only)
+{
+    constexpr int W = yzy_w<T>::v;
+    constexpr int S = YzyOwn<Q>::S;
+    const size_t smem = yzy_smem_bytes<T, P, W, S>(a.nz);
+    if (smem > 227 * 1024 || a.LX % W != 0 || a.nz > NZ / 2) return -1;
+    auto kern = k_yzy<T, P, Q, NZ, W>;
+    static bool opened = false;   // per instantiation: one fixed ceiling for every launch of it
+    if (!opened) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess) return -1;
+        opened = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((a.LX / W) * YZY_C, 1, 1);
+    cfg.blockDim = dim3(YZY_NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = YZY_C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (check_only) {
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg) != cudaSuccess || ncl < 1) {
+            cudaGetLastError();
+            return -1;
+        }
+        return 0;
+    }
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
+    return (int)e;
+}
+
+template <typename T, int P, int Q>
+static int yzy_nz(const YZArgs<T> &a, cudaStream_t s, bool check_only)
+{
+    switch (a.Nz) {
+    case 4: return launch_yzy_t<T, P, Q, 4>(a, s, check_only);
+    case 8: return launch_yzy_t<T, P, Q, 8>(a, s, check_only);
+    case 12: return launch_yzy_t<T, P, Q, 12>(a, s, check_only);
+    case 16: return launch_yzy_t<T, P, Q, 16>(a, s, check_only);
+    case 24: return launch_yzy_t<T, P, Q, 24>(a, s, check_only);
+    case 32: return launch_yzy_t<T, P, Q, 32>(a, s, check_only);
+    default: return -1;
+    }
+}
+
+template <typename T>
+static int yzy_dispatch(const YZArgs<T> &a, cudaStream_t s, bool check_only)
+{
+    if (a.nz < 2) return -1;
+    switch (a.Ny) {
+    case 512: return yzy_nz<T, 32, 16>(a, s, check_only);
+    case 1024: return yzy_nz<T, 32, 32>(a, s, check_only);
+    default: return -1;
+    }
+}
+
+// 0 when the fused cluster pass applies to this mesh (and the device can run its clusters)
+template <typename T> int yzy_available(const YZArgs<T> &a) { return yzy_dispatch<T>(a, nullptr, true); }
+template <typename T> int launch_yzy(const YZArgs<T> &a, cudaStream_t s) { return yzy_dispatch<T>(a, s, false); }
+
+template int yzy_available<float>(const YZArgs<float> &);
+template int yzy_available<double>(const YZArgs<double> &);
+template int launch_yzy<float>(const YZArgs<float> &, cudaStream_t);
+template int launch_yzy<double>(const YZArgs<double> &, cudaStream_t);

@@ -249,15 +249,15 @@ int bm_time_kernels(bm_ctx *ctx, int mesh, int reps, double *ms4, double *bytes4
 /* Run `steps` steps (RKDP54: attempts) of every mesh eagerly, with the launches, buffers and
  * arguments of the captured step graph, recording a CUDA event after every launch, and report
  * per kernel kind the summed device ms, the summed algorithmic bytes (what each launch must read
- * and write once, from its arguments) and the launch count: [0] fused stage kernel, [1] y forward,
- * [2] z pass, [3] y inverse, [4] 2D y pass, [5] other (restore launches, timed, no bytes). The
- * simulation advances. Not for batched meshes, the multilayered convolution or the evaluation
+ * and write once, from its arguments) and the launch count, in arrays of 8: [0] fused stage kernel,
+ * [1] y forward, [2] z pass, [3] y inverse, [4] 2D y pass, [5] other (restore launches, timed, no
+ * bytes), [6] fused y -> z -> y cluster pass, [7] unused. The simulation advances. Not for batched meshes, the multilayered convolution or the evaluation
  * speedup (BM_EUNSUPPORTED). No counterpart in the reference (measurement). */
 int bm_time_step(bm_ctx *ctx, int steps, double *ms6, double *bytes6, int *launches6);
 
 /* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width (plus 100
  * when the 3D y passes use the radix-16 Stockham transform),
- * z-pass width, stage rows per block (plus 100 when the stage kernel uses the radix-8
+ * z-pass width (plus 1000 when the fused y -> z -> y cluster pass replaces the three 3D passes), stage rows per block (plus 100 when the stage kernel uses the radix-8
  * Stockham x transform; negative when it prefetches its per-cell rows into shared
  * memory)]. Valid after the first compute or run. */
 int bm_tiles(bm_ctx *ctx, int mesh, int *tiles4);
