@@ -652,6 +652,13 @@ def main():
                     out["cpu_baseline"] = cb
             except Exception as e:
                 out["precision"] = {"error": str(e)}
+        if not ml and not cfg.get("batched"):
+            try:
+                out["reference_gpu"] = reference_gpu_bar(bm, cfg, local)
+                if "mixed" in out["reference_gpu"]:
+                    out["vs_ref_gpu_demag"] = out["reference_gpu"]["mixed"]["speedup"]
+            except Exception as e:
+                out["reference_gpu"] = {"error": str(e)}
         if not args.no_cpu_baseline and "cpu_baseline" not in out:
             try:
                 out["cpu_baseline"] = cpu_reference_rate(cfg)
@@ -730,6 +737,34 @@ def precision_film(bm, cfg, device, with_reference=True, ref_steps=2, gpu_steps=
                                      "iDMI+exchange" if cfg["modules"] & 4 else "exchange", setup),
             "sec_per_step": tsum / done}
     return res
+
+
+def reference_gpu_bar(bm, cfg, device, reps=20):
+    """The same-box reference GPU bar: one H_demag evaluation of the workload's film by the reference's
+    own GPU convolution (ConvolutionCUDA<., DemagKernelCUDA>: cuFFT plans, transposes and its fused
+    q2D z-product kernels, built unmodified for sm_100a by baseline/Makefile) in FP32 and FP64, against
+    one evaluation of this path (bm_time_demag: x transform, y / z passes, inverse x), device time
+    with CUDA events, plus the two fields' difference on the same M."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_libs import reference_gpu, ReferenceGPUDemag
+    M = init_m(cfg, 4321)
+    out = {"reps": reps}
+    for name, ours, refp in (("mixed", bm.MIXED, "f32"), ("fp64", bm.FP64, "f64")):
+        if reference_gpu(refp) is None:
+            return {"error": "reference GPU build (baseline/_ref) not present"}
+        c = make_ctx(bm, cfg, device, ours)
+        c.set_m(M)
+        H = c.demag_field()
+        t_ours = c.time_demag(0, reps)
+        c.close()
+        g = ReferenceGPUDemag(cfg["n"], cfg["h"], refp)
+        Hr = g.field(M)
+        t_ref = g.time(reps)
+        g.close()
+        out[name] = {"ours_ms_per_eval": t_ours, "reference_gpu_ms_per_eval": t_ref,
+                     "reference_gpu_precision": refp, "speedup": t_ref / t_ours,
+                     "h_demag_vs_reference_gpu": rel_err(H, Hr)}
+    return out
 
 
 def quick_rate(bm, cfg, prec, steps, warmup, device, ml_timing=False):

@@ -92,6 +92,10 @@ _SIGS = {
     "bm_run_timed": (_I, [_P, _I, ctypes.POINTER(Stats), _DP]),
     "bm_time_kernels": (_I, [_P, _I, _I, _DP, _DP]),
     "bm_time_step": (_I, [_P, _I, _DP, _DP, _IP]),
+    "bm_time_demag": (_I, [_P, _I, _I, _DP]),
+    "bm_demag_field_device": (_I, [_P, _I, _P, _P, _I, _I, _DP, _P]),
+    "bm_set_m_device": (_I, [_P, _I, _P, _I, _P]),
+    "bm_get_m_device": (_I, [_P, _I, _P, _I, _P]),
     "bm_tiles": (_I, [_P, _I, _IP]),
     "bm_debug_kernels": (_I, [_P, _I, _DP]),
     "bm_debug_tensor": (_I, [_I, _I, _I, _I, _D, _D, _D, _DP]),
@@ -390,6 +394,12 @@ class Context:
         by = np.zeros(4)
         _check(lib().bm_time_kernels(self._h, mesh, int(reps), _dp(ms), _dp(by)))
         return ms, by
+
+    def time_demag(self, mesh=0, reps=20):
+        """Device ms of one demag field evaluation (x transform, y / z passes, inverse x into H)."""
+        ms = ctypes.c_double(0.0)
+        _check(lib().bm_time_demag(self._h, mesh, int(reps), ctypes.byref(ms)))
+        return ms.value
 
     TIME_KINDS = ("stage", "yfwd", "zmid", "yinv", "ymid2d", "other", "yzy", "")
 

@@ -24,10 +24,6 @@ def _sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
-def _deps_mtime():
-    return max(os.path.getmtime(os.path.join(CSRC, f)) for f in os.listdir(CSRC))
-
-
 def _compile(src, extra):
     obj = os.path.join(OBJDIR, src + ".o")
     cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
@@ -37,18 +33,30 @@ def _compile(src, extra):
     return obj, r.stderr
 
 
+def _stale(src, hdr_mtime, force):
+    """A translation unit is recompiled when forced, when its object is missing, or when the object is
+    older than the source or than the newest shared header / build recipe."""
+    obj = os.path.join(OBJDIR, src + ".o")
+    if force or not os.path.exists(obj):
+        return True
+    return os.path.getmtime(obj) < max(os.path.getmtime(os.path.join(CSRC, src)), hdr_mtime)
+
+
 def build(force=False, verbose=False, extra=None):
-    """Compile (if stale) and return the path of the shared library."""
+    """Compile the stale translation units and link; returns the path of the shared library."""
     extra = list(extra or [])
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(OBJDIR, exist_ok=True)
     hdr = os.path.join(HERE, "..", "include", "boris_b200.h")
-    newest = max(_deps_mtime(), os.path.getmtime(hdr), os.path.getmtime(__file__))
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if not f.endswith((".cu", ".cpp"))]
+    hdr_mtime = max([os.path.getmtime(h) for h in headers] + [os.path.getmtime(hdr), os.path.getmtime(__file__)])
+    todo = [s for s in _sources() if extra or _stale(s, hdr_mtime, force)]
+    objs = [os.path.join(OBJDIR, s + ".o") for s in _sources()]
+    if not todo and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
         return LIB
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
-        results = list(ex.map(lambda s: _compile(s, extra), _sources()))
-    objs = [o for o, _ in results]
+        results = list(ex.map(lambda s: _compile(s, extra), todo))
+    objs = [os.path.join(OBJDIR, s + ".o") for s in _sources()]
     if verbose:
         for _, err in results:
             if err.strip():

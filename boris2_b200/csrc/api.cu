@@ -2323,6 +2323,112 @@ int bm_compute_hdemag(bm_ctx *c, int mesh, double *H, double *energy)
     return 0;
 }
 
+}  // extern "C"
+
+namespace {
+// Device-resident demag field for a caller that keeps M and Heff on the GPU as AoS vectors (the
+// reference's cuVEC<cuReal3> data): M into the context's state planes, x transform, y / z passes,
+// inverse x with the demag term alone, then H set or added into the caller's AoS array.
+template <typename T, typename S>
+int demag_device_T(bm_ctx *c, Mesh &m, const S *M, S *H, int add, double *energy)
+{
+    cudaStream_t s = c->stream;
+    CKL((launch_daos_to_planes<S, T>(B<T>(m, 0), M, m.n, s)), "M in");
+    StageArgs<T> a = stage_args<T>(c, m);
+    a.mode = BM_MODE_UPDATE;
+    a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0);
+    CKL(launch_stage<T>(a, s), "xfwd");
+    int cnt = 0;
+    if (int rc = enqueue_yz<T>(c, m, BM_GATE_ALWAYS, &cnt)) return rc;
+    StageArgs<T> h = stage_args<T>(c, m);
+    h.mode = BM_MODE_HEFF;
+    h.modules = BM_DEMAG;
+    h.do_xfwd = 0;
+    h.Min = B<T>(m, 0);
+    h.Hout = (T *)m.Hout;
+    CKL(launch_stage<T>(h, s), "inverse x");
+    double *dot = energy ? m.stage64 : nullptr;
+    if (dot) CK(cudaMemsetAsync(dot, 0, sizeof(double), s));
+    CKL((launch_planes_to_daos<S, T>(H, (const T *)m.Hout, m.n, add, M, dot, s)), "H out");
+    if (dot) {
+        double d = 0.0;
+        CK(cudaMemcpyAsync(&d, dot, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        *energy = -BM_MU0 * d / (2.0 * (double)m.n);
+    }
+    CK(cudaStreamSynchronize(s));
+    c->s1_dirty = true;
+    return 0;
+}
+
+template <typename T>
+int set_m_device_T(bm_ctx *c, Mesh &m, const void *M, int eb)
+{
+    if (eb == 4) CKL((launch_daos_to_planes<float, T>(B<T>(m, 0), (const float *)M, m.n, c->stream)), "M in");
+    else CKL((launch_daos_to_planes<double, T>(B<T>(m, 0), (const double *)M, m.n, c->stream)), "M in");
+    return 0;
+}
+
+template <typename T>
+int get_m_device_T(bm_ctx *c, Mesh &m, void *M, int eb)
+{
+    if (eb == 4) CKL((launch_planes_to_daos<float, T>((float *)M, B<T>(m, 0), m.n, 0, nullptr, nullptr, c->stream)), "M out");
+    else CKL((launch_planes_to_daos<double, T>((double *)M, B<T>(m, 0), m.n, 0, nullptr, nullptr, c->stream)), "M out");
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int device_entry_checks(bm_ctx *c, int mesh, const void *p, int eb, void *stream)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!p) return fail(BM_EINVAL, "null device array");
+    if (eb != 4 && eb != 8) return fail(BM_EINVAL, "element size must be 4 (float) or 8 (double)");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    // the caller's writes to its arrays on its stream come first
+    CK(cudaStreamSynchronize((cudaStream_t)stream));
+    return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int bm_demag_field_device(bm_ctx *c, int mesh, const void *M, void *H, int elem_bytes, int add, double *energy,
+                          void *stream)
+{
+    if (int rc = device_entry_checks(c, mesh, M, elem_bytes, stream)) return rc;
+    if (!H) return fail(BM_EINVAL, "null device array");
+    Mesh &m = c->meshes[mesh];
+    if (!(m.modules & BM_DEMAG) || m.ml_role) return fail(BM_ESTATE, "mesh has no demag convolution of its own");
+    if (c->precision == BM_FP64)
+        return elem_bytes == 4 ? demag_device_T<double, float>(c, m, (const float *)M, (float *)H, add, energy)
+                               : demag_device_T<double, double>(c, m, (const double *)M, (double *)H, add, energy);
+    return elem_bytes == 4 ? demag_device_T<float, float>(c, m, (const float *)M, (float *)H, add, energy)
+                           : demag_device_T<float, double>(c, m, (const double *)M, (double *)H, add, energy);
+}
+
+int bm_set_m_device(bm_ctx *c, int mesh, const void *M, int elem_bytes, void *stream)
+{
+    if (int rc = device_entry_checks(c, mesh, M, elem_bytes, stream)) return rc;
+    Mesh &m = c->meshes[mesh];
+    int rc = c->precision == BM_FP64 ? set_m_device_T<double>(c, m, M, elem_bytes) : set_m_device_T<float>(c, m, M, elem_bytes);
+    if (rc) return rc;
+    c->s1_dirty = true;
+    if ((rc = read_state(c))) return rc;
+    c->host_st.primed = 0;
+    c->host_st.error = 0;
+    c->es_reset = true;
+    c->dt = c->host_st.dT;
+    return upload_state(c);
+}
+
+int bm_get_m_device(bm_ctx *c, int mesh, void *M, int elem_bytes, void *stream)
+{
+    if (int rc = device_entry_checks(c, mesh, M, elem_bytes, stream)) return rc;
+    Mesh &m = c->meshes[mesh];
+    return c->precision == BM_FP64 ? get_m_device_T<double>(c, m, M, elem_bytes) : get_m_device_T<float>(c, m, M, elem_bytes);
+}
+
 int bm_compute_heff(bm_ctx *c, int mesh, double *H)
 {
     if (int rc = check_mesh(c, mesh)) return rc;
@@ -2617,6 +2723,50 @@ int bm_ml_time_kernels(bm_ctx *c, int reps, double *ms6, double *bytes6)
     if (!c->ml) return fail(BM_ESTATE, "multilayered convolution is off");
     cudaSetDevice(c->device);
     return (c->precision == BM_FP64) ? ml_time_T<double>(c, reps, ms6, bytes6) : ml_time_T<float>(c, reps, ms6, bytes6);
+}
+
+int bm_time_demag(bm_ctx *c, int mesh, int reps, double *ms)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (reps < 1 || !ms) return fail(BM_EINVAL, "bm_time_demag: bad arguments");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    Mesh &m = c->meshes[mesh];
+    if (!(m.modules & BM_DEMAG) || m.ml_role) return fail(BM_EUNSUPPORTED, "bm_time_demag: a mesh with its own demag convolution");
+    auto one = [&](auto tag) -> int {
+        using T = decltype(tag);
+        StageArgs<T> a = stage_args<T>(c, m);
+        a.mode = BM_MODE_UPDATE;
+        a.Min = B<T>(m, 0); a.Mbase = B<T>(m, 0);
+        if (int rc = launch_stage<T>(a, c->stream)) return rc;
+        int cnt = 0;
+        if (int rc = enqueue_yz<T>(c, m, BM_GATE_ALWAYS, &cnt)) return rc;
+        StageArgs<T> h = stage_args<T>(c, m);
+        h.mode = BM_MODE_HEFF;
+        h.modules = BM_DEMAG;
+        h.do_xfwd = 0;
+        h.Min = B<T>(m, 0);
+        h.Hout = (T *)m.Hout;
+        return launch_stage<T>(h, c->stream);
+    };
+    auto run = [&]() -> int { return c->precision == BM_FP64 ? one(0.0) : one(0.0f); };
+    if (int rc = run()) return fail(BM_ECUDA, "bm_time_demag: launch failed (" + std::to_string(rc) + ")");
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, c->stream));
+    int rc = 0;
+    for (int i = 0; i < reps && !rc; i++) rc = run();
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->s1_dirty = true;
+    if (rc) return fail(BM_ECUDA, "bm_time_demag: launch failed (" + std::to_string(rc) + ")");
+    *ms = (double)t / reps;
+    return 0;
 }
 
 int bm_time_step(bm_ctx *c, int steps, double *ms6, double *bytes6, int *launches6)

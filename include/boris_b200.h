@@ -209,6 +209,21 @@ int bm_save_ovf2_mag(bm_ctx *ctx, int mesh, const char *path, const char *data_t
  * DemagCUDA::UpdateField (Boris/DemagCUDA.cpp:106). */
 int bm_compute_hdemag(bm_ctx *ctx, int mesh, double *H, double *energy);
 
+/* Device-resident variants for a caller that keeps its vectors on the GPU as AoS arrays of
+ * float (elem_bytes 4) or double (8), x, y, z per cell, cells x fastest: the data of the
+ * reference's cuVEC<cuReal3> (BorisCUDALib/cuVEC.h). `stream` (a cudaStream_t, NULL for the
+ * default stream) is synchronised first, so the caller's pending writes to its arrays land before
+ * they are read; each call returns with its results written.
+ * bm_demag_field_device: the mesh's M becomes the given M, and its demag field is set (add = 0) or
+ * added (add = 1) into H; energy (optional) receives -mu0/(2 n) sum M.H_demag. Replaces the
+ * Convolute call of DemagCUDA::UpdateField (Boris/DemagCUDA.cpp:106-121), which adds into Heff.
+ * bm_set_m_device / bm_get_m_device: bm_set_m / bm_get_m with device arrays (the ODE state
+ * exchange of a forwarder of ODECommon_Base::IterateCUDA, Boris/DiffEq_CommonBase_IterateCUDA.cpp:13). */
+int bm_demag_field_device(bm_ctx *ctx, int mesh, const void *M, void *H, int elem_bytes, int add, double *energy,
+                          void *stream);
+int bm_set_m_device(bm_ctx *ctx, int mesh, const void *M, int elem_bytes, void *stream);
+int bm_get_m_device(bm_ctx *ctx, int mesh, void *M, int elem_bytes, void *stream);
+
 /* Effective field of the current M with all modules of the mesh (Zeeman, demag,
  * exchange / iDMI, anisotropy), as MeshBase::UpdateModules leaves Heff
  * (Boris/MeshBaseModules.cpp:76). */
@@ -254,6 +269,12 @@ int bm_time_kernels(bm_ctx *ctx, int mesh, int reps, double *ms4, double *bytes4
  * bytes), [6] fused y -> z -> y cluster pass, [7] unused. The simulation advances. Not for batched meshes, the multilayered convolution or the evaluation
  * speedup (BM_EUNSUPPORTED). No counterpart in the reference (measurement). */
 int bm_time_step(bm_ctx *ctx, int steps, double *ms6, double *bytes6, int *launches6);
+
+/* Device time (ms, CUDA events, average of reps) of one demag field evaluation of a mesh as the
+ * pipeline runs it: x transform of M, the y / z passes with the kernel product, inverse x transform
+ * into H (the demag term alone). The counterpart of one Convolute call of the reference's
+ * ConvolutionCUDA (Boris/ConvolutionCUDA.h:478), for the same-box comparison. */
+int bm_time_demag(bm_ctx *ctx, int mesh, int reps, double *ms);
 
 /* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width (plus 100
  * when the 3D y passes use the radix-16 Stockham transform),

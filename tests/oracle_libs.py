@@ -113,6 +113,65 @@ def ref_available():
     return os.path.exists(REF_SO) or os.path.isdir(REF_TREE)
 
 
+REFGPU_DIR = os.path.join(ROOT, "baseline", "_ref")
+_refgpu = {}
+
+
+def reference_gpu(precision="f32"):
+    """The reference's own GPU demag convolution (ConvolutionCUDA<., DemagKernelCUDA>, cuFFT) built for
+    sm_100a by baseline/Makefile, in FP32 ("f32", SINGLEPRECISION 1) or FP64 ("f64"); None when
+    neither the .so nor the reference tree is present. Loading it needs no GPU; calling it does."""
+    if precision not in _refgpu:
+        so = os.path.join(REFGPU_DIR, "librefgpu_%s.so" % precision)
+        if REF_TREE and os.path.isdir(REF_TREE):
+            reference()   # the CPU objects it links
+            subprocess.run(["make", "-C", os.path.join(ROOT, "baseline"), "-j8", "REF=" + REF_TREE], check=True,
+                           capture_output=True)
+        elif not os.path.exists(so):
+            return None
+        L = ctypes.CDLL(so)
+        L.refgpu_create.restype = P
+        L.refgpu_create.argtypes = [I, I, I, D, D, D, I]
+        L.refgpu_set_m.argtypes = [P, DP]
+        L.refgpu_eval.restype = D
+        L.refgpu_eval.argtypes = [P, I]
+        L.refgpu_get_h.argtypes = [P, DP]
+        L.refgpu_destroy.argtypes = [P]
+        _refgpu[precision] = L
+    return _refgpu[precision]
+
+
+class ReferenceGPUDemag:
+    """One reference GPU convolution of an n, h mesh (kernels built on the GPU as the reference does
+    by default)."""
+
+    def __init__(self, n, h, precision="f32"):
+        self.L = reference_gpu(precision)
+        self.n = int(np.prod(n))
+        self.h = self.L.refgpu_create(n[0], n[1], n[2], h[0], h[1], h[2], 1)
+        assert self.h, "reference GPU convolution could not be built"
+
+    def field(self, M):
+        Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+        assert self.L.refgpu_set_m(P(self.h), dp(Mf)) == 0
+        H = np.zeros(3 * self.n)
+        assert self.L.refgpu_get_h(P(self.h), dp(H)) == 0
+        return H.reshape(-1, 3)
+
+    def time(self, reps=20):
+        ms = self.L.refgpu_eval(P(self.h), int(reps))
+        assert ms > 0, "reference GPU evaluation failed"
+        return ms
+
+    def close(self):
+        if self.h:
+            self.L.refgpu_destroy(P(self.h))
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 def reference():
     """The reference's compiled CPU code (None when neither the .so nor the tree is present)."""
     global _ref
