@@ -413,6 +413,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="timed steps only (for profiler launch lists)")
+    ap.add_argument("--reference-gpu-bar", action="store_true",
+                    help="only the same-box reference GPU bar of the workload (for profiler launch lists)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     ncell = total_cells(cfg)
@@ -478,6 +480,13 @@ def main():
         return
 
     import boris2_b200 as bm
+    if args.reference_gpu_bar:
+        if rank == 0:
+            print(json.dumps(dict(base, reference_gpu=reference_gpu_bar(bm, cfg, local, reps=args.steps))))
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     prec = bm.MIXED if args.precision == "mixed" else bm.FP64
     c = make_ctx(bm, cfg, local, prec)
     M0 = init_all(cfg, 1234 + rank)
@@ -632,8 +641,10 @@ def main():
                 rk = dict(cfg, eval="RK4")
                 plain = quick_rate(bm, rk, bm.MIXED, extra_steps, args.warmup, local)
                 es3 = quick_rate(bm, dict(rk, evalspeedup=3), bm.MIXED, extra_steps + 3, args.warmup, local)
-                out["evalspeedup"] = {"workload": "film3d_512x512x16 RK4 dt 1e-14", "rk4_plain": plain,
-                                      "rk4_quadratic": es3, "speedup": es3["value"] / plain["value"]}
+                dp3 = quick_rate(bm, dict(cfg, evalspeedup=3), bm.MIXED, extra_steps + 3, args.warmup, local)
+                out["evalspeedup"] = {"workload": "film3d_512x512x16 RK4 dt 1e-14 / RKDP54 tol 1e-5", "rk4_plain": plain,
+                                      "rk4_quadratic": es3, "speedup": es3["value"] / plain["value"],
+                                      "rkdp54_quadratic": dp3, "rkdp54_speedup": dp3["value"] / value}
             except Exception as e:
                 out["evalspeedup"] = {"error": str(e)}
         # the differentiation workload: adjoint / forward device time

@@ -444,6 +444,8 @@ int upload_state(bm_ctx *c)
     if (c->es_reset) {
         h.es_saved = 0;
         for (int k = 0; k < 6; k++) h.es_t[k] = 0.0;
+        h.es_available = 1;
+        h.es_mode = 0;
         c->es_reset = false;
     }
     h.reject_flag = 0;
@@ -1514,9 +1516,62 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
     return 0;
 }
 
+// One RKDP54 field evaluation with the evaluation speedup: the device decides (k_es_decide) whether
+// it computes and saves the field or extrapolates; the save kernels, the y / z passes and the
+// extrapolation are all captured and each runs or skips on that decision.
+template <typename T>
+int enqueue_es_fields_dp(bm_ctx *c, int eval, double c_eval, int bi, int *count)
+{
+    const bool launch = !c->bp.collect;   // the speedup kernels are not part of a batched plan
+    const bool tab = c->es_tab != nullptr;
+    if (launch) {
+        CKL(launch_es_decide(c->st, eval, c_eval, c->stream), "es_decide");
+        (*count)++;
+        if (tab) {
+            CKL(launch_es_pre_batch<T>(c->es_tab, c->es_nmesh, c->es_max_plane, c->st, c->stream, 1), "es_pre_batch");
+            (*count)++;
+        } else {
+            for (auto &m : c->meshes) {
+                if (!(m.modules & BM_DEMAG)) continue;
+                CKL(launch_es_pre<T>((const cpx<T> *)m.S1, (cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c->stream, 1), "es_pre");
+                (*count)++;
+            }
+        }
+    }
+    if (int rc = enqueue_fields<T>(c, eval ? BM_GATE_ES_ACC : BM_GATE_ES, bi, count)) return rc;
+    if (!launch) return 0;
+    if (tab) {
+        CKL(launch_es_post_batch<T>(c->es_tab, c->es_nmesh, c->es_max_plane, c->st, c->stream, 1), "es_post_batch");
+        (*count)++;
+    } else {
+        for (auto &m : c->meshes) {
+            if (!(m.modules & BM_DEMAG)) continue;
+            CKL(launch_es_post<T>((const cpx<T> *)m.S1, (cpx<T> *)m.G, es_plane(m), c->st, c->stream, 1), "es_post");
+            (*count)++;
+        }
+    }
+    CKL(launch_es_commit(c->st, c->stream, 1), "es_commit");
+    (*count)++;
+    if (tab) {
+        CKL(launch_es_extrap_batch<T>(c->es_tab, c->es_nmesh, c->es_max_plane, c->st, c_eval, c->stream, 1), "es_extrap_batch");
+        (*count)++;
+    } else {
+        for (auto &m : c->meshes) {
+            if (!(m.modules & BM_DEMAG)) continue;
+            CKL(launch_es_extrap<T>((cpx<T> *)m.S1, (const cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c_eval, c->stream, 1),
+                "es_extrap");
+            (*count)++;
+        }
+    }
+    return 0;
+}
+
 template <typename T>
 int enqueue_rkdp_attempt(bm_ctx *c, int *count)
 {
+    // evaluation times of the Dormand-Prince stages (Get_EvalStep_Time, Boris/DiffEq_CommonBase_Iterate.cpp:1562)
+    static const double c_dp[6] = {0.0, 0.2, 0.3, 0.8, 8.0 / 9, 1.0};
+    const bool es = c->es_level > 0;
     // buffers: 0 = M, 1 = P (sM1), 2 = B, 3 = C ; evals 0..5
     const int nm = (int)c->meshes.size();
     // restore after a rejection: M = sM1 and its x transform
@@ -1535,7 +1590,7 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
     }
     // evaluation 0: FSAL rhs + error of the previous step + controller
     {
-        int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, 0, count);
+        int rc = es ? enqueue_es_fields_dp<T>(c, 0, c_dp[0], 0, count) : enqueue_fields<T>(c, BM_GATE_ALWAYS, 0, count);
         if (rc) return rc;
     }
     static const double bs[5] = {5179.0 / 57600, 7571.0 / 16695, 393.0 / 640, -92097.0 / 339200, 187.0 / 2100};
@@ -1591,7 +1646,8 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
         {35.0 / 384, 0.0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
     for (int s = 1; s <= 5; s++) {
         {
-            int rc = enqueue_fields<T>(c, BM_GATE_ACCEPTED, (s % 2 == 1) ? 2 : 3, count);
+            const int bi = (s % 2 == 1) ? 2 : 3;
+            int rc = es ? enqueue_es_fields_dp<T>(c, s, c_dp[s], bi, count) : enqueue_fields<T>(c, BM_GATE_ACCEPTED, bi, count);
             if (rc) return rc;
         }
         std::vector<StageArgs<T>> v;
@@ -1629,9 +1685,10 @@ int build_graph(bm_ctx *c)
 {
     drop_graph(c);
     int count = 0;
-    // evaluation speedup: one graph for the steps that still save fields, one for the extrapolating steps
+    // evaluation speedup: under RK4 one graph for the steps that still save fields, one for the
+    // extrapolating steps; under RKDP54 one graph whose evaluations decide on the device
     const bool es = c->es_level > 0 && c->eval == BM_RK4;
-    if (es && c->batched && c->meshes.size() > 1) {
+    if (c->es_level > 0 && c->batched && c->meshes.size() > 1) {
         std::vector<EsMesh> tab;
         for (auto &m : c->meshes) {
             if (!(m.modules & BM_DEMAG)) continue;
@@ -2443,7 +2500,6 @@ int bm_run(bm_ctx *c, int steps, bm_stats *out)
 {
     if (int rc = check_ctx(c)) return rc;
     if (steps < 0) return fail(BM_EINVAL, "steps < 0");
-    if (c->es_level > 0 && c->eval != BM_RK4) return fail(BM_EUNSUPPORTED, "evaluation speedup needs RK4");
     if (int rc = prepare(c)) return rc;
     cudaSetDevice(c->device);
     if (steps > 0) {
@@ -2509,7 +2565,6 @@ int bm_kernels_per_step(bm_ctx *c, int *count)
 int bm_run_timed(bm_ctx *c, int steps, bm_stats *out, double *device_ms)
 {
     if (int rc = check_ctx(c)) return rc;
-    if (c->es_level > 0 && c->eval != BM_RK4) return fail(BM_EUNSUPPORTED, "evaluation speedup needs RK4");
     if (int rc = prepare(c)) return rc;
     cudaSetDevice(c->device);
     if (c->s1_dirty) {

@@ -78,4 +78,11 @@ struct StepState {
     // evaluation speedup: fields saved so far (<= es_K) and the times they were saved at
     int es_saved, es_K;
     double es_t[6];
+    // evaluation speedup under RKDP54: the decision for the current evaluation (0 none, 1 compute and
+    // save into es_slot at time es_tnew, 2 extrapolate with the weights es_a), whether that save
+    // replaces the field of an already saved time (es_pad 1), and the reference's `available` flag
+    // (the previous step completed)
+    int es_mode, es_slot, es_available, es_pad;
+    double es_tnew;
+    double es_a[6];
 };

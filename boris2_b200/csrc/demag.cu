@@ -20,6 +20,9 @@ __device__ __forceinline__ bool gated_out(const StepState *st, int gate)
 {
     if (gate == BM_GATE_ALWAYS || st == nullptr) return false;
     if (gate == BM_GATE_ACCEPTED) return *((volatile const int *)&st->reject_flag) != 0;
+    if (gate == BM_GATE_ES || gate == BM_GATE_ES_ACC)
+        return *((volatile const int *)&st->es_mode) != 1 ||
+               (gate == BM_GATE_ES_ACC && *((volatile const int *)&st->reject_flag) != 0);
     return *((volatile const int *)&st->need_restore) == 0;
 }
 

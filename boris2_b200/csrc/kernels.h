@@ -22,6 +22,8 @@ void bm_far_coeffs(double hx, double hy, double hz, double *out);
 #define BM_GATE_ALWAYS 0
 #define BM_GATE_ACCEPTED 1      // skip when the current attempt was rejected
 #define BM_GATE_RESTORE 2       // run only when a restore is pending
+#define BM_GATE_ES 3            // evaluation speedup (RKDP54): run unless the evaluation extrapolates
+#define BM_GATE_ES_ACC 4        // as BM_GATE_ES, and skip when the current attempt was rejected
 
 // ---------------------------------------------------------------- y / z passes
 template <typename T>
@@ -217,11 +219,15 @@ void self_demag_host(double hx, double hy, double hz, double out3[3]);   // -N o
 // component). G holds es_K slots of 3 planes: the saved field minus its self term. cs[c] is the
 // self-demag coefficient (-N_c) times Ny Nz, the factor between the x-spectrum of M the stage kernel
 // writes and the x-spectrum of H the y inverse pass leaves.
+// sel 0: RK4 (the first evaluation of a step saves, the rest extrapolate once es_K are saved);
+// sel 1: RKDP54, each kernel acting on the decision k_es_decide recorded for the evaluation
 template <typename T>
-int launch_es_pre(const cpx<T> *S1, cpx<T> *G, long long plane, const double *cs, const StepState *st, cudaStream_t s);
+int launch_es_pre(const cpx<T> *S1, cpx<T> *G, long long plane, const double *cs, const StepState *st, cudaStream_t s,
+                  int sel = 0);
 template <typename T>
-int launch_es_post(const cpx<T> *S1, cpx<T> *G, long long plane, const StepState *st, cudaStream_t s);
-int launch_es_commit(StepState *st, cudaStream_t s);
+int launch_es_post(const cpx<T> *S1, cpx<T> *G, long long plane, const StepState *st, cudaStream_t s, int sel = 0);
+int launch_es_commit(StepState *st, cudaStream_t s, int sel = 0);
+int launch_es_decide(StepState *st, int eval, double c_eval, cudaStream_t s);
 // all meshes of a batched context in one launch: a device table of one EsMesh per mesh with demag
 struct EsMesh {
     void *S1, *G;
@@ -229,12 +235,12 @@ struct EsMesh {
     double cs[3];
 };
 template <typename T>
-int launch_es_pre_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, cudaStream_t s);
+int launch_es_pre_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, cudaStream_t s, int sel = 0);
 template <typename T>
-int launch_es_post_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, cudaStream_t s);
+int launch_es_post_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, cudaStream_t s, int sel = 0);
 template <typename T>
 int launch_es_extrap_batch(const EsMesh *tab, int nmesh, long long max_plane, const StepState *st, double c_eval,
-                           cudaStream_t s);
+                           cudaStream_t s, int sel = 0);
 template <typename T>
 int launch_es_extrap(cpx<T> *S1, const cpx<T> *G, long long plane, const double *cs, const StepState *st, double c_eval,
-                     cudaStream_t s);
+                     cudaStream_t s, int sel = 0);

@@ -487,6 +487,7 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, u
         st->time = st->time + st->dT;
         st->stagetime = st->stagetime + st->dT;
         st->accepted = st->accepted + 1;
+        st->es_available = 1;   // the step completed (the reference's `available`)
     } else if (a.last_kind == BM_LAST_RESTORED) {
         st->need_restore = 0;
     } else if (a.last_kind == BM_LAST_CONTROL) {
@@ -502,6 +503,7 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, u
                 st->accepted = st->accepted - 1;
                 st->rejected = st->rejected + 1;
                 st->need_restore = 1;
+                st->es_available = 0;
             }
             st->primed = 0;
             st->reject_flag = 1;
@@ -515,6 +517,7 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, u
             double ord = (double)(st->eval_order + 1);
             if (dmin != dmax) {
                 if (lte > tol && dT > dmin) {
+                    st->es_available = 0;   // failed, must repeat (SetAdaptiveTimeStep)
                     st->time = st->time - dT;
                     st->stagetime = st->stagetime - dT;
                     st->accepted = st->accepted - 1;

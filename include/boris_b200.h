@@ -164,12 +164,15 @@ int bm_prepare(bm_ctx *ctx);
 
 /* Evaluation speedup, the reference's `evalspeedup` command (Boris/Simulation.cpp:551,
  * Boris/DemagCUDA.cpp:106): level 0 off, 1 step, 2 linear, 3 quadratic, 4 cubic, 5 quartic,
- * 6 quintic. The demag field is computed at the first evaluation of every RK4 step and saved
- * without its self term; the other evaluations extrapolate it from the last `level` saved fields
- * (polynomial in time) plus the self term of the current M, once that many are saved. RK4 only
- * (bm_run gives BM_EUNSUPPORTED with RKDP54), no multilayered convolution; with batched meshes the
- * y/z passes stay batched and the extrapolation covers every mesh in one launch. Setting M drops the
- * saved fields. */
+ * 6 quintic. A computed demag field is saved without its self term; other evaluations extrapolate
+ * it from the last `level` saved fields (polynomial in time) plus the self term of the current M.
+ * RK4: the field is computed and saved at the first evaluation of every step, the other
+ * evaluations extrapolate once `level` fields are saved. RKDP54: the reference's rule, decided on
+ * the device per evaluation: compute and save at the first evaluation of an attempt that follows a
+ * completed step, and at every evaluation while fewer than `level` are saved; extrapolate otherwise
+ * (so after a rejected step the repeated first evaluation extrapolates). No multilayered
+ * convolution; with batched meshes the y/z passes stay batched and the speedup kernels cover every
+ * mesh in one launch. Setting M drops the saved fields. */
 int bm_set_evalspeedup(bm_ctx *ctx, int level);
 /* Self-demagnetising coefficients -N (x, y, z) of one cell of size hx, hy, hz (DemagTFunc::SelfDemag,
  * Boris/DemagTFunc_Self.cpp:6); host only. */

@@ -49,6 +49,9 @@ void bm_fft_exec(int n, const double *tw, double *data, int sign, double *scratc
 
 /* ------------------------------------------------------------------ sums */
 
+/* cell loops run in parallel only above this many cells (thread start-up dominates small meshes) */
+#define ORC_PAR_MIN 32768
+
 /* Neumaier compensated sum of v[0..n) */
 static double csum(const double *v, int n)
 {
@@ -874,7 +877,7 @@ int orc_ml_eval(orc_ml *s, const double *M, double *H)
         for (int q = 0; q < L; q++) {
             const ml_kernel *K = &s->ker[y->kidx[q]];
             const int inv = y->kinv[q];
-#pragma omp parallel for
+#pragma omp parallel for if ((np) > ORC_PAR_MIN)
             for (long p = 0; p < (long)np; p++) {
                 for (int a = 0; a < 3; a++) {
                     double re = 0.0, im = 0.0;
@@ -972,7 +975,7 @@ void orc_field_exchange(int nx, int ny, int nz, double hx, double hy, double hz,
                         double A, const double *Ms_cell, double *H)
 {
     static const double zero[3] = {0, 0, 0};
-#pragma omp parallel for collapse(2)
+#pragma omp parallel for collapse(2) if (((long)nx * ny * nz) > ORC_PAR_MIN)
     for (int k = 0; k < nz; k++)
         for (int j = 0; j < ny; j++)
             for (int i = 0; i < nx; i++) {
@@ -991,7 +994,7 @@ void orc_field_idmi(int nx, int ny, int nz, double hx, double hy, double hz, con
                     double A, double D, const double *Ms_cell, double *H)
 {
     static const double zero[3] = {0, 0, 0};
-#pragma omp parallel for collapse(2)
+#pragma omp parallel for collapse(2) if (((long)nx * ny * nz) > ORC_PAR_MIN)
     for (int k = 0; k < nz; k++)
         for (int j = 0; j < ny; j++)
             for (int i = 0; i < nx; i++) {
@@ -1015,7 +1018,7 @@ void orc_field_idmi(int nx, int ny, int nz, double hx, double hy, double hz, con
 void orc_field_aniuni(int n, const double *M, const double *Ms_cell, const double *K1_cell, double K2,
                       const double *ea, double *H)
 {
-#pragma omp parallel for
+#pragma omp parallel for if ((n) > ORC_PAR_MIN)
     for (int i = 0; i < n; i++) {
         double Ms = Ms_cell[i], K1 = K1_cell[i];
         const double *m = M + 3 * (size_t)i;
@@ -1056,6 +1059,7 @@ struct orc_solver {
        saved fields, es_mode of the current evaluation (0 full, 1 full + save, 2 extrapolate) */
     int es_level, es_saved, es_mode, es_slot;
     double es_t[6], es_a[6];
+    int es_available;    /* the reference's ODECommon_Base::available: the previous step completed */
 };
 
 static int fft_size(int n) { return n > 1 ? 2 * n : 1; }
@@ -1137,6 +1141,9 @@ int orc_set_m(orc_solver *s, int q, const double *M)
 {
     memcpy(s->m[q].M, M, sizeof(double) * 3 * s->m[q].n);
     s->primed = 0;
+    /* a new state drops the fields saved for the evaluation speedup */
+    s->es_saved = 0;
+    s->es_available = 1;
     return 0;
 }
 
@@ -1179,7 +1186,7 @@ static void update_fields(orc_solver *s, orc_mesh *m)
     size_t n = (size_t)m->n;
     double Ha[3];
     applied_field(d, s->stagetime, Ha);
-#pragma omp parallel for
+#pragma omp parallel for if ((n) > ORC_PAR_MIN)
     for (long i = 0; i < (long)n; i++) { m->H[3 * i] = Ha[0]; m->H[3 * i + 1] = Ha[1]; m->H[3 * i + 2] = Ha[2]; }
     if (m->hook) {
         m->hook(m->hook_user, m->M, m->H);
@@ -1284,6 +1291,54 @@ static int adaptive_dt(orc_solver *s, double lte)
    (into the next free slot, then into the slot holding the earliest time); the others compute it in
    full until `level` fields are saved, then extrapolate with the Lagrange polynomial through the
    saved times. */
+/* the slot the next saved field goes to (Boris/DemagCUDA.cpp:158-280): the next free one while fewer
+   than K are saved; then the first when the saved times increase, else the first slot whose time is
+   below its predecessor's, else the last */
+static int es_slot_rule(const orc_solver *s)
+{
+    int K = s->es_level;
+    if (s->es_saved < K) return s->es_saved;
+    if (K == 1) return 0;
+    int inc = 1;
+    for (int k = 1; k < K; k++) inc = inc && (s->es_t[k] > s->es_t[k - 1]);
+    if (inc) return 0;
+    for (int j = 1; j < K - 1; j++)
+        if (s->es_t[j - 1] > s->es_t[j]) return j;
+    return K - 1;
+}
+
+/* save the field of this evaluation (time t) into the slot of the rule; a save at a time already
+   saved replaces that slot instead (deviation: under RKDP54 the last stage and the next step's first
+   evaluation share the time t + dT, and the reference's rule would then keep two fields at one time,
+   a zero Lagrange denominator at level 6) */
+static void es_save_at(orc_solver *s, double t)
+{
+    for (int k = 0; k < s->es_saved; k++)
+        if (s->es_t[k] == t) {
+            s->es_slot = k;
+            s->es_mode = 1;
+            return;
+        }
+    int slot = es_slot_rule(s);
+    /* a level-1 (step) save keeps its time once cycling (Boris/DemagCUDA.cpp:276) */
+    if (!(s->es_level == 1 && s->es_saved >= 1)) s->es_t[slot] = t;
+    if (s->es_saved < s->es_level) s->es_saved++;
+    s->es_slot = slot;
+    s->es_mode = 1;
+}
+
+static void es_weights(orc_solver *s, double t)
+{
+    int K = s->es_level;
+    for (int k = 0; k < K; k++) {
+        double a = 1.0;
+        for (int j = 0; j < K; j++)
+            if (j != k) a *= (t - s->es_t[j]) / (s->es_t[k] - s->es_t[j]);
+        s->es_a[k] = a;
+    }
+    s->es_mode = 2;
+}
+
 static void es_prepare(orc_solver *s, int stage)
 {
     static const double c_rk4[4] = {0.0, 0.5, 0.5, 1.0};
@@ -1291,22 +1346,22 @@ static void es_prepare(orc_solver *s, int stage)
     if (!s->es_level) return;
     int K = s->es_level;
     double t = s->time + s->dT * c_rk4[stage];
-    if (stage == 0) {
-        int slot = 0;
-        if (s->es_saved < K) slot = s->es_saved++;
-        else for (int k = 1; k < K; k++) if (s->es_t[k] < s->es_t[slot]) slot = k;
-        s->es_t[slot] = t;
-        s->es_slot = slot;
-        s->es_mode = 1;
-    } else if (s->es_saved >= K) {
-        for (int k = 0; k < K; k++) {
-            double a = 1.0;
-            for (int j = 0; j < K; j++)
-                if (j != k) a *= (t - s->es_t[j]) / (s->es_t[k] - s->es_t[j]);
-            s->es_a[k] = a;
-        }
-        s->es_mode = 2;
-    }
+    if (stage == 0) es_save_at(s, t);
+    else if (s->es_saved >= K) es_weights(s, t);
+}
+
+/* RKDP54 (DemagCUDA::UpdateField, Boris/DemagCUDA.cpp:139-144, with Check_Step_Update returning
+   `available` and Get_EvalStep_Time at the Dormand-Prince nodes, Boris/DiffEq_CommonBase_Iterate.cpp:
+   1562,1656): compute and save when the previous step completed and this is the attempt's first
+   evaluation, or while fewer than K are saved; extrapolate otherwise */
+static void es_prepare_dp(orc_solver *s, int eval)
+{
+    static const double c_dp[6] = {0.0, 0.2, 0.3, 0.8, 8.0 / 9, 1.0};
+    s->es_mode = 0;
+    if (!s->es_level) return;
+    double t = s->time + s->dT * c_dp[eval];
+    if ((eval == 0 && s->es_available) || s->es_saved < s->es_level) es_save_at(s, t);
+    else es_weights(s, t);
 }
 
 int orc_solver_set_evalspeedup(orc_solver *s, int level)
@@ -1314,6 +1369,7 @@ int orc_solver_set_evalspeedup(orc_solver *s, int level)
     if (level < 0 || level > 6 || s->ml) return 1;
     s->es_level = level;
     s->es_saved = 0;
+    s->es_available = 1;
     for (int q = 0; q < s->nmesh; q++) {
         orc_mesh *m = &s->m[q];
         orc_selfdemag(m->d.hx, m->d.hy, m->d.hz, m->self);
@@ -1334,7 +1390,7 @@ static void rk4_step(orc_solver *s)
         for (int q = 0; q < s->nmesh; q++) {
             orc_mesh *m = &s->m[q];
             const orc_mesh_desc *d = &m->d;
-#pragma omp parallel for
+#pragma omp parallel for if ((m->n) > ORC_PAR_MIN)
             for (int i = 0; i < m->n; i++) {
                 double *M = m->M + 3 * (size_t)i, *H = m->H + 3 * (size_t)i;
                 double *M1 = m->sM1 + 3 * (size_t)i;
@@ -1360,6 +1416,7 @@ static void rk4_step(orc_solver *s)
 static int rkdp_attempt(orc_solver *s)
 {
     /* evalStep 0: FSAL rhs, 4th-order prediction, lte (DiffEqFM_Evals_RKDP54.cpp:52-88) */
+    es_prepare_dp(s, 0);
     update_all_fields(s);
     double lte = 0.0;
     for (int q = 0; q < s->nmesh; q++) {
@@ -1367,7 +1424,7 @@ static int rkdp_attempt(orc_solver *s)
         const orc_mesh_desc *d = &m->d;
         double dT = s->dT;
         double lmax = 0.0;
-#pragma omp parallel for reduction(max:lmax)
+#pragma omp parallel for reduction(max:lmax) if ((m->n) > ORC_PAR_MIN)
         for (int i = 0; i < m->n; i++) {
             size_t o = 3 * (size_t)i;
             double f[3];
@@ -1392,13 +1449,14 @@ static int rkdp_attempt(orc_solver *s)
             for (int q = 0; q < s->nmesh; q++) memcpy(s->m[q].M, s->m[q].sM1, sizeof(double) * 3 * s->m[q].n);
             s->primed = 0;
             s->rejected++;
+            s->es_available = 0;   /* failed - must repeat (SetAdaptiveTimeStep) */
             return 0;
         }
     } else s->primed = 1;
     double dT = s->dT;
     for (int q = 0; q < s->nmesh; q++) {
         orc_mesh *m = &s->m[q];
-#pragma omp parallel for
+#pragma omp parallel for if ((m->n) > ORC_PAR_MIN)
         for (long o = 0; o < 3 * (long)m->n; o++) {
             m->sM1[o] = m->M[o];
             m->M[o] += m->sEval[0][o] * (dT / 5);
@@ -1412,11 +1470,12 @@ static int rkdp_attempt(orc_solver *s)
         {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656},
         {35.0 / 384, 0.0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
     for (int st = 1; st <= 5; st++) {
+        es_prepare_dp(s, st);
         update_all_fields(s);
         for (int q = 0; q < s->nmesh; q++) {
             orc_mesh *m = &s->m[q];
             const orc_mesh_desc *d = &m->d;
-#pragma omp parallel for
+#pragma omp parallel for if ((m->n) > ORC_PAR_MIN)
             for (int i = 0; i < m->n; i++) {
                 size_t o = 3 * (size_t)i;
                 double f[3];
@@ -1434,6 +1493,7 @@ static int rkdp_attempt(orc_solver *s)
     s->time += dT;
     s->stagetime += dT;
     s->accepted++;
+    s->es_available = 1;   /* done for this step (the reference's `available = true`) */
     return 1;
 }
 

@@ -1,8 +1,10 @@
-"""Evaluation speedup of RK4 on cuda:0 against the oracle's restatement of the reference's
+"""Evaluation speedup on cuda:0 against the oracle's restatement of the reference's
 (DemagCUDA::UpdateField, Boris/DemagCUDA.cpp:106-470): levels 1 (step) .. 6 (quintic), 2D and 3D
-meshes. FP64 <= 1e-9 of Ms after the run; mixed precision <= 1e-4. The runs must also differ from
-the run without the speedup by more than those tolerances, so the extrapolating path is the one
-measured."""
+meshes, under RK4 and under RKDP54 (the reference's rule decided on the device per evaluation,
+including the repeated first evaluation after a rejected step). FP64 <= 1e-9 of Ms after the run
+(RKDP54: also the same accepted and rejected counts); mixed precision <= 1e-4. The runs must also
+differ from the run without the speedup by more than those tolerances, so the extrapolating path is
+the one measured."""
 import numpy as np
 import pytest
 
@@ -15,16 +17,19 @@ FILM = dict(n=(32, 16, 1), h=(5e-9, 5e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.5, m
 BOX = dict(n=(16, 12, 4), h=(3e-9, 3e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(0, 2e3, 0))
 
 
-def _oracle(mesh, M, steps, dt, level):
-    s = OracleSolver([mesh], evaluation=0, dt=dt)
+def _oracle(mesh, M, steps, dt, level, evaluation=0, ctrl=None):
+    kw = {} if ctrl is None else dict(tol=ctrl[0], dT_incr=ctrl[1], dT_min=ctrl[2], dT_max=ctrl[3])
+    s = OracleSolver([mesh], evaluation=evaluation, dt=dt, **kw)
     s.evalspeedup(level)
     s.set_m(M)
-    s.run(steps)
-    return s.get_m()
+    st = s.run(steps)
+    m = s.get_m()
+    s.close()
+    return (m, st) if evaluation else m
 
 
 @pytest.mark.parametrize("mesh", [FILM, BOX], ids=["film2d", "box3d"])
-@pytest.mark.parametrize("level", [1, 2, 3, 4, 6])
+@pytest.mark.parametrize("level", [1, 2, 3, 4, 5, 6])
 def test_evalspeedup_fp64(bm, mesh, level):
     N = int(np.prod(mesh["n"]))
     M = sphere_random(N, seed=77 + level, Ms=8e5)
@@ -69,12 +74,82 @@ def test_evalspeedup_refusals(bm):
     c = _make(bm, "fp64", mesh, M, "RKDP54", 1e-13)
     with pytest.raises(bm.BorisError):
         c.evalspeedup(7)
-    c.evalspeedup(3)
-    with pytest.raises(bm.BorisError):
-        c.run(2)                                    # RKDP54 with the speedup is refused
     c.evalspeedup(0)
-    c.run(2)                                        # and the context stays usable
+    c.run(2)                                        # the context stays usable
     c.close()
+
+
+CTRL = (1e-5, 2.0, 1e-15, 3e-12)
+
+
+@pytest.mark.parametrize("mesh", [FILM, BOX], ids=["film2d", "box3d"])
+@pytest.mark.parametrize("level", [1, 2, 3, 4, 5, 6])
+def test_evalspeedup_rkdp54_fp64(bm, mesh, level):
+    """RKDP54 with the speedup: every accepted and rejected step, the simulated time and m follow the
+    oracle."""
+    N = int(np.prod(mesh["n"]))
+    M = sphere_random(N, seed=31 + level, Ms=8e5)
+    steps, dt = 25, 2e-14
+    (mref, sref) = _oracle(mesh, M, steps, dt, level, evaluation=1, ctrl=CTRL)
+    (mplain, _) = _oracle(mesh, M, steps, dt, 0, evaluation=1, ctrl=CTRL)
+    c = _make(bm, "fp64", mesh, M, "RKDP54", dt, CTRL)
+    c.evalspeedup(level)
+    st = c.run(steps)
+    m = c.get_m()
+    c.close()
+    assert st["accepted"] == steps and st["rejected"] == sref["rejected"]
+    assert abs(st["time"] - sref["time"]) <= 1e-9 * sref["time"]
+    err = np.abs(m - mref).max() / 8e5
+    assert err < 1e-9, err
+    assert np.abs(mref - mplain).max() / 8e5 > 1e-8
+
+
+@pytest.mark.parametrize("level", [2, 3, 6])
+def test_evalspeedup_rkdp54_rejections(bm, level):
+    """A large first step forces rejections: the repeated first evaluation extrapolates, with the field
+    saved at the rejected step's end kept in its slot, exactly as in the oracle (FP64 counts, time and
+    m). The mixed-precision path completes with a finite state (from this random start with a tight
+    tolerance FP32 takes its own accept / reject decisions, so it is not compared cell by cell)."""
+    mesh = dict(n=(16, 16, 1), h=(4e-9, 4e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.5, modules=1 | 2 | 16, Ha=(1e4, 0, 0))
+    M = sphere_random(256, seed=21, Ms=8e5)
+    ctrl = (1e-6, 2.0, 1e-16, 1e-11)
+    (mref, sref) = _oracle(mesh, M, 30, 2e-12, level, evaluation=1, ctrl=ctrl)
+    assert sref["rejected"] > 0
+    for prec, tol in (("fp64", 1e-8), ("mixed", 1e-4)):
+        c = _make(bm, prec, mesh, M, "RKDP54", 2e-12, ctrl)
+        c.evalspeedup(level)
+        st = c.run(30)
+        m = c.get_m()
+        c.close()
+        assert st["accepted"] == 30 and np.isfinite(m).all()
+        if prec == "fp64":
+            assert st["rejected"] == sref["rejected"]
+            assert abs(st["time"] - sref["time"]) <= 1e-9 * sref["time"]
+            assert np.abs(m - mref).max() / 8e5 < tol
+
+
+def test_evalspeedup_rkdp54_batched(bm):
+    """Batched uneven meshes under RKDP54 with quadratic extrapolation: the speedup kernels cover every
+    mesh in one launch and the run follows the oracle (FP64, 1e-9 of each mesh's Ms)."""
+    from test_gpu_batch import _descs, _ctx, _init
+    descs = _descs(modules=1 | 2 | 16)
+    M0 = _init(descs, "sphere")
+    s = OracleSolver(descs, evaluation=1, dt=2e-14, tol=CTRL[0], dT_incr=CTRL[1], dT_min=CTRL[2], dT_max=CTRL[3])
+    s.evalspeedup(3)
+    for q, M in enumerate(M0):
+        s.set_m(M, q)
+    sref = s.run(10)
+    c = _ctx(bm, "fp64", True, descs, "RKDP54", 2e-14)
+    c.astepctrl(*CTRL)
+    c.evalspeedup(3)
+    for q, M in enumerate(M0):
+        c.set_m(M, q)
+    st = c.run(10)
+    assert st["rejected"] == sref["rejected"]
+    err = max(np.abs(c.get_m(q) - s.get_m(q)).max() / d["Ms"] for q, d in enumerate(descs))
+    c.close()
+    s.close()
+    assert err < 1e-9, err
 
 
 def test_evalspeedup_batched_uneven_systems(bm):

@@ -40,6 +40,40 @@ def test_warmup_steps_are_exact():
     assert not np.array_equal(_run(6, steps=7), _run(0, steps=7))
 
 
+def _run_dp(level, steps=20, dt=2e-14, ctrl=(1e-5, 2.0, 1e-15, 3e-12), seed=4, Ha=(1e3, 0, 0)):
+    M = sphere_random(16 * 8, seed=seed, Ms=8e5)
+    s = OracleSolver([dict(FILM, Ha=Ha)], evaluation=1, dt=dt, tol=ctrl[0], dT_incr=ctrl[1], dT_min=ctrl[2],
+                     dT_max=ctrl[3])
+    s.evalspeedup(level)
+    s.set_m(M)
+    st = s.run(steps)
+    m = s.get_m()
+    s.close()
+    return m, st
+
+
+def test_rkdp54_levels_approach_plain():
+    """RKDP54 with the reference's rule (save while fewer than `level` are saved and at the first
+    evaluation after a completed step, extrapolate otherwise), at a fixed step (dT_min = dT_max) so
+    every run ends at the same time: the extrapolation error shrinks with the polynomial order up to
+    quadratic and stays small beyond (measured 8e-5, 6e-7, 1e-8, 1e-8, 2e-8, 8e-8 of Ms for levels 1..6)."""
+    ctrl = (1e-5, 2.0, 2e-14, 2e-14)
+    plain, sp = _run_dp(0, ctrl=ctrl, steps=30)
+    errs = [np.abs(_run_dp(k, ctrl=ctrl, steps=30)[0] - plain).max() / 8e5 for k in (1, 2, 3, 4, 5, 6)]
+    assert errs[0] > errs[1] > errs[2] > 0
+    assert max(errs[2:]) < 1e-6
+
+
+def test_rkdp54_rejections_stay_finite():
+    """With rejections (a large first step and a tight tolerance) the repeated first evaluation
+    extrapolates from fields that include one saved at the rejected step's end; the run completes with
+    finite m and rejections counted."""
+    for level in (1, 2, 3, 6):
+        m, st = _run_dp(level, steps=30, dt=2e-12, ctrl=(1e-6, 2.0, 1e-16, 1e-11), Ha=(1e4, 0, 0))
+        assert st["rejected"] > 0 and st["accepted"] == 30
+        assert np.isfinite(m).all()
+
+
 @pytest.mark.parametrize("h", [(1.0, 1.0, 1.0), (1.0, 1.0, 0.6), (0.5, 1.0, 0.75), (5.0, 5.0, 3.0)])
 def test_self_demag_matches_reference(h):
     import boris2_b200
