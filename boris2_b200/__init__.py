@@ -49,6 +49,7 @@ class BorisError(RuntimeError):
 
 
 OK, EINVAL, ECUDA, ENOMEM, ESTATE, EUNSUPPORTED, ENONFINITE = 0, 1, 2, 3, 4, 5, 6
+PBC_MAX_IMAGES = 1000   # BM_PBC_MAX_IMAGES
 
 
 class Stats(ctypes.Structure):
@@ -75,6 +76,8 @@ _SIGS = {
     "bm_set_material": (_I, [_P, _I, _D, _D, _D, _D, _D, _D, _DP, _D]),
     "bm_set_material_maps": (_I, [_P, _I, _DP, _DP]),
     "bm_set_modules": (_I, [_P, _I, _I]),
+    "bm_set_pbc": (_I, [_P, _I, _I, _I, _I]),
+    "bm_get_pbc": (_I, [_P, _I, _IP]),
     "bm_set_field": (_I, [_P, _I, _DP, _I, _D]),
     "bm_set_ode": (_I, [_P, _I, _D]),
     "bm_set_astepctrl": (_I, [_P, _D, _D, _D, _D]),
@@ -99,6 +102,7 @@ _SIGS = {
     "bm_tiles": (_I, [_P, _I, _IP]),
     "bm_debug_kernels": (_I, [_P, _I, _DP]),
     "bm_debug_tensor": (_I, [_I, _I, _I, _I, _D, _D, _D, _DP]),
+    "bm_debug_tensor_pbc": (_I, [_I, _I, _I, _I, _D, _D, _D, _IP, _DP]),
     "bm_debug_fft": (_I, [_I, _I, _I, _I, _I, _DP]),
     "bm_fft_noalloc": (_I, [_I, _I, _I, _I, _P, _P, _P]),
     "bm_set_multiconvolution": (_I, [_P, _I, _IP]),
@@ -250,6 +254,17 @@ class Context:
 
     def set_modules(self, mesh=0, modules=DEMAG | EXCH | ZEEMAN):
         _check(lib().bm_set_modules(self._h, mesh, int(modules)))
+
+    def set_pbc(self, mesh=0, images=(0, 0, 0)):
+        """Periodic boundary conditions: images per axis (0 = not periodic), as the reference's
+        Demag::Set_PBC / "pbc" command."""
+        x, y, z = (int(v) for v in images)
+        _check(lib().bm_set_pbc(self._h, mesh, x, y, z))
+
+    def get_pbc(self, mesh=0):
+        out = (ctypes.c_int * 3)()
+        _check(lib().bm_get_pbc(self._h, mesh, out))
+        return tuple(out)
 
     def set_field(self, mesh=0, Ha=(0.0, 0.0, 0.0), t_span=0.0):
         a = np.ascontiguousarray(np.asarray(Ha, dtype=np.float64).reshape(-1, 3))
@@ -457,9 +472,15 @@ class Context:
         return K.reshape(6, N[2] // 2 + 1, N[1] // 2 + 1, N[0] // 2 + 1)
 
 
-def debug_tensor(n, h, device=0):
+def debug_tensor(n, h, device=0, pbc=None):
     oct6 = np.empty(6 * n[0] * n[1] * n[2])
-    _check(lib().bm_debug_tensor(device, int(n[0]), int(n[1]), int(n[2]), float(h[0]), float(h[1]), float(h[2]), _dp(oct6)))
+    if pbc is None:
+        _check(lib().bm_debug_tensor(device, int(n[0]), int(n[1]), int(n[2]), float(h[0]), float(h[1]), float(h[2]),
+                                     _dp(oct6)))
+    else:
+        p3 = (ctypes.c_int * 3)(*(int(v) for v in pbc))
+        _check(lib().bm_debug_tensor_pbc(device, int(n[0]), int(n[1]), int(n[2]), float(h[0]), float(h[1]), float(h[2]),
+                                         p3, _dp(oct6)))
     return oct6.reshape(n[2], n[1], n[0], 6)
 
 

@@ -37,19 +37,29 @@ __device__ __forceinline__ void block_sum_add(double v, double *out)
     __syncthreads();
 }
 
-// Neumann Laplacian of one component at cell (x, y, z): only existing neighbours
+// Neumann Laplacian of one component at cell (x, y, z): only existing neighbours; along a periodic
+// axis the far-side cell, times the axis' sign, stands in for the missing one (the operator stays
+// symmetric for either sign)
 template <typename T>
 __device__ __forceinline__ T adj_lap(const T *V, int x, int y, int z, long long cell, const AdjArgs<T> &a)
 {
     const T v = V[cell];
     T s = 0;
-    if (x > 0) s += (V[cell - 1] - v) / (a.hx * a.hx);
-    if (x + 1 < a.nx) s += (V[cell + 1] - v) / (a.hx * a.hx);
-    if (y > 0) s += (V[cell - a.nx] - v) / (a.hy * a.hy);
-    if (y + 1 < a.ny) s += (V[cell + a.nx] - v) / (a.hy * a.hy);
     const long long nxy = (long long)a.nx * a.ny;
+    const long long wx = a.nx - 1, wy = (long long)(a.ny - 1) * a.nx, wz = (long long)(a.nz - 1) * nxy;
+    const bool px = a.pbc[0] && a.nx > 1, py = a.pbc[1] && a.ny > 1, pz = a.pbc[2] && a.nz > 1;
+    if (x > 0) s += (V[cell - 1] - v) / (a.hx * a.hx);
+    else if (px) s += ((T)a.pbc[0] * V[cell + wx] - v) / (a.hx * a.hx);
+    if (x + 1 < a.nx) s += (V[cell + 1] - v) / (a.hx * a.hx);
+    else if (px) s += ((T)a.pbc[0] * V[cell - wx] - v) / (a.hx * a.hx);
+    if (y > 0) s += (V[cell - a.nx] - v) / (a.hy * a.hy);
+    else if (py) s += ((T)a.pbc[1] * V[cell + wy] - v) / (a.hy * a.hy);
+    if (y + 1 < a.ny) s += (V[cell + a.nx] - v) / (a.hy * a.hy);
+    else if (py) s += ((T)a.pbc[1] * V[cell - wy] - v) / (a.hy * a.hy);
     if (z > 0) s += (V[cell - nxy] - v) / (a.hz * a.hz);
+    else if (pz) s += ((T)a.pbc[2] * V[cell + wz] - v) / (a.hz * a.hz);
     if (z + 1 < a.nz) s += (V[cell + nxy] - v) / (a.hz * a.hz);
+    else if (pz) s += ((T)a.pbc[2] * V[cell - wz] - v) / (a.hz * a.hz);
     return s;
 }
 

@@ -66,6 +66,7 @@ struct Mesh {
     std::vector<double> Ha{0.0, 0.0, 0.0};
     double Ha_tspan = 0.0;
     std::vector<double> M0;     // host copy of M until the device is ready
+    int pbc[3] = {0, 0, 0};     // periodic images per axis (0: none; the sign is the stencil's wrap sign)
     // derived
     long long n = 0;
     int Nx = 1, Ny = 1, Nz = 1, LX = 1;
@@ -375,7 +376,8 @@ int prepare_mesh(bm_ctx *c, Mesh &m)
             if (cudaMalloc(&m.G, s1 * c->es_level) != cudaSuccess) return fail(BM_ENOMEM, "evaluation speedup slots");
             cudaMemsetAsync(m.G, 0, s1 * c->es_level, s);
             double S[3];
-            self_demag_host(m.h[0], m.h[1], m.h[2], S);
+            const int nc3[3] = {m.nx, m.ny, m.nz};
+            self_demag_pbc_host(m.h[0], m.h[1], m.h[2], nc3, m.pbc, S);
             for (int k = 0; k < 3; k++) m.es_cs[k] = S[k] * (double)m.Ny * (double)m.Nz;
         }
         if (m.nz > 1 || m.ml_role == 1) {
@@ -402,7 +404,7 @@ int prepare_mesh(bm_ctx *c, Mesh &m)
         bm_far_coeffs(m.h[0] / hm, m.h[1] / hm, m.h[2] / hm, fq.data());
         CK(cudaMemcpyAsync(c->farq, fq.data(), sizeof(double) * fq.size(), cudaMemcpyHostToDevice, s));
         rc = build_kernels_device<T>((T *)m.K, m.nx, m.ny, m.nz, m.Nx, m.Ny, m.Nz, m.h[0], m.h[1], m.h[2], c->farq,
-                                     (const cpx<double> *)tx, (const cpx<double> *)ty, (const cpx<double> *)tz, s);
+                                     (const cpx<double> *)tx, (const cpx<double> *)ty, (const cpx<double> *)tz, s, m.pbc);
         cudaFree(tx); cudaFree(ty); cudaFree(tz);
         if (rc) return fail(BM_ECUDA, "kernel build failed (" + std::to_string(rc) + ")");
     }
@@ -893,6 +895,21 @@ int prepare(bm_ctx *c)
     if (c->batched && c->ml_mode >= 0) return fail(BM_EUNSUPPORTED, "batched meshes with a multilayered convolution");
     if (c->es_level > 0 && c->ml_mode >= 0)
         return fail(BM_EUNSUPPORTED, "evaluation speedup with a multilayered convolution");
+    for (auto &m : c->meshes) {
+        if (!(m.modules & BM_DEMAG) || !(m.pbc[0] || m.pbc[1] || m.pbc[2])) continue;
+        if (c->ml_mode >= 0) return fail(BM_EUNSUPPORTED, "periodic boundary conditions with a multilayered convolution");
+        // the periodic tensor build evaluates (octant points) x (image terms) tensor values; bound
+        // it so a set-up cannot hold the device for minutes
+        const int nc[3] = {m.nx, m.ny, m.nz};
+        double work = 1.0;
+        for (int a = 0; a < 3; a++) {
+            const int X = std::abs(m.pbc[a]);
+            work *= X ? (double)(nc[a] / 2 + 1) * (2.0 * X + 2.0) : (double)nc[a];
+        }
+        if (work > 1e10)
+            return fail(BM_EUNSUPPORTED, "periodic tensor build of " + std::to_string(work) +
+                                             " tensor evaluations is above the limit of 1e10 (fewer images or cells)");
+    }
     CK(cudaSetDevice(c->device));
     // refuse up front, before any allocation, when the meshes cannot fit: the free device memory,
     // or the context's own limit (bm_set_memory_limit) when it is lower
@@ -1042,6 +1059,7 @@ StageArgs<T> stage_args(bm_ctx *c, Mesh &m)
     a.do_xfwd = (m.modules & BM_DEMAG) ? 1 : 0;
     a.staged = m.staged;
     a.xv = m.xv;
+    for (int i = 0; i < 3; i++) a.pbc[i] = (m.pbc[i] > 0) - (m.pbc[i] < 0);
     stage_derive(a);
     if (m.ml_role == 2) {
         // multilayer with mesh transfer: the demag field arrives in Hd, no x transforms here
@@ -1912,6 +1930,7 @@ int adjoint_T(bm_ctx *c, int steps, int k, const double *target, int m0_scales, 
     double en = std::sqrt(m.ea[0] * m.ea[0] + m.ea[1] * m.ea[1] + m.ea[2] * m.ea[2]);
     for (int q = 0; q < 3; q++) aa.ea[q] = (T)(en > 0 ? m.ea[q] / en : 0.0);
     aa.modules = m.modules;
+    for (int q = 0; q < 3; q++) aa.pbc[q] = (m.pbc[q] > 0) - (m.pbc[q] < 0);
     const double dt = c->dt;
     // the two segment graphs
     cudaGraph_t gr = nullptr, gb = nullptr;
@@ -2113,6 +2132,27 @@ int bm_set_material_maps(bm_ctx *c, int mesh, const double *Ms_map, const double
     } else m.Ms_map.clear();
     if (K1_map) m.K1_map.assign(K1_map, K1_map + m.n);
     else m.K1_map.clear();
+    return 0;
+}
+
+int bm_set_pbc(bm_ctx *c, int mesh, int x_images, int y_images, int z_images)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    const int img[3] = {x_images, y_images, z_images};
+    for (int a = 0; a < 3; a++)
+        if (img[a] > BM_PBC_MAX_IMAGES || img[a] < -BM_PBC_MAX_IMAGES)
+            return fail(BM_EINVAL, "PBC images must be within +-" + std::to_string(BM_PBC_MAX_IMAGES));
+    unprepare(c);
+    Mesh &m = c->meshes[mesh];
+    for (int a = 0; a < 3; a++) m.pbc[a] = img[a];
+    return 0;
+}
+
+int bm_get_pbc(bm_ctx *c, int mesh, int *images3)
+{
+    if (int rc = check_mesh(c, mesh)) return rc;
+    if (!images3) return fail(BM_EINVAL, "null out");
+    for (int a = 0; a < 3; a++) images3[a] = c->meshes[mesh].pbc[a];
     return 0;
 }
 
@@ -2872,7 +2912,8 @@ int bm_debug_kernels(bm_ctx *c, int mesh, double *K6)
     bm_far_coeffs(m.h[0] / hm, m.h[1] / hm, m.h[2] / hm, fq.data());
     CK(cudaMemcpy(c->farq, fq.data(), sizeof(double) * fq.size(), cudaMemcpyHostToDevice));
     rc = build_kernels_device<double>(K, m.nx, m.ny, m.nz, Nx, Ny, Nz, m.h[0], m.h[1], m.h[2], c->farq,
-                                      (const cpx<double> *)tx, (const cpx<double> *)ty, (const cpx<double> *)tz, c->stream);
+                                      (const cpx<double> *)tx, (const cpx<double> *)ty, (const cpx<double> *)tz, c->stream,
+                                      m.pbc);
     cudaFree(tx); cudaFree(ty); cudaFree(tz);
     if (rc) { cudaFree(K); return fail(BM_ECUDA, "kernel build failed"); }
     CK(cudaMemcpy(K6, K, sizeof(double) * 6 * nk, cudaMemcpyDeviceToHost));
@@ -2881,6 +2922,11 @@ int bm_debug_kernels(bm_ctx *c, int mesh, double *K6)
 }
 
 int bm_debug_tensor(int device, int nx, int ny, int nz, double hx, double hy, double hz, double *oct6)
+{
+    return bm_debug_tensor_pbc(device, nx, ny, nz, hx, hy, hz, nullptr, oct6);
+}
+
+int bm_debug_tensor_pbc(int device, int nx, int ny, int nz, double hx, double hy, double hz, const int *pbc3, double *oct6)
 {
     if (nx < 1 || ny < 1 || nz < 1 || !oct6) return fail(BM_EINVAL, "args");
     CK(cudaSetDevice(device));
@@ -2892,7 +2938,7 @@ int bm_debug_tensor(int device, int nx, int ny, int nz, double hx, double hy, do
     std::vector<double> fq(6 * BM_FARQ_PER_COMP);
     bm_far_coeffs(hx / hm, hy / hm, hz / hm, fq.data());
     CK(cudaMemcpy(fq_d, fq.data(), sizeof(double) * fq.size(), cudaMemcpyHostToDevice));
-    int rc = tensor_octant_device(d, nx, ny, nz, hx, hy, hz, fq_d, 0);
+    int rc = tensor_octant_device(d, nx, ny, nz, hx, hy, hz, fq_d, 0, pbc3);
     CK(cudaDeviceSynchronize());
     CK(cudaMemcpy(oct6, d, sizeof(double) * 6 * np, cudaMemcpyDeviceToHost));
     cudaFree(d);

@@ -9,9 +9,9 @@
 template <typename T>
 int build_kernels_device(T *K, int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz,
                          const double *farq_dev, const cpx<double> *twx, const cpx<double> *twy,
-                         const cpx<double> *twz, cudaStream_t s);
+                         const cpx<double> *twz, cudaStream_t s, const int *pbc = nullptr);
 int tensor_octant_device(double *oct_dev, int nx, int ny, int nz, double hx, double hy, double hz, const double *farq_dev,
-                         cudaStream_t s);
+                         cudaStream_t s, const int *pbc = nullptr);
 template <typename T>
 int launch_fft_strided(cpx<T> *data, const FFTPlan &P, const cpx<T> *tw, long long es, long long ls, int ninner,
                        long long os, int nouter, bool inv, cudaStream_t s);
@@ -123,6 +123,7 @@ struct StageArgs {
     T exA, exD;               // 2 A / mu0, -2 D / mu0 (times 1 / Ms^2 per cell)
     T two_mu0;                // 2 / mu0
     T llg_pre;                // -gamma grel / (1 + alpha^2)
+    int pbc[3];               // per axis: 0 no wrap, +1 / -1 periodic neighbour with that sign (mesh PBC)
 };
 
 // fills the derived constants of a StageArgs from its material and cellsize fields
@@ -199,6 +200,7 @@ struct AdjArgs {
     T Ms, K1, A, alpha, grel;
     T ea[3];
     int modules;
+    int pbc[3];   // per axis: 0 no wrap, +1 / -1 periodic neighbour with that sign
 };
 template <typename T>
 int launch_adj_loss(const AdjArgs<T> &a, const T *M, const double *target, T *lam, double *gMs, double *loss, cudaStream_t s);
@@ -215,6 +217,8 @@ int launch_adj_m0(const AdjArgs<T> &a, const T *M0, const T *lam, double *gMs, c
 
 // ---------------------------------------------------------------- evaluation speedup (RK4)
 void self_demag_host(double hx, double hy, double hz, double out3[3]);   // -N of one cell (tensor.cu)
+// -N of one cell plus the far field of its PBC images (tensor.cu); n = cells, img = images per axis
+void self_demag_pbc_host(double hx, double hy, double hz, const int n[3], const int img[3], double out3[3]);
 // Demag extrapolation in the x-spectrum domain S1[c][z][y][kx] (plane = nz ny LX complex values per
 // component). G holds es_K slots of 3 planes: the saved field minus its self term. cs[c] is the
 // self-demag coefficient (-N_c) times Ny Nz, the factor between the x-spectrum of M the stage kernel

@@ -311,14 +311,47 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                     mzm[c] = hzm ? acc.m(r, 3, c, x, cell) : (T)0;
                     mzp[c] = hzp ? acc.m(r, 4, c, x, cell) : (T)0;
                 }
+                // periodic axes: the missing neighbour is the cell on the far side, times the axis'
+                // sign (the PBC branch of delsq_nneu / grad_nneu, BorisLib/VEC_VC_Del.h:141,
+                // BorisLib/VEC_VC_Grad.h:139); a one-cell axis has no neighbours either way
+                bool bxp = hxp, bxm = hxm, byp = hyp, bym = hym, bzp = hzp, bzm = hzm;
+                if (a.pbc[0] && nx > 1) {
+                    const T sg = (T)a.pbc[0];
+                    if (!hxp) { bxp = true;
+#pragma unroll
+                        for (int c = 0; c < 3; c++) mxp[c] = sg * acc.m(r, 0, c, 0, cell - (nx - 1)); }
+                    if (!hxm) { bxm = true;
+#pragma unroll
+                        for (int c = 0; c < 3; c++) mxm[c] = sg * acc.m(r, 0, c, nx - 1, cell + (nx - 1)); }
+                }
+                if (a.pbc[1] && ny > 1) {
+                    const T sg = (T)a.pbc[1];
+                    const long long w = (long long)(ny - 1) * nx;
+                    if (!hyp) { byp = true;
+#pragma unroll
+                        for (int c = 0; c < 3; c++) myp[c] = sg * (a.Min + (cell - w))[c * n]; }
+                    if (!hym) { bym = true;
+#pragma unroll
+                        for (int c = 0; c < 3; c++) mym[c] = sg * (a.Min + (cell + w))[c * n]; }
+                }
+                if (a.pbc[2] && nz > 1) {
+                    const T sg = (T)a.pbc[2];
+                    const long long w = (long long)(nz - 1) * nx * ny;
+                    if (!hzp) { bzp = true;
+#pragma unroll
+                        for (int c = 0; c < 3; c++) mzp[c] = sg * (a.Min + (cell - w))[c * n]; }
+                    if (!hzm) { bzm = true;
+#pragma unroll
+                        for (int c = 0; c < 3; c++) mzm[c] = sg * (a.Min + (cell + w))[c * n]; }
+                }
                 const T rr = idmi ? a.rrD : (T)0;
                 T bx[3] = {rr * m[2], 0, -rr * m[0]};
                 T by[3] = {0, rr * m[2], -rr * m[1]};
                 T bz[3] = {0, 0, 0};
                 T dx2[3], dy2[3], dz2[3], gx[3], gy[3], gz[3];
-                axis_stencil<T>(m, mxp, mxm, hxp, hxm, a.hh[0], a.ih[0], a.ih2[0], bx, dx2, gx);
-                axis_stencil<T>(m, myp, mym, hyp, hym, a.hh[1], a.ih[1], a.ih2[1], by, dy2, gy);
-                axis_stencil<T>(m, mzp, mzm, hzp, hzm, a.hh[2], a.ih[2], a.ih2[2], bz, dz2, gz);
+                axis_stencil<T>(m, mxp, mxm, bxp, bxm, a.hh[0], a.ih[0], a.ih2[0], bx, dx2, gx);
+                axis_stencil<T>(m, myp, mym, byp, bym, a.hh[1], a.ih[1], a.ih2[1], by, dy2, gy);
+                axis_stencil<T>(m, mzp, mzm, bzp, bzm, a.hh[2], a.ih[2], a.ih2[2], bz, dz2, gz);
                 const T iMs2 = iMs * iMs;
                 const T Ac = a.exA * iMs2;
                 const T Dc = idmi ? a.exD * iMs2 : (T)0;

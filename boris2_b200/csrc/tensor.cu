@@ -98,7 +98,7 @@ extern "C" int bm_self_demag(double hx, double hy, double hz, double *out3)
 
 // far field: D_c = V/(4 pi) sum_n Q_{c,n}(u,v,w) / R^(n+1), coefficient layout per comp c:
 // for n in {2,4,6,8}: monomials (i,j,k), i+j+k = n, ordered i descending then j descending
-__device__ double far_eval(const double *__restrict__ q, double u, double v, double w, double R)
+__host__ __device__ double far_eval(const double *__restrict__ q, double u, double v, double w, double R)
 {
     double pu[9], pv[9], pw[9];
     pu[0] = pv[0] = pw[0] = 1.0;
@@ -119,6 +119,30 @@ __device__ double far_eval(const double *__restrict__ q, double u, double v, dou
     return csum_d(tot, 4);
 }
 
+// D = -N of one cell pair at the non-negative offset (i, j, k) cells (normalised cellsize): the
+// exact Newell differences within 40 cells, the far-field expansion beyond, the reference's rule
+// (Boris/DemagTFunc.cpp:40-58). v = xx, yy, zz, xy, xz, yz; a one-cell-thick mesh has no xz, yz.
+__device__ __forceinline__ void tensor_point(int i, int j, int k, double hx, double hy, double hz,
+                                             const double *__restrict__ farq, int two_d, double v[6])
+{
+    double x = i * hx, y = j * hy, z = k * hz;
+    bool far = (i >= BM_ASYMPT_DIST || j >= BM_ASYMPT_DIST || k >= BM_ASYMPT_DIST ||
+                (long long)i * i + (long long)j * j + (long long)k * k >= (long long)BM_ASYMPT_DIST * BM_ASYMPT_DIST);
+    if (far) {
+        double R = sqrt(x * x + y * y + z * z);
+        double u = x / R, vv = y / R, w = z / R;
+        double V = hx * hy * hz / (4.0 * M_PI);
+        for (int c = 0; c < 6; c++) v[c] = (two_d && c >= 4) ? 0.0 : V * far_eval(farq + c * BM_FARQ_PER_COMP, u, vv, w, R);
+    } else {
+        v[0] = -newellL<false>(x, y, z, hx, hy, hz);
+        v[1] = -newellL<false>(y, x, z, hy, hx, hz);
+        v[2] = -newellL<false>(z, y, x, hz, hy, hx);
+        v[3] = -newellL<true>(x, y, z, hx, hy, hz);
+        v[4] = two_d ? 0.0 : -newellL<true>(x, z, y, hx, hz, hy);
+        v[5] = two_d ? 0.0 : -newellL<true>(y, z, x, hy, hz, hx);
+    }
+}
+
 // octant values D(i,j,k), i<nx, j<ny, k<nz -> oct[((k*ny + j)*nx + i)*6 + c], c = xx,yy,zz,xy,xz,yz
 __global__ void k_tensor_octant(double *oct, int nx, int ny, int nz, double hx, double hy, double hz,
                                 const double *__restrict__ farq, int two_d)
@@ -128,25 +152,131 @@ __global__ void k_tensor_octant(double *oct, int nx, int ny, int nz, double hx, 
         int i = (int)(p % nx);
         int j = (int)((p / nx) % ny);
         int k = (int)(p / ((long long)nx * ny));
-        double x = i * hx, y = j * hy, z = k * hz;
         double v[6];
-        bool far = (i >= BM_ASYMPT_DIST || j >= BM_ASYMPT_DIST || k >= BM_ASYMPT_DIST ||
-                    (long long)i * i + (long long)j * j + (long long)k * k >= (long long)BM_ASYMPT_DIST * BM_ASYMPT_DIST);
-        if (far) {
-            double R = sqrt(x * x + y * y + z * z);
-            double u = x / R, vv = y / R, w = z / R;
-            double V = hx * hy * hz / (4.0 * M_PI);
-            for (int c = 0; c < 6; c++) v[c] = V * far_eval(farq + c * BM_FARQ_PER_COMP, u, vv, w, R);
-        } else {
-            v[0] = -newellL<false>(x, y, z, hx, hy, hz);
-            v[1] = -newellL<false>(y, x, z, hy, hx, hz);
-            v[2] = -newellL<false>(z, y, x, hz, hy, hx);
-            v[3] = -newellL<true>(x, y, z, hx, hy, hz);
-            v[4] = two_d ? 0.0 : -newellL<true>(x, z, y, hx, hz, hy);
-            v[5] = two_d ? 0.0 : -newellL<true>(y, z, x, hy, hz, hx);
-        }
+        tensor_point(i, j, k, hx, hy, hz, farq, two_d, v);
         for (int c = 0; c < 6; c++) oct[p * 6 + c] = v[c];
     }
+}
+
+// ---------------------------------------------------------------- periodic boundary conditions
+// The reference convolves a PBC axis cyclically over its n cells (FFT length n,
+// Boris/ConvolutionData.cpp:115-145) with the tensor summed over +-images periods
+// (Boris/DemagTFunc_PBC.cpp:5,97,185,300): D(i0) = sum_{m=-X..X} T(m n + i0) for i0 in [0, n), and it
+// keeps only the real (even components) or imaginary (odd components) part of each axis' DFT
+// (Boris/DemagKernel.cpp:250-300,365-460). Those parts are the DFT of the tensor made even or odd
+// about i0 = 0 along the axis: Ds(i0) = (D(i0) +- D((n - i0) mod n)) / 2. A cyclic convolution of
+// period n over n cells only uses offsets d in (-n, n), so it is the linear convolution with the
+// kernel Ds(d mod n) there; this path therefore keeps its zero-padded transforms and fills the
+// octant [0, n) of each PBC axis with Ds. Written out, with T(-x) = +-T(x):
+//   i0 = 0:  Ds = sum_{m=-X..X} T(m n)                              (odd components: 0)
+//   i0 > 0:  Ds = sum_{m=-X-1..X} w_m T(m n + i0), w = 1/2 at m = -X-1 and m = X, 1 otherwise,
+// and Ds(n - i0) = +-Ds(i0), so a thread evaluates i0 <= n / 2 and writes both. Odd components take
+// the sign of each offset with sign(0) = 0 (BorisLib/Funcs_Math.h:103, get_sign), as the reference.
+struct PbcSpec {
+    int n[3];     // cells per axis
+    int img[3];   // images per axis (0: no PBC along it)
+};
+
+__device__ __forceinline__ int isgn(int v) { return (v > 0) - (v < 0); }
+
+__global__ void k_tensor_octant_pbc(double *oct, PbcSpec P, double hx, double hy, double hz,
+                                    const double *__restrict__ farq, int two_d)
+{
+    int ce[3];   // canonical extent per axis
+    for (int a = 0; a < 3; a++) ce[a] = P.img[a] ? P.n[a] / 2 + 1 : P.n[a];
+    const long long Nc = (long long)ce[0] * ce[1] * ce[2];
+    const int nx = P.n[0], ny = P.n[1];
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < Nc; p += (long long)gridDim.x * blockDim.x) {
+        int q[3];
+        q[0] = (int)(p % ce[0]);
+        q[1] = (int)((p / ce[0]) % ce[1]);
+        q[2] = (int)(p / ((long long)ce[0] * ce[1]));
+        // image range per axis: [lo, hi] with half weights at the ends when `half`
+        int lo[3], hi[3], half[3];
+        for (int a = 0; a < 3; a++) {
+            const int X = P.img[a];
+            if (!X) { lo[a] = hi[a] = 0; half[a] = 0; }
+            else if (q[a] == 0) { lo[a] = -X; hi[a] = X; half[a] = 0; }
+            else { lo[a] = -X - 1; hi[a] = X; half[a] = 1; }
+        }
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int mx = lo[0]; mx <= hi[0]; mx++) {
+            const double wx = (half[0] && (mx == lo[0] || mx == hi[0])) ? 0.5 : 1.0;
+            const int i = mx * P.n[0] + q[0];
+            for (int my = lo[1]; my <= hi[1]; my++) {
+                const double wy = (half[1] && (my == lo[1] || my == hi[1])) ? 0.5 : 1.0;
+                const int j = my * P.n[1] + q[1];
+                for (int mz = lo[2]; mz <= hi[2]; mz++) {
+                    const double w = wx * wy * ((half[2] && (mz == lo[2] || mz == hi[2])) ? 0.5 : 1.0);
+                    const int k = mz * P.n[2] + q[2];
+                    const int si = isgn(i), sj = isgn(j), sk = isgn(k);
+                    double v[6];
+                    tensor_point(abs(i), abs(j), abs(k), hx, hy, hz, farq, two_d, v);
+                    acc[0] += w * v[0];
+                    acc[1] += w * v[1];
+                    acc[2] += w * v[2];
+                    acc[3] += w * v[3] * (si * sj);
+                    acc[4] += w * v[4] * (si * sk);
+                    acc[5] += w * v[5] * (sj * sk);
+                }
+            }
+        }
+        if (q[0] == 0 && P.img[0]) { acc[3] = 0.0; acc[4] = 0.0; }
+        if (q[1] == 0 && P.img[1]) { acc[3] = 0.0; acc[5] = 0.0; }
+        if (q[2] == 0 && P.img[2]) { acc[4] = 0.0; acc[5] = 0.0; }
+        // write the point and its mirrors n - i0 on the PBC axes (odd components change sign)
+        for (int f = 0; f < 8; f++) {
+            int r[3];
+            int par[3] = {1, 1, 1};   // -1 on a mirrored axis
+            bool ok = true;
+            for (int a = 0; a < 3 && ok; a++) {
+                if (f & (1 << a)) {
+                    if (!P.img[a] || q[a] == 0 || 2 * q[a] == P.n[a]) { ok = false; break; }
+                    r[a] = P.n[a] - q[a];
+                    par[a] = -1;
+                } else r[a] = q[a];
+            }
+            if (!ok) continue;
+            const long long o = (((long long)r[2] * ny + r[1]) * nx + r[0]) * 6;
+            oct[o + 0] = acc[0];
+            oct[o + 1] = acc[1];
+            oct[o + 2] = acc[2];
+            oct[o + 3] = acc[3] * (par[0] * par[1]);
+            oct[o + 4] = acc[4] * (par[0] * par[2]);
+            oct[o + 5] = acc[5] * (par[1] * par[2]);
+        }
+    }
+}
+
+// Self coefficients of the evaluation speedup under PBC, DemagTFunc::SelfDemag_PBC
+// (Boris/DemagTFunc_Self.cpp:57): the cell's own -N plus, for every image period other than the
+// cell itself, the far-field D at the image's offset (images at multiples of the mesh length). As
+// there, all three diagonal terms use the expansion of the (hx, hy, hz) cell with the xx form, the
+// yy and zz terms at the offsets permuted (y, x, z) and (z, y, x). Cellsizes are normalised by the
+// largest, as for the tensor.
+void self_demag_pbc_host(double hx, double hy, double hz, const int n[3], const int img[3], double out3[3])
+{
+    // the reference's image loops run from -images to images: a negative count on any axis (a
+    // stencil sign of -1) leaves them empty and the coefficient zero, self term included
+    if (img[0] < 0 || img[1] < 0 || img[2] < 0) { out3[0] = out3[1] = out3[2] = 0.0; return; }
+    self_demag_host(hx, hy, hz, out3);
+    double hm = fmax(hx, fmax(hy, hz));
+    hx /= hm; hy /= hm; hz /= hm;
+    int X = img[0], Y = img[1], Z = img[2];
+    if (!X && !Y && !Z) return;
+    double q[6 * BM_FARQ_PER_COMP];
+    bm_far_coeffs(hx, hy, hz, q);
+    const double V = hx * hy * hz / (4.0 * M_PI);
+    for (int a = -X; a <= X; a++)
+        for (int b = -Y; b <= Y; b++)
+            for (int c = -Z; c <= Z; c++) {
+                if (!a && !b && !c) continue;
+                double x = fabs((double)a * n[0]) * hx, y = fabs((double)b * n[1]) * hy, z = fabs((double)c * n[2]) * hz;
+                double R = sqrt(x * x + y * y + z * z);
+                out3[0] += V * far_eval(q, x / R, y / R, z / R, R);
+                out3[1] += V * far_eval(q, y / R, x / R, z / R, R);
+                out3[2] += V * far_eval(q, z / R, y / R, x / R, R);
+            }
 }
 
 // fill one component on the full N grid (complex, imaginary zero) from the octant with parity
@@ -252,12 +382,30 @@ static int grid_for(long long n)
     return (int)b;
 }
 
+static bool pbc_on(const int *pbc) { return pbc && (pbc[0] || pbc[1] || pbc[2]); }
+
+static void launch_octant(double *oct, int nx, int ny, int nz, double hx, double hy, double hz, const double *farq_dev,
+                          const int *pbc, cudaStream_t s)
+{
+    if (pbc_on(pbc)) {
+        PbcSpec P;
+        P.n[0] = nx; P.n[1] = ny; P.n[2] = nz;
+        for (int a = 0; a < 3; a++) P.img[a] = abs(pbc[a]);
+        long long nc = 1;
+        for (int a = 0; a < 3; a++) nc *= P.img[a] ? P.n[a] / 2 + 1 : P.n[a];
+        k_tensor_octant_pbc<<<grid_for(nc), 128, 0, s>>>(oct, P, hx, hy, hz, farq_dev, nz == 1);
+    } else {
+        k_tensor_octant<<<grid_for((long long)nx * ny * nz), 256, 0, s>>>(oct, nx, ny, nz, hx, hy, hz, farq_dev, nz == 1);
+    }
+}
+
 // Build the kernel planes (6 components, type T) for one mesh on the device.
-// twx/twy/twz are FP64 tables of exp(-2 pi i m / N) for N = Nx, Ny, Nz.
+// twx/twy/twz are FP64 tables of exp(-2 pi i m / N) for N = Nx, Ny, Nz. pbc: images per axis
+// (negative values count as their magnitude, as for the reference's demag) or nullptr.
 template <typename T>
 int build_kernels_device(T *K, int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz,
                          const double *farq_dev, const cpx<double> *twx, const cpx<double> *twy,
-                         const cpx<double> *twz, cudaStream_t s)
+                         const cpx<double> *twz, cudaStream_t s, const int *pbc)
 {
     double hm = fmax(hx, fmax(hy, hz));
     hx /= hm; hy /= hm; hz /= hm;
@@ -267,7 +415,7 @@ int build_kernels_device(T *K, int nx, int ny, int nz, int Nx, int Ny, int Nz, d
     cpx<double> *F = nullptr;
     if (cudaMalloc(&oct, sizeof(double) * 6 * noct) != cudaSuccess) return 2;
     if (cudaMalloc(&F, sizeof(cpx<double>) * Ntot) != cudaSuccess) { cudaFree(oct); return 2; }
-    k_tensor_octant<<<grid_for(noct), 256, 0, s>>>(oct, nx, ny, nz, hx, hy, hz, farq_dev, nz == 1);
+    launch_octant(oct, nx, ny, nz, hx, hy, hz, farq_dev, pbc, s);
     FFTPlan px, py, pz;
     bm_make_plan(Nx, px); bm_make_plan(Ny, py); bm_make_plan(Nz, pz);
     int rc = 0;
@@ -294,16 +442,18 @@ int build_kernels_device(T *K, int nx, int ny, int nz, int Nx, int Ny, int Nz, d
 }
 
 template int build_kernels_device<float>(float *, int, int, int, int, int, int, double, double, double, const double *,
-                                         const cpx<double> *, const cpx<double> *, const cpx<double> *, cudaStream_t);
+                                         const cpx<double> *, const cpx<double> *, const cpx<double> *, cudaStream_t,
+                                         const int *);
 template int build_kernels_device<double>(double *, int, int, int, int, int, int, double, double, double, const double *,
-                                          const cpx<double> *, const cpx<double> *, const cpx<double> *, cudaStream_t);
+                                          const cpx<double> *, const cpx<double> *, const cpx<double> *, cudaStream_t,
+                                          const int *);
 
-// raw tensor octant to host (tests)
+// raw tensor octant to host (tests); with pbc the octant of the periodic kernel
 int tensor_octant_device(double *oct_dev, int nx, int ny, int nz, double hx, double hy, double hz, const double *farq_dev,
-                         cudaStream_t s)
+                         cudaStream_t s, const int *pbc)
 {
     double hm = fmax(hx, fmax(hy, hz));
-    k_tensor_octant<<<grid_for((long long)nx * ny * nz), 256, 0, s>>>(oct_dev, nx, ny, nz, hx / hm, hy / hm, hz / hm, farq_dev, nz == 1);
+    launch_octant(oct_dev, nx, ny, nz, hx / hm, hy / hm, hz / hm, farq_dev, pbc, s);
     return (int)cudaGetLastError();
 }
 

@@ -77,6 +77,22 @@ int bm_set_material_maps(bm_ctx *ctx, int mesh, const double *Ms_map, const doub
  * (Boris/SimSharedData.cpp:179). */
 int bm_set_modules(bm_ctx *ctx, int mesh, int modules);
 
+/* Periodic boundary conditions of a mesh: the number of images summed along each axis (0: the axis
+ * is not periodic; at most BM_PBC_MAX_IMAGES in magnitude). Replaces Demag::Set_PBC
+ * (Boris/Demag.cpp:137) with Mesh::Set_Magnetic_PBC (Boris/MeshControl.cpp:49), which the "pbc"
+ * command reaches through SuperMesh::Set_PBC (Boris/SuperMeshMeshes_Settings.cpp:659):
+ *   - demag: along a periodic axis the convolution is cyclic over the mesh's n cells with the
+ *     tensor summed over +-|images| periods (Boris/DemagTFunc_PBC.cpp:5,97,185,300,
+ *     Boris/ConvolutionData.cpp:115-145); the evaluation speedup's self term adds the images'
+ *     far field (DemagTFunc::SelfDemag_PBC, Boris/DemagTFunc_Self.cpp:57);
+ *   - exchange / iDMI: a cell on a periodic face takes the cell on the opposite face as its missing
+ *     neighbour, times the sign of images (a negative count wraps with -1, as the reference's
+ *     differential operators do, BorisLib/VEC_VC_Del.h:141, BorisLib/VEC_VC_Grad.h:139).
+ * Not combined with bm_set_multiconvolution (BM_EUNSUPPORTED at set-up). */
+#define BM_PBC_MAX_IMAGES 1000
+int bm_set_pbc(bm_ctx *ctx, int mesh, int x_images, int y_images, int z_images);
+int bm_get_pbc(bm_ctx *ctx, int mesh, int *images3);
+
 /* Applied field: nsamples piecewise-constant 3-vectors (A/m) over [0, t_span); with
  * nsamples == 1 the field is constant. Replaces Zeeman::SetField / H_equation
  * (Boris/Zeeman.cpp:164); as there, the field is evaluated at the step start time. */
@@ -291,6 +307,11 @@ int bm_tiles(bm_ctx *ctx, int mesh, int *tiles4);
 int bm_debug_kernels(bm_ctx *ctx, int mesh, double *K6);
 /* Raw FP64 tensor octant values D(i,j,k) for i<nx, j<ny, k<nz: 6 per point. */
 int bm_debug_tensor(int device, int nx, int ny, int nz, double hx, double hy, double hz, double *oct6);
+/* As bm_debug_tensor for a mesh of nx x ny x nz cells with pbc3 images per axis (NULL: none): along
+ * a periodic axis the octant holds the image-summed tensor made even (xx, yy, zz) or odd (the
+ * off-diagonal components odd in that axis) about the origin with period n. */
+int bm_debug_tensor_pbc(int device, int nx, int ny, int nz, double hx, double hy, double hz, const int *pbc3,
+                        double *oct6);
 /* Batched complex FFT on the device of `howmany` contiguous lines of length L (in place,
  * interleaved re/im doubles on the host); precision BM_FP64 or BM_MIXED; inverse != 0
  * uses exp(+2 pi i ...), unnormalised. */

@@ -120,6 +120,38 @@ void orc_selfdemag(double hx, double hy, double hz, double *out3)
     out3[2] = -newell_L(orc_newell_f, 0, 0, 0, hz, hy, hx);
 }
 
+/* DemagTFunc::SelfDemag_PBC (Boris/DemagTFunc_Self.cpp:57): the cell's own D plus, for each image
+ * period other than (0,0,0), the far-field D at that period's offset (|img * n| cells per axis). As
+ * the reference does, the xx, yy and zz image terms all take the expansion of the (hx, hy, hz)
+ * cell in its xx form, yy evaluated at the offset (y, x, z) and zz at (z, y, x). Cellsizes are
+ * normalised by the largest (the product's choice for the self term; the expansion is scale free). */
+void orc_selfdemag_pbc(double hx, double hy, double hz, const int *n3, const int *pbc, double *out3)
+{
+    double hm = hx;
+    if (hy > hm) hm = hy;
+    if (hz > hm) hm = hz;
+    hx /= hm; hy /= hm; hz /= hm;
+    /* the reference's loops run i_img from -images to images: a negative count on any axis leaves
+       them empty, so the coefficient is zero (self term included) */
+    if (pbc && (pbc[0] < 0 || pbc[1] < 0 || pbc[2] < 0)) { out3[0] = out3[1] = out3[2] = 0.0; return; }
+    orc_selfdemag(hx, hy, hz, out3);
+    if (!pbc) return;
+    int X = pbc[0], Y = pbc[1], Z = pbc[2];
+    for (int a = -X; a <= X; a++)
+        for (int b = -Y; b <= Y; b++)
+            for (int c = -Z; c <= Z; c++) {
+                if (!a && !b && !c) continue;
+                double x = fabs((double)a * n3[0]) * hx, y = fabs((double)b * n3[1]) * hy, z = fabs((double)c * n3[2]) * hz;
+                double v[6];
+                orc_asymptotic(hx, hy, hz, x, y, z, v);
+                out3[0] += v[0];
+                orc_asymptotic(hx, hy, hz, y, x, z, v);
+                out3[1] += v[0];
+                orc_asymptotic(hx, hy, hz, z, y, x, v);
+                out3[2] += v[0];
+            }
+}
+
 /* ------------------------------------------------------------------ far field */
 
 /* Derivatives of 1/R: d^p_x d^q_y d^r_z (1/R) = P_pqr(x,y,z) / R^(2n+1), n = p+q+r, where P is
@@ -342,6 +374,164 @@ int orc_kernels(int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, doubl
     return 0;
 }
 
+/* ------------------------------------------------------------------ periodic boundary conditions */
+
+static int isgn(int v) { return (v > 0) - (v < 0); }   /* get_sign, BorisLib/Funcs_Math.h:103 */
+
+/* D = -N on the N grid with PBC images (DemagTFunc::CalcDiagTens2D_PBC / CalcOffDiagTens2D_PBC,
+ * Boris/DemagTFunc_PBC.cpp:5,97, and the 3D forms :185,:300): along a periodic axis N = n and every
+ * index i0 in [0, N) holds the sum over images m in [-X, X] of the free tensor at m N + i0 (off-diagonal
+ * components with the signs of the offsets, sign(0) = 0); along a non-periodic axis i0 runs over
+ * [0, N/2) and the mirrors (N - i0) mod N are filled by parity. A one-cell-thick mesh (nz == 1) sums
+ * its z images at k = k_img and has no xz, yz. */
+int orc_tensor_pbc(int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz, const int *pbc,
+                   double *diag, double *odiag)
+{
+    double hm = hx;
+    if (hy > hm) hm = hy;
+    if (hz > hm) hm = hz;
+    hx /= hm; hy /= hm; hz /= hm;
+    const int X = abs(pbc[0]), Y = abs(pbc[1]), Z = abs(pbc[2]);
+    const int two_d = (nz == 1);
+    size_t np = (size_t)Nx * Ny * Nz;
+    memset(diag, 0, sizeof(double) * 3 * np);
+    memset(odiag, 0, sizeof(double) * 3 * np);
+    const int ei = X ? Nx : Nx / 2, ej = Y ? Ny : Ny / 2, ek = two_d ? 1 : (Z ? Nz : Nz / 2);
+    const int per[3] = {X != 0, Y != 0, two_d || Z != 0};
+    const int Ng[3] = {Nx, Ny, Nz};
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int k0 = 0; k0 < ek; k0++)
+        for (int j0 = 0; j0 < ej; j0++)
+            for (int i0 = 0; i0 < ei; i0++) {
+                double dv[3] = {0, 0, 0}, ov[3] = {0, 0, 0};
+                for (int ii = -X; ii <= X; ii++)
+                    for (int jj = -Y; jj <= Y; jj++)
+                        for (int kk = -Z; kk <= Z; kk++) {
+                            int i = ii * Nx + i0, j = jj * Ny + j0, k = two_d ? kk : kk * Nz + k0;
+                            int si = isgn(i), sj = isgn(j), sk = isgn(k);
+                            i = abs(i); j = abs(j); k = abs(k);
+                            double x = i * hx, y = j * hy, z = k * hz;
+                            double a[6];
+                            if (use_asympt(i, j, k)) orc_asymptotic(hx, hy, hz, x, y, z, a);
+                            else {
+                                a[0] = -newell_L(orc_newell_f, x, y, z, hx, hy, hz);
+                                a[1] = -newell_L(orc_newell_f, y, x, z, hy, hx, hz);
+                                a[2] = -newell_L(orc_newell_f, z, y, x, hz, hy, hx);
+                                a[3] = -newell_L(orc_newell_g, x, y, z, hx, hy, hz);
+                                a[4] = two_d ? 0.0 : -newell_L(orc_newell_g, x, z, y, hx, hz, hy);
+                                a[5] = two_d ? 0.0 : -newell_L(orc_newell_g, y, z, x, hy, hz, hx);
+                            }
+                            dv[0] += a[0]; dv[1] += a[1]; dv[2] += a[2];
+                            ov[0] += a[3] * si * sj;
+                            if (!two_d) { ov[1] += a[4] * si * sk; ov[2] += a[5] * sj * sk; }
+                        }
+                const int q[3] = {i0, j0, k0};
+                /* the point and, along non-periodic axes with a non-zero index, its mirrors */
+                for (int f = 0; f < 8; f++) {
+                    int r[3], sg[3] = {1, 1, 1}, ok = 1;
+                    for (int ax = 0; ax < 3; ax++) {
+                        if (f & (1 << ax)) {
+                            if (per[ax] || q[ax] == 0) { ok = 0; break; }
+                            r[ax] = (Ng[ax] - q[ax]) % Ng[ax];
+                            sg[ax] = -1;
+                        } else r[ax] = q[ax];
+                    }
+                    if (!ok) continue;
+                    size_t p = (size_t)r[0] + (size_t)r[1] * Nx + (size_t)r[2] * Nx * Ny;
+                    diag[3 * p] = dv[0]; diag[3 * p + 1] = dv[1]; diag[3 * p + 2] = dv[2];
+                    odiag[3 * p] = ov[0] * sg[0] * sg[1];
+                    odiag[3 * p + 1] = ov[1] * sg[0] * sg[2];
+                    odiag[3 * p + 2] = ov[2] * sg[1] * sg[2];
+                }
+            }
+    return 0;
+}
+
+/* in-place complex DFT of c[Nx*Ny*Nz] along one axis */
+static void dft_axis(double *c, int Nx, int Ny, int Nz, int ax, int sign)
+{
+    int dims[3] = {Nx, Ny, Nz};
+    size_t strides[3] = {1, (size_t)Nx, (size_t)Nx * Ny};
+    int L = dims[ax];
+    if (L == 1) return;
+    double *tw = bm_fft_table(L);
+    size_t nlines = (size_t)Nx * Ny * Nz / L;
+#pragma omp parallel if (nlines * (size_t)L > ORC_PAR_MIN)
+    {
+        double *line = (double *)malloc(sizeof(double) * 2 * L);
+        double *scr = (double *)malloc(sizeof(double) * 4 * L);
+#pragma omp for
+        for (long li = 0; li < (long)nlines; li++) {
+            size_t base;
+            if (ax == 0) base = (size_t)li * Nx;
+            else if (ax == 1) base = ((size_t)li % Nx) + ((size_t)li / Nx) * Nx * Ny;
+            else base = (size_t)li;
+            for (int t = 0; t < L; t++) {
+                line[2 * t] = c[2 * (base + t * strides[ax])];
+                line[2 * t + 1] = c[2 * (base + t * strides[ax]) + 1];
+            }
+            bm_fft_exec(L, tw, line, sign, scr);
+            for (int t = 0; t < L; t++) {
+                c[2 * (base + t * strides[ax])] = line[2 * t];
+                c[2 * (base + t * strides[ax]) + 1] = line[2 * t + 1];
+            }
+        }
+        free(line); free(scr);
+    }
+    bm_fft_table_free(tw);
+}
+
+/* Octant spectra from a tensor on the N grid the way DemagKernel builds them
+ * (Boris/DemagKernel.cpp:171-300 2D, :317-470 3D): a real forward DFT along x, y, z in turn, after
+ * each of which only the real part (even along that axis) or the imaginary part (odd along it) is
+ * kept as the next input: xx, yy, zz Re Re Re; xy Im Im, then -Re along z; xz Im, Re, -Im; yz Re, Im,
+ * -Im (2D: xy Im along x, -Im along y). Same layout as orc_kernels. */
+int orc_kernels_from_tensor(const double *dg, const double *od, int nz, int Nx, int Ny, int Nz, double *kdiag,
+                            double *kodiag)
+{
+    size_t np = (size_t)Nx * Ny * Nz;
+    double *c = (double *)malloc(sizeof(double) * 2 * np);
+    int Kx = Nx / 2 + 1, Ky = Ny / 2 + 1, Kz = Nz / 2 + 1;
+    /* part kept after each axis: 0 Re, 1 Im; final sign */
+    static const int keep[6][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+    for (int comp = 0; comp < 6; comp++) {
+        const double *src = comp < 3 ? dg : od;
+        int cc = comp % 3;
+        double *dst = comp < 3 ? kdiag : kodiag;
+        if (nz == 1 && comp >= 4) {
+            for (size_t q = 0; q < (size_t)Kx * Ky * Kz; q++) dst[3 * q + cc] = 0.0;
+            continue;
+        }
+        for (size_t p = 0; p < np; p++) { c[2 * p] = src[3 * p + cc]; c[2 * p + 1] = 0.0; }
+        int dims[3] = {Nx, Ny, Nz};
+        int last = (Nz > 1) ? 2 : 1;
+        double sgn = comp < 3 ? 1.0 : -1.0;
+        for (int ax = 0; ax <= last; ax++) {
+            if (dims[ax] > 1) dft_axis(c, Nx, Ny, Nz, ax, -1);
+            int part = keep[comp][ax];
+            for (size_t p = 0; p < np; p++) { c[2 * p] = c[2 * p + part]; c[2 * p + 1] = 0.0; }
+        }
+        for (int k = 0; k < Kz; k++)
+            for (int j = 0; j < Ky; j++)
+                for (int i = 0; i < Kx; i++) {
+                    size_t p = (size_t)i + (size_t)j * Nx + (size_t)k * Nx * Ny;
+                    size_t q = (size_t)i + (size_t)j * Kx + (size_t)k * Kx * Ky;
+                    dst[3 * q + cc] = sgn * c[2 * p];
+                }
+    }
+    free(c);
+    return 0;
+}
+
+/* FFT sizes of ConvolutionData::SetConvolutionDimensions (Boris/ConvolutionData.cpp:115-145):
+ * n along a periodic axis, 2n otherwise, 1 along z for a one-cell-thick mesh */
+void orc_pbc_dims(int nx, int ny, int nz, const int *pbc, int *N3)
+{
+    N3[0] = (pbc && pbc[0]) ? nx : 2 * nx;
+    N3[1] = (pbc && pbc[1]) ? ny : 2 * ny;
+    N3[2] = nz > 1 ? ((pbc && pbc[2]) ? nz : 2 * nz) : 1;
+}
+
 /* ------------------------------------------------------------------ convolution */
 
 struct orc_demag {
@@ -357,6 +547,25 @@ orc_demag *orc_demag_create(int nx, int ny, int nz, double hx, double hy, double
     d->kd = (double *)malloc(sizeof(double) * 3 * nk);
     d->ko = (double *)malloc(sizeof(double) * 3 * nk);
     orc_kernels(nx, ny, nz, Nx, Ny, Nz, hx, hy, hz, d->kd, d->ko);
+    return d;
+}
+
+/* demag with PBC images per axis (pbc NULL or all zero: the plain convolution with N = 2n) */
+orc_demag *orc_demag_create_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const int *pbc)
+{
+    int N3[3];
+    orc_pbc_dims(nx, ny, nz, pbc, N3);
+    if (!pbc || !(pbc[0] || pbc[1] || pbc[2])) return orc_demag_create(nx, ny, nz, hx, hy, hz, N3[0], N3[1], N3[2]);
+    orc_demag *d = (orc_demag *)calloc(1, sizeof(orc_demag));
+    d->nx = nx; d->ny = ny; d->nz = nz; d->Nx = N3[0]; d->Ny = N3[1]; d->Nz = N3[2];
+    size_t np = (size_t)N3[0] * N3[1] * N3[2];
+    size_t nk = (size_t)(N3[0] / 2 + 1) * (N3[1] / 2 + 1) * (N3[2] / 2 + 1);
+    d->kd = (double *)malloc(sizeof(double) * 3 * nk);
+    d->ko = (double *)malloc(sizeof(double) * 3 * nk);
+    double *dg = (double *)malloc(sizeof(double) * 3 * np), *od = (double *)malloc(sizeof(double) * 3 * np);
+    orc_tensor_pbc(nx, ny, nz, N3[0], N3[1], N3[2], hx, hy, hz, pbc, dg, od);
+    orc_kernels_from_tensor(dg, od, nz, N3[0], N3[1], N3[2], d->kd, d->ko);
+    free(dg); free(od);
     return d;
 }
 
@@ -945,15 +1154,23 @@ int orc_ml_transfer(orc_ml *s, int l, const double *M, double *Mc, const double 
 static double ms_at(const double *Ms_cell, size_t i) { return Ms_cell[i]; }
 
 /* one axis of delsq_nneu / grad_nneu (VEC_VC_Del.h:141-200, VEC_VC_Grad.h:139-183) for a
- * full rectangular mesh without PBC; bd = boundary differential along this axis (0 = neu) */
-static void axis_terms(const double *M, size_t idx, int coord, int ncoord, size_t stride, double h,
-                       const double *bd, double *d2, double *g)
+ * full rectangular mesh; bd = boundary differential along this axis (0 = neu); wrap = 0, or the
+ * sign (+1 / -1) of a periodic axis, whose missing neighbour is the cell on the far side times wrap
+ * (the NF_PBC branches there; a one-cell axis has no neighbour either way) */
+static void axis_terms_w(const double *M, size_t idx, int coord, int ncoord, size_t stride, double h,
+                         const double *bd, int wrap, double *d2, double *g)
 {
     int has_p = coord + 1 < ncoord, has_m = coord > 0;
+    size_t ip = idx + stride, im = idx - stride;
+    double sp = 1.0, sm = 1.0;
+    if (wrap && ncoord > 1) {
+        if (!has_p) { has_p = 1; ip = idx - (size_t)(ncoord - 1) * stride; sp = wrap; }
+        if (!has_m) { has_m = 1; im = idx + (size_t)(ncoord - 1) * stride; sm = wrap; }
+    }
     for (int c = 0; c < 3; c++) {
         double q = M[3 * idx + c];
         if (has_p && has_m) {
-            double qp = M[3 * (idx + stride) + c], qm = M[3 * (idx - stride) + c];
+            double qp = sp * M[3 * ip + c], qm = sm * M[3 * im + c];
             d2[c] = (qp + qm - 2.0 * q) / (h * h);
             g[c] = (qp - qm) / (2.0 * h);
         } else if (has_p) {
@@ -971,8 +1188,16 @@ static void axis_terms(const double *M, size_t idx, int coord, int ncoord, size_
     }
 }
 
-void orc_field_exchange(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
-                        double A, const double *Ms_cell, double *H)
+static void axis_terms(const double *M, size_t idx, int coord, int ncoord, size_t stride, double h,
+                       const double *bd, double *d2, double *g)
+{
+    axis_terms_w(M, idx, coord, ncoord, stride, h, bd, 0, d2, g);
+}
+
+static int wrap_of(const int *pbc, int ax) { return pbc ? isgn(pbc[ax]) : 0; }
+
+void orc_field_exchange_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
+                            double A, const double *Ms_cell, const int *pbc, double *H)
 {
     static const double zero[3] = {0, 0, 0};
 #pragma omp parallel for collapse(2) if (((long)nx * ny * nz) > ORC_PAR_MIN)
@@ -981,17 +1206,23 @@ void orc_field_exchange(int nx, int ny, int nz, double hx, double hy, double hz,
             for (int i = 0; i < nx; i++) {
                 size_t idx = (size_t)i + (size_t)j * nx + (size_t)k * nx * ny;
                 double dx[3], dy[3], dz[3], g[3];
-                axis_terms(M, idx, i, nx, 1, hx, zero, dx, g);
-                axis_terms(M, idx, j, ny, nx, hy, zero, dy, g);
-                axis_terms(M, idx, k, nz, (size_t)nx * ny, hz, zero, dz, g);
+                axis_terms_w(M, idx, i, nx, 1, hx, zero, wrap_of(pbc, 0), dx, g);
+                axis_terms_w(M, idx, j, ny, nx, hy, zero, wrap_of(pbc, 1), dy, g);
+                axis_terms_w(M, idx, k, nz, (size_t)nx * ny, hz, zero, wrap_of(pbc, 2), dz, g);
                 double Ms = ms_at(Ms_cell, idx);
                 double cst = 2.0 * A / (ORC_MU0 * Ms * Ms);
                 for (int c = 0; c < 3; c++) H[3 * idx + c] += cst * (dx[c] + dy[c] + dz[c]);
             }
 }
 
-void orc_field_idmi(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
-                    double A, double D, const double *Ms_cell, double *H)
+void orc_field_exchange(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
+                        double A, const double *Ms_cell, double *H)
+{
+    orc_field_exchange_pbc(nx, ny, nz, hx, hy, hz, M, A, Ms_cell, NULL, H);
+}
+
+void orc_field_idmi_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
+                        double A, double D, const double *Ms_cell, const int *pbc, double *H)
 {
     static const double zero[3] = {0, 0, 0};
 #pragma omp parallel for collapse(2) if (((long)nx * ny * nz) > ORC_PAR_MIN)
@@ -1004,15 +1235,21 @@ void orc_field_idmi(int nx, int ny, int nz, double hx, double hy, double hz, con
                 double bx[3] = {r * m[2], 0.0, -r * m[0]};
                 double by[3] = {0.0, r * m[2], -r * m[1]};
                 double dx[3], dy[3], dz[3], gx[3], gy[3], gz[3];
-                axis_terms(M, idx, i, nx, 1, hx, bx, dx, gx);
-                axis_terms(M, idx, j, ny, nx, hy, by, dy, gy);
-                axis_terms(M, idx, k, nz, (size_t)nx * ny, hz, zero, dz, gz);
+                axis_terms_w(M, idx, i, nx, 1, hx, bx, wrap_of(pbc, 0), dx, gx);
+                axis_terms_w(M, idx, j, ny, nx, hy, by, wrap_of(pbc, 1), dy, gy);
+                axis_terms_w(M, idx, k, nz, (size_t)nx * ny, hz, zero, wrap_of(pbc, 2), dz, gz);
                 double Ms = ms_at(Ms_cell, idx);
                 double Ac = 2.0 * A / (ORC_MU0 * Ms * Ms);
                 double Dc = -2.0 * D / (ORC_MU0 * Ms * Ms);
                 double hd[3] = {gx[2], gy[2], -gx[0] - gy[1]};
                 for (int c = 0; c < 3; c++) H[3 * idx + c] += Ac * (dx[c] + dy[c] + dz[c]) + Dc * hd[c];
             }
+}
+
+void orc_field_idmi(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
+                    double A, double D, const double *Ms_cell, double *H)
+{
+    orc_field_idmi_pbc(nx, ny, nz, hx, hy, hz, M, A, D, Ms_cell, NULL, H);
 }
 
 void orc_field_aniuni(int n, const double *M, const double *Ms_cell, const double *K1_cell, double K2,
@@ -1088,8 +1325,8 @@ orc_solver *orc_solver_create(int nmesh, const orc_mesh_desc *desc, int eval, do
         m->sM1 = (double *)calloc(n3, sizeof(double));
         for (int e = 0; e < 6; e++) m->sEval[e] = (double *)calloc(n3, sizeof(double));
         if (desc[q].modules & ORC_DEMAG)
-            m->dm = orc_demag_create(desc[q].nx, desc[q].ny, desc[q].nz, desc[q].hx, desc[q].hy, desc[q].hz,
-                                     fft_size(desc[q].nx), fft_size(desc[q].ny), fft_size(desc[q].nz));
+            m->dm = orc_demag_create_pbc(desc[q].nx, desc[q].ny, desc[q].nz, desc[q].hx, desc[q].hy, desc[q].hz,
+                                         desc[q].pbc);
     }
     return s;
 }
@@ -1215,8 +1452,10 @@ static void update_fields(orc_solver *s, orc_mesh *m)
             m->H[i] += v;
         }
     } else if (d->modules & ORC_DEMAG) orc_demag_apply(m->dm, m->M, m->H, 1);
-    if (d->modules & ORC_IDMI) orc_field_idmi(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, m->M, d->A, d->D, m->Ms, m->H);
-    else if (d->modules & ORC_EXCH) orc_field_exchange(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, m->M, d->A, m->Ms, m->H);
+    if (d->modules & ORC_IDMI)
+        orc_field_idmi_pbc(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, m->M, d->A, d->D, m->Ms, d->pbc, m->H);
+    else if (d->modules & ORC_EXCH)
+        orc_field_exchange_pbc(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, m->M, d->A, m->Ms, d->pbc, m->H);
     if (d->modules & ORC_ANIUNI) orc_field_aniuni(m->n, m->M, m->Ms, m->K1, d->K2, d->ea, m->H);
 }
 
@@ -1372,7 +1611,10 @@ int orc_solver_set_evalspeedup(orc_solver *s, int level)
     s->es_available = 1;
     for (int q = 0; q < s->nmesh; q++) {
         orc_mesh *m = &s->m[q];
-        orc_selfdemag(m->d.hx, m->d.hy, m->d.hz, m->self);
+        {
+            const int n3[3] = {m->d.nx, m->d.ny, m->d.nz};
+            orc_selfdemag_pbc(m->d.hx, m->d.hy, m->d.hz, n3, m->d.pbc, m->self);
+        }
         for (int k = 0; k < 6; k++) {
             free(m->Hs[k]);
             m->Hs[k] = k < level ? (double *)calloc(3 * (size_t)m->n, sizeof(double)) : NULL;
@@ -1536,7 +1778,7 @@ static void adj_fields(adj_ctx *a, const double *X, const double *Ha, double *H)
     const orc_mesh_desc *d = a->d;
     for (int i = 0; i < a->n; i++) { H[3 * i] = Ha[0]; H[3 * i + 1] = Ha[1]; H[3 * i + 2] = Ha[2]; }
     if (d->modules & ORC_DEMAG) orc_demag_apply(a->dm, X, H, 1);
-    if (d->modules & ORC_EXCH) orc_field_exchange(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, X, d->A, a->Ms, H);
+    if (d->modules & ORC_EXCH) orc_field_exchange_pbc(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, X, d->A, a->Ms, d->pbc, H);
     if (d->modules & ORC_ANIUNI) orc_field_aniuni(a->n, X, a->Ms, a->K1, 0.0, d->ea, H);
 }
 
@@ -1550,9 +1792,9 @@ static void adj_lap(const orc_mesh_desc *d, const double *V, double *out)
             for (int i = 0; i < nx; i++) {
                 size_t idx = (size_t)i + (size_t)j * nx + (size_t)k * nx * ny;
                 double dx[3], dy[3], dz[3], g[3];
-                axis_terms(V, idx, i, nx, 1, d->hx, zero, dx, g);
-                axis_terms(V, idx, j, ny, nx, d->hy, zero, dy, g);
-                axis_terms(V, idx, k, nz, (size_t)nx * ny, d->hz, zero, dz, g);
+                axis_terms_w(V, idx, i, nx, 1, d->hx, zero, wrap_of(d->pbc, 0), dx, g);
+                axis_terms_w(V, idx, j, ny, nx, d->hy, zero, wrap_of(d->pbc, 1), dy, g);
+                axis_terms_w(V, idx, k, nz, (size_t)nx * ny, d->hz, zero, wrap_of(d->pbc, 2), dz, g);
                 for (int c = 0; c < 3; c++) out[3 * idx + c] = dx[c] + dy[c] + dz[c];
             }
 }
@@ -1663,8 +1905,7 @@ int orc_adjoint_rk4(const orc_mesh_desc *d, const double *m0, const double *targ
         K1[i] = d->K1_map ? d->K1_map[i] : d->K1;
     }
     a.Ms = Ms; a.K1 = K1;
-    a.dm = (d->modules & ORC_DEMAG) ? orc_demag_create(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, fft_size(d->nx),
-                                                       fft_size(d->ny), fft_size(d->nz)) : 0;
+    a.dm = (d->modules & ORC_DEMAG) ? orc_demag_create_pbc(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, d->pbc) : 0;
     a.tmp = (double *)calloc(21 * (size_t)n, sizeof(double));
     size_t v3 = 3 * (size_t)n;
     double *Ms_hist = (double *)malloc(sizeof(double) * v3 * (steps + 1));

@@ -33,18 +33,36 @@ int orc_tensor(int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double
 int orc_kernels(int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz,
                 double *kdiag, double *kodiag);
 
+/* ---- periodic boundary conditions (pbc: images per axis) ---- */
+/* D = -N on the N grid with images (DemagTFunc_PBC.cpp); N from orc_pbc_dims */
+int orc_tensor_pbc(int nx, int ny, int nz, int Nx, int Ny, int Nz, double hx, double hy, double hz, const int *pbc,
+                   double *diag, double *odiag);
+/* octant spectra of a tensor on the N grid, built axis by axis as DemagKernel does */
+int orc_kernels_from_tensor(const double *diag, const double *odiag, int nz, int Nx, int Ny, int Nz, double *kdiag,
+                            double *kodiag);
+/* FFT sizes: n along a periodic axis, 2n otherwise (ConvolutionData.cpp:115-145) */
+void orc_pbc_dims(int nx, int ny, int nz, const int *pbc, int *N3);
+/* SelfDemag_PBC (DemagTFunc_Self.cpp:57) on normalised cellsizes */
+void orc_selfdemag_pbc(double hx, double hy, double hz, const int *n3, const int *pbc, double *out3);
+
 /* ---- demag convolution ---- */
 typedef struct orc_demag orc_demag;
 orc_demag *orc_demag_create(int nx, int ny, int nz, double hx, double hy, double hz, int Nx, int Ny, int Nz);
 /* H = D * M; if add, H += instead of H =. Returns sum_i M_i . Hdemag_i */
 double orc_demag_apply(orc_demag *d, const double *M, double *H, int add);
 void orc_demag_destroy(orc_demag *d);
+/* with PBC images per axis (NULL / zeros: as orc_demag_create with N = 2n) */
+orc_demag *orc_demag_create_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const int *pbc);
 
 /* ---- field terms (add into H) ---- */
 void orc_field_exchange(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
                         double A, const double *Ms_cell, double *H);
 void orc_field_idmi(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
                     double A, double D, const double *Ms_cell, double *H);
+void orc_field_exchange_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
+                            double A, const double *Ms_cell, const int *pbc, double *H);
+void orc_field_idmi_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const double *M,
+                        double A, double D, const double *Ms_cell, const int *pbc, double *H);
 void orc_field_aniuni(int n, const double *M, const double *Ms_cell, const double *K1_cell, double K2,
                       const double *ea, double *H);
 
@@ -60,6 +78,7 @@ typedef struct {
     const double *Ha;      /* 3 * nHa piecewise-constant applied-field samples over [0, Ha_tspan) */
     int nHa;
     double Ha_tspan;
+    int pbc[3];            /* periodic images per axis (0: none; the sign is the stencils' wrap sign) */
 } orc_mesh_desc;
 
 typedef struct {

@@ -26,6 +26,12 @@
  *                      layer with the rectangle rules of SDemag (Boris/SDemag.cpp:173,215,441), the
  *                      weighted mesh transfer of SDemag_Demag (Boris/SDemag_Demag.cpp:64,349) and the
  *                      evaluation order of SDemag::UpdateField (Boris/SDemag.cpp:786-900)
+ *   ref_*_pbc          the same with periodic boundary conditions: DemagTFunc::Calc{Diag,OffDiag}Tens
+ *                      {2D,3D}_PBC (Boris/DemagTFunc_PBC.cpp:5,97,185,300), the convolution set up by
+ *                      SetDimensions(n, h, true, pbc_images) (Boris/Convolution.h:248,
+ *                      Boris/ConvolutionData.cpp:100) as Demag::Initialize does (Boris/Demag.cpp:111),
+ *                      the stencils on a VEC_VC with set_pbc (BorisLib/VEC_VC_flags.h:890), and
+ *                      DemagTFunc::SelfDemag_PBC (Boris/DemagTFunc_Self.cpp:57)
  *   ref_ovf2_read      OVF2::Read_OVF2_VEC                  (Boris/OVF2_Handlers.cpp:364)
  *   ref_ovf2_write     OVF2::Write_OVF2_VEC                 (Boris/OVF2_Handlers.cpp:701)
  *   ref_ovf2_load      the loadovf2mag command's data path (Boris/Commands.cpp:5025): read,
@@ -46,11 +52,17 @@
 namespace {
 
 struct OracleDemag : public Convolution<OracleDemag, DemagKernel> {
+    BError pbc_err;
     OracleDemag(INT3 n_, DBL3 h_) : Convolution<OracleDemag, DemagKernel>(n_, h_) {}
+    /* with PBC images, set up as Demag::Initialize does (Boris/Demag.cpp:111) */
+    OracleDemag(INT3 n_, DBL3 h_, INT3 pbc) : Convolution<OracleDemag, DemagKernel>()
+    {
+        pbc_err = SetDimensions(n_, h_, true, pbc);
+    }
     BError calc(void) { return Calculate_Demag_Kernels(true); }
     SZ3 get_N(void) const { return N; }
     SZ3 get_n(void) const { return n; }
-    bool create_failed(void) { return (bool)Convolution_Error_on_Create(); }
+    bool create_failed(void) { return (bool)Convolution_Error_on_Create() || (bool)pbc_err; }
     double convolute(VEC<DBL3> &In, VEC<DBL3> &Out) { return Convolute(In, Out, true); }
 };
 
@@ -330,6 +342,113 @@ void ref_film_fields_destroy(void *h)
     if (!s) return;
     delete s->od;
     delete s;
+}
+
+/* ---- periodic boundary conditions: pbc = images per axis ---- */
+
+/* D = -N on the PBC N grid (N = n along periodic axes, ConvolutionData.cpp:115-145), cellsizes
+ * normalised by the largest as DemagKernel passes them; 2D: odiag holds Dxy in component 0 only. */
+int ref_tensor_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const int *pbc, double *diag, double *odiag,
+                   int *N3)
+{
+    DBL3 h(hx, hy, hz);
+    double hm = maximum(hx, hy, hz);
+    INT3 N(pbc[0] ? nx : 2 * nx, pbc[1] ? ny : 2 * ny, nz > 1 ? (pbc[2] ? nz : 2 * nz) : 1);
+    N3[0] = N.x; N3[1] = N.y; N3[2] = N.z;
+    if (!diag) return 0;
+    DemagTFunc dtf;
+    VEC<DBL3> D;
+    if (!D.resize(SZ3(N.x, N.y, N.z))) return 1;
+    size_t np = (size_t)N.x * N.y * N.z;
+    if (nz == 1) {
+        if (!dtf.CalcDiagTens2D_PBC(D, N, h / hm, true, ASYMPTOTIC_DISTANCE, pbc[0], pbc[1], pbc[2])) return 2;
+        memcpy(diag, D.data(), sizeof(double) * 3 * np);
+        std::vector<double> od(np, 0.0);
+        if (!dtf.CalcOffDiagTens2D_PBC(od, N, h / hm, true, ASYMPTOTIC_DISTANCE, pbc[0], pbc[1], pbc[2])) return 3;
+        for (size_t i = 0; i < np; i++) { odiag[3 * i] = od[i]; odiag[3 * i + 1] = 0; odiag[3 * i + 2] = 0; }
+    }
+    else {
+        if (!dtf.CalcDiagTens3D_PBC(D, N, h / hm, true, ASYMPTOTIC_DISTANCE, pbc[0], pbc[1], pbc[2])) return 2;
+        memcpy(diag, D.data(), sizeof(double) * 3 * np);
+        if (!dtf.CalcOffDiagTens3D_PBC(D, N, h / hm, true, ASYMPTOTIC_DISTANCE, pbc[0], pbc[1], pbc[2])) return 3;
+        memcpy(odiag, D.data(), sizeof(double) * 3 * np);
+    }
+    return 0;
+}
+
+/* Kernel spectra of the PBC convolution as DemagKernel stores them (layouts as ref_kernels). */
+int ref_kernels_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const int *pbc, double *kdiag, double *kodiag)
+{
+    OracleDemag od(INT3(nx, ny, nz), DBL3(hx, hy, hz), INT3(pbc[0], pbc[1], pbc[2]));
+    if (od.create_failed()) return 1;
+    if (od.calc()) return 2;
+    memcpy(kdiag, od.Kdiag.data(), sizeof(double) * 3 * od.Kdiag.linear_size());
+    if (nz == 1) memcpy(kodiag, od.K2D_odiag.data(), sizeof(double) * od.K2D_odiag.size());
+    else memcpy(kodiag, od.Kodiag.data(), sizeof(double) * 3 * od.Kodiag.linear_size());
+    return 0;
+}
+
+/* H = D * M with PBC (Out cleared first); energy as ref_demag_eval. */
+int ref_hdemag_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const int *pbc, const double *M, double *H,
+                   double *energy)
+{
+    OracleDemag od(INT3(nx, ny, nz), DBL3(hx, hy, hz), INT3(pbc[0], pbc[1], pbc[2]));
+    if (od.create_failed()) return 1;
+    if (od.calc()) return 2;
+    Rect r(DBL3(0, 0, 0), DBL3(hx * nx, hy * ny, hz * nz));
+    VEC<DBL3> In(DBL3(hx, hy, hz), r), Out(DBL3(hx, hy, hz), r);
+    int n = nx * ny * nz;
+    memcpy(In.data(), M, sizeof(double) * 3 * n);
+    double dot = od.convolute(In, Out);
+    memcpy(H, Out.data(), sizeof(double) * 3 * n);
+    if (energy) *energy = -MU0 * dot / (2.0 * n);
+    return 0;
+}
+
+/* exchange (modules 2) or exchange + iDMI (modules 4) field with PBC on the stencils, per-cell A, D, Ms
+ * (D ignored for exchange); the formulas of ref_exchange / ref_idmi */
+int ref_stencil_pbc(int nx, int ny, int nz, double hx, double hy, double hz, const int *pbc, int modules, const double *M,
+                    const double *A, const double *D, const double *Ms, double *H)
+{
+    Rect r(DBL3(0, 0, 0), DBL3(hx * nx, hy * ny, hz * nz));
+    VEC_VC<DBL3> V(DBL3(hx, hy, hz), r, DBL3(1, 0, 0));
+    V.set_pbc(pbc[0], pbc[1], pbc[2]);
+    int n = nx * ny * nz;
+    memcpy(V.data(), M, sizeof(double) * 3 * n);
+    for (int idx = 0; idx < n; idx++) {
+        double Aconst = 2 * A[idx] / (MU0 * Ms[idx] * Ms[idx]);
+        DBL3 Ht;
+        if (modules & 4) {
+            double Dconst = -2 * D[idx] / (MU0 * Ms[idx] * Ms[idx]);
+            DBL3 HA, HD;
+            if (V.is_plane_interior(idx)) {
+                HA = Aconst * V.delsq_neu(idx);
+                DBL33 Md = V.grad_neu(idx);
+                HD = Dconst * DBL3(Md.x.z, Md.y.z, -Md.x.x - Md.y.y);
+            }
+            else {
+                DBL3 bx = (D[idx] / (2 * A[idx])) * DBL3(V[idx].z, 0, -V[idx].x);
+                DBL3 by = (D[idx] / (2 * A[idx])) * DBL3(0, V[idx].z, -V[idx].y);
+                DBL33 bnd(bx, by, DBL3());
+                HA = Aconst * V.delsq_nneu(idx, bnd);
+                DBL33 Md = V.grad_nneu(idx, bnd);
+                HD = Dconst * DBL3(Md.x.z, Md.y.z, -Md.x.x - Md.y.y);
+            }
+            Ht = HA + HD;
+        }
+        else Ht = Aconst * V.delsq_neu(idx);
+        H[3 * idx] = Ht.x; H[3 * idx + 1] = Ht.y; H[3 * idx + 2] = Ht.z;
+    }
+    return 0;
+}
+
+/* DemagTFunc::SelfDemag_PBC(h, n, pbc) as Demag.cpp:62 and DemagCUDA.cpp:39 call it */
+int ref_selfdemag_pbc(double hx, double hy, double hz, int nx, int ny, int nz, const int *pbc, double *out3)
+{
+    DemagTFunc dtf;
+    DBL3 s = dtf.SelfDemag_PBC(DBL3(hx, hy, hz), DBL3(nx, ny, nz), INT3(pbc[0], pbc[1], pbc[2]));
+    out3[0] = s.x; out3[1] = s.y; out3[2] = s.z;
+    return 0;
 }
 
 /* Shifted real-space tensors D = -N on the N grid (AoS, 3 doubles per point).

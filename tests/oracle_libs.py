@@ -57,7 +57,7 @@ class MeshDesc(ctypes.Structure):
     _fields_ = [("nx", I), ("ny", I), ("nz", I), ("hx", D), ("hy", D), ("hz", D),
                 ("Ms", D), ("A", D), ("D", D), ("alpha", D), ("grel", D), ("K1", D), ("K2", D),
                 ("ea", D * 3), ("Ms_map", DP), ("K1_map", DP), ("modules", I),
-                ("Ha", DP), ("nHa", I), ("Ha_tspan", D)]
+                ("Ha", DP), ("nHa", I), ("Ha_tspan", D), ("pbc", I * 3)]
 
 
 class OrcStats(ctypes.Structure):
@@ -105,6 +105,14 @@ def oracle():
         L.orc_solver_set_evalspeedup.argtypes = [P, I]
         L.orc_adjoint_rk4.argtypes = [ctypes.POINTER(MeshDesc), DP, DP, I, D, DP, DP, DP, DP]
         L.orc_solver_set_field_hook.argtypes = [P, I, P, P]
+        L.orc_tensor_pbc.argtypes = [I, I, I, I, I, I, D, D, D, IP, DP, DP]
+        L.orc_kernels_from_tensor.argtypes = [DP, DP, I, I, I, I, DP, DP]
+        L.orc_pbc_dims.argtypes = [I, I, I, IP, IP]
+        L.orc_selfdemag_pbc.argtypes = [D, D, D, IP, IP, DP]
+        L.orc_demag_create_pbc.restype = P
+        L.orc_demag_create_pbc.argtypes = [I, I, I, D, D, D, IP]
+        L.orc_field_exchange_pbc.argtypes = [I, I, I, D, D, D, DP, D, DP, IP, DP]
+        L.orc_field_idmi_pbc.argtypes = [I, I, I, D, D, D, DP, D, D, DP, IP, DP]
         _orc = L
     return _orc
 
@@ -194,6 +202,11 @@ def reference():
         L.ref_exchange.argtypes = [I, I, I, D, D, D, DP, DP, DP, DP]
         L.ref_idmi.argtypes = [I, I, I, D, D, D, DP, DP, DP, DP, DP]
         L.ref_tensor_shifted.argtypes = [I, I, I, I, I, I, I, DP, DP, DP, I, DP, DP]
+        L.ref_tensor_pbc.argtypes = [I, I, I, D, D, D, IP, DP, DP, IP]
+        L.ref_kernels_pbc.argtypes = [I, I, I, D, D, D, IP, DP, DP]
+        L.ref_hdemag_pbc.argtypes = [I, I, I, D, D, D, IP, DP, DP, DP]
+        L.ref_stencil_pbc.argtypes = [I, I, I, D, D, D, IP, I, DP, DP, DP, DP, DP]
+        L.ref_selfdemag_pbc.argtypes = [D, D, D, I, I, I, IP, DP]
         L.ref_ml_create.restype = P
         L.ref_ml_create.argtypes = [I, IP, DP, DP, I, IP]
         L.ref_ml_info.argtypes = [P, IP, IP, IP, IP, DP, IP]
@@ -286,6 +299,113 @@ class MultiLayer:
         self.close()
 
 
+def _i3(v):
+    return (ctypes.c_int * 3)(*(int(x) for x in v))
+
+
+def orc_hdemag_pbc(M, n, h, pbc):
+    """FP64 demag field of M with PBC images per axis (oracle: the reference's algorithm, N = n along
+    periodic axes)."""
+    L = oracle()
+    d = L.orc_demag_create_pbc(n[0], n[1], n[2], h[0], h[1], h[2], _i3(pbc))
+    Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+    H = np.zeros_like(Mf)
+    dot = L.orc_demag_apply(P(d), dp(Mf), dp(H), 0)
+    L.orc_demag_destroy(P(d))
+    return H.reshape(-1, 3), dot
+
+
+def ref_hdemag_pbc(M, n, h, pbc):
+    R = reference()
+    Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+    H = np.zeros_like(Mf)
+    e = np.zeros(1)
+    assert R.ref_hdemag_pbc(n[0], n[1], n[2], h[0], h[1], h[2], _i3(pbc), dp(Mf), dp(H), dp(e)) == 0
+    return H.reshape(-1, 3), e[0]
+
+
+def pbc_dims(n, pbc):
+    N3 = (ctypes.c_int * 3)()
+    oracle().orc_pbc_dims(n[0], n[1], n[2], _i3(pbc), N3)
+    return tuple(N3)
+
+
+def orc_tensor_pbc(n, h, pbc):
+    """(diag, odiag) on the PBC N grid, shape (Nz, Ny, Nx, 3) each."""
+    N = pbc_dims(n, pbc)
+    np_ = N[0] * N[1] * N[2]
+    dg = np.zeros(3 * np_)
+    od = np.zeros(3 * np_)
+    oracle().orc_tensor_pbc(n[0], n[1], n[2], N[0], N[1], N[2], h[0], h[1], h[2], _i3(pbc), dp(dg), dp(od))
+    return dg.reshape(N[2], N[1], N[0], 3), od.reshape(N[2], N[1], N[0], 3)
+
+
+def ref_tensor_pbc(n, h, pbc):
+    R = reference()
+    N3 = (ctypes.c_int * 3)()
+    assert R.ref_tensor_pbc(n[0], n[1], n[2], h[0], h[1], h[2], _i3(pbc), None, None, N3) == 0
+    N = tuple(N3)
+    np_ = N[0] * N[1] * N[2]
+    dg = np.zeros(3 * np_)
+    od = np.zeros(3 * np_)
+    assert R.ref_tensor_pbc(n[0], n[1], n[2], h[0], h[1], h[2], _i3(pbc), dp(dg), dp(od), N3) == 0
+    return dg.reshape(N[2], N[1], N[0], 3), od.reshape(N[2], N[1], N[0], 3)
+
+
+def orc_kernels_pbc(n, h, pbc):
+    """Octant spectra (kdiag, kodiag), each (Kz, Ky, Kx, 3), of the oracle's PBC convolution."""
+    N = pbc_dims(n, pbc)
+    dg, od = orc_tensor_pbc(n, h, pbc)
+    K = (N[0] // 2 + 1, N[1] // 2 + 1, N[2] // 2 + 1)
+    nk = K[0] * K[1] * K[2]
+    kd = np.zeros(3 * nk)
+    ko = np.zeros(3 * nk)
+    oracle().orc_kernels_from_tensor(dp(np.ascontiguousarray(dg.reshape(-1))), dp(np.ascontiguousarray(od.reshape(-1))),
+                                     n[2], N[0], N[1], N[2], dp(kd), dp(ko))
+    return kd.reshape(K[2], K[1], K[0], 3), ko.reshape(K[2], K[1], K[0], 3)
+
+
+def ref_kernels_pbc(n, h, pbc):
+    """The reference's PBC kernel spectra; 2D: kodiag is Kxy only, returned in component 0."""
+    N = pbc_dims(n, pbc)
+    K = (N[0] // 2 + 1, N[1] // 2 + 1, N[2] // 2 + 1)
+    nk = K[0] * K[1] * K[2]
+    kd = np.zeros(3 * nk)
+    ko = np.zeros(3 * nk)
+    assert reference().ref_kernels_pbc(n[0], n[1], n[2], h[0], h[1], h[2], _i3(pbc), dp(kd), dp(ko)) == 0
+    if n[2] == 1:
+        k2 = ko[:nk].copy()
+        ko = np.zeros(3 * nk)
+        ko[0::3] = k2
+    return kd.reshape(K[2], K[1], K[0], 3), ko.reshape(K[2], K[1], K[0], 3)
+
+
+def orc_stencil_pbc(M, n, h, pbc, A, Ms, D=0.0, idmi=False):
+    L = oracle()
+    nc = n[0] * n[1] * n[2]
+    Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+    Msc = np.full(nc, float(Ms)) if np.isscalar(Ms) else np.ascontiguousarray(np.asarray(Ms, dtype=np.float64))
+    H = np.zeros_like(Mf)
+    if idmi:
+        L.orc_field_idmi_pbc(n[0], n[1], n[2], h[0], h[1], h[2], dp(Mf), A, D, dp(Msc), _i3(pbc), dp(H))
+    else:
+        L.orc_field_exchange_pbc(n[0], n[1], n[2], h[0], h[1], h[2], dp(Mf), A, dp(Msc), _i3(pbc), dp(H))
+    return H.reshape(-1, 3)
+
+
+def ref_stencil_pbc(M, n, h, pbc, A, Ms, D=0.0, idmi=False):
+    R = reference()
+    nc = n[0] * n[1] * n[2]
+    Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+    Ac = np.full(nc, float(A))
+    Dc = np.full(nc, float(D))
+    Msc = np.full(nc, float(Ms)) if np.isscalar(Ms) else np.ascontiguousarray(np.asarray(Ms, dtype=np.float64))
+    H = np.zeros_like(Mf)
+    assert R.ref_stencil_pbc(n[0], n[1], n[2], h[0], h[1], h[2], _i3(pbc), 4 if idmi else 2, dp(Mf), dp(Ac), dp(Dc),
+                             dp(Msc), dp(H)) == 0
+    return H.reshape(-1, 3)
+
+
 def ref_hdemag(M, n, h):
     R = reference()
     Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
@@ -324,6 +444,8 @@ class OracleSolver:
             d.Ha = dp(Ha)
             d.nHa = Ha.size // 3
             d.Ha_tspan = m.get("Ha_tspan", 0.0)
+            for k, v in enumerate(m.get("pbc", (0, 0, 0))):
+                d.pbc[k] = int(v)
         self._arr = arr
         self._meshes = meshes
         self._ref_fields = []
@@ -438,6 +560,8 @@ def orc_adjoint(mesh, m0, target, steps, dt):
     d.nHa = Ha.size // 3
     d.Ha_tspan = mesh["Ha_tspan"]
     d.modules = mesh.get("modules", 1 | 2 | 8 | 16)
+    for k, v in enumerate(mesh.get("pbc", (0, 0, 0))):
+        d.pbc[k] = int(v)
     n = int(np.prod(mesh["n"]))
     m0a = np.ascontiguousarray(np.asarray(m0, dtype=np.float64).reshape(-1))
     ta = np.ascontiguousarray(np.asarray(target, dtype=np.float64).reshape(-1))

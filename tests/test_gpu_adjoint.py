@@ -32,6 +32,8 @@ def _gpu(bm, mesh, m0, tgt, steps, dt, prec, ckpt, modules=1 | 2 | 8 | 16):
     c.set_material(0, Ms=8e5, A=mesh["A"], alpha=mesh["alpha"], ea=(0, 0, 1))
     c.set_material_maps(0, Ms_map=mesh["Ms_map"], K1_map=mesh["K1_map"])
     c.set_modules(0, modules)
+    if mesh.get("pbc") is not None:
+        c.set_pbc(0, mesh["pbc"])
     c.set_field(0, mesh["Ha"], mesh["Ha_tspan"])
     c.setode("RK4", dt)
     c.set_m(m0 * mesh["Ms_map"][:, None])

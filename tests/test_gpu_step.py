@@ -21,6 +21,8 @@ def _make(bm, prec, mesh, M, evaluation, dt, ctrl=None):
     if mesh.get("Ms_map") is not None or mesh.get("K1_map") is not None:
         c.set_material_maps(0, Ms_map=mesh.get("Ms_map"), K1_map=mesh.get("K1_map"))
     c.set_modules(0, mesh["modules"])
+    if mesh.get("pbc") is not None:
+        c.set_pbc(0, mesh["pbc"])
     c.set_field(0, mesh.get("Ha", (0, 0, 0)), mesh.get("Ha_tspan", 0.0))
     c.setode(evaluation, dt)
     if ctrl:
