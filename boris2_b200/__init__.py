@@ -35,7 +35,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libboris_b200.so")
 DEMAG, EXCH, IDMI, ANIUNI, ZEEMAN = 1, 2, 4, 8, 16
 RK4, RKDP54 = 0, 1
 FP64, MIXED = 0, 1
-ML_OFF, ML_3D, ML_2D, ML_2D_LAYERED = -1, 0, 1, 2
+ML_OFF, ML_3D, ML_2D, ML_2D_LAYERED, ML_SUPERMESH = -1, 0, 1, 2, 3
 
 _lib = None
 
@@ -106,6 +106,9 @@ _SIGS = {
     "bm_debug_fft": (_I, [_I, _I, _I, _I, _I, _DP]),
     "bm_fft_noalloc": (_I, [_I, _I, _I, _I, _P, _P, _P]),
     "bm_set_multiconvolution": (_I, [_P, _I, _IP]),
+    "bm_set_supermesh_cellsize": (_I, [_P, _D, _D, _D]),
+    "bm_set_supermesh_pbc": (_I, [_P, _I, _I, _I]),
+    "bm_supermesh_info": (_I, [_P, _IP, _DP, _DP, ctypes.POINTER(ctypes.c_longlong)]),
     "bm_ml_info": (_I, [_P, _IP, _IP, _IP, _IP, _DP, _IP]),
     "bm_prepare": (_I, [_P]),
     "bm_ml_time_kernels": (_I, [_P, _I, _DP, _DP]),
@@ -320,6 +323,23 @@ class Context:
         n = L.value
         return {"L": n, "n_common": tuple(nc), "layer_mesh": list(lm)[:n], "transfer": list(tr)[:n],
                 "rects": rc[:6 * n].reshape(n, 6).copy(), "kinds": np.array(list(kk)[:n * n]).reshape(n, n)}
+
+    def supermesh_cellsize(self, h):
+        """Requested supermesh cellsize (the reference's ``fmscellsize``; default 5 nm)."""
+        _check(lib().bm_set_supermesh_cellsize(self._h, float(h[0]), float(h[1]), float(h[2])))
+
+    def supermesh_pbc(self, images=(0, 0, 0)):
+        """PBC images of the supermesh convolution, also every mesh's stencil PBC (SDemag::Set_PBC)."""
+        x, y, z = (int(v) for v in images)
+        _check(lib().bm_set_supermesh_pbc(self._h, x, y, z))
+
+    def supermesh_info(self):
+        n = (ctypes.c_int * 3)()
+        h = np.zeros(3)
+        r = np.zeros(6)
+        ne = ctypes.c_longlong(0)
+        _check(lib().bm_supermesh_info(self._h, n, _dp(h), _dp(r), ctypes.byref(ne)))
+        return {"n": tuple(n), "h": tuple(h), "rect": r.reshape(2, 3).copy(), "nonempty": ne.value}
 
     def prepare(self):
         _check(lib().bm_prepare(self._h))

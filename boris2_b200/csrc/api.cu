@@ -105,6 +105,12 @@ struct MLRun {
     void *twz = nullptr;
     int W = 8;
     long long ncc = 0;
+    // supermesh demag (BM_ML_SUPERMESH): one demag grid over the meshes' bounding box
+    bool sm = false;
+    SMGeom smg;
+    Mesh smgrid;
+    std::vector<int *> sm_in_ptr, sm_in_idx;   // per mesh of mesh_of
+    std::vector<void *> sm_in_w;
 };
 
 // Graphs of a context with many meshes per launch are built in two passes: the first collects
@@ -165,7 +171,9 @@ struct bm_ctx {
     StepState host_st;
     bool batched = false;       // many meshes per launch (work lists) instead of one launch per mesh
     BatchPlan bp;
-    int ml_mode = -1;           // -1 off; 0 3D, 1 2D, 2 2D layered
+    int ml_mode = -1;           // -1 off; 0 3D, 1 2D, 2 2D layered, 3 supermesh
+    double sm_h[3] = {5e-9, 5e-9, 5e-9};   // requested supermesh cellsize (the reference's default h_fm)
+    int sm_pbc[3] = {0, 0, 0};  // PBC images of the supermesh convolution
     bool ml_nc_set = false;
     int ml_nc[3] = {1, 1, 1};
     MLRun *ml = nullptr;
@@ -211,6 +219,10 @@ void free_ml(bm_ctx *c)
     for (auto p : r.in_ptr) if (p) cudaFree(p);
     for (auto p : r.in_idx) if (p) cudaFree(p);
     for (auto p : r.in_w) if (p) cudaFree(p);
+    for (auto p : r.sm_in_ptr) if (p) cudaFree(p);
+    for (auto p : r.sm_in_idx) if (p) cudaFree(p);
+    for (auto p : r.sm_in_w) if (p) cudaFree(p);
+    free_mesh(r.smgrid);
     if (r.K) cudaFree(r.K);
     if (r.twz) cudaFree(r.twz);
     delete c->ml;
@@ -575,14 +587,12 @@ int tune_grid_x(bm_ctx *c, Mesh &G)
 }
 
 template <typename T>
-int autotune_mesh(bm_ctx *c, Mesh &m)
+void tune_grid_yz(bm_ctx *c, Mesh &m)
 {
     cudaStream_t s = c->stream;
     const int lim = bm_lb<T>::v;
-    const size_t cs = sizeof(cpx<T>);
     const int reps = 3;
-    if ((m.modules & BM_DEMAG) && m.ml_role == 1) tune_ypass<T>(c, m);   // its y passes feed the multilayer z pass
-    if ((m.modules & BM_DEMAG) && m.ml_role == 0) {
+    {
         YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
         if (m.nz == 1) {
             float best = 1e30f; int bw = m.W2;
@@ -621,6 +631,17 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
             }
         }
     }
+}
+
+template <typename T>
+int autotune_mesh(bm_ctx *c, Mesh &m)
+{
+    cudaStream_t s = c->stream;
+    const int lim = bm_lb<T>::v;
+    const size_t cs = sizeof(cpx<T>);
+    const int reps = 3;
+    if ((m.modules & BM_DEMAG) && m.ml_role == 1) tune_ypass<T>(c, m);   // its y passes feed the multilayer z pass
+    if ((m.modules & BM_DEMAG) && m.ml_role == 0) tune_grid_yz<T>(c, m);
     // stage kernel: rows per block
     T *tmp = nullptr;
     if (cudaMalloc(&tmp, sizeof(T) * 6 * m.n) != cudaSuccess) return 0;   // keep heuristic choice
@@ -661,6 +682,21 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
     return 0;
 }
 
+// The periodic tensor build evaluates (octant points) x (image terms) tensor values; bound it so a
+// set-up cannot hold the device for minutes.
+int pbc_work_check(const int nc[3], const int pbc[3])
+{
+    double work = 1.0;
+    for (int a = 0; a < 3; a++) {
+        const int X = std::abs(pbc[a]);
+        work *= X ? (double)(nc[a] / 2 + 1) * (2.0 * X + 2.0) : (double)nc[a];
+    }
+    if (work > 1e10)
+        return fail(BM_EUNSUPPORTED, "periodic tensor build of " + std::to_string(work) +
+                                         " tensor evaluations is above the limit of 1e10 (fewer images or cells)");
+    return 0;
+}
+
 // ------------------------------------------------------------------ multilayered convolution setup
 // Geometry and roles (host only, before the meshes allocate): every mesh with the demag module
 // takes part; a layer whose grid is its mesh's grid keeps its spectra in the mesh's S1/S2,
@@ -684,6 +720,15 @@ int ml_plan(bm_ctx *c)
     c->ml = r;
     r->mesh_of = of;
     std::string err;
+    if (c->ml_mode == BM_ML_SUPERMESH) {
+        r->sm = true;
+        if (sm_build_geometry(in, c->sm_h, r->smg, err)) return fail(BM_EINVAL, err);
+        const int *n = r->smg.n;
+        if (nice_size(n[0]) > 4096 || nice_size(n[1]) > 4096 || nice_size(n[2]) > 2048)
+            return fail(BM_EUNSUPPORTED, "supermesh: cell counts above the supported FFT size");
+        for (int k : of) c->meshes[k].ml_role = 2;
+        return pbc_work_check(n, c->sm_pbc);
+    }
     if (ml_build_geometry(in, c->ml_mode, c->ml_nc_set ? c->ml_nc : nullptr, r->g, err)) return fail(BM_EINVAL, err);
     if (!zmid_ml_supported(r->g.N[2])) return fail(BM_EUNSUPPORTED, "multilayer: common n.z above 32 is not supported");
     for (int l = 0; l < r->g.L; l++) c->meshes[of[r->g.layers[l].mesh]].ml_role = r->g.layers[l].transfer ? 2 : 1;
@@ -739,9 +784,64 @@ std::vector<T> as_type(const std::vector<double> &v)
 template <typename T> MLZArgs<T> ml_zargs(bm_ctx *c, int W, int gate);
 
 template <typename T>
+int prepare_sm(bm_ctx *c)
+{
+    MLRun &r = *c->ml;
+    const SMGeom &g = r.smg;
+    cudaStream_t s = c->stream;
+    Mesh &G = r.smgrid;
+    G.nx = g.n[0]; G.ny = g.n[1]; G.nz = g.n[2];
+    for (int a = 0; a < 3; a++) { G.h[a] = g.h[a]; G.o[a] = g.rs[a]; G.pbc[a] = c->sm_pbc[a]; }
+    G.modules = BM_DEMAG;
+    int rc;
+    if ((rc = prepare_grid<T>(c, G))) return rc;
+    size_t v3 = sizeof(T) * 3 * (size_t)G.n;
+    if (cudaMalloc(&G.Hout, v3) != cudaSuccess) return fail(BM_ENOMEM, "supermesh field");
+    cudaMemsetAsync(G.Hout, 0, v3, s);
+    // kernel spectra of the supermesh grid (with its PBC images)
+    size_t nk = (size_t)(G.Nx / 2 + 1) * (G.Ny / 2 + 1) * (G.Nz / 2 + 1);
+    if (cudaMalloc(&G.K, sizeof(T) * 6 * nk) != cudaSuccess) return fail(BM_ENOMEM, "supermesh kernel spectra");
+    void *tx = nullptr, *ty = nullptr, *tz = nullptr;
+    if ((rc = upload_table<double>(&tx, G.Nx, true, s)) || (rc = upload_table<double>(&ty, G.Ny, true, s)) ||
+        (rc = upload_table<double>(&tz, G.Nz, true, s))) return rc;
+    double hm = std::fmax(G.h[0], std::fmax(G.h[1], G.h[2]));
+    std::vector<double> fq(6 * BM_FARQ_PER_COMP);
+    bm_far_coeffs(G.h[0] / hm, G.h[1] / hm, G.h[2] / hm, fq.data());
+    CK(cudaMemcpyAsync(c->farq, fq.data(), sizeof(double) * fq.size(), cudaMemcpyHostToDevice, s));
+    rc = build_kernels_device<T>((T *)G.K, G.nx, G.ny, G.nz, G.Nx, G.Ny, G.Nz, G.h[0], G.h[1], G.h[2], c->farq,
+                                 (const cpx<double> *)tx, (const cpx<double> *)ty, (const cpx<double> *)tz, s, G.pbc);
+    cudaFree(tx); cudaFree(ty); cudaFree(tz);
+    if (rc) return fail(BM_ECUDA, "supermesh kernel build failed (" + std::to_string(rc) + ")");
+    // transfer lists: in per mesh (into the supermesh cells), out per mesh (into the mesh's Hd)
+    const size_t nm = r.mesh_of.size();
+    r.sm_in_ptr.assign(nm, nullptr);
+    r.sm_in_idx.assign(nm, nullptr);
+    r.sm_in_w.assign(nm, nullptr);
+    for (size_t k = 0; k < nm; k++) {
+        const SMMeshXfer &x = g.mesh[k];
+        Mesh &m = c->meshes[r.mesh_of[k]];
+        if ((rc = upload_vec<int>((void **)&r.sm_in_ptr[k], x.in_ptr, s))) return rc;
+        if ((rc = upload_vec<int>((void **)&r.sm_in_idx[k], x.in_idx, s))) return rc;
+        if ((rc = upload_vec<T>(&r.sm_in_w[k], as_type<T>(x.in_w), s))) return rc;
+        if ((rc = upload_vec<int>((void **)&m.out_ptr, x.out_ptr, s))) return rc;
+        if ((rc = upload_vec<int>((void **)&m.out_idx, x.out_idx, s))) return rc;
+        if ((rc = upload_vec<T>(&m.out_w, as_type<T>(x.out_w), s))) return rc;
+    }
+    CK(cudaStreamSynchronize(s));
+    if (c->autotune) {
+        tune_grid_yz<T>(c, G);
+        if ((rc = tune_grid_x<T>(c, G))) return rc;
+    }
+    cudaGetLastError();
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+template <typename T>
 int prepare_ml(bm_ctx *c)
 {
     if (!c->ml) return 0;
+    if (c->ml->sm) return prepare_sm<T>(c);
     MLRun &r = *c->ml;
     MLGeom &g = r.g;
     cudaStream_t s = c->stream;
@@ -896,19 +996,10 @@ int prepare(bm_ctx *c)
     if (c->es_level > 0 && c->ml_mode >= 0)
         return fail(BM_EUNSUPPORTED, "evaluation speedup with a multilayered convolution");
     for (auto &m : c->meshes) {
-        if (!(m.modules & BM_DEMAG) || !(m.pbc[0] || m.pbc[1] || m.pbc[2])) continue;
+        if (!(m.modules & BM_DEMAG) || !(m.pbc[0] || m.pbc[1] || m.pbc[2]) || c->ml_mode == BM_ML_SUPERMESH) continue;
         if (c->ml_mode >= 0) return fail(BM_EUNSUPPORTED, "periodic boundary conditions with a multilayered convolution");
-        // the periodic tensor build evaluates (octant points) x (image terms) tensor values; bound
-        // it so a set-up cannot hold the device for minutes
         const int nc[3] = {m.nx, m.ny, m.nz};
-        double work = 1.0;
-        for (int a = 0; a < 3; a++) {
-            const int X = std::abs(m.pbc[a]);
-            work *= X ? (double)(nc[a] / 2 + 1) * (2.0 * X + 2.0) : (double)nc[a];
-        }
-        if (work > 1e10)
-            return fail(BM_EUNSUPPORTED, "periodic tensor build of " + std::to_string(work) +
-                                             " tensor evaluations is above the limit of 1e10 (fewer images or cells)");
+        if (int rc = pbc_work_check(nc, m.pbc)) return rc;
     }
     CK(cudaSetDevice(c->device));
     // refuse up front, before any allocation, when the meshes cannot fit: the free device memory,
@@ -1408,9 +1499,52 @@ int ml_enqueue_part(bm_ctx *c, int part, int gate, int bi, int *count)
     return 0;
 }
 
+// Supermesh demag: every mesh's M gathered onto the supermesh grid (one accumulating gather per mesh),
+// its x forward transform, the y / z passes with the supermesh kernel, the inverse x transform into
+// the grid's field, and one gather per mesh into its Hd (SDemag::UpdateField, Boris/SDemag.cpp:737-760:
+// transfer_in, Convolute, transfer_out).
+template <typename T>
+int sm_enqueue(bm_ctx *c, int gate, int bi, int *count)
+{
+    MLRun &r = *c->ml;
+    Mesh &G = r.smgrid;
+    cudaStream_t s = c->stream;
+    for (size_t k = 0; k < r.mesh_of.size(); k++) {
+        Mesh &M = c->meshes[r.mesh_of[k]];
+        CKL(launch_ml_gather<T>(B<T>(G, 0), G.n, G.n, B<T>(M, bi), M.n, r.sm_in_ptr[k], r.sm_in_idx[k],
+                                (const T *)r.sm_in_w[k], c->st, gate, s, k > 0), "supermesh transfer in");
+        (*count)++;
+    }
+    StageArgs<T> a = stage_args<T>(c, G);
+    a.mode = BM_MODE_UPDATE;
+    a.gate = gate;
+    a.Min = B<T>(G, 0); a.Mbase = B<T>(G, 0);
+    a.nev = 0;
+    CKL(launch_stage<T>(a, s), "supermesh x forward");
+    (*count)++;
+    if (int rc = enqueue_yz<T>(c, G, gate, count)) return rc;
+    StageArgs<T> h = stage_args<T>(c, G);
+    h.mode = BM_MODE_HEFF;
+    h.modules = BM_DEMAG;
+    h.do_xfwd = 0;
+    h.gate = gate;
+    h.Min = B<T>(G, 0);
+    h.Hout = (T *)G.Hout;
+    CKL(launch_stage<T>(h, s), "supermesh x inverse");
+    (*count)++;
+    for (size_t k = 0; k < r.mesh_of.size(); k++) {
+        Mesh &M = c->meshes[r.mesh_of[k]];
+        CKL(launch_ml_gather<T>((T *)M.Hd, M.n, M.n, (const T *)G.Hout, G.n, M.out_ptr, M.out_idx, (const T *)M.out_w,
+                                c->st, gate, s), "supermesh transfer out");
+        (*count)++;
+    }
+    return 0;
+}
+
 template <typename T>
 int enqueue_fields(bm_ctx *c, int gate, int bi, int *count)
 {
+    if (c->ml && c->ml->sm) return sm_enqueue<T>(c, gate, bi, count);
     if (!c->ml) {
         if (c->batched && c->meshes.size() > 1) return yz_multi<T>(c, gate, count);
         for (auto &m : c->meshes) {
@@ -2261,7 +2395,7 @@ int bm_set_precision(bm_ctx *c, int precision)
 int bm_set_multiconvolution(bm_ctx *c, int mode, const int *n_common)
 {
     if (int rc = check_ctx(c)) return rc;
-    if (mode < BM_ML_OFF || mode > BM_ML_2D_LAYERED) return fail(BM_EINVAL, "multiconvolution mode");
+    if (mode < BM_ML_OFF || mode > BM_ML_SUPERMESH) return fail(BM_EINVAL, "multiconvolution mode");
     if (n_common && (n_common[0] < 1 || n_common[1] < 1 || n_common[2] < 1)) return fail(BM_EINVAL, "n_common must be >= 1");
     if (n_common && (nice_size(n_common[0]) > 4096 || nice_size(n_common[1]) > 4096 || n_common[2] > 32))
         return fail(BM_EUNSUPPORTED, "n_common above the supported FFT size");
@@ -2272,10 +2406,51 @@ int bm_set_multiconvolution(bm_ctx *c, int mode, const int *n_common)
     return 0;
 }
 
+int bm_set_supermesh_cellsize(bm_ctx *c, double hx, double hy, double hz)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (!(hx > 0) || !(hy > 0) || !(hz > 0)) return fail(BM_EINVAL, "supermesh cellsize must be > 0");
+    unprepare(c);
+    c->sm_h[0] = hx; c->sm_h[1] = hy; c->sm_h[2] = hz;
+    return 0;
+}
+
+int bm_set_supermesh_pbc(bm_ctx *c, int x_images, int y_images, int z_images)
+{
+    if (int rc = check_ctx(c)) return rc;
+    const int img[3] = {x_images, y_images, z_images};
+    for (int a = 0; a < 3; a++)
+        if (img[a] > BM_PBC_MAX_IMAGES || img[a] < -BM_PBC_MAX_IMAGES)
+            return fail(BM_EINVAL, "PBC images must be within +-" + std::to_string(BM_PBC_MAX_IMAGES));
+    unprepare(c);
+    // SDemag::Set_PBC: the supermesh convolution and every mesh's stencils (Set_Magnetic_PBC)
+    for (int a = 0; a < 3; a++) c->sm_pbc[a] = img[a];
+    for (auto &m : c->meshes)
+        for (int a = 0; a < 3; a++) m.pbc[a] = img[a];
+    return 0;
+}
+
+int bm_supermesh_info(bm_ctx *c, int *n3, double *h3, double *rect6, long long *nonempty)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (c->ml_mode != BM_ML_SUPERMESH) return fail(BM_ESTATE, "supermesh demag is off");
+    if (int rc = prepare(c)) return rc;
+    if (!c->ml || !c->ml->sm) return fail(BM_ESTATE, "no mesh with demag on the supermesh");
+    const SMGeom &g = c->ml->smg;
+    for (int a = 0; a < 3; a++) {
+        if (n3) n3[a] = g.n[a];
+        if (h3) h3[a] = g.h[a];
+        if (rect6) { rect6[a] = g.rs[a]; rect6[3 + a] = g.re[a]; }
+    }
+    if (nonempty) *nonempty = g.nonempty;
+    return 0;
+}
+
 int bm_ml_info(bm_ctx *c, int *L, int *nc3, int *layer_mesh, int *transfer, double *rects6, int *kinds)
 {
     if (int rc = check_ctx(c)) return rc;
     if (c->ml_mode < 0) return fail(BM_ESTATE, "multilayered convolution is off");
+    if (c->ml_mode == BM_ML_SUPERMESH) return fail(BM_ESTATE, "supermesh demag: see bm_supermesh_info");
     if (int rc = prepare(c)) return rc;
     if (!c->ml) return fail(BM_ESTATE, "no mesh with demag in the multilayered convolution");
     const MLRun &r = *c->ml;
@@ -2296,7 +2471,7 @@ int bm_ml_tile(bm_ctx *c, int *W)
 {
     if (int rc = check_ctx(c)) return rc;
     if (int rc = prepare(c)) return rc;
-    if (!c->ml) return fail(BM_ESTATE, "multilayered convolution is off");
+    if (!c->ml || c->ml->sm) return fail(BM_ESTATE, "multilayered convolution is off");
     if (W) *W = c->ml->W;
     return 0;
 }
@@ -2815,7 +2990,7 @@ int bm_ml_time_kernels(bm_ctx *c, int reps, double *ms6, double *bytes6)
     if (int rc = check_ctx(c)) return rc;
     if (!ms6 || !bytes6 || reps < 1) return fail(BM_EINVAL, "args");
     if (int rc = prepare(c)) return rc;
-    if (!c->ml) return fail(BM_ESTATE, "multilayered convolution is off");
+    if (!c->ml || c->ml->sm) return fail(BM_ESTATE, "multilayered convolution is off");
     cudaSetDevice(c->device);
     return (c->precision == BM_FP64) ? ml_time_T<double>(c, reps, ms6, bytes6) : ml_time_T<float>(c, reps, ms6, bytes6);
 }

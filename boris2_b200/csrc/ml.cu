@@ -27,7 +27,7 @@ __device__ __forceinline__ bool ml_gated_out(const StepState *st, int gate)
 template <typename T>
 __global__ void k_ml_gather(T *__restrict__ dst, long long n_dst, long long dst_plane, const T *__restrict__ src,
                             long long src_plane, const int *__restrict__ ptr, const int *__restrict__ idx,
-                            const T *__restrict__ w, StepState *st, int gate)
+                            const T *__restrict__ w, StepState *st, int gate, int add)
 {
     if (ml_gated_out<T>(st, gate)) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_dst; i += (long long)gridDim.x * blockDim.x) {
@@ -40,6 +40,11 @@ __global__ void k_ml_gather(T *__restrict__ dst, long long n_dst, long long dst_
             v1 += wq * src[e + src_plane];
             v2 += wq * src[e + 2 * src_plane];
         }
+        if (add) {
+            v0 += dst[i];
+            v1 += dst[i + dst_plane];
+            v2 += dst[i + 2 * dst_plane];
+        }
         dst[i] = v0;
         dst[i + dst_plane] = v1;
         dst[i + 2 * dst_plane] = v2;
@@ -48,19 +53,19 @@ __global__ void k_ml_gather(T *__restrict__ dst, long long n_dst, long long dst_
 
 template <typename T>
 int launch_ml_gather(T *dst, long long n_dst, long long dst_plane, const T *src, long long src_plane, const int *ptr,
-                     const int *idx, const T *w, StepState *st, int gate, cudaStream_t s)
+                     const int *idx, const T *w, StepState *st, int gate, cudaStream_t s, int add)
 {
     long long b = (n_dst + 255) / 256;
     if (b > 148 * 16) b = 148 * 16;
     if (b < 1) b = 1;
-    k_ml_gather<T><<<(int)b, 256, 0, s>>>(dst, n_dst, dst_plane, src, src_plane, ptr, idx, w, st, gate);
+    k_ml_gather<T><<<(int)b, 256, 0, s>>>(dst, n_dst, dst_plane, src, src_plane, ptr, idx, w, st, gate, add);
     return (int)cudaGetLastError();
 }
 
 template int launch_ml_gather<float>(float *, long long, long long, const float *, long long, const int *, const int *,
-                                     const float *, StepState *, int, cudaStream_t);
+                                     const float *, StepState *, int, cudaStream_t, int);
 template int launch_ml_gather<double>(double *, long long, long long, const double *, long long, const int *, const int *,
-                                      const double *, StepState *, int, cudaStream_t);
+                                      const double *, StepState *, int, cudaStream_t, int);
 
 // ------------------------------------------------------------------------------ fused z pass
 // Block: W columns from kx0, the pencil pair ky / Ny - ky (ky <= Ny/2), every layer and component.

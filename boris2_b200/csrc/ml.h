@@ -71,6 +71,34 @@ struct MLGeom {
 // N is the project's FFT size 2 * nice(n_common) per axis. Returns 0 or sets err.
 int ml_build_geometry(const std::vector<MLMeshIn> &meshes, int mode, const int *nc_user, MLGeom &g, std::string &err);
 
+// ------------------------------------------------------------------------------ supermesh
+// Supermesh demag (the reference's SDemag with the multilayered convolution off, Boris/SDemag.cpp:
+// 737-760): one convolution on the grid that spans every magnetic mesh, the meshes' M moved onto it
+// and the field moved back by the weighted mesh transfer.
+struct SMMeshXfer {
+    // in: per supermesh cell, (cell of this mesh, weight); weights already carry the normalisation
+    // over every mesh that covers the supermesh cell
+    std::vector<int> in_ptr, in_idx;
+    std::vector<double> in_w;
+    // out: per cell of this mesh, (supermesh cell, weight)
+    std::vector<int> out_ptr, out_idx;
+    std::vector<double> out_w;
+};
+
+struct SMGeom {
+    int n[3] = {1, 1, 1};           // supermesh cells
+    double h[3] = {0, 0, 0};        // supermesh cellsize (the requested one adjusted to divide the rectangle)
+    double rs[3] = {0, 0, 0}, re[3] = {0, 0, 0};   // supermesh rectangle
+    long long nonempty = 0;         // supermesh cells covered by a mesh
+    std::vector<SMMeshXfer> mesh;   // per input mesh
+};
+
+// Supermesh rectangle: the bounding box of the meshes (Rect::operator+=, BorisLib/Types_Rect.h:290);
+// cells: round(size / h_request) per axis, at least 1, and h = size / cells
+// (SuperMesh::UpdateConfiguration, Boris/SuperMeshControl.cpp:22-44); transfer weights of
+// MESHTRANSFERTYPE_WEIGHTED over several input meshes (BorisLib/VEC_MeshTransfer.h:901,1221).
+int sm_build_geometry(const std::vector<MLMeshIn> &meshes, const double h_request[3], SMGeom &g, std::string &err);
+
 // ------------------------------------------------------------------------------ device arguments
 // one unique kernel as the z pass sees it: storage kind, element offset in the kernel buffer,
 // byte offset of its staged tile in shared memory
@@ -120,9 +148,10 @@ template <typename T> int launch_zmid_ml(const MLZArgs<T> &a, cudaStream_t s);
 bool zmid_ml_supported(int Nz);
 
 // dst[c * dst_plane + i] = sum_q w[q] * src[idx[q] + c * src_plane], q in [ptr[i], ptr[i+1])
+// (add != 0: dst += instead of dst =)
 template <typename T>
 int launch_ml_gather(T *dst, long long n_dst, long long dst_plane, const T *src, long long src_plane, const int *ptr,
-                     const int *idx, const T *w, StepState *st, int gate, cudaStream_t s);
+                     const int *idx, const T *w, StepState *st, int gate, cudaStream_t s, int add = 0);
 
 // kernel build: 6 components of one shifted kernel (type T) into K (layout by kind)
 template <typename T>

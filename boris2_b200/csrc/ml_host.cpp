@@ -318,3 +318,90 @@ int ml_build_geometry(const std::vector<MLMeshIn> &meshes, int mode, const int *
     }
     return 0;
 }
+
+// ------------------------------------------------------------------------------ supermesh
+int sm_build_geometry(const std::vector<MLMeshIn> &meshes, const double h_request[3], SMGeom &g, std::string &err)
+{
+    g = SMGeom();
+    const int nm = (int)meshes.size();
+    if (nm < 1) { err = "supermesh: no mesh with demag"; return 1; }
+    for (int a = 0; a < 3; a++)
+        if (!(h_request[a] > 0)) { err = "supermesh: cellsize must be > 0"; return 1; }
+    std::vector<Box> mrect(nm);
+    std::vector<V3> mh(nm);
+    Box u;
+    bool first = true;
+    for (int m = 0; m < nm; m++) {
+        mh[m] = V3(meshes[m].h[0], meshes[m].h[1], meshes[m].h[2]);
+        mrect[m].s = V3(meshes[m].o[0], meshes[m].o[1], meshes[m].o[2]);
+        mrect[m].e = mrect[m].s + V3(mh[m].x * meshes[m].n[0], mh[m].y * meshes[m].n[1], mh[m].z * meshes[m].n[2]);
+        if (first) { u = mrect[m]; first = false; continue; }
+        for (int a = 0; a < 3; a++) {
+            u.s[a] = std::min(u.s[a], mrect[m].s[a]);
+            u.e[a] = std::max(u.e[a], mrect[m].e[a]);
+        }
+    }
+    V3 sz = u.size();
+    V3 hs;
+    for (int a = 0; a < 3; a++) {
+        long long c = std::llround(sz[a] / h_request[a]);
+        if (c < 1) c = 1;
+        if (c > (1 << 20)) { err = "supermesh: more than 2^20 cells along an axis"; return 1; }
+        g.n[a] = (int)c;
+        hs[a] = sz[a] / g.n[a];
+        g.h[a] = hs[a];
+        g.rs[a] = u.s[a];
+        g.re[a] = u.e[a];
+    }
+    const long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    g.mesh.assign(nm, SMMeshXfer());
+    for (int m = 0; m < nm; m++) g.mesh[m].in_ptr.assign(ncell + 1, 0);
+    // in: every supermesh cell gathers from every mesh it overlaps; one normalisation over all of them
+    std::vector<std::vector<int>> idx(nm);
+    std::vector<std::vector<double>> w(nm);
+    for (long long c = 0; c < ncell; c++) {
+        int i = (int)(c % g.n[0]), j = (int)((c / g.n[0]) % g.n[1]), k = (int)(c / ((long long)g.n[0] * g.n[1]));
+        Box cell;
+        cell.s = u.s + V3(hs.x * i, hs.y * j, hs.z * k);
+        cell.e = cell.s + hs;
+        double tot = 0.0, cov = 0.0;
+        std::vector<size_t> start(nm);
+        for (int m = 0; m < nm; m++) start[m] = idx[m].size();
+        for (int m = 0; m < nm; m++) {
+            Box ri;
+            if (intersection(mrect[m], cell, ri) && !is_plane(ri) && !is_point(ri)) {
+                V3 si = ri.size(), sc = cell.size();
+                cov += (si.x / sc.x) * (si.y / sc.y) * (si.z / sc.z);
+                tot += recip_weights(cell, meshes[m].n, mh[m], mrect[m].s, idx[m], w[m]);
+            }
+        }
+        if (cov > 0) g.nonempty++;
+        for (int m = 0; m < nm; m++) {
+            if (tot > 0)
+                for (size_t q = start[m]; q < w[m].size(); q++) w[m][q] *= cov / tot;
+            g.mesh[m].in_ptr[c + 1] = (int)idx[m].size();
+        }
+    }
+    for (int m = 0; m < nm; m++) { g.mesh[m].in_idx = idx[m]; g.mesh[m].in_w = w[m]; }
+    // out: every mesh cell gathers from the supermesh cells it overlaps
+    for (int m = 0; m < nm; m++) {
+        SMMeshXfer &x = g.mesh[m];
+        const int n = meshes[m].n[0] * meshes[m].n[1] * meshes[m].n[2];
+        x.out_ptr.assign(n + 1, 0);
+        for (int c = 0; c < n; c++) {
+            int i = c % meshes[m].n[0], j = (c / meshes[m].n[0]) % meshes[m].n[1], k = c / (meshes[m].n[0] * meshes[m].n[1]);
+            Box cell;
+            cell.s = mrect[m].s + V3(mh[m].x * i, mh[m].y * j, mh[m].z * k);
+            cell.e = cell.s + mh[m];
+            std::vector<int> oi;
+            std::vector<double> ow;
+            double tot = recip_weights(cell, g.n, hs, u.s, oi, ow);
+            for (size_t q = 0; q < oi.size(); q++) {
+                x.out_idx.push_back(oi[q]);
+                x.out_w.push_back(tot > 0 ? ow[q] * (1.0 / tot) : ow[q]);
+            }
+            x.out_ptr[c + 1] = (int)x.out_idx.size();
+        }
+    }
+    return 0;
+}

@@ -88,7 +88,8 @@ int bm_set_modules(bm_ctx *ctx, int mesh, int modules);
  *   - exchange / iDMI: a cell on a periodic face takes the cell on the opposite face as its missing
  *     neighbour, times the sign of images (a negative count wraps with -1, as the reference's
  *     differential operators do, BorisLib/VEC_VC_Del.h:141, BorisLib/VEC_VC_Grad.h:139).
- * Not combined with bm_set_multiconvolution (BM_EUNSUPPORTED at set-up). */
+ * Not combined with the multilayered modes of bm_set_multiconvolution (BM_EUNSUPPORTED at set-up);
+ * with the supermesh mode the supermesh convolution takes its images from bm_set_supermesh_pbc. */
 #define BM_PBC_MAX_IMAGES 1000
 int bm_set_pbc(bm_ctx *ctx, int mesh, int x_images, int y_images, int z_images);
 int bm_get_pbc(bm_ctx *ctx, int mesh, int *images3);
@@ -146,7 +147,28 @@ int bm_set_precision(bm_ctx *ctx, int precision);
 #define BM_ML_3D 0
 #define BM_ML_2D 1
 #define BM_ML_2D_LAYERED 2
+#define BM_ML_SUPERMESH 3   /* supermesh demag, below (n_common unused) */
 int bm_set_multiconvolution(bm_ctx *ctx, int mode, const int *n_common);
+
+/* Supermesh demag (mode BM_ML_SUPERMESH): the reference's SDemag module with the multilayered
+ * convolution off (Boris/SDemag.cpp:737-760, `multiconvolution 0` with the supermesh demag module
+ * added). One demag convolution runs on a grid over the bounding box of every mesh with BM_DEMAG:
+ * the meshes' M are moved onto it by the weighted mesh transfer (a supermesh cell takes the
+ * covered-volume ratio times the reciprocal-distance weights over every mesh it overlaps,
+ * BorisLib/VEC_MeshTransfer.h:901), convolved with the supermesh's own kernel, and the field is
+ * moved back into every mesh (VEC_MeshTransfer.h:1221). The grid has round(size / h) cells per axis
+ * (at least 1) and cellsize size / cells (SuperMesh::UpdateConfiguration,
+ * Boris/SuperMeshControl.cpp:22-44). As in the reference there is no evaluation speedup for it
+ * (bm_set_evalspeedup is refused) and it is not combined with bm_set_batched or the adjoint.
+ *   bm_set_supermesh_cellsize  requested cellsize (SuperMesh::SetFMSMeshCellsize, `fmscellsize`,
+ *                              Boris/SuperMeshSettings.cpp:79; default 5 nm, Boris/SuperMesh.h:117)
+ *   bm_set_supermesh_pbc       PBC images of the supermesh convolution, also set as every mesh's
+ *                              stencil PBC (SDemag::Set_PBC / Set_Magnetic_PBC, Boris/SDemag.cpp:404)
+ *   bm_supermesh_info          cells, cellsize, rectangle (start, end) and the count of supermesh
+ *                              cells covered by a mesh (the reference's non_empty_cells) */
+int bm_set_supermesh_cellsize(bm_ctx *ctx, double hx, double hy, double hz);
+int bm_set_supermesh_pbc(bm_ctx *ctx, int x_images, int y_images, int z_images);
+int bm_supermesh_info(bm_ctx *ctx, int *n3, double *h3, double *rect6, long long *nonempty);
 
 /* Geometry of the multilayered convolution once prepared (after a run or field call, or
  * bm_prepare): layer count, n_common, and per layer the mesh, whether it is moved by mesh

@@ -1149,6 +1149,165 @@ int orc_ml_transfer(orc_ml *s, int l, const double *M, double *Mc, const double 
     return 0;
 }
 
+/* ------------------------------------------------------------------ supermesh demag */
+
+/* SDemag with the multilayered convolution off (Boris/SDemag.cpp:737-760): M of every mesh moved onto
+ * the ferromagnetic supermesh by the weighted mesh transfer, one demag convolution there (with the
+ * supermesh's PBC images), the field moved back into every mesh.
+ *   rectangle, cells  SuperMesh::UpdateConfiguration (Boris/SuperMeshControl.cpp:22-44): the bounding
+ *                     box of the meshes (Rect::operator+=, BorisLib/Types_Rect.h:290), n = round(size /
+ *                     h_request) per axis (at least 1), h = size / n
+ *   transfer in       initialize_transfer_in_weighted over every input mesh (BorisLib/VEC_MeshTransfer.h:
+ *                     901): per supermesh cell the covered-volume ratios and reciprocal-distance weights
+ *                     summed over every overlapping mesh, then one normalisation
+ *   transfer out      initialize_transfer_out (VEC_MeshTransfer.h:1221), reciprocal-distance weights
+ *   non-empty cells   supermesh cells that a mesh covers (VEC::get_nonempty_cells after transfer_in,
+ *                     SDemag.cpp:574-576, for a magnetisation without zero cells) */
+struct orc_sm {
+    int nmesh;
+    int (*mn)[3];
+    size_t *moff;
+    int n[3];
+    d3 h;
+    rect3 rect;
+    long nonempty;
+    wlist **tin;      /* per mesh, per supermesh cell */
+    wlist **tout;     /* per mesh, per mesh cell */
+    orc_demag *dm;
+};
+
+orc_sm *orc_sm_create(int nmesh, const int *n3, const double *h3, const double *o3, const double *h_request,
+                      const int *pbc)
+{
+    if (nmesh < 1) return NULL;
+    orc_sm *s = (orc_sm *)calloc(1, sizeof(orc_sm));
+    s->nmesh = nmesh;
+    s->mn = (int (*)[3])calloc(nmesh, sizeof(int[3]));
+    s->moff = (size_t *)calloc(nmesh + 1, sizeof(size_t));
+    d3 *mh = (d3 *)calloc(nmesh, sizeof(d3));
+    rect3 *mr = (rect3 *)calloc(nmesh, sizeof(rect3));
+    for (int m = 0; m < nmesh; m++) {
+        for (int a = 0; a < 3; a++) s->mn[m][a] = n3[3 * m + a];
+        mh[m] = d3m(h3[3 * m], h3[3 * m + 1], h3[3 * m + 2]);
+        mr[m].s = d3m(o3[3 * m], o3[3 * m + 1], o3[3 * m + 2]);
+        mr[m].e = d3add(mr[m].s, d3m(mh[m].x * n3[3 * m], mh[m].y * n3[3 * m + 1], mh[m].z * n3[3 * m + 2]));
+        s->moff[m + 1] = s->moff[m] + (size_t)n3[3 * m] * n3[3 * m + 1] * n3[3 * m + 2];
+        if (m == 0) s->rect = mr[0];
+        else {
+            if (mr[m].s.x < s->rect.s.x) s->rect.s.x = mr[m].s.x;
+            if (mr[m].s.y < s->rect.s.y) s->rect.s.y = mr[m].s.y;
+            if (mr[m].s.z < s->rect.s.z) s->rect.s.z = mr[m].s.z;
+            if (mr[m].e.x > s->rect.e.x) s->rect.e.x = mr[m].e.x;
+            if (mr[m].e.y > s->rect.e.y) s->rect.e.y = mr[m].e.y;
+            if (mr[m].e.z > s->rect.e.z) s->rect.e.z = mr[m].e.z;
+        }
+    }
+    d3 sz = rsize(s->rect);
+    double szv[3] = {sz.x, sz.y, sz.z}, hv[3];
+    for (int a = 0; a < 3; a++) {
+        double c = round(szv[a] / h_request[a]);
+        s->n[a] = c < 1 ? 1 : (int)c;
+        hv[a] = szv[a] / s->n[a];
+    }
+    s->h = d3m(hv[0], hv[1], hv[2]);
+    size_t ncell = (size_t)s->n[0] * s->n[1] * s->n[2];
+    s->tin = (wlist **)calloc(nmesh, sizeof(wlist *));
+    s->tout = (wlist **)calloc(nmesh, sizeof(wlist *));
+    for (int m = 0; m < nmesh; m++) s->tin[m] = (wlist *)calloc(ncell, sizeof(wlist));
+    for (size_t c = 0; c < ncell; c++) {
+        int ii = (int)(c % s->n[0]), jj = (int)((c / s->n[0]) % s->n[1]), kk = (int)(c / ((size_t)s->n[0] * s->n[1]));
+        rect3 rc;
+        rc.s = d3add(s->rect.s, d3m(s->h.x * ii, s->h.y * jj, s->h.z * kk));
+        rc.e = d3add(rc.s, s->h);
+        double tot = 0.0, cov = 0.0;
+        for (int m = 0; m < nmesh; m++) {
+            rect3 ri;
+            if (rect_intersection(mr[m], rc, &ri) && !rect_isplane(ri) && !rect_ispoint(ri)) {
+                d3 si = rsize(ri), sc = rsize(rc);
+                cov += (si.x / sc.x) * (si.y / sc.y) * (si.z / sc.z);
+                tot += recip_weights(&s->tin[m][c], rc, s->mn[m], mh[m], mr[m].s);
+            }
+        }
+        if (cov > 0) s->nonempty++;
+        if (tot > 0)
+            for (int m = 0; m < nmesh; m++)
+                for (int q = 0; q < s->tin[m][c].n; q++) s->tin[m][c].w[q] *= cov / tot;
+    }
+    for (int m = 0; m < nmesh; m++) {
+        size_t n = s->moff[m + 1] - s->moff[m];
+        s->tout[m] = (wlist *)calloc(n, sizeof(wlist));
+        for (size_t c = 0; c < n; c++) {
+            int ii = (int)(c % s->mn[m][0]), jj = (int)((c / s->mn[m][0]) % s->mn[m][1]);
+            int kk = (int)(c / ((size_t)s->mn[m][0] * s->mn[m][1]));
+            rect3 rc;
+            rc.s = d3add(mr[m].s, d3m(mh[m].x * ii, mh[m].y * jj, mh[m].z * kk));
+            rc.e = d3add(rc.s, mh[m]);
+            double tot = recip_weights(&s->tout[m][c], rc, s->n, s->h, s->rect.s);
+            if (tot > 0) for (int q = 0; q < s->tout[m][c].n; q++) s->tout[m][c].w[q] *= 1.0 / tot;
+        }
+    }
+    s->dm = orc_demag_create_pbc(s->n[0], s->n[1], s->n[2], s->h.x, s->h.y, s->h.z, pbc);
+    free(mh); free(mr);
+    return s;
+}
+
+void orc_sm_destroy(orc_sm *s)
+{
+    if (!s) return;
+    size_t ncell = (size_t)s->n[0] * s->n[1] * s->n[2];
+    for (int m = 0; m < s->nmesh; m++) {
+        for (size_t c = 0; c < ncell; c++) { free(s->tin[m][c].idx); free(s->tin[m][c].w); }
+        size_t n = s->moff[m + 1] - s->moff[m];
+        for (size_t c = 0; c < n; c++) { free(s->tout[m][c].idx); free(s->tout[m][c].w); }
+        free(s->tin[m]); free(s->tout[m]);
+    }
+    free(s->tin); free(s->tout); free(s->mn); free(s->moff);
+    orc_demag_destroy(s->dm);
+    free(s);
+}
+
+int orc_sm_info(orc_sm *s, int *n3, double *h3, double *rect6, long *nonempty)
+{
+    for (int a = 0; a < 3; a++) {
+        if (n3) n3[a] = s->n[a];
+    }
+    if (h3) { h3[0] = s->h.x; h3[1] = s->h.y; h3[2] = s->h.z; }
+    if (rect6) {
+        rect6[0] = s->rect.s.x; rect6[1] = s->rect.s.y; rect6[2] = s->rect.s.z;
+        rect6[3] = s->rect.e.x; rect6[4] = s->rect.e.y; rect6[5] = s->rect.e.z;
+    }
+    if (nonempty) *nonempty = s->nonempty;
+    return 0;
+}
+
+/* H_demag of every mesh (AoS, meshes concatenated) from M of every mesh; returns the reference's
+ * supermesh energy density -mu0 / (2 non_empty_cells) sum_supermesh M . H */
+double orc_sm_eval(orc_sm *s, const double *M, double *H)
+{
+    size_t ncell = (size_t)s->n[0] * s->n[1] * s->n[2];
+    double *Ms = (double *)calloc(3 * ncell, sizeof(double));
+    double *Hs = (double *)calloc(3 * ncell, sizeof(double));
+    for (int m = 0; m < s->nmesh; m++) {
+        const double *Mm = M + 3 * s->moff[m];
+        for (size_t c = 0; c < ncell; c++)
+            for (int q = 0; q < s->tin[m][c].n; q++)
+                for (int a = 0; a < 3; a++) Ms[3 * c + a] += Mm[3 * (size_t)s->tin[m][c].idx[q] + a] * s->tin[m][c].w[q];
+    }
+    double dot = orc_demag_apply(s->dm, Ms, Hs, 0);
+    for (int m = 0; m < s->nmesh; m++) {
+        double *Hm = H + 3 * s->moff[m];
+        size_t n = s->moff[m + 1] - s->moff[m];
+        for (size_t c = 0; c < n; c++) {
+            double v[3] = {0, 0, 0};
+            for (int q = 0; q < s->tout[m][c].n; q++)
+                for (int a = 0; a < 3; a++) v[a] += Hs[3 * (size_t)s->tout[m][c].idx[q] + a] * s->tout[m][c].w[q];
+            for (int a = 0; a < 3; a++) Hm[3 * c + a] = v[a];
+        }
+    }
+    free(Ms); free(Hs);
+    return s->nonempty ? -ORC_MU0 * dot / (2.0 * (double)s->nonempty) : 0.0;
+}
+
 /* ------------------------------------------------------------------ field terms */
 
 static double ms_at(const double *Ms_cell, size_t i) { return Ms_cell[i]; }
@@ -1283,6 +1442,7 @@ struct orc_solver {
     int nmesh;
     orc_mesh *m;
     orc_ml *ml;          /* multilayered convolution over the meshes with demag, or NULL */
+    orc_sm *sm;          /* supermesh demag over the meshes with demag, or NULL */
     int *ml_mesh;        /* solver mesh of each multilayer mesh */
     int ml_nmesh;
     double *ml_M, *ml_H; /* concatenated M and H_demag of the multilayer meshes */
@@ -1360,9 +1520,39 @@ int orc_solver_set_multilayer(orc_solver *s, const double *o3, int mode, const i
     return s->ml ? 0 : 2;
 }
 
+/* Replace the per-mesh demag of every mesh with ORC_DEMAG by one supermesh convolution (SDemag with
+ * the multilayered convolution off); origins give the meshes' positions. */
+int orc_solver_set_supermesh(orc_solver *s, const double *o3, const double *h_request, const int *pbc)
+{
+    int cnt = 0;
+    for (int q = 0; q < s->nmesh; q++) if (s->m[q].d.modules & ORC_DEMAG) cnt++;
+    if (!cnt || s->ml || s->sm) return 1;
+    int *n3 = (int *)malloc(sizeof(int) * 3 * cnt);
+    double *h3 = (double *)malloc(sizeof(double) * 3 * cnt), *oo = (double *)malloc(sizeof(double) * 3 * cnt);
+    s->ml_mesh = (int *)malloc(sizeof(int) * cnt);
+    size_t tot = 0;
+    int k = 0;
+    for (int q = 0; q < s->nmesh; q++) {
+        const orc_mesh_desc *d = &s->m[q].d;
+        if (!(d->modules & ORC_DEMAG)) continue;
+        n3[3 * k] = d->nx; n3[3 * k + 1] = d->ny; n3[3 * k + 2] = d->nz;
+        h3[3 * k] = d->hx; h3[3 * k + 1] = d->hy; h3[3 * k + 2] = d->hz;
+        for (int a = 0; a < 3; a++) oo[3 * k + a] = o3[3 * q + a];
+        s->ml_mesh[k++] = q;
+        tot += (size_t)s->m[q].n;
+    }
+    s->ml_nmesh = cnt;
+    s->sm = orc_sm_create(cnt, n3, h3, oo, h_request, pbc);
+    s->ml_M = (double *)calloc(3 * tot, sizeof(double));
+    s->ml_H = (double *)calloc(3 * tot, sizeof(double));
+    free(n3); free(h3); free(oo);
+    return s->sm ? 0 : 2;
+}
+
 void orc_solver_destroy(orc_solver *s)
 {
     if (!s) return;
+    if (s->sm) { orc_sm_destroy(s->sm); free(s->ml_mesh); free(s->ml_M); free(s->ml_H); }
     if (s->ml) { orc_ml_destroy(s->ml); free(s->ml_mesh); free(s->ml_M); free(s->ml_H); }
     for (int q = 0; q < s->nmesh; q++) {
         orc_mesh *m = &s->m[q];
@@ -1414,7 +1604,8 @@ static void update_ml(orc_solver *s)
         memcpy(s->ml_M + 3 * off, m->M, sizeof(double) * 3 * m->n);
         off += (size_t)m->n;
     }
-    orc_ml_eval(s->ml, s->ml_M, s->ml_H);
+    if (s->sm) orc_sm_eval(s->sm, s->ml_M, s->ml_H);
+    else orc_ml_eval(s->ml, s->ml_M, s->ml_H);
 }
 
 static void update_fields(orc_solver *s, orc_mesh *m)
@@ -1430,7 +1621,7 @@ static void update_fields(orc_solver *s, orc_mesh *m)
         if (d->modules & ORC_ANIUNI) orc_field_aniuni(m->n, m->M, m->Ms, m->K1, d->K2, d->ea, m->H);
         return;
     }
-    if ((d->modules & ORC_DEMAG) && s->ml) {
+    if ((d->modules & ORC_DEMAG) && (s->ml || s->sm)) {
         size_t off = 0;
         for (int k = 0; k < s->ml_nmesh; k++) {
             orc_mesh *mk = &s->m[s->ml_mesh[k]];
@@ -1461,14 +1652,14 @@ static void update_fields(orc_solver *s, orc_mesh *m)
 
 static void update_all_fields(orc_solver *s)
 {
-    if (s->ml) update_ml(s);
+    if (s->ml || s->sm) update_ml(s);
     for (int q = 0; q < s->nmesh; q++) update_fields(s, &s->m[q]);
     s->evals++;
 }
 
 int orc_solver_set_field_hook(orc_solver *s, int q, orc_field_fn fn, void *user)
 {
-    if (q < 0 || q >= s->nmesh || s->ml || s->es_level) return 1;
+    if (q < 0 || q >= s->nmesh || s->ml || s->sm || s->es_level) return 1;
     s->m[q].hook = fn;
     s->m[q].hook_user = user;
     return 0;
@@ -1476,7 +1667,7 @@ int orc_solver_set_field_hook(orc_solver *s, int q, orc_field_fn fn, void *user)
 
 int orc_compute_heff(orc_solver *s, int q, double *H)
 {
-    if (s->ml) update_ml(s);
+    if (s->ml || s->sm) update_ml(s);
     update_fields(s, &s->m[q]);
     memcpy(H, s->m[q].H, sizeof(double) * 3 * s->m[q].n);
     return 0;
@@ -1605,7 +1796,7 @@ static void es_prepare_dp(orc_solver *s, int eval)
 
 int orc_solver_set_evalspeedup(orc_solver *s, int level)
 {
-    if (level < 0 || level > 6 || s->ml) return 1;
+    if (level < 0 || level > 6 || s->ml || s->sm) return 1;
     s->es_level = level;
     s->es_saved = 0;
     s->es_available = 1;

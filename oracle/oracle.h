@@ -125,6 +125,19 @@ int orc_ml_eval(orc_ml *s, const double *M, double *H);
 int orc_ml_transfer(orc_ml *s, int layer, const double *M, double *Mc, const double *Hc, double *Hmesh);
 void orc_ml_destroy(orc_ml *s);
 
+/* ---- supermesh demag (SDemag with the multilayered convolution off) ----
+ * meshes: n3, h3, o3 (3 per mesh); h_request: requested supermesh cellsize; pbc: images of the
+ * supermesh convolution (NULL: none) */
+typedef struct orc_sm orc_sm;
+orc_sm *orc_sm_create(int nmesh, const int *n3, const double *h3, const double *o3, const double *h_request,
+                      const int *pbc);
+int orc_sm_info(orc_sm *s, int *n3, double *h3, double *rect6, long *nonempty);
+/* H (meshes concatenated, AoS) from M; returns the supermesh energy density */
+double orc_sm_eval(orc_sm *s, const double *M, double *H);
+void orc_sm_destroy(orc_sm *s);
+/* one supermesh convolution replaces the per-mesh demag of every mesh with ORC_DEMAG */
+int orc_solver_set_supermesh(orc_solver *s, const double *o3, const double *h_request, const int *pbc);
+
 /* ---- discrete adjoint of RK4 (FP64) ----
  * One mesh, modules demag / exchange / uniaxial anisotropy (K2 = 0) / Zeeman (piecewise-constant
  * samples, the sample at each step's start time), per-cell Ms and K1 maps; initial state Ms * m0;

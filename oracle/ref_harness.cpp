@@ -32,6 +32,11 @@
  *                      Boris/ConvolutionData.cpp:100) as Demag::Initialize does (Boris/Demag.cpp:111),
  *                      the stencils on a VEC_VC with set_pbc (BorisLib/VEC_VC_flags.h:890), and
  *                      DemagTFunc::SelfDemag_PBC (Boris/DemagTFunc_Self.cpp:57)
+ *   ref_sm_*           the supermesh demag of SDemag with the multilayered convolution off: the supermesh
+ *                      rectangle and cells of SuperMesh::UpdateConfiguration (Boris/SuperMeshControl.cpp:
+ *                      22-44), sm_Vals with Initialize_MeshTransfer(M of every mesh, Heff of every mesh,
+ *                      MESHTRANSFERTYPE_WEIGHTED), transfer_in, Convolute, transfer_out and the energy of
+ *                      SDemag::UpdateField (Boris/SDemag.cpp:566-576,737-760)
  *   ref_ovf2_read      OVF2::Read_OVF2_VEC                  (Boris/OVF2_Handlers.cpp:364)
  *   ref_ovf2_write     OVF2::Write_OVF2_VEC                 (Boris/OVF2_Handlers.cpp:701)
  *   ref_ovf2_load      the loadovf2mag command's data path (Boris/Commands.cpp:5025): read,
@@ -449,6 +454,96 @@ int ref_selfdemag_pbc(double hx, double hy, double hz, int nx, int ny, int nz, c
     DBL3 s = dtf.SelfDemag_PBC(DBL3(hx, hy, hz), DBL3(nx, ny, nz), INT3(pbc[0], pbc[1], pbc[2]));
     out3[0] = s.x; out3[1] = s.y; out3[2] = s.z;
     return 0;
+}
+
+/* ---- supermesh demag ---- */
+struct ref_sm_s {
+    std::vector<VEC<DBL3> *> M, Heff;
+    VEC<DBL3> sm_Vals;
+    OracleDemag *od = nullptr;
+    SZ3 n_fm;
+    DBL3 h_fm;
+    Rect rect;
+    int non_empty = 0;
+    std::vector<int> ncell;
+};
+
+void ref_sm_destroy(void *h)
+{
+    ref_sm_s *s = (ref_sm_s *)h;
+    if (!s) return;
+    for (auto p : s->M) delete p;
+    for (auto p : s->Heff) delete p;
+    delete s->od;
+    delete s;
+}
+
+void *ref_sm_create(int nmesh, const int *n3, const double *h3, const double *o3, const double *h_request, const int *pbc)
+{
+    ref_sm_s *s = new ref_sm_s();
+    Rect sMeshRect_fm;
+    for (int m = 0; m < nmesh; m++) {
+        DBL3 h(h3[3 * m], h3[3 * m + 1], h3[3 * m + 2]);
+        DBL3 o(o3[3 * m], o3[3 * m + 1], o3[3 * m + 2]);
+        Rect r(o, o + (h & DBL3(n3[3 * m], n3[3 * m + 1], n3[3 * m + 2])));
+        VEC<DBL3> *M = new VEC<DBL3>(), *H = new VEC<DBL3>();
+        M->resize(h, r);
+        H->resize(h, r);
+        s->M.push_back(M);
+        s->Heff.push_back(H);
+        s->ncell.push_back(n3[3 * m] * n3[3 * m + 1] * n3[3 * m + 2]);
+        sMeshRect_fm += r;
+    }
+    /* SuperMesh::UpdateConfiguration (SuperMeshControl.cpp:40-44) */
+    DBL3 h_fm(h_request[0], h_request[1], h_request[2]);
+    s->n_fm = round(sMeshRect_fm / h_fm);
+    if (s->n_fm.x == 0) s->n_fm.x = 1;
+    if (s->n_fm.y == 0) s->n_fm.y = 1;
+    if (s->n_fm.z == 0) s->n_fm.z = 1;
+    if (!sMeshRect_fm.IsNull()) h_fm = sMeshRect_fm / s->n_fm;
+    s->h_fm = h_fm;
+    s->rect = sMeshRect_fm;
+    /* SDemag::UpdateConfiguration / Initialize / Initialize_Mesh_Transfer (SDemag.cpp:451-454,566-576,659-661) */
+    s->od = new OracleDemag(INT3(s->n_fm.x, s->n_fm.y, s->n_fm.z), h_fm,
+                            pbc ? INT3(pbc[0], pbc[1], pbc[2]) : INT3());
+    if (s->od->create_failed() || s->od->calc()) { ref_sm_destroy(s); return nullptr; }
+    if (!s->sm_Vals.resize(h_fm, sMeshRect_fm)) { ref_sm_destroy(s); return nullptr; }
+    if (!s->sm_Vals.Initialize_MeshTransfer(s->M, s->Heff, MESHTRANSFERTYPE_WEIGHTED)) { ref_sm_destroy(s); return nullptr; }
+    return s;
+}
+
+int ref_sm_info(void *h, int *n3, double *h3, double *rect6)
+{
+    ref_sm_s *s = (ref_sm_s *)h;
+    n3[0] = s->n_fm.x; n3[1] = s->n_fm.y; n3[2] = s->n_fm.z;
+    h3[0] = s->h_fm.x; h3[1] = s->h_fm.y; h3[2] = s->h_fm.z;
+    rect6[0] = s->rect.s.x; rect6[1] = s->rect.s.y; rect6[2] = s->rect.s.z;
+    rect6[3] = s->rect.e.x; rect6[4] = s->rect.e.y; rect6[5] = s->rect.e.z;
+    return 0;
+}
+
+/* H (meshes concatenated, AoS, overwritten) from M; returns the energy density of SDemag::UpdateField
+ * with non_empty_cells counted after the first transfer in (SDemag.cpp:573-576) */
+double ref_sm_eval(void *h, const double *M, double *H)
+{
+    ref_sm_s *s = (ref_sm_s *)h;
+    size_t off = 0;
+    for (size_t m = 0; m < s->M.size(); m++) {
+        memcpy(s->M[m]->data(), M + 3 * off, sizeof(double) * 3 * s->ncell[m]);
+        s->Heff[m]->set(DBL3());
+        off += s->ncell[m];
+    }
+    s->sm_Vals.transfer_in();
+    if (!s->non_empty) s->non_empty = s->sm_Vals.get_nonempty_cells();
+    double energy = s->od->convolute(s->sm_Vals, s->sm_Vals);
+    energy *= -MU0 / (2 * s->non_empty);
+    s->sm_Vals.transfer_out();
+    off = 0;
+    for (size_t m = 0; m < s->M.size(); m++) {
+        memcpy(H + 3 * off, s->Heff[m]->data(), sizeof(double) * 3 * s->ncell[m]);
+        off += s->ncell[m];
+    }
+    return energy;
 }
 
 /* Shifted real-space tensors D = -N on the N grid (AoS, 3 doubles per point).

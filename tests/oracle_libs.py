@@ -113,6 +113,13 @@ def oracle():
         L.orc_demag_create_pbc.argtypes = [I, I, I, D, D, D, IP]
         L.orc_field_exchange_pbc.argtypes = [I, I, I, D, D, D, DP, D, DP, IP, DP]
         L.orc_field_idmi_pbc.argtypes = [I, I, I, D, D, D, DP, D, D, DP, IP, DP]
+        L.orc_sm_create.restype = P
+        L.orc_sm_create.argtypes = [I, IP, DP, DP, DP, IP]
+        L.orc_sm_info.argtypes = [P, IP, DP, DP, ctypes.POINTER(ctypes.c_long)]
+        L.orc_sm_eval.restype = D
+        L.orc_sm_eval.argtypes = [P, DP, DP]
+        L.orc_sm_destroy.argtypes = [P]
+        L.orc_solver_set_supermesh.argtypes = [P, DP, DP, IP]
         _orc = L
     return _orc
 
@@ -207,6 +214,12 @@ def reference():
         L.ref_hdemag_pbc.argtypes = [I, I, I, D, D, D, IP, DP, DP, DP]
         L.ref_stencil_pbc.argtypes = [I, I, I, D, D, D, IP, I, DP, DP, DP, DP, DP]
         L.ref_selfdemag_pbc.argtypes = [D, D, D, I, I, I, IP, DP]
+        L.ref_sm_create.restype = P
+        L.ref_sm_create.argtypes = [I, IP, DP, DP, DP, IP]
+        L.ref_sm_info.argtypes = [P, IP, DP, DP]
+        L.ref_sm_eval.restype = D
+        L.ref_sm_eval.argtypes = [P, DP, DP]
+        L.ref_sm_destroy.argtypes = [P]
         L.ref_ml_create.restype = P
         L.ref_ml_create.argtypes = [I, IP, DP, DP, I, IP]
         L.ref_ml_info.argtypes = [P, IP, IP, IP, IP, DP, IP]
@@ -406,6 +419,50 @@ def ref_stencil_pbc(M, n, h, pbc, A, Ms, D=0.0, idmi=False):
     return H.reshape(-1, 3)
 
 
+class SuperMesh:
+    """The supermesh demag of the oracle (which="oracle") or of the reference build (which="reference").
+    meshes: list of (n, h, origin); h_request: supermesh cellsize asked for; pbc: its images."""
+
+    def __init__(self, meshes, h_request=(5e-9, 5e-9, 5e-9), pbc=(0, 0, 0), which="oracle"):
+        self.lib = oracle() if which == "oracle" else reference()
+        self.pre = "orc_" if which == "oracle" else "ref_"
+        n3 = np.array([m[0] for m in meshes], dtype=np.int32).reshape(-1)
+        h3 = np.array([m[1] for m in meshes], dtype=np.float64).reshape(-1)
+        o3 = np.array([m[2] for m in meshes], dtype=np.float64).reshape(-1)
+        hr = np.array(h_request, dtype=np.float64)
+        self.h = getattr(self.lib, self.pre + "sm_create")(len(meshes), ip(n3), dp(h3), dp(o3), dp(hr), _i3(pbc))
+        assert self.h
+        self.ncell = [int(np.prod(m[0])) for m in meshes]
+
+    def info(self):
+        n = np.zeros(3, np.int32)
+        h = np.zeros(3)
+        r = np.zeros(6)
+        out = {}
+        if self.pre == "orc_":
+            ne = ctypes.c_long(0)
+            self.lib.orc_sm_info(P(self.h), ip(n), dp(h), dp(r), ctypes.byref(ne))
+            out["nonempty"] = ne.value
+        else:
+            self.lib.ref_sm_info(P(self.h), ip(n), dp(h), dp(r))
+        out.update({"n": tuple(int(v) for v in n), "h": tuple(h), "rect": r.reshape(2, 3)})
+        return out
+
+    def eval(self, M):
+        Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
+        H = np.zeros_like(Mf)
+        e = getattr(self.lib, self.pre + "sm_eval")(P(self.h), dp(Mf), dp(H))
+        return H.reshape(-1, 3), e
+
+    def close(self):
+        if self.h:
+            getattr(self.lib, self.pre + "sm_destroy")(P(self.h))
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 def ref_hdemag(M, n, h):
     R = reference()
     Mf = np.ascontiguousarray(np.asarray(M, dtype=np.float64).reshape(-1))
@@ -462,6 +519,13 @@ class OracleSolver:
 
     def evalspeedup(self, level):
         assert oracle().orc_solver_set_evalspeedup(P(self.h), int(level)) == 0
+
+    def supermesh(self, origins, h_request=(5e-9, 5e-9, 5e-9), pbc=(0, 0, 0)):
+        """Demag of all meshes with the demag bit as one supermesh convolution."""
+        o3 = np.ascontiguousarray(np.asarray(origins, dtype=np.float64).reshape(-1))
+        hr = np.array(h_request, dtype=np.float64)
+        self._keep += [o3, hr]
+        assert oracle().orc_solver_set_supermesh(P(self.h), dp(o3), dp(hr), _i3(pbc)) == 0
 
     def use_reference_fields(self, mesh=0):
         """Take this mesh's demag and exchange / iDMI terms from the reference's own compiled code
