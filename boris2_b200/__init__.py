@@ -450,7 +450,8 @@ class Context:
                 for i, k in enumerate(self.TIME_KINDS) if nl[i] > 0}
 
     def tiles(self, mesh=0):
-        """Autotuned tile shapes: 2D y width, 3D y width and variant (1: radix-16 Stockham), z width,
+        """Autotuned tile shapes: 2D y width, 3D y width and variant (1: radix-16 Stockham, 2: two-level
+        register transform fed by pipelined bulk tensor copies), z width,
         stage rows per block (negative when the per-cell rows are prefetched), stage x-transform
         variant (1: radix-8 Stockham), yzy (1: the fused y -> z -> y cluster pass of a 3D mesh)."""
         t = (ctypes.c_int * 4)()

@@ -515,10 +515,15 @@ void tune_ypass(bm_ctx *c, Mesh &m)
     const size_t cs = sizeof(cpx<T>);
     YZArgs<T> a = yz_args<T>(c, m, BM_GATE_ALWAYS);
     float best = 1e30f; int bw = m.Wy, byv = m.yv;
-    for (int yv = 0; yv <= (ypass_has_st(m.Ny) ? 1 : 0); yv++)
+    const char *tma = getenv("BM_Y_TMA");   // "0": leave the pipelined bulk-copy y passes out of the tuning
+    for (int yv = 0; yv <= 2; yv++)
         for (int W = 1; W <= 32 && W <= m.LX; W *= 2) {
             if ((size_t)m.Ny * W * cs > 200 * 1024) continue;
-            if (yv) {
+            a.W = W;
+            if (yv == 2) {
+                if ((tma && tma[0] == '0') || !ypass_tma_fits<T>(a)) continue;
+            } else if (yv == 1) {
+                if (!ypass_has_st(m.Ny)) continue;
                 const int nt = ypass_st_threads(m.Ny, W);
                 if (nt > lim || nt % 32) continue;
             } else if (ypass_has_reg(m.Ny) ? ypass_reg_threads(m.Ny, W) > yreg_maxt<T>::v : W * m.py.tpl > lim) {
@@ -954,6 +959,11 @@ int prepare_T(bm_ctx *c)
             m.xv = (sx && sx[0] == '1' && stage_reg_q(m.LX, 1)) ? 1 : (sx && sx[0] == '2' && stage_reg_q(m.LX, 2)) ? 2 : 0;
             const char *sy = getenv("BM_Y_XV");
             m.yv = (sy && sy[0] == '1' && ypass_has_st(m.Ny) && m.nz > 1 && ypass_st_threads(m.Ny, m.Wy) % 32 == 0) ? 1 : 0;
+            if (sy && sy[0] == '2' && m.nz > 1) {
+                YZArgs<T> ya = yz_args<T>(c, m, BM_GATE_ALWAYS);
+                ya.W = m.Wy;
+                if (ypass_tma_fits<T>(ya)) m.yv = 2;
+            }
             const char *sz = getenv("BM_YZY");
             m.yzy = 0;
             if (sz && sz[0] == '1' && m.nz > 1 && m.ml_role == 0 && (m.modules & BM_DEMAG) && !c->batched)
@@ -1932,6 +1942,8 @@ int run_T(bm_ctx *c, int steps)
         for (long long i = warm; i < k; i++) CK(cudaGraphLaunch(c->gexec_es, c->stream));
         guard += k;
         if ((rc = read_state(c))) return rc;
+        if (c->host_st.error & BM_ERR_WAIT)
+            return fail(BM_ECUDA, "a kernel's bounded wait for its bulk tensor copies gave up");
         if (c->host_st.error & BM_ERR_NONFINITE)
             return fail(BM_ENONFINITE, c->eval == BM_RK4
                                            ? "a step produced a non-finite M (NaN or infinity); its steps are counted"

@@ -62,6 +62,7 @@ __device__ __forceinline__ void cp_async_real(T *smem, const T *gmem, bool valid
 
 // StepState.error bits (sticky until the next bm_set_m)
 #define BM_ERR_NONFINITE 1   // a stage produced a NaN or infinite M or error estimate
+#define BM_ERR_WAIT 2        // a kernel's bounded wait on its own bulk copies gave up
 
 // device-resident step state shared by all kernels of a solver
 struct StepState {

@@ -1080,7 +1080,11 @@ template <typename T> int launch_ymid2d(const YZArgs<T> &a, cudaStream_t s)
 
 template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s)
 {
-    if (a.yv) {
+    if (a.yv == 2) {
+        int rc = launch_ypass_tma<T, false>(a, s);
+        if (rc >= 0) return rc;
+    }
+    if (a.yv == 1) {
         int rc = launch_ypass_st_dispatch<T, false>(a, s);
         if (rc >= 0) return rc;
     }
@@ -1101,7 +1105,11 @@ template <typename T> int launch_yfwd(const YZArgs<T> &a, cudaStream_t s)
 
 template <typename T> int launch_yinv(const YZArgs<T> &a, cudaStream_t s)
 {
-    if (a.yv) {
+    if (a.yv == 2) {
+        int rc = launch_ypass_tma<T, true>(a, s);
+        if (rc >= 0) return rc;
+    }
+    if (a.yv == 1) {
         int rc = launch_ypass_st_dispatch<T, true>(a, s);
         if (rc >= 0) return rc;
     }

@@ -37,7 +37,8 @@ struct YZArgs {
     int W;               // column tile width
     StepState *st;
     int gate;
-    int yv;              // 3D y transform: 0 two-level register kernel, 1 radix-16 Stockham (Ny >= 256)
+    int yv;              // 3D y transform: 0 two-level register kernel, 1 radix-16 Stockham (Ny >= 256),
+                         // 2 the two-level kernel fed by bulk tensor copies (persistent, pipelined)
 };
 
 template <typename T> size_t ymid2d_smem(int Ny, int W)
@@ -64,6 +65,10 @@ bool ypass_has_st(int Ny);            // lengths with the Stockham y transform (
 int ypass_st_threads(int Ny, int W);
 int ymid2d_reg_threads(int Ny, int W);   // block size of the register 2D y pass
 int ypass_reg_threads(int Ny, int W);
+// pipelined 3D y passes with bulk tensor copies (ytma.cu): whether they apply, and the launches
+// (-1 when they do not apply)
+template <typename T> bool ypass_tma_fits(const YZArgs<T> &a);
+template <typename T, bool INV> int launch_ypass_tma(const YZArgs<T> &a, cudaStream_t s);
 // fused y -> z -> y pass of a 3D mesh in one thread-block-cluster kernel (yzy.cu): 0 when it
 // applies to the mesh (sizes, shared memory, the device's cluster occupancy)
 template <typename T> int yzy_available(const YZArgs<T> &a);

@@ -67,6 +67,16 @@ BError DemagB200::UpdateConfiguration(UPDATECONFIG_ cfgMessage)
     return Initialize();
 }
 
+BError DemagB200::Set_PBC(INT3 demag_pbc_images)
+{
+    BError error(CLASS_STR(DemagB200));
+    if (bm_set_pbc(ctx, mesh, demag_pbc_images.x, demag_pbc_images.y, demag_pbc_images.z))
+        return error(BERROR_INCORRECTVALUE);
+    pbc = demag_pbc_images;
+    Uninitialize();
+    return Initialize();
+}
+
 void DemagB200::UpdateField(void)
 {
     double e = 0.0;

@@ -26,6 +26,7 @@ class DemagB200 : public ModulesCUDA {
     cuReal3 *M_data = nullptr, *H_data = nullptr;
     bool own_ctx = false;
     double last_energy = 0.0;
+    INT3 pbc;
 
 public:
     // M and Heff: the mesh's vectors (MeshCUDA::M, MeshCUDA::Heff); h the cellsize (m). The module
@@ -38,6 +39,12 @@ public:
     BError UpdateConfiguration(UPDATECONFIG_ cfgMessage);
     void UpdateConfiguration_Values(UPDATECONFIG_ cfgMessage) {}
     void UpdateField(void);
+
+    // DemagBase::Set_PBC / Get_PBC (Boris/DemagBase.h:55, Boris/Demag.cpp:137): images per axis of the
+    // periodic demag, also the periodic neighbours of the library's stencils (bm_set_pbc); the kernels
+    // are rebuilt by the following Initialize, as UpdateConfiguration(UPDATECONFIG_DEMAG_CONVCHANGE) does
+    BError Set_PBC(INT3 demag_pbc_images);
+    INT3 Get_PBC(void) const { return pbc; }
 
     // the energy density of the last UpdateField (also in the module's device `energy`)
     double GetLastEnergyDensity(void) const { return last_energy; }

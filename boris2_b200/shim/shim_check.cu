@@ -74,6 +74,16 @@ int shim_demag_update(void *h, const double *M, const double *Hpre, double *Heff
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
+// DemagB200::Set_PBC, then the images it reports
+int shim_demag_set_pbc(void *h, int x, int y, int z, int *out3)
+{
+    ShimDemag *s = (ShimDemag *)h;
+    int rc = (int)s->mod->Set_PBC(INT3(x, y, z)).code();
+    INT3 p = s->mod->Get_PBC();
+    out3[0] = p.x; out3[1] = p.y; out3[2] = p.z;
+    return rc;
+}
+
 void shim_demag_destroy(void *h)
 {
     ShimDemag *s = (ShimDemag *)h;

@@ -318,7 +318,8 @@ int bm_time_step(bm_ctx *ctx, int steps, double *ms6, double *bytes6, int *launc
 int bm_time_demag(bm_ctx *ctx, int mesh, int reps, double *ms);
 
 /* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width (plus 100
- * when the 3D y passes use the radix-16 Stockham transform),
+ * when the 3D y passes use the radix-16 Stockham transform, plus 200 when they are the persistent
+ * kernels fed by pipelined bulk tensor copies),
  * z-pass width (plus 1000 when the fused y -> z -> y cluster pass replaces the three 3D passes), stage rows per block (plus 100 when the stage kernel uses the radix-8
  * Stockham x transform; negative when it prefetches its per-cell rows into shared
  * memory)]. Valid after the first compute or run. */

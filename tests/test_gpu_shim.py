@@ -37,6 +37,7 @@ def shim():
     L.shim_demag_create.argtypes = [I, I, I, D, D, D, I]
     L.shim_demag_update.argtypes = [P, DP, DP, DP, DP]
     L.shim_demag_destroy.argtypes = [P]
+    L.shim_demag_set_pbc.argtypes = [P, I, I, I, ctypes.POINTER(ctypes.c_int)]
     L.shim_ode_create.restype = P
     L.shim_ode_create.argtypes = [I, I, I, D, D, D, I]
     L.shim_ode_context.restype = P
@@ -73,6 +74,33 @@ def test_demag_module_adds_field(bm, n):
     Hd = (H - Hpre).reshape(-1, 3)
     assert np.abs(Hd - Href).max() / np.abs(Href).max() < 1e-6
     assert abs(e[0] - eref) <= 1e-6 * abs(eref)
+
+
+def test_demag_module_set_pbc(bm):
+    """DemagB200::Set_PBC (DemagBase::Set_PBC) rebuilds the kernels with the images; the field equals the
+    library's own periodic demag of the same M (mixed precision, 1e-6 of max |H|)."""
+    L = shim()
+    n, h, pbc = (32, 32, 2), (3e-9, 3e-9, 2e-9), (4, 4, 0)
+    N = int(np.prod(n))
+    M = np.ascontiguousarray(sphere_random(N, seed=6, Ms=8e5).reshape(-1))
+    Hpre = np.zeros(3 * N)
+    H = np.zeros(3 * N)
+    e = np.zeros(1)
+    s = L.shim_demag_create(n[0], n[1], n[2], h[0], h[1], h[2], 0)
+    assert s
+    got = (ctypes.c_int * 3)()
+    assert L.shim_demag_set_pbc(s, pbc[0], pbc[1], pbc[2], got) == 0
+    assert tuple(got) == pbc
+    assert L.shim_demag_update(s, _dp(M), _dp(Hpre), _dp(H), _dp(e)) == 0
+    L.shim_demag_destroy(s)
+    c = bm.Context(precision=bm.MIXED)
+    c.add_mesh(n, h)
+    c.set_modules(0, bm.DEMAG)
+    c.set_pbc(0, pbc)
+    c.set_m(M.reshape(-1, 3))
+    Href = c.demag_field()
+    c.close()
+    assert np.abs(H.reshape(-1, 3) - Href).max() / np.abs(Href).max() < 1e-6
 
 
 @pytest.mark.parametrize("evaluation,steps", [("RK4", 12), ("RKDP54", 8)])
