@@ -867,6 +867,16 @@ int prepare_ml(bm_ctx *c)
         for (int a = 0; a < 3; a++) { G.h[a] = y.hc[a]; G.o[a] = y.rs[a]; }
         G.modules = BM_DEMAG;
         if ((rc = prepare_grid<T>(c, G))) return rc;
+        if (c->es_level > 0) {
+            // evaluation speedup: the layer's saved fields, and its self term SelfDemag_PBC(h_common,
+            // n_common) (Boris/SDemag_Demag.cpp:328) scaled as the unnormalised transforms carry it
+            size_t s1 = sizeof(cpx<T>) * 3 * (size_t)G.nz * G.ny * G.LX;
+            if (cudaMalloc(&G.G, s1 * c->es_level) != cudaSuccess) return fail(BM_ENOMEM, "evaluation speedup slots");
+            cudaMemsetAsync(G.G, 0, s1 * c->es_level, s);
+            double S[3];
+            self_demag_host(G.h[0], G.h[1], G.h[2], S);
+            for (int k = 0; k < 3; k++) G.es_cs[k] = S[k] * (double)G.Ny * (double)G.Nz;
+        }
         if ((rc = upload_vec<int>((void **)&r.in_ptr[l], y.in_ptr, s))) return rc;
         if ((rc = upload_vec<int>((void **)&r.in_idx[l], y.in_idx, s))) return rc;
         if ((rc = upload_vec<T>(&r.in_w[l], as_type<T>(y.in_w), s))) return rc;
@@ -1003,8 +1013,9 @@ int prepare(bm_ctx *c)
     if (c->ready) return 0;
     if (c->meshes.empty()) return fail(BM_ESTATE, "no mesh");
     if (c->batched && c->ml_mode >= 0) return fail(BM_EUNSUPPORTED, "batched meshes with a multilayered convolution");
-    if (c->es_level > 0 && c->ml_mode >= 0)
-        return fail(BM_EUNSUPPORTED, "evaluation speedup with a multilayered convolution");
+    // the reference has no evaluation speedup for the supermesh convolution (Boris/SDemag.cpp:742)
+    if (c->es_level > 0 && c->ml_mode == BM_ML_SUPERMESH)
+        return fail(BM_EUNSUPPORTED, "evaluation speedup with the supermesh demag");
     for (auto &m : c->meshes) {
         if (!(m.modules & BM_DEMAG) || !(m.pbc[0] || m.pbc[1] || m.pbc[2]) || c->ml_mode == BM_ML_SUPERMESH) continue;
         if (c->ml_mode >= 0) return fail(BM_EUNSUPPORTED, "periodic boundary conditions with a multilayered convolution");
@@ -1588,6 +1599,57 @@ int enqueue_prime(bm_ctx *c, int *count)
 
 long long es_plane(const Mesh &m) { return (long long)m.nz * m.ny * m.LX; }
 
+// The spectra the evaluation speedup saves and extrapolates: every mesh with demag, or with the
+// multilayered convolution every layer's (its common grid, or its mesh when the mesh's grid is the
+// common grid), as SDemagCUDA::UpdateField does per layer (Boris/SDemagCUDA.cpp:587-930).
+std::vector<Mesh *> es_targets(bm_ctx *c)
+{
+    std::vector<Mesh *> v;
+    if (c->ml) {
+        for (int l = 0; l < c->ml->g.L; l++) v.push_back(&ml_grid(c, l));
+    } else {
+        for (auto &m : c->meshes)
+            if (m.modules & BM_DEMAG) v.push_back(&m);
+    }
+    return v;
+}
+
+// Multilayered convolution with the speedup, one evaluation: the layers' x forward transforms (part 0)
+// give the x spectra of their inputs; a saving evaluation then runs es_pre, the y / z passes and the
+// L x L product (parts 1-3, gated on the decision), es_post and es_commit; an extrapolating one runs
+// es_extrap on the same spectra; the x inverse and the transfers out (part 4) finish both.
+// mode: 1 save (RK4), 2 extrapolate (RK4), 3 decided on the device (RKDP54, sel 1).
+template <typename T>
+int enqueue_ml_es(bm_ctx *c, int mode, int gate_xt, int gate_yz, double c_eval, int bi, int *count)
+{
+    const int sel = (mode == 3) ? 1 : 0;
+    if (int rc = ml_enqueue_part<T>(c, 0, gate_xt, bi, count)) return rc;
+    const std::vector<Mesh *> tg = es_targets(c);
+    if (mode != 2) {
+        for (Mesh *m : tg) {
+            CKL(launch_es_pre<T>((const cpx<T> *)m->S1, (cpx<T> *)m->G, es_plane(*m), m->es_cs, c->st, c->stream, sel),
+                "es_pre");
+            (*count)++;
+        }
+        for (int part = 1; part <= 3; part++)
+            if (int rc = ml_enqueue_part<T>(c, part, gate_yz, bi, count)) return rc;
+        for (Mesh *m : tg) {
+            CKL(launch_es_post<T>((const cpx<T> *)m->S1, (cpx<T> *)m->G, es_plane(*m), c->st, c->stream, sel), "es_post");
+            (*count)++;
+        }
+        CKL(launch_es_commit(c->st, c->stream, sel), "es_commit");
+        (*count)++;
+    }
+    if (mode != 1) {
+        for (Mesh *m : tg) {
+            CKL(launch_es_extrap<T>((cpx<T> *)m->S1, (const cpx<T> *)m->G, es_plane(*m), m->es_cs, c->st, c_eval,
+                                    c->stream, sel), "es_extrap");
+            (*count)++;
+        }
+    }
+    return ml_enqueue_part<T>(c, 4, gate_xt, bi, count);
+}
+
 template <typename T>
 int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void *const *cacheH = nullptr, void *cacheY = nullptr)
 {
@@ -1602,7 +1664,9 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
         // collect pass (which must launch nothing)
         const bool es_launch = !c->bp.collect;
         const bool es_tab = c->es_tab != nullptr;
-        if (c->es_level > 0 && s == 0) {
+        if (c->es_level > 0 && s == 0 && c->ml) {
+            if (int rc = enqueue_ml_es<T>(c, 1, BM_GATE_ALWAYS, BM_GATE_ALWAYS, 0.0, min_buf[s], count)) return rc;
+        } else if (c->es_level > 0 && s == 0) {
             // evaluation speedup: compute and save the field at the first evaluation of the step
             if (es_tab && es_launch) {
                 CKL(launch_es_pre_batch<T>(c->es_tab, c->es_nmesh, c->es_max_plane, c->st, c->stream), "es_pre_batch");
@@ -1630,6 +1694,8 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
         } else if (c->es_level > 0 && c->es_phase != 2) {
             // too few fields saved yet: the full field
             if (int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count)) return rc;
+        } else if (c->es_level > 0 && c->ml) {
+            if (int rc = enqueue_ml_es<T>(c, 2, BM_GATE_ALWAYS, BM_GATE_ALWAYS, c_eval[s], min_buf[s], count)) return rc;
         } else if (c->es_level > 0) {
             // the extrapolation in place of the y/z passes
             if (es_tab && es_launch) {
@@ -1686,6 +1752,12 @@ int enqueue_es_fields_dp(bm_ctx *c, int eval, double c_eval, int bi, int *count)
 {
     const bool launch = !c->bp.collect;   // the speedup kernels are not part of a batched plan
     const bool tab = c->es_tab != nullptr;
+    if (c->ml) {
+        CKL(launch_es_decide(c->st, eval, c_eval, c->stream), "es_decide");
+        (*count)++;
+        return enqueue_ml_es<T>(c, 3, eval ? BM_GATE_ACCEPTED : BM_GATE_ALWAYS, eval ? BM_GATE_ES_ACC : BM_GATE_ES, c_eval,
+                                bi, count);
+    }
     if (launch) {
         CKL(launch_es_decide(c->st, eval, c_eval, c->stream), "es_decide");
         (*count)++;

@@ -741,6 +741,11 @@ struct orc_ml {
     ml_layer *lay;
     ml_kernel *ker;
     int nker;
+    /* evaluation speedup (SDemagCUDA::UpdateField, Boris/SDemagCUDA.cpp:587-930): per slot, every
+       layer's common-grid field minus its self term [slot][layer][3 ncell], and the layers' self
+       coefficients SelfDemag_PBC(h_common, n_common) (Boris/SDemag_Demag.cpp:328) */
+    double *es_H[6];
+    double *es_self;
 };
 
 /* one tensor point D = -N (xx,yy,zz,xy,xz,yz) at grid offset (i,j,k) for a kernel */
@@ -837,6 +842,8 @@ void orc_ml_destroy(orc_ml *s)
         free(y->kidx); free(y->kinv); free(y->kkind);
     }
     for (int q = 0; q < s->nker; q++) free(s->ker[q].F);
+    for (int k = 0; k < 6; k++) free(s->es_H[k]);
+    free(s->es_self);
     free(s->ker); free(s->lay); free(s->mn); free(s->mh); free(s->mrect); free(s->moff);
     free(s);
 }
@@ -1047,8 +1054,28 @@ int orc_ml_info(orc_ml *s, int *L, int *nc3, int *layer_mesh, int *do_transfer, 
     return 0;
 }
 
-/* H_demag of every mesh (AoS, meshes concatenated) from M of every mesh */
-int orc_ml_eval(orc_ml *s, const double *M, double *H)
+/* the field of destination layer d on the common grid (tmp) into every mesh of that layer */
+static void ml_transfer_out(orc_ml *s, int d, const double *tmp, double *H)
+{
+    ml_layer *y = &s->lay[d];
+    double *Hm = H + 3 * s->moff[y->mesh];
+    size_t n = s->moff[y->mesh + 1] - s->moff[y->mesh];
+    if (y->transfer) {
+        for (size_t c = 0; c < n; c++)
+            for (int q = 0; q < y->tout[c].n; q++)
+                for (int a = 0; a < 3; a++) Hm[3 * c + a] += tmp[3 * (size_t)y->tout[c].idx[q] + a] * y->tout[c].w[q];
+    } else {
+        for (size_t c = 0; c < 3 * n; c++) Hm[c] += tmp[c];
+    }
+}
+
+/* Evaluation with the speedup (es_mode 0 plain, 1 compute and save into es_slot, 2 extrapolate with
+ * the weights es_a of K saved fields), per layer on its common grid as SDemagCUDA::UpdateField does
+ * (Boris/SDemagCUDA.cpp:587-930): a save keeps H - S Mc (SDemag_EvalSpeedup_SubSelf /
+ * AddField_SubSelf), an extrapolation sets sum_k a_k (H_k - S Mc_k) + S Mc before the transfer out
+ * (SDemag_EvalSpeedup_SetExtrapField_AddSelf / AddExtrapField_AddSelf); Mc is the layer's input on
+ * the common grid (the mesh's M when the layer needs no transfer). */
+int orc_ml_eval_es(orc_ml *s, const double *M, double *H, int es_mode, int es_slot, const double *es_a, int K)
 {
     const int Nx = s->N[0], Ny = s->N[1], Nz = s->N[2];
     const int nx = s->nc[0], ny = s->nc[1], nz = s->nc[2];
@@ -1056,6 +1083,13 @@ int orc_ml_eval(orc_ml *s, const double *M, double *H)
     const int L = s->L;
     double **F = (double **)calloc(L, sizeof(double *));
     double *tmp = (double *)malloc(sizeof(double) * 3 * ncell);
+    double *Mcs = es_mode ? (double *)malloc(sizeof(double) * 3 * ncell * L) : NULL;
+    if (es_mode && !s->es_self) {
+        s->es_self = (double *)malloc(sizeof(double) * 3 * L);
+        for (int l = 0; l < L; l++)
+            orc_selfdemag_pbc(s->lay[l].hc.x, s->lay[l].hc.y, s->lay[l].hc.z, s->nc, NULL, s->es_self + 3 * l);
+    }
+    if (es_mode == 1 && !s->es_H[es_slot]) s->es_H[es_slot] = (double *)calloc(3 * ncell * L, sizeof(double));
     memset(H, 0, sizeof(double) * 3 * s->moff[s->nmesh]);
     for (int l = 0; l < L; l++) {
         ml_layer *y = &s->lay[l];
@@ -1068,6 +1102,8 @@ int orc_ml_eval(orc_ml *s, const double *M, double *H)
                 for (int a = 0; a < 3; a++) tmp[3 * c + a] = v[a];
             }
         } else memcpy(tmp, Mm, sizeof(double) * 3 * ncell);
+        if (Mcs) memcpy(Mcs + 3 * ncell * l, tmp, sizeof(double) * 3 * ncell);
+        if (es_mode == 2) continue;
         F[l] = (double *)calloc(3 * 2 * np, sizeof(double));
         for (int a = 0; a < 3; a++) {
             double *Fa = F[l] + 2 * a * np;
@@ -1077,6 +1113,19 @@ int orc_ml_eval(orc_ml *s, const double *M, double *H)
                         Fa[2 * ((size_t)i + (size_t)j * Nx + (size_t)k * Nx * Ny)] = tmp[3 * ((size_t)i + (size_t)j * nx + (size_t)k * nx * ny) + a];
             dft3(Fa, Nx, Ny, Nz, -1);
         }
+    }
+    if (es_mode == 2) {
+        for (int d = 0; d < L; d++) {
+            const double *Mc = Mcs + 3 * ncell * d, *S = s->es_self + 3 * d;
+            for (size_t i = 0; i < 3 * ncell; i++) {
+                double v = S[i % 3] * Mc[i];
+                for (int k = 0; k < K; k++) v += es_a[k] * s->es_H[k][3 * ncell * d + i];
+                tmp[i] = v;
+            }
+            ml_transfer_out(s, d, tmp, H);
+        }
+        free(F); free(tmp); free(Mcs);
+        return 0;
     }
     double *O = (double *)malloc(sizeof(double) * 3 * 2 * np);
     static const int cmap[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
@@ -1111,19 +1160,22 @@ int orc_ml_eval(orc_ml *s, const double *M, double *H)
                 tmp[3 * c + a] = Oa[2 * ((size_t)i + (size_t)j * Nx + (size_t)k * Nx * Ny)] / (double)np;
             }
         }
-        double *Hm = H + 3 * s->moff[y->mesh];
-        size_t n = s->moff[y->mesh + 1] - s->moff[y->mesh];
-        if (y->transfer) {
-            for (size_t c = 0; c < n; c++)
-                for (int q = 0; q < y->tout[c].n; q++)
-                    for (int a = 0; a < 3; a++) Hm[3 * c + a] += tmp[3 * (size_t)y->tout[c].idx[q] + a] * y->tout[c].w[q];
-        } else {
-            for (size_t c = 0; c < 3 * n; c++) Hm[c] += tmp[c];
+        if (es_mode == 1) {
+            const double *Mc = Mcs + 3 * ncell * d, *S = s->es_self + 3 * d;
+            double *Hs = s->es_H[es_slot] + 3 * ncell * d;
+            for (size_t i = 0; i < 3 * ncell; i++) Hs[i] = tmp[i] - S[i % 3] * Mc[i];
         }
+        ml_transfer_out(s, d, tmp, H);
     }
     for (int l = 0; l < L; l++) free(F[l]);
-    free(F); free(tmp); free(O);
+    free(F); free(tmp); free(O); free(Mcs);
     return 0;
+}
+
+/* H_demag of every mesh (AoS, meshes concatenated) from M of every mesh */
+int orc_ml_eval(orc_ml *s, const double *M, double *H)
+{
+    return orc_ml_eval_es(s, M, H, 0, 0, NULL, 0);
 }
 
 /* the transfer of one layer alone (tests): Mc = transfer_in(M), Hmesh = transfer_out(Hc) */
@@ -1605,7 +1657,7 @@ static void update_ml(orc_solver *s)
         off += (size_t)m->n;
     }
     if (s->sm) orc_sm_eval(s->sm, s->ml_M, s->ml_H);
-    else orc_ml_eval(s->ml, s->ml_M, s->ml_H);
+    else orc_ml_eval_es(s->ml, s->ml_M, s->ml_H, s->es_mode, s->es_slot, s->es_a, s->es_level);
 }
 
 static void update_fields(orc_solver *s, orc_mesh *m)
@@ -1796,7 +1848,7 @@ static void es_prepare_dp(orc_solver *s, int eval)
 
 int orc_solver_set_evalspeedup(orc_solver *s, int level)
 {
-    if (level < 0 || level > 6 || s->ml || s->sm) return 1;
+    if (level < 0 || level > 6 || s->sm) return 1;
     s->es_level = level;
     s->es_saved = 0;
     s->es_available = 1;

@@ -97,7 +97,8 @@ int orc_get_m(orc_solver *s, int mesh, double *M);
 /* one multilayered convolution (orc_ml, below) replaces the per-mesh demag of every mesh with
  * ORC_DEMAG; o3 = origin of every solver mesh (3 per mesh) */
 int orc_solver_set_multilayer(orc_solver *s, const double *o3, int mode, const int *ncommon);
-/* Evaluation speedup of RK4 (level 0 off, 1 step .. 6 quintic): demag extrapolated from saved fields. */
+/* Evaluation speedup (level 0 off, 1 step .. 6 quintic): demag extrapolated from saved fields, per
+ * mesh or, with the multilayered convolution, per layer on the common grid. */
 int orc_solver_set_evalspeedup(orc_solver *s, int level);
 /* Replace the demag and exchange / iDMI terms of one mesh by a caller's function that adds them
  * into H (3n doubles) for the mesh's M; Zeeman, anisotropy, LLG and the stages stay the solver's.
@@ -121,6 +122,9 @@ orc_ml *orc_ml_create(int nmesh, const int *n3, const double *h3, const double *
 int orc_ml_info(orc_ml *s, int *L, int *nc3, int *layer_mesh, int *do_transfer, double *rects6, int *kinds);
 /* H_demag of every mesh (AoS, meshes concatenated in order) from M of every mesh */
 int orc_ml_eval(orc_ml *s, const double *M, double *H);
+/* with the evaluation speedup: es_mode 0 plain, 1 compute and save into slot es_slot, 2 extrapolate
+ * with the weights es_a of K saved fields (per layer on the common grid) */
+int orc_ml_eval_es(orc_ml *s, const double *M, double *H, int es_mode, int es_slot, const double *es_a, int K);
 /* one layer's mesh transfer alone: Mc = transfer in of M, Hmesh = transfer out of Hc */
 int orc_ml_transfer(orc_ml *s, int layer, const double *M, double *Mc, const double *Hc, double *Hmesh);
 void orc_ml_destroy(orc_ml *s);

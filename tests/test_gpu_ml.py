@@ -90,9 +90,10 @@ def test_ml_hdemag_vs_reference_build(bm, name, meshes, mode):
     assert _relmax(H, Href) < 2e-9
 
 
-def _stack_run(bm, prec, evaluation, steps, mode=0, dt=5e-14, ctrl=None, start="sphere"):
+def _stack_run(bm, prec, evaluation, steps, mode=0, dt=5e-14, ctrl=None, start="sphere", es=0):
     """The three-mesh stack with exchange, anisotropy on the top mesh and an applied field;
-    start "sphere" (random directions) or "tilted" (+z with up to 15 degree tilts)."""
+    start "sphere" (random directions) or "tilted" (+z with up to 15 degree tilts); es: evaluation
+    speedup level (both runs)."""
     descs = []
     for q, (m, Ms) in enumerate(zip(STACK3, MS3)):
         d = dict(n=m[0], h=m[1], Ms=Ms, A=1.5e-11, alpha=0.05, modules=1 | 2 | 16, Ha=(2e4, 0, 0))
@@ -104,6 +105,8 @@ def _stack_run(bm, prec, evaluation, steps, mode=0, dt=5e-14, ctrl=None, start="
     s = OracleSolver(descs, evaluation=evaluation, dt=dt, **({} if ctrl is None else
                                                             dict(tol=ctrl[0], dT_incr=ctrl[1], dT_min=ctrl[2], dT_max=ctrl[3])))
     s.multilayer([m[2] for m in STACK3], mode=mode)
+    if es:
+        s.evalspeedup(es)
     for q, M0 in enumerate(Ms0):
         s.set_m(M0, q)
     st_o = s.run(steps)
@@ -114,6 +117,8 @@ def _stack_run(bm, prec, evaluation, steps, mode=0, dt=5e-14, ctrl=None, start="
         c.set_modules(q, d["modules"])
         c.set_field(q, d["Ha"])
     c.multiconvolution(mode)
+    if es:
+        c.evalspeedup(es)
     c.setode("RK4" if evaluation == 0 else "RKDP54", dt)
     if ctrl:
         c.astepctrl(*ctrl)
@@ -140,3 +145,32 @@ def test_ml_rkdp54_stack(bm, prec, tol):
         assert st_g["accepted"] == st_o["accepted"] and st_g["rejected"] == st_o["rejected"]
         assert abs(st_g["time"] - st_o["time"]) <= 1e-9 * st_o["time"]
     assert err < tol
+
+
+# ---------------------------------------------------------------- evaluation speedup, per layer
+@pytest.mark.parametrize("level", [1, 2, 3, 6])
+@pytest.mark.parametrize("mode", [0, 2])
+def test_ml_evalspeedup_rk4_stack(bm, level, mode):
+    """The speedup on the multilayered convolution (SDemagCUDA::UpdateField, Boris/SDemagCUDA.cpp:
+    587-930): each layer's common-grid field minus its self term saved and extrapolated; FP64 follows
+    the oracle to 1e-9 of Ms (that the oracle's speedup changes the trajectory is checked on the CPU,
+    test_oracle_evalspeedup.py)."""
+    err, st_g, st_o = _stack_run(bm, "fp64", 0, 20, mode=mode, es=level)
+    assert st_g["accepted"] == st_o["accepted"] == 20
+    assert err < 1e-9
+
+
+@pytest.mark.parametrize("level", [1, 3])
+def test_ml_evalspeedup_rkdp54_stack(bm, level):
+    """RKDP54 with the speedup on the multilayered convolution, the reference's rule decided on the
+    device per evaluation: accepted / rejected counts, time and m follow the oracle (FP64)."""
+    err, st_g, st_o = _stack_run(bm, "fp64", 1, 15, dt=1e-13, ctrl=(1e-5, 2.0, 1e-15, 3e-12), start="tilted", es=level)
+    assert st_g["accepted"] == st_o["accepted"] and st_g["rejected"] == st_o["rejected"]
+    assert abs(st_g["time"] - st_o["time"]) <= 1e-9 * st_o["time"]
+    assert err < 1e-8
+
+
+def test_ml_evalspeedup_mixed(bm):
+    err, st_g, _ = _stack_run(bm, "mixed", 0, 20, es=3)
+    assert st_g["accepted"] == 20
+    assert err < 1e-4

@@ -88,3 +88,50 @@ def test_self_demag_matches_reference(h):
     assert np.abs(got - want).max() < 1e-13
     # scale invariance: the library normalises the cellsize, so nanometre cells give the same
     assert np.abs(boris2_b200.self_demag(np.asarray(h) * 1e-9) - want).max() < 1e-13
+
+
+# ---------------------------------------------------------------- multilayered convolution
+ML_MESHES = [dict(n=(24, 16, 1), h=(4e-9, 4e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(1e3, 0, 0)),
+             dict(n=(16, 16, 1), h=(5e-9, 4e-9, 3e-9), Ms=1.1e6, A=1.5e-11, alpha=0.1, modules=1 | 2 | 16, Ha=(0, 1e3, 0))]
+ML_ORIGINS = [(0.0, 0.0, 0.0), (10e-9, 0.0, 6e-9)]
+
+
+def _run_ml(level, evaluation=0, steps=12, dt=5e-14, meshes=ML_MESHES, origins=ML_ORIGINS, mode=1):
+    # RKDP54 at a fixed step (dT_min = dT_max), so every run ends at the same time
+    kw = dict(tol=1e-5, dT_incr=2.0, dT_min=dt, dT_max=dt) if evaluation else {}
+    s = OracleSolver(meshes, evaluation=evaluation, dt=dt, **kw)
+    s.multilayer(origins, mode=mode)
+    s.evalspeedup(level)
+    for q, d in enumerate(meshes):
+        s.set_m(sphere_random(int(np.prod(d["n"])), seed=30 + q, Ms=d["Ms"]), q)
+    st = s.run(steps)
+    out = [s.get_m(q) / d["Ms"] for q, d in enumerate(meshes)]
+    s.close()
+    return out, st
+
+
+def test_multilayer_one_direct_layer_equals_mesh_speedup():
+    """One mesh as the only layer of the multilayered convolution (its grid is the common grid): the
+    per-layer speedup (SDemagCUDA) follows the per-mesh one (DemagCUDA) with the same self term."""
+    mesh = [dict(n=(16, 12, 2), h=(4e-9, 4e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(1e3, 0, 0))]
+    for level in (1, 3):
+        a, _ = _run_ml(level, meshes=mesh, origins=[(0.0, 0.0, 0.0)], mode=0)
+        s = OracleSolver(mesh, evaluation=0, dt=5e-14)
+        s.evalspeedup(level)
+        s.set_m(sphere_random(384, seed=30, Ms=8e5))
+        s.run(12)
+        b = s.get_m() / 8e5
+        s.close()
+        assert np.abs(a[0] - b).max() < 1e-12, level
+
+
+@pytest.mark.parametrize("evaluation", [0, 1])
+def test_multilayer_speedup_approaches_plain(evaluation):
+    plain, _ = _run_ml(0, evaluation)
+    errs = []
+    for level in (1, 2, 3):
+        m, st = _run_ml(level, evaluation)
+        assert st["accepted"] == 12
+        errs.append(max(np.abs(x - y).max() for x, y in zip(m, plain)))
+    assert errs[0] > 1e-9                      # the extrapolating path is the one run
+    assert errs[2] < errs[0] and errs[2] < 1e-4
