@@ -208,9 +208,11 @@ int bm_prepare(bm_ctx *ctx);
  * evaluations extrapolate once `level` fields are saved. RKDP54: the reference's rule, decided on
  * the device per evaluation: compute and save at the first evaluation of an attempt that follows a
  * completed step, and at every evaluation while fewer than `level` are saved; extrapolate otherwise
- * (so after a rejected step the repeated first evaluation extrapolates). No multilayered
- * convolution; with batched meshes the y/z passes stay batched and the speedup kernels cover every
- * mesh in one launch. Setting M drops the saved fields. */
+ * (so after a rejected step the repeated first evaluation extrapolates). With the multilayered
+ * convolution every layer's field is saved and extrapolated on its common grid with the layer's own
+ * self term, as SDemagCUDA::UpdateField does (Boris/SDemagCUDA.cpp:587-930); not with the supermesh
+ * demag (BM_EUNSUPPORTED at set-up). With batched meshes the y/z passes stay batched and the speedup
+ * kernels cover every mesh in one launch. Setting M drops the saved fields. */
 int bm_set_evalspeedup(bm_ctx *ctx, int level);
 /* Self-demagnetising coefficients -N (x, y, z) of one cell of size hx, hy, hz (DemagTFunc::SelfDemag,
  * Boris/DemagTFunc_Self.cpp:6); host only. */
