@@ -51,7 +51,7 @@ def test_ytma_hdemag(bm, monkeypatch, n, W, prec):
 
 def test_ytma_rk4_steps(bm, monkeypatch):
     _force(monkeypatch, 8)
-    mesh = dict(n=(32, 24, 4), h=(3e-9, 3e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(1e3, 0, 0))
+    mesh = dict(n=(32, 32, 4), h=(3e-9, 3e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(1e3, 0, 0))
     N = int(np.prod(mesh["n"]))
     M = sphere_random(N, seed=7, Ms=8e5)
     s = OracleSolver([mesh], evaluation=0, dt=1e-13)
