@@ -182,6 +182,8 @@ struct bm_ctx {
     cudaGraphExec_t gexec_es = nullptr;   // evaluation speedup: the extrapolating step (gexec saves)
     cudaGraph_t graph_es = nullptr;
     EsMesh *es_tab = nullptr;   // batched meshes: device table for the one-launch extrapolation kernels
+    int es_fold_pending = 0;    // the evaluation being captured extrapolates in its stage kernels (1 RK4, 2 RKDP54)
+    double es_fold_ceval = 0.0; // its time as a fraction of dT
     int es_nmesh = 0;
     long long es_max_plane = 0;
     bool es_reset = true;       // clear the saved fields at the next state upload
@@ -1599,6 +1601,26 @@ int enqueue_prime(bm_ctx *c, int *count)
 
 long long es_plane(const Mesh &m) { return (long long)m.nz * m.ny * m.LX; }
 
+// Whether a mesh's extrapolated spectrum is formed by its own stage kernel (the register stage kernels,
+// one launch per mesh, no multilayered convolution) in place of a k_es_extrap pass. BM_ES_FOLD=0 keeps
+// the separate pass (comparison timings).
+bool es_fold_ok(const bm_ctx *c, const Mesh &m)
+{
+    static const char *env = getenv("BM_ES_FOLD");
+    if (env && env[0] == '0') return false;
+    return !c->ml && !c->batched && (m.modules & BM_DEMAG) && m.G && stage_reg_path(m.LX, m.xv);
+}
+
+template <typename T>
+void es_fold_args(const bm_ctx *c, const Mesh &m, StageArgs<T> &a)
+{
+    if (!c->es_fold_pending || !es_fold_ok(c, m)) return;
+    a.es_fold = c->es_fold_pending;
+    a.esG = (const cpx<T> *)m.G;
+    for (int k = 0; k < 3; k++) a.es_cs[k] = m.es_cs[k];
+    a.es_ceval = c->es_fold_ceval;
+}
+
 // The spectra the evaluation speedup saves and extrapolates: every mesh with demag, or with the
 // multilayered convolution every layer's (its common grid, or its mesh when the mesh's grid is the
 // common grid), as SDemagCUDA::UpdateField does per layer (Boris/SDemagCUDA.cpp:587-930).
@@ -1704,11 +1726,12 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
                 (*count)++;
             }
             for (auto &m : c->meshes) {
-                if (!(m.modules & BM_DEMAG) || !es_launch || es_tab) continue;
+                if (!(m.modules & BM_DEMAG) || !es_launch || es_tab || es_fold_ok(c, m)) continue;
                 CKL(launch_es_extrap<T>((cpx<T> *)m.S1, (const cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c_eval[s],
                                         c->stream), "es_extrap");
                 (*count)++;
             }
+            if (!es_tab) { c->es_fold_pending = 1; c->es_fold_ceval = c_eval[s]; }
         } else {
             int rc = enqueue_fields<T>(c, BM_GATE_ALWAYS, min_buf[s], count);
             if (rc) return rc;
@@ -1737,8 +1760,10 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
                 a.Hsave = (T *)cacheH[s];
                 if (s == 3) a.Ysave = (T *)cacheY;
             }
+            es_fold_args<T>(c, m, a);
             v.push_back(a);
         }
+        c->es_fold_pending = 0;
         if (int rc = stage_multi<T>(c, v, count)) return rc;
     }
     return 0;
@@ -1791,11 +1816,13 @@ int enqueue_es_fields_dp(bm_ctx *c, int eval, double c_eval, int bi, int *count)
         (*count)++;
     } else {
         for (auto &m : c->meshes) {
-            if (!(m.modules & BM_DEMAG)) continue;
+            if (!(m.modules & BM_DEMAG) || es_fold_ok(c, m)) continue;
             CKL(launch_es_extrap<T>((cpx<T> *)m.S1, (const cpx<T> *)m.G, es_plane(m), m.es_cs, c->st, c_eval, c->stream, 1),
                 "es_extrap");
             (*count)++;
         }
+        c->es_fold_pending = 2;
+        c->es_fold_ceval = c_eval;
     }
     return 0;
 }
@@ -1852,8 +1879,10 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
             }
             a.ev_out = E<T>(m, 0);
             if (i == nm - 1) a.last_kind = BM_LAST_CONTROL;
+            es_fold_args<T>(c, m, a);
             v.push_back(a);
         }
+        c->es_fold_pending = 0;
         if (int rc = stage_multi<T>(c, v, count)) return rc;
     }
     // advance: sM1 = M, M1 = M + dT/5 k0
@@ -1907,8 +1936,10 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
                 a.renorm = 1;
                 if (i == nm - 1) a.last_kind = BM_LAST_FINISH;
             }
+            es_fold_args<T>(c, m, a);
             v.push_back(a);
         }
+        c->es_fold_pending = 0;
         if (int rc = stage_multi<T>(c, v, count)) return rc;
     }
     return 0;

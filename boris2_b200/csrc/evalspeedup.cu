@@ -151,19 +151,7 @@ __global__ void k_es_decide(StepState *st, int eval, double c_eval)
 template <typename T>
 __device__ __forceinline__ void es_weights(const StepState *st, int sel, double c_eval, T a[6])
 {
-    const int K = st->es_K;
-    const double t = st->time + c_eval * st->dT;
-#pragma unroll
-    for (int k = 0; k < 6; k++) {
-        double w = 0.0;
-        if (sel) w = st->es_a[k];
-        else if (k < K) {
-            w = 1.0;
-            for (int j = 0; j < K; j++)
-                if (j != k) w *= (t - st->es_t[j]) / (st->es_t[k] - st->es_t[j]);
-        }
-        a[k] = (T)w;
-    }
+    bm_es_weights<T>(st, sel, c_eval, a);
 }
 
 template <typename T>

@@ -129,6 +129,13 @@ struct StageArgs {
     T two_mu0;                // 2 / mu0
     T llg_pre;                // -gamma grel / (1 + alpha^2)
     int pbc[3];               // per axis: 0 no wrap, +1 / -1 periodic neighbour with that sign (mesh PBC)
+    // evaluation speedup formed in the stage kernel: es_fold 0 off, 1 RK4 (extrapolate once es_K are
+    // saved, weights from the saved times), 2 RKDP54 (extrapolate when the decision says so, its
+    // weights); the S1 row becomes es_cs[c] S1 + sum_k a_k G_k before the inverse x transform
+    int es_fold;
+    const cpx<T> *esG;        // saved slots [slot][c][row][LX]
+    double es_cs[3];
+    double es_ceval;          // evaluation time as a fraction of dT
 };
 
 // fills the derived constants of a StageArgs from its material and cellsize fields
@@ -221,6 +228,39 @@ template <typename T>
 int launch_adj_m0(const AdjArgs<T> &a, const T *M0, const T *lam, double *gMs, cudaStream_t s);
 
 // ---------------------------------------------------------------- evaluation speedup (RK4)
+// Lagrange weights of the saved fields at this evaluation: RK4 (sel 0) from the saved times at
+// time + c_eval dT, RKDP54 (sel 1) as k_es_decide recorded them
+template <typename T>
+__device__ __forceinline__ void bm_es_weights(const StepState *st, int sel, double c_eval, T a[6])
+{
+    const int K = st->es_K;
+    const double t = st->time + c_eval * st->dT;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        double w = 0.0;
+        if (sel) w = st->es_a[k];
+        else if (k < K) {
+            w = 1.0;
+            for (int j = 0; j < K; j++)
+                if (j != k) w *= (t - st->es_t[j]) / (st->es_t[k] - st->es_t[j]);
+        }
+        a[k] = (T)w;
+    }
+}
+// the weight of saved field k alone (as bm_es_weights)
+__device__ __forceinline__ double bm_es_weight(const StepState *st, int sel, double c_eval, int k)
+{
+    if (sel) return st->es_a[k];
+    const int K = st->es_K;
+    const double t = st->time + c_eval * st->dT;
+    double w = 1.0;
+    for (int j = 0; j < K; j++)
+        if (j != k) w *= (t - st->es_t[j]) / (st->es_t[k] - st->es_t[j]);
+    return w;
+}
+// whether the register stage kernels (which can form the extrapolated spectrum themselves) serve
+// this x length and variant
+bool stage_reg_path(int LX, int xv);
 void self_demag_host(double hx, double hy, double hz, double out3[3]);   // -N of one cell (tensor.cu)
 // -N of one cell plus the far field of its PBC images (tensor.cu); n = cells, img = images per axis
 void self_demag_pbc_host(double hx, double hy, double hz, const int n[3], const int img[3], double out3[3]);

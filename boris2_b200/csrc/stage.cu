@@ -800,6 +800,32 @@ __device__ __forceinline__ void x_reg(cpx<T> *line, int t, bool act, const cpx<T
     else x_stockham<T, LX, 1, INV, !INV, 16>(line, t, act, tw, nkeep);
 }
 
+// The evaluation speedup's extrapolation on one x line in shared memory (element e at line[A(e)]):
+// es_cs[c] line + sum_k a_k G_k[c][row] (the sum of k_es_extrap), when this evaluation extrapolates:
+// RK4 (es_fold 1) once es_K fields are saved, RKDP54 (es_fold 2) when the decision says so.
+template <typename T, int LX, int PAD>
+__device__ __noinline__ void es_fold_line(const StepState *st, int fold, const cpx<T> *esG, T f, double ceval, int nrows,
+                                          cpx<T> *line, int c, int row, int t, int TPL)
+{
+    const bool act = (fold == 2) ? (*((volatile const int *)&st->es_mode) == 2) : (st->es_saved >= st->es_K);
+    if (!act) return;
+    addrP<PAD> A;
+    const int K = st->es_K;
+    const long long slot = (long long)3 * nrows * LX;
+    const cpx<T> *g = esG + ((long long)c * nrows + row) * LX;
+    for (int m = t; m < LX; m += TPL) line[A(m)] = cscale(line[A(m)], f);
+#pragma unroll 1
+    for (int k = 0; k < K; k++) {
+        const T wk = (T)bm_es_weight(st, fold == 2, ceval, k);
+        const cpx<T> *gk = g + k * slot;
+        for (int m = t; m < LX; m += TPL) {
+            const cpx<T> gv = gk[m];
+            const cpx<T> v = line[A(m)];
+            line[A(m)] = mk<T>(v.x + wk * gv.x, v.y + wk * gv.y);
+        }
+    }
+}
+
 template <typename T, int LX, int XV>
 __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, unsigned int total)
 {
@@ -909,6 +935,15 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
     if (demag) {
         cp_async_wait_group<1>();
         __syncthreads();
+        if (a.es_fold) {
+            // evaluation speedup: an extrapolating evaluation turns the row of X[M] into the
+            // extrapolated field's row (the k_es_extrap sum, formed here so the spectrum is not
+            // written and read back); kept out of line so the hot path's registers are untouched
+            if (qact)
+                es_fold_line<T, LX, C::PAD>(a.st, a.es_fold, a.esG, (T)a.es_cs[qc], a.es_ceval, nrows, line, qc, r0 + qr, t,
+                                            TPL);
+            __syncthreads();
+        }
         xinv_pre_f<T>(line, LX, a.twx2, t, TPL, qact, A);
         x_reg<T, LX, XV, true>(line, t, qact, a.twx, half);
     }
@@ -1065,6 +1100,15 @@ template <typename T> int launch_stage(const StageArgs<T> &a, cudaStream_t s)
     dim3 grid((nrows + a.rpb - 1) / a.rpb);
     k_stage<T><<<grid, nt, smem, s>>>(a);
     return (int)cudaGetLastError();
+}
+
+bool stage_reg_path(int LX, int xv)
+{
+    switch (LX) {
+    case 16: case 32: case 64: case 128: case 256: case 512: case 1024: return true;
+    case 24: case 48: case 96: case 192: case 384: case 768: return xv != 0;
+    default: return false;
+    }
 }
 
 template int launch_stage<float>(const StageArgs<float> &, cudaStream_t);
