@@ -118,6 +118,8 @@ _SIGS = {
     "bm_adjoint_rk4": (_I, [_P, _I, _I, _DP, _I, _DP, _DP, _DP, _DP, _DP]),
     "bm_set_evalspeedup": (_I, [_P, _I]),
     "bm_self_demag": (_I, [_D, _D, _D, _DP]),
+    "bm_self_demag_metres": (_I, [_D, _D, _D, _DP]),
+    "bm_set_evalspeedup_self": (_I, [_P, _I]),
     "bm_ovf2_read": (_I, [ctypes.c_char_p, _IP, _DP, _DP, _DP, ctypes.c_longlong]),
     "bm_ovf2_write": (_I, [ctypes.c_char_p, _IP, _DP, _DP, _DP, ctypes.c_char_p, _D]),
     "bm_map_cells": (_I, [_DP, _IP, _DP, _IP]),
@@ -158,10 +160,12 @@ def _vec(a, n):
     return a
 
 
-def self_demag(h):
-    """Self-demagnetising coefficients -N of a cell of size h (host only)."""
+def self_demag(h, metres=False):
+    """Self-demagnetising coefficients -N of a cell of size h (host only); metres: as the reference's
+    evaluation speedup computes them on the cellsize in metres."""
     out = np.empty(3)
-    _check(lib().bm_self_demag(float(h[0]), float(h[1]), float(h[2]), _dp(out)))
+    f = lib().bm_self_demag_metres if metres else lib().bm_self_demag
+    _check(f(float(h[0]), float(h[1]), float(h[2]), _dp(out)))
     return out
 
 
@@ -373,6 +377,11 @@ class Context:
         """The reference's evalspeedup: 0 off, 1 step .. 6 quintic extrapolation of the demag field
         between RK4 steps."""
         _check(lib().bm_set_evalspeedup(self._h, int(level)))
+
+    def evalspeedup_self(self, metres):
+        """The speedup's self term: False the cell's -N on normalised cellsizes (default), True as the
+        reference computes it on cellsizes in metres."""
+        _check(lib().bm_set_evalspeedup_self(self._h, int(bool(metres))))
 
     def astepctrl(self, err_fail, dT_incr, dT_min, dT_max):
         _check(lib().bm_set_astepctrl(self._h, float(err_fail), float(dT_incr), float(dT_min), float(dT_max)))

@@ -183,6 +183,7 @@ struct bm_ctx {
     cudaGraph_t graph_es = nullptr;
     EsMesh *es_tab = nullptr;   // batched meshes: device table for the one-launch extrapolation kernels
     int es_fold_pending = 0;    // the evaluation being captured extrapolates in its stage kernels (1 RK4, 2 RKDP54)
+    int es_self_metres = 0;     // the speedup's self term on the cellsize in metres, as the reference computes it
     double es_fold_ceval = 0.0; // its time as a fraction of dT
     int es_nmesh = 0;
     long long es_max_plane = 0;
@@ -391,7 +392,7 @@ int prepare_mesh(bm_ctx *c, Mesh &m)
             cudaMemsetAsync(m.G, 0, s1 * c->es_level, s);
             double S[3];
             const int nc3[3] = {m.nx, m.ny, m.nz};
-            self_demag_pbc_host(m.h[0], m.h[1], m.h[2], nc3, m.pbc, S);
+            self_demag_pbc_host(m.h[0], m.h[1], m.h[2], nc3, m.pbc, S, c->es_self_metres);
             for (int k = 0; k < 3; k++) m.es_cs[k] = S[k] * (double)m.Ny * (double)m.Nz;
         }
         if (m.nz > 1 || m.ml_role == 1) {
@@ -876,7 +877,8 @@ int prepare_ml(bm_ctx *c)
             if (cudaMalloc(&G.G, s1 * c->es_level) != cudaSuccess) return fail(BM_ENOMEM, "evaluation speedup slots");
             cudaMemsetAsync(G.G, 0, s1 * c->es_level, s);
             double S[3];
-            self_demag_host(G.h[0], G.h[1], G.h[2], S);
+            if (c->es_self_metres) self_demag_metres_host(G.h[0], G.h[1], G.h[2], S);
+            else self_demag_host(G.h[0], G.h[1], G.h[2], S);
             for (int k = 0; k < 3; k++) G.es_cs[k] = S[k] * (double)G.Ny * (double)G.Nz;
         }
         if ((rc = upload_vec<int>((void **)&r.in_ptr[l], y.in_ptr, s))) return rc;
@@ -1602,12 +1604,14 @@ int enqueue_prime(bm_ctx *c, int *count)
 long long es_plane(const Mesh &m) { return (long long)m.nz * m.ny * m.LX; }
 
 // Whether a mesh's extrapolated spectrum is formed by its own stage kernel (the register stage kernels,
-// one launch per mesh, no multilayered convolution) in place of a k_es_extrap pass. BM_ES_FOLD=0 keeps
-// the separate pass (comparison timings).
+// one launch per mesh, no multilayered convolution) in place of a k_es_extrap pass. Opt-in (BM_ES_FOLD=1):
+// on the headline film the separate pass is faster (RK4 quadratic 2779 against 2351 Mcell-steps/s,
+// RKDP54 1599 against 1358): the stage kernel's slot loads come after its spectrum row has landed and
+// stall it, where the separate pass streams the slots at 75 % of the copy bandwidth.
 bool es_fold_ok(const bm_ctx *c, const Mesh &m)
 {
-    static const char *env = getenv("BM_ES_FOLD");
-    if (env && env[0] == '0') return false;
+    const char *env = getenv("BM_ES_FOLD");
+    if (!(env && env[0] == '1')) return false;
     return !c->ml && !c->batched && (m.modules & BM_DEMAG) && m.G && stage_reg_path(m.LX, m.xv);
 }
 
@@ -2464,6 +2468,17 @@ int bm_set_evalspeedup(bm_ctx *c, int level)
     if (level == c->es_level) return 0;
     unprepare(c);
     c->es_level = level;
+    c->es_reset = true;
+    return 0;
+}
+
+int bm_set_evalspeedup_self(bm_ctx *c, int metres)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (metres != 0 && metres != 1) return fail(BM_EINVAL, "evaluation speedup self term: 0 normalised, 1 metres");
+    if (metres == c->es_self_metres) return 0;
+    unprepare(c);
+    c->es_self_metres = metres;
     c->es_reset = true;
     return 0;
 }

@@ -262,8 +262,12 @@ __device__ __forceinline__ double bm_es_weight(const StepState *st, int sel, dou
 // this x length and variant
 bool stage_reg_path(int LX, int xv);
 void self_demag_host(double hx, double hy, double hz, double out3[3]);   // -N of one cell (tensor.cu)
-// -N of one cell plus the far field of its PBC images (tensor.cu); n = cells, img = images per axis
-void self_demag_pbc_host(double hx, double hy, double hz, const int n[3], const int img[3], double out3[3]);
+// -N of one cell as the reference's evaluation speedup computes it, on the cellsize in metres (tensor.cu)
+void self_demag_metres_host(double hx, double hy, double hz, double out3[3]);
+// -N of one cell plus the far field of its PBC images (tensor.cu); n = cells, img = images per axis;
+// metres: the cell's own term as self_demag_metres_host
+void self_demag_pbc_host(double hx, double hy, double hz, const int n[3], const int img[3], double out3[3],
+                         int metres = 0);
 // Demag extrapolation in the x-spectrum domain S1[c][z][y][kx] (plane = nz ny LX complex values per
 // component). G holds es_K slots of 3 planes: the saved field minus its self term. cs[c] is the
 // self-demag coefficient (-N_c) times Ny Nz, the factor between the x-spectrum of M the stage kernel

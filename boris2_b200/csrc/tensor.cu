@@ -89,6 +89,61 @@ void self_demag_host(double hx, double hy, double hz, double out3[3])
     out3[2] = -newellL<false>(0.0, 0.0, 0.0, hz, hy, hx);
 }
 
+// The self coefficients as the reference's evaluation speedup gets them: DemagTFunc::SelfDemag on the
+// cellsize in metres (Boris/DemagCUDA.cpp:39, Boris/DemagTFunc_Self.cpp:6), whose Newell f
+// (Boris/DemagTFunc_fg.cpp:10) leaves out a log or atan term when its squared length or coordinate is
+// not above the library's zero threshold (BorisLib/Funcs_Aux_base.h:9,35: 1e-12 as a float). For
+// nanometre cells those squared lengths (~1e-17 m^2) fall under it, so the coefficients differ from the
+// tensor's own self term; this reproduces that.
+namespace {
+const double kRefZero = (double)1e-12f;
+bool ref_nz(double v) { return v > kRefZero || v < -kRefZero; }
+
+double f_thresholded(double x, double y, double z)
+{
+    const double xsq = x * x, ysq = y * y, zsq = z * z;
+    const double Rxy = xsq + ysq, Rxz = xsq + zsq;
+    const double R = sqrt(xsq + ysq + zsq);
+    double t[4] = {(2.0 * xsq - ysq - zsq) * R / 6.0, 0.0, 0.0, 0.0};
+    if (ref_nz(Rxz)) {
+        const double arg = 2.0 * y * (y + R) / Rxz;
+        if (arg > -1.0) t[1] = y * (zsq - xsq) * log1p(arg) / 4.0;
+    }
+    if (ref_nz(Rxy)) {
+        const double arg = 2.0 * z * (z + R) / Rxy;
+        if (arg > -1.0) t[2] = z * (ysq - xsq) * log1p(arg) / 4.0;
+    }
+    if (ref_nz(x)) t[3] = -x * y * z * atan(y * z / (x * R));
+    return csum_d(t, 4);
+}
+
+// -N_xx of the cell (a, b, c): the second difference of f over the cell's 27 corner offsets
+double self_thresholded(double a, double b, double c)
+{
+    double v[27];
+    int m = 0;
+    const double cw[3] = {-1.0, 2.0, -1.0};
+    for (int i = -1; i <= 1; i++)
+        for (int j = -1; j <= 1; j++)
+            for (int k = -1; k <= 1; k++) v[m++] = cw[i + 1] * cw[j + 1] * cw[k + 1] * f_thresholded(i * a, j * b, k * c);
+    return -csum_d(v, 27) / (4.0 * M_PI * a * b * c);
+}
+}  // namespace
+
+void self_demag_metres_host(double hx, double hy, double hz, double out3[3])
+{
+    out3[0] = self_thresholded(hx, hy, hz);
+    out3[1] = self_thresholded(hy, hx, hz);
+    out3[2] = self_thresholded(hz, hy, hx);
+}
+
+extern "C" int bm_self_demag_metres(double hx, double hy, double hz, double *out3)
+{
+    if (!out3 || !(hx > 0) || !(hy > 0) || !(hz > 0)) return bm_set_error(BM_EINVAL, "bm_self_demag_metres: cellsizes must be > 0");
+    self_demag_metres_host(hx, hy, hz, out3);
+    return 0;
+}
+
 extern "C" int bm_self_demag(double hx, double hy, double hz, double *out3)
 {
     if (!out3 || !(hx > 0) || !(hy > 0) || !(hz > 0)) return bm_set_error(BM_EINVAL, "bm_self_demag: cellsizes must be > 0");
@@ -254,12 +309,13 @@ __global__ void k_tensor_octant_pbc(double *oct, PbcSpec P, double hx, double hy
 // there, all three diagonal terms use the expansion of the (hx, hy, hz) cell with the xx form, the
 // yy and zz terms at the offsets permuted (y, x, z) and (z, y, x). Cellsizes are normalised by the
 // largest, as for the tensor.
-void self_demag_pbc_host(double hx, double hy, double hz, const int n[3], const int img[3], double out3[3])
+void self_demag_pbc_host(double hx, double hy, double hz, const int n[3], const int img[3], double out3[3], int metres)
 {
     // the reference's image loops run from -images to images: a negative count on any axis (a
     // stencil sign of -1) leaves them empty and the coefficient zero, self term included
     if (img[0] < 0 || img[1] < 0 || img[2] < 0) { out3[0] = out3[1] = out3[2] = 0.0; return; }
-    self_demag_host(hx, hy, hz, out3);
+    if (metres) self_demag_metres_host(hx, hy, hz, out3);
+    else self_demag_host(hx, hy, hz, out3);
     double hm = fmax(hx, fmax(hy, hz));
     hx /= hm; hy /= hm; hz /= hm;
     int X = img[0], Y = img[1], Z = img[2];

@@ -214,9 +214,19 @@ int bm_prepare(bm_ctx *ctx);
  * demag (BM_EUNSUPPORTED at set-up). With batched meshes the y/z passes stay batched and the speedup
  * kernels cover every mesh in one launch. Setting M drops the saved fields. */
 int bm_set_evalspeedup(bm_ctx *ctx, int level);
+/* The self term of the evaluation speedup: 0 (default) -N of the cell on its cellsize normalised by
+ * the largest, the tensor's own self term; 1 as the reference computes it, DemagTFunc::SelfDemag on
+ * the cellsize in metres (Boris/DemagCUDA.cpp:39, Boris/SDemag_Demag.cpp:328). For nanometre cells
+ * the reference's Newell f then drops terms under its 1e-12 zero threshold (Boris/DemagTFunc_fg.cpp:10),
+ * so its coefficients differ (5 x 5 x 3 nm: (-0.232, -0.232, -0.535) against (-0.274, -0.274, -0.452));
+ * 1 follows the reference's trajectories with the speedup on. */
+int bm_set_evalspeedup_self(bm_ctx *ctx, int metres);
 /* Self-demagnetising coefficients -N (x, y, z) of one cell of size hx, hy, hz (DemagTFunc::SelfDemag,
  * Boris/DemagTFunc_Self.cpp:6); host only. */
 int bm_self_demag(double hx, double hy, double hz, double *out3);
+/* The same on the cellsize in metres as DemagTFunc::SelfDemag computes it there (the speedup's self term
+ * with bm_set_evalspeedup_self(ctx, 1)); host only. */
+int bm_self_demag_metres(double hx, double hy, double hz, double *out3);
 
 /* Magnetization M (A/m, |M| = Ms), AoS doubles, 3 * n values. Replaces writes/reads of
  * MeshBase::M (VEC_VC<DBL3>, Boris/Mesh.h). Setting M un-primes RKDP54 as a restart does. */

@@ -120,21 +120,60 @@ void orc_selfdemag(double hx, double hy, double hz, double *out3)
     out3[2] = -newell_L(orc_newell_f, 0, 0, 0, hz, hy, hx);
 }
 
+/* DemagTFunc::SelfDemag (Boris/DemagTFunc_Self.cpp:6) on the cellsize in metres, as the reference's
+ * evaluation speedup calls it (Boris/DemagCUDA.cpp:39): its Newell f (Boris/DemagTFunc_fg.cpp:10) leaves
+ * out the log and atan terms whose squared lengths / coordinate are not above the zero threshold
+ * (BorisLib/Funcs_Aux_base.h:9,35, 1e-12 as a float) */
+static int ref_nz(double v) { const double e = (double)1e-12f; return v > e || v < -e; }
+
+static double f_thresholded(double x, double y, double z)
+{
+    double xsq = x * x, ysq = y * y, zsq = z * z;
+    double Rxy = xsq + ysq, Rxz = xsq + zsq, R = sqrt(xsq + ysq + zsq);
+    double t[4] = {(2.0 * xsq - ysq - zsq) * R / 6.0, 0, 0, 0};
+    if (ref_nz(Rxz)) {
+        double arg = 2.0 * y * (y + R) / Rxz;
+        if (arg > -1.0) t[1] = y * (zsq - xsq) * log1p(arg) / 4.0;
+    }
+    if (ref_nz(Rxy)) {
+        double arg = 2.0 * z * (z + R) / Rxy;
+        if (arg > -1.0) t[2] = z * (ysq - xsq) * log1p(arg) / 4.0;
+    }
+    if (ref_nz(x)) t[3] = -x * y * z * atan(y * z / (x * R));
+    return csum(t, 4);
+}
+
+void orc_selfdemag_metres(double hx, double hy, double hz, double *out3)
+{
+    const double h3[3][3] = {{hx, hy, hz}, {hy, hx, hz}, {hz, hy, hx}};
+    static const double cw[3] = {-1.0, 2.0, -1.0};
+    for (int c = 0; c < 3; c++) {
+        double v[27];
+        int m = 0;
+        for (int i = -1; i <= 1; i++)
+            for (int j = -1; j <= 1; j++)
+                for (int k = -1; k <= 1; k++)
+                    v[m++] = cw[i + 1] * cw[j + 1] * cw[k + 1] * f_thresholded(i * h3[c][0], j * h3[c][1], k * h3[c][2]);
+        out3[c] = -csum(v, 27) / (4.0 * M_PI * h3[c][0] * h3[c][1] * h3[c][2]);
+    }
+}
+
 /* DemagTFunc::SelfDemag_PBC (Boris/DemagTFunc_Self.cpp:57): the cell's own D plus, for each image
  * period other than (0,0,0), the far-field D at that period's offset (|img * n| cells per axis). As
  * the reference does, the xx, yy and zz image terms all take the expansion of the (hx, hy, hz)
  * cell in its xx form, yy evaluated at the offset (y, x, z) and zz at (z, y, x). Cellsizes are
  * normalised by the largest (the product's choice for the self term; the expansion is scale free). */
-void orc_selfdemag_pbc(double hx, double hy, double hz, const int *n3, const int *pbc, double *out3)
+static void selfdemag_pbc_core(double hx, double hy, double hz, const int *n3, const int *pbc, double *out3, int metres)
 {
+    /* the reference's loops run i_img from -images to images: a negative count on any axis leaves
+       them empty, so the coefficient is zero (self term included) */
+    if (pbc && (pbc[0] < 0 || pbc[1] < 0 || pbc[2] < 0)) { out3[0] = out3[1] = out3[2] = 0.0; return; }
+    if (metres) orc_selfdemag_metres(hx, hy, hz, out3);
     double hm = hx;
     if (hy > hm) hm = hy;
     if (hz > hm) hm = hz;
     hx /= hm; hy /= hm; hz /= hm;
-    /* the reference's loops run i_img from -images to images: a negative count on any axis leaves
-       them empty, so the coefficient is zero (self term included) */
-    if (pbc && (pbc[0] < 0 || pbc[1] < 0 || pbc[2] < 0)) { out3[0] = out3[1] = out3[2] = 0.0; return; }
-    orc_selfdemag(hx, hy, hz, out3);
+    if (!metres) orc_selfdemag(hx, hy, hz, out3);
     if (!pbc) return;
     int X = pbc[0], Y = pbc[1], Z = pbc[2];
     for (int a = -X; a <= X; a++)
@@ -150,6 +189,16 @@ void orc_selfdemag_pbc(double hx, double hy, double hz, const int *n3, const int
                 orc_asymptotic(hx, hy, hz, z, y, x, v);
                 out3[2] += v[0];
             }
+}
+
+void orc_selfdemag_pbc(double hx, double hy, double hz, const int *n3, const int *pbc, double *out3)
+{
+    selfdemag_pbc_core(hx, hy, hz, n3, pbc, out3, 0);
+}
+
+void orc_selfdemag_pbc_metres(double hx, double hy, double hz, const int *n3, const int *pbc, double *out3)
+{
+    selfdemag_pbc_core(hx, hy, hz, n3, pbc, out3, 1);
 }
 
 /* ------------------------------------------------------------------ far field */
@@ -746,6 +795,7 @@ struct orc_ml {
        coefficients SelfDemag_PBC(h_common, n_common) (Boris/SDemag_Demag.cpp:328) */
     double *es_H[6];
     double *es_self;
+    int es_metres;   /* self coefficients on the cellsize in metres (the reference's computation) */
 };
 
 /* one tensor point D = -N (xx,yy,zz,xy,xz,yz) at grid offset (i,j,k) for a kernel */
@@ -1087,7 +1137,8 @@ int orc_ml_eval_es(orc_ml *s, const double *M, double *H, int es_mode, int es_sl
     if (es_mode && !s->es_self) {
         s->es_self = (double *)malloc(sizeof(double) * 3 * L);
         for (int l = 0; l < L; l++)
-            orc_selfdemag_pbc(s->lay[l].hc.x, s->lay[l].hc.y, s->lay[l].hc.z, s->nc, NULL, s->es_self + 3 * l);
+            selfdemag_pbc_core(s->lay[l].hc.x, s->lay[l].hc.y, s->lay[l].hc.z, s->nc, NULL, s->es_self + 3 * l,
+                               s->es_metres);
     }
     if (es_mode == 1 && !s->es_H[es_slot]) s->es_H[es_slot] = (double *)calloc(3 * ncell * L, sizeof(double));
     memset(H, 0, sizeof(double) * 3 * s->moff[s->nmesh]);
@@ -1509,6 +1560,7 @@ struct orc_solver {
     int es_level, es_saved, es_mode, es_slot;
     double es_t[6], es_a[6];
     int es_available;    /* the reference's ODECommon_Base::available: the previous step completed */
+    int es_metres;       /* the speedup's self term on cellsizes in metres (DemagCUDA.cpp:39 as is) */
 };
 
 static int fft_size(int n) { return n > 1 ? 2 * n : 1; }
@@ -1846,6 +1898,19 @@ static void es_prepare_dp(orc_solver *s, int eval)
     else es_weights(s, t);
 }
 
+/* the speedup's self term: 0 on normalised cellsizes, 1 on cellsizes in metres as the reference computes
+   it; takes effect at the next orc_solver_set_evalspeedup */
+int orc_solver_set_evalspeedup_self(orc_solver *s, int metres)
+{
+    s->es_metres = metres != 0;
+    if (s->ml) {
+        s->ml->es_metres = s->es_metres;
+        free(s->ml->es_self);
+        s->ml->es_self = NULL;
+    }
+    return 0;
+}
+
 int orc_solver_set_evalspeedup(orc_solver *s, int level)
 {
     if (level < 0 || level > 6 || s->sm) return 1;
@@ -1856,7 +1921,7 @@ int orc_solver_set_evalspeedup(orc_solver *s, int level)
         orc_mesh *m = &s->m[q];
         {
             const int n3[3] = {m->d.nx, m->d.ny, m->d.nz};
-            orc_selfdemag_pbc(m->d.hx, m->d.hy, m->d.hz, n3, m->d.pbc, m->self);
+            selfdemag_pbc_core(m->d.hx, m->d.hy, m->d.hz, n3, m->d.pbc, m->self, s->es_metres);
         }
         for (int k = 0; k < 6; k++) {
             free(m->Hs[k]);

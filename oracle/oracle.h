@@ -44,6 +44,9 @@ int orc_kernels_from_tensor(const double *diag, const double *odiag, int nz, int
 void orc_pbc_dims(int nx, int ny, int nz, const int *pbc, int *N3);
 /* SelfDemag_PBC (DemagTFunc_Self.cpp:57) on normalised cellsizes */
 void orc_selfdemag_pbc(double hx, double hy, double hz, const int *n3, const int *pbc, double *out3);
+/* DemagTFunc::SelfDemag on the cellsize in metres, with the reference's zero thresholds in f */
+void orc_selfdemag_metres(double hx, double hy, double hz, double *out3);
+void orc_selfdemag_pbc_metres(double hx, double hy, double hz, const int *n3, const int *pbc, double *out3);
 
 /* ---- demag convolution ---- */
 typedef struct orc_demag orc_demag;
@@ -100,6 +103,9 @@ int orc_solver_set_multilayer(orc_solver *s, const double *o3, int mode, const i
 /* Evaluation speedup (level 0 off, 1 step .. 6 quintic): demag extrapolated from saved fields, per
  * mesh or, with the multilayered convolution, per layer on the common grid. */
 int orc_solver_set_evalspeedup(orc_solver *s, int level);
+/* the speedup's self term: 0 normalised cellsizes (default), 1 metres as the reference computes it;
+   call before orc_solver_set_evalspeedup */
+int orc_solver_set_evalspeedup_self(orc_solver *s, int metres);
 /* Replace the demag and exchange / iDMI terms of one mesh by a caller's function that adds them
  * into H (3n doubles) for the mesh's M; Zeeman, anisotropy, LLG and the stages stay the solver's.
  * Used to drive the reference's own compiled field code (oracle/ref_harness.cpp) with this

@@ -103,6 +103,8 @@ def oracle():
         L.orc_ml_destroy.argtypes = [P]
         L.orc_solver_set_multilayer.argtypes = [P, DP, I, IP]
         L.orc_solver_set_evalspeedup.argtypes = [P, I]
+        L.orc_solver_set_evalspeedup_self.argtypes = [P, I]
+        L.orc_selfdemag_metres.argtypes = [D, D, D, DP]
         L.orc_adjoint_rk4.argtypes = [ctypes.POINTER(MeshDesc), DP, DP, I, D, DP, DP, DP, DP]
         L.orc_solver_set_field_hook.argtypes = [P, I, P, P]
         L.orc_tensor_pbc.argtypes = [I, I, I, I, I, I, D, D, D, IP, DP, DP]
@@ -517,7 +519,9 @@ class OracleSolver:
         rc = oracle().orc_solver_set_multilayer(P(self.h), dp(o3), mode, ip(nc) if nc is not None else None)
         assert rc == 0
 
-    def evalspeedup(self, level):
+    def evalspeedup(self, level, metres=False):
+        """metres: the self term on cellsizes in metres, as the reference computes it."""
+        assert oracle().orc_solver_set_evalspeedup_self(P(self.h), int(bool(metres))) == 0
         assert oracle().orc_solver_set_evalspeedup(P(self.h), int(level)) == 0
 
     def supermesh(self, origins, h_request=(5e-9, 5e-9, 5e-9), pbc=(0, 0, 0)):

@@ -177,3 +177,49 @@ def test_evalspeedup_batched_uneven_systems(bm):
     same = max(np.abs(a - b).max() / d["Ms"] for a, b, d in zip(out[0], out[1], descs))
     assert same < 1e-11, same
 
+
+
+@pytest.mark.parametrize("mesh", [FILM, BOX], ids=["film2d", "box3d"])
+def test_evalspeedup_self_term_in_metres(bm, mesh):
+    """bm_set_evalspeedup_self(ctx, 1): the self term as the reference computes it, on the cellsize in
+    metres; FP64 follows the oracle with the same choice to 1e-9 of Ms (RK4, quadratic)."""
+    N = int(np.prod(mesh["n"]))
+    M = sphere_random(N, seed=91, Ms=8e5)
+    s = OracleSolver([mesh], evaluation=0, dt=1e-13)
+    s.evalspeedup(3, metres=True)
+    s.set_m(M)
+    s.run(20)
+    mref = s.get_m()
+    s.close()
+    c = _make(bm, "fp64", mesh, M, "RK4", 1e-13)
+    c.evalspeedup_self(True)
+    c.evalspeedup(3)
+    c.run(20)
+    m = c.get_m()
+    c.close()
+    assert np.abs(m - mref).max() / 8e5 < 1e-9
+
+
+@pytest.mark.parametrize("evaluation", ["RK4", "RKDP54"])
+def test_evalspeedup_folded_into_stage_kernel(bm, monkeypatch, evaluation):
+    """BM_ES_FOLD=1: the extrapolated spectrum formed by the stage kernel instead of k_es_extrap (an
+    opt-in variant, slower on the headline film); FP64 follows the oracle to 1e-9 (RK4) / 1e-8 with the
+    same counts (RKDP54)."""
+    monkeypatch.setenv("BM_ES_FOLD", "1")
+    mesh = BOX
+    N = int(np.prod(mesh["n"]))
+    M = sphere_random(N, seed=93, Ms=8e5)
+    if evaluation == "RK4":
+        mref = _oracle(mesh, M, 20, 1e-13, 3)
+        c = _make(bm, "fp64", mesh, M, "RK4", 1e-13)
+        c.evalspeedup(3)
+        c.run(20)
+        assert np.abs(c.get_m() - mref).max() / 8e5 < 1e-9
+    else:
+        mref, sr = _oracle(mesh, M, 20, 1e-14, 3, evaluation=1, ctrl=CTRL)
+        c = _make(bm, "fp64", mesh, M, "RKDP54", 1e-14, CTRL)
+        c.evalspeedup(3)
+        st = c.run(20)
+        assert st["rejected"] == sr["rejected"]
+        assert np.abs(c.get_m() - mref).max() / 8e5 < 1e-8
+    c.close()

@@ -90,6 +90,54 @@ def test_self_demag_matches_reference(h):
     assert np.abs(boris2_b200.self_demag(np.asarray(h) * 1e-9) - want).max() < 1e-13
 
 
+@pytest.mark.parametrize("h", [(5e-9, 5e-9, 3e-9), (2e-9, 2e-9, 2e-9), (4e-9, 3e-9, 1e-9), (1e-6, 1e-6, 5e-7)])
+def test_self_demag_metres_matches_reference(h):
+    """The reference's speedup self term, SelfDemag on the cellsize in metres with its zero thresholds:
+    the library's host function and the oracle's agree with the reference's own build."""
+    import boris2_b200
+    from boris2_b200 import build
+    build.build()
+    from oracle_libs import oracle
+    R = reference()
+    if R is None:
+        pytest.skip("reference build unavailable")
+    want = np.zeros(3)
+    R.ref_selfdemag(h[0], h[1], h[2], dp(want))
+    got = boris2_b200.self_demag(h, metres=True)
+    orc = np.zeros(3)
+    oracle().orc_selfdemag_metres(h[0], h[1], h[2], dp(orc))
+    assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+    assert np.abs(orc - want).max() <= 1e-13 * np.abs(want).max()
+
+
+def test_self_demag_metres_deviates_on_nanometre_cells():
+    """The documented difference: on 5 x 5 x 3 nm cells the reference's thresholds drop terms, giving
+    (-0.232, -0.232, -0.535) instead of the tensor's (-0.274, -0.274, -0.452); micrometre cells agree."""
+    import boris2_b200
+    m = boris2_b200.self_demag((5e-9, 5e-9, 3e-9), metres=True)
+    n = boris2_b200.self_demag((5e-9, 5e-9, 3e-9))
+    assert np.allclose(m, (-0.232, -0.232, -0.535), atol=2e-3)
+    assert np.allclose(n, (-0.274, -0.274, -0.452), atol=2e-3)
+    assert np.abs(boris2_b200.self_demag((5e-6, 5e-6, 3e-6), metres=True) - n).max() < 1e-12
+
+
+def test_metres_self_term_trajectory_difference():
+    """Size of the trajectory difference between the two self-term choices (RK4, quadratic speedup,
+    12 steps of the film): both are consistent splittings of the same field, so they differ only by the
+    extrapolation error of S M; measured 7e-8 of Ms, well under the 1e-4 mixed tolerance."""
+    M = sphere_random(16 * 8, seed=4, Ms=8e5)
+    out = []
+    for metres in (False, True):
+        s = OracleSolver([FILM], evaluation=0, dt=5e-14)
+        s.evalspeedup(3, metres=metres)
+        s.set_m(M)
+        s.run(12)
+        out.append(s.get_m() / 8e5)
+        s.close()
+    d = np.abs(out[0] - out[1]).max()
+    assert 1e-12 < d < 1e-4
+
+
 # ---------------------------------------------------------------- multilayered convolution
 ML_MESHES = [dict(n=(24, 16, 1), h=(4e-9, 4e-9, 3e-9), Ms=8e5, A=1.3e-11, alpha=0.3, modules=1 | 2 | 16, Ha=(1e3, 0, 0)),
              dict(n=(16, 16, 1), h=(5e-9, 4e-9, 3e-9), Ms=1.1e6, A=1.5e-11, alpha=0.1, modules=1 | 2 | 16, Ha=(0, 1e3, 0))]
