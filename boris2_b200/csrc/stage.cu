@@ -100,8 +100,9 @@ __device__ __forceinline__ void xfwd_post_f(cpx<T> *line, int LX, const cpx<T> *
     __syncthreads();
 }
 
-template <typename T, typename AddrF>
-__device__ __forceinline__ void xinv_pre_f(cpx<T> *line, int LX, const cpx<T> *__restrict__ tw2, int t, int tpl, bool act, AddrF A)
+template <typename T, typename AddrF, typename SyncF>
+__device__ __forceinline__ void xinv_pre_f(cpx<T> *line, int LX, const cpx<T> *__restrict__ tw2, int t, int tpl, bool act, AddrF A,
+                                           SyncF sync)
 {
     if (act) {
         for (int k = t; k <= LX / 2; k += tpl) {
@@ -118,7 +119,7 @@ __device__ __forceinline__ void xinv_pre_f(cpx<T> *line, int LX, const cpx<T> *_
             if (k2 != k) line[A(k2)] = conj(E) + mul_i(conj(O));
         }
     }
-    __syncthreads();
+    sync();
 }
 
 template <typename T>
@@ -245,13 +246,8 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         dr = nt / nx; dx = nt - dr * nx;
         r = tid / nx; x = tid - r * nx;
     }
-    int yrow = -1, y = 0, z = 0;
-    for (; r < rpb; x += dx, r += dr) {
-        if (x >= nx) { x -= nx; r++; if (r >= rpb) break; }
-        const int row = r0 + r;
-        if (row >= nrows) break;
-        if (row != yrow) { yrow = row; z = row / ny; y = row - z * ny; }
-        const long long cell = (long long)row * nx + x;
+    // one cell (r, x) of the block's rows at (y, z): fields, LLG rhs, stage update and outputs
+    auto cell_body = [&](int r, int x, int y, int z, long long cell) {
         T *sp = reinterpret_cast<T *>(&sm[r * LSP + addr(x >> 1)]) + (x & 1);   // packed line slot of x
         T m[3];
 #pragma unroll
@@ -369,7 +365,7 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             if (a.mode == BM_MODE_HEFF) {
 #pragma unroll
                 for (int c = 0; c < 3; c++) (a.Hout + cell)[c * n] = H[c];
-                continue;
+                return;
             }
             if (a.Hsave) {
 #pragma unroll
@@ -435,7 +431,7 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             if (l > lmax) lmax = l;
 #pragma unroll
             for (int c = 0; c < 3; c++) (a.ev_out + cell)[c * n] = rhs[c];
-            continue;
+            return;
         }
         T mn[3];
         {
@@ -481,6 +477,14 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 if ((x & 1) == 0 && x == nx - 1) sp[c * cstride + 1] = 0;   // odd nx: zero the partner slot
             }
         }
+    };
+    int yrow = -1, y = 0, z = 0;
+    for (; r < rpb; x += dx, r += dr) {
+        if (x >= nx) { x -= nx; r++; if (r >= rpb) break; }
+        const int row = r0 + r;
+        if (row >= nrows) break;
+        if (row != yrow) { yrow = row; z = row / ny; y = row - z * ny; }
+        cell_body(r, x, y, z, (long long)row * nx + x);
     }
 }
 
@@ -732,6 +736,19 @@ __device__ __forceinline__ void x_twolevel(cpx<T> *line, int t, bool act, const 
     __syncthreads();
 }
 
+// Barrier between the radix passes of x lines: where the threads of a line divide a warp (and the
+// block is whole warps), every warp owns whole lines and synchronises alone; otherwise the block.
+template <int TPL> __device__ __forceinline__ void xs_sync()
+{
+    if constexpr (32 % TPL == 0) {
+        if ((blockDim.x & 31) == 0) {
+            __syncwarp();
+            return;
+        }
+    }
+    __syncthreads();
+}
+
 // One Stockham pass of stride NS (radix R from xs_radix) and the passes after it. Butterfly j
 // reads elements j + r * L / R, twiddles them by w_L^(r k L / (NS R)) (k = j mod NS), and writes
 // the R-point DFT to (j - k) R + k + r NS. ZHALF: the input is zero beyond L / 2 (only the first
@@ -761,7 +778,7 @@ __device__ __forceinline__ void x_stockham(cpx<T> *line, int t, bool act, const 
             }
         }
     }
-    __syncthreads();
+    xs_sync<TPL>();
     if (act) {
 #pragma unroll
         for (int b = 0; b < BPT; b++) {
@@ -788,7 +805,7 @@ __device__ __forceinline__ void x_stockham(cpx<T> *line, int t, bool act, const 
             }
         }
     }
-    __syncthreads();
+    xs_sync<TPL>();
     if constexpr (!LAST) x_stockham<T, L, NS * R, INV, false, VW>(line, t, act, tw, nkeep);
 }
 
@@ -944,7 +961,8 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
                                             TPL);
             __syncthreads();
         }
-        xinv_pre_f<T>(line, LX, a.twx2, t, TPL, qact, A);
+        if constexpr (XV == 0) xinv_pre_f<T>(line, LX, a.twx2, t, TPL, qact, A, [] { __syncthreads(); });
+        else xinv_pre_f<T>(line, LX, a.twx2, t, TPL, qact, A, [] { xs_sync<TPL>(); });
         x_reg<T, LX, XV, true>(line, t, qact, a.twx, half);
     }
     cp_async_wait_group<0>();
