@@ -1114,6 +1114,7 @@ template <typename T>
 YZArgs<T> yz_args(bm_ctx *c, Mesh &m, int gate)
 {
     YZArgs<T> a;
+    memset(&a, 0, sizeof(a));
     a.S1 = (cpx<T> *)m.S1; a.S2 = (cpx<T> *)m.S2; a.K = (const T *)m.K;
     a.twy = (const cpx<T> *)m.twy; a.twz = (const cpx<T> *)m.twz;
     a.py = m.py; a.pz = m.pz;

@@ -454,6 +454,14 @@ __device__ __forceinline__ void zmid_reg_body(const YZArgs<T> &a, int bx, int ky
         if (e < nz) a.S2[gbase + e * gstride] = v[e];
 }
 
+// L2 prefetch of the bytes p0 .. p1 of one row segment (at most two 128-byte lines)
+__device__ __forceinline__ void pf_segment(const void *p0, const void *p1)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p0));
+    if ((reinterpret_cast<uintptr_t>(p0) >> 7) != (reinterpret_cast<uintptr_t>(p1) >> 7))
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p1));
+}
+
 template <typename T, int NZ, int WC>
 __global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_reg(YZArgs<T> a)
 {
@@ -577,10 +585,33 @@ __device__ __forceinline__ void ypass_reg_body(const YZArgs<T> &a, int bx, int z
     }
 }
 
+// Look-ahead L2 prefetch of a y pass: the block one residency wave ahead in launch order (a.pf_ahead
+// = blocks of the grid resident at once) starts about when this one ends, so this block asks L2 for
+// that block's input column tile (rows rows of the plane at stride LX, columns kx0 .. kx1) before its
+// own loads. Its loads then hit L2, and DRAM keeps streaming while the resident blocks transform.
+// Every prefetched address lies inside the input plane.
+template <typename T, bool INV>
+__device__ __forceinline__ void ypass_prefetch_ahead(const YZArgs<T> &a, int L)
+{
+    const long long gx = gridDim.x, gy = gridDim.y;
+    const long long nxt = blockIdx.x + gx * (blockIdx.y + gy * blockIdx.z) + a.pf_ahead;
+    if (nxt >= gx * gy * gridDim.z) return;
+    const int bx = (int)(nxt % gx);
+    const long long rest = nxt / gx;
+    const int z = (int)(rest % gy), c = (int)(rest / gy);
+    const int LX = a.LX, rows = INV ? L : a.ny;
+    const int kx0 = bx * a.W, kx1 = min(kx0 + a.W, LX) - 1;
+    const cpx<T> *base = (INV ? a.S2 : a.S1) + ((long long)c * a.nz + z) * rows * LX;
+    for (int e = threadIdx.x; e < rows; e += blockDim.x) {
+        pf_segment(base + (long long)e * LX + kx0, base + (long long)e * LX + kx1);
+    }
+}
+
 template <typename T, int P, int Q, bool INV>
 __global__ void __launch_bounds__(yreg_maxt<T>::v) k_ypass_reg(YZArgs<T> a)
 {
     if (gated_out<T>(a.st, a.gate)) return;
+    if (a.pf_ahead > 0) ypass_prefetch_ahead<T, INV>(a, P * Q);
     ypass_reg_body<T, P, Q, INV>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -618,7 +649,9 @@ static int launch_ypass_reg(const YZArgs<T> &a, cudaStream_t s)
         if (e != cudaSuccess) return (int)e;
     }
     dim3 grid((a.LX + a.W - 1) / a.W, a.nz, 3);
-    k_ypass_reg<T, P, Q, INV><<<grid, nt, smem, s>>>(a);
+    YZArgs<T> b = a;
+    b.pf_ahead = resident_blocks(k_ypass_reg<T, P, Q, INV>, nt, smem);
+    k_ypass_reg<T, P, Q, INV><<<grid, nt, smem, s>>>(b);
     return (int)cudaGetLastError();
 }
 

@@ -39,7 +39,33 @@ struct YZArgs {
     int gate;
     int yv;              // 3D y transform: 0 two-level register kernel, 1 radix-16 Stockham (Ny >= 256),
                          // 2 the two-level kernel fed by bulk tensor copies (persistent, pipelined)
+    int pf_ahead;        // set by the launchers: blocks of the grid resident at once (0: no look-ahead prefetch)
 };
+
+// Blocks of a launch resident on the whole GPU at once (occupancy per SM times the SMs), or 0 when
+// the occupancy query fails; the look-ahead distance of the y passes' L2 prefetch. The query depends
+// only on the kernel, the block size and the dynamic shared memory, so its result is kept per kernel
+// for the last block shape asked.
+template <typename K> inline int resident_blocks(K kern, int nt, size_t smem)
+{
+    static int nsm = 0;
+    static thread_local const void *last_k = nullptr;
+    static thread_local int last_nt = -1, last_res = 0;
+    static thread_local size_t last_smem = 0;
+    if (last_k == (const void *)kern && last_nt == nt && last_smem == smem) return last_res;
+    if (nsm == 0) {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+            nsm = v;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 0;
+    }
+    last_k = (const void *)kern; last_nt = nt; last_smem = smem; last_res = per_sm * nsm;
+    return last_res;
+}
 
 template <typename T> size_t ymid2d_smem(int Ny, int W)
 {

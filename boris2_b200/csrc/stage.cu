@@ -843,6 +843,40 @@ __device__ __noinline__ void es_fold_line(const StepState *st, int fold, const c
     }
 }
 
+// L2 prefetch of the per-cell input rows of the block whose rows start at r0 (this row and the z + 1
+// row of M, the update base, the earlier stage evaluations, the material maps). Every prefetched
+// address lies inside its row.
+template <typename T>
+__device__ __forceinline__ void stage_prefetch_rows(const StageArgs<T> &a, int r0)
+{
+    const int nx = a.nx, ny = a.ny, nz = a.nz, rpb = a.rpb, tid = threadIdx.x;
+    const int nrows = ny * nz;
+    const long long n = a.n;
+    const int lpr = (int)((nx * sizeof(T) + 127) / 128);   // 128-byte lines per row
+    const StageLayout L = stage_layout(a);
+    const int nzr = L.ns > 1 ? 3 : 0;                        // z + 1 rows of M
+    const int nev = (a.mode == BM_MODE_HEFF) ? 0 : a.nev;
+    const int o_mb = 3 + nzr, o_ev = o_mb + 3 * L.mb, o_ms = o_ev + 3 * nev, o_k1 = o_ms + L.ms;
+    const int nrow = o_k1 + L.k1;
+    const int lsh = 32 - __clz(lpr - 1), lpr2 = 1 << lsh;   // lines per row rounded up to a power of two
+    for (int job = tid; job < rpb * nrow * lpr2; job += blockDim.x) {
+        const int line_i = job & (lpr2 - 1), rk = job >> lsh;
+        if (line_i >= lpr) continue;
+        const int r = rpb == 1 ? 0 : rk / nrow, k = rk - r * nrow;
+        const int row = r0 + r;
+        if (row >= nrows) continue;
+        const long long ro = (long long)row * nx;
+        const T *src = nullptr;
+        if (k < 3) src = a.Min + k * n + ro;
+        else if (k < o_mb) src = (row + ny < nrows) ? a.Min + (k - 3) * n + ro + (long long)ny * nx : nullptr;
+        else if (k < o_ev) src = a.Mbase + (k - o_mb) * n + ro;
+        else if (k < o_ms) src = a.ev[(k - o_ev) / 3] + ((k - o_ev) % 3) * n + ro;
+        else if (k < o_k1) src = a.Ms_map + ro;
+        else src = a.K1_map + ro;
+        if (src) asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(src) + 128 * line_i));
+    }
+}
+
 template <typename T, int LX, int XV>
 __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, unsigned int total)
 {
@@ -868,36 +902,9 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
         for (int m = t; m < LX; m += TPL) cp_async_cpx<T>(&line[A(m)], &src[m], true);
     }
     cp_async_commit();
-    // without staging: L2 prefetch of the rows the per-cell phase reads from DRAM (this row and the
-    // z + 1 row of M, the update base, the earlier stage evaluations, the material maps), so that
-    // they arrive while the inverse transform runs. Every prefetched address lies inside its row.
-    if (!a.staged && (a.mode != BM_MODE_UPDATE || a.Mbase != a.Min)) {
-        const int nx = a.nx, ny = a.ny, nz = a.nz;
-        const long long n = a.n;
-        const int lpr = (int)((nx * sizeof(T) + 127) / 128);   // 128-byte lines per row
-        const StageLayout L = stage_layout(a);
-        const int nzr = L.ns > 1 ? 3 : 0;                        // z + 1 rows of M
-        const int nev = (a.mode == BM_MODE_HEFF) ? 0 : a.nev;
-        const int o_mb = 3 + nzr, o_ev = o_mb + 3 * L.mb, o_ms = o_ev + 3 * nev, o_k1 = o_ms + L.ms;
-        const int nrow = o_k1 + L.k1;
-        const int lsh = 32 - __clz(lpr - 1), lpr2 = 1 << lsh;   // lines per row rounded up to a power of two
-        for (int job = tid; job < rpb * nrow * lpr2; job += blockDim.x) {
-            const int line_i = job & (lpr2 - 1), rk = job >> lsh;
-            if (line_i >= lpr) continue;
-            const int r = rpb == 1 ? 0 : rk / nrow, k = rk - r * nrow;
-            const int row = r0 + r;
-            if (row >= nrows) continue;
-            const long long ro = (long long)row * nx;
-            const T *src = nullptr;
-            if (k < 3) src = a.Min + k * n + ro;
-            else if (k < o_mb) src = (row + ny < nrows) ? a.Min + (k - 3) * n + ro + (long long)ny * nx : nullptr;
-            else if (k < o_ev) src = a.Mbase + (k - o_mb) * n + ro;
-            else if (k < o_ms) src = a.ev[(k - o_ev) / 3] + ((k - o_ev) % 3) * n + ro;
-            else if (k < o_k1) src = a.Ms_map + ro;
-            else src = a.K1_map + ro;
-            if (src) asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(src) + 128 * line_i));
-        }
-    }
+    // without staging: L2 prefetch of the rows the per-cell phase reads from DRAM, so that they arrive
+    // while the inverse transform runs
+    if (!a.staged && (a.mode != BM_MODE_UPDATE || a.Mbase != a.Min)) stage_prefetch_rows<T>(a, r0);
     // group 2: the per-cell input rows, arriving while the inverse transform runs
     AccStaged<T> st;
     if (a.staged) {
