@@ -462,7 +462,8 @@ class Context:
         """Autotuned tile shapes: 2D y width, 3D y width and variant (1: radix-16 Stockham, 2: two-level
         register transform fed by pipelined bulk tensor copies), z width,
         stage rows per block (negative when the per-cell rows are prefetched), stage x-transform
-        variant (1: radix-8 Stockham), yzy (1: the fused y -> z -> y cluster pass of a 3D mesh)."""
+        variant (1: radix-8 Stockham, 2: radix-16 Stockham, 3: radix 16 at the lower FP32 register
+        cap), yzy (1: the fused y -> z -> y cluster pass of a 3D mesh)."""
         t = (ctypes.c_int * 4)()
         _check(lib().bm_tiles(self._h, mesh, t))
         sgn = -1 if t[3] < 0 else 1

@@ -573,7 +573,7 @@ int tune_grid_x(bm_ctx *c, Mesh &G)
     h.Hout = tmp;
     float best = 1e30f; int br = G.rpb, bx = G.xv;
     const int rows = G.ny * G.nz;
-    for (int xv = 0; xv <= (stage_reg_q(G.LX, 2) ? 2 : 1); xv++)
+    for (int xv = 0; xv <= (stage_reg_q(G.LX, 2) ? (sizeof(T) == 4 ? 3 : 2) : 1); xv++)
         for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
             const int tpl = stage_reg_q(G.LX, xv) ? stage_reg_q(G.LX, xv) : G.px.tpl;
             if (((3 * rpb * tpl + 31) & ~31) > lim) break;
@@ -668,7 +668,7 @@ int autotune_mesh(bm_ctx *c, Mesh &m)
         const bool reg = stage_reg_q(m.LX, 1) != 0;
         // x-transform variant x rows per block x (per-cell rows prefetched to shared memory or
         // read from global); variants and staging apply to the register kernels only
-        for (int xv = 0; xv <= (stage_reg_q(m.LX, 2) ? 2 : reg ? 1 : 0); xv++)
+        for (int xv = 0; xv <= (stage_reg_q(m.LX, 2) ? (sizeof(T) == 4 ? 3 : 2) : reg ? 1 : 0); xv++)
             for (int stg = 0; stg <= (reg ? 1 : 0); stg++)
                 for (int rpb = 1; rpb <= 16 && rpb <= rows; rpb++) {
                     const int tpl = stage_reg_q(m.LX, xv) ? stage_reg_q(m.LX, xv) : m.px.tpl;
@@ -970,7 +970,8 @@ int prepare_T(bm_ctx *c)
             const char *sr = getenv("BM_STAGE_ROWS");
             m.staged = (sr && sr[0] == '1') ? 1 : 0;
             const char *sx = getenv("BM_STAGE_XV");
-            m.xv = (sx && sx[0] == '1' && stage_reg_q(m.LX, 1)) ? 1 : (sx && sx[0] == '2' && stage_reg_q(m.LX, 2)) ? 2 : 0;
+            m.xv = (sx && sx[0] == '1' && stage_reg_q(m.LX, 1)) ? 1 : (sx && sx[0] == '2' && stage_reg_q(m.LX, 2)) ? 2
+                 : (sx && sx[0] == '3' && stage_reg_q(m.LX, 2)) ? 3 : 0;
             const char *sy = getenv("BM_Y_XV");
             m.yv = (sy && sy[0] == '1' && ypass_has_st(m.Ny) && m.nz > 1 && ypass_st_threads(m.Ny, m.Wy) % 32 == 0) ? 1 : 0;
             if (sy && sy[0] == '2' && m.nz > 1) {

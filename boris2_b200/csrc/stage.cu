@@ -662,6 +662,11 @@ __global__ void __launch_bounds__(bm_lb<T>::v) k_stage_batch(const StageArgs<T> 
 #ifndef BM_RX_MAXNREG_F
 #define BM_RX_MAXNREG_F 64
 #endif
+// xv 3: the radix-16 kernel of xv 2 at a lower FP32 cap (12 instead of 10 resident 96-thread
+// blocks per SM, more spills); the autotuner times both
+#ifndef BM_RX16_LO_MAXNREG_F
+#define BM_RX16_LO_MAXNREG_F 56
+#endif
 
 template <int P> struct addrP {
     __device__ __forceinline__ int operator()(int e) const { return e + e / P; }
@@ -1028,6 +1033,13 @@ __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx16
     stage_reg_body<T, LX, 2>(a, blockIdx.x, gridDim.x);
 }
 
+template <typename T, int LX>
+__global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX16_LO_MAXNREG_F) k_stage_rx16_lo(StageArgs<T> a)
+{
+    if (stage_gated_out<T>(a.st, a.gate)) return;
+    stage_reg_body<T, LX, 2>(a, blockIdx.x, gridDim.x);
+}
+
 // many meshes with the same x length in one launch (radix-8 transform): work item (mesh, row
 // block); the error-norm maximum and the step bookkeeping follow k_stage_batch
 template <typename T, int LX>
@@ -1042,7 +1054,7 @@ __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx_b
 template <typename T, int LX, int XV>
 static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
 {
-    using C = xr_cfg<LX, XV>;
+    using C = xr_cfg<LX, XV == 3 ? 2 : XV>;
     int nt = (3 * a.rpb * C::TPL + 31) & ~31;   // whole warps: the error-norm reduction shuffles full warps
     if (nt > bm_lb<T>::v) return 203;
     size_t smem = (size_t)3 * a.rpb * C::LSP * sizeof(cpx<T>);
@@ -1058,7 +1070,8 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
     void (*kern)(StageArgs<T>);
     if constexpr (XV == 0) kern = k_stage_reg<T, LX>;
     else if constexpr (XV == 1) kern = k_stage_rx<T, LX>;
-    else kern = k_stage_rx16<T, LX>;
+    else if constexpr (XV == 2) kern = k_stage_rx16<T, LX>;
+    else kern = k_stage_rx16_lo<T, LX>;
     if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return 2000 + (int)e;   // the shared-memory ceiling was refused
@@ -1072,6 +1085,7 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
 // x lengths with a register kernel and their threads per line
 int stage_reg_q(int LX, int xv)
 {
+    if (xv == 3) xv = 2;   // the radix-16 kernel at the lower register cap: the same shape
     switch (LX) {
     case 16: return xv == 2 ? 0 : xv ? 2 : 4;
     case 32: return xv == 2 ? 0 : xv ? 4 : 8;
@@ -1089,7 +1103,11 @@ int stage_reg_q(int LX, int xv)
 template <typename T, int LX> static int launch_stage_xv(const StageArgs<T> &a, cudaStream_t s)
 {
     if constexpr (LX >= 256) {
-        if (a.xv == 2) return launch_stage_reg<T, LX, 2>(a, s);
+        // xv 3 is its own kernel for FP32 only (the FP64 cap is the same for both)
+        if constexpr (sizeof(T) == 4) {
+            if (a.xv == 3) return launch_stage_reg<T, LX, 3>(a, s);
+        }
+        if (a.xv == 2 || a.xv == 3) return launch_stage_reg<T, LX, 2>(a, s);
     }
     return a.xv ? launch_stage_reg<T, LX, 1>(a, s) : launch_stage_reg<T, LX, 0>(a, s);
 }

@@ -333,8 +333,9 @@ int bm_time_demag(bm_ctx *ctx, int mesh, int reps, double *ms);
  * when the 3D y passes use the radix-16 Stockham transform, plus 200 when they are the persistent
  * kernels fed by pipelined bulk tensor copies),
  * z-pass width (plus 1000 when the fused y -> z -> y cluster pass replaces the three 3D passes), stage rows per block (plus 100 when the stage kernel uses the radix-8
- * Stockham x transform; negative when it prefetches its per-cell rows into shared
- * memory)]. Valid after the first compute or run. */
+ * Stockham x transform, 200 the radix-16 one, 300 the radix-16 one at the lower FP32 register
+ * cap; negative when it prefetches its per-cell rows into shared memory)]. Valid after the first
+ * compute or run. */
 int bm_tiles(bm_ctx *ctx, int mesh, int *tiles4);
 
 /* Test hooks (used by the test suite only). */

@@ -267,13 +267,15 @@ def test_ymid2d_register_every_length(bm, ny, W, prec, tol, monkeypatch):
 
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
 @pytest.mark.parametrize("nx", [256, 512, 1024])
-def test_stage_radix16_lengths(bm, nx, prec, tol, monkeypatch):
+@pytest.mark.parametrize("xv", ["2", "3"])
+def test_stage_radix16_lengths(bm, nx, prec, tol, xv, monkeypatch):
     """The radix-16 Stockham x transform of the stage kernel (16 values and half the threads per
     line; radix tails 16x16, 16x16x2, 16x16x4) against the oracle with demag, exchange, iDMI,
     anisotropy and Zeeman, for a power-of-two nx and an odd one: RKDP54 with step control in FP64,
-    fixed-step RK4 in mixed precision (an FP32 adaptive trajectory may choose other steps)."""
+    fixed-step RK4 in mixed precision (an FP32 adaptive trajectory may choose other steps). Variant
+    3 is the same kernel body compiled at the lower FP32 register cap."""
     monkeypatch.setenv("BM_TILES", "1,4,8,1")
-    monkeypatch.setenv("BM_STAGE_XV", "2")
+    monkeypatch.setenv("BM_STAGE_XV", xv)
     for n in [(nx, 3, 2), (nx - 1, 2, 2)]:
         N = n[0] * n[1] * n[2]
         mesh = dict(n=n, h=(2e-9, 2e-9, 2e-9), Ms=1.1e6, A=1.5e-11, D=1.5e-3, alpha=0.1, K1=5e5,
@@ -291,5 +293,5 @@ def test_stage_radix16_lengths(bm, nx, prec, tol, monkeypatch):
         t = c.tiles()
         m = c.get_m()
         c.close()
-        assert t["stage_xv"] == 2
+        assert t["stage_xv"] == int(xv)
         assert np.abs(m - s.get_m()).max() / 1.1e6 < tol
