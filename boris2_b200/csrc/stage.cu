@@ -206,16 +206,25 @@ __device__ __forceinline__ double ev_sum_d(const Acc &acc, const double *cev, in
     return sum;
 }
 
-template <typename T, typename AddrF, typename Acc>
+// SPEC 1: the plain stage update (stage_plain on the host): mode, the outputs written and the demag
+// and exchange terms are compile-time, so their run-time checks leave the per-cell loop
+template <typename T, int SPEC = 0, typename AddrF, typename Acc>
 __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, int LSP, AddrF addr, int r0, double &lmax,
                                             const Acc &acc)
 {
+    constexpr bool PS = SPEC == 1;
     const int nx = a.nx, ny = a.ny, nz = a.nz, rpb = a.rpb;
     const int nrows = ny * nz;
     const int tid = threadIdx.x, nt = blockDim.x;
     const long long n = a.n;
-    const bool fields = (a.mode != BM_MODE_UPDATE);
-    const bool demag = fields && (a.modules & BM_MOD_DEMAG);
+    const int mode = PS ? BM_MODE_STAGE : a.mode;
+    const T *Hd = PS ? nullptr : a.Hd;
+    T *Hsave = PS ? nullptr : a.Hsave;
+    T *Ysave = PS ? nullptr : a.Ysave;
+    T *copy_to = PS ? nullptr : a.copy_to;
+    const bool has_ev_out = PS || a.ev_out, has_Mout = PS || a.Mout, do_xfwd = PS || a.do_xfwd;
+    const bool fields = PS || (mode != BM_MODE_UPDATE);
+    const bool demag = PS || (fields && (a.modules & BM_MOD_DEMAG));
     const double dT = a.st ? *((volatile double *)&a.st->dT) : 0.0;
     T Ha[3] = {0, 0, 0};
     if (fields && (a.modules & BM_MOD_ZEEMAN) && a.Ha && a.nHa > 0) {
@@ -231,7 +240,7 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         }
         Ha[0] = (T)a.Ha[3 * hi]; Ha[1] = (T)a.Ha[3 * hi + 1]; Ha[2] = (T)a.Ha[3 * hi + 2];
     }
-    const bool exch = fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
+    const bool exch = PS || (fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI)));
     const bool idmi = (a.modules & BM_MOD_IDMI) != 0;
     const bool zflat = (nz == 1);
     const int nev = a.nev;
@@ -261,9 +270,9 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
                 for (int c = 0; c < 3; c++) H[c] += a.scale * sp[c * cstride];
             }
-            if (a.Hd) {
+            if (Hd) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) H[c] += (a.Hd + cell)[c * n];
+                for (int c = 0; c < 3; c++) H[c] += (Hd + cell)[c * n];
             }
             const bool hxp = x + 1 < nx, hxm = x > 0, hyp = y + 1 < ny, hym = y > 0, hzp = z + 1 < nz, hzm = z > 0;
             if (exch && hxp && hxm && hyp && hym && (zflat || (hzp && hzm))) {
@@ -362,14 +371,14 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
                 for (int c = 0; c < 3; c++) H[c] += s * a.ea[c];
             }
-            if (a.mode == BM_MODE_HEFF) {
+            if (mode == BM_MODE_HEFF) {
 #pragma unroll
                 for (int c = 0; c < 3; c++) (a.Hout + cell)[c * n] = H[c];
                 return;
             }
-            if (a.Hsave) {
+            if (Hsave) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) (a.Hsave + cell)[c * n] = H[c];
+                for (int c = 0; c < 3; c++) (Hsave + cell)[c * n] = H[c];
             }
             T mxh[3] = {m[1] * H[2] - m[2] * H[1], m[2] * H[0] - m[0] * H[2], m[0] * H[1] - m[1] * H[0]};
             T mu[3] = {m[0] * iMs, m[1] * iMs, m[2] * iMs};
@@ -377,7 +386,7 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
             for (int c = 0; c < 3; c++) rhs[c] = a.llg_pre * (mxh[c] + a.alpha * mmxh[c]);
         }
-        if (a.mode == BM_MODE_LTE) {
+        if (mode == BM_MODE_LTE) {
             // 4th-order prediction from the previous step's stages (FSAL), error in FP64
             double d2 = 0.0, m2 = 0.0;
             double sb[3], sa[3];
@@ -448,9 +457,9 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
             for (int c = 0; c < 3; c++) mn[c] = acc.mb(r, c, x, cell) + sum[c];
         }
-        if (a.Ysave) {
+        if (Ysave) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) (a.Ysave + cell)[c * n] = mn[c];
+            for (int c = 0; c < 3; c++) (Ysave + cell)[c * n] = mn[c];
         }
         if (a.renorm) {
             T f = Ms / sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
@@ -458,19 +467,19 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             // the step's new state must be finite (the sum is non-finite if any component is)
             if (!isfinite(mn[0] + mn[1] + mn[2]) && a.st) atomicOr(&a.st->error, BM_ERR_NONFINITE);
         }
-        if (a.ev_out) {
+        if (has_ev_out) {
 #pragma unroll
             for (int c = 0; c < 3; c++) (a.ev_out + cell)[c * n] = rhs[c];
         }
-        if (a.copy_to) {
+        if (copy_to) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) (a.copy_to + cell)[c * n] = m[c];
+            for (int c = 0; c < 3; c++) (copy_to + cell)[c * n] = m[c];
         }
-        if (a.Mout) {
+        if (has_Mout) {
 #pragma unroll
             for (int c = 0; c < 3; c++) (a.Mout + cell)[c * n] = mn[c];
         }
-        if (a.do_xfwd) {
+        if (do_xfwd) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 sp[c * cstride] = mn[c];
@@ -490,13 +499,13 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 
 // LTE block reduction and the last-block bookkeeping (step finish / controller / restore flag)
 // total: launch items that each call the tail once (blocks, or work items of a batched launch)
-template <typename T>
+template <typename T, int SPEC = 0>
 __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, unsigned int total)
 {
     __shared__ double red[32];
     __shared__ int is_last;
     const int tid = threadIdx.x, nt = blockDim.x;
-    if (a.mode == BM_MODE_LTE) {
+    if (SPEC != 1 && a.mode == BM_MODE_LTE) {
         for (int o = 16; o > 0; o >>= 1) {
             double v = __shfl_xor_sync(0xffffffffu, lmax, o);
             if (v > lmax) lmax = v;
@@ -882,7 +891,7 @@ __device__ __forceinline__ void stage_prefetch_rows(const StageArgs<T> &a, int r
     }
 }
 
-template <typename T, int LX, int XV>
+template <typename T, int LX, int XV, int SPEC = 0>
 __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, unsigned int total)
 {
     extern __shared__ unsigned char smraw[];
@@ -898,7 +907,7 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
     const int qc = rpb == 1 ? q : q / rpb, qr = q - qc * rpb;
     const bool qact = (q < 3 * rpb) && (r0 + qr < nrows);
     cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
-    const bool demag = (a.mode != BM_MODE_UPDATE) && (a.modules & BM_MOD_DEMAG);
+    const bool demag = SPEC == 1 || ((a.mode != BM_MODE_UPDATE) && (a.modules & BM_MOD_DEMAG));
     const int half = (a.nx + 1) >> 1;   // packed elements that carry mesh cells
     // group 1: the spectrum rows
     if (demag && qact) {
@@ -964,7 +973,7 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
     if (demag) {
         cp_async_wait_group<1>();
         __syncthreads();
-        if (a.es_fold) {
+        if (SPEC != 1 && a.es_fold) {
             // evaluation speedup: an extrapolating evaluation turns the row of X[M] into the
             // extrapolated field's row (the k_es_extrap sum, formed here so the spectrum is not
             // written and read back); kept out of line so the hot path's registers are untouched
@@ -980,9 +989,9 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
     cp_async_wait_group<0>();
     __syncthreads();
     double lmax = 0.0;
-    if (a.staged) stage_cells<T>(a, sm, LSP, A, r0, lmax, st);
-    else stage_cells<T>(a, sm, LSP, A, r0, lmax, AccGlobal<T>(a));
-    if (a.do_xfwd) {
+    if (SPEC != 1 && a.staged) stage_cells<T>(a, sm, LSP, A, r0, lmax, st);
+    else stage_cells<T, SPEC>(a, sm, LSP, A, r0, lmax, AccGlobal<T>(a));
+    if (SPEC == 1 || a.do_xfwd) {
         for (int idx = tid; idx < 3 * rpb * (LX / 2); idx += blockDim.x) {
             int qq = idx / (LX / 2), mm = idx - qq * (LX / 2);
             if (mm >= half) sm[qq * LSP + A(mm)] = mk<T>(0, 0);
@@ -1009,7 +1018,7 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
             }
         }
     }
-    stage_tail<T>(a, lmax, total);
+    stage_tail<T, SPEC>(a, lmax, total);
 }
 
 template <typename T, int LX>
@@ -1026,18 +1035,27 @@ __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx(S
     stage_reg_body<T, LX, 1>(a, blockIdx.x, gridDim.x);
 }
 
-template <typename T, int LX>
+template <typename T, int LX, int SPEC>
 __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx16(StageArgs<T> a)
 {
     if (stage_gated_out<T>(a.st, a.gate)) return;
-    stage_reg_body<T, LX, 2>(a, blockIdx.x, gridDim.x);
+    stage_reg_body<T, LX, 2, SPEC>(a, blockIdx.x, gridDim.x);
 }
 
-template <typename T, int LX>
+template <typename T, int LX, int SPEC>
 __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX16_LO_MAXNREG_F) k_stage_rx16_lo(StageArgs<T> a)
 {
     if (stage_gated_out<T>(a.st, a.gate)) return;
-    stage_reg_body<T, LX, 2>(a, blockIdx.x, gridDim.x);
+    stage_reg_body<T, LX, 2, SPEC>(a, blockIdx.x, gridDim.x);
+}
+
+// the plain stage update of the RK stages (the radix-16 kernels' SPEC 1): stage mode, exchange and
+// demag on, the rhs and new M written, the new M's x transform; no saved fields or states, no
+// external field, no copy, no staging, no folded extrapolation
+template <typename T> static bool stage_plain(const StageArgs<T> &a)
+{
+    return a.mode == BM_MODE_STAGE && !a.staged && !a.es_fold && !a.Hd && !a.Hsave && !a.Ysave && !a.copy_to && a.ev_out &&
+           a.Mout && a.do_xfwd && (a.modules & BM_MOD_DEMAG) && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
 }
 
 // many meshes with the same x length in one launch (radix-8 transform): work item (mesh, row
@@ -1070,8 +1088,8 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
     void (*kern)(StageArgs<T>);
     if constexpr (XV == 0) kern = k_stage_reg<T, LX>;
     else if constexpr (XV == 1) kern = k_stage_rx<T, LX>;
-    else if constexpr (XV == 2) kern = k_stage_rx16<T, LX>;
-    else kern = k_stage_rx16_lo<T, LX>;
+    else if constexpr (XV == 2) kern = stage_plain(b) ? k_stage_rx16<T, LX, 1> : k_stage_rx16<T, LX, 0>;
+    else kern = stage_plain(b) ? k_stage_rx16_lo<T, LX, 1> : k_stage_rx16_lo<T, LX, 0>;
     if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return 2000 + (int)e;   // the shared-memory ceiling was refused
