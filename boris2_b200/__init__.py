@@ -463,12 +463,14 @@ class Context:
         register transform fed by pipelined bulk tensor copies), z width,
         stage rows per block (negative when the per-cell rows are prefetched), stage x-transform
         variant (1: radix-8 Stockham, 2: radix-16 Stockham, 3: radix 16 at the lower FP32 register
-        cap), yzy (1: the fused y -> z -> y cluster pass of a 3D mesh)."""
+        cap), yzy (1: the fused y -> z -> y cluster pass of a 3D mesh), z-pass variant (1: the parity
+        split, two threads per pencil line)."""
         t = (ctypes.c_int * 4)()
         _check(lib().bm_tiles(self._h, mesh, t))
         sgn = -1 if t[3] < 0 else 1
         return {"ymid2d_W": t[0], "ypass_W": t[1] % 100, "ypass_yv": t[1] // 100, "zmid_W": t[2] % 1000,
-                "yzy": t[2] // 1000, "stage_rows": sgn * (abs(t[3]) % 100), "stage_xv": abs(t[3]) // 100}
+                "yzy": (t[2] // 1000) % 10, "zmid_zv": t[2] // 10000, "stage_rows": sgn * (abs(t[3]) % 100),
+                "stage_xv": abs(t[3]) // 100}
 
     def stats(self):
         st = Stats()

@@ -73,6 +73,7 @@ struct Mesh {
     FFTPlan px, py, pz;
     int W2 = 1, Wy = 1, Wz = 1, rpb = 1, staged = 0, xv = 0, yv = 0;
     int yzy = 0;                // 3D: the fused y -> z -> y cluster pass instead of three launches
+    int zv = 0;                 // 3D z pass: 1 the parity split (two threads per pencil line)
     // device (element type depends on the context precision)
     void *buf[4] = {nullptr, nullptr, nullptr, nullptr};   // A (M), P (sM1), B, C
     void *ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -614,15 +615,21 @@ void tune_grid_yz(bm_ctx *c, Mesh &m)
         } else {
             tune_ypass<T>(c, m);
             a.yv = m.yv;
-            float best = 1e30f; int bw = m.Wz;
+            float best = 1e30f; int bw = m.Wz, bzv = 0;
             for (int W = 4; W <= 128 && W <= m.LX; W *= 2) {
                 if (zmid_has_reg(m.Nz) ? (zmid_reg_smem<T>(m.Nz, W) > 200 * 1024 || 6 * W > lim)
                                        : (zmid_smem<T>(m.Nz, W) > 200 * 1024 || 2 * W * m.pz.tpl > lim)) continue;
                 a.W = W;
-                float t = time_launches(s, [&]() { return launch_zmid<T>(a, s); }, reps);
-                if (t < best) { best = t; bw = W; }
+                // one thread per pencil line, and the parity split where it applies
+                for (int zv = 0; zv <= (zmid_has_par(m.Nz, W) ? 1 : 0); zv++) {
+                    a.zv = zv;
+                    float t = time_launches(s, [&]() { return launch_zmid<T>(a, s); }, reps);
+                    if (t < best) { best = t; bw = W; bzv = zv; }
+                }
             }
+            a.zv = 0;
             m.Wz = bw;
+            m.zv = bzv;
             // the fused cluster pass, where it applies, against the three tuned launches
             // (BM_YZY=0 keeps the three launches)
             const char *sz = getenv("BM_YZY");
@@ -979,6 +986,8 @@ int prepare_T(bm_ctx *c)
                 ya.W = m.Wy;
                 if (ypass_tma_fits<T>(ya)) m.yv = 2;
             }
+            const char *szv = getenv("BM_Z_XV");
+            m.zv = (szv && szv[0] == '1' && m.nz > 1 && zmid_has_par(m.Nz, m.Wz)) ? 1 : 0;
             const char *sz = getenv("BM_YZY");
             m.yzy = 0;
             if (sz && sz[0] == '1' && m.nz > 1 && m.ml_role == 0 && (m.modules & BM_DEMAG) && !c->batched)
@@ -1123,6 +1132,7 @@ YZArgs<T> yz_args(bm_ctx *c, Mesh &m, int gate)
     a.W = m.nz > 1 ? m.Wy : m.W2;
     a.st = c->st; a.gate = gate;
     a.yv = m.yv;
+    a.zv = m.zv;
     return a;
 }
 
@@ -3197,7 +3207,7 @@ int bm_tiles(bm_ctx *c, int mesh, int *tiles4)
     if (int rc = check_mesh(c, mesh)) return rc;
     if (!tiles4) return fail(BM_EINVAL, "null out");
     Mesh &m = c->meshes[mesh];
-    tiles4[0] = m.W2; tiles4[1] = m.Wy + 100 * m.yv; tiles4[2] = m.Wz + 1000 * m.yzy; tiles4[3] = (m.staged ? -1 : 1) * (m.rpb + 100 * m.xv);
+    tiles4[0] = m.W2; tiles4[1] = m.Wy + 100 * m.yv; tiles4[2] = m.Wz + 1000 * m.yzy + 10000 * m.zv; tiles4[3] = (m.staged ? -1 : 1) * (m.rpb + 100 * m.xv);
     return 0;
 }
 

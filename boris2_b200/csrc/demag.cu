@@ -514,6 +514,214 @@ bool zmid_has_reg(int Nz)
     return Nz == 4 || Nz == 6 || Nz == 8 || Nz == 12 || Nz == 16 || Nz == 24 || Nz == 32 || Nz == 48 || Nz == 64;
 }
 
+// ------------------------------------------------------------------------------ 3D z pass, parity split
+// The register z pass with each pencil's even and odd kz in two threads, so a thread holds Nz/2
+// values instead of Nz (fewer registers, twice the resident warps). With the upper half of the
+// padded input zero, X[2k + h] = DFT_{Nz/2}( x[e] w_Nz^(e h) )[k] for parity h; each thread forms
+// its own output component for its Nz/2 values of kz from the shared forward spectra, and inverts:
+// z_h[e] = w_Nz^(-e h) IDFT_{Nz/2}(Y_h)[e]; the pencil's inverse is z_0 + z_1, each thread adding
+// half of the outputs through shared memory. The block is two groups of whole warps, one per
+// parity (G threads each: the 6 W threads (c, p, w), w fastest, rounded up to warps), so both
+// parities run compile-time code paths. Shared memory and the kernel tile are those of
+// zmid_reg_body.
+template <typename T, int NZ, int HP>
+__device__ __forceinline__ void zpar_forward(const YZArgs<T> &a, cpx<T> *v, bool own, long long gbase, long long gstride, int nz)
+{
+    constexpr int H = NZ / 2;
+#pragma unroll
+    for (int e = 0; e < H; e++) v[e] = mk<T>(0, 0);
+    if (own) {
+#pragma unroll
+        for (int e = 0; e < H; e++)
+            if (e < nz) v[e] = a.S2[gbase + e * gstride];
+    }
+    if (HP) {
+#pragma unroll
+        for (int e = 1; e < H; e++) v[e] = cmul(v[e], a.twz[e]);
+    }
+    RegFFT<T, H, false>::run(v, a.twz, 2);
+}
+
+template <typename T, int NZ, int HP, int WC>
+__device__ __forceinline__ void zpar_product(const YZArgs<T> &a, cpx<T> *v, const cpx<T> *sm, const T *Ks, const T *Kn, cpx<T> *O,
+                                             int c, int p, int w, int kx, bool single, int W)
+{
+    constexpr int H = NZ / 2, KZ1 = NZ / 2 + 1;
+    auto S = [&](int cc, int pp, int e) -> cpx<T> { return sm[((cc * 2 + pp) * NZ + e) * W + w]; };
+    const int q0 = c == 0 ? 0 : c == 1 ? 3 : 4;
+    const int q1 = c == 0 ? 3 : c == 1 ? 1 : 5;
+    const int q2 = c == 0 ? 4 : c == 1 ? 5 : 2;
+    auto has_y = [](int q) { return q == 3 || q == 5; };
+    auto has_z = [](int q) { return q == 4 || q == 5; };
+    if (kx != 0) {
+        const T sy = p ? (T)-1 : (T)1;
+        const T y0 = has_y(q0) ? sy : (T)1, y1 = has_y(q1) ? sy : (T)1, y2 = has_y(q2) ? sy : (T)1;
+        const T z0 = has_z(q0) ? (T)-1 : (T)1, z1 = has_z(q1) ? (T)-1 : (T)1, z2 = has_z(q2) ? (T)-1 : (T)1;
+#pragma unroll
+        for (int k = 0; k < H; k++) {
+            const int kz = 2 * k + HP;
+            const int akz = kz <= NZ / 2 ? kz : NZ - kz;
+            const bool neg = kz > NZ / 2;
+            const T a0 = (neg ? y0 * z0 : y0) * Ks[(q0 * KZ1 + akz) * W + w];
+            const T a1 = (neg ? y1 * z1 : y1) * Ks[(q1 * KZ1 + akz) * W + w];
+            const T a2 = (neg ? y2 * z2 : y2) * Ks[(q2 * KZ1 + akz) * W + w];
+            const cpx<T> m0 = S(0, p, kz), m1 = S(1, p, kz), m2 = S(2, p, kz);
+            v[k] = mk<T>(a0 * m0.x + a1 * m1.x + a2 * m2.x, a0 * m0.y + a1 * m1.y + a2 * m2.y);
+        }
+    } else {
+        // the packed column (as zmid_reg_body), for this thread's kz
+        const int pm = single ? 0 : 1 - p;
+        const T zq0 = has_z(q0) ? (T)-1 : (T)1, zq1 = has_z(q1) ? (T)-1 : (T)1, zq2 = has_z(q2) ? (T)-1 : (T)1;
+#pragma unroll 1
+        for (int k = 0; k < H; k++) {
+            const int kz = 2 * k + HP;
+            const int kzm = (NZ - kz) % NZ;
+            const int akz = kz <= NZ / 2 ? kz : NZ - kz;
+            const int kq = single ? (kz <= NZ / 2 ? kz : kzm) : (p == 0 ? kz : kzm);
+            const bool neg = kq > NZ / 2;
+            cpx<T> A[3], B[3];
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) {
+                const cpx<T> C = S(cc, p, kz), cj = conj(S(cc, pm, kzm));
+                A[cc] = cscale(C + cj, (T)0.5);
+                B[cc] = cscale(mul_mi(C - cj), (T)0.5);
+            }
+            const T s0 = neg ? zq0 : (T)1, s1 = neg ? zq1 : (T)1, s2 = neg ? zq2 : (T)1;
+            const T a0 = s0 * Ks[(q0 * KZ1 + akz) * W + w], a1 = s1 * Ks[(q1 * KZ1 + akz) * W + w],
+                    a2 = s2 * Ks[(q2 * KZ1 + akz) * W + w];
+            const T b0 = s0 * Kn[q0 * KZ1 + akz], b1 = s1 * Kn[q1 * KZ1 + akz], b2 = s2 * Kn[q2 * KZ1 + akz];
+            const cpx<T> Ap = mk<T>(a0 * A[0].x + a1 * A[1].x + a2 * A[2].x, a0 * A[0].y + a1 * A[1].y + a2 * A[2].y);
+            const cpx<T> Bp = mk<T>(b0 * B[0].x + b1 * B[1].x + b2 * B[2].x, b0 * B[0].y + b1 * B[1].y + b2 * B[2].y);
+            O[kz] = Ap + mul_i(Bp);
+        }
+#pragma unroll
+        for (int k = 0; k < H; k++) v[k] = O[2 * k + HP];
+    }
+    RegFFT<T, H, true>::run(v, a.twz, 2);
+    if (HP) {
+#pragma unroll
+        for (int e = 1; e < H; e++) {
+            cpx<T> t = a.twz[e];
+            t.y = -t.y;
+            v[e] = cmul(v[e], t);
+        }
+    }
+}
+
+template <typename T, int NZ, int WC>
+__device__ __forceinline__ void zpar_body(const YZArgs<T> &a, int bx, int ky)
+{
+    extern __shared__ unsigned char smraw[];
+    constexpr int H = NZ / 2, KZ1 = NZ / 2 + 1;
+    const int W = WC, Ny = a.Ny, nz = a.nz, LX = a.LX;
+    constexpr int lw = WC == 16 ? 4 : 3;
+    const int Kx1 = LX + 1, Ky1 = Ny / 2 + 1;
+    cpx<T> *sm = reinterpret_cast<cpx<T> *>(smraw);
+    T *Ks = reinterpret_cast<T *>(sm + 6 * NZ * W);
+    T *Kn = Ks + 6 * KZ1 * W;
+    const int kx0 = bx * W;
+    const int kym = (Ny - ky) % Ny;
+    const bool single = (ky == kym);
+    const int np = single ? 1 : 2;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const long long nk = (long long)Kx1 * Ky1 * KZ1;
+    const long long kzs = (long long)Ky1 * Kx1;
+    constexpr int G = ((6 * WC + 31) / 32) * 32;   // threads per parity group
+    const int h = tid >= G ? 1 : 0;                 // warp-uniform
+    const int r = tid - h * G;
+    const int w = r & (W - 1);
+    const int jj = r >> lw;                         // (c, p) row, 0 .. 5 (idle rows past 5)
+    const int kx = kx0 + w;
+    if (h == 0 && jj < 6) {
+        const bool ok = kx < LX;
+        const T *src = a.K + jj * nk + (long long)ky * Kx1 + (ok ? kx : 0);
+#pragma unroll
+        for (int kz = 0; kz < KZ1; kz++) cp_async_real<T>(&Ks[(jj * KZ1 + kz) * W + w], src + kz * kzs, ok);
+    }
+    if (kx0 == 0) {
+        for (int idx = tid; idx < 6 * KZ1; idx += nt) {
+            int kz = idx % KZ1, c = idx / KZ1;
+            cp_async_real<T>(&Kn[c * KZ1 + kz], &a.K[c * nk + kz * kzs + (long long)ky * Kx1 + LX], true);
+        }
+    }
+    const int p = jj & 1, c = jj >> 1;
+    const bool own = (jj < 6) && (p < np) && (kx < LX);
+    const int kyp = p ? kym : ky;
+    const long long gbase = ((long long)c * nz * Ny + kyp) * LX + kx;
+    const long long gstride = (long long)Ny * LX;
+    cpx<T> v[H];
+    if (h == 0) zpar_forward<T, NZ, 0>(a, v, own, gbase, gstride, nz);
+    else zpar_forward<T, NZ, 1>(a, v, own, gbase, gstride, nz);
+    if (jj < 6) {
+#pragma unroll
+        for (int k = 0; k < H; k++) sm[((c * 2 + p) * NZ + 2 * k + h) * W + w] = v[k];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    cpx<T> *O = sm + 6 * NZ * W + ((6 * KZ1 * (W + 1) * sizeof(T) + sizeof(cpx<T>) - 1) / sizeof(cpx<T>)) + (c * 2 + p) * NZ;
+    if (own) {
+        if (h == 0) zpar_product<T, NZ, 0, WC>(a, v, sm, Ks, Kn, O, c, p, w, kx, single, W);
+        else zpar_product<T, NZ, 1, WC>(a, v, sm, Ks, Kn, O, c, p, w, kx, single, W);
+    }
+    __syncthreads();   // every spectrum read before the slab takes the halves
+    // z_0 + z_1: parity h keeps outputs [h H/2, (h + 1) H/2) and hands the other half to its partner
+    // through its (c, p) slab of the spectra (slots e of column w)
+    cpx<T> *X = sm + (size_t)(c * 2 + p) * NZ * W + w;
+    if (own) {
+#pragma unroll
+        for (int e = 0; e < H; e++)
+            if ((e < H / 2) == (h == 1)) X[e * W] = v[e];
+    }
+    __syncthreads();
+    if (own) {
+#pragma unroll
+        for (int e = 0; e < H; e++) {
+            if ((e < H / 2) != (h == 0)) continue;
+            const cpx<T> o = X[e * W];
+            if (e < nz) a.S2[gbase + e * gstride] = v[e] + o;
+        }
+    }
+}
+
+template <typename T, int NZ, int WC>
+__global__ void __launch_bounds__(bm_lb<T>::v) k_zmid_par(YZArgs<T> a)
+{
+    if (gated_out<T>(a.st, a.gate)) return;
+    zpar_body<T, NZ, WC>(a, blockIdx.x, blockIdx.y);
+}
+
+// whether the parity-split z pass applies: Nz 12, 16, 24, 32, 48 or 64, a tile width of 8 or 16
+bool zmid_has_par(int Nz, int W)
+{
+    return (Nz == 12 || Nz == 16 || Nz == 24 || Nz == 32 || Nz == 48 || Nz == 64) && (W == 8 || W == 16);
+}
+
+template <typename T, int NZ, int WC>
+static int launch_zmid_par_w(const YZArgs<T> &a, cudaStream_t s)
+{
+    const int nt = 2 * (((6 * WC + 31) / 32) * 32);   // two parity groups of whole warps
+    if (nt > bm_lb<T>::v) return 104;
+    size_t smem = zmid_reg_smem<T>(NZ, WC);
+    if (smem > 200 * 1024) return 105;
+    if (smem > BM_SMEM_DEFAULT_SAFE) {
+        cudaError_t e = cudaFuncSetAttribute(k_zmid_par<T, NZ, WC>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        if (e != cudaSuccess) return (int)e;
+    }
+    dim3 grid((a.LX + WC - 1) / WC, a.Ny / 2 + 1);
+    k_zmid_par<T, NZ, WC><<<grid, nt, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, int NZ>
+static int launch_zmid_par(const YZArgs<T> &a, cudaStream_t s)
+{
+    switch (a.W) {
+    case 8: return launch_zmid_par_w<T, NZ, 8>(a, s);
+    case 16: return launch_zmid_par_w<T, NZ, 16>(a, s);
+    default: return 104;
+    }
+}
+
 // ------------------------------------------------------------------------------ 3D y passes, two-level register FFT
 // Ny = P * Q (P <= Q <= 32). Stage 1: thread (w, n1) holds x[n1 + P n2], n2 < Q, in registers,
 // does DFT_Q, twiddles by w_Ny^(n1 k2) and writes u[k2][n1] to shared memory. Stage 2: thread
@@ -1163,6 +1371,17 @@ template <typename T> int launch_yinv(const YZArgs<T> &a, cudaStream_t s)
 
 template <typename T> int launch_zmid(const YZArgs<T> &a, cudaStream_t s)
 {
+    if (a.zv == 1 && zmid_has_par(a.Nz, a.W)) {
+        switch (a.Nz) {
+        case 12: return launch_zmid_par<T, 12>(a, s);
+        case 16: return launch_zmid_par<T, 16>(a, s);
+        case 24: return launch_zmid_par<T, 24>(a, s);
+        case 32: return launch_zmid_par<T, 32>(a, s);
+        case 48: return launch_zmid_par<T, 48>(a, s);
+        case 64: return launch_zmid_par<T, 64>(a, s);
+        default: break;
+        }
+    }
     if ((a.W & (a.W - 1)) == 0) {
         switch (a.Nz) {
         case 4: return launch_zmid_reg<T, 4>(a, s);

@@ -40,6 +40,7 @@ struct YZArgs {
     int yv;              // 3D y transform: 0 two-level register kernel, 1 radix-16 Stockham (Ny >= 256),
                          // 2 the two-level kernel fed by bulk tensor copies (persistent, pipelined)
     int pf_ahead;        // set by the launchers: blocks of the grid resident at once (0: no look-ahead prefetch)
+    int zv;              // 3D z pass: 0 one thread per pencil line, 1 the parity split (two threads per line)
 };
 
 // Blocks of a launch resident on the whole GPU at once (occupancy per SM times the SMs), or 0 when
@@ -83,6 +84,7 @@ template <typename T> size_t zmid_reg_smem(int Nz, int W)
     return (size_t)6 * Nz * W * sizeof(cpx<T>) + kb + (size_t)6 * Nz * sizeof(cpx<T>);
 }
 bool zmid_has_reg(int Nz);
+bool zmid_has_par(int Nz, int W);   // lengths and tile widths of the parity-split z pass
 bool ypass_has_reg(int Ny);
 // block-size ceiling of the two-level register y kernel: FP64 lines of 32 values need the registers
 // a 256-thread bound allows

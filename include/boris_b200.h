@@ -332,7 +332,8 @@ int bm_time_demag(bm_ctx *ctx, int mesh, int reps, double *ms);
 /* Tile shapes the autotuner chose for a mesh: [2D y-pass width, 3D y-pass width (plus 100
  * when the 3D y passes use the radix-16 Stockham transform, plus 200 when they are the persistent
  * kernels fed by pipelined bulk tensor copies),
- * z-pass width (plus 1000 when the fused y -> z -> y cluster pass replaces the three 3D passes), stage rows per block (plus 100 when the stage kernel uses the radix-8
+ * z-pass width (plus 1000 when the fused y -> z -> y cluster pass replaces the three 3D passes,
+ * plus 10000 when the z pass is the parity split: two threads per pencil line), stage rows per block (plus 100 when the stage kernel uses the radix-8
  * Stockham x transform, 200 the radix-16 one, 300 the radix-16 one at the lower FP32 register
  * cap; negative when it prefetches its per-cell rows into shared memory)]. Valid after the first
  * compute or run. */
