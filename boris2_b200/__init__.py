@@ -88,6 +88,8 @@ _SIGS = {
     "bm_compute_heff": (_I, [_P, _I, _DP]),
     "bm_run": (_I, [_P, _I, ctypes.POINTER(Stats)]),
     "bm_get_stats": (_I, [_P, ctypes.POINTER(Stats)]),
+    "bm_get_mxh": (_I, [_P, _DP]),
+    "bm_get_dmdt": (_I, [_P, _DP]),
     "bm_mesh_info": (_I, [_P, _I, _IP, _IP]),
     "bm_device_m": (_I, [_P, _I, ctypes.POINTER(_P), _IP]),
     "bm_sync": (_I, [_P]),
@@ -476,6 +478,20 @@ class Context:
         st = Stats()
         _check(lib().bm_get_stats(self._h, ctypes.byref(st)))
         return st.as_dict()
+
+    def get_mxh(self):
+        """The reference's Get_mxh: max over cells of |M x Heff| / |M|^2 at the first evaluation of the
+        last step that computed it (0 before any); the call asks the next step to compute it."""
+        v = ctypes.c_double()
+        _check(lib().bm_get_mxh(self._h, ctypes.byref(v)))
+        return v.value
+
+    def get_dmdt(self):
+        """The reference's Get_dmdt: max over cells of |M - M_step_start| / (dT GAMMA |M|^2) after the
+        last stage of the last step that computed it (0 before any); the call asks the next step."""
+        v = ctypes.c_double()
+        _check(lib().bm_get_dmdt(self._h, ctypes.byref(v)))
+        return v.value
 
     def fft_sizes(self, mesh=0):
         n3 = (ctypes.c_int * 3)()

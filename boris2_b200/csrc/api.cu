@@ -470,6 +470,8 @@ int upload_state(bm_ctx *c)
     h.need_restore = 0;
     h.lte_bits = 0;
     h.blocks_done = 0;
+    h.mxh_acc = 0;
+    h.dmdt_acc = 0;
     CK(cudaMemcpyAsync(c->st, &h, sizeof(StepState), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->state_dirty = false;
@@ -1274,14 +1276,18 @@ int stage_multi(bm_ctx *c, std::vector<StageArgs<T>> &v, int *count)
         }
         return 0;
     }
-    int lk = BM_LAST_NONE;
+    int lk = BM_LAST_NONE, pub = 0;
     for (auto &a : v) if (a.last_kind != BM_LAST_NONE) lk = a.last_kind;
+    for (auto &a : v) if (a.diag & BM_DIAG_PUBLISH) pub = BM_DIAG_PUBLISH;
     std::map<int, std::vector<StageArgs<T>>> groups;   // x length with a register kernel, or 0
     for (auto &a : v) groups[stage_reg_q(a.LX, 1) ? a.LX : 0].push_back(a);
     size_t gi = 0;
     for (auto &kv : groups) {
         const bool last = (++gi == groups.size());
-        for (auto &a : kv.second) a.last_kind = last ? lk : BM_LAST_NONE;
+        for (auto &a : kv.second) {
+            a.last_kind = last ? lk : BM_LAST_NONE;
+            a.diag = (a.diag & ~BM_DIAG_PUBLISH) | (last ? pub : 0);   // every block of the last launch counts
+        }
         if (int rc = stage_batch_one<T>(c, kv.first, kv.second, count)) return rc;
     }
     return 0;
@@ -1758,7 +1764,10 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
             StageArgs<T> a = stage_args<T>(c, m);
             a.mode = BM_MODE_STAGE;
             a.Mbase = B<T>(m, 0);
-            if (s == 0) { a.Min = B<T>(m, 0); a.ev_out = E<T>(m, 0); a.crhs = 0.5; a.Mout = B<T>(m, 2); }
+            if (s == 0) {
+                a.Min = B<T>(m, 0); a.ev_out = E<T>(m, 0); a.crhs = 0.5; a.Mout = B<T>(m, 2);
+                a.diag = BM_DIAG_MXH | (i == nm - 1 ? BM_DIAG_PUBLISH : 0);   // the step's first evaluation
+            }
             else if (s == 1) { a.Min = B<T>(m, 2); a.ev_out = E<T>(m, 1); a.crhs = 0.5; a.Mout = B<T>(m, 3); }
             else if (s == 2) { a.Min = B<T>(m, 3); a.ev_out = E<T>(m, 2); a.crhs = 1.0; a.Mout = B<T>(m, 2); }
             else {
@@ -1769,6 +1778,7 @@ int enqueue_rk4_step(bm_ctx *c, int *count, void *const *cacheX = nullptr, void 
                 a.crhs = 1.0 / 6;
                 a.Mout = B<T>(m, 0);
                 a.renorm = 1;
+                a.diag = BM_DIAG_DMDT | (i == nm - 1 ? BM_DIAG_PUBLISH : 0);   // the step's last stage
                 if (i == nm - 1) a.last_kind = BM_LAST_FINISH;
             }
             if (cacheX) {
@@ -1894,6 +1904,7 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
                 a.lte_embedded = 1;
             }
             a.ev_out = E<T>(m, 0);
+            a.diag = BM_DIAG_MXH | (i == nm - 1 ? BM_DIAG_PUBLISH : 0);   // evaluation 0 at the step's M
             if (i == nm - 1) a.last_kind = BM_LAST_CONTROL;
             es_fold_args<T>(c, m, a);
             v.push_back(a);
@@ -1950,6 +1961,7 @@ int enqueue_rkdp_attempt(bm_ctx *c, int *count)
             else {
                 a.Mout = B<T>(m, 0);
                 a.renorm = 1;
+                a.diag = BM_DIAG_DMDT | (i == nm - 1 ? BM_DIAG_PUBLISH : 0);   // the 5th-order state
                 if (i == nm - 1) a.last_kind = BM_LAST_FINISH;
             }
             es_fold_args<T>(c, m, a);
@@ -2881,6 +2893,29 @@ int bm_get_stats(bm_ctx *c, bm_stats *out)
     }
     return 0;
 }
+
+// ODECommon_Base::Get_mxh / Get_dmdt (Boris/DiffEq_CommonBase_Get.cpp:7,19): the value of the last
+// step that computed it (0 before any), and a request that the next step computes it; only the
+// device's request flag is written, so the rest of the step state stays the device's
+static int get_diag(bm_ctx *c, int which, double *v)
+{
+    if (int rc = check_ctx(c)) return rc;
+    if (!v) return fail(BM_EINVAL, "null output");
+    if (int rc = prepare(c)) return rc;
+    cudaSetDevice(c->device);
+    double val = 0.0;
+    static const int one = 1;
+    const double *src = which ? &c->st->dmdt : &c->st->mxh;
+    int *flag = which ? &c->st->calc_dmdt : &c->st->calc_mxh;
+    CK(cudaMemcpyAsync(&val, src, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(flag, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *v = val;
+    return 0;
+}
+
+int bm_get_mxh(bm_ctx *c, double *mxh) { return get_diag(c, 0, mxh); }
+int bm_get_dmdt(bm_ctx *c, double *dmdt) { return get_diag(c, 1, dmdt); }
 
 int bm_mesh_info(bm_ctx *c, int mesh, int *n3, int *N3)
 {

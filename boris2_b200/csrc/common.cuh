@@ -52,6 +52,11 @@ __device__ __forceinline__ void cp_async_real(T *smem, const T *gmem, bool valid
 // Physical constants (the reference's BorisLib/Funcs_Math_base.h:9,16)
 #define BM_MU0 1.256637061435916e-6
 #define BM_GAMMA 2.212761569e5
+// StageArgs::diag bits: the step's first evaluation (|M x Heff| / |M|^2), its last stage
+// (|M - M_start| / (dT GAMMA |M|^2)), and the set's last launch (publishes the maxima)
+#define BM_DIAG_MXH 1
+#define BM_DIAG_DMDT 2
+#define BM_DIAG_PUBLISH 4
 
 // module bits
 #define BM_MOD_DEMAG 1
@@ -86,4 +91,10 @@ struct StepState {
     int es_mode, es_slot, es_available, es_pad;
     double es_tnew;
     double es_a[6];
+    // torque and dm/dt diagnostics (the reference's Get_mxh / Get_dmdt): calc_* are requests from the
+    // host; the launches that evaluate them take running maxima into *_acc (non-negative doubles as
+    // bits), and the last block of the set's last launch publishes mxh / dmdt and clears both
+    int calc_mxh, calc_dmdt;
+    unsigned long long mxh_acc, dmdt_acc;
+    double mxh, dmdt;
 };

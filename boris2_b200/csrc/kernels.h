@@ -144,6 +144,7 @@ struct StageArgs {
     double cev[6];
     double crhs;
     int renorm, mode, do_xfwd, last_kind, gate;
+    int diag;            // BM_DIAG_* bits: this launch evaluates mxh / dmdt when requested, and publishes
     int lte_embedded;    // LTE mode: the 5th-order solution recomputed in FP64 from the base and cev5 (nev 5)
     double cev5[6];      // LTE mode with lte_embedded: 5th-order weights of the same stage rhs as cev
     long long n;         // cells

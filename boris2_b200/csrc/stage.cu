@@ -206,6 +206,24 @@ __device__ __forceinline__ double ev_sum_d(const Acc &acc, const double *cev, in
     return sum;
 }
 
+// Per-block maxima of the torque and dm/dt diagnostics (non-negative doubles as bits)
+__device__ __forceinline__ unsigned long long *stage_diag_slots()
+{
+    __shared__ unsigned long long slots[2];
+    return slots;
+}
+
+// the BM_DIAG_MXH / BM_DIAG_DMDT bits of this launch that the host requested (the request stays set
+// until the last block of the set's publishing launch clears it, so every block reads the same)
+template <typename T> __device__ __forceinline__ int stage_diag_active(const StageArgs<T> &a)
+{
+    if (!a.diag || !a.st) return 0;
+    int d = 0;
+    if ((a.diag & BM_DIAG_MXH) && *((volatile const int *)&a.st->calc_mxh)) d |= BM_DIAG_MXH;
+    if ((a.diag & BM_DIAG_DMDT) && *((volatile const int *)&a.st->calc_dmdt)) d |= BM_DIAG_DMDT;
+    return d;
+}
+
 // SPEC 1: the plain stage update (stage_plain on the host): mode, the outputs written and the demag
 // and exchange terms are compile-time, so their run-time checks leave the per-cell loop
 template <typename T, int SPEC = 0, typename AddrF, typename Acc>
@@ -243,6 +261,14 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
     const bool exch = PS || (fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI)));
     const bool idmi = (a.modules & BM_MOD_IDMI) != 0;
     const bool zflat = (nz == 1);
+    // torque / dm/dt diagnostics of this launch (meshes with grel = 0 take no part, as in the
+    // reference's reductions)
+    const int dg = (a.grel != (T)0) ? stage_diag_active(a) : 0;
+    unsigned long long *dslot = stage_diag_slots();
+    if (stage_diag_active(a)) {
+        if (tid == 0) { dslot[0] = 0ull; dslot[1] = 0ull; }
+        __syncthreads();
+    }
     const int nev = a.nev;
     T cev[6];
 #pragma unroll
@@ -381,6 +407,12 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 for (int c = 0; c < 3; c++) (Hsave + cell)[c * n] = H[c];
             }
             T mxh[3] = {m[1] * H[2] - m[2] * H[1], m[2] * H[0] - m[0] * H[2], m[0] * H[1] - m[1] * H[0]};
+            if (dg & BM_DIAG_MXH) {
+                // |M x Heff| / |M|^2 (DiffEqFM_EvalsCUDA_RKDP54.cu:31-32, DiffEqFM_EvalsLLGCUDA.cu:445-446)
+                const double x2 = (double)mxh[0] * mxh[0] + (double)mxh[1] * mxh[1] + (double)mxh[2] * mxh[2];
+                const double m2 = (double)m[0] * m[0] + (double)m[1] * m[1] + (double)m[2] * m[2];
+                atomicMax(&dslot[0], (unsigned long long)__double_as_longlong(sqrt(x2) / m2));
+            }
             T mu[3] = {m[0] * iMs, m[1] * iMs, m[2] * iMs};
             T mmxh[3] = {mu[1] * mxh[2] - mu[2] * mxh[1], mu[2] * mxh[0] - mu[0] * mxh[2], mu[0] * mxh[1] - mu[1] * mxh[0]};
 #pragma unroll
@@ -467,6 +499,18 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             // the step's new state must be finite (the sum is non-finite if any component is)
             if (!isfinite(mn[0] + mn[1] + mn[2]) && a.st) atomicOr(&a.st->error, BM_ERR_NONFINITE);
         }
+        if (dg & BM_DIAG_DMDT) {
+            // |M - M_start| / (dT GAMMA |M|^2) after the last stage (DiffEqFM_EvalsLLGCUDA.cu:583-584,
+            // DiffEqFM_EvalsCUDA_RKDP54.cu:216-217); the step base is read before this cell's M is written
+            double d2 = 0.0, m2 = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const double d = (double)mn[c] - (double)acc.mb(r, c, x, cell);
+                d2 += d * d;
+                m2 += (double)mn[c] * mn[c];
+            }
+            atomicMax(&dslot[1], (unsigned long long)__double_as_longlong(sqrt(d2) / (dT * BM_GAMMA * m2)));
+        }
         if (has_ev_out) {
 #pragma unroll
             for (int c = 0; c < 3; c++) (a.ev_out + cell)[c * n] = rhs[c];
@@ -518,7 +562,18 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, u
             atomicMax(&a.st->lte_bits, (unsigned long long)__double_as_longlong(b));
         }
     }
-    if (a.last_kind == BM_LAST_NONE || a.st == nullptr) return;
+    const int dg = stage_diag_active(a);
+    if (dg) {
+        // the block's diagnostic maxima into the running maxima of the set
+        __syncthreads();
+        if (tid == 0) {
+            const unsigned long long *dslot = stage_diag_slots();
+            if (dg & BM_DIAG_MXH) atomicMax(&a.st->mxh_acc, dslot[0]);
+            if (dg & BM_DIAG_DMDT) atomicMax(&a.st->dmdt_acc, dslot[1]);
+        }
+    }
+    const bool publish = dg && (a.diag & BM_DIAG_PUBLISH);
+    if ((a.last_kind == BM_LAST_NONE && !publish) || a.st == nullptr) return;
     __threadfence();
     __syncthreads();
     if (tid == 0) {
@@ -529,6 +584,17 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, u
     if (!is_last || tid != 0) return;
     __threadfence();
     volatile StepState *st = a.st;
+    if (publish) {
+        // the set's maxima become the values Get_mxh / Get_dmdt return; the request is served
+        if (dg & BM_DIAG_MXH) {
+            st->mxh = __longlong_as_double((long long)atomicExch(&a.st->mxh_acc, 0ull));
+            st->calc_mxh = 0;
+        }
+        if (dg & BM_DIAG_DMDT) {
+            st->dmdt = __longlong_as_double((long long)atomicExch(&a.st->dmdt_acc, 0ull));
+            st->calc_dmdt = 0;
+        }
+    }
     if (a.last_kind == BM_LAST_FINISH) {
         st->time = st->time + st->dT;
         st->stagetime = st->stagetime + st->dT;

@@ -293,6 +293,17 @@ int bm_compute_heff(bm_ctx *ctx, int mesh, double *H);
 int bm_run(bm_ctx *ctx, int steps, bm_stats *out);
 int bm_get_stats(bm_ctx *ctx, bm_stats *out);
 
+/* The torque and dm/dt diagnostics of the evaluators, replacing ODECommon_Base::Get_mxh / Get_dmdt
+ * (Boris/DiffEq_CommonBase_Get.cpp:7,19; reductions in Boris/DiffEqFM_EvalsLLGCUDA.cu:416-640 for
+ * RK4 and Boris/DiffEqFM_EvalsCUDA_RKDP54.cu:15-53,188-232 for RKDP54). mxh: the maximum over the
+ * cells of |M x Heff| / |M|^2 at the step's first evaluation; dmdt: the maximum of
+ * |M - M_step_start| / (dT GAMMA |M|^2) after its last stage (GAMMA = 2.212761569e5); both over the
+ * meshes whose grel is non-zero. As in the reference a call returns the value of the last step that
+ * computed it (0 before any) and asks the next step to compute it, so a value runs one step behind
+ * the call that asked for it. */
+int bm_get_mxh(bm_ctx *ctx, double *mxh);
+int bm_get_dmdt(bm_ctx *ctx, double *dmdt);
+
 /* Number of cells of a mesh and the FFT sizes its demag convolution uses. */
 int bm_mesh_info(bm_ctx *ctx, int mesh, int *n3, int *N3);
 

@@ -1561,6 +1561,10 @@ struct orc_solver {
     double es_t[6], es_a[6];
     int es_available;    /* the reference's ODECommon_Base::available: the previous step completed */
     int es_metres;       /* the speedup's self term on cellsizes in metres (DemagCUDA.cpp:39 as is) */
+    /* torque and dm/dt diagnostics (ODECommon_Base::Get_mxh / Get_dmdt, DiffEq_CommonBase_Get.cpp:7,19):
+       a request makes the next step compute them, which clears the request */
+    int calc_mxh, calc_dmdt;
+    double mxh, dmdt;
 };
 
 static int fft_size(int n) { return n > 1 ? 2 * n : 1; }
@@ -1794,6 +1798,68 @@ static inline void renorm(double *M, double Ms)
     M[0] *= f; M[1] *= f; M[2] *= f;
 }
 
+/* |M x H| / |M|^2 of one cell (DiffEqFM_Evals_RK4.cpp:78-79, DiffEqFM_EvalsCUDA_RKDP54.cu:31-32) */
+static inline double cell_mxh(const double *M, const double *H)
+{
+    double x[3] = {M[1] * H[2] - M[2] * H[1], M[2] * H[0] - M[0] * H[2], M[0] * H[1] - M[1] * H[0]};
+    double m2 = M[0] * M[0] + M[1] * M[1] + M[2] * M[2];
+    return sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]) / m2;
+}
+
+/* |M - M1| / (dT GAMMA |M|^2) of one cell after the step's last stage (DiffEqFM_Evals_RK4.cpp:191-199,
+   DiffEqFM_EvalsCUDA_RKDP54.cu:215-217) */
+static inline double cell_dmdt(const double *M, const double *M1, double dT)
+{
+    double d[3] = {M[0] - M1[0], M[1] - M1[1], M[2] - M1[2]};
+    double m2 = M[0] * M[0] + M[1] * M[1] + M[2] * M[2];
+    return sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / (dT * ORC_GAMMA * m2);
+}
+
+/* the maximum over the meshes whose grel is non-zero of cell_mxh at the current M and H (the
+   stage-0 reduction of the RK4 and RKDP54 evaluators) */
+static double max_mxh(orc_solver *s)
+{
+    double v = 0.0;
+    for (int q = 0; q < s->nmesh; q++) {
+        orc_mesh *m = &s->m[q];
+        if (m->d.grel == 0.0) continue;
+        for (int i = 0; i < m->n; i++) {
+            double c = cell_mxh(m->M + 3 * (size_t)i, m->H + 3 * (size_t)i);
+            if (c > v) v = c;
+        }
+    }
+    return v;
+}
+
+/* the maximum over the meshes whose grel is non-zero of cell_dmdt after the last stage */
+static double max_dmdt(orc_solver *s, double dT)
+{
+    double v = 0.0;
+    for (int q = 0; q < s->nmesh; q++) {
+        orc_mesh *m = &s->m[q];
+        if (m->d.grel == 0.0) continue;
+        for (int i = 0; i < m->n; i++) {
+            double c = cell_dmdt(m->M + 3 * (size_t)i, m->sM1 + 3 * (size_t)i, dT);
+            if (c > v) v = c;
+        }
+    }
+    return v;
+}
+
+int orc_solver_get_mxh(orc_solver *s, double *v)
+{
+    s->calc_mxh = 1;
+    if (v) *v = s->mxh;
+    return 0;
+}
+
+int orc_solver_get_dmdt(orc_solver *s, double *v)
+{
+    s->calc_dmdt = 1;
+    if (v) *v = s->dmdt;
+    return 0;
+}
+
 /* SetAdaptiveTimeStep (DiffEq_CommonBase_Iterate.cpp:15); returns 1 to accept */
 static int adaptive_dt(orc_solver *s, double lte)
 {
@@ -1937,6 +2003,10 @@ static void rk4_step(orc_solver *s)
     for (int stage = 0; stage < 4; stage++) {
         es_prepare(s, stage);
         update_all_fields(s);
+        if (stage == 0 && s->calc_mxh) {
+            s->mxh = max_mxh(s);
+            s->calc_mxh = 0;
+        }
         for (int q = 0; q < s->nmesh; q++) {
             orc_mesh *m = &s->m[q];
             const orc_mesh_desc *d = &m->d;
@@ -1957,6 +2027,10 @@ static void rk4_step(orc_solver *s)
             }
         }
     }
+    if (s->calc_dmdt) {
+        s->dmdt = max_dmdt(s, dT);
+        s->calc_dmdt = 0;
+    }
     s->time += dT;
     s->stagetime += dT;
     s->accepted++;
@@ -1968,6 +2042,10 @@ static int rkdp_attempt(orc_solver *s)
     /* evalStep 0: FSAL rhs, 4th-order prediction, lte (DiffEqFM_Evals_RKDP54.cpp:52-88) */
     es_prepare_dp(s, 0);
     update_all_fields(s);
+    if (s->calc_mxh) {
+        s->mxh = max_mxh(s);
+        s->calc_mxh = 0;
+    }
     double lte = 0.0;
     for (int q = 0; q < s->nmesh; q++) {
         orc_mesh *m = &s->m[q];
@@ -2039,6 +2117,10 @@ static int rkdp_attempt(orc_solver *s)
                 if (st == 5) renorm(m->M + o, m->Ms[i]);
             }
         }
+    }
+    if (s->calc_dmdt) {
+        s->dmdt = max_dmdt(s, dT);
+        s->calc_dmdt = 0;
     }
     s->time += dT;
     s->stagetime += dT;

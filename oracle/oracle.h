@@ -116,6 +116,12 @@ int orc_solver_set_field_hook(orc_solver *s, int mesh, orc_field_fn fn, void *us
 int orc_compute_heff(orc_solver *s, int mesh, double *H);
 /* advance until `steps` more steps are accepted */
 int orc_run(orc_solver *s, int steps, orc_stats *st);
+/* ODECommon_Base::Get_mxh / Get_dmdt (DiffEq_CommonBase_Get.cpp:7,19): the value of the last step
+ * that computed it (0 before any), and a request that the next step computes it: max over cells of
+ * |M x Heff| / |M|^2 at the step's first evaluation, and of |M - M_step_start| / (dT GAMMA |M|^2)
+ * after its last stage, over the meshes with grel != 0 */
+int orc_solver_get_mxh(orc_solver *s, double *v);
+int orc_solver_get_dmdt(orc_solver *s, double *v);
 void orc_solver_destroy(orc_solver *s);
 
 /* ---- multilayered convolution (SDemag multilayer mode) ----

@@ -104,6 +104,8 @@ def oracle():
         L.orc_solver_set_multilayer.argtypes = [P, DP, I, IP]
         L.orc_solver_set_evalspeedup.argtypes = [P, I]
         L.orc_solver_set_evalspeedup_self.argtypes = [P, I]
+        L.orc_solver_get_mxh.argtypes = [P, DP]
+        L.orc_solver_get_dmdt.argtypes = [P, DP]
         L.orc_selfdemag_metres.argtypes = [D, D, D, DP]
         L.orc_adjoint_rk4.argtypes = [ctypes.POINTER(MeshDesc), DP, DP, I, D, DP, DP, DP, DP]
         L.orc_solver_set_field_hook.argtypes = [P, I, P, P]
@@ -576,6 +578,18 @@ class OracleSolver:
         rc = oracle().orc_run(P(self.h), steps, ctypes.byref(st))
         assert rc == 0
         return {k: getattr(st, k) for k, _ in OrcStats._fields_}
+
+    def get_mxh(self):
+        """Get_mxh: the value of the last step that computed it; the next step computes it."""
+        v = ctypes.c_double()
+        assert oracle().orc_solver_get_mxh(P(self.h), ctypes.byref(v)) == 0
+        return v.value
+
+    def get_dmdt(self):
+        """Get_dmdt: the value of the last step that computed it; the next step computes it."""
+        v = ctypes.c_double()
+        assert oracle().orc_solver_get_dmdt(P(self.h), ctypes.byref(v)) == 0
+        return v.value
 
     def close(self):
         if self.h:
