@@ -96,8 +96,8 @@ REF_TIME_CAP = 150
 
 # DRAM traffic per cell of one launch of the roofline kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture on the half-size case, divided by its cells;
-# profiles/stage_film3d_512x512x8.md, profiles/zmid_ml_multilayer_stack3_512.md)
-TRAFFIC_PER_CELL = {("film3d", "stage"): 257.17e6 / (512 * 512 * 8),
+# profiles/stage_rx16_lo_film3d_512x512x8.md, profiles/zmid_ml_multilayer_stack3_512.md)
+TRAFFIC_PER_CELL = {("film3d", "stage"): (201.792e6 + 61.450496e6) / (512 * 512 * 8),
                     ("multilayer", "ml_zmid"): 383.30e6 / (512 * 512 + 256 * 256 * 2 + 512 * 512)}
 
 
