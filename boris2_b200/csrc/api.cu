@@ -123,6 +123,7 @@ struct BatchRec {
     size_t args_off, work_off;
     int nwork, nt;
     size_t smem;
+    int plain = 0;        // stage launch: every argument block is a plain stage update (stage_plain)
 };
 struct BatchPlan {
     bool collect = false;
@@ -1250,6 +1251,8 @@ int stage_batch_one(bm_ctx *c, int key, std::vector<StageArgs<T>> &v, int *count
         r.nwork = (int)work.size();
         r.nt = nt;
         r.smem = smem;
+        r.plain = key ? 1 : 0;
+        for (auto &a : v) if (!stage_plain(a)) r.plain = 0;
         bp.recs.push_back(r);
         return 0;
     }
@@ -1257,7 +1260,7 @@ int stage_batch_one(bm_ctx *c, int key, std::vector<StageArgs<T>> &v, int *count
     const BatchRec &r = bp.recs[bp.next++];
     const char *base = (const char *)bp.dbuf;
     CKL(launch_stage_batch<T>(r.key, (const StageArgs<T> *)(base + r.args_off), (const int2 *)(base + r.work_off), r.nwork,
-                              r.nt, r.smem, c->stream), "stage batch");
+                              r.nt, r.smem, c->stream, r.plain), "stage batch");
     (*count)++;
     return 0;
 }

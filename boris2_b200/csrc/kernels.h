@@ -225,8 +225,18 @@ template <typename T>
 int launch_yz_batch(int kind, int key, const YZArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem,
                     cudaStream_t s);
 // key 0: generic-length stage kernel; key LX: the radix-8 register kernel of that length
+// the plain stage update of the RK stages (SPEC 1 of the radix-16 and batched register stage kernels):
+// stage mode, exchange and demag on, the rhs and new M written, the new M's x transform; no saved
+// fields or states, no external field, no copy, no staging, no folded extrapolation
+template <typename T> inline bool stage_plain(const StageArgs<T> &a)
+{
+    return a.mode == BM_MODE_STAGE && !a.staged && !a.es_fold && !a.Hd && !a.Hsave && !a.Ysave && !a.copy_to && a.ev_out &&
+           a.Mout && a.do_xfwd && (a.modules & BM_MOD_DEMAG) && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
+}
+// plain: every argument block of the launch satisfies stage_plain (FP32 takes the SPEC 1 kernels)
 template <typename T>
-int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s);
+int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s,
+                       int plain = 0);
 int stage_reg_q(int LX, int xv = 0);   // threads per x line of the register stage kernel, variant xv (0: generic kernel)
 int launch_scalar_reset(StepState *st, cudaStream_t s);
 

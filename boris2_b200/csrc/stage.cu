@@ -408,10 +408,11 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             }
             T mxh[3] = {m[1] * H[2] - m[2] * H[1], m[2] * H[0] - m[0] * H[2], m[0] * H[1] - m[1] * H[0]};
             if (dg & BM_DIAG_MXH) {
-                // |M x Heff| / |M|^2 (DiffEqFM_EvalsCUDA_RKDP54.cu:31-32, DiffEqFM_EvalsLLGCUDA.cu:445-446)
-                const double x2 = (double)mxh[0] * mxh[0] + (double)mxh[1] * mxh[1] + (double)mxh[2] * mxh[2];
-                const double m2 = (double)m[0] * m[0] + (double)m[1] * m[1] + (double)m[2] * m[2];
-                atomicMax(&dslot[0], (unsigned long long)__double_as_longlong(sqrt(x2) / m2));
+                // |M x Heff| / |M|^2 (DiffEqFM_EvalsCUDA_RKDP54.cu:31-32, DiffEqFM_EvalsLLGCUDA.cu:445-446),
+                // in the stage's precision as the reference's reduction kernels compute it
+                const T x2 = mxh[0] * mxh[0] + mxh[1] * mxh[1] + mxh[2] * mxh[2];
+                const T m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+                atomicMax(&dslot[0], (unsigned long long)__double_as_longlong((double)(sqrt(x2) / m2)));
             }
             T mu[3] = {m[0] * iMs, m[1] * iMs, m[2] * iMs};
             T mmxh[3] = {mu[1] * mxh[2] - mu[2] * mxh[1], mu[2] * mxh[0] - mu[0] * mxh[2], mu[0] * mxh[1] - mu[1] * mxh[0]};
@@ -502,14 +503,14 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         if (dg & BM_DIAG_DMDT) {
             // |M - M_start| / (dT GAMMA |M|^2) after the last stage (DiffEqFM_EvalsLLGCUDA.cu:583-584,
             // DiffEqFM_EvalsCUDA_RKDP54.cu:216-217); the step base is read before this cell's M is written
-            double d2 = 0.0, m2 = 0.0;
+            T d2 = 0, m2 = 0;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const double d = (double)mn[c] - (double)acc.mb(r, c, x, cell);
+                const T d = mn[c] - acc.mb(r, c, x, cell);
                 d2 += d * d;
-                m2 += (double)mn[c] * mn[c];
+                m2 += mn[c] * mn[c];
             }
-            atomicMax(&dslot[1], (unsigned long long)__double_as_longlong(sqrt(d2) / (dT * BM_GAMMA * m2)));
+            atomicMax(&dslot[1], (unsigned long long)__double_as_longlong((double)sqrt(d2) / (dT * BM_GAMMA * (double)m2)));
         }
         if (has_ev_out) {
 #pragma unroll
@@ -1115,24 +1116,16 @@ __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX16_LO_MAXNREG_F) k_stage
     stage_reg_body<T, LX, 2, SPEC>(a, blockIdx.x, gridDim.x);
 }
 
-// the plain stage update of the RK stages (the radix-16 kernels' SPEC 1): stage mode, exchange and
-// demag on, the rhs and new M written, the new M's x transform; no saved fields or states, no
-// external field, no copy, no staging, no folded extrapolation
-template <typename T> static bool stage_plain(const StageArgs<T> &a)
-{
-    return a.mode == BM_MODE_STAGE && !a.staged && !a.es_fold && !a.Hd && !a.Hsave && !a.Ysave && !a.copy_to && a.ev_out &&
-           a.Mout && a.do_xfwd && (a.modules & BM_MOD_DEMAG) && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
-}
 
 // many meshes with the same x length in one launch (radix-8 transform): work item (mesh, row
 // block); the error-norm maximum and the step bookkeeping follow k_stage_batch
-template <typename T, int LX>
+template <typename T, int LX, int SPEC = 0>
 __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx_batch(const StageArgs<T> *__restrict__ args,
                                                                          const int2 *__restrict__ work, int nwork)
 {
     if (stage_gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
     const int2 it = work[blockIdx.x];
-    stage_reg_body<T, LX, 1>(args[it.x], it.y, (unsigned int)nwork);
+    stage_reg_body<T, LX, 1, SPEC>(args[it.x], it.y, (unsigned int)nwork);
 }
 
 template <typename T, int LX, int XV>
@@ -1242,55 +1235,68 @@ template int launch_stage<float>(const StageArgs<float> &, cudaStream_t);
 template int launch_stage<double>(const StageArgs<double> &, cudaStream_t);
 
 // radix-16 variant (x lengths 256 .. 1024)
-template <typename T, int LX>
+template <typename T, int LX, int SPEC = 0>
 __global__ void __maxnreg__(sizeof(T) == 8 ? 128 : BM_RX_MAXNREG_F) k_stage_rx16_batch(const StageArgs<T> *__restrict__ args,
                                                                                        const int2 *__restrict__ work, int nwork)
 {
     if (stage_gated_out<T>(args[0].st, args[0].gate) || (int)blockIdx.x >= nwork) return;
     const int2 it = work[blockIdx.x];
-    stage_reg_body<T, LX, 2>(args[it.x], it.y, (unsigned int)nwork);
+    stage_reg_body<T, LX, 2, SPEC>(args[it.x], it.y, (unsigned int)nwork);
 }
 
-template <typename T, int LX>
-static int launch_stage_rx_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+template <typename T, int LX, int SPEC>
+static int launch_stage_rx_batch_s(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
 {
     if constexpr (LX >= 256 && (LX % 3) != 0) {
         if (smem > BM_SMEM_DEFAULT_SAFE) {
-            cudaError_t e = cudaFuncSetAttribute(k_stage_rx16_batch<T, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+            cudaError_t e = cudaFuncSetAttribute(k_stage_rx16_batch<T, LX, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 BM_SMEM_CAP);
             if (e != cudaSuccess) return 2000 + (int)e;
         }
-        k_stage_rx16_batch<T, LX><<<nwork, nt, smem, s>>>(dargs, dwork, nwork);
+        k_stage_rx16_batch<T, LX, SPEC><<<nwork, nt, smem, s>>>(dargs, dwork, nwork);
         return (int)cudaGetLastError();
     }
     if (smem > BM_SMEM_DEFAULT_SAFE) {
-        cudaError_t e = cudaFuncSetAttribute(k_stage_rx_batch<T, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
+        cudaError_t e = cudaFuncSetAttribute(k_stage_rx_batch<T, LX, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return (int)e;
     }
-    k_stage_rx_batch<T, LX><<<nwork, nt, smem, s>>>(dargs, dwork, nwork);
+    k_stage_rx_batch<T, LX, SPEC><<<nwork, nt, smem, s>>>(dargs, dwork, nwork);
     return (int)cudaGetLastError();
 }
 
+// the plain-stage instantiation for FP32 launches whose argument blocks are all plain (stage_plain)
+template <typename T, int LX>
+static int launch_stage_rx_batch(const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s,
+                                 int plain)
+{
+    if constexpr (sizeof(T) == 4) {
+        if (plain) return launch_stage_rx_batch_s<T, LX, 1>(dargs, dwork, nwork, nt, smem, s);
+    }
+    return launch_stage_rx_batch_s<T, LX, 0>(dargs, dwork, nwork, nt, smem, s);
+}
+
 template <typename T>
-int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s)
+int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s,
+                       int plain)
 {
     if (nwork < 1) return 0;
     if (nt > bm_lb<T>::v || nt < 32) return 211;
     if (smem > 200 * 1024) return 212;
     switch (key) {
     case 0: break;
-    case 16: return launch_stage_rx_batch<T, 16>(dargs, dwork, nwork, nt, smem, s);
-    case 32: return launch_stage_rx_batch<T, 32>(dargs, dwork, nwork, nt, smem, s);
-    case 64: return launch_stage_rx_batch<T, 64>(dargs, dwork, nwork, nt, smem, s);
-    case 128: return launch_stage_rx_batch<T, 128>(dargs, dwork, nwork, nt, smem, s);
-    case 256: return launch_stage_rx_batch<T, 256>(dargs, dwork, nwork, nt, smem, s);
-    case 512: return launch_stage_rx_batch<T, 512>(dargs, dwork, nwork, nt, smem, s);
-    case 1024: return launch_stage_rx_batch<T, 1024>(dargs, dwork, nwork, nt, smem, s);
-    case 24: return launch_stage_rx_batch<T, 24>(dargs, dwork, nwork, nt, smem, s);
-    case 48: return launch_stage_rx_batch<T, 48>(dargs, dwork, nwork, nt, smem, s);
-    case 96: return launch_stage_rx_batch<T, 96>(dargs, dwork, nwork, nt, smem, s);
-    case 192: return launch_stage_rx_batch<T, 192>(dargs, dwork, nwork, nt, smem, s);
-    case 384: return launch_stage_rx_batch<T, 384>(dargs, dwork, nwork, nt, smem, s);
-    case 768: return launch_stage_rx_batch<T, 768>(dargs, dwork, nwork, nt, smem, s);
+    case 16: return launch_stage_rx_batch<T, 16>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 32: return launch_stage_rx_batch<T, 32>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 64: return launch_stage_rx_batch<T, 64>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 128: return launch_stage_rx_batch<T, 128>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 256: return launch_stage_rx_batch<T, 256>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 512: return launch_stage_rx_batch<T, 512>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 1024: return launch_stage_rx_batch<T, 1024>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 24: return launch_stage_rx_batch<T, 24>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 48: return launch_stage_rx_batch<T, 48>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 96: return launch_stage_rx_batch<T, 96>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 192: return launch_stage_rx_batch<T, 192>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 384: return launch_stage_rx_batch<T, 384>(dargs, dwork, nwork, nt, smem, s, plain);
+    case 768: return launch_stage_rx_batch<T, 768>(dargs, dwork, nwork, nt, smem, s, plain);
     default: return 213;
     }
     if (smem > BM_SMEM_DEFAULT_SAFE) {
@@ -1301,5 +1307,5 @@ int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, in
     return (int)cudaGetLastError();
 }
 
-template int launch_stage_batch<float>(int, const StageArgs<float> *, const int2 *, int, int, size_t, cudaStream_t);
-template int launch_stage_batch<double>(int, const StageArgs<double> *, const int2 *, int, int, size_t, cudaStream_t);
+template int launch_stage_batch<float>(int, const StageArgs<float> *, const int2 *, int, int, size_t, cudaStream_t, int);
+template int launch_stage_batch<double>(int, const StageArgs<double> *, const int2 *, int, int, size_t, cudaStream_t, int);
