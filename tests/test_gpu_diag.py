@@ -74,3 +74,39 @@ def test_diag_meshes(bm, evaluation, batched):
     s.run(1); c.run(1)
     _check(s, c, 1e-9)
     s.close(); c.close()
+
+
+@pytest.mark.parametrize("evaluation", ["RK4", "RKDP54"])
+def test_diag_multilayer_stack(bm, evaluation):
+    """The diagnostics over the meshes of a multilayered convolution: Heff carries the demag field the
+    transfer brings back from the common grid."""
+    from test_gpu_ml import STACK3, MS3
+    descs = []
+    for q, (m, Ms) in enumerate(zip(STACK3, MS3)):
+        d = dict(n=m[0], h=m[1], Ms=Ms, A=1.5e-11, alpha=0.05, modules=1 | 2 | 16, Ha=(2e4, 0, 0))
+        if q == 2:
+            d.update(K1=3e5, modules=1 | 2 | 8 | 16)
+        descs.append(d)
+    dt = 5e-14
+    ev = EVALS[evaluation]
+    kw = dict(tol=1e-5, dT_incr=2.0, dT_min=1e-15, dT_max=3e-12) if ev == 1 else {}
+    s = OracleSolver(descs, evaluation=ev, dt=dt, **kw)
+    s.multilayer([m[2] for m in STACK3], mode=0)
+    c = bm.Context(precision=bm.FP64)
+    for q, (m, d) in enumerate(zip(STACK3, descs)):
+        c.add_mesh(m[0], m[1], m[2])
+        c.set_material(q, Ms=d["Ms"], A=d["A"], alpha=d["alpha"], K1=d.get("K1", 0.0), ea=(0, 0, 1))
+        c.set_modules(q, d["modules"])
+        c.set_field(q, d["Ha"])
+    c.multiconvolution(0)
+    c.setode(evaluation, dt)
+    if ev == 1:
+        c.astepctrl(1e-5, 2.0, 1e-15, 3e-12)
+    for q, d in enumerate(descs):
+        M = tilted_z(int(np.prod(d["n"])), seed=90 + q, Ms=d["Ms"])
+        s.set_m(M, q)
+        c.set_m(M, q)
+    s.get_mxh(); s.get_dmdt(); c.get_mxh(); c.get_dmdt()
+    s.run(2); c.run(2)
+    _check(s, c, 1e-9)
+    s.close(); c.close()
