@@ -233,6 +233,19 @@ template <typename T> inline bool stage_plain(const StageArgs<T> &a)
     return a.mode == BM_MODE_STAGE && !a.staged && !a.es_fold && !a.Hd && !a.Hsave && !a.Ysave && !a.copy_to && a.ev_out &&
            a.Mout && a.do_xfwd && (a.modules & BM_MOD_DEMAG) && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
 }
+// the plain RKDP54 error estimate (SPEC 2): the rhs written, no new M, no forward transform, fields on
+template <typename T> inline bool stage_lte_plain(const StageArgs<T> &a)
+{
+    return a.mode == BM_MODE_LTE && !a.staged && !a.es_fold && !a.Hd && !a.Hsave && !a.Ysave && !a.copy_to && a.ev_out &&
+           !a.Mout && !a.do_xfwd && (a.modules & BM_MOD_DEMAG) && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI));
+}
+// the plain advance of the base state (SPEC 3): no fields, the base copied, the new M written and
+// transformed, no rhs output, no renormalisation
+template <typename T> inline bool stage_adv_plain(const StageArgs<T> &a)
+{
+    return a.mode == BM_MODE_UPDATE && !a.staged && !a.es_fold && !a.Hd && !a.Hsave && !a.Ysave && a.copy_to && a.Mout &&
+           a.do_xfwd && !a.ev_out && !a.renorm;
+}
 // plain: every argument block of the launch satisfies stage_plain (FP32 takes the SPEC 1 kernels)
 template <typename T>
 int launch_stage_batch(int key, const StageArgs<T> *dargs, const int2 *dwork, int nwork, int nt, size_t smem, cudaStream_t s,

@@ -225,24 +225,27 @@ template <typename T> __device__ __forceinline__ int stage_diag_active(const Sta
 }
 
 // SPEC 1: the plain stage update (stage_plain on the host): mode, the outputs written and the demag
-// and exchange terms are compile-time, so their run-time checks leave the per-cell loop
+// and exchange terms are compile-time, so their run-time checks leave the per-cell loop; SPEC 2 the
+// plain RKDP54 error estimate (stage_lte_plain), SPEC 3 the plain advance of the base state
+// (stage_adv_plain), likewise
 template <typename T, int SPEC = 0, typename AddrF, typename Acc>
 __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, int LSP, AddrF addr, int r0, double &lmax,
                                             const Acc &acc)
 {
-    constexpr bool PS = SPEC == 1;
+    constexpr bool PS = SPEC == 1, PL = SPEC == 2, PA = SPEC == 3, SP = SPEC != 0;
     const int nx = a.nx, ny = a.ny, nz = a.nz, rpb = a.rpb;
     const int nrows = ny * nz;
     const int tid = threadIdx.x, nt = blockDim.x;
     const long long n = a.n;
-    const int mode = PS ? BM_MODE_STAGE : a.mode;
-    const T *Hd = PS ? nullptr : a.Hd;
-    T *Hsave = PS ? nullptr : a.Hsave;
-    T *Ysave = PS ? nullptr : a.Ysave;
-    T *copy_to = PS ? nullptr : a.copy_to;
-    const bool has_ev_out = PS || a.ev_out, has_Mout = PS || a.Mout, do_xfwd = PS || a.do_xfwd;
-    const bool fields = PS || (mode != BM_MODE_UPDATE);
-    const bool demag = PS || (fields && (a.modules & BM_MOD_DEMAG));
+    const int mode = PS ? BM_MODE_STAGE : PL ? BM_MODE_LTE : PA ? BM_MODE_UPDATE : a.mode;
+    const T *Hd = SP ? nullptr : a.Hd;
+    T *Hsave = SP ? nullptr : a.Hsave;
+    T *Ysave = SP ? nullptr : a.Ysave;
+    T *copy_to = (PS || PL) ? nullptr : a.copy_to;
+    const bool has_ev_out = (PS || PL) || (!PA && a.ev_out), has_Mout = (PS || PA) || (!PL && a.Mout);
+    const bool do_xfwd = (PS || PA) || (!PL && a.do_xfwd);
+    const bool fields = (PS || PL) || (!PA && mode != BM_MODE_UPDATE);
+    const bool demag = (PS || PL) || (!PA && fields && (a.modules & BM_MOD_DEMAG));
     const double dT = a.st ? *((volatile double *)&a.st->dT) : 0.0;
     T Ha[3] = {0, 0, 0};
     if (fields && (a.modules & BM_MOD_ZEEMAN) && a.Ha && a.nHa > 0) {
@@ -258,7 +261,7 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
         }
         Ha[0] = (T)a.Ha[3 * hi]; Ha[1] = (T)a.Ha[3 * hi + 1]; Ha[2] = (T)a.Ha[3 * hi + 2];
     }
-    const bool exch = PS || (fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI)));
+    const bool exch = (PS || PL) || (!PA && fields && (a.modules & (BM_MOD_EXCH | BM_MOD_IDMI)));
     const bool idmi = (a.modules & BM_MOD_IDMI) != 0;
     const bool zflat = (nz == 1);
     // torque / dm/dt diagnostics of this launch (meshes with grel = 0 take no part, as in the
@@ -494,7 +497,7 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
 #pragma unroll
             for (int c = 0; c < 3; c++) (Ysave + cell)[c * n] = mn[c];
         }
-        if (a.renorm) {
+        if (!PA && a.renorm) {
             T f = Ms / sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
             mn[0] *= f; mn[1] *= f; mn[2] *= f;
             // the step's new state must be finite (the sum is non-finite if any component is)
@@ -550,7 +553,7 @@ __device__ __forceinline__ void stage_tail(const StageArgs<T> &a, double lmax, u
     __shared__ double red[32];
     __shared__ int is_last;
     const int tid = threadIdx.x, nt = blockDim.x;
-    if (SPEC != 1 && a.mode == BM_MODE_LTE) {
+    if (SPEC == 2 || (SPEC == 0 && a.mode == BM_MODE_LTE)) {
         for (int o = 16; o > 0; o >>= 1) {
             double v = __shfl_xor_sync(0xffffffffu, lmax, o);
             if (v > lmax) lmax = v;
@@ -974,7 +977,7 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
     const int qc = rpb == 1 ? q : q / rpb, qr = q - qc * rpb;
     const bool qact = (q < 3 * rpb) && (r0 + qr < nrows);
     cpx<T> *line = sm + (q < 3 * rpb ? q : 0) * LSP;
-    const bool demag = SPEC == 1 || ((a.mode != BM_MODE_UPDATE) && (a.modules & BM_MOD_DEMAG));
+    const bool demag = SPEC == 1 || SPEC == 2 || (SPEC == 0 && (a.mode != BM_MODE_UPDATE) && (a.modules & BM_MOD_DEMAG));
     const int half = (a.nx + 1) >> 1;   // packed elements that carry mesh cells
     // group 1: the spectrum rows
     if (demag && qact) {
@@ -1040,7 +1043,7 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
     if (demag) {
         cp_async_wait_group<1>();
         __syncthreads();
-        if (SPEC != 1 && a.es_fold) {
+        if (SPEC == 0 && a.es_fold) {
             // evaluation speedup: an extrapolating evaluation turns the row of X[M] into the
             // extrapolated field's row (the k_es_extrap sum, formed here so the spectrum is not
             // written and read back); kept out of line so the hot path's registers are untouched
@@ -1056,9 +1059,9 @@ __device__ __forceinline__ void stage_reg_body(const StageArgs<T> &a, int bid, u
     cp_async_wait_group<0>();
     __syncthreads();
     double lmax = 0.0;
-    if (SPEC != 1 && a.staged) stage_cells<T>(a, sm, LSP, A, r0, lmax, st);
+    if (SPEC == 0 && a.staged) stage_cells<T>(a, sm, LSP, A, r0, lmax, st);
     else stage_cells<T, SPEC>(a, sm, LSP, A, r0, lmax, AccGlobal<T>(a));
-    if (SPEC == 1 || a.do_xfwd) {
+    if (SPEC == 1 || SPEC == 3 || (SPEC == 0 && a.do_xfwd)) {
         for (int idx = tid; idx < 3 * rpb * (LX / 2); idx += blockDim.x) {
             int qq = idx / (LX / 2), mm = idx - qq * (LX / 2);
             if (mm >= half) sm[qq * LSP + A(mm)] = mk<T>(0, 0);
@@ -1147,8 +1150,15 @@ static int launch_stage_reg(const StageArgs<T> &a, cudaStream_t s)
     void (*kern)(StageArgs<T>);
     if constexpr (XV == 0) kern = k_stage_reg<T, LX>;
     else if constexpr (XV == 1) kern = k_stage_rx<T, LX>;
-    else if constexpr (XV == 2) kern = stage_plain(b) ? k_stage_rx16<T, LX, 1> : k_stage_rx16<T, LX, 0>;
-    else kern = stage_plain(b) ? k_stage_rx16_lo<T, LX, 1> : k_stage_rx16_lo<T, LX, 0>;
+    else {
+        const int sp = stage_plain(b) ? 1 : stage_lte_plain(b) ? 2 : stage_adv_plain(b) ? 3 : 0;
+        if constexpr (XV == 2)
+            kern = sp == 1 ? k_stage_rx16<T, LX, 1> : sp == 2 ? k_stage_rx16<T, LX, 2> : sp == 3 ? k_stage_rx16<T, LX, 3>
+                                                                                          : k_stage_rx16<T, LX, 0>;
+        else
+            kern = sp == 1 ? k_stage_rx16_lo<T, LX, 1> : sp == 2 ? k_stage_rx16_lo<T, LX, 2>
+                         : sp == 3 ? k_stage_rx16_lo<T, LX, 3> : k_stage_rx16_lo<T, LX, 0>;
+    }
     if (smem > BM_SMEM_DEFAULT_SAFE) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_SMEM_CAP);
         if (e != cudaSuccess) return 2000 + (int)e;   // the shared-memory ceiling was refused
