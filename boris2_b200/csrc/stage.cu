@@ -196,6 +196,23 @@ __device__ __forceinline__ void ev_acc(const Acc &acc, const T *cev, int r, int 
         for (int i = 0; i < NEV; i++) sum[c] += cev[i] * acc.ev(i, r, c, x, cell);
 }
 
+// sum_{i < NEV} c1[i] * ev_i[c] and sum_{i < NEV} c2[i] * ev_i[c] in FP64, i ascending, each ev_i
+// loaded once (the RKDP54 error estimate's 4th-order prediction and embedded 5th-order solution)
+template <int NEV, typename Acc>
+__device__ __forceinline__ void ev_sum2_d(const Acc &acc, const double *c1, const double *c2, int r, int c, int x,
+                                          long long cell, double &s1, double &s2)
+{
+    double a1 = 0.0, a2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < NEV; i++) {
+        const double e = (double)acc.ev(i, r, c, x, cell);
+        a1 += c1[i] * e;
+        a2 += c2[i] * e;
+    }
+    s1 = a1;
+    s2 = a2;
+}
+
 // sum_{i < NEV} cev[i] * ev_i[c] in FP64 (error estimate)
 template <int NEV, typename Acc>
 __device__ __forceinline__ double ev_sum_d(const Acc &acc, const double *cev, int r, int c, int x, long long cell)
@@ -430,6 +447,11 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
             for (int c = 0; c < 3; c++) {
                 sb[c] = 0.0;
                 sa[c] = 0.0;
+                if (a.lte_embedded && nev == 5) {
+                    // both weightings of the five stage evaluations from one load of each
+                    ev_sum2_d<5>(acc, a.cev, a.cev5, r, c, x, cell, sb[c], sa[c]);
+                    continue;
+                }
                 switch (nev) {   // block-uniform: unrolled sums without predicated loads
                 case 6: sb[c] = ev_sum_d<6>(acc, a.cev, r, c, x, cell); break;
                 case 5: sb[c] = ev_sum_d<5>(acc, a.cev, r, c, x, cell); break;
@@ -439,7 +461,6 @@ __device__ __forceinline__ void stage_cells(const StageArgs<T> &a, cpx<T> *sm, i
                 case 1: sb[c] = ev_sum_d<1>(acc, a.cev, r, c, x, cell); break;
                 default: break;
                 }
-                if (a.lte_embedded && nev == 5) sa[c] = ev_sum_d<5>(acc, a.cev5, r, c, x, cell);
             }
             if (a.lte_embedded) {
                 // the step's 5th-order solution recomputed in FP64 from its base and stage rhs,
